@@ -1,0 +1,219 @@
+/*
+ * owl_ssg.h -- C ABI of the B200 standard-staggered-grid (SSG) finite-difference
+ * solver: forward modelling and adjoint-state FWI gradients for the media of
+ * OWL's SSG solvers.
+ *
+ * The ABI replaces the type-bound procedures of OWL's solver objects:
+ *   wave_solver_acoustic_iso_2d%forward / %adjoint
+ *       src/solver/acoustic_iso_2d/interface.f90:30-60
+ *   wave_solver_acoustic_iso_3d%forward / %adjoint
+ *       src/solver/acoustic_iso_3d/interface.f90:30-60
+ *   wave_solver_elastic_vhtiort_2d%forward / %adjoint
+ *       src/solver/elastic_vhtiort_2d/interface.f90:29-77
+ * One handle holds what the Fortran module variables hold there (padded model,
+ * CFS-PML coefficients, wavefields), but per handle, so handles are re-entrant.
+ *
+ * Conventions shared with the reference:
+ *   - model and gradient arrays are float32 (nz, nx) or (nz, ny, nx) with z
+ *     fastest, i.e. the raw layout of OWL's model files
+ *     (src/lib/module_model.f90:237-334) and of grad_<name>.bin outputs
+ *     (src/inverse/2d/module_gradient.f90:454-468);
+ *   - source / receiver node indices gx, gz, hx, hz and the 9-tap Kaiser
+ *     windowed sinc vectors are exactly those of prepare_geometry
+ *     (src/lib/module_source_receiver.f90:556-830), 1-based;
+ *   - the source time function is the prepared STF (prepare_stf,
+ *     src/lib/module_source_receiver.f90:1002-1130), injected from step nbeg.
+ *
+ * Every entry point returns OWL_OK (0) or a negative status; it never aborts
+ * the process. owl_last_error() returns a thread-local message for the last
+ * failure. Calls on one handle are not thread safe; distinct handles are.
+ */
+#ifndef OWL_SSG_H
+#define OWL_SSG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OWL_SSG_ABI_VERSION 1
+
+/* status codes */
+#define OWL_OK 0
+#define OWL_ERR_INVALID (-1)     /* bad argument or descriptor */
+#define OWL_ERR_CUDA (-2)        /* CUDA runtime error */
+#define OWL_ERR_OOM (-3)         /* device allocation failed */
+#define OWL_ERR_NONFINITE (-4)   /* NaN / Inf detected in a wavefield */
+#define OWL_ERR_UNSTABLE (-5)    /* dt above the CFL bound and no adjustment allowed */
+#define OWL_ERR_TIMEOUT (-6)     /* a bounded device wait gave up */
+#define OWL_ERR_UNSUPPORTED (-7) /* medium / option not built */
+#define OWL_ERR_NO_DEVICE (-8)   /* no usable CUDA device */
+
+/* media (which_medium in OWL's parameter files, src/lib/module_parameters.f90:397) */
+#define OWL_ACOUSTIC_ISO_2D 1
+#define OWL_ACOUSTIC_ISO_3D 2
+#define OWL_ELASTIC_VHTIORT_2D 3
+#define OWL_ELASTIC_VHTIORT_3D 4
+
+/* source mechanisms (src/lib/module_source_receiver.f90:66-83) */
+#define OWL_SRC_EXPLOSION 0
+#define OWL_SRC_FORCE 1
+#define OWL_SRC_MT 2
+
+/* memory kinds of the data buffers passed to forward / gradient */
+#define OWL_MEM_HOST 0
+#define OWL_MEM_DEVICE 1
+
+/* checkpoint storage precision */
+#define OWL_CKPT_FP32 0
+#define OWL_CKPT_FP16 1
+#define OWL_CKPT_BF16 2
+
+/* adjoint-source kinds for owl_ssg_gradient */
+#define OWL_ADJ_L2_RESIDUAL 0 /* adj = syn - obs, misfit = sum (obs - syn)^2 */
+#define OWL_ADJ_GIVEN 1       /* adj given directly (the reference's adjoint SU) */
+
+typedef struct owl_ssg owl_ssg;
+
+/* Solver descriptor: the scalar fields of wave_solver_* (interface.f90:32-40). */
+typedef struct {
+    int medium;          /* OWL_ACOUSTIC_ISO_2D, ... */
+    int nx, ny, nz;      /* model cells; ny = 1 in 2D */
+    float dx, dy, dz;    /* grid spacing (m) */
+    float ox, oy, oz;    /* model origin (m) */
+    int pml;             /* CFS-PML width in cells, outside the model */
+    int fdhalf;          /* FD half-width: 4 (8th order) or 8 (16th order) */
+    int free_surface;    /* 1: free surface on the top face */
+    float dt;            /* time step (s) */
+    int nt;              /* number of time steps */
+    float f0_max;        /* max source f0 (Hz): PML alphamax = pi * f0_max */
+    int max_shots;       /* capacity of one batched launch (>= 1) */
+    int allow_dt_adjust; /* 0: dt above the CFL bound is OWL_ERR_UNSTABLE */
+} owl_ssg_desc;
+
+/* One source after prepare_geometry / prepare_stf. */
+typedef struct {
+    int mechanism;                  /* OWL_SRC_* */
+    int gx, gy, gz;                 /* nearest integer node, 1-based */
+    int hx, hy, hz;                 /* nearest half node, 1-based */
+    float interp_ix[9], interp_iy[9], interp_iz[9];
+    float interp_hx[9], interp_hy[9], interp_hz[9];
+    float amp;                      /* amplitude */
+    float polar, azimuth;           /* force direction, radians */
+    float mt[6];                    /* moment tensor xx, yy, zz, xy, xz, yz */
+    int nbeg;                       /* first step of injection (1-based) = nint(t0/dt)+1 */
+    int nt_stf;                     /* samples in stf */
+    const float *stf;               /* prepared source time function (host) */
+} owl_source;
+
+/* One receiver after prepare_geometry. weight == 0 disables the trace. */
+typedef struct {
+    int gx, gy, gz;
+    int hx, hy, hz;
+    float interp_ix[9], interp_iy[9], interp_iz[9];
+    float interp_hx[9], interp_hy[9], interp_hz[9];
+    float weight;
+} owl_receiver;
+
+/* One shot (one geometry file of OWL). */
+typedef struct {
+    int id;
+    int nsrc;
+    const owl_source *src;
+    int nrec;
+    const owl_receiver *rec;
+} owl_shot;
+
+/* Per-call execution options. Zero-initialised means defaults. */
+typedef struct {
+    int shots_per_launch;     /* shots per batched launch; 0 = max_shots; 1 = plain per-shot path */
+    int checkpoint_interval;  /* k of every-k-step checkpoints; 0 = 50 */
+    int checkpoint_precision; /* OWL_CKPT_* */
+    int use_graph;            /* 1: capture the time loop in CUDA graphs (default when 0 is -1) */
+    int shots_per_cta;        /* shots handled per CTA; 0 = autotuned */
+    int tile_x, tile_z;       /* CTA tile; 0 = autotuned */
+    int check_every;          /* NaN/Inf check interval in steps; 0 = never */
+} owl_run_opts;
+
+/* Filled by forward / gradient. */
+typedef struct {
+    double elapsed_ms;        /* device time of the whole call (CUDA events) */
+    double steps_cell_updates;/* padded cells x steps x shots x stencil passes */
+    long long gpu_launches;   /* kernels launched by the library in the call */
+    float dt_used;
+    float dt_stable;
+    int shots_per_cta;
+    int tile_x, tile_z;
+    int batches;
+} owl_run_info;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+
+/* Replaces prepare_modeling + compute_cfspml_damping_coef + alloc_*_wavefield
+ * (src/solver/acoustic_iso_2d/module_vars.f90:90-208,
+ *  src/solver/acoustic_iso_2d/module_cfspml.f90:61-133). */
+int owl_ssg_create(const owl_ssg_desc *desc, owl_ssg **out);
+
+/* Sets the model. Parameters (each a (nz[,ny],nx) z-fastest float32 host array):
+ *   acoustic: vp, rho                                     (nparam = 2)
+ *   elastic 2D: vp, vs, rho, epsilon, delta (Thomsen VTI) (nparam = 5)
+ *   elastic 3D: c11,c12,c13,c22,c23,c33,c44,c55,c66, rho  (nparam = 10)
+ * Replaces the transpose / pad_array / bk = rho*vp^2 part of prepare_modeling
+ * (src/solver/acoustic_iso_2d/module_vars.f90:109-115). */
+int owl_ssg_set_model(owl_ssg *h, int nparam, const float *const *fields);
+
+/* Forward modelling of nshots shots (batched by opts->shots_per_launch).
+ * Replaces compute_forward (src/solver/acoustic_iso_2d/submodule_forward_modeling.f90:31-132).
+ * seis: per shot, ncomp x nrec x nt float32 (trace-major, the SU trace order),
+ * shots concatenated; ncomp = 1 (p) for acoustic, 2 (vx, vz) for elastic 2D. */
+int owl_ssg_forward(owl_ssg *h, int nshots, const owl_shot *shots,
+                    const owl_run_opts *opts, float *seis, int mem_kind,
+                    owl_run_info *info);
+
+/* Adjoint-state gradient. Replaces the per-shot pipeline of compute_gradient_shots
+ * (src/inverse/2d/module_gradient.f90:114-135,323-358): forward, adjoint source
+ * (compute_adjsrc_waveform, src/inverse/module_inversion_adjoint_source.f90:371-383),
+ * adjoint propagation and imaging (src/solver/acoustic_iso_2d/submodule_fwi_gradient.f90:31-269),
+ * stacked over the shots. The adjoint is the exact discrete transpose of the
+ * forward with every-k-step checkpoints and segment recomputation.
+ *   data: OWL_ADJ_L2_RESIDUAL -> observed seismograms; OWL_ADJ_GIVEN -> adjoint source;
+ *         same layout as seis in owl_ssg_forward.
+ *   misfit: nshots doubles (may be NULL), sum over traces of (obs - syn)^2.
+ *   grad: nparam x (nz[,ny],nx) float32, z fastest, of J = 0.5 * misfit
+ *         (the reference's adjoint source syn - obs), w.r.t. the model parameters
+ *         in the order of owl_ssg_set_model.
+ *   seis_out: optional synthetic seismograms (may be NULL). */
+int owl_ssg_gradient(owl_ssg *h, int nshots, const owl_shot *shots,
+                     const float *data, int adj_kind, const owl_run_opts *opts,
+                     double *misfit, float *grad, float *seis_out, int mem_kind,
+                     owl_run_info *info);
+
+/* Gradient of the same J w.r.t. each source's STF samples (the adjoint of
+ * add_source, src/solver/acoustic_iso_2d/module_wavefield.f90:192-263):
+ * stf_grad holds, per shot and source, nt floats (step index 1..nt). Used for
+ * source estimation and for the source-side dot-product test. */
+int owl_ssg_source_gradient(owl_ssg *h, int nshots, const owl_shot *shots,
+                            const float *adj, const owl_run_opts *opts,
+                            float *stf_grad, int mem_kind, owl_run_info *info);
+
+void owl_ssg_destroy(owl_ssg *h);
+
+/* ---- queries ------------------------------------------------------------ */
+
+const char *owl_last_error(void);
+int owl_ssg_abi_version(void);
+/* dt_stable of the current model (module_vars.f90:121-125); 0 before set_model. */
+float owl_ssg_dt_stable(const owl_ssg *h);
+/* number of parameters and seismogram components of a medium */
+int owl_ssg_nparam(int medium);
+int owl_ssg_ncomp(int medium);
+/* 1 if the CUDA kernels for sm_100a are present and a device is usable */
+int owl_ssg_device_ok(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OWL_SSG_H */

@@ -1,0 +1,7 @@
+"""CPU oracle: a C++ restatement of OWL's SSG loops (see oracle_ac2d.cpp).
+
+TEST INFRASTRUCTURE ONLY. Imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, as the checker. The product (owl_b200) never
+imports it.
+"""
+from .oracle import ORACLE_LIB, build, load, ac2d_forward, ac2d_gradient, ac2d_jvp  # noqa: F401

@@ -1,0 +1,90 @@
+"""ctypes wrapper of oracle/lib/liboracle.so (test infrastructure only)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "lib", "liboracle.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    srcs = [os.path.join(HERE, f) for f in ("oracle_ac2d.cpp", "oracle_common.hpp")]
+    if force or not os.path.exists(ORACLE_LIB) or any(os.path.getmtime(s) > os.path.getmtime(ORACLE_LIB) for s in srcs):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return ORACLE_LIB
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_LIB):
+            build()
+        _lib = C.CDLL(ORACLE_LIB)
+        vp = C.c_void_p
+        _lib.oracle_ac2d_forward_f32.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+        _lib.oracle_ac2d_forward_f64.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+        _lib.oracle_ac2d_jvp_c128.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp, vp, vp]
+        _lib.oracle_ac2d_gradient_f64.argtypes = [vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp, vp]
+        _lib.oracle_ac2d_gradient_f32.argtypes = [vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp, vp]
+    return _lib
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _fort(a, dt):
+    return np.asfortranarray(np.asarray(a, dtype=dt))
+
+
+def _nseis(ps, nt):
+    return sum(ps.arr[s].nrec for s in range(ps.nshots)) * nt
+
+
+def ac2d_forward(desc, vp, rho, ps, precision="f32"):
+    """Seismograms (flat, shot-major, trace-major) of the restated reference loops."""
+    lib = load()
+    dt = np.float32 if precision == "f32" else np.float64
+    vp, rho = _fort(vp, dt), _fort(rho, dt)
+    out = np.zeros(_nseis(ps, desc.nt), dtype=dt)
+    fn = lib.oracle_ac2d_forward_f32 if precision == "f32" else lib.oracle_ac2d_forward_f64
+    rc = fn(C.byref(desc), _p(vp), _p(rho), ps.nshots, C.cast(ps.arr, C.c_void_p), _p(out))
+    if rc != 0:
+        raise RuntimeError("oracle forward failed")
+    return out
+
+
+def ac2d_jvp(desc, vp, rho, dvp, drho, ps):
+    """(seis, d seis . (dvp, drho)) by complex-step differentiation in FP64."""
+    lib = load()
+    a = [_fort(v, np.float64) for v in (vp, rho, dvp, drho)]
+    n = _nseis(ps, desc.nt)
+    seis, jvp = np.zeros(n), np.zeros(n)
+    rc = lib.oracle_ac2d_jvp_c128(C.byref(desc), *[_p(v) for v in a], ps.nshots, C.cast(ps.arr, C.c_void_p),
+                                  _p(seis), _p(jvp))
+    if rc != 0:
+        raise RuntimeError("oracle jvp failed")
+    return seis, jvp
+
+
+def ac2d_gradient(desc, vp, rho, ps, data, adj_kind=0, k=50, precision="f64", stf_grad=False):
+    """(misfit per shot, grad (2, nz*nx) z-fastest, stf gradient or None) of the exact adjoint."""
+    lib = load()
+    dt = np.float64 if precision == "f64" else np.float32
+    vp, rho = _fort(vp, dt), _fort(rho, dt)
+    data = np.ascontiguousarray(data, dtype=dt)
+    misfit = np.zeros(ps.nshots)
+    grad = np.zeros(2 * desc.nx * desc.nz, dtype=dt)
+    nsrc = sum(ps.arr[s].nsrc for s in range(ps.nshots))
+    sg = np.zeros(nsrc * desc.nt, dtype=dt) if stf_grad else None
+    fn = lib.oracle_ac2d_gradient_f64 if precision == "f64" else lib.oracle_ac2d_gradient_f32
+    rc = fn(C.byref(desc), _p(vp), _p(rho), ps.nshots, C.cast(ps.arr, C.c_void_p), _p(data), adj_kind, k,
+            _p(misfit), _p(grad), _p(sg))
+    if rc != 0:
+        raise RuntimeError("oracle gradient failed")
+    return misfit, grad, sg

@@ -1,0 +1,158 @@
+// capi.cu -- extern "C" entry points declared in include/owl_ssg.h.
+#include <memory>
+#include <mutex>
+
+#include "engine.cuh"
+
+struct owl_ssg {
+    std::unique_ptr<owl::Engine> eng;
+};
+
+namespace owl {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+template <typename F>
+static int guarded(F&& f) {
+    try {
+        f();
+        return OWL_OK;
+    } catch (const OwlError& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return OWL_ERR_OOM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return OWL_ERR_INVALID;
+    }
+}
+
+static void check_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        throw OwlError(OWL_ERR_NO_DEVICE, "no CUDA device available");
+    }
+}
+
+static owl_run_opts opts_or_default(const owl_run_opts* o) {
+    owl_run_opts r{};
+    if (o) r = *o;
+    return r;
+}
+
+}  // namespace owl
+
+using namespace owl;
+
+extern "C" {
+
+int owl_ssg_abi_version(void) { return OWL_SSG_ABI_VERSION; }
+
+const char* owl_last_error(void) { return g_last_error.c_str(); }
+
+int owl_ssg_nparam(int medium) {
+    switch (medium) {
+        case OWL_ACOUSTIC_ISO_2D:
+        case OWL_ACOUSTIC_ISO_3D: return 2;
+        case OWL_ELASTIC_VHTIORT_2D: return 5;
+        case OWL_ELASTIC_VHTIORT_3D: return 10;
+        default: return -1;
+    }
+}
+
+int owl_ssg_ncomp(int medium) {
+    switch (medium) {
+        case OWL_ACOUSTIC_ISO_2D:
+        case OWL_ACOUSTIC_ISO_3D: return 1;
+        case OWL_ELASTIC_VHTIORT_2D: return 2;
+        case OWL_ELASTIC_VHTIORT_3D: return 3;
+        default: return -1;
+    }
+}
+
+int owl_ssg_device_ok(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, 0) != cudaSuccess) return 0;
+    return p.major == 10 ? 1 : 0;
+}
+
+int owl_ssg_create(const owl_ssg_desc* desc, owl_ssg** out) {
+    return guarded([&] {
+        OWL_CHECK(desc && out, OWL_ERR_INVALID, "null argument");
+        *out = nullptr;
+        check_device();
+        std::unique_ptr<owl_ssg> h(new owl_ssg);
+        switch (desc->medium) {
+            case OWL_ACOUSTIC_ISO_2D: h->eng.reset(make_ac2d_engine(*desc)); break;
+            default: throw OwlError(OWL_ERR_UNSUPPORTED, "medium not built");
+        }
+        *out = h.release();
+    });
+}
+
+int owl_ssg_set_model(owl_ssg* h, int nparam, const float* const* fields) {
+    return guarded([&] {
+        OWL_CHECK(h && h->eng, OWL_ERR_INVALID, "null handle");
+        h->eng->set_model(nparam, fields);
+    });
+}
+
+int owl_ssg_forward(owl_ssg* h, int nshots, const owl_shot* shots, const owl_run_opts* opts, float* seis,
+                    int mem_kind, owl_run_info* info) {
+    return guarded([&] {
+        OWL_CHECK(h && h->eng, OWL_ERR_INVALID, "null handle");
+        OWL_CHECK(nshots >= 0 && (nshots == 0 || shots), OWL_ERR_INVALID, "bad shots");
+        OWL_CHECK(seis || nshots == 0, OWL_ERR_INVALID, "null seismogram buffer");
+        OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
+        owl_run_info tmp{};
+        h->eng->forward(nshots, shots, opts_or_default(opts), seis, mem_kind, info ? *info : tmp);
+    });
+}
+
+int owl_ssg_gradient(owl_ssg* h, int nshots, const owl_shot* shots, const float* data, int adj_kind,
+                     const owl_run_opts* opts, double* misfit, float* grad, float* seis_out, int mem_kind,
+                     owl_run_info* info) {
+    return guarded([&] {
+        OWL_CHECK(h && h->eng, OWL_ERR_INVALID, "null handle");
+        OWL_CHECK(nshots >= 0 && (nshots == 0 || shots), OWL_ERR_INVALID, "bad shots");
+        OWL_CHECK(data || nshots == 0, OWL_ERR_INVALID, "null data buffer");
+        OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
+        owl_run_info tmp{};
+        h->eng->gradient(nshots, shots, data, adj_kind, opts_or_default(opts), misfit, grad, seis_out, mem_kind,
+                         info ? *info : tmp);
+    });
+}
+
+int owl_ssg_source_gradient(owl_ssg* h, int nshots, const owl_shot* shots, const float* adj, const owl_run_opts* opts,
+                            float* stf_grad, int mem_kind, owl_run_info* info) {
+    return guarded([&] {
+        OWL_CHECK(h && h->eng, OWL_ERR_INVALID, "null handle");
+        OWL_CHECK(nshots >= 0 && (nshots == 0 || shots) && adj && stf_grad, OWL_ERR_INVALID, "bad arguments");
+        owl_run_info tmp{};
+        h->eng->source_gradient(nshots, shots, adj, opts_or_default(opts), stf_grad, mem_kind, info ? *info : tmp);
+    });
+}
+
+void owl_ssg_destroy(owl_ssg* h) {
+    if (!h) return;
+    try {
+        if (h->eng) cudaStreamSynchronize(h->eng->stream);
+    } catch (...) {
+    }
+    delete h;
+}
+
+float owl_ssg_dt_stable(const owl_ssg* h) { return (h && h->eng) ? h->eng->dt_stable_ : 0.f; }
+
+}  // extern "C"

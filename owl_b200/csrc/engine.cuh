@@ -1,0 +1,65 @@
+// engine.cuh -- medium-independent engine interface and shared kernels.
+#pragma once
+
+#include "common.cuh"
+
+namespace owl {
+
+struct Engine {
+    owl_ssg_desc desc{};
+    cudaStream_t stream = nullptr;
+    float dt_stable_ = 0.f;
+    bool model_set = false;
+    virtual ~Engine() {}
+    virtual void set_model(int nparam, const float* const* fields) = 0;
+    virtual void forward(int nshots, const owl_shot* shots, const owl_run_opts& o, float* seis, int mem,
+                         owl_run_info& info) = 0;
+    virtual void gradient(int nshots, const owl_shot* shots, const float* data, int adj_kind,
+                          const owl_run_opts& o, double* misfit, float* grad, float* seis_out, int mem,
+                          owl_run_info& info) = 0;
+    virtual void source_gradient(int nshots, const owl_shot* shots, const float* adj, const owl_run_opts& o,
+                                 float* stf_grad, int mem, owl_run_info& info) = 0;
+};
+
+Engine* make_ac2d_engine(const owl_ssg_desc& d);
+Engine* make_ac3d_engine(const owl_ssg_desc& d);
+Engine* make_el2d_engine(const owl_ssg_desc& d);
+
+// -------- shared device helpers (defined in shared.cu) ----------------------
+
+// Kahan-compensated accumulation of v into (s, c)
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+    float y = v - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
+// one-thread-per-CTA tick of the step counter after all CTAs of a launch have
+// read it: the last CTA to finish applies `delta` (the threadfence-reduction
+// pattern; no CTA ever waits on another).
+__device__ __forceinline__ void tick_last_block(int* d_step, int* d_done, int delta) {
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        __threadfence();
+        int prev = atomicAdd(d_done, 1);
+        if (prev == (int)(gridDim.x * gridDim.y * gridDim.z) - 1) {
+            *d_step += delta;
+            *d_done = 0;
+            __threadfence();
+        }
+    }
+}
+
+// launches of shared kernels (shared.cu)
+void launch_transpose_rec_to_seis(const float* rec, float* seis, int nt, int rtot, cudaStream_t s);
+void launch_transpose_seis_to_rec(const float* seis, float* rec, int nt, int rtot, cudaStream_t s);
+// residual = syn - obs on live traces (weight != 0); misfit[shot] = sum (obs - syn)^2 (FP64,
+// deterministic per-shot block reduction). Traces are indexed by the global receiver id.
+void launch_residual_l2(const float* syn, const float* obs, float* res, const unsigned char* live,
+                        const int* shot_rec_ptr, int nshots, int nt, int rtot, double* misfit,
+                        cudaStream_t s);
+void launch_check_finite(const float* f, size_t n, int* flag, cudaStream_t s);
+void launch_fill_f64(double* p, size_t n, double v, cudaStream_t s);
+
+}  // namespace owl

@@ -1,0 +1,135 @@
+// shared.cu -- kernels and host helpers used by every medium.
+#include <algorithm>
+#include <cmath>
+
+#include "engine.cuh"
+
+namespace owl {
+
+int nint_f(float v) { return (int)std::lround(v); }
+
+void damp_coef(float bdvp, float d, float dist, int pml, float dt, float alphamax, float& a, float& b) {
+    // npower_d = 2, npower_a = 1, kmax = 1, R0 = 1e-5 (module_cfspml.f90:27-30,68-70)
+    const float R0 = 1.0e-5f, kmax = 1.0f;
+    float nd = dist / ((float)pml * d);
+    float alpha = std::max(alphamax * (1.0f - nd), 0.25f * alphamax);
+    float damp = bdvp * (2.0f + 1.0f) * std::log(1.0f / R0) / (2.0f * (float)pml * d) * (nd * nd);
+    float k = 1.0f + (kmax - 1.0f) * (nd * nd);
+    float adt = std::fabs(dt);
+    a = -2.0f * adt * damp / k / (2.0f + adt * (alpha + damp / k));
+    b = (2.0f - adt * (alpha + damp / k)) / (2.0f + adt * (alpha + damp / k));
+}
+
+Pml1DHost build_pml_1d(int n, int pml, int R, int len, float d, float dt, float pmlvp, float alphamax) {
+    Pml1DHost h;
+    h.ai.assign(len, 0.f);
+    h.bi.assign(len, 0.f);
+    h.ah.assign(len, 0.f);
+    h.bh.assign(len, 0.f);
+    for (int i = -pml + 1; i <= n + pml; ++i) {
+        float disti = 0.f, disth = 0.f;
+        if (i <= 1) {
+            disti = std::fabs((float)(i - 1) * d);
+            disth = std::fabs(((float)(i - 1) - 0.5f) * d);
+        } else if (i >= n + 1) {
+            disti = std::fabs((float)(i - n) * d);
+            disth = std::fabs(((float)(i - n) - 0.5f) * d);
+        }
+        if (i <= 1 || i >= n + 1) {
+            int x = i + pml + R - 1;
+            damp_coef(pmlvp, d, disti, pml, dt, alphamax, h.ai[x], h.bi[x]);
+            damp_coef(pmlvp, d, disth, pml, dt, alphamax, h.ah[x], h.bh[x]);
+        }
+    }
+    return h;
+}
+
+// ---------------------------------------------------------------------------
+// record buffer [t][rtot]  <->  seismogram [rtot][t]
+// ---------------------------------------------------------------------------
+__global__ void k_transpose(const float* __restrict__ in, float* __restrict__ out, int rows, int cols) {
+    // in: rows x cols, out: cols x rows
+    __shared__ float tile[32][33];
+    int c = blockIdx.x * 32 + threadIdx.x;
+    for (int r = blockIdx.y * 32 + threadIdx.y; r < min(rows, (int)(blockIdx.y * 32 + 32)); r += 8)
+        if (c < cols) tile[r - blockIdx.y * 32][threadIdx.x] = in[(size_t)r * cols + c];
+    __syncthreads();
+    int r2 = blockIdx.y * 32 + threadIdx.x;
+    for (int c2 = blockIdx.x * 32 + threadIdx.y; c2 < min(cols, (int)(blockIdx.x * 32 + 32)); c2 += 8)
+        if (r2 < rows) out[(size_t)c2 * rows + r2] = tile[threadIdx.x][c2 - blockIdx.x * 32];
+}
+
+static void launch_transpose(const float* in, float* out, int rows, int cols, cudaStream_t s) {
+    if (rows <= 0 || cols <= 0) return;
+    dim3 b(32, 8), g((cols + 31) / 32, (rows + 31) / 32);
+    k_transpose<<<g, b, 0, s>>>(in, out, rows, cols);
+    OWL_LAUNCH_CHECK();
+}
+
+void launch_transpose_rec_to_seis(const float* rec, float* seis, int nt, int rtot, cudaStream_t s) {
+    launch_transpose(rec, seis, nt, rtot, s);
+}
+void launch_transpose_seis_to_rec(const float* seis, float* rec, int nt, int rtot, cudaStream_t s) {
+    launch_transpose(seis, rec, rtot, nt, s);
+}
+
+// residual and misfit: one CTA per shot, fixed assignment -> deterministic
+__global__ void k_residual_l2(const float* __restrict__ syn, const float* __restrict__ obs, float* __restrict__ res,
+                              const unsigned char* __restrict__ live, const int* __restrict__ shot_rec_ptr, int nt,
+                              int rtot, double* __restrict__ misfit) {
+    int s = blockIdx.x;
+    int r0 = shot_rec_ptr[s], r1 = shot_rec_ptr[s + 1];
+    int nr = r1 - r0;
+    double acc = 0.0;
+    long long n = (long long)nr * nt;
+    for (long long q = threadIdx.x; q < n; q += blockDim.x) {
+        int t = (int)(q / nr), r = r0 + (int)(q % nr);
+        size_t o = (size_t)t * rtot + r;
+        float rv = 0.f;
+        if (live[r]) {
+            rv = syn[o] - obs[o];
+            double dd = (double)obs[o] - (double)syn[o];
+            acc += dd * dd;
+        }
+        res[o] = rv;
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && misfit) misfit[s] = red[0];
+}
+
+void launch_residual_l2(const float* syn, const float* obs, float* res, const unsigned char* live,
+                        const int* shot_rec_ptr, int nshots, int nt, int rtot, double* misfit, cudaStream_t s) {
+    if (nshots <= 0) return;
+    k_residual_l2<<<nshots, 256, 0, s>>>(syn, obs, res, live, shot_rec_ptr, nt, rtot, misfit);
+    OWL_LAUNCH_CHECK();
+}
+
+__global__ void k_check_finite(const float* __restrict__ f, size_t n, int* flag) {
+    bool bad = false;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        bad |= !isfinite(f[i]);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+void launch_check_finite(const float* f, size_t n, int* flag, cudaStream_t s) {
+    if (!n) return;
+    k_check_finite<<<148 * 4, 256, 0, s>>>(f, n, flag);
+    OWL_LAUNCH_CHECK();
+}
+
+__global__ void k_fill_f64(double* p, size_t n, double v) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+void launch_fill_f64(double* p, size_t n, double v, cudaStream_t s) {
+    if (!n) return;
+    k_fill_f64<<<148 * 2, 256, 0, s>>>(p, n, v);
+    OWL_LAUNCH_CHECK();
+}
+
+}  // namespace owl

@@ -1,0 +1,166 @@
+"""Python handle over the C ABI (include/owl_ssg.h).
+
+``SSGSolver`` is the batched, B200-first entry: many shots per call, model
+set once, seismograms and gradients as numpy arrays (host) or torch CUDA
+tensors (device, no host round trip).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib as L
+from .geometry import GridSpec, PreparedShots
+
+f32 = np.float32
+
+
+@dataclass
+class RunOpts:
+    shots_per_launch: int = 0      # 0 = all shots of the call in one launch (<= max_shots)
+    checkpoint_interval: int = 50
+    checkpoint_precision: int = L.OWL_CKPT_FP32
+    use_graph: int = 0             # 0 / 1: CUDA graphs on; -1: plain launches
+    shots_per_cta: int = 0
+    tile_x: int = 0
+    tile_z: int = 0
+    check_every: int = 0
+
+    def c(self) -> L.OwlRunOpts:
+        o = L.OwlRunOpts()
+        for k in ("shots_per_launch", "checkpoint_interval", "checkpoint_precision", "use_graph",
+                  "shots_per_cta", "tile_x", "tile_z", "check_every"):
+            setattr(o, k, int(getattr(self, k)))
+        return o
+
+
+def _ptr(a) -> C.c_void_p:
+    """host numpy array or torch tensor -> void*"""
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return C.c_void_p(a.ctypes.data)
+
+
+def _mem_kind(a) -> int:
+    if hasattr(a, "is_cuda") and a.is_cuda:
+        return L.OWL_MEM_DEVICE
+    return L.OWL_MEM_HOST
+
+
+class SSGSolver:
+    """One solver handle: grid, PML, time axis and model of one medium."""
+
+    def __init__(self, medium: int, nx: int, nz: int, dx: float, dz: float, dt: float, nt: int,
+                 pml: int = 15, fdhalf: int = 4, free_surface: bool = False, f0_max: float = 20.0,
+                 max_shots: int = 1, ny: int = 1, dy: float = 0.0, ox: float = 0.0, oy: float = 0.0,
+                 oz: float = 0.0, allow_dt_adjust: bool = False):
+        self.lib = L.load()
+        d = L.OwlSsgDesc()
+        d.medium = medium
+        d.nx, d.ny, d.nz = nx, ny, nz
+        d.dx, d.dy, d.dz = dx, (dy if dy else dx), dz
+        d.ox, d.oy, d.oz = ox, oy, oz
+        d.pml, d.fdhalf, d.free_surface = pml, fdhalf, int(bool(free_surface))
+        d.dt, d.nt, d.f0_max = dt, nt, f0_max
+        d.max_shots = max_shots
+        d.allow_dt_adjust = int(bool(allow_dt_adjust))
+        self.desc = d
+        self.grid = GridSpec(nx=nx, nz=nz, dx=dx, dz=dz, ox=ox, oz=oz, ny=ny, dy=(dy if dy else dx), oy=oy)
+        h = C.c_void_p()
+        L.check(self.lib.owl_ssg_create(C.byref(d), C.byref(h)))
+        self.h = h
+        self.ncomp = self.lib.owl_ssg_ncomp(medium)
+        self.nparam = self.lib.owl_ssg_nparam(medium)
+        self.last_info = L.OwlRunInfo()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.owl_ssg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def dt_stable(self) -> float:
+        return float(self.lib.owl_ssg_dt_stable(self.h))
+
+    def set_model(self, *fields: np.ndarray) -> None:
+        """fields: (nz, nx) [or (nz, ny, nx)] arrays in the order of owl_ssg_set_model."""
+        self._model = [np.asfortranarray(np.asarray(f, dtype=f32)) for f in fields]
+        arr = (C.POINTER(C.c_float) * len(self._model))()
+        for i, f in enumerate(self._model):
+            arr[i] = f.ctypes.data_as(C.POINTER(C.c_float))
+        L.check(self.lib.owl_ssg_set_model(self.h, len(self._model), arr))
+
+    def prepare(self, shots, f0factor: float = 1.0, time_integration: int = 0) -> PreparedShots:
+        return PreparedShots(shots, self.grid, self.desc.dt, f0factor, time_integration)
+
+    def seis_size(self, ps: PreparedShots) -> int:
+        return sum(ps.nrec(s) for s in range(ps.nshots)) * self.ncomp * self.desc.nt
+
+    def split(self, ps: PreparedShots, flat) -> List:
+        """flat seismogram buffer -> per-shot (ncomp, nrec, nt) views"""
+        out, off = [], 0
+        nt = self.desc.nt
+        for s in range(ps.nshots):
+            n = ps.nrec(s) * self.ncomp * nt
+            out.append(flat[off:off + n].reshape(self.ncomp, ps.nrec(s), nt))
+            off += n
+        return out
+
+    def forward(self, ps: PreparedShots, opts: Optional[RunOpts] = None, out=None):
+        """Seismograms of all shots; returns the flat buffer (numpy or torch)."""
+        opts = opts or RunOpts()
+        if out is None:
+            out = np.zeros(self.seis_size(ps), dtype=f32)
+        o = opts.c()
+        L.check(self.lib.owl_ssg_forward(self.h, ps.nshots, ps.arr, C.byref(o), _ptr(out), _mem_kind(out),
+                                         C.byref(self.last_info)))
+        return out
+
+    def gradient(self, ps: PreparedShots, data, adj_kind: int = L.OWL_ADJ_L2_RESIDUAL,
+                 opts: Optional[RunOpts] = None, grad=None, misfit=None, seis_out=None):
+        """Stacked gradient of 0.5 * sum (syn - obs)^2 (or of <syn, adj> for OWL_ADJ_GIVEN).
+
+        Returns (misfit per shot, gradient (nparam, nz*nx) flat buffer)."""
+        opts = opts or RunOpts()
+        nm = self.desc.nx * self.desc.nz * max(1, self.desc.ny)
+        dev = _mem_kind(data) == L.OWL_MEM_DEVICE
+        if grad is None:
+            if dev:
+                import torch
+                grad = torch.zeros(self.nparam * nm, dtype=torch.float32, device=data.device)
+                misfit = torch.zeros(ps.nshots, dtype=torch.float64, device=data.device)
+            else:
+                grad = np.zeros(self.nparam * nm, dtype=f32)
+                misfit = np.zeros(ps.nshots, dtype=np.float64)
+        o = opts.c()
+        L.check(self.lib.owl_ssg_gradient(self.h, ps.nshots, ps.arr, _ptr(data), adj_kind, C.byref(o),
+                                          _ptr(misfit) if misfit is not None else None, _ptr(grad),
+                                          _ptr(seis_out) if seis_out is not None else None,
+                                          _mem_kind(data), C.byref(self.last_info)))
+        return misfit, grad
+
+    def grad_fields(self, grad) -> List[np.ndarray]:
+        """flat gradient -> list of (nz, nx) [or (nz, ny, nx)] arrays (z fastest like OWL files)"""
+        d = self.desc
+        shape = (d.nz, d.nx) if d.ny <= 1 else (d.nz, d.ny, d.nx)
+        nm = int(np.prod(shape))
+        g = grad if isinstance(grad, np.ndarray) else grad.detach().cpu().numpy()
+        return [g[i * nm:(i + 1) * nm].reshape(tuple(reversed(shape))).T for i in range(self.nparam)]
+
+    def source_gradient(self, ps: PreparedShots, adj: np.ndarray, opts: Optional[RunOpts] = None):
+        opts = opts or RunOpts()
+        nsrc = sum(ps.arr[s].nsrc for s in range(ps.nshots))
+        out = np.zeros(nsrc * self.desc.nt, dtype=f32)
+        o = opts.c()
+        L.check(self.lib.owl_ssg_source_gradient(self.h, ps.nshots, ps.arr, _ptr(adj), C.byref(o), _ptr(out),
+                                                 L.OWL_MEM_HOST, C.byref(self.last_info)))
+        return out
