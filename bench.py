@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark: adjoint-state FWI gradient seconds per shot on the 2D acoustic
+workload (201 x 401 grid, dx 10 m, 20-cell CFS-PML, 8th order, dt 1 ms, 2000
+steps, 32 shots with offset-truncated receiver spreads, L2 waveform misfit,
+every-50-step FP32 checkpoints).
+
+One step = one batched gradient over the 32 shots of a GPU (forward with
+checkpoints, residual + FP64 misfit, reverse sweep with segment recompute and
+exact adjoint, FP64 chain rule). With N GPUs each rank runs its own 32 shots and
+the stacked gradient is summed over ranks with one NCCL all-reduce per step.
+
+Prints one JSON line (rank 0). ``--impl reference`` times the reference's own
+CPU gradient algorithm (restated loops, OpenMP on all host cores) instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NSHOTS = 32
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="owl", choices=["owl", "reference"])
+    p.add_argument("--no-plain", action="store_true", help="skip the per-shot plain-path measurement")
+    p.add_argument("--no-check", action="store_true", help="skip the FP64-oracle gradient check")
+    p.add_argument("--cpu-nt", type=int, default=500, help="time steps of the CPU-baseline sample")
+    p.add_argument("--nshots", type=int, default=NSHOTS, help="shots per GPU (32 for the benchmark)")
+    p.add_argument("--profile", action="store_true",
+                   help="profiling target: one gradient step of --nshots shots, nothing else, no JSON line")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for ln in fh:
+                parts = [x.strip() for x in ln.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        busy = [v for v in sm if v > 0.5 * smax] or sm
+        return {"sm_mhz": busy[len(busy) // 2], "sm_max_mhz": smax, "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per launch of a kernel from the committed ncu summary, scaled to
+    the bench's launch (None if absent)."""
+    p = os.path.join(ROOT, "profiles", "ac2d_gradient_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(kernel)
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def cpu_reference_sample(nt_sample: int):
+    """Time the reference's own gradient algorithm (restated loops, OpenMP on all
+    cores) on one shot of the workload with nt_sample steps; return (s/shot
+    scaled to the full 2000-step shot, threads, sample description)."""
+    import numpy as np
+    import oracle
+    from owl_b200 import configs
+    from owl_b200.geometry import GridSpec, PreparedShots
+
+    d, (vp, rho), (vp0, rho0), shots = configs.config2(NSHOTS)
+    nt_full = d.nt
+    d.nt = nt_sample
+    ps = PreparedShots(shots[:1], GridSpec(nx=d.nx, nz=d.nz, dx=d.dx, dz=d.dz), d.dt)
+    nrec = ps.arr[0].nrec
+    adj = np.random.default_rng(0).standard_normal(nrec * nt_sample).astype(np.float32)
+    oracle.build()
+    hnt = ps.hnt[0]
+    t0 = time.perf_counter()
+    oracle.ac2d_ref_gradient(d, vp0, rho0, ps, adj, cc=1)
+    el = time.perf_counter() - t0
+    # forward nt steps + 2 updates per reverse step from nt down to hnt
+    work_full = nt_full + 2 * (nt_full - hnt + 1)
+    work_smp = nt_sample + 2 * (nt_sample - hnt + 1)
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return el * work_full / work_smp, threads, (
+        f"1 shot of the workload, {nt_sample} of {nt_full} steps (forward with boundary saving + "
+        f"-dt reconstruction + adjoint + imaging every step), scaled by update count to 2000 steps; "
+        f"{el:.1f} s measured")
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, threads, sample = cpu_reference_sample(args.cpu_nt)
+        if i >= args.warmup:
+            vals.append(v)
+    v = sum(vals) / len(vals)
+    line = {
+        "impl": "reference", "metric": "fwi_gradient_s_per_shot", "value": v, "unit": "s/shot",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "2D acoustic FWI gradient, 201x401 grid, 2000 steps, 32 shots (per GPU), "
+                               "L2 misfit; reference algorithm (time-reversed -dt propagation with boundary "
+                               "saving) on the host CPU"},
+        "cpu_baseline": {"value": v, "unit": "s/shot", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "s/shot", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from owl_b200 import _lib as L
+    from owl_b200 import configs
+    from owl_b200.solver import RunOpts, SSGSolver
+
+    nshots = args.nshots
+    d, (vp, rho), (vp0, rho0), shots = configs.config2(NSHOTS)
+    shots = [shots[(i * NSHOTS) // nshots] for i in range(nshots)] if nshots != NSHOTS else shots
+    s = SSGSolver(L.OWL_ACOUSTIC_ISO_2D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
+                  f0_max=d.f0_max, max_shots=nshots)
+    ps = s.prepare(shots)
+    s.set_model(vp, rho)
+    obs = s.forward(ps)  # observed data from the true model (not timed)
+    s.set_model(vp0, rho0)
+    opts = RunOpts(checkpoint_interval=50)
+    nm = d.nx * d.nz
+    obs_dev = torch.from_numpy(obs).cuda()
+    g_dev = torch.zeros(2 * nm, dtype=torch.float32, device="cuda")
+    m_dev = torch.zeros(nshots, dtype=torch.float64, device="cuda")
+    if args.profile:
+        s.gradient(ps, obs_dev, opts=opts, grad=g_dev, misfit=m_dev)
+        torch.cuda.synchronize()
+        print(f"profile step: {s.last_info.elapsed_ms:.1f} ms, {s.last_info.gpu_launches} launches")
+        s.close()
+        return
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def step_device():
+        s.gradient(ps, obs_dev, opts=opts, grad=g_dev, misfit=m_dev)
+        ms = s.last_info.elapsed_ms
+        if world > 1:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            dist.all_reduce(g_dev)
+            ev1.record()
+            ev1.synchronize()
+            ms += ev0.elapsed_time(ev1)
+        return ms
+
+    for _ in range(args.warmup):
+        step_device()
+    barrier()
+    clk = Clocks(local)
+    clk.start()
+    t_wall = time.perf_counter()
+    step_ms = [step_device() for _ in range(args.steps)]
+    barrier()
+    wall = time.perf_counter() - t_wall
+    clocks = clk.stop()
+    launches = int(s.last_info.gpu_launches) * args.steps
+    tot = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    ms_step = float(tot.item()) / args.steps
+    shots_job = nshots * world
+    value = ms_step / 1e3 / shots_job
+    cells = (d.nx + 2 * d.pml) * (d.nz + 2 * d.pml)
+    gcells = 3.0 * cells * d.nt * shots_job / (ms_step / 1e3) / 1e9
+
+    # e2e: same call through the C ABI with pinned host buffers (H2D of the
+    # observed data and D2H of gradient + misfit inside the timed region)
+    obs_pin = torch.from_numpy(obs).pin_memory().numpy()
+    g_pin = torch.zeros(2 * nm, dtype=torch.float32).pin_memory().numpy()
+    m_pin = torch.zeros(nshots, dtype=torch.float64).pin_memory().numpy()
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        s.gradient(ps, obs_pin, opts=opts, grad=g_pin, misfit=m_pin)
+        ms = s.last_info.elapsed_ms
+        if world > 1:
+            gt = torch.from_numpy(g_pin).cuda()
+            t0 = time.perf_counter()
+            dist.all_reduce(gt)
+            torch.cuda.synchronize()
+            g_pin[:] = gt.cpu().numpy()
+            ms += (time.perf_counter() - t0) * 1e3
+        if i >= args.warmup:
+            e2e_ms.append(ms)
+    te = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = float(te.item()) / args.steps / 1e3 / shots_job
+
+    # roofline of the dominant kernel (standalone launches on the batch state)
+    s.gradient(ps, obs_dev, opts=opts, grad=g_dev, misfit=m_dev)
+    names = {L.OWL_K_FWD_P: "k_ac2d_fwd_p", L.OWL_K_FWD_V: "k_ac2d_fwd_v", L.OWL_K_ADJ_P: "k_ac2d_adj_p",
+             L.OWL_K_ADJ_V: "k_ac2d_adj_v"}
+    per_step = {L.OWL_K_FWD_P: 2 * d.nt, L.OWL_K_FWD_V: 2 * d.nt, L.OWL_K_ADJ_P: d.nt, L.OWL_K_ADJ_V: d.nt}
+    kt = {}
+    for kid in names:
+        ms, b = s.kernel_time(kid, 50)
+        kt[kid] = (ms, b)
+    dom = max(kt, key=lambda k: kt[k][0] * per_step[k])
+    ms_k, bytes_k = kt[dom]
+    peak, peak_kind = measured_peak_hbm()
+    achieved = bytes_k / (ms_k / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": profile_traffic(names[dom]),
+                "alg_bytes_per_launch": bytes_k, "ms_per_launch": ms_k,
+                "kernel_ms_per_launch": {names[k]: kt[k][0] for k in kt}}
+
+    line = {
+        "metric": "fwi_gradient_s_per_shot", "value": value, "unit": "s/shot", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "2D acoustic FWI gradient (L2 misfit), 201x401 grid, dx 10 m, 20-cell CFS-PML, "
+                               "8th order, dt 1 ms, 2000 steps, 32 shots per GPU with +-1500 m receiver spreads, "
+                               "exact adjoint, every-50-step FP32 checkpoints, one batched launch per step",
+                   "shots_per_gpu": nshots, "parallelism": f"shots sharded over {world} GPU(s)",
+                   "l2_flush": "working set (checkpoints + segment buffers, several GB) exceeds L2"},
+        "gcells_per_s": gcells,
+        "wall_s_timed": wall,
+        "e2e": {"value": e2e_value, "unit": "s/shot", "h2d_bytes_per_step": int(obs.nbytes),
+                "d2h_bytes_per_step": int(g_pin.nbytes + m_pin.nbytes)},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "clocks": clocks,
+    }
+
+    if rank == 0 and not args.no_plain:
+        # plain per-shot path: one shot per launch sequence, no graphs, FP32 checkpoints
+        sub = s.prepare(shots[:4])
+        obs_sub = torch.from_numpy(obs[: s.seis_size(sub)]).cuda()
+        po = RunOpts(checkpoint_interval=50, shots_per_launch=1, use_graph=-1)
+        s.gradient(sub, obs_sub, opts=po)
+        s.gradient(sub, obs_sub, opts=po)
+        line["plain_s_per_shot"] = s.last_info.elapsed_ms / 1e3 / sub.nshots
+        line["batched_vs_plain"] = line["plain_s_per_shot"] / value * world
+
+    if rank == 0 and not args.no_check:
+        import oracle
+        one = s.prepare(shots[:1])
+        n1 = s.seis_size(one)
+        _, g1 = s.gradient(one, obs[:n1].copy(), opts=opts)
+        _, gref, _ = oracle.ac2d_gradient(s.desc, vp0, rho0, one, obs[:n1], adj_kind=0, k=50, precision="f64")
+        line["grad_rel_err_vs_fp64_oracle"] = float(np.linalg.norm(g1 - gref) / np.linalg.norm(gref))
+
+    if rank == 0 and world == 1:
+        v, threads, sample = cpu_reference_sample(args.cpu_nt)
+        line["cpu_baseline"] = {"value": v, "unit": "s/shot", "cores": threads, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

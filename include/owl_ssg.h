@@ -200,6 +200,22 @@ int owl_ssg_source_gradient(owl_ssg *h, int nshots, const owl_shot *shots,
 
 void owl_ssg_destroy(owl_ssg *h);
 
+/* ---- diagnostics (no counterpart in the reference) ------------------------ */
+
+/* Kernel ids for owl_ssg_kernel_time. */
+#define OWL_K_FWD_P 0   /* pressure / stress update with fused CFS-PML */
+#define OWL_K_FWD_V 1   /* velocity update with fused CFS-PML */
+#define OWL_K_ADJ_P 2   /* adjoint of the velocity update (writes p^) */
+#define OWL_K_ADJ_V 3   /* adjoint of the pressure update (writes v^) */
+
+/* Times nlaunch back-to-back standalone launches of one kernel on the state of
+ * the last batch of the last forward / gradient call (CUDA events on the
+ * handle's stream). avg_ms: mean duration of one launch. alg_bytes: compulsory
+ * HBM bytes of one launch (each state field read / written once per shot,
+ * materials once per launch, PML memory only inside the PML). Leaves the
+ * wavefields in an unspecified state. */
+int owl_ssg_kernel_time(owl_ssg *h, int kernel_id, int nlaunch, double *avg_ms, double *alg_bytes);
+
 /* ---- queries ------------------------------------------------------------ */
 
 const char *owl_last_error(void);

@@ -31,6 +31,7 @@ def load():
         _lib.oracle_ac2d_jvp_c128.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp, vp, vp]
         _lib.oracle_ac2d_gradient_f64.argtypes = [vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp, vp]
         _lib.oracle_ac2d_gradient_f32.argtypes = [vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp, vp]
+        _lib.oracle_ac2d_ref_gradient_f32.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp, C.c_int, vp]
     return _lib
 
 
@@ -88,3 +89,18 @@ def ac2d_gradient(desc, vp, rho, ps, data, adj_kind=0, k=50, precision="f64", st
     if rc != 0:
         raise RuntimeError("oracle gradient failed")
     return misfit, grad, sg
+
+
+def ac2d_ref_gradient(desc, vp, rho, ps, adj, cc=1):
+    """The reference's own (time-reversed, -dt) gradient, FP32, summed over shots:
+    grad (2, nz*nx) z-fastest for (vp, rho)."""
+    lib = load()
+    vp, rho = _fort(vp, np.float32), _fort(rho, np.float32)
+    adj = np.ascontiguousarray(adj, dtype=np.float32)
+    hnt = np.array([max(1, h) for h in ps.hnt], dtype=np.int32)
+    grad = np.zeros(2 * desc.nx * desc.nz, dtype=np.float32)
+    rc = lib.oracle_ac2d_ref_gradient_f32(C.byref(desc), _p(vp), _p(rho), ps.nshots, C.cast(ps.arr, C.c_void_p),
+                                          _p(adj), _p(hnt), cc, _p(grad))
+    if rc != 0:
+        raise RuntimeError("oracle ref gradient failed")
+    return grad

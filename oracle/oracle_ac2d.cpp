@@ -358,6 +358,88 @@ struct Ac2d {
         }
     }
 
+    // ---------------- the reference's own gradient ------------------------------
+    // Restates compute_forward with yn_reconstruct (boundary rings of vx / vz
+    // saved before every step, final wavefield saved at the top of step nt,
+    // module_boundary_saving.f90:52-153) and compute_adjoint
+    // (submodule_fwi_gradient.f90:31-199): source-wavefield reconstruction and
+    // adjoint propagation both by update_wavefield(-dt), adjoint-source
+    // injection, and the imaging condition of compute_gradient (:201-269) every
+    // cc steps, for t = nt down to hnt. Rings are kept in memory instead of a
+    // direct-access file. Output: grad_vp, grad_rho on the model cells.
+    void ref_gradient_shot(const owl_shot& sh, const T* adj, int hnt, int cc, T* gvp, T* grho) const {
+        const int P = pml;
+        Ac2dState<T> s;
+        s.init(lo_x, hi_x, lo_z, hi_z);
+        // ring extents (prepare_boundary_saving)
+        const int xb1 = 1 - R + 1, xb2 = 1, xe1 = nx + 1, xe2 = nx + R, xz0 = 1 - R, xz1 = nz + R;
+        const int zx0 = 1 - R, zx1 = nx + R, zb1 = 1 - R + 1, zb2 = 1, ze1 = nz + 1, ze2 = nz + R;
+        auto save = [&](std::vector<T>& r) {
+            r.clear();
+            for (int j = xz0; j <= xz1; ++j) for (int i = xb1; i <= xb2; ++i) r.push_back(s.vx(i, j));
+            for (int j = xz0; j <= xz1; ++j) for (int i = xe1; i <= xe2; ++i) r.push_back(s.vx(i, j));
+            for (int j = zb1; j <= zb2; ++j) for (int i = zx0; i <= zx1; ++i) r.push_back(s.vz(i, j));
+            for (int j = ze1; j <= ze2; ++j) for (int i = zx0; i <= zx1; ++i) r.push_back(s.vz(i, j));
+        };
+        auto inject = [&](const std::vector<T>& r, Ac2dState<T>& d) {
+            size_t q = 0;
+            for (int j = xz0; j <= xz1; ++j) for (int i = xb1; i <= xb2; ++i) d.vx(i, j) = r[q++];
+            for (int j = xz0; j <= xz1; ++j) for (int i = xe1; i <= xe2; ++i) d.vx(i, j) = r[q++];
+            for (int j = zb1; j <= zb2; ++j) for (int i = zx0; i <= zx1; ++i) d.vz(i, j) = r[q++];
+            for (int j = ze1; j <= ze2; ++j) for (int i = zx0; i <= zx1; ++i) d.vz(i, j) = r[q++];
+        };
+        std::vector<std::vector<T>> rings(nt + 1);
+        Ac2dState<T> fin;
+        std::vector<T> seis((size_t)sh.nrec * nt, T(0));
+        for (int t = 1; t <= nt; ++t) {
+            save(rings[t]);
+            if (t == nt) fin = s;
+            sample(t, sh, s, seis.data());
+            update(dt, s, nullptr);
+            add_source(t, sh, s);
+        }
+        // adjoint
+        Ac2dState<T> f, a;
+        f.init(lo_x, hi_x, lo_z, hi_z);
+        a.init(lo_x, hi_x, lo_z, hi_z);
+        Arr2<T> pp(lo_x, hi_x, lo_z, hi_z), pvx(lo_x, hi_x, lo_z, hi_z), pvz(lo_x, hi_x, lo_z, hi_z);
+        Arr2<T> gv(1, nx, 1, nz), gr(1, nx, 1, nz);
+        for (int t = nt; t >= hnt; --t) {
+            pp = f.p; pvx = f.vx; pvz = f.vz;
+            if (t == nt) { f.p = fin.p; f.vx = fin.vx; f.vz = fin.vz; }
+            inject(rings[t], f);
+            update(-dt, f, nullptr);
+            update(-dt, a, nullptr);
+            for (int r = 0; r < sh.nrec; ++r) {
+                const owl_receiver& q = sh.rec[r];
+                if (q.weight == 0.f) continue;
+                T rv = adj[(size_t)r * nt + (t - 1)];
+                for (int irz = -4; irz <= 4; ++irz)
+                    for (int irx = -4; irx <= 4; ++irx)
+                        a.p(q.gx + irx, q.gz + irz) = a.p(q.gx + irx, q.gz + irz) +
+                            rv * T(q.interp_ix[irx + 4]) * T(q.interp_iz[irz + 4]) * T(q.weight);
+            }
+            if (t % cc == 0) {
+#pragma omp parallel for collapse(2) schedule(static)
+                for (int j = 1; j <= nz; ++j)
+                    for (int i = 1; i <= nx; ++i) {
+                        T sp = f.p(i, j) - pp(i, j);
+                        gv(i, j) = gv(i, j) - sp * a.p(i, j) / (rho(i, j) * vp(i, j) * vp(i, j) * vp(i, j));
+                        T sx = (f.vx(i, j) + f.vx(i + 1, j)) - (pvx(i, j) + pvx(i + 1, j));
+                        T rx = a.vx(i, j) + a.vx(i + 1, j);
+                        T sz = (f.vz(i, j) + f.vz(i, j + 1)) - (pvz(i, j) + pvz(i, j + 1));
+                        T rz = a.vz(i, j) + a.vz(i, j + 1);
+                        gr(i, j) = gr(i, j) + sx * rx + sz * rz;
+                    }
+            }
+        }
+        for (int i = 1; i <= nx; ++i)
+            for (int j = 1; j <= nz; ++j) {
+                gvp[(size_t)(i - 1) * nz + (j - 1)] += gv(i, j);
+                grho[(size_t)(i - 1) * nz + (j - 1)] += gr(i, j);
+            }
+    }
+
     // fold the padded-grid gradient onto the model cells (adjoint of pad_array's
     // edge replication) and write (nz,nx) z-fastest.
     void fold(const Arr2<T>& gp, T* out) const {
@@ -483,4 +565,25 @@ extern "C" int oracle_ac2d_gradient_f32(const owl_ssg_desc* d, const float* vp, 
                                         const owl_shot* shots, const float* data, int adj_kind, int k,
                                         double* misfit, float* grad, float* stf_grad) {
     return grad_impl<float>(d, vp, rho, nshots, shots, data, adj_kind, k, misfit, grad, stf_grad);
+}
+
+// the reference's own gradient (time-reversed -dt propagation), summed over shots.
+// hnt: per shot, the last reverse step (prepare_stf's hnt of the shot's first source);
+// cc: cc_step_interval. adj: adjoint sources, same layout as seismograms.
+extern "C" int oracle_ac2d_ref_gradient_f32(const owl_ssg_desc* d, const float* vp, const float* rho, int nshots,
+                                            const owl_shot* shots, const float* adj, const int* hnt, int cc,
+                                            float* grad) {
+    try {
+        Ac2d<float> m(*d, vp, rho);
+        size_t nm = (size_t)d->nx * d->nz, off = 0;
+        std::fill(grad, grad + 2 * nm, 0.f);
+        for (int s = 0; s < nshots; ++s) {
+            m.ref_gradient_shot(shots[s], adj + off, hnt[s], cc, grad, grad + nm);
+            off += (size_t)shots[s].nrec * d->nt;
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle: %s\n", e.what());
+        return -1;
+    }
 }

@@ -134,8 +134,13 @@ class OwlRunInfo(C.Structure):
 EXPORTED = [
     "owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
     "owl_ssg_source_gradient", "owl_ssg_destroy", "owl_last_error", "owl_ssg_abi_version",
-    "owl_ssg_dt_stable", "owl_ssg_nparam", "owl_ssg_ncomp", "owl_ssg_device_ok",
+    "owl_ssg_dt_stable", "owl_ssg_nparam", "owl_ssg_ncomp", "owl_ssg_device_ok", "owl_ssg_kernel_time",
 ]
+
+OWL_K_FWD_P = 0
+OWL_K_FWD_V = 1
+OWL_K_ADJ_P = 2
+OWL_K_ADJ_V = 3
 
 
 class OwlError(RuntimeError):
@@ -164,6 +169,8 @@ def load() -> C.CDLL:
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, P(OwlRunInfo)]
     lib.owl_ssg_source_gradient.argtypes = [C.c_void_p, C.c_int, P(OwlShot), C.c_void_p, P(OwlRunOpts),
                                             C.c_void_p, C.c_int, P(OwlRunInfo)]
+    lib.owl_ssg_kernel_time.argtypes = [C.c_void_p, C.c_int, C.c_int, P(C.c_double), P(C.c_double)]
+    lib.owl_ssg_kernel_time.restype = C.c_int
     lib.owl_ssg_destroy.argtypes = [C.c_void_p]
     lib.owl_ssg_destroy.restype = None
     lib.owl_last_error.restype = C.c_char_p

@@ -23,6 +23,7 @@
 //                same captured CUDA graph serves every segment of k steps.
 #include <algorithm>
 #include <cmath>
+#include <array>
 #include <map>
 
 #include "engine.cuh"
@@ -45,7 +46,7 @@ struct Ac2dDev {
     int k;
     int* d_step;
     float *ap, *avx, *avz, *am1, *am2, *am3, *am4;
-    long long mbuf;
+    float *aex, *aez, *aepx, *aepz;
     float *Gbk, *Gbx, *Gbz, *Cbk, *Cbx, *Cbz;
 };
 
@@ -54,7 +55,7 @@ __device__ __forceinline__ bool pml_half(int x, int pr, int n) { return x <= pr 
 
 // ------------------------------- forward ------------------------------------
 template <int R, bool STORE>
-__global__ void __launch_bounds__(256) k_ac2d_fwd_p(Ac2dDev a) {
+__global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = a.zp0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
@@ -98,7 +99,7 @@ __global__ void __launch_bounds__(256) k_ac2d_fwd_p(Ac2dDev a) {
 }
 
 template <int R, bool STORE>
-__global__ void __launch_bounds__(256) k_ac2d_fwd_v(Ac2dDev a) {
+__global__ void __launch_bounds__(512) k_ac2d_fwd_v(Ac2dDev a) {
     const int zr0 = min(a.zvx0, a.zvz0);
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -146,146 +147,136 @@ __global__ void __launch_bounds__(256) k_ac2d_fwd_v(Ac2dDev a) {
 }
 
 // ------------------------------- adjoint ------------------------------------
-// Reverse of the v updates of step t: p^ += D^T e, with e the adjoint of the
-// PML-corrected derivative at each vx / vz node; updates the memory adjoints
-// of the thread's own nodes into the other half of their double buffer, and
-// accumulates the dtbx / dtbz gradient sums (Kahan, FP32).
+// The exact adjoint of step t, in two stencil launches that mirror the forward:
+//
+//   k_ac2d_adj_p : reverse of the vx / vz updates, p^ += Dx^T e_x + Dz^T e_z,
+//                  where e_x, e_z are the adjoint PML terms of the vx / vz nodes
+//                  (arrays written by k_ac2d_adj_v of the step after); then, per
+//                  cell, the reverse of the p update's PML: q = -dtbk p^,
+//                  e_p = q + a_i (q + psi^), psi^ <- b_i (q + psi^), written as
+//                  the arrays e_px, e_pz; Kahan sums of v^ . S_v and p^ . S_p
+//                  for the coefficient gradients.
+//   k_ac2d_adj_v : reverse of the p update, vx^ += Dx^T e_px, vz^ += Dz^T e_pz;
+//                  then, per node, the adjoint PML terms e_x, e_z of step t-1.
+//
+// Every node's e is computed once by its owner and read by its neighbours in
+// the next launch, so no double buffering and no halo recomputation is needed.
+// Entries of e outside a field's update range stay zero.
 template <int R>
-__device__ __forceinline__ float e_vx(const Ac2dDev& a, long long base, int z, int m, int rd) {
-    if (m < a.x0 || m >= a.x1 || z < a.zvx0) return 0.f;
-    const long long o = (long long)z * a.pitch + m;
-    float q = -a.dtbx[o] * a.avx[base + o];
-    if (pml_half(m, a.pr, a.nx)) {
-        float u = q + a.am3[rd * a.mbuf + base + o];
-        return q + a.axh[m] * u;
-    }
-    return q;
-}
-template <int R>
-__device__ __forceinline__ float e_vz(const Ac2dDev& a, long long base, int z, int x, int rd) {
-    if (z < a.zvz0 || z >= a.z1) return 0.f;
-    const long long o = (long long)z * a.pitch + x;
-    float q = -a.dtbz[o] * a.avz[base + o];
-    if ((!a.fsurf && z <= a.pr) || z >= a.pr + a.nz) {
-        float u = q + a.am4[rd * a.mbuf + base + o];
-        return q + a.azh[z] * u;
-    }
-    return q;
-}
-
-template <int R>
-__global__ void __launch_bounds__(256) k_ac2d_adj_p(Ac2dDev a) {
-    int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
-    int z = a.zp0 + blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= a.x1 || z >= a.z1) return;
-    const int t = *a.d_step;
-    const long long slot = (long long)((t - 1) % a.k) * a.sslot;
-    const int rd = t & 1, wr = rd ^ 1;
-    const long long o = (long long)z * a.pitch + x;
-    const bool ownx = z >= a.zvx0, ownz = z >= a.zvz0;
-    const bool px = pml_half(x, a.pr, a.nx);
-    const bool pz = (!a.fsurf && z <= a.pr) || z >= a.pr + a.nz;
-    const float bxc = a.dtbx[o], bzc = a.dtbz[o];
-    const bool mirror = a.fsurf && z <= a.pr + a.P;
-    const int zm = 2 * a.pr - z;
-    const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
-    float gbx = 0.f, gbz = 0.f;
-    for (int s = s0; s < s1; ++s) {
-        const long long base = s * a.fs;
-        float sx = 0.f, sz = 0.f;
-#pragma unroll
-        for (int k = 1; k <= R; ++k) sx = sx + c_fd[k - 1] * (e_vx<R>(a, base, z, x - k + 1, rd) - e_vx<R>(a, base, z, x + k, rd));
-#pragma unroll
-        for (int k = 1; k <= R; ++k) sz = sz + c_fd[k - 1] * (e_vz<R>(a, base, z - k + 1, x, rd) - e_vz<R>(a, base, z + k, x, rd));
-        float dP = a.idx * sx + a.idz * sz;
-        if (mirror) {
-            // p(i, 2-j) = -p(i, j) for j <= 0: the mirror row's adjoint folds back with a minus
-            float sm = 0.f;
-#pragma unroll
-            for (int k = 1; k <= R; ++k) sm = sm + c_fd[k - 1] * (e_vz<R>(a, base, zm - k + 1, x, rd) - e_vz<R>(a, base, zm + k, x, rd));
-            dP = dP - a.idz * sm;
-        }
-        a.ap[base + o] += dP;
-        if (ownx) {
-            const float xh = a.avx[base + o];
-            if (px) {
-                float q = -bxc * xh;
-                a.am3[wr * a.mbuf + base + o] = a.bxh[x] * (q + a.am3[rd * a.mbuf + base + o]);
-            }
-            gbx += xh * a.Svx[slot + base + o];
-        }
-        if (ownz) {
-            const float zh = a.avz[base + o];
-            if (pz) {
-                float q = -bzc * zh;
-                a.am4[wr * a.mbuf + base + o] = a.bzh[z] * (q + a.am4[rd * a.mbuf + base + o]);
-            }
-            gbz += zh * a.Svz[slot + base + o];
-        }
-    }
-    const long long go = (long long)blockIdx.z * a.fs + o;
-    float s, c;
-    s = a.Gbx[go]; c = a.Cbx[go]; kahan_add(s, c, gbx); a.Gbx[go] = s; a.Cbx[go] = c;
-    s = a.Gbz[go]; c = a.Cbz[go]; kahan_add(s, c, gbz); a.Gbz[go] = s; a.Cbz[go] = c;
-}
-
-__device__ __forceinline__ float e_p(const Ac2dDev& a, long long base, int z, int x, int rd, bool xdir) {
-    if (x < a.x0 || x >= a.x1 || z < a.zp0 || z >= a.z1) return 0.f;
-    const long long o = (long long)z * a.pitch + x;
-    float q = -a.dtbk[o] * a.ap[base + o];
-    if (xdir) {
-        if (pml_int(x, a.pr, a.nx)) return q + a.axi[x] * (q + a.am1[rd * a.mbuf + base + o]);
-    } else {
-        if ((!a.fsurf && z < a.pr) || z >= a.pr + a.nz) return q + a.azi[z] * (q + a.am2[rd * a.mbuf + base + o]);
-    }
-    return q;
-}
-
-// Reverse of the p update of step t: vx^ += Dx^T e_px, vz^ += Dz^T e_pz.
-template <int R>
-__global__ void __launch_bounds__(256) k_ac2d_adj_v(Ac2dDev a) {
+__global__ void __launch_bounds__(512) k_ac2d_adj_p(Ac2dDev a) {
     const int zr0 = min(min(a.zvx0, a.zvz0), a.zp0);
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
     const int t = *a.d_step;
     const long long slot = (long long)((t - 1) % a.k) * a.sslot;
-    const int rd = t & 1, wr = rd ^ 1;
     const long long o = (long long)z * a.pitch + x;
-    const bool dox = z >= a.zvx0, doz = z >= a.zvz0, dop = z >= a.zp0;
+    const bool dop = z >= a.zp0, ownx = z >= a.zvx0, ownz = z >= a.zvz0;
     const bool px = pml_int(x, a.pr, a.nx);
     const bool pz = (!a.fsurf && z < a.pr) || z >= a.pr + a.nz;
     const float bk = a.dtbk[o];
+    const float axi = px ? a.axi[x] : 0.f, bxi = px ? a.bxi[x] : 0.f;
+    const float azi = pz ? a.azi[z] : 0.f, bzi = pz ? a.bzi[z] : 0.f;
+    const bool mirror = a.fsurf && z <= a.pr + a.P;
+    const long long om = (long long)(2 * a.pr - z) * a.pitch + x;
+    const int pt = a.pitch;
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
-    float gbk = 0.f;
+    float gbk = 0.f, gbx = 0.f, gbz = 0.f;
     for (int s = s0; s < s1; ++s) {
-        const long long base = s * a.fs;
+        const long long so = s * a.fs + o;
+        if (ownx) gbx += a.avx[so] * a.Svx[slot + so];
+        if (ownz) gbz += a.avz[so] * a.Svz[slot + so];
+        if (!dop) continue;
+        const float* ex = a.aex + so;
+        const float* ez = a.aez + so;
+        float sx = 0.f, sz = 0.f;
+#pragma unroll
+        for (int k = 1; k <= R; ++k) sx = sx + c_fd[k - 1] * (ex[1 - k] - ex[k]);
+#pragma unroll
+        for (int k = 1; k <= R; ++k) sz = sz + c_fd[k - 1] * (ez[(1 - k) * pt] - ez[k * pt]);
+        float dP = a.idx * sx + a.idz * sz;
+        if (mirror) {
+            // p(i, 2-j) = -p(i, j), j <= 0: the adjoint landing on the mirror row folds back with a minus
+            const float* em = a.aez + s * a.fs + om;
+            float sm = 0.f;
+#pragma unroll
+            for (int k = 1; k <= R; ++k) sm = sm + c_fd[k - 1] * (em[(1 - k) * pt] - em[k * pt]);
+            dP = dP - a.idz * sm;
+        }
+        const float ph = a.ap[so] + dP;
+        a.ap[so] = ph;
+        gbk += ph * a.Sp[slot + so];
+        const float q = -bk * ph;
+        float epx = q, epz = q;
+        if (px) {
+            float u = q + a.am1[so];
+            a.am1[so] = bxi * u;
+            epx = q + axi * u;
+        }
+        if (pz) {
+            float u = q + a.am2[so];
+            a.am2[so] = bzi * u;
+            epz = q + azi * u;
+        }
+        a.aepx[so] = epx;
+        a.aepz[so] = epz;
+    }
+    const long long go = (long long)blockIdx.z * a.fs + o;
+    float sm, c;
+    if (dop) { sm = a.Gbk[go]; c = a.Cbk[go]; kahan_add(sm, c, gbk); a.Gbk[go] = sm; a.Cbk[go] = c; }
+    if (ownx) { sm = a.Gbx[go]; c = a.Cbx[go]; kahan_add(sm, c, gbx); a.Gbx[go] = sm; a.Cbx[go] = c; }
+    if (ownz) { sm = a.Gbz[go]; c = a.Cbz[go]; kahan_add(sm, c, gbz); a.Gbz[go] = sm; a.Cbz[go] = c; }
+}
+
+template <int R>
+__global__ void __launch_bounds__(512) k_ac2d_adj_v(Ac2dDev a) {
+    const int zr0 = min(a.zvx0, a.zvz0);
+    int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
+    int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.x1 || z >= a.z1) return;
+    const long long o = (long long)z * a.pitch + x;
+    const bool dox = z >= a.zvx0, doz = z >= a.zvz0;
+    const bool px = pml_half(x, a.pr, a.nx);
+    const bool pz = (!a.fsurf && z <= a.pr) || z >= a.pr + a.nz;
+    const float bxc = a.dtbx[o], bzc = a.dtbz[o];
+    const float axh = px ? a.axh[x] : 0.f, bxh = px ? a.bxh[x] : 0.f;
+    const float azh = pz ? a.azh[z] : 0.f, bzh = pz ? a.bzh[z] : 0.f;
+    const int pt = a.pitch;
+    const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
+    for (int s = s0; s < s1; ++s) {
+        const long long so = s * a.fs + o;
         if (dox) {
+            const float* ep = a.aepx + so;
             float sx = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sx = sx + c_fd[k - 1] * (e_p(a, base, z, x - k, rd, true) - e_p(a, base, z, x + k - 1, rd, true));
-            a.avx[base + o] += a.idx * sx;
+            for (int k = 1; k <= R; ++k) sx = sx + c_fd[k - 1] * (ep[-k] - ep[k - 1]);
+            const float xh = a.avx[so] + a.idx * sx;
+            a.avx[so] = xh;
+            const float q = -bxc * xh;
+            float e = q;
+            if (px) {
+                float u = q + a.am3[so];
+                a.am3[so] = bxh * u;
+                e = q + axh * u;
+            }
+            a.aex[so] = e;
         }
         if (doz) {
+            const float* ep = a.aepz + so;
             float sz = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sz = sz + c_fd[k - 1] * (e_p(a, base, z - k, x, rd, false) - e_p(a, base, z + k - 1, x, rd, false));
-            a.avz[base + o] += a.idz * sz;
+            for (int k = 1; k <= R; ++k) sz = sz + c_fd[k - 1] * (ep[-k * pt] - ep[(k - 1) * pt]);
+            const float zh = a.avz[so] + a.idz * sz;
+            a.avz[so] = zh;
+            const float q = -bzc * zh;
+            float e = q;
+            if (pz) {
+                float u = q + a.am4[so];
+                a.am4[so] = bzh * u;
+                e = q + azh * u;
+            }
+            a.aez[so] = e;
         }
-        if (dop) {
-            const float ph = a.ap[base + o];
-            const float q = -bk * ph;
-            if (px) a.am1[wr * a.mbuf + base + o] = a.bxi[x] * (q + a.am1[rd * a.mbuf + base + o]);
-            if (pz) a.am2[wr * a.mbuf + base + o] = a.bzi[z] * (q + a.am2[rd * a.mbuf + base + o]);
-            gbk += ph * a.Sp[slot + base + o];
-        }
-    }
-    if (dop) {
-        const long long go = (long long)blockIdx.z * a.fs + o;
-        float s = a.Gbk[go], c = a.Cbk[go];
-        kahan_add(s, c, gbk);
-        a.Gbk[go] = s;
-        a.Cbk[go] = c;
     }
 }
 
@@ -454,7 +445,7 @@ struct Ac2dEngine : Engine {
     DevBuf<double> pt_val;
     GraphCache g_fwd, g_rec, g_adj;
     long long launches = 0;
-    int cur_k = 0, cur_S = 0, cur_spt = 1, tile_x = 32, tile_z = 8;
+    int cur_k = 0, cur_S = 0, tile_x = 32;
 
     explicit Ac2dEngine(const owl_ssg_desc& d) {
         desc = d;
@@ -674,7 +665,7 @@ struct Ac2dEngine : Engine {
         }
     }
 
-    Ac2dDev dev(int S, int spt, int k) {
+    Ac2dDev dev(int S, int k) {
         Ac2dDev a{};
         a.nx = nx; a.nz = nz; a.P = P; a.R = R; a.pr = pr; a.pitch = pitch; a.fs = fs;
         a.x0 = R; a.x1 = R + NXp; a.z1 = R + NZp;
@@ -683,7 +674,7 @@ struct Ac2dEngine : Engine {
         a.zvx0 = a.fsurf ? pr : R;
         a.zvz0 = a.fsurf ? pr + 1 : R;
         a.idx = idx; a.idz = idz;
-        a.nshots = S; a.spt = spt;
+        a.nshots = S; a.spt = spt_f;
         a.dtbk = dtbk.p; a.dtbx = dtbx.p; a.dtbz = dtbz.p;
         a.axi = pml_x.p; a.bxi = pml_x.p + pitch; a.axh = pml_x.p + 2 * pitch; a.bxh = pml_x.p + 3 * pitch;
         a.azi = pml_z.p; a.bzi = pml_z.p + NZs; a.azh = pml_z.p + 2 * NZs; a.bzh = pml_z.p + 3 * NZs;
@@ -698,11 +689,11 @@ struct Ac2dEngine : Engine {
         }
         if (ad.p && ad.n >= (size_t)11 * F) {
             a.ap = ad.p; a.avx = ad.p + F; a.avz = ad.p + 2 * F;
-            a.mbuf = F;
-            a.am1 = ad.p + 3 * F; a.am2 = ad.p + 5 * F; a.am3 = ad.p + 7 * F; a.am4 = ad.p + 9 * F;
+            a.am1 = ad.p + 3 * F; a.am2 = ad.p + 4 * F; a.am3 = ad.p + 5 * F; a.am4 = ad.p + 6 * F;
+            a.aex = ad.p + 7 * F; a.aez = ad.p + 8 * F; a.aepx = ad.p + 9 * F; a.aepz = ad.p + 10 * F;
         }
         if (G.p) {
-            long long gg = (long long)((S + spt - 1) / spt) * fs;
+            long long gg = (long long)((S + spt_a - 1) / spt_a) * fs;
             a.Gbk = G.p; a.Gbx = G.p + gg; a.Gbz = G.p + 2 * gg;
             a.Cbk = G.p + 3 * gg; a.Cbx = G.p + 4 * gg; a.Cbz = G.p + 5 * gg;
         }
@@ -726,38 +717,65 @@ struct Ac2dEngine : Engine {
         return q;
     }
 
-    dim3 grid_for(int rows, int S, int spt) const {
-        return dim3((NXp + tile_x - 1) / tile_x, (rows + tile_z - 1) / tile_z, (S + spt - 1) / spt);
+    dim3 grid_for(int rows, int S, int spt, int tz) const {
+        return dim3((NXp + tile_x - 1) / tile_x, (rows + tz - 1) / tz, (S + spt - 1) / spt);
     }
 
-    template <int RR>
-    void launch_step(int kind, const Ac2dDev& a, const PointDev& q, int S) {
-        dim3 b(tile_x, tile_z);
-        const int rows_p = a.z1 - a.zp0;
-        const int rows_v = a.z1 - std::min(a.zvx0, a.zvz0);
-        const int rows_a = a.z1 - std::min(std::min(a.zvx0, a.zvz0), a.zp0);
-        if (kind == 0 || kind == 1) {
-            if (kind == 0) {
-                k_ac2d_fwd_p<RR, false><<<grid_for(rows_p, S, a.spt), b, 0, stream>>>(a);
-                k_ac2d_fwd_v<RR, false><<<grid_for(rows_v, S, a.spt), b, 0, stream>>>(a);
-                k_point_fwd<<<S, 256, 0, stream>>>(q, PT_INJECT | PT_SAMPLE | PT_TICK);
-            } else {
-                k_ac2d_fwd_p<RR, true><<<grid_for(rows_p, S, a.spt), b, 0, stream>>>(a);
-                k_ac2d_fwd_v<RR, true><<<grid_for(rows_v, S, a.spt), b, 0, stream>>>(a);
-                k_point_fwd<<<S, 256, 0, stream>>>(q, PT_INJECT | PT_TICK);
-            }
+    // forward kernels: block tile_x x tz_f, spt_f shots per thread
+    template <int RR, bool STORE>
+    void launch_fwd(int which, const Ac2dDev& a, int S) {
+        dim3 b(tile_x, tz_f);
+        if (which == 0) {
+            k_ac2d_fwd_p<RR, STORE><<<grid_for(a.z1 - a.zp0, S, spt_f, tz_f), b, 0, stream>>>(a);
         } else {
-            k_ac2d_adj_p<RR><<<grid_for(rows_p, S, a.spt), b, 0, stream>>>(a);
-            k_ac2d_adj_v<RR><<<grid_for(rows_a, S, a.spt), b, 0, stream>>>(a);
+            k_ac2d_fwd_v<RR, STORE><<<grid_for(a.z1 - std::min(a.zvx0, a.zvz0), S, spt_f, tz_f), b, 0, stream>>>(a);
+        }
+    }
+
+    // adjoint kernels: block tile_x x tz_a, spt_a shots per thread (one gradient
+    // accumulator group per spt_a shots)
+    template <int RR>
+    void launch_adj(int which, const Ac2dDev& a0, int S) {
+        Ac2dDev a = a0;
+        a.spt = spt_a;
+        dim3 b(tile_x, tz_a);
+        if (which == 0) {
+            const int rows = a.z1 - std::min(std::min(a.zvx0, a.zvz0), a.zp0);
+            k_ac2d_adj_p<RR><<<grid_for(rows, S, spt_a, tz_a), b, 0, stream>>>(a);
+        } else {
+            const int rows = a.z1 - std::min(a.zvx0, a.zvz0);
+            k_ac2d_adj_v<RR><<<grid_for(rows, S, spt_a, tz_a), b, 0, stream>>>(a);
+        }
+    }
+
+    void launch_kernel(int id, const Ac2dDev& a, int S, bool store = false) {
+        if (R == 4) {
+            if (id == OWL_K_FWD_P) store ? launch_fwd<4, true>(0, a, S) : launch_fwd<4, false>(0, a, S);
+            if (id == OWL_K_FWD_V) store ? launch_fwd<4, true>(1, a, S) : launch_fwd<4, false>(1, a, S);
+            if (id == OWL_K_ADJ_P) launch_adj<4>(0, a, S);
+            if (id == OWL_K_ADJ_V) launch_adj<4>(1, a, S);
+        } else {
+            if (id == OWL_K_FWD_P) store ? launch_fwd<8, true>(0, a, S) : launch_fwd<8, false>(0, a, S);
+            if (id == OWL_K_FWD_V) store ? launch_fwd<8, true>(1, a, S) : launch_fwd<8, false>(1, a, S);
+            if (id == OWL_K_ADJ_P) launch_adj<8>(0, a, S);
+            if (id == OWL_K_ADJ_V) launch_adj<8>(1, a, S);
+        }
+    }
+
+    void launch_step(int kind, const Ac2dDev& a, const PointDev& q, int S) {
+        if (kind == 0 || kind == 1) {
+            launch_kernel(OWL_K_FWD_P, a, S, kind == 1);
+            launch_kernel(OWL_K_FWD_V, a, S, kind == 1);
+            k_point_fwd<<<S, 256, 0, stream>>>(q, kind == 0 ? (PT_INJECT | PT_SAMPLE | PT_TICK) : (PT_INJECT | PT_TICK));
+        } else {
+            launch_kernel(OWL_K_ADJ_P, a, S);
+            launch_kernel(OWL_K_ADJ_V, a, S);
             k_point_adj<<<S, 256, 0, stream>>>(q);
         }
         launches += 3;
     }
 
-    void launch_step_any(int kind, const Ac2dDev& a, const PointDev& q, int S) {
-        if (R == 4) launch_step<4>(kind, a, q, S);
-        else launch_step<8>(kind, a, q, S);
-    }
+    void launch_step_any(int kind, const Ac2dDev& a, const PointDev& q, int S) { launch_step(kind, a, q, S); }
 
     // run n steps of a kind (0 forward, 1 recompute storing S, 2 adjoint)
     void run_steps(int kind, int n, const Ac2dDev& a, const PointDev& q, int S, bool graph) {
@@ -768,14 +786,15 @@ struct Ac2dEngine : Engine {
             return;
         }
         GraphCache& gc = kind == 0 ? g_fwd : (kind == 1 ? g_rec : g_adj);
-        std::vector<uintptr_t> sig = {(uintptr_t)n, (uintptr_t)S, (uintptr_t)a.spt, (uintptr_t)a.k,
+        std::vector<uintptr_t> sig = {(uintptr_t)n, (uintptr_t)S, (uintptr_t)spt_f, (uintptr_t)spt_a,
+                                      (uintptr_t)tz_f, (uintptr_t)tz_a, (uintptr_t)a.k,
                                       (uintptr_t)st.p, (uintptr_t)ad.p, (uintptr_t)Sbuf.p, (uintptr_t)G.p,
                                       (uintptr_t)rec.p, (uintptr_t)res.p, (uintptr_t)src_adj.p,
                                       (uintptr_t)q.src_adj, (uintptr_t)inj.ptr.p, (uintptr_t)inj.w.p,
                                       (uintptr_t)smp.ptr.p, (uintptr_t)smp.w.p, (uintptr_t)sct.ptr.p,
                                       (uintptr_t)sct.w.p, (uintptr_t)amp.p, (uintptr_t)inj_shot_ptr.p,
                                       (uintptr_t)rec_shot_ptr.p, (uintptr_t)sct_shot_ptr.p, (uintptr_t)q.rtot,
-                                      (uintptr_t)tile_x, (uintptr_t)tile_z, (uintptr_t)dtbk.p};
+                                      (uintptr_t)tile_x, (uintptr_t)dtbk.p};
         if (!gc.exec || gc.sig != sig) {
             gc.reset();
             cudaGraph_t g;
@@ -801,18 +820,59 @@ struct Ac2dEngine : Engine {
         OWL_CUDA(cudaMemcpyAsync(ctr.p, h, 2 * sizeof(int), cudaMemcpyHostToDevice, stream));
     }
 
-    void resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, int& spt, bool& graph) {
+    bool tune = false;
+    int spt_f = 1, spt_a = 1, tz_f = 8, tz_a = 8;
+    void resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bool& graph) {
+        tune = o.shots_per_cta <= 0 && o.tile_z <= 0;
         B = o.shots_per_launch > 0 ? o.shots_per_launch : std::max(1, desc.max_shots);
         B = std::min(B, std::max(1, nshots));
         k = o.checkpoint_interval > 0 ? o.checkpoint_interval : 50;
         k = std::min(k, desc.nt);
-        spt = o.shots_per_cta > 0 ? o.shots_per_cta : 1;
-        spt = std::min(spt, B);
+        spt_f = spt_a = std::min(o.shots_per_cta > 0 ? o.shots_per_cta : 1, B);
         graph = o.use_graph >= 0;  // default on; -1 disables
         tile_x = o.tile_x > 0 ? o.tile_x : 32;
-        tile_z = o.tile_z > 0 ? o.tile_z : 8;
-        OWL_CHECK(tile_x * tile_z <= 256 && tile_x % 32 == 0, OWL_ERR_INVALID,
-                  "tile_x must be a multiple of 32 and tile_x*tile_z <= 256");
+        tz_f = tz_a = o.tile_z > 0 ? o.tile_z : 8;
+        OWL_CHECK(tile_x % 32 == 0 && tz_f >= 1 && tile_x * tz_f <= 512, OWL_ERR_INVALID,
+                  "tile_x must be a multiple of 32 and tile_x * tile_z <= 512");
+    }
+
+    // Autotuner: times the stencil kernels of one step for each (shots per CTA,
+    // tile height) candidate on this batch's buffers and keeps the fastest, for
+    // the forward pair and the adjoint pair separately. Cached per batch size.
+    // The buffers' contents are reset by the caller afterwards.
+    std::map<std::pair<int, int>, std::array<int, 4>> tune_cache;
+    void autotune(int S, int k, bool grad) {
+        auto key = std::make_pair(S, grad ? 1 : 0);
+        auto it = tune_cache.find(key);
+        if (it != tune_cache.end()) {
+            spt_f = it->second[0]; tz_f = it->second[1]; spt_a = it->second[2]; tz_a = it->second[3];
+            return;
+        }
+        set_step(k);
+        for (int pass = 0; pass < (grad ? 2 : 1); ++pass) {
+            float best = 1e30f;
+            int bs = 1, bt = 8;
+            for (int spt : {1, 2, 4, 8, 16, 32}) {
+                if (spt > S) break;
+                for (int tz : {4, 8, 16}) {
+                    if (pass == 0) { spt_f = spt; tz_f = tz; } else { spt_a = spt; tz_a = tz; }
+                    Ac2dDev a = dev(S, k);
+                    auto run = [&]() {
+                        if (pass == 0) { launch_kernel(OWL_K_FWD_P, a, S); launch_kernel(OWL_K_FWD_V, a, S); }
+                        else { launch_kernel(OWL_K_ADJ_P, a, S); launch_kernel(OWL_K_ADJ_V, a, S); }
+                    };
+                    run();
+                    OWL_LAUNCH_CHECK();
+                    EventTimer tm(stream);
+                    for (int i = 0; i < 5; ++i) run();
+                    float ms = (float)tm.stop_ms();
+                    launches += 12;
+                    if (ms < best) { best = ms; bs = spt; bt = tz; }
+                }
+            }
+            if (pass == 0) { spt_f = bs; tz_f = bt; } else { spt_a = bs; tz_a = bt; }
+        }
+        tune_cache[key] = {spt_f, tz_f, spt_a, tz_a};
     }
 
     size_t seis_count(int n, const owl_shot* shots) const {
@@ -822,9 +882,9 @@ struct Ac2dEngine : Engine {
     }
 
     // forward pass of one batch (state zeroed); optional checkpoints
-    void forward_batch(int S, int spt, int k, bool graph, bool save_ckpt) {
+    void forward_batch(int S, int k, bool graph, bool save_ckpt) {
         const int nt = desc.nt;
-        Ac2dDev a = dev(S, spt, k);
+        Ac2dDev a = dev(S, k);
         PointDev q = pdev(S, false, false);
         OWL_CUDA(cudaMemsetAsync(st.p, 0, sizeof(float) * 7 * S * fs, stream));
         set_step(0);
@@ -859,9 +919,9 @@ struct Ac2dEngine : Engine {
     void forward(int nshots, const owl_shot* shots, const owl_run_opts& o, float* seis, int mem,
                  owl_run_info& info) override {
         OWL_CHECK(model_set, OWL_ERR_INVALID, "set_model must be called first");
-        int B, k, spt;
+        int B, k;
         bool graph;
-        resolve_opts(o, nshots, B, k, spt, graph);
+        resolve_opts(o, nshots, B, k, graph);
         launches = 0;
         EventTimer tm(stream);
         size_t out_off = 0;
@@ -869,10 +929,12 @@ struct Ac2dEngine : Engine {
         for (int b0 = 0; b0 < nshots; b0 += B) {
             int S = std::min(B, nshots - b0);
             build_tables(S, shots + b0, false);
-            ensure_state(S, (S + spt - 1) / spt, k, false);
+            ensure_state(S, S, k, false);
+            if (tune) autotune(S, k, false);
             rec.reserve((size_t)desc.nt * std::max(rtot, 1));
             OWL_CUDA(cudaMemsetAsync(rec.p, 0, sizeof(float) * desc.nt * std::max(rtot, 1), stream));
-            forward_batch(S, spt, k, graph, false);
+            forward_batch(S, k, graph, false);
+            cur_S = S; cur_k = k;
             if (o.check_every > 0) check_nonfinite(st.p, (size_t)S * fs);
             size_t n = (size_t)rtot * desc.nt;
             if (n) {
@@ -889,9 +951,9 @@ struct Ac2dEngine : Engine {
         info.steps_cell_updates = (double)NXp * NZp * desc.nt * nshots;
         info.dt_used = dt;
         info.dt_stable = dt_stable_;
-        info.shots_per_cta = spt;
+        info.shots_per_cta = spt_f;
         info.tile_x = tile_x;
-        info.tile_z = tile_z;
+        info.tile_z = tz_f;
         info.batches = batches;
     }
 
@@ -901,9 +963,9 @@ struct Ac2dEngine : Engine {
         OWL_CHECK(adj_kind == OWL_ADJ_L2_RESIDUAL || adj_kind == OWL_ADJ_GIVEN, OWL_ERR_INVALID, "bad adj_kind");
         OWL_CHECK(o.checkpoint_precision == OWL_CKPT_FP32, OWL_ERR_UNSUPPORTED,
                   "acoustic 2D checkpoints are FP32 in this build");
-        int B, k, spt;
+        int B, k;
         bool graph;
-        resolve_opts(o, nshots, B, k, spt, graph);
+        resolve_opts(o, nshots, B, k, graph);
         launches = 0;
         const int nt = desc.nt;
         const int nxq = NXp + 2, nzq = NZp + 2;
@@ -917,9 +979,10 @@ struct Ac2dEngine : Engine {
         for (int b0 = 0; b0 < nshots; b0 += B) {
             int S = std::min(B, nshots - b0);
             const owl_shot* sh = shots + b0;
-            int groups = (S + spt - 1) / spt;
             build_tables(S, sh, true);
-            ensure_state(S, groups, k, true);
+            ensure_state(S, S, k, true);
+            if (tune) autotune(S, k, true);
+            int groups = (S + spt_a - 1) / spt_a;
             int nseg = (nt + k - 1) / k;
             ckpt.reserve((size_t)nseg * 7 * S * fs);
             size_t nrt = (size_t)nt * std::max(rtot, 1);
@@ -933,7 +996,8 @@ struct Ac2dEngine : Engine {
             src_adj.reserve(std::max<size_t>(1, nitems * nt));
             if (want_src) OWL_CUDA(cudaMemsetAsync(src_adj.p, 0, sizeof(float) * std::max<size_t>(1, nitems * nt), stream));
             // 1. forward with checkpoints
-            forward_batch(S, spt, k, graph, true);
+            forward_batch(S, k, graph, true);
+            cur_S = S; cur_k = k;
             if (o.check_every > 0) check_nonfinite(st.p, (size_t)S * fs);
             // 2. adjoint source
             size_t n = (size_t)rtot * nt;
@@ -963,7 +1027,7 @@ struct Ac2dEngine : Engine {
             long long F = (long long)S * fs;
             OWL_CUDA(cudaMemsetAsync(ad.p, 0, sizeof(float) * 11 * F, stream));
             OWL_CUDA(cudaMemsetAsync(G.p, 0, sizeof(float) * 6 * groups * fs, stream));
-            Ac2dDev a = dev(S, spt, k);
+            Ac2dDev a = dev(S, k);
             PointDev qf = pdev(S, false, false);
             PointDev qa = pdev(S, true, want_src);
             for (int sg = nseg - 1; sg >= 0; --sg) {
@@ -1045,10 +1109,54 @@ struct Ac2dEngine : Engine {
         info.steps_cell_updates = 3.0 * NXp * NZp * nt * nshots;
         info.dt_used = dt;
         info.dt_stable = dt_stable_;
-        info.shots_per_cta = spt;
+        info.shots_per_cta = spt_a;
         info.tile_x = tile_x;
-        info.tile_z = tile_z;
+        info.tile_z = tz_a;
         info.batches = batches;
+    }
+
+    // compulsory bytes of one launch of a kernel (each state field read / written
+    // once per shot, materials once per launch, PML memory only inside the PML,
+    // gradient accumulators once per shot group)
+    double alg_bytes(int id, int S, int groups) const {
+        const double cells = (double)NXp * NZp;
+        double npx_i = 0, npz_i = 0, npx_h = 0, npz_h = 0;
+        const bool fsf = desc.free_surface != 0;
+        for (int x = R; x < R + NXp; ++x) {
+            npx_i += (x < pr || x >= pr + nx) ? NZp : 0;
+            npx_h += (x <= pr || x >= pr + nx) ? NZp : 0;
+        }
+        for (int z = R; z < R + NZp; ++z) {
+            npz_i += ((!fsf && z < pr) || z >= pr + nz) ? NXp : 0;
+            npz_h += ((!fsf && z <= pr) || z >= pr + nz) ? NXp : 0;
+        }
+        switch (id) {
+            case OWL_K_FWD_P: return S * (cells * 16.0 + (npx_i + npz_i) * 8.0) + cells * 4.0;
+            case OWL_K_FWD_V: return S * (cells * 20.0 + (npx_h + npz_h) * 8.0) + cells * 8.0;
+            case OWL_K_ADJ_P: return S * (cells * 44.0 + (npx_i + npz_i) * 8.0) + cells * 4.0 + groups * cells * 48.0;
+            case OWL_K_ADJ_V: return S * (cells * 32.0 + (npx_h + npz_h) * 8.0) + cells * 8.0;
+        }
+        return 0;
+    }
+
+    void kernel_time(int id, int nlaunch, double* avg_ms, double* bytes) override {
+        OWL_CHECK(cur_S > 0, OWL_ERR_INVALID, "no batch has run on this handle");
+        OWL_CHECK(id >= OWL_K_FWD_P && id <= OWL_K_ADJ_V, OWL_ERR_INVALID, "bad kernel id");
+        const int S = cur_S, k = cur_k;
+        OWL_CHECK(id < OWL_K_ADJ_P || (ad.p && G.p && Sbuf.p), OWL_ERR_INVALID,
+                  "adjoint kernels need a gradient call first");
+        Ac2dDev a = dev(S, k);
+        if (id >= OWL_K_ADJ_P)
+            OWL_CHECK(a.ap && a.Sp, OWL_ERR_INVALID, "adjoint buffers too small for the last batch");
+        set_step(k);
+        auto launch = [&]() { launch_kernel(id, a, S); };
+        for (int i = 0; i < 3; ++i) launch();
+        OWL_LAUNCH_CHECK();
+        EventTimer tm(stream);
+        for (int i = 0; i < nlaunch; ++i) launch();
+        OWL_LAUNCH_CHECK();
+        *avg_ms = tm.stop_ms() / nlaunch;
+        *bytes = alg_bytes(id, S, (S + spt_a - 1) / spt_a);
     }
 
     void gradient(int nshots, const owl_shot* shots, const float* data, int adj_kind, const owl_run_opts& o,

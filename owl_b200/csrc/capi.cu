@@ -144,6 +144,13 @@ int owl_ssg_source_gradient(owl_ssg* h, int nshots, const owl_shot* shots, const
     });
 }
 
+int owl_ssg_kernel_time(owl_ssg* h, int kernel_id, int nlaunch, double* avg_ms, double* alg_bytes) {
+    return guarded([&] {
+        OWL_CHECK(h && h->eng && avg_ms && alg_bytes && nlaunch > 0, OWL_ERR_INVALID, "bad arguments");
+        h->eng->kernel_time(kernel_id, nlaunch, avg_ms, alg_bytes);
+    });
+}
+
 void owl_ssg_destroy(owl_ssg* h) {
     if (!h) return;
     try {

@@ -17,6 +17,7 @@ struct Engine {
     virtual void gradient(int nshots, const owl_shot* shots, const float* data, int adj_kind,
                           const owl_run_opts& o, double* misfit, float* grad, float* seis_out, int mem,
                           owl_run_info& info) = 0;
+    virtual void kernel_time(int id, int nlaunch, double* avg_ms, double* alg_bytes) = 0;
     virtual void source_gradient(int nshots, const owl_shot* shots, const float* adj, const owl_run_opts& o,
                                  float* stf_grad, int mem, owl_run_info& info) = 0;
 };

@@ -164,3 +164,9 @@ class SSGSolver:
         L.check(self.lib.owl_ssg_source_gradient(self.h, ps.nshots, ps.arr, _ptr(adj), C.byref(o), _ptr(out),
                                                  L.OWL_MEM_HOST, C.byref(self.last_info)))
         return out
+
+    def kernel_time(self, kernel_id: int, nlaunch: int = 20) -> Tuple[float, float]:
+        """(mean ms per launch, algorithmic bytes per launch) of one kernel on the last batch state."""
+        ms, b = C.c_double(), C.c_double()
+        L.check(self.lib.owl_ssg_kernel_time(self.h, kernel_id, nlaunch, C.byref(ms), C.byref(b)))
+        return ms.value, b.value
