@@ -1,0 +1,717 @@
+// ssg_base.cu -- medium-independent host engine and point / checkpoint kernels.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+
+#include "ssg_base.cuh"
+
+namespace owl {
+
+// ------------------------------ point operators ----------------------------
+// One CTA per shot. Forward: add_source(t) (sources in order, taps of one
+// source in parallel, as the reference's loops), then record the receivers of
+// step t+1 (each trace a sequential sum over its taps). The last CTA advances
+// the device step counter, so one captured graph serves every segment.
+__global__ void k_point_fwd(PointDev a, int mode) {
+    const int s = blockIdx.x;
+    const int cur = *a.d_step;
+    const int t = cur + 1;
+    if (mode & PT_INJECT) {
+        for (int it = a.inj_shot_ptr[s]; it < a.inj_shot_ptr[s + 1]; ++it) {
+            const float A = a.amp[(size_t)it * a.nt + (t - 1)];
+            if (A != 0.f) {
+                for (int j = a.inj.ptr[it] + threadIdx.x; j < a.inj.ptr[it + 1]; j += blockDim.x) {
+                    float* f = a.fld[a.inj.field[j]] + s * a.sstride + a.inj.off[j];
+                    *f = *f + A * a.inj.w[j];
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (mode & PT_SAMPLE) {
+        const int tr = (mode & PT_INJECT) ? t + 1 : t;
+        if (tr <= a.nt) {
+            for (int r = a.rec_shot_ptr[s] + threadIdx.x; r < a.rec_shot_ptr[s + 1]; r += blockDim.x) {
+                float acc = 0.f;
+                for (int j = a.smp.ptr[r]; j < a.smp.ptr[r + 1]; ++j)
+                    acc = acc + a.fld[a.smp.field[j]][s * a.sstride + a.smp.off[j]] * a.smp.w[j];
+                a.rec[(size_t)(tr - 1) * a.rtot + r] = acc;
+            }
+        }
+    }
+    if (mode & PT_TICK) tick_last_block(a.d_step, a.d_done, 1);
+}
+
+// Adjoint of the sampling of step t (residual into the adjoint fields, one
+// thread per distinct target node, contributions summed in a fixed order),
+// then the source-side adjoint taps . lambda_{t-1}; the last CTA steps back.
+__global__ void k_point_adj(PointDev a) {
+    const int s = blockIdx.x;
+    const int t = *a.d_step;
+    for (int it = a.sct_shot_ptr[s] + threadIdx.x; it < a.sct_shot_ptr[s + 1]; it += blockDim.x) {
+        float acc = 0.f;
+        const int j0 = a.sct.ptr[it], j1 = a.sct.ptr[it + 1];
+        for (int j = j0; j < j1; ++j) acc = acc + a.res[(size_t)(t - 1) * a.rtot + a.sct.item[j]] * a.sct.w[j];
+        float* f = a.fld[a.sct.field[j0]] + s * a.sstride + a.sct.off[j0];
+        *f = *f + acc;
+    }
+    __syncthreads();
+    if (a.src_adj && t - 1 >= 1) {
+        for (int it = a.inj_shot_ptr[s] + threadIdx.x; it < a.inj_shot_ptr[s + 1]; it += blockDim.x) {
+            float acc = 0.f;
+            for (int j = a.inj.ptr[it]; j < a.inj.ptr[it + 1]; ++j)
+                acc = acc + a.fld[a.inj.field[j]][s * a.sstride + a.inj.off[j]] * a.inj.w[j];
+            a.src_adj[(size_t)it * a.nt + (t - 2)] = acc;
+        }
+    }
+    tick_last_block(a.d_step, a.d_done, -1);
+}
+
+void launch_point_fwd(const PointDev& q, int S, int mode, cudaStream_t s) { k_point_fwd<<<S, 256, 0, s>>>(q, mode); }
+void launch_point_adj(const PointDev& q, int S, cudaStream_t s) { k_point_adj<<<S, 256, 0, s>>>(q); }
+
+// ------------------------- compressed checkpoints ---------------------------
+// Per (shot, state field) scale = max |x|; values stored as x / scale in FP16 or
+// BF16. Blocks: (segment, shot); each block loops over its segment.
+struct SegDev {
+    const long long* off;
+    const long long* len;
+    int nseg;
+};
+
+__global__ void k_absmax(const float* __restrict__ st, long long sstride, SegDev sg, float* __restrict__ scale) {
+    const int g = blockIdx.x, s = blockIdx.y;
+    const float* p = st + s * sstride + sg.off[g];
+    const long long n = sg.len[g];
+    float m = 0.f;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, fabsf(p[i]));
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float r = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmaxf(r, red[w]);
+        scale[s * sg.nseg + g] = r;
+    }
+}
+
+template <bool BF16>
+__global__ void k_pack(const float* __restrict__ st, long long sstride, SegDev sg, const float* __restrict__ scale,
+                       unsigned short* __restrict__ out) {
+    const int g = blockIdx.x, s = blockIdx.y;
+    const float* p = st + s * sstride + sg.off[g];
+    unsigned short* q = out + s * sstride + sg.off[g];
+    const long long n = sg.len[g];
+    const float sc = scale[s * sg.nseg + g];
+    const float inv = sc > 0.f ? 1.0f / sc : 0.f;
+    for (long long i = blockIdx.z * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.z * blockDim.x) {
+        float v = p[i] * inv;
+        if (BF16) {
+            __nv_bfloat16 h = __float2bfloat16_rn(v);
+            q[i] = *reinterpret_cast<unsigned short*>(&h);
+        } else {
+            __half h = __float2half_rn(v);
+            q[i] = *reinterpret_cast<unsigned short*>(&h);
+        }
+    }
+}
+
+template <bool BF16>
+__global__ void k_unpack(const unsigned short* __restrict__ in, long long sstride, SegDev sg,
+                         const float* __restrict__ scale, float* __restrict__ st) {
+    const int g = blockIdx.x, s = blockIdx.y;
+    float* p = st + s * sstride + sg.off[g];
+    const unsigned short* q = in + s * sstride + sg.off[g];
+    const long long n = sg.len[g];
+    const float sc = scale[s * sg.nseg + g];
+    for (long long i = blockIdx.z * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.z * blockDim.x) {
+        unsigned short u = q[i];
+        float v;
+        if (BF16) v = __bfloat162float(*reinterpret_cast<__nv_bfloat16*>(&u));
+        else v = __half2float(*reinterpret_cast<__half*>(&u));
+        p[i] = v * sc;
+    }
+}
+
+// ------------------------------ fold ----------------------------------------
+// Padded-grid FP64 gradient -> model cells (adjoint of pad_array's edge
+// replication), output (nz[,ny],nx) with z fastest.
+__global__ void k_fold(const double* __restrict__ gp, int nxq, int nyq, int P, int nx, int ny, int nz, int dim,
+                       float* __restrict__ out) {
+    const long long n = (long long)nx * ny * nz;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int iz = (int)(q % nz) + 1;
+        const long long r = q / nz;
+        const int iy = (int)(r % ny) + 1, ix = (int)(r / ny) + 1;
+        const int xa = ix == 1 ? -P : ix, xb = ix == nx ? nx + P + 1 : ix;
+        const int za = iz == 1 ? -P : iz, zb = iz == nz ? nz + P + 1 : iz;
+        int ya = 0, yb = 0;
+        if (dim == 3) { ya = iy == 1 ? -P : iy; yb = iy == ny ? ny + P + 1 : iy; }
+        double acc = 0;
+        for (int k = za; k <= zb; ++k)
+            for (int j = ya; j <= yb; ++j)
+                for (int i = xa; i <= xb; ++i)
+                    acc += gp[((long long)(k + P) * nyq + (dim == 3 ? j + P : 0)) * nxq + (i + P)];
+        out[q] = (float)acc;
+    }
+}
+
+__global__ void k_add_points_f64(double* g, const long long* idx, const double* val, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) g[idx[i]] += val[i];
+}
+
+// ============================================================================
+// host side
+// ============================================================================
+SsgBase::SsgBase(const owl_ssg_desc& d, int dim_) {
+    desc = d;
+    dim = dim_;
+    OWL_CHECK(d.nx >= 8 && d.nz >= 8 && (dim == 2 || d.ny >= 8), OWL_ERR_INVALID, "grid dimensions must be >= 8");
+    OWL_CHECK(d.fdhalf == 4 || d.fdhalf == 8, OWL_ERR_INVALID, "fdhalf must be 4 or 8");
+    OWL_CHECK(d.pml >= 1, OWL_ERR_INVALID, "pml must be >= 1");
+    OWL_CHECK(d.dx > 0 && d.dz > 0 && (dim == 2 || d.dy > 0) && d.dt > 0 && d.nt >= 1, OWL_ERR_INVALID,
+              "dx, dy, dz, dt, nt must be positive");
+    nx = d.nx; ny = dim == 3 ? d.ny : 1; nz = d.nz;
+    P = d.pml; R = d.fdhalf; pr = P + R;
+    NXp = nx + 2 * P; NYp = dim == 3 ? ny + 2 * P : 1; NZp = nz + 2 * P;
+    NXs = NXp + 2 * R; NYs = dim == 3 ? NYp + 2 * R : 1; NZs = NZp + 2 * R;
+    pitch = (NXs + 31) / 32 * 32;
+    plane = (long long)pitch * NYs;
+    fs = plane * NZs;
+    dt = d.dt;
+    OWL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    ctr.reserve(4);
+}
+
+SsgBase::~SsgBase() {
+    invalidate_graphs();
+    if (stream) cudaStreamDestroy(stream);
+}
+
+void SsgBase::invalidate_graphs() {
+    g_fwd.reset();
+    g_rec.reset();
+    g_adj.reset();
+}
+
+DevBuf<long long>& SsgBase::seg_off() {
+    const size_t n = st_segments.size();
+    if (segbuf.n < 2 * n || !segbuf.p) {
+        std::vector<long long> h(2 * n);
+        for (size_t i = 0; i < n; ++i) { h[i] = st_segments[i].first; h[n + i] = st_segments[i].second; }
+        segbuf.upload(h.data(), h.size(), stream);
+    }
+    return segbuf;
+}
+
+void SsgBase::set_step(int v) {
+    int h[2] = {v, 0};
+    OWL_CUDA(cudaMemcpyAsync(ctr.p, h, 2 * sizeof(int), cudaMemcpyHostToDevice, stream));
+}
+
+void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
+    HostCSR hinj, hsmp, hsct;
+    std::vector<int> hinj_ptr(1, 0), hrec_ptr(1, 0), hsct_ptr(1, 0);
+    std::vector<float> hamp;
+    std::vector<unsigned char> hlive;
+    item_src.clear(); item_comp.clear(); item_shot.clear(); item_rho_cell.clear(); item_rho.clear();
+    const int nt = desc.nt;
+    std::vector<TapPt> taps, mapped;
+    rtot = 0;
+    for (int s = 0; s < S; ++s) {
+        const owl_shot& sh = shots[s];
+        OWL_CHECK(sh.nsrc >= 0 && sh.nrec >= 0 && (sh.nsrc == 0 || sh.src) && (sh.nrec == 0 || sh.rec),
+                  OWL_ERR_INVALID, "bad shot arrays");
+        for (int kk = 0; kk < sh.nsrc; ++kk) {
+            const owl_source& q = sh.src[kk];
+            OWL_CHECK(q.nt_stf >= 0 && (q.nt_stf == 0 || q.stf), OWL_ERR_INVALID, "bad source STF");
+            const int nc = src_ncomp(q);
+            for (int comp = 0; comp < nc; ++comp) {
+                taps.clear();
+                long long rc = -1;
+                float rv = 0.f;
+                src_taps(q, comp, taps, rc, rv);
+                for (const TapPt& t : taps) {
+                    if (t.w == 0.f) continue;
+                    OWL_CHECK(in_wavefield(t.i, t.j, t.k), OWL_ERR_INVALID, "source tap outside the padded grid");
+                    hinj.push(Tap{t.field, s, soff(t.i, t.j, t.k), t.w, 0});
+                }
+                hinj.close_item();
+                item_src.push_back(kk); item_comp.push_back(comp); item_shot.push_back(s);
+                item_rho_cell.push_back(rc); item_rho.push_back(rv);
+                size_t base = hamp.size();
+                hamp.resize(base + nt, 0.f);
+                for (int t = std::max(1, q.nbeg); t <= q.nbeg + q.nt_stf - 1 && t <= nt; ++t)
+                    hamp[base + t - 1] = q.stf[t - q.nbeg] * q.amp * dt;
+            }
+        }
+        hinj_ptr.push_back(hinj.nitems());
+        std::map<std::pair<int, long long>, std::vector<std::pair<int, float>>> cells;
+        for (int comp = 0; comp < ncomp; ++comp) {
+            for (int r = 0; r < sh.nrec; ++r) {
+                const owl_receiver& q = sh.rec[r];
+                const int rg = rtot + comp * sh.nrec + r;
+                hlive.push_back(q.weight != 0.f);
+                if (q.weight != 0.f) {
+                    taps.clear();
+                    rec_taps(q, comp, taps);
+                    for (const TapPt& t : taps) {
+                        if (t.w == 0.f) continue;
+                        OWL_CHECK(in_wavefield(t.i, t.j, t.k), OWL_ERR_INVALID, "receiver tap outside the padded grid");
+                        hsmp.push(Tap{t.field, s, soff(t.i, t.j, t.k), t.w, rg});
+                        if (need_sct) {
+                            mapped.clear();
+                            scatter_map(t, mapped);
+                            for (const TapPt& m : mapped)
+                                cells[{m.field, soff(m.i, m.j, m.k)}].push_back({rg, m.w});
+                        }
+                    }
+                }
+                hsmp.close_item();
+            }
+        }
+        for (auto& kv : cells) {
+            for (auto& e : kv.second) hsct.push(Tap{kv.first.first, s, kv.first.second, e.second, e.first});
+            hsct.close_item();
+        }
+        rtot += ncomp * sh.nrec;
+        hrec_ptr.push_back(rtot);
+        hsct_ptr.push_back(hsct.nitems());
+    }
+    inj.upload(hinj, stream);
+    smp.upload(hsmp, stream);
+    sct.upload(hsct, stream);
+    inj_shot_ptr.upload(hinj_ptr.data(), hinj_ptr.size(), stream);
+    rec_shot_ptr.upload(hrec_ptr.data(), hrec_ptr.size(), stream);
+    sct_shot_ptr.upload(hsct_ptr.data(), hsct_ptr.size(), stream);
+    amp.upload(hamp.data(), hamp.size(), stream);
+    live.upload(hlive.data(), hlive.size(), stream);
+}
+
+void SsgBase::ensure_state(int S, int k, bool grad) {
+    st.reserve((size_t)sst * S);
+    if (grad) {
+        ad.reserve((size_t)sad * S);
+        G.reserve((size_t)2 * ngrad * S * fs);
+        Sbuf.reserve((size_t)nS * k * S * fs);
+    }
+}
+
+PointDev SsgBase::pdev(int S, bool adjoint, bool want_src_adj) {
+    PointDev q{};
+    for (int f = 0; f < MAX_PT_FIELDS; ++f) q.fld[f] = nullptr;
+    for (int f = 0; f < MAX_PT_FIELDS; ++f) {
+        float* p = adjoint ? ad_field(f) : st_field(f);
+        if (!p) break;
+        q.fld[f] = p;
+    }
+    q.sstride = adjoint ? sad : sst;
+    q.nt = desc.nt;
+    q.rtot = rtot;
+    q.inj = view(inj); q.inj_shot_ptr = inj_shot_ptr.p; q.amp = amp.p;
+    q.smp = view(smp); q.rec_shot_ptr = rec_shot_ptr.p; q.rec = rec.p;
+    q.sct = view(sct); q.sct_shot_ptr = sct_shot_ptr.p; q.res = res.p;
+    q.src_adj = want_src_adj ? src_adj.p : nullptr;
+    q.d_step = ctr.p; q.d_done = ctr.p + 1;
+    return q;
+}
+
+void SsgBase::launch_step(int kind, int S, const PointDev& q) {
+    if (kind == 0 || kind == 1) {
+        launch_kernel(OWL_K_FWD_P, S, kind == 1);
+        launch_kernel(OWL_K_FWD_V, S, kind == 1);
+        launch_point_fwd(q, S, kind == 0 ? (PT_INJECT | PT_SAMPLE | PT_TICK) : (PT_INJECT | PT_TICK), stream);
+    } else {
+        launch_kernel(OWL_K_ADJ_P, S, false);
+        launch_kernel(OWL_K_ADJ_V, S, false);
+        launch_point_adj(q, S, stream);
+    }
+    launches += 3;
+}
+
+void SsgBase::run_steps(int kind, int n, int S, const PointDev& q, bool graph) {
+    if (n <= 0) return;
+    if (!graph) {
+        for (int i = 0; i < n; ++i) launch_step(kind, S, q);
+        OWL_LAUNCH_CHECK();
+        return;
+    }
+    GraphCache& gc = kind == 0 ? g_fwd : (kind == 1 ? g_rec : g_adj);
+    std::vector<uintptr_t> sig = {(uintptr_t)n, (uintptr_t)S, (uintptr_t)spt_f, (uintptr_t)spt_a, (uintptr_t)tz_f,
+                                  (uintptr_t)tz_a, (uintptr_t)cur_k, (uintptr_t)tile_x, (uintptr_t)st.p,
+                                  (uintptr_t)ad.p, (uintptr_t)Sbuf.p, (uintptr_t)G.p, (uintptr_t)rec.p,
+                                  (uintptr_t)res.p, (uintptr_t)q.src_adj, (uintptr_t)inj.ptr.p, (uintptr_t)inj.w.p,
+                                  (uintptr_t)inj.off.p, (uintptr_t)smp.ptr.p, (uintptr_t)smp.w.p, (uintptr_t)smp.off.p,
+                                  (uintptr_t)sct.ptr.p, (uintptr_t)sct.w.p, (uintptr_t)sct.off.p, (uintptr_t)amp.p,
+                                  (uintptr_t)inj_shot_ptr.p, (uintptr_t)rec_shot_ptr.p, (uintptr_t)sct_shot_ptr.p,
+                                  (uintptr_t)q.rtot};
+    if (!gc.exec || gc.sig != sig) {
+        gc.reset();
+        cudaGraph_t g;
+        OWL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        long long l0 = launches;
+        for (int i = 0; i < n; ++i) launch_step(kind, S, q);
+        cudaError_t e1 = cudaGetLastError();
+        cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+        OWL_CUDA(e1);
+        OWL_CUDA(e2);
+        launches = l0;
+        cudaError_t e3 = cudaGraphInstantiate(&gc.exec, g, 0);
+        cudaGraphDestroy(g);
+        OWL_CUDA(e3);
+        gc.sig = sig;
+    }
+    OWL_CUDA(cudaGraphLaunch(gc.exec, stream));
+    launches += 3LL * n;
+}
+
+void SsgBase::resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bool& graph) {
+    tune = o.shots_per_cta <= 0 && o.tile_z <= 0;
+    B = o.shots_per_launch > 0 ? o.shots_per_launch : std::max(1, desc.max_shots);
+    B = std::min(B, std::max(1, nshots));
+    k = o.checkpoint_interval > 0 ? o.checkpoint_interval : 50;
+    k = std::min(k, desc.nt);
+    spt_f = spt_a = std::min(o.shots_per_cta > 0 ? o.shots_per_cta : 1, B);
+    graph = o.use_graph >= 0;
+    tile_x = o.tile_x > 0 ? o.tile_x : 32;
+    tz_f = tz_a = o.tile_z > 0 ? o.tile_z : (dim == 3 ? 4 : 8);
+    OWL_CHECK(tile_x % 32 == 0 && tz_f >= 1 && tile_x * tz_f <= 512, OWL_ERR_INVALID,
+              "tile_x must be a multiple of 32 and tile_x * tile_z <= 512");
+    OWL_CHECK(o.checkpoint_precision >= OWL_CKPT_FP32 && o.checkpoint_precision <= OWL_CKPT_BF16, OWL_ERR_INVALID,
+              "bad checkpoint precision");
+    ckpt_prec = o.checkpoint_precision;
+}
+
+// Times the stencil kernels of one step for each (shots per CTA, tile height)
+// candidate on this batch's buffers, forward pair and adjoint pair separately,
+// and keeps the fastest. Cached per (batch size, gradient). The buffers'
+// contents are reset by the caller afterwards.
+void SsgBase::autotune(int S, int k, bool grad) {
+    auto key = std::make_pair(S, grad ? 1 : 0);
+    auto it = tune_cache.find(key);
+    if (it != tune_cache.end()) {
+        spt_f = it->second[0]; tz_f = it->second[1]; spt_a = it->second[2]; tz_a = it->second[3];
+        return;
+    }
+    cur_k = k;
+    set_step(k);
+    const std::vector<int> tzs = dim == 3 ? std::vector<int>{2, 4, 8} : std::vector<int>{4, 8, 16};
+    for (int pass = 0; pass < (grad ? 2 : 1); ++pass) {
+        float best = 1e30f;
+        int bs = 1, bt = tzs[1];
+        for (int spt : {1, 2, 4, 8, 16, 32}) {
+            if (spt > S) break;
+            for (int tz : tzs) {
+                if (pass == 0) { spt_f = spt; tz_f = tz; } else { spt_a = spt; tz_a = tz; }
+                auto run = [&]() {
+                    if (pass == 0) { launch_kernel(OWL_K_FWD_P, S, false); launch_kernel(OWL_K_FWD_V, S, false); }
+                    else { launch_kernel(OWL_K_ADJ_P, S, false); launch_kernel(OWL_K_ADJ_V, S, false); }
+                };
+                run();
+                OWL_LAUNCH_CHECK();
+                EventTimer tm(stream);
+                for (int i = 0; i < 3; ++i) run();
+                float ms = (float)tm.stop_ms();
+                launches += 8;
+                if (ms < best) { best = ms; bs = spt; bt = tz; }
+            }
+        }
+        if (pass == 0) { spt_f = bs; tz_f = bt; } else { spt_a = bs; tz_a = bt; }
+    }
+    tune_cache[key] = {spt_f, tz_f, spt_a, tz_a};
+}
+
+void SsgBase::save_ckpt(int slot, int S) {
+    const size_t n = (size_t)sst * S;
+    if (ckpt_prec == OWL_CKPT_FP32) {
+        OWL_CUDA(cudaMemcpyAsync(ckpt.p + slot * n, st.p, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream));
+        return;
+    }
+    const int nseg = (int)st_segments.size();
+    DevBuf<long long>& so = seg_off();
+    SegDev sg{so.p, so.p + nseg, nseg};
+    float* sc = ck_scale.p + (size_t)slot * S * nseg;
+    dim3 g1(nseg, S);
+    k_absmax<<<g1, 256, 0, stream>>>(st.p, sst, sg, sc);
+    dim3 g2(nseg, S, 64);
+    if (ckpt_prec == OWL_CKPT_BF16) k_pack<true><<<g2, 256, 0, stream>>>(st.p, sst, sg, sc, ckpt16.p + slot * n);
+    else k_pack<false><<<g2, 256, 0, stream>>>(st.p, sst, sg, sc, ckpt16.p + slot * n);
+    OWL_LAUNCH_CHECK();
+    launches += 2;
+}
+
+void SsgBase::restore_ckpt(int slot, int S) {
+    const size_t n = (size_t)sst * S;
+    if (ckpt_prec == OWL_CKPT_FP32) {
+        OWL_CUDA(cudaMemcpyAsync(st.p, ckpt.p + slot * n, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream));
+        return;
+    }
+    const int nseg = (int)st_segments.size();
+    DevBuf<long long>& so = seg_off();
+    SegDev sg{so.p, so.p + nseg, nseg};
+    const float* sc = ck_scale.p + (size_t)slot * S * nseg;
+    dim3 g2(nseg, S, 64);
+    if (ckpt_prec == OWL_CKPT_BF16) k_unpack<true><<<g2, 256, 0, stream>>>(ckpt16.p + slot * n, sst, sg, sc, st.p);
+    else k_unpack<false><<<g2, 256, 0, stream>>>(ckpt16.p + slot * n, sst, sg, sc, st.p);
+    OWL_LAUNCH_CHECK();
+    launches += 1;
+}
+
+void SsgBase::forward_batch(int S, int k, bool graph, bool save) {
+    const int nt = desc.nt;
+    cur_k = k;
+    PointDev q = pdev(S, false, false);
+    OWL_CUDA(cudaMemsetAsync(st.p, 0, sizeof(float) * sst * S, stream));
+    set_step(0);
+    launch_point_fwd(q, S, PT_SAMPLE, stream);
+    OWL_LAUNCH_CHECK();
+    launches++;
+    const int nseg = (nt + k - 1) / k;
+    for (int sg = 0; sg < nseg; ++sg) {
+        if (save) save_ckpt(sg, S);
+        const int n = std::min(k, nt - sg * k);
+        run_steps(0, n, S, q, graph && n == k);
+    }
+}
+
+void SsgBase::check_nonfinite(const float* f, size_t n) {
+    OWL_CUDA(cudaMemsetAsync(ctr.p + 2, 0, sizeof(int), stream));
+    launch_check_finite(f, n, ctr.p + 2, stream);
+    launches++;
+    int flag = 0;
+    OWL_CUDA(cudaMemcpyAsync(&flag, ctr.p + 2, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    OWL_CUDA(cudaStreamSynchronize(stream));
+    if (flag) throw OwlError(OWL_ERR_NONFINITE, "non-finite values in the wavefield");
+}
+
+void SsgBase::copy_out(void* dst, const void* src, size_t bytes, int mem) {
+    OWL_CUDA(cudaMemcpyAsync(dst, src, bytes,
+                             mem == OWL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream));
+}
+
+void SsgBase::fill_info(owl_run_info& info, int nshots, int batches, bool grad) {
+    info.gpu_launches = launches;
+    info.steps_cell_updates = (grad ? 3.0 : 1.0) * (double)NXp * NYp * NZp * desc.nt * nshots;
+    info.dt_used = dt;
+    info.dt_stable = dt_stable_;
+    info.shots_per_cta = grad ? spt_a : spt_f;
+    info.tile_x = tile_x;
+    info.tile_z = grad ? tz_a : tz_f;
+    info.batches = batches;
+}
+
+void SsgBase::forward(int nshots, const owl_shot* shots, const owl_run_opts& o, float* seis, int mem,
+                      owl_run_info& info) {
+    OWL_CHECK(model_set, OWL_ERR_INVALID, "set_model must be called first");
+    int B, k;
+    bool graph;
+    resolve_opts(o, nshots, B, k, graph);
+    launches = 0;
+    EventTimer tm(stream);
+    size_t out_off = 0;
+    int batches = 0;
+    for (int b0 = 0; b0 < nshots; b0 += B) {
+        const int S = std::min(B, nshots - b0);
+        build_tables(S, shots + b0, false);
+        ensure_state(S, k, false);
+        cur_S = S;
+        if (tune) autotune(S, k, false);
+        const size_t nrt = (size_t)desc.nt * std::max(rtot, 1);
+        rec.reserve(nrt);
+        OWL_CUDA(cudaMemsetAsync(rec.p, 0, sizeof(float) * nrt, stream));
+        forward_batch(S, k, graph, false);
+        if (o.check_every > 0) check_nonfinite(st.p, (size_t)S * sst);
+        const size_t n = (size_t)rtot * desc.nt;
+        if (n) {
+            seis_tmp.reserve(n);
+            launch_transpose_rec_to_seis(rec.p, seis_tmp.p, desc.nt, rtot, stream);
+            launches++;
+            copy_out(seis + out_off, seis_tmp.p, n * sizeof(float), mem);
+        }
+        out_off += n;
+        batches++;
+    }
+    info.elapsed_ms = tm.stop_ms();
+    fill_info(info, nshots, batches, false);
+}
+
+void SsgBase::fold_out(float* grad, int mem) {
+    const size_t nm = (size_t)nx * ny * nz;
+    seis_tmp.reserve((size_t)nparam * nm);
+    for (int p = 0; p < nparam; ++p) {
+        k_fold<<<148 * 4, 256, 0, stream>>>(gpad.p + (size_t)p * npad(), nxq(), nyq(), P, nx, ny, nz, dim,
+                                            seis_tmp.p + (size_t)p * nm);
+        launches++;
+    }
+    OWL_LAUNCH_CHECK();
+    copy_out(grad, seis_tmp.p, (size_t)nparam * nm * sizeof(float), mem);
+}
+
+void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data, int adj_kind, const owl_run_opts& o,
+                            double* misfit, float* grad, float* seis_out, float* stf_grad, int mem,
+                            owl_run_info& info) {
+    OWL_CHECK(model_set, OWL_ERR_INVALID, "set_model must be called first");
+    OWL_CHECK(adj_kind == OWL_ADJ_L2_RESIDUAL || adj_kind == OWL_ADJ_GIVEN, OWL_ERR_INVALID, "bad adj_kind");
+    int B, k;
+    bool graph;
+    resolve_opts(o, nshots, B, k, graph);
+    launches = 0;
+    const int nt = desc.nt;
+    EventTimer tm(stream);
+    gpad.reserve((size_t)nparam * npad());
+    OWL_CUDA(cudaMemsetAsync(gpad.p, 0, sizeof(double) * nparam * npad(), stream));
+    size_t data_off = 0, stf_off = 0;
+    int batches = 0, shot0 = 0;
+    for (int b0 = 0; b0 < nshots; b0 += B) {
+        const int S = std::min(B, nshots - b0);
+        const owl_shot* sh = shots + b0;
+        build_tables(S, sh, true);
+        ensure_state(S, k, true);
+        cur_S = S;
+        cur_k = k;
+        if (tune) autotune(S, k, true);
+        const int groups = (S + spt_a - 1) / spt_a;
+        const int nseg = (nt + k - 1) / k;
+        if (ckpt_prec == OWL_CKPT_FP32) {
+            ckpt.reserve((size_t)nseg * sst * S);
+        } else {
+            ckpt16.reserve((size_t)nseg * sst * S);
+            ck_scale.reserve((size_t)nseg * S * st_segments.size());
+        }
+        const size_t nrt = (size_t)nt * std::max(rtot, 1);
+        rec.reserve(nrt);
+        res.reserve(nrt);
+        obs_t.reserve(nrt);
+        OWL_CUDA(cudaMemsetAsync(rec.p, 0, sizeof(float) * nrt, stream));
+        bool want_src = stf_grad != nullptr;
+        for (long long rc : item_rho_cell) want_src |= rc >= 0;
+        const size_t nitems = item_src.size();
+        src_adj.reserve(std::max<size_t>(1, nitems * nt));
+        if (want_src) OWL_CUDA(cudaMemsetAsync(src_adj.p, 0, sizeof(float) * std::max<size_t>(1, nitems * nt), stream));
+        // 1. forward with checkpoints
+        forward_batch(S, k, graph, true);
+        if (o.check_every > 0) check_nonfinite(st.p, (size_t)S * sst);
+        // 2. adjoint source and misfit
+        const size_t n = (size_t)rtot * nt;
+        misfit_d.reserve(S);
+        OWL_CUDA(cudaMemsetAsync(misfit_d.p, 0, sizeof(double) * S, stream));
+        if (n) {
+            seis_tmp.reserve(n);
+            OWL_CUDA(cudaMemcpyAsync(seis_tmp.p, data + data_off, n * sizeof(float),
+                                     mem == OWL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+            launch_transpose_seis_to_rec(seis_tmp.p, obs_t.p, nt, rtot, stream);
+            launches++;
+            if (adj_kind == OWL_ADJ_L2_RESIDUAL)
+                launch_residual_l2(rec.p, obs_t.p, res.p, live.p, rec_shot_ptr.p, S, nt, rtot, misfit_d.p, stream);
+            else
+                OWL_CUDA(cudaMemcpyAsync(res.p, obs_t.p, n * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+            launches++;
+            if (seis_out) {
+                launch_transpose_rec_to_seis(rec.p, seis_tmp.p, nt, rtot, stream);
+                launches++;
+                copy_out(seis_out + data_off, seis_tmp.p, n * sizeof(float), mem);
+            }
+        }
+        if (misfit) copy_out(misfit + shot0, misfit_d.p, sizeof(double) * S, mem);
+        // 3. reverse sweep: restore a checkpoint, recompute its segment storing
+        //    the stencil terms, run the exact adjoint back through it
+        OWL_CUDA(cudaMemsetAsync(ad.p, 0, sizeof(float) * sad * S, stream));
+        OWL_CUDA(cudaMemsetAsync(G.p, 0, sizeof(float) * 2 * ngrad * groups * fs, stream));
+        PointDev qf = pdev(S, false, false);
+        PointDev qa = pdev(S, true, want_src);
+        for (int sg = nseg - 1; sg >= 0; --sg) {
+            const int n0 = sg * k, nn = std::min(k, nt - n0);
+            restore_ckpt(sg, S);
+            set_step(n0);
+            run_steps(1, nn, S, qf, graph && nn == k);
+            run_steps(2, nn, S, qa, graph && nn == k);
+        }
+        if (o.check_every > 0) check_nonfinite(ad.p, (size_t)S * sad);
+        // 4. chain rule (FP64) into the padded accumulators
+        chain_rule(S, groups);
+        // 5. source-side terms: rho of force sources, STF gradient
+        if (want_src && nitems) {
+            std::vector<float> hsa(nitems * nt), hamp(nitems * nt);
+            OWL_CUDA(cudaMemcpyAsync(hsa.data(), src_adj.p, sizeof(float) * nitems * nt, cudaMemcpyDeviceToHost, stream));
+            OWL_CUDA(cudaMemcpyAsync(hamp.data(), amp.p, sizeof(float) * nitems * nt, cudaMemcpyDeviceToHost, stream));
+            OWL_CUDA(cudaStreamSynchronize(stream));
+            std::map<long long, double> pts;
+            for (size_t it = 0; it < nitems; ++it) {
+                if (item_rho_cell[it] < 0) continue;
+                double acc = 0;
+                for (int t = 0; t < nt; ++t) acc += (double)hamp[it * nt + t] * (double)hsa[it * nt + t];
+                // the force weights carry 1/rho: d/drho (A w lambda) = -A w lambda / rho
+                pts[item_rho_cell[it] + (long long)rho_param() * (long long)npad()] += -acc / (double)item_rho[it];
+            }
+            if (!pts.empty()) {
+                std::vector<long long> hi;
+                std::vector<double> hv;
+                for (auto& kv : pts) { hi.push_back(kv.first); hv.push_back(kv.second); }
+                DevBuf<long long> didx;
+                didx.upload(hi.data(), hi.size(), stream);
+                pt_val.upload(hv.data(), hv.size(), stream);
+                k_add_points_f64<<<(int)(hi.size() + 127) / 128, 128, 0, stream>>>(gpad.p, didx.p, pt_val.p,
+                                                                                   (int)hi.size());
+                OWL_LAUNCH_CHECK();
+                OWL_CUDA(cudaStreamSynchronize(stream));
+                launches++;
+            }
+            if (stf_grad) {
+                for (int s = 0; s < S; ++s) {
+                    const owl_shot& shs = sh[s];
+                    for (int kk = 0; kk < shs.nsrc; ++kk)
+                        std::fill(stf_grad + stf_off + (size_t)kk * nt, stf_grad + stf_off + (size_t)(kk + 1) * nt, 0.f);
+                    for (size_t it = 0; it < nitems; ++it) {
+                        if (item_shot[it] != s) continue;
+                        const owl_source& q = shs.src[item_src[it]];
+                        float* outk = stf_grad + stf_off + (size_t)item_src[it] * nt;
+                        for (int t = 0; t < nt; ++t)
+                            outk[t] += (float)((double)hsa[it * nt + t] * (double)q.amp * (double)dt);
+                    }
+                    stf_off += (size_t)shs.nsrc * nt;
+                }
+            }
+        }
+        data_off += n;
+        shot0 += S;
+        batches++;
+    }
+    if (grad) fold_out(grad, mem);
+    info.elapsed_ms = tm.stop_ms();
+    fill_info(info, nshots, batches, true);
+}
+
+void SsgBase::gradient(int nshots, const owl_shot* shots, const float* data, int adj_kind, const owl_run_opts& o,
+                       double* misfit, float* grad, float* seis_out, int mem, owl_run_info& info) {
+    gradient_impl(nshots, shots, data, adj_kind, o, misfit, grad, seis_out, nullptr, mem, info);
+}
+
+void SsgBase::source_gradient(int nshots, const owl_shot* shots, const float* adj, const owl_run_opts& o,
+                              float* stf_grad, int mem, owl_run_info& info) {
+    OWL_CHECK(mem == OWL_MEM_HOST, OWL_ERR_UNSUPPORTED, "source_gradient takes host buffers");
+    gradient_impl(nshots, shots, adj, OWL_ADJ_GIVEN, o, nullptr, nullptr, nullptr, stf_grad, mem, info);
+}
+
+void SsgBase::kernel_time(int id, int nlaunch, double* avg_ms, double* bytes) {
+    OWL_CHECK(cur_S > 0, OWL_ERR_INVALID, "no batch has run on this handle");
+    OWL_CHECK(id >= OWL_K_FWD_P && id <= OWL_K_ADJ_V, OWL_ERR_INVALID, "bad kernel id");
+    const int S = cur_S;
+    OWL_CHECK(id < OWL_K_ADJ_P || (ad.p && G.p && Sbuf.p && ad.n >= (size_t)sad * S &&
+                                   Sbuf.n >= (size_t)nS * cur_k * S * fs),
+              OWL_ERR_INVALID, "adjoint kernels need a gradient call first");
+    set_step(cur_k);
+    for (int i = 0; i < 3; ++i) launch_kernel(id, S, false);
+    OWL_LAUNCH_CHECK();
+    EventTimer tm(stream);
+    for (int i = 0; i < nlaunch; ++i) launch_kernel(id, S, false);
+    OWL_LAUNCH_CHECK();
+    *avg_ms = tm.stop_ms() / nlaunch;
+    *bytes = alg_bytes(id, S, (S + spt_a - 1) / spt_a);
+}
+
+}  // namespace owl

@@ -1,0 +1,166 @@
+// ssg_base.cuh -- medium-independent host engine of the SSG solvers.
+//
+// A medium (2D/3D acoustic, 2D/3D elastic) supplies its stencil kernels, its
+// source / receiver taps and its chain rule; this base supplies everything
+// around them: point-operator tables (source injection, receiver sampling,
+// adjoint-source injection), the shot-batched state, every-k-step checkpoints
+// (FP32 or FP16 / BF16 with a per-field, per-shot scale), the device step
+// counter and CUDA-graph capture of the time loop, the gradient driver
+// (forward -> FP64 misfit / residual -> reverse sweep with segment
+// recomputation -> FP64 chain rule -> fold onto the model cells), the
+// autotuner and kernel timing.
+//
+// Layouts. Storage index of the reference's node (i, j, k) (x, y, z; 1-based,
+// padded range [-pml-R+1, n+pml+R]) is x = i + pml + R - 1 (same for y, z);
+// a field is (NZs, NYs, pitch) floats with x fastest (NYs = 1 in 2D). The
+// forward state and the adjoint state are shot-major: shot s of field f lives
+// at base + s * shot_stride + field_offset[f].
+#pragma once
+
+#include <array>
+#include <map>
+#include <vector>
+
+#include "engine.cuh"
+
+namespace owl {
+
+constexpr int MAX_PT_FIELDS = 10;
+
+struct PointDev {
+    float* fld[MAX_PT_FIELDS];
+    long long sstride;  // shot stride of the fields
+    int nt, rtot;
+    CSRView inj;
+    const int* inj_shot_ptr;
+    const float* amp;
+    CSRView smp;
+    const int* rec_shot_ptr;
+    float* rec;
+    CSRView sct;
+    const int* sct_shot_ptr;
+    const float* res;
+    float* src_adj;
+    int* d_step;
+    int* d_done;
+};
+
+enum { PT_INJECT = 1, PT_SAMPLE = 2, PT_TICK = 4 };
+
+void launch_point_fwd(const PointDev& q, int S, int mode, cudaStream_t s);
+void launch_point_adj(const PointDev& q, int S, cudaStream_t s);
+
+// one interpolation tap of a source / receiver on field `field` at reference node (i, j, k)
+struct TapPt {
+    int field;
+    int i, j, k;
+    float w;
+};
+
+struct SsgBase : Engine {
+    // grid
+    int dim, nx, ny, nz, P, R, pr, NXp, NYp, NZp, NXs, NYs, NZs, pitch;
+    long long plane, fs;  // floats per z-plane and per full field
+    float dt;
+    // layout sizes, set by the medium
+    long long sst = 0;   // floats of forward state per shot
+    long long sad = 0;   // floats of adjoint state per shot
+    int nS = 0;          // full fields stored per step in the segment buffer
+    int ngrad = 0;       // gradient accumulators (each with a Kahan compensation)
+    int nparam = 0;      // model parameters
+    int ncomp = 1;       // seismogram components
+    std::vector<std::pair<long long, long long>> st_segments;  // (offset, length) of each state field in a shot
+
+    // buffers
+    DevBuf<float> st, ad, G, Sbuf, ckpt, ck_scale;
+    DevBuf<unsigned short> ckpt16;
+    DevBuf<int> ctr;
+    DevBuf<float> rec, res, obs_t, src_adj, seis_tmp, amp;
+    DevBuf<double> gpad, misfit_d, pt_val;
+    DevBuf<int> pt_idx;
+    DevCSR inj, smp, sct;
+    DevBuf<int> inj_shot_ptr, rec_shot_ptr, sct_shot_ptr;
+    DevBuf<unsigned char> live;
+    DevBuf<long long> segbuf;  // st_segments offsets then lengths, on the device
+    GraphCache g_fwd, g_rec, g_adj;
+
+    long long launches = 0;
+    int cur_k = 0, cur_S = 0, tile_x = 32;
+    bool tune = false;
+    int spt_f = 1, spt_a = 1, tz_f = 8, tz_a = 8;
+    int ckpt_prec = OWL_CKPT_FP32;
+    int rtot = 0;
+    std::vector<int> item_src, item_comp, item_shot;
+    std::vector<long long> item_rho_cell;  // padded-grid index of the rho scaling a force component, -1 otherwise
+    std::vector<float> item_rho;
+    std::map<std::pair<int, int>, std::array<int, 4>> tune_cache;
+    std::vector<float> h_rhop;  // padded rho, storage layout (force-source weights)
+
+    SsgBase(const owl_ssg_desc& d, int dim_);
+    ~SsgBase() override;
+
+    // ---------------- medium hooks ----------------
+    virtual int src_ncomp(const owl_source& q) const = 0;
+    virtual void src_taps(const owl_source& q, int comp, std::vector<TapPt>& taps, long long& rho_cell,
+                          float& rho_val) const = 0;
+    virtual void rec_taps(const owl_receiver& q, int comp, std::vector<TapPt>& taps) const = 0;
+    // adjoint of one sampling tap (free-surface images route through the mirrored node)
+    virtual void scatter_map(const TapPt& t, std::vector<TapPt>& out) const { out.push_back(t); }
+    virtual void launch_kernel(int id, int S, bool store) = 0;
+    virtual double alg_bytes(int id, int S, int groups) const = 0;
+    virtual void chain_rule(int S, int groups) = 0;  // += into gpad
+    virtual int rho_param() const = 0;
+    virtual float* st_field(int f) const = 0;  // base pointer (shot 0) of forward field f
+    virtual float* ad_field(int f) const = 0;  // base pointer (shot 0) of adjoint field f
+
+    // ---------------- helpers ----------------
+    long long soff(int i, int j, int k) const {
+        return (long long)(k + pr - 1) * plane + (dim == 3 ? (long long)(j + pr - 1) * pitch : 0LL) + (i + pr - 1);
+    }
+    // padded model grid [-P, n+P+1] per axis
+    int nxq() const { return NXp + 2; }
+    int nyq() const { return dim == 3 ? NYp + 2 : 1; }
+    int nzq() const { return NZp + 2; }
+    size_t npad() const { return (size_t)nxq() * nyq() * nzq(); }
+    long long pad_index(int i, int j, int k) const {
+        return ((long long)(k + P) * nyq() + (dim == 3 ? (j + P) : 0)) * nxq() + (i + P);
+    }
+    bool in_wavefield(int i, int j, int k) const {
+        bool ok = i >= -P - R + 1 && i <= nx + P + R && k >= -P - R + 1 && k <= nz + P + R;
+        if (dim == 3) ok = ok && j >= -P - R + 1 && j <= ny + P + R;
+        return ok;
+    }
+    dim3 grid_for(int rows, int S, int spt, int tz) const {
+        return dim3((NXp + tile_x - 1) / tile_x, (rows + tz - 1) / tz, (S + spt - 1) / spt);
+    }
+
+    DevBuf<long long>& seg_off();
+    void set_step(int v);
+    void build_tables(int S, const owl_shot* shots, bool need_sct);
+    void ensure_state(int S, int k, bool grad);
+    PointDev pdev(int S, bool adjoint, bool want_src_adj);
+    void launch_step(int kind, int S, const PointDev& q);
+    void run_steps(int kind, int n, int S, const PointDev& q, bool graph);
+    void resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bool& graph);
+    void autotune(int S, int k, bool grad);
+    void save_ckpt(int slot, int S);
+    void restore_ckpt(int slot, int S);
+    void forward_batch(int S, int k, bool graph, bool save);
+    void check_nonfinite(const float* f, size_t n);
+    void copy_out(void* dst, const void* src, size_t bytes, int mem);
+    void fold_out(float* grad, int mem);
+    void invalidate_graphs();
+    void fill_info(owl_run_info& info, int nshots, int batches, bool grad);
+
+    void forward(int nshots, const owl_shot* shots, const owl_run_opts& o, float* seis, int mem,
+                 owl_run_info& info) override;
+    void gradient(int nshots, const owl_shot* shots, const float* data, int adj_kind, const owl_run_opts& o,
+                  double* misfit, float* grad, float* seis_out, int mem, owl_run_info& info) override;
+    void source_gradient(int nshots, const owl_shot* shots, const float* adj, const owl_run_opts& o, float* stf_grad,
+                         int mem, owl_run_info& info) override;
+    void kernel_time(int id, int nlaunch, double* avg_ms, double* alg_bytes) override;
+    void gradient_impl(int nshots, const owl_shot* shots, const float* data, int adj_kind, const owl_run_opts& o,
+                       double* misfit, float* grad, float* seis_out, float* stf_grad, int mem, owl_run_info& info);
+};
+
+}  // namespace owl

@@ -95,3 +95,62 @@ def test_source_dot_product():
             rhs += float(np.dot(stf, g[off:off + nt].astype(np.float64)))
             off += nt
     assert abs(lhs - rhs) / abs(lhs) < 1e-5, (lhs, rhs)
+
+
+@pytest.mark.parametrize("prec,tol", [(L.OWL_CKPT_FP16, 2e-3), (L.OWL_CKPT_BF16, 2e-2)])
+def test_gradient_compressed_checkpoints(prec, tol):
+    """FP16 / BF16 checkpoints with a per-field, per-shot scale: the gradient
+    error against the FP64 oracle stays within the stated bound."""
+    nx, nz, dx, dt, nt = 48, 40, 10.0, 1e-3, 300
+    d = desc(nx, nz, dx, dt, nt)
+    vp, rho = random_model(nx, nz)
+    ps = prepare(small_shots(nx, nz, dx), nx, nz, dx, dt)
+    obs = oracle.ac2d_forward(d, vp, rho, ps, "f64").astype(np.float32)
+    vp0 = vp * np.float32(1.02)
+    _, g_ref, _ = oracle.ac2d_gradient(d, vp0, rho, ps, obs, adj_kind=0, k=30, precision="f64")
+    s = make_solver(d, vp0, rho)
+    _, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=30, checkpoint_precision=prec))
+    e = rel(g, g_ref)
+    print("checkpoint precision", prec, "gradient rel err", e)
+    assert e < tol, e
+
+
+def test_device_buffers_match_host_buffers():
+    """OWL_MEM_DEVICE (torch CUDA tensors) and OWL_MEM_HOST give the same results."""
+    import torch
+    nx, nz, dx, dt, nt = 48, 40, 10.0, 1e-3, 200
+    d = desc(nx, nz, dx, dt, nt)
+    vp, rho = random_model(nx, nz)
+    ps = prepare(small_shots(nx, nz, dx), nx, nz, dx, dt)
+    s = make_solver(d, vp, rho)
+    h = s.forward(ps, RunOpts())
+    dv = s.forward(ps, RunOpts(), out=torch.zeros(h.size, dtype=torch.float32, device="cuda"))
+    assert np.array_equal(h, dv.cpu().numpy())
+    obs = (h * 0.9).astype(np.float32)
+    mh, gh = s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=40))
+    md, gd = s.gradient(ps, torch.from_numpy(obs).cuda(), opts=RunOpts(checkpoint_interval=40))
+    assert np.allclose(mh, md.cpu().numpy(), rtol=1e-12)
+    assert np.array_equal(gh, gd.cpu().numpy())
+
+
+def test_nonfinite_detected():
+    """A blown-up run returns OWL_ERR_NONFINITE instead of garbage (dt far above
+    the CFL bound with the stability check relaxed)."""
+    nx, nz, dx, nt = 40, 40, 10.0, 400
+    d = desc(nx, nz, dx, 4e-3, nt)
+    vp, rho = random_model(nx, nz)
+    s = SSGSolver(L.OWL_ACOUSTIC_ISO_2D, nx, nz, dx, dx, 4e-3, nt, pml=10, f0_max=15.0, allow_dt_adjust=True)
+    s.set_model(vp, rho)
+    ps = prepare(small_shots(nx, nz, dx)[:1], nx, nz, dx, 4e-3)
+    with pytest.raises(L.OwlError) as e:
+        s.forward(ps, RunOpts(check_every=1))
+    assert e.value.code == L.OWL_ERR_NONFINITE
+
+
+def test_unstable_dt_rejected():
+    nx, nz, dx = 40, 40, 10.0
+    vp, rho = random_model(nx, nz)
+    s = SSGSolver(L.OWL_ACOUSTIC_ISO_2D, nx, nz, dx, dx, 4e-3, 10, pml=10, f0_max=15.0)
+    with pytest.raises(L.OwlError) as e:
+        s.set_model(vp, rho)
+    assert e.value.code == L.OWL_ERR_UNSTABLE
