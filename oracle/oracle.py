@@ -13,7 +13,7 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("oracle_ac2d.cpp", "oracle_common.hpp")]
+    srcs = [os.path.join(HERE, f) for f in ("oracle_ac2d.cpp", "oracle_ac3d.cpp", "oracle_common.hpp")]
     if force or not os.path.exists(ORACLE_LIB) or any(os.path.getmtime(s) > os.path.getmtime(ORACLE_LIB) for s in srcs):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return ORACLE_LIB
@@ -32,6 +32,10 @@ def load():
         _lib.oracle_ac2d_gradient_f64.argtypes = [vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp, vp]
         _lib.oracle_ac2d_gradient_f32.argtypes = [vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp, vp]
         _lib.oracle_ac2d_ref_gradient_f32.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp, C.c_int, vp]
+        _lib.oracle_ac3d_forward_f32.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+        _lib.oracle_ac3d_forward_f64.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+        _lib.oracle_ac3d_jvp_c128.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp, vp]
+        _lib.oracle_ac3d_gradient_f64.argtypes = [vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp]
     return _lib
 
 
@@ -104,3 +108,37 @@ def ac2d_ref_gradient(desc, vp, rho, ps, adj, cc=1):
     if rc != 0:
         raise RuntimeError("oracle ref gradient failed")
     return grad
+
+
+def ac3d_forward(desc, vp, rho, ps, precision="f32"):
+    """3D seismograms; vp, rho are (nz, ny, nx) arrays."""
+    lib = load()
+    dt = np.float32 if precision == "f32" else np.float64
+    vp, rho = _fort(vp, dt), _fort(rho, dt)
+    out = np.zeros(_nseis(ps, desc.nt), dtype=dt)
+    fn = lib.oracle_ac3d_forward_f32 if precision == "f32" else lib.oracle_ac3d_forward_f64
+    if fn(C.byref(desc), _p(vp), _p(rho), ps.nshots, C.cast(ps.arr, C.c_void_p), _p(out)) != 0:
+        raise RuntimeError("oracle ac3d forward failed")
+    return out
+
+
+def ac3d_jvp(desc, vp, rho, dvp, drho, ps):
+    lib = load()
+    a = [_fort(v, np.float64) for v in (vp, rho, dvp, drho)]
+    out = np.zeros(_nseis(ps, desc.nt))
+    if lib.oracle_ac3d_jvp_c128(C.byref(desc), *[_p(v) for v in a], ps.nshots, C.cast(ps.arr, C.c_void_p), _p(out)):
+        raise RuntimeError("oracle ac3d jvp failed")
+    return out
+
+
+def ac3d_gradient(desc, vp, rho, ps, data, adj_kind=0, k=50):
+    """(misfit per shot, grad (2, nz*ny*nx) z-fastest) of the exact adjoint in FP64."""
+    lib = load()
+    vp, rho = _fort(vp, np.float64), _fort(rho, np.float64)
+    data = np.ascontiguousarray(data, dtype=np.float64)
+    misfit = np.zeros(ps.nshots)
+    grad = np.zeros(2 * desc.nx * desc.ny * desc.nz)
+    if lib.oracle_ac3d_gradient_f64(C.byref(desc), _p(vp), _p(rho), ps.nshots, C.cast(ps.arr, C.c_void_p), _p(data),
+                                    adj_kind, k, _p(misfit), _p(grad)):
+        raise RuntimeError("oracle ac3d gradient failed")
+    return misfit, grad

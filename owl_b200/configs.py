@@ -68,3 +68,45 @@ def config2(nshots=32):
     vp, rho = acoustic_2d_true_model(nz, nx, dx)
     vp0, rho0 = smooth(vp, 15.0), smooth(rho, 15.0)
     return d, (vp, rho), (vp0, rho0), config2_shots(nshots, nx, dx)
+
+
+def value_noise_3d(shape, cells_per_node, seed):
+    """Smooth seeded noise in [-1, 1]: uniform random values on a coarse lattice
+    every `cells_per_node` cells, cubic-spline interpolated to the grid."""
+    from scipy.ndimage import zoom
+    rng = np.random.default_rng(seed)
+    coarse = [max(2, int(np.ceil(n / cells_per_node)) + 1) for n in shape]
+    c = rng.uniform(-1.0, 1.0, size=coarse)
+    f = zoom(c, [n / m for n, m in zip(shape, coarse)], order=3, mode="nearest")[: shape[0], : shape[1], : shape[2]]
+    f = f - f.mean()
+    return (f / max(1e-12, np.abs(f).max())).astype(np.float32)
+
+
+def acoustic_3d_model(n=400, dx=10.0, nlayers=8, vmax_layer=4000.0):
+    """8 layers with Vp uniform in [1500, vmax_layer] (seed 3) at sorted uniform
+    depths (seed 4), times (1 + 0.05 noise) with smooth value noise (seed 5,
+    ~500 m wavelength); Gardner rho. vmax_layer = 4000 keeps Vp <= 4200 m/s, the
+    CFL bound of dt = 1 ms at dx = 10 m for the 8th-order scheme (the layer
+    range [1500, 4500] of the benchmark description would need dt <= 0.92 ms)."""
+    v = np.random.default_rng(3).uniform(1500.0, vmax_layer, nlayers)
+    tops = np.sort(np.random.default_rng(4).uniform(0.0, (n - 1) * dx, nlayers - 1))
+    z = np.arange(n) * dx
+    idx = np.searchsorted(tops, z, side="right")
+    vz = v[idx].astype(np.float32)
+    noise = value_noise_3d((n, n, n), max(2, int(round(500.0 / dx))), 5)
+    vp = (vz[:, None, None] * (1.0 + 0.05 * noise)).astype(np.float32)
+    rho = (310.0 * vp.astype(np.float64) ** 0.25).astype(np.float32)
+    return vp, rho
+
+
+def config3(n=400, nt=1500):
+    """3D acoustic: 400^3, dx 10 m, 8th order, PML 20, dt 1 ms, 1500 steps, one
+    12 Hz Ricker at the centre x, y and z = 20 m, 200 x 200 receivers every 20 m at z = 20 m."""
+    dx, dt = 10.0, 1e-3
+    d = _desc(L.OWL_ACOUSTIC_ISO_3D, n, n, dx, dt, nt, pml=20, f0=12.0, ny=n)
+    vp, rho = acoustic_3d_model(n, dx)
+    c = (n // 2) * dx
+    nr = min(200, n // 2)
+    recs = [Receiver(x=20.0 * i, y=20.0 * j, z=20.0) for j in range(nr) for i in range(nr)]
+    shots = [Shot(1, [Source(x=c, y=c, z=20.0, f0=12.0)], recs)]
+    return d, vp, rho, shots

@@ -95,6 +95,7 @@ int owl_ssg_create(const owl_ssg_desc* desc, owl_ssg** out) {
         std::unique_ptr<owl_ssg> h(new owl_ssg);
         switch (desc->medium) {
             case OWL_ACOUSTIC_ISO_2D: h->eng.reset(make_ac2d_engine(*desc)); break;
+            case OWL_ACOUSTIC_ISO_3D: h->eng.reset(make_ac3d_engine(*desc)); break;
             default: throw OwlError(OWL_ERR_UNSUPPORTED, "medium not built");
         }
         *out = h.release();

@@ -11,15 +11,17 @@
 namespace owl {
 
 // ------------------------------ point operators ----------------------------
-// One CTA per shot. Forward: add_source(t) (sources in order, taps of one
-// source in parallel, as the reference's loops), then record the receivers of
-// step t+1 (each trace a sequential sum over its taps). The last CTA advances
+// Grid (shots, NB). Forward: add_source(t) by the CTAs of row 0 (sources in
+// order, taps of one source in parallel, as the reference's loops), then the
+// receivers of step t+1 (each trace a sequential sum over its taps) spread over
+// the NB CTAs of the shot. With NB > 1 injection and sampling are two launches
+// (the sampling must see every injected tap). The last CTA to finish advances
 // the device step counter, so one captured graph serves every segment.
 __global__ void k_point_fwd(PointDev a, int mode) {
     const int s = blockIdx.x;
     const int cur = *a.d_step;
     const int t = cur + 1;
-    if (mode & PT_INJECT) {
+    if ((mode & PT_INJECT) && blockIdx.y == 0) {
         for (int it = a.inj_shot_ptr[s]; it < a.inj_shot_ptr[s + 1]; ++it) {
             const float A = a.amp[(size_t)it * a.nt + (t - 1)];
             if (A != 0.f) {
@@ -32,9 +34,10 @@ __global__ void k_point_fwd(PointDev a, int mode) {
         }
     }
     if (mode & PT_SAMPLE) {
-        const int tr = (mode & PT_INJECT) ? t + 1 : t;
+        const int tr = (mode & PT_NEXT) ? t + 1 : t;
         if (tr <= a.nt) {
-            for (int r = a.rec_shot_ptr[s] + threadIdx.x; r < a.rec_shot_ptr[s + 1]; r += blockDim.x) {
+            const int step = gridDim.y * blockDim.x;
+            for (int r = a.rec_shot_ptr[s] + blockIdx.y * blockDim.x + threadIdx.x; r < a.rec_shot_ptr[s + 1]; r += step) {
                 float acc = 0.f;
                 for (int j = a.smp.ptr[r]; j < a.smp.ptr[r + 1]; ++j)
                     acc = acc + a.fld[a.smp.field[j]][s * a.sstride + a.smp.off[j]] * a.smp.w[j];
@@ -48,30 +51,40 @@ __global__ void k_point_fwd(PointDev a, int mode) {
 // Adjoint of the sampling of step t (residual into the adjoint fields, one
 // thread per distinct target node, contributions summed in a fixed order),
 // then the source-side adjoint taps . lambda_{t-1}; the last CTA steps back.
-__global__ void k_point_adj(PointDev a) {
+// Same split as the forward when a shot has many target nodes.
+__global__ void k_point_adj(PointDev a, int mode) {
     const int s = blockIdx.x;
     const int t = *a.d_step;
-    for (int it = a.sct_shot_ptr[s] + threadIdx.x; it < a.sct_shot_ptr[s + 1]; it += blockDim.x) {
-        float acc = 0.f;
-        const int j0 = a.sct.ptr[it], j1 = a.sct.ptr[it + 1];
-        for (int j = j0; j < j1; ++j) acc = acc + a.res[(size_t)(t - 1) * a.rtot + a.sct.item[j]] * a.sct.w[j];
-        float* f = a.fld[a.sct.field[j0]] + s * a.sstride + a.sct.off[j0];
-        *f = *f + acc;
-    }
-    __syncthreads();
-    if (a.src_adj && t - 1 >= 1) {
-        for (int it = a.inj_shot_ptr[s] + threadIdx.x; it < a.inj_shot_ptr[s + 1]; it += blockDim.x) {
+    if (mode & PA_SCATTER) {
+        const int step = gridDim.y * blockDim.x;
+        for (int it = a.sct_shot_ptr[s] + blockIdx.y * blockDim.x + threadIdx.x; it < a.sct_shot_ptr[s + 1]; it += step) {
             float acc = 0.f;
-            for (int j = a.inj.ptr[it]; j < a.inj.ptr[it + 1]; ++j)
-                acc = acc + a.fld[a.inj.field[j]][s * a.sstride + a.inj.off[j]] * a.inj.w[j];
-            a.src_adj[(size_t)it * a.nt + (t - 2)] = acc;
+            const int j0 = a.sct.ptr[it], j1 = a.sct.ptr[it + 1];
+            for (int j = j0; j < j1; ++j) acc = acc + a.res[(size_t)(t - 1) * a.rtot + a.sct.item[j]] * a.sct.w[j];
+            float* f = a.fld[a.sct.field[j0]] + s * a.sstride + a.sct.off[j0];
+            *f = *f + acc;
         }
     }
-    tick_last_block(a.d_step, a.d_done, -1);
+    if ((mode & PA_SRC) && blockIdx.y == 0) {
+        __syncthreads();
+        if (a.src_adj && t - 1 >= 1) {
+            for (int it = a.inj_shot_ptr[s] + threadIdx.x; it < a.inj_shot_ptr[s + 1]; it += blockDim.x) {
+                float acc = 0.f;
+                for (int j = a.inj.ptr[it]; j < a.inj.ptr[it + 1]; ++j)
+                    acc = acc + a.fld[a.inj.field[j]][s * a.sstride + a.inj.off[j]] * a.inj.w[j];
+                a.src_adj[(size_t)it * a.nt + (t - 2)] = acc;
+            }
+        }
+    }
+    if (mode & PA_TICK) tick_last_block(a.d_step, a.d_done, -1);
 }
 
-void launch_point_fwd(const PointDev& q, int S, int mode, cudaStream_t s) { k_point_fwd<<<S, 256, 0, s>>>(q, mode); }
-void launch_point_adj(const PointDev& q, int S, cudaStream_t s) { k_point_adj<<<S, 256, 0, s>>>(q); }
+void launch_point_fwd(const PointDev& q, int S, int nb, int mode, cudaStream_t s) {
+    k_point_fwd<<<dim3(S, nb), 256, 0, s>>>(q, mode);
+}
+void launch_point_adj(const PointDev& q, int S, int nb, int mode, cudaStream_t s) {
+    k_point_adj<<<dim3(S, nb), 256, 0, s>>>(q, mode);
+}
 
 // ------------------------- compressed checkpoints ---------------------------
 // Per (shot, state field) scale = max |x|; values stored as x / scale in FP16 or
@@ -283,6 +296,11 @@ void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
         hrec_ptr.push_back(rtot);
         hsct_ptr.push_back(hsct.nitems());
     }
+    int mr = 0, ms = 0;
+    for (size_t i = 0; i + 1 < hrec_ptr.size(); ++i) mr = std::max(mr, hrec_ptr[i + 1] - hrec_ptr[i]);
+    for (size_t i = 0; i + 1 < hsct_ptr.size(); ++i) ms = std::max(ms, hsct_ptr[i + 1] - hsct_ptr[i]);
+    nb_rec = std::max(1, std::min(1024, (mr + 255) / 256));
+    nb_sct = std::max(1, std::min(1024, (ms + 255) / 256));
     inj.upload(hinj, stream);
     smp.upload(hsmp, stream);
     sct.upload(hsct, stream);
@@ -322,16 +340,34 @@ PointDev SsgBase::pdev(int S, bool adjoint, bool want_src_adj) {
 }
 
 void SsgBase::launch_step(int kind, int S, const PointDev& q) {
+    // point operators of shots with more than 1024 traces / target nodes use
+    // NB CTAs per shot and a separate launch for the dependent phase
     if (kind == 0 || kind == 1) {
         launch_kernel(OWL_K_FWD_P, S, kind == 1);
         launch_kernel(OWL_K_FWD_V, S, kind == 1);
-        launch_point_fwd(q, S, kind == 0 ? (PT_INJECT | PT_SAMPLE | PT_TICK) : (PT_INJECT | PT_TICK), stream);
+        if (kind == 1) {
+            launch_point_fwd(q, S, 1, PT_INJECT | PT_TICK, stream);
+            launches += 3;
+        } else if (nb_rec <= 4) {
+            launch_point_fwd(q, S, 1, PT_INJECT | PT_SAMPLE | PT_NEXT | PT_TICK, stream);
+            launches += 3;
+        } else {
+            launch_point_fwd(q, S, 1, PT_INJECT, stream);
+            launch_point_fwd(q, S, nb_rec, PT_SAMPLE | PT_NEXT | PT_TICK, stream);
+            launches += 4;
+        }
     } else {
         launch_kernel(OWL_K_ADJ_P, S, false);
         launch_kernel(OWL_K_ADJ_V, S, false);
-        launch_point_adj(q, S, stream);
+        if (nb_sct <= 4) {
+            launch_point_adj(q, S, 1, PA_SCATTER | PA_SRC | PA_TICK, stream);
+            launches += 3;
+        } else {
+            launch_point_adj(q, S, nb_sct, PA_SCATTER, stream);
+            launch_point_adj(q, S, 1, PA_SRC | PA_TICK, stream);
+            launches += 4;
+        }
     }
-    launches += 3;
 }
 
 void SsgBase::run_steps(int kind, int n, int S, const PointDev& q, bool graph) {
@@ -349,7 +385,7 @@ void SsgBase::run_steps(int kind, int n, int S, const PointDev& q, bool graph) {
                                   (uintptr_t)inj.off.p, (uintptr_t)smp.ptr.p, (uintptr_t)smp.w.p, (uintptr_t)smp.off.p,
                                   (uintptr_t)sct.ptr.p, (uintptr_t)sct.w.p, (uintptr_t)sct.off.p, (uintptr_t)amp.p,
                                   (uintptr_t)inj_shot_ptr.p, (uintptr_t)rec_shot_ptr.p, (uintptr_t)sct_shot_ptr.p,
-                                  (uintptr_t)q.rtot};
+                                  (uintptr_t)q.rtot, (uintptr_t)nb_rec, (uintptr_t)nb_sct};
     if (!gc.exec || gc.sig != sig) {
         gc.reset();
         cudaGraph_t g;
@@ -367,11 +403,13 @@ void SsgBase::run_steps(int kind, int n, int S, const PointDev& q, bool graph) {
         gc.sig = sig;
     }
     OWL_CUDA(cudaGraphLaunch(gc.exec, stream));
-    launches += 3LL * n;
+    launches += (long long)n * (kind == 1 ? 3 : kind == 0 ? (nb_rec <= 4 ? 3 : 4) : (nb_sct <= 4 ? 3 : 4));
 }
 
 void SsgBase::resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bool& graph) {
-    tune = o.shots_per_cta <= 0 && o.tile_z <= 0;
+    // tile_z: 0 = autotuned; > 0 explicit tile height (3D forward: rows per
+    // thread); < 0 in 3D: one thread per cell for the forward kernels
+    tune = o.shots_per_cta <= 0 && o.tile_z == 0;
     B = o.shots_per_launch > 0 ? o.shots_per_launch : std::max(1, desc.max_shots);
     B = std::min(B, std::max(1, nshots));
     k = o.checkpoint_interval > 0 ? o.checkpoint_interval : 50;
@@ -380,7 +418,8 @@ void SsgBase::resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bo
     graph = o.use_graph >= 0;
     tile_x = o.tile_x > 0 ? o.tile_x : 32;
     tz_f = tz_a = o.tile_z > 0 ? o.tile_z : (dim == 3 ? 4 : 8);
-    OWL_CHECK(tile_x % 32 == 0 && tz_f >= 1 && tile_x * tz_f <= 512, OWL_ERR_INVALID,
+    if (dim == 3 && o.tile_z < 0) tz_f = 0;
+    OWL_CHECK(tile_x % 32 == 0 && tz_a >= 1 && tile_x * tz_a <= 512 && (tz_f >= 1 || dim == 3), OWL_ERR_INVALID,
               "tile_x must be a multiple of 32 and tile_x * tile_z <= 512");
     OWL_CHECK(o.checkpoint_precision >= OWL_CKPT_FP32 && o.checkpoint_precision <= OWL_CKPT_BF16, OWL_ERR_INVALID,
               "bad checkpoint precision");
@@ -400,8 +439,10 @@ void SsgBase::autotune(int S, int k, bool grad) {
     }
     cur_k = k;
     set_step(k);
-    const std::vector<int> tzs = dim == 3 ? std::vector<int>{2, 4, 8} : std::vector<int>{4, 8, 16};
     for (int pass = 0; pass < (grad ? 2 : 1); ++pass) {
+        // 3D forward kernels take rows per thread (1, 2, 4); other kernels a tile height
+        const std::vector<int> tzs = dim == 3 ? (pass == 0 ? std::vector<int>{0, 1, 2, 4} : std::vector<int>{2, 4, 8})
+                                              : std::vector<int>{4, 8, 16};
         float best = 1e30f;
         int bs = 1, bt = tzs[1];
         for (int spt : {1, 2, 4, 8, 16, 32}) {
@@ -468,7 +509,7 @@ void SsgBase::forward_batch(int S, int k, bool graph, bool save) {
     PointDev q = pdev(S, false, false);
     OWL_CUDA(cudaMemsetAsync(st.p, 0, sizeof(float) * sst * S, stream));
     set_step(0);
-    launch_point_fwd(q, S, PT_SAMPLE, stream);
+    launch_point_fwd(q, S, nb_rec, PT_SAMPLE, stream);
     OWL_LAUNCH_CHECK();
     launches++;
     const int nseg = (nt + k - 1) / k;

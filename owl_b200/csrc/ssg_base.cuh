@@ -45,10 +45,11 @@ struct PointDev {
     int* d_done;
 };
 
-enum { PT_INJECT = 1, PT_SAMPLE = 2, PT_TICK = 4 };
+enum { PT_INJECT = 1, PT_SAMPLE = 2, PT_TICK = 4, PT_NEXT = 8 };  // forward point kernel phases
+enum { PA_SCATTER = 1, PA_SRC = 2, PA_TICK = 4 };                  // adjoint point kernel phases
 
-void launch_point_fwd(const PointDev& q, int S, int mode, cudaStream_t s);
-void launch_point_adj(const PointDev& q, int S, cudaStream_t s);
+void launch_point_fwd(const PointDev& q, int S, int nb, int mode, cudaStream_t s);
+void launch_point_adj(const PointDev& q, int S, int nb, int mode, cudaStream_t s);
 
 // one interpolation tap of a source / receiver on field `field` at reference node (i, j, k)
 struct TapPt {
@@ -90,6 +91,7 @@ struct SsgBase : Engine {
     int spt_f = 1, spt_a = 1, tz_f = 8, tz_a = 8;
     int ckpt_prec = OWL_CKPT_FP32;
     int rtot = 0;
+    int nb_rec = 1, nb_sct = 1;  // CTAs per shot of the sampling / adjoint-injection point kernels
     std::vector<int> item_src, item_comp, item_shot;
     std::vector<long long> item_rho_cell;  // padded-grid index of the rho scaling a force component, -1 otherwise
     std::vector<float> item_rho;

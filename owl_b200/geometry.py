@@ -15,6 +15,7 @@ bit-for-bit to the reference build.
 from __future__ import annotations
 
 import ctypes as C
+import functools
 import math
 import os
 from dataclasses import dataclass, field
@@ -51,7 +52,12 @@ def bessel_i0(x: float) -> float:
 
 def kaiser_sinc_kernel(x) -> np.ndarray:
     """9-tap Kaiser-windowed sinc for a fractional offset x (module_source_receiver.f90:789-828)."""
-    x = f32(x)
+    return _kaiser_cached(float(f32(x))).copy()
+
+
+@functools.lru_cache(maxsize=65536)
+def _kaiser_cached(xv: float) -> np.ndarray:
+    x = f32(xv)
     h = np.zeros(2 * NKW + 1, dtype=f32)
     if x == 0:
         h[NKW] = 1.0
