@@ -40,7 +40,61 @@ def parse():
     p.add_argument("--nshots", type=int, default=NSHOTS, help="shots per GPU (32 for the benchmark)")
     p.add_argument("--profile", action="store_true",
                    help="profiling target: one gradient step of --nshots shots, nothing else, no JSON line")
+    p.add_argument("--no-3d", action="store_true", help="skip the 3D acoustic forward roofline block")
+    p.add_argument("--profile3d", type=int, default=0, metavar="N",
+                   help="profiling target: 12-step 3D acoustic forward of an N^3 model, no JSON line")
     return p.parse_args()
+
+
+def profile_3d(n):
+    """Small 3D forward for kernel captures: N^3 layered model, one shot, 12 steps,
+    forward tiles fixed at one row per thread (no autotuning launches)."""
+    from owl_b200 import _lib as L
+    from owl_b200 import configs
+    from owl_b200.geometry import Receiver, Shot, Source
+    from owl_b200.solver import RunOpts, SSGSolver
+
+    vp, rho = configs.acoustic_3d_model(n, 10.0)
+    c = n // 2 * 10.0
+    shots = [Shot(1, [Source(x=c, y=c, z=20.0, f0=12.0)], [Receiver(x=20.0 * i, y=c, z=20.0) for i in range(n // 2)])]
+    s = SSGSolver(L.OWL_ACOUSTIC_ISO_3D, n, n, 10.0, 10.0, 1e-3, 12, pml=20, f0_max=12.0, ny=n, dy=10.0)
+    s.set_model(vp, rho)
+    s.forward(s.prepare(shots), RunOpts(shots_per_cta=1, tile_z=1, use_graph=-1))
+    print(f"profile3d: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
+    s.close()
+
+
+def forward_3d_block(peak, peak_kind):
+    """3D acoustic forward of the 400^3 workload (440^3 padded cells, 1500 steps,
+    one shot, 40,000 receivers): Gcell-updates/s of the whole forward and the
+    HBM roofline of its two stencil kernels (standalone launches, CUDA events)."""
+    from owl_b200 import _lib as L
+    from owl_b200 import configs
+    from owl_b200.solver import RunOpts, SSGSolver
+
+    d, vp, rho, shots = configs.config3(400, nt=1500)
+    s = SSGSolver(L.OWL_ACOUSTIC_ISO_3D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
+                  f0_max=d.f0_max, ny=d.ny, dy=d.dy)
+    s.set_model(vp, rho)
+    ps = s.prepare(shots)
+    s.forward(ps, RunOpts())
+    ms = []
+    for _ in range(2):
+        s.forward(ps, RunOpts())
+        ms.append(s.last_info.elapsed_ms)
+    cells = float(d.nx + 2 * d.pml) ** 3
+    out = {"workload": "3D acoustic forward, 400^3 model (440^3 padded), dt 1 ms, 1500 steps, 1 shot, "
+                       "40,000 receivers", "ms_per_forward": sum(ms) / len(ms),
+           "gcells_per_s": cells * d.nt / (sum(ms) / len(ms) / 1e3) / 1e9,
+           "tile_rows_per_thread": s.last_info.tile_z, "kernels": {}}
+    for kid, name in ((L.OWL_K_FWD_P, "k_ac3d_fwd_p"), (L.OWL_K_FWD_V, "k_ac3d_fwd_v")):
+        kms, b = s.kernel_time(kid, 20)
+        ach = b / (kms / 1e3) / 1e9
+        out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
+                                "traffic": profile_traffic(name)}
+    s.close()
+    return out
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -99,7 +153,7 @@ def measured_peak_hbm():
 def profile_traffic(kernel: str):
     """DRAM bytes per launch of a kernel from the committed ncu summary, scaled to
     the bench's launch (None if absent)."""
-    p = os.path.join(ROOT, "profiles", "ac2d_gradient_traffic.json")
+    p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(p) as f:
             return json.load(f).get(kernel)
@@ -168,6 +222,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.profile3d:
+        return profile_3d(args.profile3d)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
@@ -322,9 +378,12 @@ def main():
         v, threads, sample = cpu_reference_sample(args.cpu_nt)
         line["cpu_baseline"] = {"value": v, "unit": "s/shot", "cores": threads, "kind": "port", "sample": sample}
 
+    s.close()
+    if rank == 0 and not args.no_3d:
+        line["forward_3d"] = forward_3d_block(peak, peak_kind)
+
     if rank == 0:
         print(json.dumps(line), flush=True)
-    s.close()
     if world > 1:
         dist.destroy_process_group()
 
