@@ -216,6 +216,30 @@ void owl_ssg_destroy(owl_ssg *h);
  * wavefields in an unspecified state. */
 int owl_ssg_kernel_time(owl_ssg *h, int kernel_id, int nlaunch, double *avg_ms, double *alg_bytes);
 
+/* ---- forward without device allocation (no counterpart in the reference) -- */
+
+/* Size, in floats, of the one device array that owl_ssg_forward_noalloc works
+ * in (64 MiB). Every GPU that loads the library holds this array until the
+ * process exits. */
+#define OWL_NOALLOC_MAX_FLOATS (16 * 1024 * 1024)
+
+/* One 2D acoustic shot (explosion sources, no free surface) modelled without
+ * any device allocation, for callers that cannot call cudaMalloc: code running
+ * while a stream is captured into a CUDA graph, or applications whose device
+ * memory is reserved up front by another allocator. Materials, PML
+ * coefficients, wavefields and traces live in a static device array of
+ * OWL_NOALLOC_MAX_FLOATS floats. Inputs and outputs are host memory: vp, rho as
+ * for owl_ssg_set_model (nparam = 2), seis = nrec x nt floats in the layout of
+ * owl_ssg_forward. The same seismograms as owl_ssg_forward. Returns
+ * OWL_ERR_INVALID when the run needs more than OWL_NOALLOC_MAX_FLOATS floats.
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture starts. All calls share the array, which keeps the
+ * last call's contents (each call clears what must start at zero); calls whose
+ * GPU work overlapped would race on it, so the call holds a process-wide lock
+ * and returns only after its GPU work has finished. */
+int owl_ssg_forward_noalloc(const owl_ssg_desc *desc, int nparam, const float *const *fields,
+                            const owl_shot *shot, float *seis);
+
 /* ---- queries ------------------------------------------------------------ */
 
 const char *owl_last_error(void);

@@ -135,6 +135,7 @@ EXPORTED = [
     "owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
     "owl_ssg_source_gradient", "owl_ssg_destroy", "owl_last_error", "owl_ssg_abi_version",
     "owl_ssg_dt_stable", "owl_ssg_nparam", "owl_ssg_ncomp", "owl_ssg_device_ok", "owl_ssg_kernel_time",
+    "owl_ssg_forward_noalloc",
 ]
 
 OWL_K_FWD_P = 0
@@ -171,6 +172,8 @@ def load() -> C.CDLL:
                                             C.c_void_p, C.c_int, P(OwlRunInfo)]
     lib.owl_ssg_kernel_time.argtypes = [C.c_void_p, C.c_int, C.c_int, P(C.c_double), P(C.c_double)]
     lib.owl_ssg_kernel_time.restype = C.c_int
+    lib.owl_ssg_forward_noalloc.argtypes = [P(OwlSsgDesc), C.c_int, P(P(C.c_float)), P(OwlShot), C.c_void_p]
+    lib.owl_ssg_forward_noalloc.restype = C.c_int
     lib.owl_ssg_destroy.argtypes = [C.c_void_p]
     lib.owl_ssg_destroy.restype = None
     lib.owl_last_error.restype = C.c_char_p
