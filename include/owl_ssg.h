@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define OWL_SSG_ABI_VERSION 1
+#define OWL_SSG_ABI_VERSION 2
 
 /* status codes */
 #define OWL_OK 0
@@ -56,6 +56,13 @@ extern "C" {
 #define OWL_ACOUSTIC_ISO_3D 2
 #define OWL_ELASTIC_VHTIORT_2D 3
 #define OWL_ELASTIC_VHTIORT_3D 4
+
+/* parameterisations of the elastic 2D medium (anisotropy_type,
+ * src/solver/elastic_vhtiort_2d/module_vars.f90:235-296) */
+#define OWL_ANISO_ISO 0     /* vp, vs, rho */
+#define OWL_ANISO_THOMSEN 1 /* vp, vs, epsilon, delta, theta, rho */
+#define OWL_ANISO_AT 2      /* vp, vs, epsilon, eta, theta, rho (Alkhalifah-Tsvankin) */
+#define OWL_ANISO_CIJ 3     /* c11, c13, c33, c55, rho */
 
 /* source mechanisms (src/lib/module_source_receiver.f90:66-83) */
 #define OWL_SRC_EXPLOSION 0
@@ -91,6 +98,7 @@ typedef struct {
     float f0_max;        /* max source f0 (Hz): PML alphamax = pi * f0_max */
     int max_shots;       /* capacity of one batched launch (>= 1) */
     int allow_dt_adjust; /* 0: dt above the CFL bound is OWL_ERR_UNSTABLE */
+    int aniso;           /* OWL_ANISO_*: model parameterisation of elastic media */
 } owl_ssg_desc;
 
 /* One source after prepare_geometry / prepare_stf. */
@@ -157,11 +165,16 @@ typedef struct {
 int owl_ssg_create(const owl_ssg_desc *desc, owl_ssg **out);
 
 /* Sets the model. Parameters (each a (nz[,ny],nx) z-fastest float32 host array):
- *   acoustic: vp, rho                                     (nparam = 2)
- *   elastic 2D: vp, vs, rho, epsilon, delta (Thomsen VTI) (nparam = 5)
- *   elastic 3D: c11,c12,c13,c22,c23,c33,c44,c55,c66, rho  (nparam = 10)
+ *   acoustic: vp, rho                                           (nparam = 2)
+ *   elastic 2D, by desc.aniso (theta: tilt, radians):
+ *     OWL_ANISO_ISO      vp, vs, rho                            (nparam = 3)
+ *     OWL_ANISO_THOMSEN  vp, vs, epsilon, delta, theta, rho     (nparam = 6)
+ *     OWL_ANISO_AT       vp, vs, epsilon, eta, theta, rho       (nparam = 6)
+ *     OWL_ANISO_CIJ      c11, c13, c33, c55, rho                (nparam = 5)
  * Replaces the transpose / pad_array / bk = rho*vp^2 part of prepare_modeling
- * (src/solver/acoustic_iso_2d/module_vars.f90:109-115). */
+ * (src/solver/acoustic_iso_2d/module_vars.f90:109-115) and, for elastic 2D, the
+ * Cij set-up and M-PML coefficients (src/solver/elastic_vhtiort_2d/module_vars.f90:235-301,
+ * src/lib/module_anisotropy.f90:310-402, src/solver/elastic_vhtiort_2d/module_cfspml.f90:229-577). */
 int owl_ssg_set_model(owl_ssg *h, int nparam, const float *const *fields);
 
 /* Forward modelling of nshots shots (batched by opts->shots_per_launch).
@@ -246,8 +259,11 @@ const char *owl_last_error(void);
 int owl_ssg_abi_version(void);
 /* dt_stable of the current model (module_vars.f90:121-125); 0 before set_model. */
 float owl_ssg_dt_stable(const owl_ssg *h);
-/* number of parameters and seismogram components of a medium */
+/* number of parameters and seismogram components of a medium (elastic 2D:
+ * the OWL_ANISO_ISO parameterisation) */
 int owl_ssg_nparam(int medium);
+/* number of model parameters of a descriptor (medium and parameterisation) */
+int owl_ssg_desc_nparam(const owl_ssg_desc *desc);
 int owl_ssg_ncomp(int medium);
 /* 1 if the CUDA kernels for sm_100a are present and a device is usable */
 int owl_ssg_device_ok(void);

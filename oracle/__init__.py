@@ -4,4 +4,6 @@ TEST INFRASTRUCTURE ONLY. Imported by tests/, __graft_entry__.smoke() and the
 CPU-baseline leg of bench.py, as the checker. The product (owl_b200) never
 imports it.
 """
-from .oracle import ORACLE_LIB, build, load, ac2d_forward, ac2d_gradient, ac2d_jvp, ac2d_ref_gradient, ac3d_forward, ac3d_gradient, ac3d_jvp  # noqa: F401
+from .oracle import (ORACLE_LIB, build, load, ac2d_forward, ac2d_gradient, ac2d_jvp, ac2d_ref_gradient,  # noqa: F401
+                     ac3d_forward, ac3d_gradient, ac3d_jvp, el2d_forward, el2d_jvp, el2d_gradient, el2d_dt_stable,
+                     el2d_damp_ratio)

@@ -13,7 +13,7 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("oracle_ac2d.cpp", "oracle_ac3d.cpp", "oracle_common.hpp")]
+    srcs = [os.path.join(HERE, f) for f in ("oracle_ac2d.cpp", "oracle_ac3d.cpp", "oracle_el2d.cpp", "oracle_common.hpp")]
     if force or not os.path.exists(ORACLE_LIB) or any(os.path.getmtime(s) > os.path.getmtime(ORACLE_LIB) for s in srcs):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return ORACLE_LIB
@@ -36,6 +36,13 @@ def load():
         _lib.oracle_ac3d_forward_f64.argtypes = [vp, vp, vp, C.c_int, vp, vp]
         _lib.oracle_ac3d_jvp_c128.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp, vp]
         _lib.oracle_ac3d_gradient_f64.argtypes = [vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp]
+        _lib.oracle_el2d_forward_f32.argtypes = [vp, vp, C.c_int, vp, vp]
+        _lib.oracle_el2d_forward_f64.argtypes = [vp, vp, C.c_int, vp, vp]
+        _lib.oracle_el2d_jvp_c128.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp]
+        _lib.oracle_el2d_gradient_f64.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp, vp]
+        _lib.oracle_el2d_setup.argtypes = [vp, vp, vp]
+        _lib.oracle_el2d_damp_ratio.argtypes = [C.c_float] * 5 + [C.c_int]
+        _lib.oracle_el2d_damp_ratio.restype = C.c_float
     return _lib
 
 
@@ -142,3 +149,67 @@ def ac3d_gradient(desc, vp, rho, ps, data, adj_kind=0, k=50):
                                     adj_kind, k, _p(misfit), _p(grad)):
         raise RuntimeError("oracle ac3d gradient failed")
     return misfit, grad
+
+
+# ------------------------------- elastic 2D ----------------------------------
+def _fields(fields, dt):
+    """list of (nz, nx) arrays -> (pointer array, kept arrays), z fastest"""
+    keep = [_fort(f, dt) for f in fields]
+    arr = (C.c_void_p * len(keep))(*[a.ctypes.data for a in keep])
+    return arr, keep
+
+
+def _nseis_el(ps, nt):
+    return 2 * sum(ps.arr[s].nrec for s in range(ps.nshots)) * nt
+
+
+def el2d_forward(desc, fields, ps, precision="f32"):
+    """Elastic seismograms, per shot (vx traces, vz traces) x nt, shots concatenated."""
+    lib = load()
+    dt = np.float32 if precision == "f32" else np.float64
+    arr, keep = _fields(fields, dt)
+    out = np.zeros(_nseis_el(ps, desc.nt), dtype=dt)
+    fn = lib.oracle_el2d_forward_f32 if precision == "f32" else lib.oracle_el2d_forward_f64
+    if fn(C.byref(desc), arr, ps.nshots, C.cast(ps.arr, C.c_void_p), _p(out)) != 0:
+        raise RuntimeError("oracle el2d forward failed")
+    return out
+
+
+def el2d_jvp(desc, fields, dfields, ps):
+    """(seis, d seis . dfields) by complex-step differentiation in FP64."""
+    lib = load()
+    arr, k1 = _fields(fields, np.float64)
+    darr, k2 = _fields(dfields, np.float64)
+    n = _nseis_el(ps, desc.nt)
+    seis, jvp = np.zeros(n), np.zeros(n)
+    if lib.oracle_el2d_jvp_c128(C.byref(desc), arr, darr, ps.nshots, C.cast(ps.arr, C.c_void_p), _p(seis), _p(jvp)):
+        raise RuntimeError("oracle el2d jvp failed")
+    return seis, jvp
+
+
+def el2d_gradient(desc, fields, ps, data, adj_kind=0, k=50, stf_grad=False):
+    """(misfit per shot, grad (nparam, nz*nx) z-fastest, stf gradient or None), FP64 exact adjoint."""
+    lib = load()
+    arr, keep = _fields(fields, np.float64)
+    data = np.ascontiguousarray(data, dtype=np.float64)
+    misfit = np.zeros(ps.nshots)
+    grad = np.zeros(len(fields) * desc.nx * desc.nz)
+    nsrc = sum(ps.arr[s].nsrc for s in range(ps.nshots))
+    sg = np.zeros(nsrc * desc.nt) if stf_grad else None
+    if lib.oracle_el2d_gradient_f64(C.byref(desc), arr, ps.nshots, C.cast(ps.arr, C.c_void_p), _p(data), adj_kind,
+                                    k, _p(misfit), _p(grad), _p(sg)):
+        raise RuntimeError("oracle el2d gradient failed")
+    return misfit, grad, sg
+
+
+def el2d_dt_stable(desc, fields):
+    lib = load()
+    arr, keep = _fields(fields, np.float32)
+    out = C.c_float(0)
+    if lib.oracle_el2d_setup(C.byref(desc), arr, C.byref(out)):
+        raise RuntimeError("oracle el2d setup failed")
+    return out.value
+
+
+def el2d_damp_ratio(c11, c13, c33, c55, rho, direction="x"):
+    return load().oracle_el2d_damp_ratio(c11, c13, c33, c55, rho, 1 if direction == "z" else 0)

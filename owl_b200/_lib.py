@@ -27,6 +27,11 @@ OWL_ACOUSTIC_ISO_3D = 2
 OWL_ELASTIC_VHTIORT_2D = 3
 OWL_ELASTIC_VHTIORT_3D = 4
 
+OWL_ANISO_ISO = 0
+OWL_ANISO_THOMSEN = 1
+OWL_ANISO_AT = 2
+OWL_ANISO_CIJ = 3
+
 OWL_SRC_EXPLOSION = 0
 OWL_SRC_FORCE = 1
 OWL_SRC_MT = 2
@@ -63,6 +68,7 @@ class OwlSsgDesc(C.Structure):
         ("f0_max", C.c_float),
         ("max_shots", C.c_int),
         ("allow_dt_adjust", C.c_int),
+        ("aniso", C.c_int),
     ]
 
 
@@ -135,7 +141,7 @@ EXPORTED = [
     "owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
     "owl_ssg_source_gradient", "owl_ssg_destroy", "owl_last_error", "owl_ssg_abi_version",
     "owl_ssg_dt_stable", "owl_ssg_nparam", "owl_ssg_ncomp", "owl_ssg_device_ok", "owl_ssg_kernel_time",
-    "owl_ssg_forward_noalloc",
+    "owl_ssg_forward_noalloc", "owl_ssg_desc_nparam",
 ]
 
 OWL_K_FWD_P = 0
@@ -179,9 +185,10 @@ def load() -> C.CDLL:
     lib.owl_last_error.restype = C.c_char_p
     lib.owl_ssg_dt_stable.argtypes = [C.c_void_p]
     lib.owl_ssg_dt_stable.restype = C.c_float
+    lib.owl_ssg_desc_nparam.argtypes = [P(OwlSsgDesc)]
     for fn in ("owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
                "owl_ssg_source_gradient", "owl_ssg_abi_version", "owl_ssg_nparam", "owl_ssg_ncomp",
-               "owl_ssg_device_ok"):
+               "owl_ssg_device_ok", "owl_ssg_desc_nparam"):
         getattr(lib, fn).restype = C.c_int
     _lib = lib
     return lib

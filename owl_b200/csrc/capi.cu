@@ -60,8 +60,20 @@ int owl_ssg_nparam(int medium) {
     switch (medium) {
         case OWL_ACOUSTIC_ISO_2D:
         case OWL_ACOUSTIC_ISO_3D: return 2;
-        case OWL_ELASTIC_VHTIORT_2D: return 5;
+        case OWL_ELASTIC_VHTIORT_2D: return 3;
         case OWL_ELASTIC_VHTIORT_3D: return 10;
+        default: return -1;
+    }
+}
+
+int owl_ssg_desc_nparam(const owl_ssg_desc* d) {
+    if (!d) return -1;
+    if (d->medium != OWL_ELASTIC_VHTIORT_2D) return owl_ssg_nparam(d->medium);
+    switch (d->aniso) {
+        case OWL_ANISO_ISO: return 3;
+        case OWL_ANISO_THOMSEN:
+        case OWL_ANISO_AT: return 6;
+        case OWL_ANISO_CIJ: return 5;
         default: return -1;
     }
 }
@@ -96,6 +108,7 @@ int owl_ssg_create(const owl_ssg_desc* desc, owl_ssg** out) {
         switch (desc->medium) {
             case OWL_ACOUSTIC_ISO_2D: h->eng.reset(make_ac2d_engine(*desc)); break;
             case OWL_ACOUSTIC_ISO_3D: h->eng.reset(make_ac3d_engine(*desc)); break;
+            case OWL_ELASTIC_VHTIORT_2D: h->eng.reset(make_el2d_engine(*desc)); break;
             default: throw OwlError(OWL_ERR_UNSUPPORTED, "medium not built");
         }
         *out = h.release();

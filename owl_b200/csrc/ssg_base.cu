@@ -76,6 +76,14 @@ __global__ void k_point_adj(PointDev a, int mode) {
             }
         }
     }
+    if ((mode & PA_SRC_NOW) && blockIdx.y == 0 && a.src_adj && t >= 1) {
+        for (int it = a.inj_shot_ptr[s] + threadIdx.x; it < a.inj_shot_ptr[s + 1]; it += blockDim.x) {
+            float acc = 0.f;
+            for (int j = a.inj.ptr[it]; j < a.inj.ptr[it + 1]; ++j)
+                acc = acc + a.fld[a.inj.field[j]][s * a.sstride + a.inj.off[j]] * a.inj.w[j];
+            a.src_adj[(size_t)it * a.nt + (t - 1)] = acc;
+        }
+    }
     if (mode & PA_TICK) tick_last_block(a.d_step, a.d_done, -1);
 }
 

@@ -46,7 +46,10 @@ struct PointDev {
 };
 
 enum { PT_INJECT = 1, PT_SAMPLE = 2, PT_TICK = 4, PT_NEXT = 8 };  // forward point kernel phases
-enum { PA_SCATTER = 1, PA_SRC = 2, PA_TICK = 4 };                  // adjoint point kernel phases
+// adjoint point kernel phases. PA_SRC records the source-side adjoint of step
+// t-1 after the scatter; PA_SRC_NOW records that of step t from the fields as
+// they are (media whose adjoint kernels interleave with the source terms)
+enum { PA_SCATTER = 1, PA_SRC = 2, PA_TICK = 4, PA_SRC_NOW = 8 };
 
 void launch_point_fwd(const PointDev& q, int S, int nb, int mode, cudaStream_t s);
 void launch_point_adj(const PointDev& q, int S, int nb, int mode, cudaStream_t s);
@@ -141,7 +144,7 @@ struct SsgBase : Engine {
     void build_tables(int S, const owl_shot* shots, bool need_sct);
     void ensure_state(int S, int k, bool grad);
     PointDev pdev(int S, bool adjoint, bool want_src_adj);
-    void launch_step(int kind, int S, const PointDev& q);
+    virtual void launch_step(int kind, int S, const PointDev& q);
     void run_steps(int kind, int n, int S, const PointDev& q, bool graph);
     void resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bool& graph);
     void autotune(int S, int k, bool grad);

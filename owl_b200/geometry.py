@@ -249,7 +249,9 @@ class PreparedShots:
         o.polar = float(f32(q.polar) * deg2rad)
         o.azimuth = float(f32(q.azimuth) * deg2rad)
         o.mt[:] = [float(v) for v in q.mt]
-        ti = time_integration
+        # time_integration may depend on the mechanism (elastic media differentiate
+        # the STF of explosion and moment-tensor sources, module_vars.f90:472-477)
+        ti = time_integration(q.mechanism) if callable(time_integration) else time_integration
         stf, hnt = prepare_stf(q, dt, f0factor, ti)
         stf = np.ascontiguousarray(stf, dtype=f32)
         self._keep.append(stf)

@@ -7,7 +7,7 @@ tensors (device, no host round trip).
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
@@ -50,13 +50,33 @@ def _mem_kind(a) -> int:
     return L.OWL_MEM_HOST
 
 
+def elastic_time_integration(mechanism: str) -> int:
+    """STF time integration of the elastic media: explosion and moment-tensor
+    sources inject the derivative of the wavelet as a stress drop."""
+    return -1 if mechanism in ("explosion", "mt") else 0
+
+
+def elastic_geometry(shots, desc):
+    """With a free surface, sources above the first grid step (z < dz) are moved
+    to z = dz and their amplitude multiplied by 1.2 (module_vars.f90:466-469)."""
+    if not desc.free_surface:
+        return shots
+    dz = np.float32(desc.dz)
+    out = []
+    for sh in shots:
+        srcs = [replace(q, z=float(dz), amp=float(np.float32(q.amp) * np.float32(1.2))) if np.float32(q.z) < dz else q
+                for q in sh.sources]
+        out.append(replace(sh, sources=srcs))
+    return out
+
+
 class SSGSolver:
     """One solver handle: grid, PML, time axis and model of one medium."""
 
     def __init__(self, medium: int, nx: int, nz: int, dx: float, dz: float, dt: float, nt: int,
                  pml: int = 15, fdhalf: int = 4, free_surface: bool = False, f0_max: float = 20.0,
                  max_shots: int = 1, ny: int = 1, dy: float = 0.0, ox: float = 0.0, oy: float = 0.0,
-                 oz: float = 0.0, allow_dt_adjust: bool = False):
+                 oz: float = 0.0, allow_dt_adjust: bool = False, aniso: int = 0):
         self.lib = L.load()
         d = L.OwlSsgDesc()
         d.medium = medium
@@ -67,13 +87,14 @@ class SSGSolver:
         d.dt, d.nt, d.f0_max = dt, nt, f0_max
         d.max_shots = max_shots
         d.allow_dt_adjust = int(bool(allow_dt_adjust))
+        d.aniso = int(aniso)
         self.desc = d
         self.grid = GridSpec(nx=nx, nz=nz, dx=dx, dz=dz, ox=ox, oz=oz, ny=ny, dy=(dy if dy else dx), oy=oy)
         h = C.c_void_p()
         L.check(self.lib.owl_ssg_create(C.byref(d), C.byref(h)))
         self.h = h
         self.ncomp = self.lib.owl_ssg_ncomp(medium)
-        self.nparam = self.lib.owl_ssg_nparam(medium)
+        self.nparam = self.lib.owl_ssg_desc_nparam(C.byref(d))
         self.last_info = L.OwlRunInfo()
 
     def close(self):
@@ -99,8 +120,18 @@ class SSGSolver:
             arr[i] = f.ctypes.data_as(C.POINTER(C.c_float))
         L.check(self.lib.owl_ssg_set_model(self.h, len(self._model), arr))
 
-    def prepare(self, shots, f0factor: float = 1.0, time_integration: int = 0) -> PreparedShots:
-        return PreparedShots(shots, self.grid, self.desc.dt, f0factor, time_integration)
+    def prepare(self, shots, f0factor: float = 1.0, time_integration=None) -> PreparedShots:
+        """Sources and receivers on the grid (prepare_geometry / prepare_stf). For the
+        elastic medium the STF of explosion and moment-tensor sources is
+        differentiated (time_integration = -1) and, with a free surface, sources
+        shallower than the first grid step move down to it with 1.2 x amplitude
+        (src/solver/elastic_vhtiort_2d/module_vars.f90:466-477)."""
+        if self.desc.medium == L.OWL_ELASTIC_VHTIORT_2D:
+            shots = elastic_geometry(shots, self.desc)
+            if time_integration is None:
+                time_integration = elastic_time_integration
+        return PreparedShots(shots, self.grid, self.desc.dt, f0factor,
+                             0 if time_integration is None else time_integration)
 
     def seis_size(self, ps: PreparedShots) -> int:
         return sum(ps.nrec(s) for s in range(ps.nshots)) * self.ncomp * self.desc.nt

@@ -30,15 +30,22 @@ def test_header_symbols_exported():
 
 def test_queries():
     lib = L.load()
-    assert lib.owl_ssg_abi_version() == 1
+    assert lib.owl_ssg_abi_version() == 2
     assert lib.owl_ssg_nparam(L.OWL_ACOUSTIC_ISO_2D) == 2
     assert lib.owl_ssg_ncomp(L.OWL_ELASTIC_VHTIORT_2D) == 2
     assert lib.owl_ssg_nparam(99) == -1
+    d = L.OwlSsgDesc()
+    d.medium = L.OWL_ELASTIC_VHTIORT_2D
+    for aniso, n in ((L.OWL_ANISO_ISO, 3), (L.OWL_ANISO_THOMSEN, 6), (L.OWL_ANISO_AT, 6), (L.OWL_ANISO_CIJ, 5), (9, -1)):
+        d.aniso = aniso
+        assert lib.owl_ssg_desc_nparam(C.byref(d)) == n
+    d.medium = L.OWL_ACOUSTIC_ISO_3D
+    assert lib.owl_ssg_desc_nparam(C.byref(d)) == 2
 
 
 def test_struct_sizes_match_header():
     # ctypes mirrors the C structs field for field (no padding surprises)
-    assert C.sizeof(L.OwlSsgDesc) == 4 * 18
+    assert C.sizeof(L.OwlSsgDesc) == 4 * 19
     assert C.sizeof(L.OwlRunOpts) == 4 * 8
     assert C.sizeof(L.OwlReceiver) == 4 * (6 + 54 + 1)
 
