@@ -43,6 +43,9 @@ def parse():
     p.add_argument("--no-3d", action="store_true", help="skip the 3D acoustic forward roofline block")
     p.add_argument("--profile3d", type=int, default=0, metavar="N",
                    help="profiling target: 12-step 3D acoustic forward of an N^3 model, no JSON line")
+    p.add_argument("--no-elastic", action="store_true", help="skip the 2D elastic VTI block")
+    p.add_argument("--profile-el", type=int, default=0, metavar="S",
+                   help="profiling target: one 2D elastic VTI gradient of S shots, 60 steps, no JSON line")
     return p.parse_args()
 
 
@@ -93,6 +96,72 @@ def forward_3d_block(peak, peak_kind):
         out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                                 "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
                                 "traffic": profile_traffic(name)}
+    s.close()
+    return out
+
+
+def elastic_solver(nshots, nt):
+    from owl_b200 import _lib as L
+    from owl_b200 import configs
+    from owl_b200.solver import SSGSolver
+
+    d, f, shots = configs.config4(nshots, nt=nt)
+    s = SSGSolver(L.OWL_ELASTIC_VHTIORT_2D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
+                  free_surface=True, f0_max=d.f0_max, max_shots=nshots, aniso=d.aniso)
+    s.set_model(*f)
+    return d, f, s, s.prepare(shots)
+
+
+def profile_elastic(nshots):
+    """Small elastic gradient for kernel captures: the 2D VTI model, S shots, 60 steps."""
+    import numpy as np
+    from owl_b200.solver import RunOpts
+    d, f, s, ps = elastic_solver(nshots, 60)
+    obs = np.zeros(s.seis_size(ps), dtype=np.float32)
+    s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=20, shots_per_cta=1, tile_z=8, use_graph=-1))
+    print(f"profile-el: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
+    s.close()
+
+
+def elastic_2d_block(peak, peak_kind, ngrad=16):
+    """2D elastic VTI with a free surface (301 x 601, dx 5 m, 4000 steps, Thomsen
+    parameters): forward of all 64 shots (Gcell-updates/s), gradient of `ngrad`
+    shots (s/shot), and the HBM roofline of the four stencil kernels."""
+    import numpy as np
+    from owl_b200 import _lib as L
+    from owl_b200.solver import RunOpts
+
+    d, f, s, ps = elastic_solver(64, 4000)
+    cells = float(d.nx + 2 * d.pml) * (d.nz + d.pml)  # rows from the surface down
+    s.forward(ps, RunOpts())
+    fwd = []
+    for _ in range(2):
+        s.forward(ps, RunOpts())
+        fwd.append(s.last_info.elapsed_ms)
+    fms = sum(fwd) / len(fwd)
+    out = {"workload": "2D elastic VTI, 301 x 601 model, dx 5 m, dt 0.5 ms, 4000 steps, PML 20, free surface, "
+                       "64 shots (explosion / vertical force), 301 two-component receivers",
+           "forward_ms_64_shots": fms, "forward_gcells_per_s": cells * d.nt * 64 / (fms / 1e3) / 1e9}
+    from owl_b200 import configs
+    sub = s.prepare(configs.config4_shots(64, d.nx, d.dx)[:ngrad])
+    obs = np.zeros(s.seis_size(sub), dtype=np.float32)
+    opts = RunOpts(checkpoint_precision=L.OWL_CKPT_FP16)
+    s.gradient(sub, obs, opts=opts)
+    gms = []
+    for _ in range(2):
+        s.gradient(sub, obs, opts=opts)
+        gms.append(s.last_info.elapsed_ms)
+    out["gradient_shots"] = ngrad
+    out["gradient_s_per_shot"] = sum(gms) / len(gms) / 1e3 / ngrad
+    out["gradient_checkpoints"] = "fp16, per-field scale, every 50 steps"
+    out["kernels"] = {}
+    for kid, name in ((L.OWL_K_FWD_P, "k_el2d_fwd_s"), (L.OWL_K_FWD_V, "k_el2d_fwd_v"),
+                      (L.OWL_K_ADJ_P, "k_el2d_adj_v"), (L.OWL_K_ADJ_V, "k_el2d_adj_s")):
+        kms, b = s.kernel_time(kid, 20)
+        ach = b / (kms / 1e3) / 1e9
+        out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
+                                "shots_per_launch": ngrad, "traffic": profile_traffic(name)}
     s.close()
     return out
 
@@ -224,6 +293,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.profile3d:
         return profile_3d(args.profile3d)
+    if args.profile_el:
+        return profile_elastic(args.profile_el)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
@@ -381,6 +452,8 @@ def main():
     s.close()
     if rank == 0 and not args.no_3d:
         line["forward_3d"] = forward_3d_block(peak, peak_kind)
+    if rank == 0 and not args.no_elastic:
+        line["elastic_2d"] = elastic_2d_block(peak, peak_kind)
 
     if rank == 0:
         print(json.dumps(line), flush=True)

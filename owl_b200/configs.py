@@ -110,3 +110,53 @@ def config3(n=400, nt=1500):
     recs = [Receiver(x=20.0 * i, y=20.0 * j, z=20.0) for j in range(nr) for i in range(nr)]
     shots = [Shot(1, [Source(x=c, y=c, z=20.0, f0=12.0)], recs)]
     return d, vp, rho, shots
+
+
+def _rescaled_noise(shape, sigma_cells, seed, lo, hi):
+    """Gaussian-filtered seeded white noise rescaled to [lo, hi]."""
+    from scipy.ndimage import gaussian_filter
+    w = np.random.default_rng(seed).standard_normal(shape)
+    f = gaussian_filter(w, sigma=sigma_cells, mode="nearest")
+    f = (f - f.min()) / max(1e-30, f.max() - f.min())
+    return (lo + (hi - lo) * f).astype(np.float32)
+
+
+def elastic_2d_vti_model(nz=301, nx=601, dx=5.0, eps_max=0.2):
+    """Vp 1800 -> 4500 m/s linear in depth, Vs = Vp / 1.8, Gardner rho, Thomsen
+    epsilon in [0, eps_max] and delta in [-0.05, 0.1] as smooth seeded fields
+    (Gaussian-filtered white noise, sigma 100 m, seeds 7 and 8), no tilt.
+    Returns (vp, vs, epsilon, delta, theta, rho), each (nz, nx)."""
+    z = np.arange(nz, dtype=np.float64)[:, None] * dx
+    vp = np.broadcast_to(1800.0 + 2700.0 * z / ((nz - 1) * dx), (nz, nx)).astype(np.float32)
+    vs = (vp / np.float32(1.8)).astype(np.float32)
+    rho = (310.0 * vp.astype(np.float64) ** 0.25).astype(np.float32)
+    sig = 100.0 / dx
+    eps = _rescaled_noise((nz, nx), sig, 7, 0.0, eps_max)
+    dl = _rescaled_noise((nz, nx), sig, 8, -0.05, 0.1)
+    return vp, vs, eps, dl, np.zeros_like(vp), rho
+
+
+def config4_shots(nshots=64, nx=601, dx=5.0, zsrc=10.0):
+    """Shots evenly spaced from 100 m to (nx-1) dx - 100 m at z = zsrc, alternating an
+    explosion and a vertical force (polar 0), 15 Hz Ricker; receivers every 10 m at
+    z = 0 (two components, vx and vz)."""
+    xmax = (nx - 1) * dx
+    recs = [Receiver(x=10.0 * i, z=0.0) for i in range(int(xmax // 10.0) + 1)]
+    shots = []
+    for k in range(nshots):
+        xs = 100.0 + k * ((xmax - 200.0) / max(1, nshots - 1))
+        src = Source(x=xs, z=zsrc, f0=15.0) if k % 2 == 0 else Source(x=xs, z=zsrc, mechanism="force", polar=0.0, f0=15.0)
+        shots.append(Shot(k + 1, [src], recs))
+    return shots
+
+
+def config4(nshots=64, nt=4000):
+    """2D elastic VTI with a flat free surface on the uniform grid: 301 x 601,
+    dx = dz = 5 m, dt = 0.5 ms, 4000 steps, PML 20, 8th order, Thomsen
+    parameterisation; 64 shots (explosion / vertical force, 15 Hz); receivers every
+    10 m at the surface. epsilon is capped at 0.19 so that the fastest qP speed
+    (Vp sqrt(1 + 2 eps) at Vp = 4500) keeps dt = 0.5 ms inside the CFL bound."""
+    nz, nx, dx, dt = 301, 601, 5.0, 5e-4
+    d = _desc(L.OWL_ELASTIC_VHTIORT_2D, nx, nz, dx, dt, nt, pml=20, fs=1, f0=15.0, max_shots=nshots)
+    d.aniso = L.OWL_ANISO_THOMSEN
+    return d, elastic_2d_vti_model(nz, nx, dx, eps_max=0.19), config4_shots(nshots, nx, dx)

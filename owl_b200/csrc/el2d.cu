@@ -89,10 +89,10 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_s(El2dDev a) {
     const bool px_i = el_pml_int(x, a.pr, a.nx);
     const bool pii = px_i || (!a.fsurf && z < a.pr) || z >= a.pr + a.nz;
     const bool phh = el_pml_half(x, a.pr, a.nx) || (!a.fsurf && z <= a.pr) || z >= a.pr + a.nz;
-    const float4 cii = pii ? a.pii[o] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 chh = (phh && dxz) ? a.phh[o] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float c11 = a.c11[o], c13 = a.c13[o], c33 = a.c33[o];
-    const float c55dt = dxz ? a.dt * a.c55e[o] : 0.f;
+    const float4 cii = pii ? __ldg(a.pii + o) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 chh = (phh && dxz) ? __ldg(a.phh + o) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float c11 = __ldg(a.c11 + o), c13 = __ldg(a.c13 + o), c33 = __ldg(a.c33 + o);
+    const float c55dt = dxz ? a.dt * __ldg(a.c55e + o) : 0.f;
     const bool mir = a.fsurf && z > a.pr && z <= a.pr + a.R;
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_s(El2dDev a) {
         // sigma_xx, sigma_zz
         float sx = 0.f;
 #pragma unroll
-        for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (vx[k] - vx[1 - k]);
+        for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (__ldg(vx + (k)) - __ldg(vx + (1 - k)));
         float dxv = a.idx * sx, dzv;
         if (row1) {
             if (px_i) {
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_s(El2dDev a) {
         } else {
             float sz = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (vz[k * pt] - vz[(1 - k) * pt]);
+            for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(vz + (k * pt)) - __ldg(vz + ((1 - k) * pt)));
             dzv = a.idz * sz;
             if (pii) {
                 const float m1 = cii.x * dxv + cii.y * mem[M_DXVX * a.fs];
@@ -145,9 +145,9 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_s(El2dDev a) {
         if (dxz) {
             float szx = 0.f, sxz = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) szx = szx + c_fde[k - 1] * (vx[(k - 1) * pt] - vx[-k * pt]);
+            for (int k = 1; k <= R; ++k) szx = szx + c_fde[k - 1] * (__ldg(vx + ((k - 1) * pt)) - __ldg(vx + (-k * pt)));
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sxz = sxz + c_fde[k - 1] * (vz[k - 1] - vz[-k]);
+            for (int k = 1; k <= R; ++k) sxz = sxz + c_fde[k - 1] * (__ldg(vz + (k - 1)) - __ldg(vz + (-k)));
             float dzvx = a.idz * szx, dxvz = a.idx * sxz;
             if (phh) {
                 const float m3 = chh.x * dxvz + chh.y * mem[M_DXVZ * a.fs];
@@ -177,9 +177,9 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
     const bool dvz = z >= a.zvz0;
     const bool phi = el_pml_half(x, a.pr, a.nx) || (!a.fsurf && z < a.pr) || z >= a.pr + a.nz;
     const bool pih = el_pml_int(x, a.pr, a.nx) || (!a.fsurf && z <= a.pr) || z >= a.pr + a.nz;
-    const float4 chi = phi ? a.phi[o] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 cih = (pih && dvz) ? a.pih[o] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float bx = a.bx[o], bz = dvz ? a.bz[o] : 0.f;
+    const float4 chi = phi ? __ldg(a.phi + o) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 cih = (pih && dvz) ? __ldg(a.pih + o) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float bx = __ldg(a.bx + o), bz = dvz ? __ldg(a.bz + o) : 0.f;
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
     for (int s = s0; s < s1; ++s) {
@@ -191,9 +191,9 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
         {
             float sx = 0.f, sz = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (sxx[k - 1] - sxx[-k]);
+            for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (__ldg(sxx + (k - 1)) - __ldg(sxx + (-k)));
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (sxz[k * pt] - sxz[(1 - k) * pt]);
+            for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(sxz + (k * pt)) - __ldg(sxz + ((1 - k) * pt)));
             float hx = a.idx * sx, hz = a.idz * sz;
             if (phi) {
                 const float m1 = chi.x * hx + chi.y * mem[M_DXXX * a.fs];
@@ -211,9 +211,9 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
         if (dvz) {
             float sx = 0.f, sz = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (sxz[k] - sxz[1 - k]);
+            for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (__ldg(sxz + (k)) - __ldg(sxz + (1 - k)));
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (szz[(k - 1) * pt] - szz[-k * pt]);
+            for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(szz + ((k - 1) * pt)) - __ldg(szz + (-k * pt)));
             float hx = a.idx * sx, hz = a.idz * sz;
             if (pih) {
                 const float m1 = cih.x * hx + cih.y * mem[M_DXXZ * a.fs];
@@ -258,9 +258,9 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
     const bool dvz = z >= a.zvz0;
     const bool phi = el_pml_half(x, a.pr, a.nx) || (!a.fsurf && z < a.pr) || z >= a.pr + a.nz;
     const bool pih = el_pml_int(x, a.pr, a.nx) || (!a.fsurf && z <= a.pr) || z >= a.pr + a.nz;
-    const float4 chi = phi ? a.phi[o] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 cih = (pih && dvz) ? a.pih[o] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float bx = a.bx[o], bz = dvz ? a.bz[o] : 0.f;
+    const float4 chi = phi ? __ldg(a.phi + o) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 cih = (pih && dvz) ? __ldg(a.pih + o) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float bx = __ldg(a.bx + o), bz = dvz ? __ldg(a.bz + o) : 0.f;
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     float gbx = 0.f, gbz = 0.f;
     for (int s = s0; s < s1; ++s) {
@@ -273,13 +273,13 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
             const float* e2 = e + M_DZVX * a.fs;
             float sx = 0.f, sz = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (e1[-k] - e1[k - 1]);
+            for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (__ldg(e1 + (-k)) - __ldg(e1 + (k - 1)));
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (e2[(1 - k) * pt] - e2[k * pt]);
+            for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(e2 + ((1 - k) * pt)) - __ldg(e2 + (k * pt)));
             float* vh = ad + EL_VX * a.fs + o;
             const float v = *vh + (a.idx * sx + a.idz * sz);
             *vh = v;
-            gbx += v * a.S[3 * a.sterm + so];
+            gbx += v * __ldg(a.S + 3 * a.sterm + so);
             const float q = bx * v;
             float ex = q, ez = q;
             if (phi) {
@@ -294,13 +294,13 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
             const float* e3 = e + M_DXVZ * a.fs;
             float sz = 0.f, sx = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (e4[-k * pt] - e4[(k - 1) * pt]);
+            for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(e4 + (-k * pt)) - __ldg(e4 + ((k - 1) * pt)));
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (e3[1 - k] - e3[k]);
+            for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (__ldg(e3 + (1 - k)) - __ldg(e3 + (k)));
             float* vh = ad + EL_VZ * a.fs + o;
             const float v = *vh + (a.idz * sz + a.idx * sx);
             *vh = v;
-            gbz += v * a.S[4 * a.sterm + so];
+            gbz += v * __ldg(a.S + 4 * a.sterm + so);
             const float q = bz * v;
             float ex = q, ez = q;
             if (pih) {
@@ -334,10 +334,10 @@ __global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
     const bool px_i = el_pml_int(x, a.pr, a.nx);
     const bool pii = px_i || (!a.fsurf && z < a.pr) || z >= a.pr + a.nz;
     const bool phh = el_pml_half(x, a.pr, a.nx) || (!a.fsurf && z <= a.pr) || z >= a.pr + a.nz;
-    const float4 cii = pii ? a.pii[o] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 chh = (phh && dxz) ? a.phh[o] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float c11 = a.c11[o], c13 = a.c13[o], c33 = a.c33[o];
-    const float c55dt = dxz ? a.dt * a.c55e[o] : 0.f;
+    const float4 cii = pii ? __ldg(a.pii + o) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 chh = (phh && dxz) ? __ldg(a.phh + o) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float c11 = __ldg(a.c11 + o), c13 = __ldg(a.c13 + o), c33 = __ldg(a.c33 + o);
+    const float c55dt = dxz ? a.dt * __ldg(a.c55e + o) : 0.f;
     const bool mir = a.fsurf && z > a.pr && z <= a.pr + a.R;
     const long long ozz = (long long)(2 * a.pr - z) * pt + x;      // sigma_zz image row
     const long long oxz = (long long)(2 * a.pr + 1 - z) * pt + x;  // sigma_xz image row
@@ -354,9 +354,9 @@ __global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
         const float* e8 = e + M_DZZZ * a.fs + o;
         float sx = 0.f, sz = 0.f;
 #pragma unroll
-        for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (e5[1 - k] - e5[k]);
+        for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (__ldg(e5 + (1 - k)) - __ldg(e5 + (k)));
 #pragma unroll
-        for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (e8[(1 - k) * pt] - e8[k * pt]);
+        for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(e8 + ((1 - k) * pt)) - __ldg(e8 + (k * pt)));
         float* xhp = ad + EL_SXX * a.fs + o;
         float* zhp = ad + EL_SZZ * a.fs + o;
         const float xh = *xhp + a.idx * sx;
@@ -369,14 +369,14 @@ __global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
                 const float* em = e + M_DZZZ * a.fs + ozz;
                 float sm = 0.f;
 #pragma unroll
-                for (int k = 1; k <= R; ++k) sm = sm + c_fde[k - 1] * em[k * pt];
+                for (int k = 1; k <= R; ++k) sm = sm + c_fde[k - 1] * __ldg(em + (k * pt));
                 dz = dz + a.idz * sm;
             }
             zh = *zhp + dz;
         }
         *xhp = xh;
         *zhp = zh;
-        const float S0 = a.S[so], S1 = a.S[a.sterm + so];
+        const float S0 = __ldg(a.S + so), S1 = __ldg(a.S + a.sterm + so);
         float ex, ez = 0.f;
         if (row1) {
             g11 += xh * S0;
@@ -405,9 +405,9 @@ __global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
             const float* e7 = e + M_DXXZ * a.fs + o;
             float tz = 0.f, tx = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) tz = tz + c_fde[k - 1] * (e6[-k * pt] - e6[(k - 1) * pt]);
+            for (int k = 1; k <= R; ++k) tz = tz + c_fde[k - 1] * (__ldg(e6 + (-k * pt)) - __ldg(e6 + ((k - 1) * pt)));
 #pragma unroll
-            for (int k = 1; k <= R; ++k) tx = tx + c_fde[k - 1] * (e7[-k] - e7[k - 1]);
+            for (int k = 1; k <= R; ++k) tx = tx + c_fde[k - 1] * (__ldg(e7 + (-k)) - __ldg(e7 + (k - 1)));
             float dsum = a.idz * tz + a.idx * tx;
             if (mir) {
                 // the image row collects -e_dzxz(image + k - 1) from the vx nodes at
@@ -416,13 +416,13 @@ __global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
                 const float* em6 = e + M_DZXZ * a.fs + oxz;
                 float mz = 0.f;
 #pragma unroll
-                for (int k = 1; k <= R; ++k) mz = mz + c_fde[k - 1] * em6[(k - 1) * pt];
+                for (int k = 1; k <= R; ++k) mz = mz + c_fde[k - 1] * __ldg(em6 + ((k - 1) * pt));
                 dsum = dsum + a.idz * mz;
             }
             float* shp = ad + EL_SXZ * a.fs + o;
             const float sh = *shp + dsum;
             *shp = sh;
-            g55 += sh * a.S[2 * a.sterm + so];
+            g55 += sh * __ldg(a.S + 2 * a.sterm + so);
             const float q = c55dt * sh;
             float ezx = q, exz = q;
             if (phh) {

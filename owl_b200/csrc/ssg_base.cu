@@ -424,11 +424,7 @@ void SsgBase::resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bo
     k = std::min(k, desc.nt);
     spt_f = spt_a = std::min(o.shots_per_cta > 0 ? o.shots_per_cta : 1, B);
     graph = o.use_graph >= 0;
-    tile_x = o.tile_x > 0 ? o.tile_x : 32;
-    tz_f = tz_a = o.tile_z > 0 ? o.tile_z : (dim == 3 ? 4 : 8);
-    if (dim == 3 && o.tile_z < 0) tz_f = 0;
-    OWL_CHECK(tile_x % 32 == 0 && tz_a >= 1 && tile_x * tz_a <= 512 && (tz_f >= 1 || dim == 3), OWL_ERR_INVALID,
-              "tile_x must be a multiple of 32 and tile_x * tile_z <= 512");
+    launch_params(o);
     OWL_CHECK(o.checkpoint_precision >= OWL_CKPT_FP32 && o.checkpoint_precision <= OWL_CKPT_BF16, OWL_ERR_INVALID,
               "bad checkpoint precision");
     ckpt_prec = o.checkpoint_precision;
@@ -438,6 +434,22 @@ void SsgBase::resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bo
 // candidate on this batch's buffers, forward pair and adjoint pair separately,
 // and keeps the fastest. Cached per (batch size, gradient). The buffers'
 // contents are reset by the caller afterwards.
+void SsgBase::launch_params(const owl_run_opts& o) {
+    tile_x = o.tile_x > 0 ? o.tile_x : 32;
+    tz_f = tz_a = o.tile_z > 0 ? o.tile_z : (dim == 3 ? 4 : 8);
+    if (dim == 3 && o.tile_z < 0) tz_f = 0;
+    OWL_CHECK(tile_x % 32 == 0 && tz_a >= 1 && tile_x * tz_a <= 512 && (tz_f >= 1 || dim == 3), OWL_ERR_INVALID,
+              "tile_x must be a multiple of 32 and tile_x * tile_z <= 512");
+}
+
+std::vector<int> SsgBase::tune_spt(int) const { return {1, 2, 4, 8, 16, 32}; }
+
+// 3D forward kernels take rows per thread (1, 2, 4; 0 = the per-cell kernel); other kernels a tile height
+std::vector<int> SsgBase::tune_tz(int pass) const {
+    if (dim == 3) return pass == 0 ? std::vector<int>{0, 1, 2, 4} : std::vector<int>{2, 4, 8};
+    return {4, 8, 16};
+}
+
 void SsgBase::autotune(int S, int k, bool grad) {
     auto key = std::make_pair(S, grad ? 1 : 0);
     auto it = tune_cache.find(key);
@@ -448,12 +460,10 @@ void SsgBase::autotune(int S, int k, bool grad) {
     cur_k = k;
     set_step(k);
     for (int pass = 0; pass < (grad ? 2 : 1); ++pass) {
-        // 3D forward kernels take rows per thread (1, 2, 4); other kernels a tile height
-        const std::vector<int> tzs = dim == 3 ? (pass == 0 ? std::vector<int>{0, 1, 2, 4} : std::vector<int>{2, 4, 8})
-                                              : std::vector<int>{4, 8, 16};
+        const std::vector<int> tzs = tune_tz(pass);
         float best = 1e30f;
-        int bs = 1, bt = tzs[1];
-        for (int spt : {1, 2, 4, 8, 16, 32}) {
+        int bs = 1, bt = tzs[std::min<size_t>(1, tzs.size() - 1)];
+        for (int spt : tune_spt(pass)) {
             if (spt > S) break;
             for (int tz : tzs) {
                 if (pass == 0) { spt_f = spt; tz_f = tz; } else { spt_a = spt; tz_a = tz; }

@@ -117,6 +117,13 @@ struct SsgBase : Engine {
     virtual int rho_param() const = 0;
     virtual float* st_field(int f) const = 0;  // base pointer (shot 0) of forward field f
     virtual float* ad_field(int f) const = 0;  // base pointer (shot 0) of adjoint field f
+    // autotuner candidates of pass 0 (forward kernels) / 1 (adjoint kernels): shots
+    // per CTA and the kernel's second launch parameter (tile height, rows per
+    // thread or rows per chunk, as the medium's kernels define it)
+    virtual std::vector<int> tune_spt(int pass) const;
+    virtual std::vector<int> tune_tz(int pass) const;
+    // tile_x / tile_z of the run options (validated), spt_f / spt_a already set
+    virtual void launch_params(const owl_run_opts& o);
 
     // ---------------- helpers ----------------
     long long soff(int i, int j, int k) const {
