@@ -10,6 +10,8 @@
  *       src/solver/acoustic_iso_3d/interface.f90:30-60
  *   wave_solver_elastic_vhtiort_2d%forward / %adjoint
  *       src/solver/elastic_vhtiort_2d/interface.f90:29-77
+ *   wave_solver_elastic_vhtiort_3d%forward / %adjoint
+ *       src/solver/elastic_vhtiort_3d/interface.f90:30-79
  * One handle holds what the Fortran module variables hold there (padded model,
  * CFS-PML coefficients, wavefields), but per handle, so handles are re-entrant.
  *
@@ -171,6 +173,9 @@ int owl_ssg_create(const owl_ssg_desc *desc, owl_ssg **out);
  *     OWL_ANISO_THOMSEN  vp, vs, epsilon, delta, theta, rho     (nparam = 6)
  *     OWL_ANISO_AT       vp, vs, epsilon, eta, theta, rho       (nparam = 6)
  *     OWL_ANISO_CIJ      c11, c13, c33, c55, rho                (nparam = 5)
+ *   elastic 3D, by desc.aniso (no free surface):
+ *     OWL_ANISO_ISO      vp, vs, rho                            (nparam = 3)
+ *     OWL_ANISO_CIJ      c11, c12, c13, c22, c23, c33, c44, c55, c66, rho (nparam = 10)
  * Replaces the transpose / pad_array / bk = rho*vp^2 part of prepare_modeling
  * (src/solver/acoustic_iso_2d/module_vars.f90:109-115) and, for elastic 2D, the
  * Cij set-up and M-PML coefficients (src/solver/elastic_vhtiort_2d/module_vars.f90:235-301,
@@ -180,7 +185,8 @@ int owl_ssg_set_model(owl_ssg *h, int nparam, const float *const *fields);
 /* Forward modelling of nshots shots (batched by opts->shots_per_launch).
  * Replaces compute_forward (src/solver/acoustic_iso_2d/submodule_forward_modeling.f90:31-132).
  * seis: per shot, ncomp x nrec x nt float32 (trace-major, the SU trace order),
- * shots concatenated; ncomp = 1 (p) for acoustic, 2 (vx, vz) for elastic 2D. */
+ * shots concatenated; ncomp = 1 (p) for acoustic, 2 (vx, vz) for elastic 2D,
+ * 3 (vx, vy, vz) for elastic 3D. */
 int owl_ssg_forward(owl_ssg *h, int nshots, const owl_shot *shots,
                     const owl_run_opts *opts, float *seis, int mem_kind,
                     owl_run_info *info);

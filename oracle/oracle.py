@@ -13,7 +13,7 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("oracle_ac2d.cpp", "oracle_ac3d.cpp", "oracle_el2d.cpp", "oracle_common.hpp")]
+    srcs = [os.path.join(HERE, f) for f in ("oracle_ac2d.cpp", "oracle_ac3d.cpp", "oracle_el2d.cpp", "oracle_el3d.cpp", "oracle_common.hpp")]
     if force or not os.path.exists(ORACLE_LIB) or any(os.path.getmtime(s) > os.path.getmtime(ORACLE_LIB) for s in srcs):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return ORACLE_LIB
@@ -43,6 +43,11 @@ def load():
         _lib.oracle_el2d_setup.argtypes = [vp, vp, vp]
         _lib.oracle_el2d_damp_ratio.argtypes = [C.c_float] * 5 + [C.c_int]
         _lib.oracle_el2d_damp_ratio.restype = C.c_float
+        _lib.oracle_el3d_forward_f32.argtypes = [vp, vp, C.c_int, vp, vp]
+        _lib.oracle_el3d_forward_f64.argtypes = [vp, vp, C.c_int, vp, vp]
+        _lib.oracle_el3d_jvp_c128.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp]
+        _lib.oracle_el3d_gradient_f64.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp, vp]
+        _lib.oracle_el3d_setup.argtypes = [vp, vp, vp]
     return _lib
 
 
@@ -213,3 +218,54 @@ def el2d_dt_stable(desc, fields):
 
 def el2d_damp_ratio(c11, c13, c33, c55, rho, direction="x"):
     return load().oracle_el2d_damp_ratio(c11, c13, c33, c55, rho, 1 if direction == "z" else 0)
+
+
+# ------------------------------- elastic 3D ----------------------------------
+def _nseis_el3(ps, nt):
+    return 3 * sum(ps.arr[s].nrec for s in range(ps.nshots)) * nt
+
+
+def el3d_forward(desc, fields, ps, precision="f32"):
+    """3D elastic seismograms, per shot (vx, vy, vz traces) x nt; fields (nz, ny, nx)."""
+    lib = load()
+    dt = np.float32 if precision == "f32" else np.float64
+    arr, keep = _fields(fields, dt)
+    out = np.zeros(_nseis_el3(ps, desc.nt), dtype=dt)
+    fn = lib.oracle_el3d_forward_f32 if precision == "f32" else lib.oracle_el3d_forward_f64
+    if fn(C.byref(desc), arr, ps.nshots, C.cast(ps.arr, C.c_void_p), _p(out)) != 0:
+        raise RuntimeError("oracle el3d forward failed")
+    return out
+
+
+def el3d_jvp(desc, fields, dfields, ps):
+    lib = load()
+    arr, k1 = _fields(fields, np.float64)
+    darr, k2 = _fields(dfields, np.float64)
+    n = _nseis_el3(ps, desc.nt)
+    seis, jvp = np.zeros(n), np.zeros(n)
+    if lib.oracle_el3d_jvp_c128(C.byref(desc), arr, darr, ps.nshots, C.cast(ps.arr, C.c_void_p), _p(seis), _p(jvp)):
+        raise RuntimeError("oracle el3d jvp failed")
+    return seis, jvp
+
+
+def el3d_gradient(desc, fields, ps, data, adj_kind=0, k=50, stf_grad=False):
+    lib = load()
+    arr, keep = _fields(fields, np.float64)
+    data = np.ascontiguousarray(data, dtype=np.float64)
+    misfit = np.zeros(ps.nshots)
+    grad = np.zeros(len(fields) * desc.nx * desc.ny * desc.nz)
+    nsrc = sum(ps.arr[s].nsrc for s in range(ps.nshots))
+    sg = np.zeros(nsrc * desc.nt) if stf_grad else None
+    if lib.oracle_el3d_gradient_f64(C.byref(desc), arr, ps.nshots, C.cast(ps.arr, C.c_void_p), _p(data), adj_kind,
+                                    k, _p(misfit), _p(grad), _p(sg)):
+        raise RuntimeError("oracle el3d gradient failed")
+    return misfit, grad, sg
+
+
+def el3d_dt_stable(desc, fields):
+    lib = load()
+    arr, keep = _fields(fields, np.float32)
+    out = C.c_float(0)
+    if lib.oracle_el3d_setup(C.byref(desc), arr, C.byref(out)):
+        raise RuntimeError("oracle el3d setup failed")
+    return out.value

@@ -68,6 +68,8 @@ int owl_ssg_nparam(int medium) {
 
 int owl_ssg_desc_nparam(const owl_ssg_desc* d) {
     if (!d) return -1;
+    if (d->medium == OWL_ELASTIC_VHTIORT_3D)
+        return d->aniso == OWL_ANISO_ISO ? 3 : d->aniso == OWL_ANISO_CIJ ? 10 : -1;
     if (d->medium != OWL_ELASTIC_VHTIORT_2D) return owl_ssg_nparam(d->medium);
     switch (d->aniso) {
         case OWL_ANISO_ISO: return 3;
@@ -109,6 +111,7 @@ int owl_ssg_create(const owl_ssg_desc* desc, owl_ssg** out) {
             case OWL_ACOUSTIC_ISO_2D: h->eng.reset(make_ac2d_engine(*desc)); break;
             case OWL_ACOUSTIC_ISO_3D: h->eng.reset(make_ac3d_engine(*desc)); break;
             case OWL_ELASTIC_VHTIORT_2D: h->eng.reset(make_el2d_engine(*desc)); break;
+            case OWL_ELASTIC_VHTIORT_3D: h->eng.reset(make_el3d_engine(*desc)); break;
             default: throw OwlError(OWL_ERR_UNSUPPORTED, "medium not built");
         }
         *out = h.release();

@@ -1,0 +1,789 @@
+// el3d.cu -- 3D elastic (isotropic / orthorhombic) SSG solver for B200 (sm_100a).
+//
+// Forward (replaces update_wavefield, add_source and the sampling of
+// compute_forward, src/solver/elastic_vhtiort_3d/module_wavefield.f90:52-537,
+// :1095-1333 and submodule_forward_modeling.f90:82-145) without a free surface,
+// and the exact discrete adjoint with every-k-step checkpoints, Kahan FP32
+// correlations for the nine Cij and the three buoyancies, and the FP64 chain
+// rule to the model parameters (replaces compute_adjoint / compute_gradient,
+// submodule_fwi_gradient.f90).
+//
+// Nodes (storage index = reference index + pml + R - 1 on each axis):
+// normal stresses at (i, j, k); syz at (i, j-1/2, k-1/2); sxz at (i-1/2, j,
+// k-1/2); sxy at (i-1/2, j-1/2, k); vx at (i-1/2, j, k); vy at (i, j-1/2, k);
+// vz at (i, j, k-1/2). State per shot: 9 fields + 18 CFS-MPML memory volumes.
+//
+// Damping. The reference damps a derivative along axis a of a node in the PML
+// shell with d = d_a(pos_a) + sum of ratio * d_b(pos_b) over the other axes
+// (module_wavefield.f90:104-145). With the M-PML ratios at zero -- the
+// reference's value for isotropic media, and what this solver uses for every
+// parameterisation -- (a, b) of a derivative depend only on the node's position
+// along that axis, so they are 1D tables per axis (integer and half
+// positions); a memory whose a is 0 stays exactly 0 and is not touched.
+//
+// One step = two stencil launches (stresses, velocities) + the point kernel;
+// the adjoint of a step = velocity-node kernel, source adjoint (optional),
+// stress-node kernel, residual injection (the e-array scheme of the 2D solvers:
+// each node stores the adjoint PML terms of its own derivatives).
+#include <algorithm>
+#include <cmath>
+
+#include "ssg_base.cuh"
+
+namespace owl {
+
+__constant__ float c_fd3e[8];
+
+enum { E3_XX = 0, E3_YY, E3_ZZ, E3_YZ, E3_XZ, E3_XY, E3_VX, E3_VY, E3_VZ, E3_M0 };
+// memories (and adjoint PML terms) in the order of the forward derivatives
+enum { N_XVX = 0, N_YVY, N_ZVZ, N_ZVY, N_YVZ, N_ZVX, N_XVZ, N_YVX, N_XVY, N_XXX, N_YXY, N_ZXZ, N_XXY, N_YYY, N_ZYZ,
+       N_XXZ, N_YYZ, N_ZZZ };
+constexpr int E3_NST = 9 + 18;
+constexpr int E3_NAD = 9 + 18 + 18;
+
+struct El3dDev {
+    int nx, ny, nz, P, R, pr, pitch;
+    long long plane, fs, sst, sad;
+    int x0, x1, y0, y1, z0, z1, nzb;
+    float idx, idy, idz, dt;
+    int nshots, spt;
+    const float *c11, *c12, *c13, *c22, *c23, *c33, *c44e, *c55e, *c66e, *bx, *by, *bz;
+    // per axis: a and b at integer and half positions (storage index)
+    const float *axi, *bxi, *axh, *bxh, *ayi, *byi, *ayh, *byh, *azi, *bzi, *azh, *bzh;
+    float* st;
+    float* S;
+    long long sslot, sterm;
+    int k;
+    int* d_step;
+    float* ad;
+    float* G;  // [12][group][fs] sums then [12][group][fs] compensations
+    long long gg;
+};
+
+__device__ __forceinline__ bool e3_out(int v, int pr, int n, bool half) {
+    return half ? (v <= pr || v >= pr + n) : (v < pr || v >= pr + n);
+}
+
+template <int R>
+__device__ __forceinline__ float stP(const float* f, long long s) {
+    float a = 0.f;
+#pragma unroll
+    for (int q = 1; q <= R; ++q) a = a + c_fd3e[q - 1] * (__ldg(f + q * s) - __ldg(f + (1 - q) * s));
+    return a;
+}
+template <int R>
+__device__ __forceinline__ float stM(const float* f, long long s) {
+    float a = 0.f;
+#pragma unroll
+    for (int q = 1; q <= R; ++q) a = a + c_fd3e[q - 1] * (__ldg(f + (q - 1) * s) - __ldg(f - q * s));
+    return a;
+}
+// transposes of P and M, read at the node
+template <int R>
+__device__ __forceinline__ float tP(const float* e, long long s) {
+    float a = 0.f;
+#pragma unroll
+    for (int q = 1; q <= R; ++q) a = a + c_fd3e[q - 1] * (__ldg(e - q * s) - __ldg(e + (q - 1) * s));
+    return a;
+}
+template <int R>
+__device__ __forceinline__ float tM(const float* e, long long s) {
+    float a = 0.f;
+#pragma unroll
+    for (int q = 1; q <= R; ++q) a = a + c_fd3e[q - 1] * (__ldg(e + (1 - q) * s) - __ldg(e + q * s));
+    return a;
+}
+
+__device__ __forceinline__ float pml_fw(float D, float a, float b, float* psi) {
+    const float m = a * D + b * *psi;
+    *psi = m;
+    return D + m;
+}
+__device__ __forceinline__ float pml_ad(float q, float a, float b, float* psih) {
+    const float u = q + *psih;
+    *psih = b * u;
+    return q + a * u;
+}
+
+struct E3Cell {
+    int x, y, z, grp;
+    long long o;
+};
+__device__ __forceinline__ bool e3_cell(const El3dDev& a, E3Cell& c) {
+    const int zb = blockIdx.z % a.nzb;
+    c.grp = blockIdx.z / a.nzb;
+    c.x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
+    c.y = a.y0 + blockIdx.y * blockDim.y + threadIdx.y;
+    c.z = a.z0 + zb * blockDim.z + threadIdx.z;
+    c.o = (long long)c.z * a.plane + (long long)c.y * a.pitch + c.x;
+    return c.x < a.x1 && c.y < a.y1 && c.z < a.z1;
+}
+
+// ------------------------------- forward ------------------------------------
+template <int R, bool STORE>
+__global__ void __launch_bounds__(256) k_el3d_fwd_s(El3dDev a) {
+    E3Cell c;
+    if (!e3_cell(a, c)) return;
+    const long long o = c.o, sy = a.pitch, sz = a.plane;
+    const int x = c.x, y = c.y, z = c.z;
+    // PML shell of each node type and the 1D coefficients it needs
+    const bool oxi = e3_out(x, a.pr, a.nx, false), oxh = e3_out(x, a.pr, a.nx, true);
+    const bool oyi = e3_out(y, a.pr, a.ny, false), oyh = e3_out(y, a.pr, a.ny, true);
+    const bool ozi = e3_out(z, a.pr, a.nz, false), ozh = e3_out(z, a.pr, a.nz, true);
+    const bool sh_n = oxi || oyi || ozi, sh_yz = oxi || oyh || ozh, sh_xz = oxh || oyi || ozh, sh_xy = oxh || oyh || ozi;
+    const float axi = a.axi[x], bxi = a.bxi[x], axh = a.axh[x], bxh = a.bxh[x];
+    const float ayi = a.ayi[y], byi = a.byi[y], ayh = a.ayh[y], byh = a.byh[y];
+    const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
+    const float c11 = __ldg(a.c11 + o), c12 = __ldg(a.c12 + o), c13 = __ldg(a.c13 + o), c22 = __ldg(a.c22 + o),
+                c23 = __ldg(a.c23 + o), c33 = __ldg(a.c33 + o);
+    const float g44 = a.dt * __ldg(a.c44e + o), g55 = a.dt * __ldg(a.c55e + o), g66 = a.dt * __ldg(a.c66e + o);
+    const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
+    const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
+    for (int s = s0; s < s1; ++s) {
+        float* st = a.st + s * a.sst;
+        const float* vx = st + E3_VX * a.fs + o;
+        const float* vy = st + E3_VY * a.fs + o;
+        const float* vz = st + E3_VZ * a.fs + o;
+        float* m = st + E3_M0 * a.fs + o;
+        float dX = a.idx * stP<R>(vx, 1), dY = a.idy * stP<R>(vy, sy), dZ = a.idz * stP<R>(vz, sz);
+        if (sh_n) {
+            if (axi != 0.f) dX = pml_fw(dX, axi, bxi, m + N_XVX * a.fs);
+            if (ayi != 0.f) dY = pml_fw(dY, ayi, byi, m + N_YVY * a.fs);
+            if (azi != 0.f) dZ = pml_fw(dZ, azi, bzi, m + N_ZVZ * a.fs);
+        }
+        st[E3_XX * a.fs + o] += a.dt * (c11 * dX + c12 * dY + c13 * dZ);
+        st[E3_YY * a.fs + o] += a.dt * (c12 * dX + c22 * dY + c23 * dZ);
+        st[E3_ZZ * a.fs + o] += a.dt * (c13 * dX + c23 * dY + c33 * dZ);
+        // syz: dz vy + dy vz
+        float dzvy = a.idz * stM<R>(vy, sz), dyvz = a.idy * stM<R>(vz, sy);
+        if (sh_yz) {
+            if (ayh != 0.f) dyvz = pml_fw(dyvz, ayh, byh, m + N_YVZ * a.fs);
+            if (azh != 0.f) dzvy = pml_fw(dzvy, azh, bzh, m + N_ZVY * a.fs);
+        }
+        st[E3_YZ * a.fs + o] += g44 * (dzvy + dyvz);
+        // sxz: dz vx + dx vz
+        float dzvx = a.idz * stM<R>(vx, sz), dxvz = a.idx * stM<R>(vz, 1);
+        if (sh_xz) {
+            if (axh != 0.f) dxvz = pml_fw(dxvz, axh, bxh, m + N_XVZ * a.fs);
+            if (azh != 0.f) dzvx = pml_fw(dzvx, azh, bzh, m + N_ZVX * a.fs);
+        }
+        st[E3_XZ * a.fs + o] += g55 * (dzvx + dxvz);
+        // sxy: dy vx + dx vy
+        float dyvx = a.idy * stM<R>(vx, sy), dxvy = a.idx * stM<R>(vy, 1);
+        if (sh_xy) {
+            if (axh != 0.f) dxvy = pml_fw(dxvy, axh, bxh, m + N_XVY * a.fs);
+            if (ayh != 0.f) dyvx = pml_fw(dyvx, ayh, byh, m + N_YVX * a.fs);
+        }
+        st[E3_XY * a.fs + o] += g66 * (dyvx + dxvy);
+        if (STORE) {
+            float* S = a.S + slot + s * a.fs + o;
+            S[0] = dX; S[a.sterm] = dY; S[2 * a.sterm] = dZ;
+            S[3 * a.sterm] = dzvy + dyvz; S[4 * a.sterm] = dzvx + dxvz; S[5 * a.sterm] = dyvx + dxvy;
+        }
+    }
+}
+
+template <int R, bool STORE>
+__global__ void __launch_bounds__(256) k_el3d_fwd_v(El3dDev a) {
+    E3Cell c;
+    if (!e3_cell(a, c)) return;
+    const long long o = c.o, sy = a.pitch, sz = a.plane;
+    const int x = c.x, y = c.y, z = c.z;
+    const bool oxi = e3_out(x, a.pr, a.nx, false), oxh = e3_out(x, a.pr, a.nx, true);
+    const bool oyi = e3_out(y, a.pr, a.ny, false), oyh = e3_out(y, a.pr, a.ny, true);
+    const bool ozi = e3_out(z, a.pr, a.nz, false), ozh = e3_out(z, a.pr, a.nz, true);
+    const bool sh_vx = oxh || oyi || ozi, sh_vy = oxi || oyh || ozi, sh_vz = oxi || oyi || ozh;
+    const float axi = a.axi[x], bxi = a.bxi[x], axh = a.axh[x], bxh = a.bxh[x];
+    const float ayi = a.ayi[y], byi = a.byi[y], ayh = a.ayh[y], byh = a.byh[y];
+    const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
+    const float bx = __ldg(a.bx + o), by = __ldg(a.by + o), bz = __ldg(a.bz + o);
+    const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
+    const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
+    for (int s = s0; s < s1; ++s) {
+        float* st = a.st + s * a.sst;
+        const float* sxx = st + E3_XX * a.fs + o;
+        const float* syy = st + E3_YY * a.fs + o;
+        const float* szz = st + E3_ZZ * a.fs + o;
+        const float* syz = st + E3_YZ * a.fs + o;
+        const float* sxz = st + E3_XZ * a.fs + o;
+        const float* sxy = st + E3_XY * a.fs + o;
+        float* m = st + E3_M0 * a.fs + o;
+        // vx: dx sxx (M) + dy sxy (P) + dz sxz (P)
+        float h1 = a.idx * stM<R>(sxx, 1), h2 = a.idy * stP<R>(sxy, sy), h3 = a.idz * stP<R>(sxz, sz);
+        if (sh_vx) {
+            if (axh != 0.f) h1 = pml_fw(h1, axh, bxh, m + N_XXX * a.fs);
+            if (ayi != 0.f) h2 = pml_fw(h2, ayi, byi, m + N_YXY * a.fs);
+            if (azi != 0.f) h3 = pml_fw(h3, azi, bzi, m + N_ZXZ * a.fs);
+        }
+        const float hx = h1 + h2 + h3;
+        st[E3_VX * a.fs + o] += bx * hx;
+        // vy: dx sxy (P) + dy syy (M) + dz syz (P)
+        h1 = a.idx * stP<R>(sxy, 1); h2 = a.idy * stM<R>(syy, sy); h3 = a.idz * stP<R>(syz, sz);
+        if (sh_vy) {
+            if (axi != 0.f) h1 = pml_fw(h1, axi, bxi, m + N_XXY * a.fs);
+            if (ayh != 0.f) h2 = pml_fw(h2, ayh, byh, m + N_YYY * a.fs);
+            if (azi != 0.f) h3 = pml_fw(h3, azi, bzi, m + N_ZYZ * a.fs);
+        }
+        const float hy = h1 + h2 + h3;
+        st[E3_VY * a.fs + o] += by * hy;
+        // vz: dx sxz (P) + dy syz (P) + dz szz (M)
+        h1 = a.idx * stP<R>(sxz, 1); h2 = a.idy * stP<R>(syz, sy); h3 = a.idz * stM<R>(szz, sz);
+        if (sh_vz) {
+            if (axi != 0.f) h1 = pml_fw(h1, axi, bxi, m + N_XXZ * a.fs);
+            if (ayi != 0.f) h2 = pml_fw(h2, ayi, byi, m + N_YYZ * a.fs);
+            if (azh != 0.f) h3 = pml_fw(h3, azh, bzh, m + N_ZZZ * a.fs);
+        }
+        const float hz = h1 + h2 + h3;
+        st[E3_VZ * a.fs + o] += bz * hz;
+        if (STORE) {
+            float* S = a.S + slot + s * a.fs + o;
+            S[6 * a.sterm] = hx; S[7 * a.sterm] = hy; S[8 * a.sterm] = hz;
+        }
+    }
+}
+
+// ------------------------------- adjoint ------------------------------------
+// adjoint planes per shot: 0..8 fields, 9..26 memory adjoints, 27..44 e terms
+__device__ __forceinline__ void e3_kahan(float* G, long long gg, long long go, int q, float v) {
+    float sm = G[q * gg + go], c = G[(12 + q) * gg + go];
+    kahan_add(sm, c, v);
+    G[q * gg + go] = sm;
+    G[(12 + q) * gg + go] = c;
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) k_el3d_adj_v(El3dDev a) {
+    E3Cell c;
+    if (!e3_cell(a, c)) return;
+    const long long o = c.o, sy = a.pitch, sz = a.plane;
+    const int x = c.x, y = c.y, z = c.z;
+    const int t = *a.d_step;
+    const long long slot = (long long)((t - 1) % a.k) * a.sslot;
+    const bool oxi = e3_out(x, a.pr, a.nx, false), oxh = e3_out(x, a.pr, a.nx, true);
+    const bool oyi = e3_out(y, a.pr, a.ny, false), oyh = e3_out(y, a.pr, a.ny, true);
+    const bool ozi = e3_out(z, a.pr, a.nz, false), ozh = e3_out(z, a.pr, a.nz, true);
+    const bool sh_vx = oxh || oyi || ozi, sh_vy = oxi || oyh || ozi, sh_vz = oxi || oyi || ozh;
+    const float axi = a.axi[x], bxi = a.bxi[x], axh = a.axh[x], bxh = a.bxh[x];
+    const float ayi = a.ayi[y], byi = a.byi[y], ayh = a.ayh[y], byh = a.byh[y];
+    const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
+    const float bx = __ldg(a.bx + o), by = __ldg(a.by + o), bz = __ldg(a.bz + o);
+    const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
+    float gx = 0.f, gy = 0.f, gz = 0.f;
+    for (int s = s0; s < s1; ++s) {
+        float* ad = a.ad + s * a.sad;
+        const float* e = ad + 27 * a.fs + o;
+        float* mh = ad + 9 * a.fs + o;
+        float* ew = ad + 27 * a.fs + o;
+        const long long so = slot + s * a.fs + o;
+        // vx^ += Dx^T e_xvx (P) + Dz^T e_zvx (M) + Dy^T e_yvx (M)
+        float v = ad[E3_VX * a.fs + o] + a.idx * tP<R>(e + N_XVX * a.fs, 1) + a.idz * tM<R>(e + N_ZVX * a.fs, sz) +
+                  a.idy * tM<R>(e + N_YVX * a.fs, sy);
+        ad[E3_VX * a.fs + o] = v;
+        gx += v * __ldg(a.S + 6 * a.sterm + so);
+        float q = bx * v, e1 = q, e2 = q, e3 = q;
+        if (sh_vx) {
+            if (axh != 0.f) e1 = pml_ad(q, axh, bxh, mh + N_XXX * a.fs);
+            if (ayi != 0.f) e2 = pml_ad(q, ayi, byi, mh + N_YXY * a.fs);
+            if (azi != 0.f) e3 = pml_ad(q, azi, bzi, mh + N_ZXZ * a.fs);
+        }
+        ew[N_XXX * a.fs] = e1; ew[N_YXY * a.fs] = e2; ew[N_ZXZ * a.fs] = e3;
+        // vy^ += Dy^T e_yvy (P) + Dz^T e_zvy (M) + Dx^T e_xvy (M)
+        v = ad[E3_VY * a.fs + o] + a.idy * tP<R>(e + N_YVY * a.fs, sy) + a.idz * tM<R>(e + N_ZVY * a.fs, sz) +
+            a.idx * tM<R>(e + N_XVY * a.fs, 1);
+        ad[E3_VY * a.fs + o] = v;
+        gy += v * __ldg(a.S + 7 * a.sterm + so);
+        q = by * v; e1 = q; e2 = q; e3 = q;
+        if (sh_vy) {
+            if (axi != 0.f) e1 = pml_ad(q, axi, bxi, mh + N_XXY * a.fs);
+            if (ayh != 0.f) e2 = pml_ad(q, ayh, byh, mh + N_YYY * a.fs);
+            if (azi != 0.f) e3 = pml_ad(q, azi, bzi, mh + N_ZYZ * a.fs);
+        }
+        ew[N_XXY * a.fs] = e1; ew[N_YYY * a.fs] = e2; ew[N_ZYZ * a.fs] = e3;
+        // vz^ += Dz^T e_zvz (P) + Dy^T e_yvz (M) + Dx^T e_xvz (M)
+        v = ad[E3_VZ * a.fs + o] + a.idz * tP<R>(e + N_ZVZ * a.fs, sz) + a.idy * tM<R>(e + N_YVZ * a.fs, sy) +
+            a.idx * tM<R>(e + N_XVZ * a.fs, 1);
+        ad[E3_VZ * a.fs + o] = v;
+        gz += v * __ldg(a.S + 8 * a.sterm + so);
+        q = bz * v; e1 = q; e2 = q; e3 = q;
+        if (sh_vz) {
+            if (axi != 0.f) e1 = pml_ad(q, axi, bxi, mh + N_XXZ * a.fs);
+            if (ayi != 0.f) e2 = pml_ad(q, ayi, byi, mh + N_YYZ * a.fs);
+            if (azh != 0.f) e3 = pml_ad(q, azh, bzh, mh + N_ZZZ * a.fs);
+        }
+        ew[N_XXZ * a.fs] = e1; ew[N_YYZ * a.fs] = e2; ew[N_ZZZ * a.fs] = e3;
+    }
+    const long long go = (long long)c.grp * a.fs + o;
+    e3_kahan(a.G, a.gg, go, 9, gx);
+    e3_kahan(a.G, a.gg, go, 10, gy);
+    e3_kahan(a.G, a.gg, go, 11, gz);
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
+    E3Cell c;
+    if (!e3_cell(a, c)) return;
+    const long long o = c.o, sy = a.pitch, sz = a.plane;
+    const int x = c.x, y = c.y, z = c.z;
+    const int t = *a.d_step;
+    const long long slot = (long long)((t - 1) % a.k) * a.sslot;
+    const bool oxi = e3_out(x, a.pr, a.nx, false), oxh = e3_out(x, a.pr, a.nx, true);
+    const bool oyi = e3_out(y, a.pr, a.ny, false), oyh = e3_out(y, a.pr, a.ny, true);
+    const bool ozi = e3_out(z, a.pr, a.nz, false), ozh = e3_out(z, a.pr, a.nz, true);
+    const bool sh_n = oxi || oyi || ozi, sh_yz = oxi || oyh || ozh, sh_xz = oxh || oyi || ozh, sh_xy = oxh || oyh || ozi;
+    const float axi = a.axi[x], bxi = a.bxi[x], axh = a.axh[x], bxh = a.bxh[x];
+    const float ayi = a.ayi[y], byi = a.byi[y], ayh = a.ayh[y], byh = a.byh[y];
+    const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
+    const float c11 = __ldg(a.c11 + o), c12 = __ldg(a.c12 + o), c13 = __ldg(a.c13 + o), c22 = __ldg(a.c22 + o),
+                c23 = __ldg(a.c23 + o), c33 = __ldg(a.c33 + o);
+    const float g44 = a.dt * __ldg(a.c44e + o), g55 = a.dt * __ldg(a.c55e + o), g66 = a.dt * __ldg(a.c66e + o);
+    const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
+    float G[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int s = s0; s < s1; ++s) {
+        float* ad = a.ad + s * a.sad;
+        const float* e = ad + 27 * a.fs + o;
+        float* ew = ad + 27 * a.fs + o;
+        float* mh = ad + 9 * a.fs + o;
+        const float* S = a.S + slot + s * a.fs + o;
+        const float xh = ad[E3_XX * a.fs + o] + a.idx * tM<R>(e + N_XXX * a.fs, 1);
+        const float yh = ad[E3_YY * a.fs + o] + a.idy * tM<R>(e + N_YYY * a.fs, sy);
+        const float zh = ad[E3_ZZ * a.fs + o] + a.idz * tM<R>(e + N_ZZZ * a.fs, sz);
+        const float yzh = ad[E3_YZ * a.fs + o] + a.idz * tP<R>(e + N_ZYZ * a.fs, sz) + a.idy * tP<R>(e + N_YYZ * a.fs, sy);
+        const float xzh = ad[E3_XZ * a.fs + o] + a.idz * tP<R>(e + N_ZXZ * a.fs, sz) + a.idx * tP<R>(e + N_XXZ * a.fs, 1);
+        const float xyh = ad[E3_XY * a.fs + o] + a.idy * tP<R>(e + N_YXY * a.fs, sy) + a.idx * tP<R>(e + N_XXY * a.fs, 1);
+        ad[E3_XX * a.fs + o] = xh; ad[E3_YY * a.fs + o] = yh; ad[E3_ZZ * a.fs + o] = zh;
+        ad[E3_YZ * a.fs + o] = yzh; ad[E3_XZ * a.fs + o] = xzh; ad[E3_XY * a.fs + o] = xyh;
+        const float dX = __ldg(S), dY = __ldg(S + a.sterm), dZ = __ldg(S + 2 * a.sterm);
+        G[0] += xh * dX;
+        G[1] += xh * dY + yh * dX;
+        G[2] += xh * dZ + zh * dX;
+        G[3] += yh * dY;
+        G[4] += yh * dZ + zh * dY;
+        G[5] += zh * dZ;
+        G[6] += yzh * __ldg(S + 3 * a.sterm);
+        G[7] += xzh * __ldg(S + 4 * a.sterm);
+        G[8] += xyh * __ldg(S + 5 * a.sterm);
+        float qx = a.dt * (c11 * xh + c12 * yh + c13 * zh);
+        float qy = a.dt * (c12 * xh + c22 * yh + c23 * zh);
+        float qz = a.dt * (c13 * xh + c23 * yh + c33 * zh);
+        if (sh_n) {
+            if (axi != 0.f) qx = pml_ad(qx, axi, bxi, mh + N_XVX * a.fs);
+            if (ayi != 0.f) qy = pml_ad(qy, ayi, byi, mh + N_YVY * a.fs);
+            if (azi != 0.f) qz = pml_ad(qz, azi, bzi, mh + N_ZVZ * a.fs);
+        }
+        ew[N_XVX * a.fs] = qx; ew[N_YVY * a.fs] = qy; ew[N_ZVZ * a.fs] = qz;
+        float q = g44 * yzh, e1 = q, e2 = q;
+        if (sh_yz) {
+            if (azh != 0.f) e1 = pml_ad(q, azh, bzh, mh + N_ZVY * a.fs);
+            if (ayh != 0.f) e2 = pml_ad(q, ayh, byh, mh + N_YVZ * a.fs);
+        }
+        ew[N_ZVY * a.fs] = e1; ew[N_YVZ * a.fs] = e2;
+        q = g55 * xzh; e1 = q; e2 = q;
+        if (sh_xz) {
+            if (azh != 0.f) e1 = pml_ad(q, azh, bzh, mh + N_ZVX * a.fs);
+            if (axh != 0.f) e2 = pml_ad(q, axh, bxh, mh + N_XVZ * a.fs);
+        }
+        ew[N_ZVX * a.fs] = e1; ew[N_XVZ * a.fs] = e2;
+        q = g66 * xyh; e1 = q; e2 = q;
+        if (sh_xy) {
+            if (ayh != 0.f) e1 = pml_ad(q, ayh, byh, mh + N_YVX * a.fs);
+            if (axh != 0.f) e2 = pml_ad(q, axh, bxh, mh + N_XVY * a.fs);
+        }
+        ew[N_YVX * a.fs] = e1; ew[N_XVY * a.fs] = e2;
+    }
+    const long long go = (long long)c.grp * a.fs + o;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) e3_kahan(a.G, a.gg, go, q, G[q]);
+}
+
+// FP64 chain rule on the padded model grid: d J / d (c11 c12 c13 c22 c23 c33 c44 c55 c66 rho),
+// then the parameters (iso: vp, vs, rho; cij: the nine moduli and rho)
+__global__ void k_el3d_chain(El3dDev a, int ngroups, int iso, const float* __restrict__ p0, const float* __restrict__ p1,
+                             const float* __restrict__ c44p, const float* __restrict__ c55p,
+                             const float* __restrict__ c66p, const float* __restrict__ rhop, double* __restrict__ gpad,
+                             int nxq, int nyq, int nzq) {
+    const long long n = (long long)nxq * nyq * nzq;
+    for (long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x; cell < n;
+         cell += (long long)gridDim.x * blockDim.x) {
+        const int ix = (int)(cell % nxq), iy = (int)((cell / nxq) % nyq), iz = (int)(cell / ((long long)nxq * nyq));
+        const int x = a.R - 1 + ix, y = a.R - 1 + iy, z = a.R - 1 + iz;
+        const long long o = (long long)z * a.plane + (long long)y * a.pitch + x;
+        auto sumG = [&](int q, long long oo) {
+            double v = 0;
+            for (int g = 0; g < ngroups; ++g)
+                v += (double)a.G[q * a.gg + g * a.fs + oo] - (double)a.G[(12 + q) * a.gg + g * a.fs + oo];
+            return v;
+        };
+        auto inside = [&](int xx, int yy, int zz) {
+            return xx >= a.x0 && xx < a.x1 && yy >= a.y0 && yy < a.y1 && zz >= a.z0 && zz < a.z1;
+        };
+        const double dt = a.dt;
+        double dc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (inside(x, y, z))
+            for (int q = 0; q < 6; ++q) dc[q] = dt * sumG(q, o);
+        const double cc[3] = {c44p[o], c55p[o], c66p[o]};
+        const float* ce[3] = {a.c44e, a.c55e, a.c66e};
+        for (int d1 = 0; d1 <= 1; ++d1)
+            for (int d2 = 0; d2 <= 1; ++d2) {
+                // syz nodes (x, y+d1, z+d2), sxz nodes (x+d1, y, z+d2), sxy nodes (x+d1, y+d2, z)
+                const int nx3[3] = {x, x + d1, x + d1}, ny3[3] = {y + d1, y, y + d2}, nz3[3] = {z + d2, z + d2, z};
+                for (int q = 0; q < 3; ++q) {
+                    if (!inside(nx3[q], ny3[q], nz3[q])) continue;
+                    const long long on = (long long)nz3[q] * a.plane + (long long)ny3[q] * a.pitch + nx3[q];
+                    const double e = ce[q][on];
+                    if (e != 0.0) dc[6 + q] += dt * sumG(6 + q, on) * e * e / (4.0 * cc[q] * cc[q]);
+                }
+            }
+        for (int d = 0; d <= 1; ++d) {
+            const long long sx = 1, sy = a.pitch, sz = a.plane;
+            const int px[3] = {x + d, x, x}, py[3] = {y, y + d, y}, pz[3] = {z, z, z + d};
+            const long long st[3] = {sx, sy, sz};
+            for (int q = 0; q < 3; ++q) {
+                if (!inside(px[q], py[q], pz[q])) continue;
+                const long long on = (long long)pz[q] * a.plane + (long long)py[q] * a.pitch + px[q];
+                const double re = 0.5 * ((double)rhop[on - st[q]] + (double)rhop[on]);
+                dc[9] -= 0.5 * dt * sumG(9 + q, on) / (re * re);
+            }
+        }
+        const long long npad = n;
+        if (iso) {
+            const double vp = p0[o], vs = p1[o], rho = rhop[o];
+            const double sn = dc[0] + dc[3] + dc[5], so = dc[1] + dc[2] + dc[4], ss = dc[6] + dc[7] + dc[8];
+            gpad[cell] += 2.0 * rho * vp * (sn + so);
+            gpad[npad + cell] += 2.0 * rho * vs * ss - 4.0 * rho * vs * so;
+            gpad[2 * npad + cell] += vp * vp * sn + (vp * vp - 2.0 * vs * vs) * so + vs * vs * ss + dc[9];
+        } else {
+            for (int q = 0; q < 10; ++q) gpad[q * npad + cell] += dc[q];
+        }
+    }
+}
+
+// ============================================================================
+// host engine
+// ============================================================================
+namespace {
+// per-axis damping tables (module_cfspml.f90:517-600 profiles, damp_coef macro of
+// module_wavefield.f90:40-43, kappa = 1, zero M-PML ratio)
+void e3_axis(int n, int pml, int R, int len, float d, float dt, float pmlvp, float alphamax, std::vector<float>& out) {
+    out.assign(4 * (size_t)len, 0.f);  // ai, bi, ah, bh
+    const float R0 = 1.0e-5f, adt = std::fabs(dt);
+    auto ab = [&](float dd, float al, float& a, float& b) {
+        const float bb = dd + al;
+        a = -2.0f * adt * dd / (2.0f + adt * bb);
+        b = (2.0f - adt * bb) / (2.0f + adt * bb);
+    };
+    for (int i = -pml + 1; i <= n + pml; ++i) {
+        float nd, ndh;
+        if (i <= 1) {
+            nd = (float)std::abs(i - 1) * 1.0f / (float)pml;
+            ndh = std::fabs((float)(i - 1) - 0.5f) * 1.0f / (float)pml;
+        } else if (i >= n) {
+            nd = (float)std::abs(i - n) * 1.0f / (float)pml;
+            ndh = std::fabs((float)(i - n) - 0.5f) * 1.0f / (float)pml;
+        } else {
+            continue;
+        }
+        const float c0 = std::log(1.0f / R0) * 3.0f * pmlvp / (2.0f * (float)pml * d);
+        const int x = i + pml + R - 1;
+        ab(c0 * (nd * nd), std::max(alphamax * (1.0f - nd), 0.25f * alphamax), out[x], out[len + x]);
+        ab(c0 * (ndh * ndh), std::max(alphamax * (1.0f - ndh), 0.25f * alphamax), out[2 * len + x], out[3 * len + x]);
+    }
+}
+}  // namespace
+
+struct El3dEngine : SsgBase {
+    int aniso;
+    float idx, idy, idz;
+    DevBuf<float> c11, c12, c13, c22, c23, c33, c44e, c55e, c66e, bxp, byp, bzp;
+    DevBuf<float> c44p, c55p, c66p, rhop, p0p, p1p, tabx, taby, tabz;
+
+    explicit El3dEngine(const owl_ssg_desc& d) : SsgBase(d, 3) {
+        aniso = d.aniso;
+        OWL_CHECK(aniso == OWL_ANISO_ISO || aniso == OWL_ANISO_CIJ, OWL_ERR_UNSUPPORTED,
+                  "elastic 3D takes the iso (vp, vs, rho) or cij (nine moduli, rho) parameterisation");
+        OWL_CHECK(!d.free_surface, OWL_ERR_UNSUPPORTED, "elastic 3D free surface not built");
+        idx = (float)(1.0 / (double)d.dx);
+        idy = (float)(1.0 / (double)d.dy);
+        idz = (float)(1.0 / (double)d.dz);
+        OWL_CUDA(cudaMemcpyToSymbol(c_fd3e, fd_coefs(R), sizeof(float) * R));
+        sst = E3_NST * fs;  // fs is a multiple of 32 floats (pitch rounded to 32)
+        sad = E3_NAD * fs;
+        nS = 9;
+        ngrad = 12;
+        nparam = aniso == OWL_ANISO_ISO ? 3 : 10;
+        ncomp = 3;
+        for (int f = 0; f < E3_NST; ++f) st_segments.push_back({f * fs, fs});
+    }
+
+    float* st_field(int f) const override { return f < 9 ? st.p + f * fs : nullptr; }
+    float* ad_field(int f) const override { return f < 9 ? ad.p + f * fs : nullptr; }
+    int rho_param() const override { return nparam - 1; }
+    std::vector<int> tune_spt(int) const override { return {1, 2, 4}; }
+    std::vector<int> tune_tz(int) const override { return {2}; }
+    void launch_params(const owl_run_opts&) override {
+        tile_x = 32;
+        tz_f = tz_a = 2;
+    }
+
+    void set_model(int np, const float* const* f) override {
+        OWL_CHECK(np == nparam && f, OWL_ERR_INVALID,
+                  "elastic 3D model needs " + std::to_string(nparam) + " parameters for this parameterisation");
+        for (int q = 0; q < np; ++q) OWL_CHECK(f[q], OWL_ERR_INVALID, "null model parameter");
+        std::vector<float> hc[10];
+        for (auto& v : hc) v.assign(fs, 0.f);
+        std::vector<float> hp0, hp1;
+        if (aniso == OWL_ANISO_ISO) { hp0.assign(fs, 0.f); hp1.assign(fs, 0.f); }
+        // Cij of the padded model (module_vars.f90:278-296, 362-375; padding by pml+1, :409-418)
+        for (int k = -P; k <= nz + P + 1; ++k)
+            for (int j = -P; j <= ny + P + 1; ++j)
+                for (int i = -P; i <= nx + P + 1; ++i) {
+                    const int ii = std::min(std::max(i, 1), nx), jj = std::min(std::max(j, 1), ny),
+                              kk = std::min(std::max(k, 1), nz);
+                    const size_t src = ((size_t)(ii - 1) * ny + (jj - 1)) * nz + (kk - 1);
+                    const long long o = soff(i, j, k);
+                    float v[10];
+                    if (aniso == OWL_ANISO_ISO) {
+                        const float vp = f[0][src], vs = f[1][src], rho = f[2][src];
+                        const float a11 = rho * (vp * vp), a44 = rho * (vs * vs), a12 = a11 - 2 * a44;
+                        const float w[10] = {a11, a12, a12, a11, a12, a11, a44, a44, a44, rho};
+                        std::copy(w, w + 10, v);
+                        hp0[o] = vp;
+                        hp1[o] = vs;
+                    } else {
+                        for (int q = 0; q < 10; ++q) v[q] = f[q][src];
+                    }
+                    for (int q = 0; q < 10; ++q) OWL_CHECK(std::isfinite(v[q]), OWL_ERR_INVALID, "non-finite model value");
+                    OWL_CHECK(v[9] > 0 && v[0] > 0 && v[3] > 0 && v[5] > 0 && v[6] > 0 && v[7] > 0 && v[8] > 0,
+                              OWL_ERR_INVALID, "rho, c11, c22, c33, c44, c55, c66 must be positive");
+                    for (int q = 0; q < 10; ++q) hc[q][o] = v[q];
+                }
+        // harmonic shear moduli and buoyancies (module_wavefield.f90:30-38)
+        std::vector<float> h44(fs, 0.f), h55(fs, 0.f), h66(fs, 0.f), hbx(fs, 0.f), hby(fs, 0.f), hbz(fs, 0.f);
+        const std::vector<float>& r = hc[9];
+        for (int k = -P + 1; k <= nz + P; ++k)
+            for (int j = -P + 1; j <= ny + P; ++j)
+                for (int i = -P + 1; i <= nx + P; ++i) {
+                    const long long o = soff(i, j, k);
+                    h44[o] = 4.0f / (1.0f / hc[6][soff(i, j - 1, k - 1)] + 1.0f / hc[6][soff(i, j, k - 1)] +
+                                     1.0f / hc[6][soff(i, j - 1, k)] + 1.0f / hc[6][o]);
+                    h55[o] = 4.0f / (1.0f / hc[7][soff(i - 1, j, k - 1)] + 1.0f / hc[7][soff(i, j, k - 1)] +
+                                     1.0f / hc[7][soff(i - 1, j, k)] + 1.0f / hc[7][o]);
+                    h66[o] = 4.0f / (1.0f / hc[8][soff(i - 1, j - 1, k)] + 1.0f / hc[8][soff(i, j - 1, k)] +
+                                     1.0f / hc[8][soff(i - 1, j, k)] + 1.0f / hc[8][o]);
+                    hbx[o] = dt / (0.5f * (r[soff(i - 1, j, k)] + r[o]));
+                    hby[o] = dt / (0.5f * (r[soff(i, j - 1, k)] + r[o]));
+                    hbz[o] = dt / (0.5f * (r[soff(i, j, k - 1)] + r[o]));
+                }
+        // pmlvp over the six faces (module_vars.f90:384-406) and dt_stable (:534-537)
+        float pv = -1e30f, maxv = 0.f;
+        for (int k = 1; k <= nz; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i) {
+                    const long long o = soff(i, j, k);
+                    const bool face = i == 1 || i == nx || j == 1 || j == ny || k == 1 || k == nz;
+                    for (int q : {0, 3, 5}) {
+                        const float w = hc[q][o] / r[o];
+                        if (face) pv = std::max(pv, w);
+                        maxv = std::max(maxv, std::sqrt(w));
+                    }
+                }
+        const float pmlvp = std::sqrt(pv);
+        const float* cf = fd_coefs(R);
+        float temp = 0.f;
+        for (int q = 0; q < R; ++q) temp += std::fabs(cf[q]);
+        dt_stable_ = 1.0f / (temp * maxv *
+                             std::sqrt(1.0f / (desc.dx * desc.dx) + 1.0f / (desc.dy * desc.dy) + 1.0f / (desc.dz * desc.dz)));
+        if (dt > dt_stable_ && !desc.allow_dt_adjust)
+            throw OwlError(OWL_ERR_UNSTABLE, "dt = " + std::to_string(dt) + " exceeds the stable dt " +
+                                                 std::to_string(dt_stable_));
+        const float alphamax = (float)(1.0 * (double)desc.f0_max * 3.14159265358979323846);
+        std::vector<float> tx, ty, tz;
+        e3_axis(nx, P, R, pitch, desc.dx, dt, pmlvp, alphamax, tx);
+        e3_axis(ny, P, R, NYs, desc.dy, dt, pmlvp, alphamax, ty);
+        e3_axis(nz, P, R, NZs, desc.dz, dt, pmlvp, alphamax, tz);
+        c11.upload(hc[0].data(), fs, stream); c12.upload(hc[1].data(), fs, stream); c13.upload(hc[2].data(), fs, stream);
+        c22.upload(hc[3].data(), fs, stream); c23.upload(hc[4].data(), fs, stream); c33.upload(hc[5].data(), fs, stream);
+        c44e.upload(h44.data(), fs, stream); c55e.upload(h55.data(), fs, stream); c66e.upload(h66.data(), fs, stream);
+        bxp.upload(hbx.data(), fs, stream); byp.upload(hby.data(), fs, stream); bzp.upload(hbz.data(), fs, stream);
+        c44p.upload(hc[6].data(), fs, stream); c55p.upload(hc[7].data(), fs, stream); c66p.upload(hc[8].data(), fs, stream);
+        rhop.upload(r.data(), fs, stream);
+        if (aniso == OWL_ANISO_ISO) { p0p.upload(hp0.data(), fs, stream); p1p.upload(hp1.data(), fs, stream); }
+        tabx.upload(tx.data(), tx.size(), stream);
+        taby.upload(ty.data(), ty.size(), stream);
+        tabz.upload(tz.data(), tz.size(), stream);
+        OWL_CUDA(cudaStreamSynchronize(stream));
+        h_rhop = hc[9];
+        model_set = true;
+        invalidate_graphs();
+    }
+
+    // ---- sources / receivers (module_wavefield.f90:1095-1333, submodule_forward_modeling.f90:82-145)
+    int src_ncomp(const owl_source& q) const override {
+        OWL_CHECK(q.mechanism == OWL_SRC_EXPLOSION || q.mechanism == OWL_SRC_FORCE || q.mechanism == OWL_SRC_MT,
+                  OWL_ERR_UNSUPPORTED, "unknown source mechanism");
+        return q.mechanism == OWL_SRC_FORCE ? 3 : 1;
+    }
+    void src_taps(const owl_source& q, int comp, std::vector<TapPt>& taps, long long& rc, float& rv) const override {
+        const float* ix = q.interp_ix; const float* iy = q.interp_iy; const float* iz = q.interp_iz;
+        const float* hx = q.interp_hx; const float* hy = q.interp_hy; const float* hz = q.interp_hz;
+        if (q.mechanism == OWL_SRC_FORCE) {
+            OWL_CHECK(in_wavefield(q.gx, q.gy, q.gz), OWL_ERR_INVALID, "force source outside the grid");
+            rv = h_rhop[soff(q.gx, q.gy, q.gz)];
+            rc = pad_index(q.gx, q.gy, q.gz);
+            const float w0 = comp == 0 ? std::sin(q.polar) * std::cos(q.azimuth)
+                           : comp == 1 ? std::sin(q.polar) * std::sin(q.azimuth) : std::cos(q.polar);
+            for (int irz = -4; irz <= 4; ++irz)
+                for (int iry = -4; iry <= 4; ++iry)
+                    for (int irx = -4; irx <= 4; ++irx) {
+                        const int a = irx + 4, b = iry + 4, c = irz + 4;
+                        if (comp == 0) taps.push_back(TapPt{E3_VX, q.hx + irx, q.gy + iry, q.gz + irz, w0 / rv * hx[a] * iy[b] * iz[c]});
+                        else if (comp == 1) taps.push_back(TapPt{E3_VY, q.gx + irx, q.hy + iry, q.gz + irz, w0 / rv * ix[a] * hy[b] * iz[c]});
+                        else taps.push_back(TapPt{E3_VZ, q.gx + irx, q.gy + iry, q.hz + irz, w0 / rv * ix[a] * iy[b] * hz[c]});
+                    }
+            return;
+        }
+        const bool mt = q.mechanism == OWL_SRC_MT;
+        const float inv = 1.0f / (desc.dx * desc.dy * desc.dz);
+        for (int irz = -4; irz <= 4; ++irz)
+            for (int iry = -4; iry <= 4; ++iry)
+                for (int irx = -4; irx <= 4; ++irx) {
+                    const int a = irx + 4, b = iry + 4, c = irz + 4;
+                    const float w = ix[a] * iy[b] * iz[c];
+                    taps.push_back(TapPt{E3_XX, q.gx + irx, q.gy + iry, q.gz + irz, -inv * (mt ? q.mt[0] : 1.f) * w});
+                    taps.push_back(TapPt{E3_YY, q.gx + irx, q.gy + iry, q.gz + irz, -inv * (mt ? q.mt[1] : 1.f) * w});
+                    taps.push_back(TapPt{E3_ZZ, q.gx + irx, q.gy + iry, q.gz + irz, -inv * (mt ? q.mt[2] : 1.f) * w});
+                    if (mt) {
+                        taps.push_back(TapPt{E3_XY, q.hx + irx, q.hy + iry, q.gz + irz, -inv * q.mt[3] * hx[a] * hy[b] * iz[c]});
+                        taps.push_back(TapPt{E3_XZ, q.hx + irx, q.gy + iry, q.hz + irz, -inv * q.mt[4] * hx[a] * iy[b] * hz[c]});
+                        taps.push_back(TapPt{E3_YZ, q.gx + irx, q.hy + iry, q.hz + irz, -inv * q.mt[5] * ix[a] * hy[b] * hz[c]});
+                    }
+                }
+    }
+    void rec_taps(const owl_receiver& q, int comp, std::vector<TapPt>& taps) const override {
+        for (int irz = -4; irz <= 4; ++irz)
+            for (int iry = -4; iry <= 4; ++iry)
+                for (int irx = -4; irx <= 4; ++irx) {
+                    const int a = irx + 4, b = iry + 4, c = irz + 4;
+                    if (comp == 0)
+                        taps.push_back(TapPt{E3_VX, q.hx + irx, q.gy + iry, q.gz + irz,
+                                             q.interp_hx[a] * q.interp_iy[b] * q.interp_iz[c] * q.weight});
+                    else if (comp == 1)
+                        taps.push_back(TapPt{E3_VY, q.gx + irx, q.hy + iry, q.gz + irz,
+                                             q.interp_ix[a] * q.interp_hy[b] * q.interp_iz[c] * q.weight});
+                    else
+                        taps.push_back(TapPt{E3_VZ, q.gx + irx, q.gy + iry, q.hz + irz,
+                                             q.interp_ix[a] * q.interp_iy[b] * q.interp_hz[c] * q.weight});
+                }
+    }
+
+    El3dDev dev(int S) const {
+        El3dDev a{};
+        a.nx = nx; a.ny = ny; a.nz = nz; a.P = P; a.R = R; a.pr = pr; a.pitch = pitch;
+        a.plane = plane; a.fs = fs; a.sst = sst; a.sad = sad;
+        a.x0 = R; a.x1 = R + NXp; a.y0 = R; a.y1 = R + NYp; a.z0 = R; a.z1 = R + NZp;
+        a.nzb = (NZp + 1) / 2;
+        a.idx = idx; a.idy = idy; a.idz = idz; a.dt = dt;
+        a.nshots = S;
+        a.c11 = c11.p; a.c12 = c12.p; a.c13 = c13.p; a.c22 = c22.p; a.c23 = c23.p; a.c33 = c33.p;
+        a.c44e = c44e.p; a.c55e = c55e.p; a.c66e = c66e.p; a.bx = bxp.p; a.by = byp.p; a.bz = bzp.p;
+        a.axi = tabx.p; a.bxi = tabx.p + pitch; a.axh = tabx.p + 2 * pitch; a.bxh = tabx.p + 3 * pitch;
+        a.ayi = taby.p; a.byi = taby.p + NYs; a.ayh = taby.p + 2 * NYs; a.byh = taby.p + 3 * NYs;
+        a.azi = tabz.p; a.bzi = tabz.p + NZs; a.azh = tabz.p + 2 * NZs; a.bzh = tabz.p + 3 * NZs;
+        a.st = st.p;
+        a.k = std::max(1, cur_k);
+        a.d_step = ctr.p;
+        const long long F = (long long)S * fs;
+        if (Sbuf.p && Sbuf.n >= (size_t)nS * a.k * F) {
+            a.S = Sbuf.p;
+            a.sslot = F;
+            a.sterm = (long long)a.k * F;
+        }
+        if (ad.p && ad.n >= (size_t)sad * S) a.ad = ad.p;
+        if (G.p) {
+            a.G = G.p;
+            a.gg = (long long)((S + spt_a - 1) / spt_a) * fs;
+        }
+        return a;
+    }
+
+    template <int RR>
+    void launch_r(int id, int S, bool store) {
+        El3dDev a = dev(S);
+        const bool fwd = id == OWL_K_FWD_P || id == OWL_K_FWD_V;
+        a.spt = fwd ? spt_f : spt_a;
+        const int groups = (S + a.spt - 1) / a.spt;
+        OWL_CHECK((long long)a.nzb * groups < 65536, OWL_ERR_UNSUPPORTED, "too many z blocks x shot groups");
+        const dim3 b(32, 4, 2), g((NXp + 31) / 32, (NYp + 3) / 4, a.nzb * groups);
+        if (fwd) {
+            OWL_CHECK(!store || a.S, OWL_ERR_INVALID, "stencil-term buffer not allocated");
+            if (id == OWL_K_FWD_P) {
+                if (store) k_el3d_fwd_s<RR, true><<<g, b, 0, stream>>>(a);
+                else k_el3d_fwd_s<RR, false><<<g, b, 0, stream>>>(a);
+            } else {
+                if (store) k_el3d_fwd_v<RR, true><<<g, b, 0, stream>>>(a);
+                else k_el3d_fwd_v<RR, false><<<g, b, 0, stream>>>(a);
+            }
+        } else {
+            OWL_CHECK(a.ad && a.S && a.G, OWL_ERR_INVALID, "adjoint buffers not allocated");
+            if (id == OWL_K_ADJ_P) k_el3d_adj_v<RR><<<g, b, 0, stream>>>(a);
+            else k_el3d_adj_s<RR><<<g, b, 0, stream>>>(a);
+        }
+    }
+    void launch_kernel(int id, int S, bool store) override {
+        if (R == 4) launch_r<4>(id, S, store);
+        else launch_r<8>(id, S, store);
+    }
+
+    // the adjoint of a step: velocity nodes, source adjoint (optional), stress
+    // nodes, then the residual of the sampling of step t
+    void launch_step(int kind, int S, const PointDev& q) override {
+        if (kind != 2) {
+            SsgBase::launch_step(kind, S, q);
+            return;
+        }
+        launch_kernel(OWL_K_ADJ_P, S, false);
+        launches++;
+        if (q.src_adj) {
+            launch_point_adj(q, S, 1, PA_SRC_NOW, stream);
+            launches++;
+        }
+        launch_kernel(OWL_K_ADJ_V, S, false);
+        launches++;
+        if (nb_sct <= 4) {
+            launch_point_adj(q, S, 1, PA_SCATTER | PA_TICK, stream);
+            launches++;
+        } else {
+            launch_point_adj(q, S, nb_sct, PA_SCATTER, stream);
+            launch_point_adj(q, S, 1, PA_TICK, stream);
+            launches += 2;
+        }
+    }
+
+    // compulsory bytes per launch (fields once per shot, materials once per
+    // launch, memories and e terms once, Kahan sums once per shot group);
+    // PML memory traffic is not counted (it is a fraction of the shell)
+    double alg_bytes(int id, int S, int groups) const override {
+        const double cells = (double)NXp * NYp * NZp;
+        switch (id) {
+            case OWL_K_FWD_P: return S * cells * (3 * 4.0 + 6 * 8.0) + cells * 9 * 4.0;
+            case OWL_K_FWD_V: return S * cells * (6 * 4.0 + 3 * 8.0) + cells * 3 * 4.0;
+            case OWL_K_ADJ_P: return S * cells * (9 * 4.0 + 3 * 8.0 + 9 * 4.0 + 3 * 4.0) + cells * 3 * 4.0 + groups * cells * 3 * 16.0;
+            case OWL_K_ADJ_V: return S * cells * (9 * 4.0 + 6 * 8.0 + 9 * 4.0 + 6 * 4.0) + cells * 9 * 4.0 + groups * cells * 9 * 16.0;
+        }
+        return 0;
+    }
+
+    void chain_rule(int S, int groups) override {
+        El3dDev a = dev(S);
+        const long long n = (long long)nxq() * nyq() * nzq();
+        const int nb = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+        const bool iso = aniso == OWL_ANISO_ISO;
+        k_el3d_chain<<<nb, 256, 0, stream>>>(a, groups, iso ? 1 : 0, iso ? p0p.p : nullptr, iso ? p1p.p : nullptr, c44p.p,
+                                             c55p.p, c66p.p, rhop.p, gpad.p, nxq(), nyq(), nzq());
+        OWL_LAUNCH_CHECK();
+        launches++;
+    }
+};
+
+Engine* make_el3d_engine(const owl_ssg_desc& d) { return new El3dEngine(d); }
+
+}  // namespace owl

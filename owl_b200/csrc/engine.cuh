@@ -25,6 +25,7 @@ struct Engine {
 Engine* make_ac2d_engine(const owl_ssg_desc& d);
 Engine* make_ac3d_engine(const owl_ssg_desc& d);
 Engine* make_el2d_engine(const owl_ssg_desc& d);
+Engine* make_el3d_engine(const owl_ssg_desc& d);
 
 // -------- shared device helpers (defined in shared.cu) ----------------------
 

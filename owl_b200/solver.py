@@ -126,7 +126,7 @@ class SSGSolver:
         differentiated (time_integration = -1) and, with a free surface, sources
         shallower than the first grid step move down to it with 1.2 x amplitude
         (src/solver/elastic_vhtiort_2d/module_vars.f90:466-477)."""
-        if self.desc.medium == L.OWL_ELASTIC_VHTIORT_2D:
+        if self.desc.medium in (L.OWL_ELASTIC_VHTIORT_2D, L.OWL_ELASTIC_VHTIORT_3D):
             shots = elastic_geometry(shots, self.desc)
             if time_integration is None:
                 time_integration = elastic_time_integration
