@@ -166,6 +166,58 @@ def elastic_2d_block(peak, peak_kind, ngrad=16):
     return out
 
 
+def elastic_3d_block(peak, peak_kind, nshots=4, nt=500):
+    """3D elastic orthorhombic (nine Cij) on the 256^3 model (296^3 padded cells),
+    `nshots` vertical-force shots and `nt` steps of the 2500-step workload:
+    forward Gcell-updates/s and the HBM roofline of the four stencil kernels
+    (after a gradient of one shot of a 96^3 model, 300 steps, which sets up the
+    adjoint state the adjoint kernels are timed on)."""
+    import numpy as np
+    from owl_b200 import _lib as L
+    from owl_b200 import configs
+    from owl_b200.solver import RunOpts, SSGSolver
+
+    d, f, shots = configs.config5(nshots, nt=nt)
+    s = SSGSolver(L.OWL_ELASTIC_VHTIORT_3D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
+                  f0_max=d.f0_max, max_shots=nshots, ny=d.ny, dy=d.dy, aniso=d.aniso)
+    s.set_model(*f)
+    ps = s.prepare(shots)
+    s.forward(ps, RunOpts())
+    s.forward(ps, RunOpts())
+    fms = s.last_info.elapsed_ms
+    cells = float(d.nx + 2 * d.pml) ** 3
+    out = {"workload": f"3D elastic ORT (nine Cij), 256^3 model (296^3 padded), dt 0.8 ms, {nt} of 2500 steps, "
+                       f"{nshots} of 16 vertical-force shots, 128 x 128 three-component receivers",
+           "forward_ms": fms, "forward_gcells_per_s": cells * nt * nshots / (fms / 1e3) / 1e9, "kernels": {}}
+    for kid, name in ((L.OWL_K_FWD_P, "k_el3d_fwd_s"), (L.OWL_K_FWD_V, "k_el3d_fwd_v")):
+        kms, b = s.kernel_time(kid, 10)
+        ach = b / (kms / 1e3) / 1e9
+        out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
+                                "shots_per_launch": nshots, "traffic": profile_traffic(name)}
+    s.close()
+    # gradient of one shot on a 96^3 model (the full model's checkpoints would not fit)
+    m = 96
+    dg, fg, shg = configs.config5(1, nt=300, n=m, nrec=32)
+    g = SSGSolver(L.OWL_ELASTIC_VHTIORT_3D, dg.nx, dg.nz, dg.dx, dg.dz, dg.dt, dg.nt, pml=dg.pml, fdhalf=dg.fdhalf,
+                  f0_max=dg.f0_max, max_shots=1, ny=dg.ny, dy=dg.dy, aniso=dg.aniso)
+    g.set_model(*fg)
+    pg = g.prepare(shg)
+    obs = np.zeros(g.seis_size(pg), dtype=np.float32)
+    g.gradient(pg, obs, opts=RunOpts(checkpoint_precision=L.OWL_CKPT_FP16))
+    g.gradient(pg, obs, opts=RunOpts(checkpoint_precision=L.OWL_CKPT_FP16))
+    out["gradient_workload"] = "96^3 model of the same kind (136^3 padded), 300 steps, 1 shot, FP16 checkpoints"
+    out["gradient_s_per_shot"] = g.last_info.elapsed_ms / 1e3
+    for kid, name in ((L.OWL_K_ADJ_P, "k_el3d_adj_v"), (L.OWL_K_ADJ_V, "k_el3d_adj_s")):
+        kms, b = g.kernel_time(kid, 10)
+        ach = b / (kms / 1e3) / 1e9
+        out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
+                                "shots_per_launch": 1, "model": "96^3", "traffic": profile_traffic(name)}
+    g.close()
+    return out
+
+
 # ----------------------------------------------------------------------------- clocks
 class Clocks:
     """nvidia-smi sampling during the timed region."""
@@ -454,6 +506,7 @@ def main():
         line["forward_3d"] = forward_3d_block(peak, peak_kind)
     if rank == 0 and not args.no_elastic:
         line["elastic_2d"] = elastic_2d_block(peak, peak_kind)
+        line["elastic_3d"] = elastic_3d_block(peak, peak_kind)
 
     if rank == 0:
         print(json.dumps(line), flush=True)

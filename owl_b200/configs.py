@@ -160,3 +160,53 @@ def config4(nshots=64, nt=4000):
     d = _desc(L.OWL_ELASTIC_VHTIORT_2D, nx, nz, dx, dt, nt, pml=20, fs=1, f0=15.0, max_shots=nshots)
     d.aniso = L.OWL_ANISO_THOMSEN
     return d, elastic_2d_vti_model(nz, nx, dx, eps_max=0.19), config4_shots(nshots, nx, dx)
+
+
+def _value_noise_linear(shape, cells_per_node, seed):
+    """Seeded noise in [-1, 1]: uniform values on a coarse lattice, trilinear
+    interpolation to the grid."""
+    from scipy.ndimage import zoom
+    rng = np.random.default_rng(seed)
+    coarse = [max(2, int(np.ceil(n / cells_per_node)) + 1) for n in shape]
+    c = rng.uniform(-1.0, 1.0, size=coarse).astype(np.float32)
+    f = zoom(c, [n / m for n, m in zip(shape, coarse)], order=1, mode="nearest")[: shape[0], : shape[1], : shape[2]]
+    f = f - f.mean()
+    return (f / max(1e-12, float(np.abs(f).max()))).astype(np.float32)
+
+
+def elastic_3d_ort_model(n=256, dx=10.0):
+    """Vp 2000 -> 5000 m/s linear in depth, Vs = Vp / 1.73, Gardner rho, and an
+    orthorhombic perturbation: c11, c22, c55, c66 scaled by (1 + a) with a in
+    [0, 0.15] smooth seeded fields (value noise, seed 11, ~300 m wavelength);
+    c12 = c13 = c23 = rho (vp^2 - 2 vs^2), c33 = rho vp^2, c44 = rho vs^2. The
+    fastest qP speed, vp sqrt(1.15) <= 5362 m/s, keeps dt = 0.8 ms inside the CFL
+    bound at dx = 10 m. Returns the ten (nz, ny, nx) fields c11 c12 c13 c22 c23
+    c33 c44 c55 c66 rho."""
+    z = np.arange(n, dtype=np.float64) * dx
+    vp = (2000.0 + 3000.0 * z / ((n - 1) * dx))[:, None, None] * np.ones((1, n, n))
+    vs = vp / 1.73
+    rho = 310.0 * vp ** 0.25
+    cells = max(2, int(round(300.0 / dx)))
+    fac = [0.075 * (1.0 + _value_noise_linear((n, n, n), cells, 11 + q)) for q in range(4)]
+    c33, c44 = rho * vp ** 2, rho * vs ** 2
+    c12 = rho * (vp ** 2 - 2 * vs ** 2)
+    f = [c33 * (1 + fac[0]), c12, c12, c33 * (1 + fac[1]), c12, c33, c44, c44 * (1 + fac[2]), c44 * (1 + fac[3]), rho]
+    return [np.asarray(x, dtype=np.float32) for x in f]
+
+
+def config5(nshots=16, nt=2500, n=256, nrec=128):
+    """3D elastic orthorhombic: n^3 (256^3), dx 10 m, dt 0.8 ms, PML 20, 8th order,
+    nine-Cij parameterisation; vertical-force 10 Hz shots on a line at 20 m depth;
+    nrec x nrec three-component receivers every 2 cells at 20 m depth."""
+    dx, dt = 10.0, 8e-4
+    d = _desc(L.OWL_ELASTIC_VHTIORT_3D, n, n, dx, dt, nt, pml=20, f0=10.0, max_shots=nshots, ny=n)
+    d.aniso = L.OWL_ANISO_CIJ
+    step = 2 * dx
+    nr = min(nrec, n // 2)
+    x0 = (n - 1) * dx / 2 - step * (nr - 1) / 2
+    recs = [Receiver(x=x0 + step * i, y=x0 + step * j, z=20.0) for j in range(nr) for i in range(nr)]
+    shots = []
+    for k in range(nshots):
+        xs = 200.0 + k * (((n - 1) * dx - 400.0) / max(1, nshots - 1))
+        shots.append(Shot(k + 1, [Source(x=xs, y=(n - 1) * dx / 2, z=20.0, mechanism="force", polar=0.0, f0=10.0)], recs))
+    return d, elastic_3d_ort_model(n, dx), shots
