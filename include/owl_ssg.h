@@ -217,6 +217,18 @@ int owl_ssg_source_gradient(owl_ssg *h, int nshots, const owl_shot *shots,
                             const float *adj, const owl_run_opts *opts,
                             float *stf_grad, int mem_kind, owl_run_info *info);
 
+/* Misfit-only batched forward: the trial forwards of the step-length search
+ * (compute_step_misfit / compute_step_coef, src/inverse/module_inversion_step_size.f90:263-592)
+ * with the waveform misfit (compute_adjsrc_waveform,
+ * src/inverse/module_inversion_adjoint_source.f90:371-383). No checkpoints.
+ *   obs: observed (or reference) seismograms, the layout of owl_ssg_forward.
+ *   misfit: nshots doubles, sum over traces of (obs - syn)^2 (may be NULL).
+ *   trace_misfit: one double per trace, in seismogram trace order (may be NULL).
+ *   seis_out: the synthetic seismograms (may be NULL). */
+int owl_ssg_misfit(owl_ssg *h, int nshots, const owl_shot *shots, const float *obs,
+                   const owl_run_opts *opts, double *misfit, double *trace_misfit,
+                   float *seis_out, int mem_kind, owl_run_info *info);
+
 void owl_ssg_destroy(owl_ssg *h);
 
 /* ---- diagnostics (no counterpart in the reference) ------------------------ */

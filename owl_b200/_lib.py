@@ -141,7 +141,7 @@ EXPORTED = [
     "owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
     "owl_ssg_source_gradient", "owl_ssg_destroy", "owl_last_error", "owl_ssg_abi_version",
     "owl_ssg_dt_stable", "owl_ssg_nparam", "owl_ssg_ncomp", "owl_ssg_device_ok", "owl_ssg_kernel_time",
-    "owl_ssg_forward_noalloc", "owl_ssg_desc_nparam",
+    "owl_ssg_forward_noalloc", "owl_ssg_desc_nparam", "owl_ssg_misfit",
 ]
 
 OWL_K_FWD_P = 0
@@ -186,9 +186,11 @@ def load() -> C.CDLL:
     lib.owl_ssg_dt_stable.argtypes = [C.c_void_p]
     lib.owl_ssg_dt_stable.restype = C.c_float
     lib.owl_ssg_desc_nparam.argtypes = [P(OwlSsgDesc)]
+    lib.owl_ssg_misfit.argtypes = [C.c_void_p, C.c_int, P(OwlShot), C.c_void_p, P(OwlRunOpts), C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_int, P(OwlRunInfo)]
     for fn in ("owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
                "owl_ssg_source_gradient", "owl_ssg_abi_version", "owl_ssg_nparam", "owl_ssg_ncomp",
-               "owl_ssg_device_ok", "owl_ssg_desc_nparam"):
+               "owl_ssg_device_ok", "owl_ssg_desc_nparam", "owl_ssg_misfit"):
         getattr(lib, fn).restype = C.c_int
     _lib = lib
     return lib

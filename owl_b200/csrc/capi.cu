@@ -161,6 +161,19 @@ int owl_ssg_source_gradient(owl_ssg* h, int nshots, const owl_shot* shots, const
     });
 }
 
+int owl_ssg_misfit(owl_ssg* h, int nshots, const owl_shot* shots, const float* obs, const owl_run_opts* opts,
+                   double* misfit, double* trace_misfit, float* seis_out, int mem_kind, owl_run_info* info) {
+    return guarded([&] {
+        OWL_CHECK(h && h->eng, OWL_ERR_INVALID, "null handle");
+        OWL_CHECK(nshots >= 0 && (nshots == 0 || shots), OWL_ERR_INVALID, "bad shots");
+        OWL_CHECK(obs || nshots == 0, OWL_ERR_INVALID, "null data buffer");
+        OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
+        owl_run_info tmp{};
+        h->eng->misfit(nshots, shots, obs, opts_or_default(opts), misfit, trace_misfit, seis_out, mem_kind,
+                       info ? *info : tmp);
+    });
+}
+
 int owl_ssg_kernel_time(owl_ssg* h, int kernel_id, int nlaunch, double* avg_ms, double* alg_bytes) {
     return guarded([&] {
         OWL_CHECK(h && h->eng && avg_ms && alg_bytes && nlaunch > 0, OWL_ERR_INVALID, "bad arguments");

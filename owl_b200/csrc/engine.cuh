@@ -18,6 +18,8 @@ struct Engine {
                           const owl_run_opts& o, double* misfit, float* grad, float* seis_out, int mem,
                           owl_run_info& info) = 0;
     virtual void kernel_time(int id, int nlaunch, double* avg_ms, double* alg_bytes) = 0;
+    virtual void misfit(int nshots, const owl_shot* shots, const float* obs, const owl_run_opts& o, double* misfit,
+                        double* trace_misfit, float* seis_out, int mem, owl_run_info& info) = 0;
     virtual void source_gradient(int nshots, const owl_shot* shots, const float* adj, const owl_run_opts& o,
                                  float* stf_grad, int mem, owl_run_info& info) = 0;
 };
@@ -62,6 +64,9 @@ void launch_residual_l2(const float* syn, const float* obs, float* res, const un
                         const int* shot_rec_ptr, int nshots, int nt, int rtot, double* misfit,
                         cudaStream_t s);
 void launch_check_finite(const float* f, size_t n, int* flag, cudaStream_t s);
+// per-trace FP64 L2 misfits (trace_misfit[rtot]) and their per-shot sums (misfit[nshots])
+void launch_trace_misfit(const float* syn, const float* obs, const unsigned char* live, const int* shot_rec_ptr,
+                         int nshots, int nt, int rtot, double* trace_misfit, double* misfit, cudaStream_t s);
 void launch_fill_f64(double* p, size_t n, double v, cudaStream_t s);
 
 }  // namespace owl

@@ -110,6 +110,44 @@ void launch_residual_l2(const float* syn, const float* obs, float* res, const un
     OWL_LAUNCH_CHECK();
 }
 
+// per-trace L2 misfit sum_t (obs - syn)^2 in FP64: one warp per trace, a fixed
+// lane / shuffle order (deterministic); traces of weight 0 give 0
+__global__ void k_trace_misfit(const float* __restrict__ syn, const float* __restrict__ obs,
+                               const unsigned char* __restrict__ live, int nt, int rtot, double* __restrict__ tm) {
+    const int r = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+    if (r >= rtot) return;
+    double acc = 0.0;
+    if (live[r])
+        for (int t = lane; t < nt; t += 32) {
+            const double d = (double)obs[(size_t)t * rtot + r] - (double)syn[(size_t)t * rtot + r];
+            acc += d * d;
+        }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) tm[r] = acc;
+}
+
+// per-shot sums of the trace misfits, in trace order
+__global__ void k_shot_misfit(const double* __restrict__ tm, const int* __restrict__ shot_rec_ptr, int nshots,
+                              double* __restrict__ misfit) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nshots) return;
+    double acc = 0.0;
+    for (int r = shot_rec_ptr[s]; r < shot_rec_ptr[s + 1]; ++r) acc += tm[r];
+    misfit[s] = acc;
+}
+
+void launch_trace_misfit(const float* syn, const float* obs, const unsigned char* live, const int* shot_rec_ptr,
+                         int nshots, int nt, int rtot, double* trace_misfit, double* misfit, cudaStream_t s) {
+    if (rtot > 0) {
+        k_trace_misfit<<<(rtot + 7) / 8, 256, 0, s>>>(syn, obs, live, nt, rtot, trace_misfit);
+        OWL_LAUNCH_CHECK();
+    }
+    if (nshots > 0) {
+        k_shot_misfit<<<(nshots + 127) / 128, 128, 0, s>>>(trace_misfit, shot_rec_ptr, nshots, misfit);
+        OWL_LAUNCH_CHECK();
+    }
+}
+
 __global__ void k_check_finite(const float* __restrict__ f, size_t n, int* flag) {
     bool bad = false;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)

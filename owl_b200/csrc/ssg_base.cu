@@ -599,6 +599,60 @@ void SsgBase::forward(int nshots, const owl_shot* shots, const owl_run_opts& o, 
     fill_info(info, nshots, batches, false);
 }
 
+// Misfit-only batched forward (the trial forwards of the step-length search,
+// src/inverse/module_inversion_step_size.f90:263-592): no checkpoints, no
+// seismogram round trip unless asked for.
+void SsgBase::misfit(int nshots, const owl_shot* shots, const float* obs, const owl_run_opts& o, double* misfit,
+                     double* trace_misfit, float* seis_out, int mem, owl_run_info& info) {
+    OWL_CHECK(model_set, OWL_ERR_INVALID, "set_model must be called first");
+    int B, k;
+    bool graph;
+    resolve_opts(o, nshots, B, k, graph);
+    launches = 0;
+    EventTimer tm(stream);
+    size_t data_off = 0, tr_off = 0;
+    int batches = 0, shot0 = 0;
+    for (int b0 = 0; b0 < nshots; b0 += B) {
+        const int S = std::min(B, nshots - b0);
+        build_tables(S, shots + b0, false);
+        ensure_state(S, k, false);
+        cur_S = S;
+        if (tune) autotune(S, k, false);
+        const size_t nrt = (size_t)desc.nt * std::max(rtot, 1);
+        rec.reserve(nrt);
+        obs_t.reserve(nrt);
+        OWL_CUDA(cudaMemsetAsync(rec.p, 0, sizeof(float) * nrt, stream));
+        forward_batch(S, k, graph, false);
+        if (o.check_every > 0) check_nonfinite(st.p, (size_t)S * sst);
+        const size_t n = (size_t)rtot * desc.nt;
+        misfit_d.reserve(S);
+        trace_d.reserve(std::max(rtot, 1));
+        if (n) {
+            seis_tmp.reserve(n);
+            OWL_CUDA(cudaMemcpyAsync(seis_tmp.p, obs + data_off, n * sizeof(float),
+                                     mem == OWL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+            launch_transpose_seis_to_rec(seis_tmp.p, obs_t.p, desc.nt, rtot, stream);
+            launches++;
+        }
+        launch_trace_misfit(rec.p, obs_t.p, live.p, rec_shot_ptr.p, S, desc.nt, rtot, trace_d.p, misfit_d.p, stream);
+        launches += 2;
+        if (misfit) copy_out(misfit + shot0, misfit_d.p, sizeof(double) * S, mem);
+        if (trace_misfit && rtot) copy_out(trace_misfit + tr_off, trace_d.p, sizeof(double) * rtot, mem);
+        if (seis_out && n) {
+            launch_transpose_rec_to_seis(rec.p, seis_tmp.p, desc.nt, rtot, stream);
+            launches++;
+            copy_out(seis_out + data_off, seis_tmp.p, n * sizeof(float), mem);
+        }
+        OWL_CUDA(cudaStreamSynchronize(stream));
+        data_off += n;
+        tr_off += (size_t)rtot;
+        shot0 += S;
+        batches++;
+    }
+    info.elapsed_ms = tm.stop_ms();
+    fill_info(info, nshots, batches, false);
+}
+
 void SsgBase::fold_out(float* grad, int mem) {
     const size_t nm = (size_t)nx * ny * nz;
     seis_tmp.reserve((size_t)nparam * nm);

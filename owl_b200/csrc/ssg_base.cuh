@@ -80,7 +80,7 @@ struct SsgBase : Engine {
     DevBuf<unsigned short> ckpt16;
     DevBuf<int> ctr;
     DevBuf<float> rec, res, obs_t, src_adj, seis_tmp, amp;
-    DevBuf<double> gpad, misfit_d, pt_val;
+    DevBuf<double> gpad, misfit_d, pt_val, trace_d;
     DevBuf<int> pt_idx;
     DevCSR inj, smp, sct;
     DevBuf<int> inj_shot_ptr, rec_shot_ptr, sct_shot_ptr;
@@ -171,6 +171,8 @@ struct SsgBase : Engine {
     void source_gradient(int nshots, const owl_shot* shots, const float* adj, const owl_run_opts& o, float* stf_grad,
                          int mem, owl_run_info& info) override;
     void kernel_time(int id, int nlaunch, double* avg_ms, double* alg_bytes) override;
+    void misfit(int nshots, const owl_shot* shots, const float* obs, const owl_run_opts& o, double* misfit,
+                double* trace_misfit, float* seis_out, int mem, owl_run_info& info) override;
     void gradient_impl(int nshots, const owl_shot* shots, const float* data, int adj_kind, const owl_run_opts& o,
                        double* misfit, float* grad, float* seis_out, float* stf_grad, int mem, owl_run_info& info);
 };

@@ -196,6 +196,20 @@ class SSGSolver:
                                                  L.OWL_MEM_HOST, C.byref(self.last_info)))
         return out
 
+    def misfit(self, ps: PreparedShots, obs, opts: Optional[RunOpts] = None, traces: bool = False,
+               seis_out=None):
+        """Misfit-only forward (step-length trial forwards): per-shot sum over traces of
+        (obs - syn)^2, and with traces=True also the per-trace misfits."""
+        opts = opts or RunOpts()
+        misfit = np.zeros(ps.nshots)
+        tm = np.zeros(sum(ps.nrec(s) for s in range(ps.nshots)) * self.ncomp) if traces else None
+        o = opts.c()
+        L.check(self.lib.owl_ssg_misfit(self.h, ps.nshots, ps.arr, _ptr(obs), C.byref(o), _ptr(misfit),
+                                        _ptr(tm) if tm is not None else None,
+                                        _ptr(seis_out) if seis_out is not None else None, L.OWL_MEM_HOST,
+                                        C.byref(self.last_info)))
+        return (misfit, tm) if traces else misfit
+
     def kernel_time(self, kernel_id: int, nlaunch: int = 20) -> Tuple[float, float]:
         """(mean ms per launch, algorithmic bytes per launch) of one kernel on the last batch state."""
         ms, b = C.c_double(), C.c_double()
