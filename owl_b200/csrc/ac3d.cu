@@ -696,12 +696,49 @@ struct Ac3dEngine : SsgBase {
         }
     }
 
+    // rows per thread of the forward kernels, tuned for each kernel on its own
+    // (the shared autotuner times the pair together); -1 = use tz_f
+    int tz_fp = -1, tz_fv = -1;
+    std::map<int, std::pair<int, int>> tz_split_cache;
+    void tune_extra(int S, int k, bool) override {
+        (void)k;
+        auto it = tz_split_cache.find(S);
+        if (it != tz_split_cache.end()) {
+            tz_fp = it->second.first;
+            tz_fv = it->second.second;
+            return;
+        }
+        int best[2] = {tz_f, tz_f};
+        for (int kid : {OWL_K_FWD_P, OWL_K_FWD_V}) {
+            float bms = 1e30f;
+            for (int tz : {0, 1, 2, 4}) {
+                (kid == OWL_K_FWD_P ? tz_fp : tz_fv) = tz;
+                launch_kernel(kid, S, false);
+                OWL_LAUNCH_CHECK();
+                EventTimer tm(stream);
+                for (int i = 0; i < 3; ++i) launch_kernel(kid, S, false);
+                const float ms = (float)tm.stop_ms();
+                launches += 4;
+                if (ms < bms) { bms = ms; best[kid] = tz; }
+            }
+        }
+        tz_fp = best[0];
+        tz_fv = best[1];
+        tz_split_cache[S] = {tz_fp, tz_fv};
+    }
+    void launch_params(const owl_run_opts& o) override {
+        SsgBase::launch_params(o);
+        tz_fp = tz_fv = -1;
+    }
+
     template <int RR>
     void launch_r(int id, int S, bool store) {
         if (id <= OWL_K_FWD_V) {
-            if (tz_f == 0) launch_naive<RR>(id, S, store);
-            else if (tz_f == 2) launch_fwd<RR, 2>(id, S, store);
-            else if (tz_f == 1) launch_fwd<RR, 1>(id, S, store);
+            const int sel = id == OWL_K_FWD_P ? tz_fp : tz_fv;
+            const int tz = sel >= 0 ? sel : tz_f;
+            if (tz == 0) launch_naive<RR>(id, S, store);
+            else if (tz == 2) launch_fwd<RR, 2>(id, S, store);
+            else if (tz == 1) launch_fwd<RR, 1>(id, S, store);
             else launch_fwd<RR, 4>(id, S, store);
         } else {
             if (tz_a == 2) launch_adj<RR, 2>(id, S);

@@ -455,6 +455,7 @@ void SsgBase::autotune(int S, int k, bool grad) {
     auto it = tune_cache.find(key);
     if (it != tune_cache.end()) {
         spt_f = it->second[0]; tz_f = it->second[1]; spt_a = it->second[2]; tz_a = it->second[3];
+        tune_extra(S, k, grad);
         return;
     }
     cur_k = k;
@@ -483,6 +484,7 @@ void SsgBase::autotune(int S, int k, bool grad) {
         if (pass == 0) { spt_f = bs; tz_f = bt; } else { spt_a = bs; tz_a = bt; }
     }
     tune_cache[key] = {spt_f, tz_f, spt_a, tz_a};
+    tune_extra(S, k, grad);
 }
 
 void SsgBase::save_ckpt(int slot, int S) {

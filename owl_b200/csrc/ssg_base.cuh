@@ -124,6 +124,8 @@ struct SsgBase : Engine {
     virtual std::vector<int> tune_tz(int pass) const;
     // tile_x / tile_z of the run options (validated), spt_f / spt_a already set
     virtual void launch_params(const owl_run_opts& o);
+    // medium-specific tuning after the shared autotuner (S shots per launch)
+    virtual void tune_extra(int S, int k, bool grad) { (void)S; (void)k; (void)grad; }
 
     // ---------------- helpers ----------------
     long long soff(int i, int j, int k) const {
