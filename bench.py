@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--no-elastic", action="store_true", help="skip the 2D elastic VTI block")
     p.add_argument("--profile-el", type=int, default=0, metavar="S",
                    help="profiling target: one 2D elastic VTI gradient of S shots, 60 steps, no JSON line")
+    p.add_argument("--profile-el3", type=int, default=0, metavar="N",
+                   help="profiling target: one 3D elastic ORT gradient of 1 shot on an N^3 model, 40 steps")
     return p.parse_args()
 
 
@@ -120,6 +122,24 @@ def profile_elastic(nshots):
     obs = np.zeros(s.seis_size(ps), dtype=np.float32)
     s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=20, shots_per_cta=1, tile_z=8, use_graph=-1))
     print(f"profile-el: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
+    s.close()
+
+
+def profile_elastic3(n):
+    """Small 3D elastic gradient for kernel captures: the ORT model on n^3, 1 shot, 40 steps."""
+    import numpy as np
+    from owl_b200 import _lib as L
+    from owl_b200 import configs
+    from owl_b200.solver import RunOpts, SSGSolver
+
+    d, f, shots = configs.config5(1, nt=40, n=n, nrec=16)
+    s = SSGSolver(L.OWL_ELASTIC_VHTIORT_3D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
+                  f0_max=d.f0_max, max_shots=1, ny=d.ny, dy=d.dy, aniso=d.aniso)
+    s.set_model(*f)
+    ps = s.prepare(shots)
+    obs = np.zeros(s.seis_size(ps), dtype=np.float32)
+    s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=20, shots_per_cta=1, tile_z=2, use_graph=-1))
+    print(f"profile-el3: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
     s.close()
 
 
@@ -347,6 +367,8 @@ def main():
         return profile_3d(args.profile3d)
     if args.profile_el:
         return profile_elastic(args.profile_el)
+    if args.profile_el3:
+        return profile_elastic3(args.profile_el3)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
