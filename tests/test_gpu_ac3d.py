@@ -61,3 +61,32 @@ def test_gradient_parity_3d(fs):
         mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, opts)
         assert rel(mf, mf_ref) < 1e-4
         assert rel(g, g_ref) < 1e-4, (opts, rel(g, g_ref))
+
+
+_REF3 = {}
+
+
+def _ref3_gradient():
+    """FP64 oracle gradient of the 3D case (one shot, vp 2 % high), computed once."""
+    if not _REF3:
+        d, vp, rho, ps = case3(0, nt=200)
+        ps = PreparedShots(ps.shots[:1], GridSpec(nx=d.nx, nz=d.nz, dx=d.dx, dz=d.dz, ny=d.ny, dy=d.dy), d.dt)
+        obs = oracle.ac3d_forward(d, vp, rho, ps, "f64").astype(np.float32)
+        vp0 = vp * np.float32(1.02)
+        _, g_ref = oracle.ac3d_gradient(d, vp0, rho, ps, obs, adj_kind=0, k=25)
+        _REF3.update(d=d, vp0=vp0, rho=rho, ps=ps, obs=obs, g=g_ref)
+    return _REF3
+
+
+@pytest.mark.parametrize("prec,tol", [(L.OWL_CKPT_FP32, 1e-4), (L.OWL_CKPT_FP16, 2e-3), (L.OWL_CKPT_BF16, 2e-2)])
+def test_gradient_checkpoint_precision_3d(prec, tol):
+    """3D forward + adjoint vp/rho gradient with FP32, FP16 and BF16 checkpoints
+    (per-field, per-shot scale for the 16-bit ones), each against the FP64
+    exact-adjoint oracle."""
+    r = _ref3_gradient()
+    s = solver3(r["d"], r["vp0"], r["rho"])
+    _, g = s.gradient(r["ps"], r["obs"], L.OWL_ADJ_L2_RESIDUAL,
+                      RunOpts(checkpoint_interval=25, checkpoint_precision=prec))
+    e = rel(g, r["g"])
+    print("3D checkpoint precision", prec, "gradient rel err vs FP64 oracle", e)
+    assert e < tol, e
