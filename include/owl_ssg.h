@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define OWL_SSG_ABI_VERSION 2
+#define OWL_SSG_ABI_VERSION 3
 
 /* status codes */
 #define OWL_OK 0
@@ -71,7 +71,10 @@ extern "C" {
 #define OWL_SRC_FORCE 1
 #define OWL_SRC_MT 2
 
-/* memory kinds of the data buffers passed to forward / gradient */
+/* memory kinds of the data buffers passed to forward / gradient. Device
+ * buffers must hold their final contents, and no other work may still be
+ * using them, when a call starts (synchronise the stream that produced them);
+ * every call returns after its own GPU work has finished. */
 #define OWL_MEM_HOST 0
 #define OWL_MEM_DEVICE 1
 
@@ -83,6 +86,35 @@ extern "C" {
 /* adjoint-source kinds for owl_ssg_gradient */
 #define OWL_ADJ_L2_RESIDUAL 0 /* adj = syn - obs, misfit = sum (obs - syn)^2 */
 #define OWL_ADJ_GIVEN 1       /* adj given directly (the reference's adjoint SU) */
+
+/* data-domain misfits (misfit_type, src/inverse/module_inversion_adjoint_source.f90:1099-1145) */
+#define OWL_MISFIT_WAVEFORM 0 /* compute_adjsrc_waveform :371-383 */
+#define OWL_MISFIT_CORR 1     /* compute_adjsrc_corr :391-412 (normalised zero-lag correlation) */
+#define OWL_MISFIT_ENVELOPE 2 /* compute_adjsrc_envelope :424-451 */
+#define OWL_MISFIT_PHASE 3    /* compute_adjsrc_phase :459-482 (instantaneous phase) */
+#define OWL_MISFIT_ADAPTIVE 4 /* compute_adjsrc_adaptive :490-537 (adaptive waveform inversion) */
+
+/* penalty of the adaptive misfit (xcorr_penalty :321-363) */
+#define OWL_PENALTY_LINEAR 0
+#define OWL_PENALTY_POWER 1
+#define OWL_PENALTY_GAUSSIAN 2
+#define OWL_PENALTY_EXP 3
+
+/* Misfit options: the reference's parameters of the same names
+ * (src/lib/module_parameters.f90:550-570). Zero-initialised fields take
+ * these defaults: tlag_max 0 -> 0.1 * (nt - 1) * dt, deconv_eps 0 -> 0.1,
+ * penalty_power 0 -> 1, discard_threshold 0 -> 1e-6 (a negative value turns
+ * the relative threshold off; traces of weight 0 or with a zero norm are
+ * always dropped). */
+typedef struct {
+    int misfit;              /* OWL_MISFIT_* */
+    float dt;                /* sample interval of the traces (s) */
+    float tlag_max;          /* adaptive: largest penalised lag (s) */
+    int penalty;             /* OWL_PENALTY_* */
+    float penalty_power;     /* exponent of the power / gaussian / exp penalties */
+    float deconv_eps;        /* adaptive: water level, relative to max |D|^2 */
+    float discard_threshold; /* trace_discard_threshold (relative to the gather's largest trace norm) */
+} owl_misfit_opts;
 
 typedef struct owl_ssg owl_ssg;
 
@@ -229,7 +261,38 @@ int owl_ssg_misfit(owl_ssg *h, int nshots, const owl_shot *shots, const float *o
                    const owl_run_opts *opts, double *misfit, double *trace_misfit,
                    float *seis_out, int mem_kind, owl_run_info *info);
 
+/* owl_ssg_gradient with a data-domain misfit other than (or as well as) L2:
+ * after the forward, the adjoint source and the per-trace misfits of every
+ * gather are computed on the GPU exactly as owl_adjoint_source does (trace
+ * discard rule included), and the gradient is that of 0.5 * the misfit.
+ *   obs: observed seismograms, layout of owl_ssg_forward.
+ *   misfit: nshots doubles (may be NULL), the sum of the shot's trace misfits. */
+int owl_ssg_gradient_misfit(owl_ssg *h, int nshots, const owl_shot *shots, const float *obs,
+                            const owl_misfit_opts *mopts, const owl_run_opts *opts, double *misfit,
+                            float *grad, float *seis_out, int mem_kind, owl_run_info *info);
+
 void owl_ssg_destroy(owl_ssg *h);
+
+/* ---- adjoint sources (compute_adjoint_source,
+ *      src/inverse/module_inversion_adjoint_source.f90:985-1277) ------------ */
+
+/* Misfit and adjoint source of every trace of ngather gathers (one shot's one
+ * component each), on the GPU. Traces are rows of nt samples, gathers are
+ * contiguous: gather g holds traces gather_ptr[g] .. gather_ptr[g + 1] - 1 of
+ * syn / obs / adj (host array of ngather + 1 ints, gather_ptr[0] = 0). A trace
+ * is dropped (misfit 0, adjoint 0) when its weight is 0 or when its obs or syn
+ * norm is below discard_threshold times the gather's largest obs or syn norm or
+ * is 0 (:1047-1050). weight: one float per trace or NULL (all 1).
+ *   adj: adjoint source, the layout of syn (may be NULL).
+ *   trace_misfit: one double per trace (may be NULL).
+ *   gather_misfit: one double per gather (may be NULL).
+ * syn, obs, adj, weight, trace_misfit and gather_misfit are all host memory
+ * (OWL_MEM_HOST) or all device memory of the current device (OWL_MEM_DEVICE).
+ * Trace length: nt <= 8192 (envelope, phase) or next_power_235(2 nt) <= 8192
+ * (adaptive), else OWL_ERR_INVALID. */
+int owl_adjoint_source(const owl_misfit_opts *mopts, int ngather, const int *gather_ptr, int nt,
+                       const float *syn, const float *obs, const float *weight, float *adj,
+                       double *trace_misfit, double *gather_misfit, int mem_kind);
 
 /* ---- diagnostics (no counterpart in the reference) ------------------------ */
 

@@ -46,6 +46,23 @@ OWL_CKPT_BF16 = 2
 OWL_ADJ_L2_RESIDUAL = 0
 OWL_ADJ_GIVEN = 1
 
+OWL_MISFIT_WAVEFORM = 0
+OWL_MISFIT_CORR = 1
+OWL_MISFIT_ENVELOPE = 2
+OWL_MISFIT_PHASE = 3
+OWL_MISFIT_ADAPTIVE = 4
+
+OWL_PENALTY_LINEAR = 0
+OWL_PENALTY_POWER = 1
+OWL_PENALTY_GAUSSIAN = 2
+OWL_PENALTY_EXP = 3
+
+#: misfit_type names of the reference's parameter file
+MISFIT_NAMES = {"waveform": OWL_MISFIT_WAVEFORM, "corr": OWL_MISFIT_CORR, "envelope": OWL_MISFIT_ENVELOPE,
+                "phase": OWL_MISFIT_PHASE, "adaptive": OWL_MISFIT_ADAPTIVE}
+PENALTY_NAMES = {"linear": OWL_PENALTY_LINEAR, "power": OWL_PENALTY_POWER, "gaussian": OWL_PENALTY_GAUSSIAN,
+                 "exp": OWL_PENALTY_EXP}
+
 MEDIUM_NAMES = {
     "acoustic-iso": OWL_ACOUSTIC_ISO_2D,
     "acoustic-iso-3d": OWL_ACOUSTIC_ISO_3D,
@@ -123,6 +140,18 @@ class OwlRunOpts(C.Structure):
     ]
 
 
+class OwlMisfitOpts(C.Structure):
+    _fields_ = [
+        ("misfit", C.c_int),
+        ("dt", C.c_float),
+        ("tlag_max", C.c_float),
+        ("penalty", C.c_int),
+        ("penalty_power", C.c_float),
+        ("deconv_eps", C.c_float),
+        ("discard_threshold", C.c_float),
+    ]
+
+
 class OwlRunInfo(C.Structure):
     _fields_ = [
         ("elapsed_ms", C.c_double),
@@ -141,7 +170,8 @@ EXPORTED = [
     "owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
     "owl_ssg_source_gradient", "owl_ssg_destroy", "owl_last_error", "owl_ssg_abi_version",
     "owl_ssg_dt_stable", "owl_ssg_nparam", "owl_ssg_ncomp", "owl_ssg_device_ok", "owl_ssg_kernel_time",
-    "owl_ssg_forward_noalloc", "owl_ssg_desc_nparam", "owl_ssg_misfit",
+    "owl_ssg_forward_noalloc", "owl_ssg_desc_nparam", "owl_ssg_misfit", "owl_ssg_gradient_misfit",
+    "owl_adjoint_source",
 ]
 
 OWL_K_FWD_P = 0
@@ -188,9 +218,15 @@ def load() -> C.CDLL:
     lib.owl_ssg_desc_nparam.argtypes = [P(OwlSsgDesc)]
     lib.owl_ssg_misfit.argtypes = [C.c_void_p, C.c_int, P(OwlShot), C.c_void_p, P(OwlRunOpts), C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_int, P(OwlRunInfo)]
+    lib.owl_ssg_gradient_misfit.argtypes = [C.c_void_p, C.c_int, P(OwlShot), C.c_void_p, P(OwlMisfitOpts),
+                                            P(OwlRunOpts), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                            P(OwlRunInfo)]
+    lib.owl_adjoint_source.argtypes = [P(OwlMisfitOpts), C.c_int, P(C.c_int), C.c_int, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     for fn in ("owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
                "owl_ssg_source_gradient", "owl_ssg_abi_version", "owl_ssg_nparam", "owl_ssg_ncomp",
-               "owl_ssg_device_ok", "owl_ssg_desc_nparam", "owl_ssg_misfit"):
+               "owl_ssg_device_ok", "owl_ssg_desc_nparam", "owl_ssg_misfit", "owl_ssg_gradient_misfit",
+               "owl_adjoint_source"):
         getattr(lib, fn).restype = C.c_int
     _lib = lib
     return lib

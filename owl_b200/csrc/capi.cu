@@ -2,6 +2,7 @@
 #include <memory>
 #include <mutex>
 
+#include "adjsrc.cuh"
 #include "engine.cuh"
 
 struct owl_ssg {
@@ -171,6 +172,82 @@ int owl_ssg_misfit(owl_ssg* h, int nshots, const owl_shot* shots, const float* o
         owl_run_info tmp{};
         h->eng->misfit(nshots, shots, obs, opts_or_default(opts), misfit, trace_misfit, seis_out, mem_kind,
                        info ? *info : tmp);
+    });
+}
+
+int owl_ssg_gradient_misfit(owl_ssg* h, int nshots, const owl_shot* shots, const float* obs,
+                            const owl_misfit_opts* mopts, const owl_run_opts* opts, double* misfit, float* grad,
+                            float* seis_out, int mem_kind, owl_run_info* info) {
+    return guarded([&] {
+        OWL_CHECK(h && h->eng, OWL_ERR_INVALID, "null handle");
+        OWL_CHECK(mopts, OWL_ERR_INVALID, "null misfit options");
+        OWL_CHECK(nshots >= 0 && (nshots == 0 || shots), OWL_ERR_INVALID, "bad shots");
+        OWL_CHECK(obs || nshots == 0, OWL_ERR_INVALID, "null data buffer");
+        OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
+        OWL_CHECK(mopts->misfit >= OWL_MISFIT_WAVEFORM && mopts->misfit <= OWL_MISFIT_ADAPTIVE, OWL_ERR_INVALID,
+                  "bad misfit type");
+        h->eng->mopts = *mopts;
+        if (h->eng->mopts.dt <= 0.f) h->eng->mopts.dt = h->eng->desc.dt;
+        owl_run_info tmp{};
+        h->eng->gradient(nshots, shots, obs, ADJ_MISFIT, opts_or_default(opts), misfit, grad, seis_out, mem_kind,
+                         info ? *info : tmp);
+    });
+}
+
+int owl_adjoint_source(const owl_misfit_opts* mopts, int ngather, const int* gather_ptr, int nt, const float* syn,
+                       const float* obs, const float* weight, float* adj, double* trace_misfit,
+                       double* gather_misfit, int mem_kind) {
+    return guarded([&] {
+        check_device();
+        OWL_CHECK(mopts, OWL_ERR_INVALID, "null misfit options");
+        OWL_CHECK(ngather >= 0 && (ngather == 0 || gather_ptr) && nt >= 1, OWL_ERR_INVALID, "bad trace layout");
+        OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
+        const int ntr = ngather ? gather_ptr[ngather] : 0;
+        OWL_CHECK(ntr >= 0 && (ntr == 0 || (syn && obs)), OWL_ERR_INVALID, "null trace buffer");
+        struct Ctx {
+            cudaStream_t s = nullptr;
+            ~Ctx() {
+                if (s) cudaStreamDestroy(s);
+            }
+        } c;
+        OWL_CUDA(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+        AdjointSource as;
+        const size_t n = (size_t)ntr * nt;
+        DevBuf<float> dsyn, dobs, dadj, dw;
+        DevBuf<double> dtm, dgm;
+        DevBuf<unsigned char> dlive;
+        const bool dev = mem_kind == OWL_MEM_DEVICE;
+        const float* ps = syn;
+        const float* po = obs;
+        float* pa = adj;
+        double* ptm = trace_misfit;
+        double* pgm = gather_misfit;
+        if (!dev && ntr) {
+            dsyn.upload(syn, n, c.s);
+            dobs.upload(obs, n, c.s);
+            ps = dsyn.p;
+            po = dobs.p;
+            if (adj) { dadj.reserve(n); pa = dadj.p; }
+            if (trace_misfit) { dtm.reserve(ntr); ptm = dtm.p; }
+        }
+        if (!dev && gather_misfit && ngather) { dgm.reserve(ngather); pgm = dgm.p; }
+        const unsigned char* wl = nullptr;
+        if (weight && ntr) {
+            const float* pw = weight;
+            if (!dev) { dw.upload(weight, ntr, c.s); pw = dw.p; }
+            dlive.reserve(ntr);
+            launch_nonzero(pw, ntr, dlive.p, c.s);
+            wl = dlive.p;
+        }
+        as.run(*mopts, ngather, gather_ptr, nt, ps, po, wl, pa, ptm, pgm, c.s);
+        if (!dev) {
+            if (adj && ntr) OWL_CUDA(cudaMemcpyAsync(adj, pa, n * sizeof(float), cudaMemcpyDeviceToHost, c.s));
+            if (trace_misfit && ntr)
+                OWL_CUDA(cudaMemcpyAsync(trace_misfit, ptm, ntr * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+            if (gather_misfit && ngather)
+                OWL_CUDA(cudaMemcpyAsync(gather_misfit, pgm, ngather * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+        }
+        OWL_CUDA(cudaStreamSynchronize(c.s));
     });
 }
 

@@ -5,8 +5,13 @@
 
 namespace owl {
 
+// internal adjoint-source kind of Engine::gradient: a data-domain misfit given
+// by Engine::mopts (owl_ssg_gradient_misfit)
+constexpr int ADJ_MISFIT = 100;
+
 struct Engine {
     owl_ssg_desc desc{};
+    owl_misfit_opts mopts{};
     cudaStream_t stream = nullptr;
     float dt_stable_ = 0.f;
     bool model_set = false;
@@ -68,5 +73,10 @@ void launch_check_finite(const float* f, size_t n, int* flag, cudaStream_t s);
 void launch_trace_misfit(const float* syn, const float* obs, const unsigned char* live, const int* shot_rec_ptr,
                          int nshots, int nt, int rtot, double* trace_misfit, double* misfit, cudaStream_t s);
 void launch_fill_f64(double* p, size_t n, double v, cudaStream_t s);
+// per-shot sums of per-trace misfits, in trace order
+void launch_shot_misfit(const double* trace_misfit, const int* shot_rec_ptr, int nshots, double* misfit,
+                        cudaStream_t s);
+// out[i] = (w[i] != 0) (adjsrc.cu)
+void launch_nonzero(const float* w, int n, unsigned char* out, cudaStream_t s);
 
 }  // namespace owl

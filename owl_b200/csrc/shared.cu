@@ -136,6 +136,13 @@ __global__ void k_shot_misfit(const double* __restrict__ tm, const int* __restri
     misfit[s] = acc;
 }
 
+void launch_shot_misfit(const double* trace_misfit, const int* shot_rec_ptr, int nshots, double* misfit,
+                        cudaStream_t s) {
+    if (nshots <= 0) return;
+    k_shot_misfit<<<(nshots + 127) / 128, 128, 0, s>>>(trace_misfit, shot_rec_ptr, nshots, misfit);
+    OWL_LAUNCH_CHECK();
+}
+
 void launch_trace_misfit(const float* syn, const float* obs, const unsigned char* live, const int* shot_rec_ptr,
                          int nshots, int nt, int rtot, double* trace_misfit, double* misfit, cudaStream_t s) {
     if (rtot > 0) {

@@ -238,6 +238,7 @@ void SsgBase::set_step(int v) {
 void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
     HostCSR hinj, hsmp, hsct;
     std::vector<int> hinj_ptr(1, 0), hrec_ptr(1, 0), hsct_ptr(1, 0);
+    h_gather_ptr.assign(1, 0);
     std::vector<float> hamp;
     std::vector<unsigned char> hlive;
     item_src.clear(); item_comp.clear(); item_shot.clear(); item_rho_cell.clear(); item_rho.clear();
@@ -300,6 +301,7 @@ void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
             for (auto& e : kv.second) hsct.push(Tap{kv.first.first, s, kv.first.second, e.second, e.first});
             hsct.close_item();
         }
+        for (int comp = 0; comp < ncomp; ++comp) h_gather_ptr.push_back(rtot + (comp + 1) * sh.nrec);
         rtot += ncomp * sh.nrec;
         hrec_ptr.push_back(rtot);
         hsct_ptr.push_back(hsct.nitems());
@@ -671,7 +673,8 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
                             double* misfit, float* grad, float* seis_out, float* stf_grad, int mem,
                             owl_run_info& info) {
     OWL_CHECK(model_set, OWL_ERR_INVALID, "set_model must be called first");
-    OWL_CHECK(adj_kind == OWL_ADJ_L2_RESIDUAL || adj_kind == OWL_ADJ_GIVEN, OWL_ERR_INVALID, "bad adj_kind");
+    OWL_CHECK(adj_kind == OWL_ADJ_L2_RESIDUAL || adj_kind == OWL_ADJ_GIVEN || adj_kind == ADJ_MISFIT,
+              OWL_ERR_INVALID, "bad adj_kind");
     int B, k;
     bool graph;
     resolve_opts(o, nshots, B, k, graph);
@@ -721,11 +724,25 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
                                      mem == OWL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
             launch_transpose_seis_to_rec(seis_tmp.p, obs_t.p, nt, rtot, stream);
             launches++;
-            if (adj_kind == OWL_ADJ_L2_RESIDUAL)
+            if (adj_kind == OWL_ADJ_L2_RESIDUAL) {
                 launch_residual_l2(rec.p, obs_t.p, res.p, live.p, rec_shot_ptr.p, S, nt, rtot, misfit_d.p, stream);
-            else
+                launches++;
+            } else if (adj_kind == ADJ_MISFIT) {
+                // compute_adjoint_source on the trace-major gathers of the batch
+                // (seis_tmp holds the observed traces as uploaded)
+                syn_t.reserve(n);
+                adj_t.reserve(n);
+                trace_d.reserve(rtot);
+                launch_transpose_rec_to_seis(rec.p, syn_t.p, nt, rtot, stream);
+                adjsrc.launches = 0;
+                adjsrc.run(mopts, (int)h_gather_ptr.size() - 1, h_gather_ptr.data(), nt, syn_t.p, seis_tmp.p,
+                           live.p, adj_t.p, trace_d.p, nullptr, stream);
+                launch_shot_misfit(trace_d.p, rec_shot_ptr.p, S, misfit_d.p, stream);
+                launch_transpose_seis_to_rec(adj_t.p, res.p, nt, rtot, stream);
+                launches += adjsrc.launches + 3;
+            } else {
                 OWL_CUDA(cudaMemcpyAsync(res.p, obs_t.p, n * sizeof(float), cudaMemcpyDeviceToDevice, stream));
-            launches++;
+            }
             if (seis_out) {
                 launch_transpose_rec_to_seis(rec.p, seis_tmp.p, nt, rtot, stream);
                 launches++;

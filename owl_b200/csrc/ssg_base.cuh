@@ -21,6 +21,7 @@
 #include <map>
 #include <vector>
 
+#include "adjsrc.cuh"
 #include "engine.cuh"
 
 namespace owl {
@@ -100,6 +101,9 @@ struct SsgBase : Engine {
     std::vector<float> item_rho;
     std::map<std::pair<int, int>, std::array<int, 4>> tune_cache;
     std::vector<float> h_rhop;  // padded rho, storage layout (force-source weights)
+    std::vector<int> h_gather_ptr;  // trace ranges of the (shot, component) gathers of the batch
+    AdjointSource adjsrc;
+    DevBuf<float> syn_t, adj_t;     // trace-major synthetics / adjoint source (data-domain misfits)
 
     SsgBase(const owl_ssg_desc& d, int dim_);
     ~SsgBase() override;

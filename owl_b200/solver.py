@@ -50,6 +50,68 @@ def _mem_kind(a) -> int:
     return L.OWL_MEM_HOST
 
 
+def _ready(*bufs) -> None:
+    """Device buffers must be complete when a call starts (the library works on
+    its own stream): wait for torch's current stream when any buffer is a CUDA
+    tensor."""
+    for b in bufs:
+        if b is not None and hasattr(b, "is_cuda") and b.is_cuda:
+            import torch
+            torch.cuda.current_stream(b.device).synchronize()
+            return
+
+
+@dataclass
+class MisfitOpts:
+    """owl_misfit_opts: the reference's misfit_type and its parameters
+    (src/lib/module_parameters.f90:550-570); zeros take the reference's defaults."""
+    misfit: int = L.OWL_MISFIT_WAVEFORM
+    dt: float = 0.0
+    tlag_max: float = 0.0
+    penalty: int = L.OWL_PENALTY_LINEAR
+    penalty_power: float = 0.0
+    deconv_eps: float = 0.0
+    discard_threshold: float = 0.0
+
+    def c(self) -> L.OwlMisfitOpts:
+        o = L.OwlMisfitOpts()
+        for k in ("misfit", "penalty"):
+            setattr(o, k, int(getattr(self, k)))
+        for k in ("dt", "tlag_max", "penalty_power", "deconv_eps", "discard_threshold"):
+            setattr(o, k, float(getattr(self, k)))
+        return o
+
+
+def adjoint_source(mopts: MisfitOpts, gather_ptr, syn, obs, weight=None, adj=None, trace_misfit=None,
+                   gather_misfit=None):
+    """compute_adjoint_source on the GPU for traces given as rows (ntr, nt) of
+    numpy arrays (host) or CUDA tensors (device); gathers are the row ranges
+    gather_ptr[g] .. gather_ptr[g+1]-1. Returns (adj, trace misfits, gather misfits)."""
+    lib = L.load()
+    gp = np.ascontiguousarray(np.asarray(gather_ptr, dtype=np.int32))
+    ng = gp.size - 1
+    ntr, nt = int(syn.shape[0]), int(syn.shape[1])
+    if hasattr(syn, "is_cuda") and syn.is_cuda:
+        import torch
+        dev = syn.device
+        adj = torch.empty_like(syn) if adj is None else adj
+        trace_misfit = torch.empty(ntr, dtype=torch.float64, device=dev) if trace_misfit is None else trace_misfit
+        gather_misfit = torch.empty(ng, dtype=torch.float64, device=dev) if gather_misfit is None else gather_misfit
+        _ready(syn, obs, weight, adj, trace_misfit, gather_misfit)
+    else:
+        syn = np.ascontiguousarray(syn, dtype=f32)
+        obs = np.ascontiguousarray(obs, dtype=f32)
+        weight = None if weight is None else np.ascontiguousarray(weight, dtype=f32)
+        adj = np.empty_like(syn) if adj is None else adj
+        trace_misfit = np.empty(ntr) if trace_misfit is None else trace_misfit
+        gather_misfit = np.empty(ng) if gather_misfit is None else gather_misfit
+    o = mopts.c()
+    L.check(lib.owl_adjoint_source(C.byref(o), ng, gp.ctypes.data_as(C.POINTER(C.c_int)), nt, _ptr(syn), _ptr(obs),
+                                   _ptr(weight) if weight is not None else None, _ptr(adj), _ptr(trace_misfit),
+                                   _ptr(gather_misfit), _mem_kind(syn)))
+    return adj, trace_misfit, gather_misfit
+
+
 def elastic_time_integration(mechanism: str) -> int:
     """STF time integration of the elastic media: explosion and moment-tensor
     sources inject the derivative of the wavelet as a stress drop."""
@@ -152,6 +214,7 @@ class SSGSolver:
         if out is None:
             out = np.zeros(self.seis_size(ps), dtype=f32)
         o = opts.c()
+        _ready(out)
         L.check(self.lib.owl_ssg_forward(self.h, ps.nshots, ps.arr, C.byref(o), _ptr(out), _mem_kind(out),
                                          C.byref(self.last_info)))
         return out
@@ -173,11 +236,43 @@ class SSGSolver:
                 grad = np.zeros(self.nparam * nm, dtype=f32)
                 misfit = np.zeros(ps.nshots, dtype=np.float64)
         o = opts.c()
+        _ready(data, grad, misfit, seis_out)
         L.check(self.lib.owl_ssg_gradient(self.h, ps.nshots, ps.arr, _ptr(data), adj_kind, C.byref(o),
                                           _ptr(misfit) if misfit is not None else None, _ptr(grad),
                                           _ptr(seis_out) if seis_out is not None else None,
                                           _mem_kind(data), C.byref(self.last_info)))
         return misfit, grad
+
+    def gradient_misfit(self, ps: PreparedShots, obs, mopts: MisfitOpts, opts: Optional[RunOpts] = None,
+                        grad=None, misfit=None, seis_out=None):
+        """Stacked gradient of 0.5 * the data-domain misfit `mopts` (the adjoint
+        source and the trace selection of compute_adjoint_source, on the GPU).
+        Returns (misfit per shot, gradient flat buffer)."""
+        opts = opts or RunOpts()
+        nm = self.desc.nx * self.desc.nz * max(1, self.desc.ny)
+        if grad is None:
+            if _mem_kind(obs) == L.OWL_MEM_DEVICE:
+                import torch
+                grad = torch.zeros(self.nparam * nm, dtype=torch.float32, device=obs.device)
+                misfit = torch.zeros(ps.nshots, dtype=torch.float64, device=obs.device)
+            else:
+                grad = np.zeros(self.nparam * nm, dtype=f32)
+                misfit = np.zeros(ps.nshots, dtype=np.float64)
+        o, mo = opts.c(), mopts.c()
+        _ready(obs, grad, misfit, seis_out)
+        L.check(self.lib.owl_ssg_gradient_misfit(self.h, ps.nshots, ps.arr, _ptr(obs), C.byref(mo), C.byref(o),
+                                                 _ptr(misfit) if misfit is not None else None, _ptr(grad),
+                                                 _ptr(seis_out) if seis_out is not None else None,
+                                                 _mem_kind(obs), C.byref(self.last_info)))
+        return misfit, grad
+
+    def gather_ptr(self, ps: PreparedShots) -> np.ndarray:
+        """row ranges of the (shot, component) gathers in the seismogram layout"""
+        gp = [0]
+        for s in range(ps.nshots):
+            for _ in range(self.ncomp):
+                gp.append(gp[-1] + ps.nrec(s))
+        return np.asarray(gp, dtype=np.int32)
 
     def grad_fields(self, grad) -> List[np.ndarray]:
         """flat gradient -> list of (nz, nx) [or (nz, ny, nx)] arrays (z fastest like OWL files)"""
