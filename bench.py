@@ -41,6 +41,7 @@ def parse():
     p.add_argument("--profile", action="store_true",
                    help="profiling target: one gradient step of --nshots shots, nothing else, no JSON line")
     p.add_argument("--no-3d", action="store_true", help="skip the 3D acoustic forward roofline block")
+    p.add_argument("--no-misfits", action="store_true", help="skip the data-domain misfit block")
     p.add_argument("--profile3d", type=int, default=0, metavar="N",
                    help="profiling target: 12-step 3D acoustic forward of an N^3 model, no JSON line")
     p.add_argument("--no-elastic", action="store_true", help="skip the 2D elastic VTI block")
@@ -280,6 +281,38 @@ class Clocks:
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         busy = [v for v in sm if v > 0.5 * smax] or sm
         return {"sm_mhz": busy[len(busy) // 2], "sm_max_mhz": smax, "reasons": reasons, "samples": len(rows)}
+
+
+def misfit_block(s, ps, obs_dev, opts, l2_ms):
+    """Each data-domain misfit on the gradient workload: the gradient of the
+    32-shot batch with the misfit's adjoint source computed on the GPU, and the
+    standalone adjoint-source call on the batch's gathers (device buffers)."""
+    import torch
+    from owl_b200 import _lib as L
+    from owl_b200.solver import MisfitOpts, adjoint_source
+
+    nt = s.desc.nt
+    gp = s.gather_ptr(ps)
+    syn = torch.empty(s.seis_size(ps), dtype=torch.float32, device="cuda")
+    s.forward(ps, opts, out=syn)
+    syn2, obs2 = syn.view(-1, nt), obs_dev.view(-1, nt)
+    ntr = syn2.shape[0]
+    out = {"workload": f"the gradient workload ({ps.nshots} shots); adjoint sources of its {len(gp) - 1} gathers, "
+                       f"{ntr} traces of {nt} samples; adaptive: linear penalty, tlag_max 0.2 s, deconv_eps 0.1"}
+    for name, kind in L.MISFIT_NAMES.items():
+        mo = MisfitOpts(misfit=kind, dt=s.desc.dt, tlag_max=0.2)
+        s.gradient_misfit(ps, obs_dev, mo, opts)
+        s.gradient_misfit(ps, obs_dev, mo, opts)
+        gms = s.last_info.elapsed_ms
+        adjoint_source(mo, gp, syn2, obs2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            adjoint_source(mo, gp, syn2, obs2)
+        ams = (time.perf_counter() - t0) / 3 * 1e3
+        out[name] = {"gradient_s_per_shot": gms / 1e3 / ps.nshots, "gradient_vs_l2": gms / l2_ms,
+                     "adjoint_source_ms": ams, "traces_per_s": ntr / (ams / 1e3)}
+    return out
 
 
 def measured_peak_hbm():
@@ -522,6 +555,9 @@ def main():
     if rank == 0 and world == 1:
         v, threads, sample = cpu_reference_sample(args.cpu_nt)
         line["cpu_baseline"] = {"value": v, "unit": "s/shot", "cores": threads, "kind": "port", "sample": sample}
+
+    if rank == 0 and not args.no_misfits:
+        line["misfits"] = misfit_block(s, ps, obs_dev, opts, ms_step)
 
     s.close()
     if rank == 0 and not args.no_3d:

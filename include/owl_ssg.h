@@ -214,6 +214,37 @@ int owl_ssg_create(const owl_ssg_desc *desc, owl_ssg **out);
  * src/lib/module_anisotropy.f90:310-402, src/solver/elastic_vhtiort_2d/module_cfspml.f90:229-577). */
 int owl_ssg_set_model(owl_ssg *h, int nparam, const float *const *fields);
 
+/* Seismogram sampling of the data: data_nt samples at data_dt (s) from t = 0
+ * (the solver's data_dt / data_tmax, src/solver/acoustic_iso_2d/module_vars.f90:162-164;
+ * data_nt = nint(data_tmax / data_dt + 1)). From this call on, forward and
+ * misfit return, and gradient, gradient_misfit and source_gradient take, traces
+ * of data_nt samples: the synthetics are resampled from the time axis (nt at
+ * dt) as resample_su does after modelling (src/lib/module_su.f90:426-470,
+ * submodule_forward_modeling.f90:124-125), the misfit and adjoint source are
+ * computed at the data sampling, and the adjoint source is resampled back to
+ * the time axis before injection (submodule_fwi_gradient.f90:46). The
+ * resampling is cubic convolution (Keys, a = -1/2), zero outside the input
+ * span. data_nt <= 0 returns to the time axis. */
+int owl_ssg_set_data_sampling(owl_ssg *h, int data_nt, float data_dt);
+
+/* Cubic-convolution resampling of ntr rows of nin samples at din from oin to
+ * nout samples at dout from oout (resample_su's interp(..., 'cubic')), on the
+ * GPU. in / out: host (OWL_MEM_HOST) or device (OWL_MEM_DEVICE) memory. */
+int owl_resample_traces(int ntr, int nin, float din, float oin, const float *in, int nout, float dout, float oout,
+                        float *out, int mem_kind);
+
+/* SU files (the su type's output / load, src/lib/module_su.f90) assembled and
+ * taken apart on the GPU. A record is the 240-byte trace header followed by
+ * ns float32 samples in native byte order; the file is ntr records.
+ * owl_su_encode: every record's header is the 240-byte host template `header`
+ * (ns at byte 114, dt in microseconds at 116, d1 at 180), traces = ntr x ns
+ * rows, out = ntr x (240 + 4 ns) bytes. owl_su_decode: the samples of every
+ * record into traces. traces / out / in: host (OWL_MEM_HOST) or device
+ * (OWL_MEM_DEVICE) memory; 1 <= ns <= 32767 (the header's int16 ns). */
+int owl_su_encode(int ntr, int ns, const unsigned char *header, const float *traces, unsigned char *out,
+                  int mem_kind);
+int owl_su_decode(int ntr, int ns, const unsigned char *in, float *traces, int mem_kind);
+
 /* Forward modelling of nshots shots (batched by opts->shots_per_launch).
  * Replaces compute_forward (src/solver/acoustic_iso_2d/submodule_forward_modeling.f90:31-132).
  * seis: per shot, ncomp x nrec x nt float32 (trace-major, the SU trace order),

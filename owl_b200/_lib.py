@@ -171,7 +171,7 @@ EXPORTED = [
     "owl_ssg_source_gradient", "owl_ssg_destroy", "owl_last_error", "owl_ssg_abi_version",
     "owl_ssg_dt_stable", "owl_ssg_nparam", "owl_ssg_ncomp", "owl_ssg_device_ok", "owl_ssg_kernel_time",
     "owl_ssg_forward_noalloc", "owl_ssg_desc_nparam", "owl_ssg_misfit", "owl_ssg_gradient_misfit",
-    "owl_adjoint_source",
+    "owl_adjoint_source", "owl_ssg_set_data_sampling", "owl_resample_traces", "owl_su_encode", "owl_su_decode",
 ]
 
 OWL_K_FWD_P = 0
@@ -223,10 +223,16 @@ def load() -> C.CDLL:
                                             P(OwlRunInfo)]
     lib.owl_adjoint_source.argtypes = [P(OwlMisfitOpts), C.c_int, P(C.c_int), C.c_int, C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    lib.owl_ssg_set_data_sampling.argtypes = [C.c_void_p, C.c_int, C.c_float]
+    lib.owl_resample_traces.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p, C.c_int, C.c_float,
+                                        C.c_float, C.c_void_p, C.c_int]
+    lib.owl_su_encode.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    lib.owl_su_decode.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
     for fn in ("owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
                "owl_ssg_source_gradient", "owl_ssg_abi_version", "owl_ssg_nparam", "owl_ssg_ncomp",
                "owl_ssg_device_ok", "owl_ssg_desc_nparam", "owl_ssg_misfit", "owl_ssg_gradient_misfit",
-               "owl_adjoint_source"):
+               "owl_adjoint_source", "owl_ssg_set_data_sampling", "owl_resample_traces", "owl_su_encode",
+               "owl_su_decode"):
         getattr(lib, fn).restype = C.c_int
     _lib = lib
     return lib

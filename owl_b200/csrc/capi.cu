@@ -194,6 +194,84 @@ int owl_ssg_gradient_misfit(owl_ssg* h, int nshots, const owl_shot* shots, const
     });
 }
 
+int owl_ssg_set_data_sampling(owl_ssg* h, int data_nt, float data_dt) {
+    return guarded([&] {
+        OWL_CHECK(h && h->eng, OWL_ERR_INVALID, "null handle");
+        OWL_CHECK(data_nt <= 0 || data_dt > 0.f, OWL_ERR_INVALID, "data_dt must be positive");
+        h->eng->data_nt = data_nt > 0 ? data_nt : 0;
+        h->eng->data_dt = data_nt > 0 ? data_dt : 0.f;
+    });
+}
+
+int owl_resample_traces(int ntr, int nin, float din, float oin, const float* in, int nout, float dout, float oout,
+                        float* out, int mem_kind) {
+    return guarded([&] {
+        check_device();
+        OWL_CHECK(ntr >= 0 && nin >= 1 && nout >= 0 && din > 0.f && dout > 0.f, OWL_ERR_INVALID,
+                  "bad resampling geometry");
+        OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
+        if (ntr == 0 || nout == 0) return;
+        OWL_CHECK(in && out, OWL_ERR_INVALID, "null trace buffer");
+        struct Ctx {
+            cudaStream_t s = nullptr;
+            ~Ctx() {
+                if (s) cudaStreamDestroy(s);
+            }
+        } c;
+        OWL_CUDA(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+        DevBuf<float> din_b, dout_b;
+        const float* pi = in;
+        float* po = out;
+        if (mem_kind == OWL_MEM_HOST) {
+            din_b.upload(in, (size_t)ntr * nin, c.s);
+            dout_b.reserve((size_t)ntr * nout);
+            pi = din_b.p;
+            po = dout_b.p;
+        }
+        launch_resample_rows(pi, nin, din, oin, po, nout, dout, oout, ntr, c.s);
+        if (mem_kind == OWL_MEM_HOST)
+            OWL_CUDA(cudaMemcpyAsync(out, po, (size_t)ntr * nout * sizeof(float), cudaMemcpyDeviceToHost, c.s));
+        OWL_CUDA(cudaStreamSynchronize(c.s));
+    });
+}
+
+int owl_su_encode(int ntr, int ns, const unsigned char* header, const float* traces, unsigned char* out,
+                  int mem_kind) {
+    return guarded([&] {
+        check_device();
+        OWL_CHECK(ntr >= 0 && ns >= 1 && ns <= 32767, OWL_ERR_INVALID, "bad SU geometry (1 <= ns <= 32767)");
+        OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
+        if (ntr == 0) return;
+        OWL_CHECK(header && traces && out, OWL_ERR_INVALID, "null buffer");
+        struct Ctx {
+            cudaStream_t s = nullptr;
+            ~Ctx() {
+                if (s) cudaStreamDestroy(s);
+            }
+        } c;
+        OWL_CUDA(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+        su_encode(header, traces, ntr, ns, out, mem_kind == OWL_MEM_DEVICE, c.s);
+    });
+}
+
+int owl_su_decode(int ntr, int ns, const unsigned char* in, float* traces, int mem_kind) {
+    return guarded([&] {
+        check_device();
+        OWL_CHECK(ntr >= 0 && ns >= 1 && ns <= 32767, OWL_ERR_INVALID, "bad SU geometry (1 <= ns <= 32767)");
+        OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
+        if (ntr == 0) return;
+        OWL_CHECK(in && traces, OWL_ERR_INVALID, "null buffer");
+        struct Ctx {
+            cudaStream_t s = nullptr;
+            ~Ctx() {
+                if (s) cudaStreamDestroy(s);
+            }
+        } c;
+        OWL_CUDA(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+        su_decode(in, ntr, ns, traces, mem_kind == OWL_MEM_DEVICE, c.s);
+    });
+}
+
 int owl_adjoint_source(const owl_misfit_opts* mopts, int ngather, const int* gather_ptr, int nt, const float* syn,
                        const float* obs, const float* weight, float* adj, double* trace_misfit,
                        double* gather_misfit, int mem_kind) {

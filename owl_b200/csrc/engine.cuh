@@ -27,6 +27,10 @@ struct Engine {
                         double* trace_misfit, float* seis_out, int mem, owl_run_info& info) = 0;
     virtual void source_gradient(int nshots, const owl_shot* shots, const float* adj, const owl_run_opts& o,
                                  float* stf_grad, int mem, owl_run_info& info) = 0;
+    // seismogram sampling of the data (forward output, observed data, adjoint
+    // sources): data_nt samples at data_dt from t = 0; data_nt <= 0: the time axis
+    int data_nt = 0;
+    float data_dt = 0.f;
 };
 
 Engine* make_ac2d_engine(const owl_ssg_desc& d);
@@ -73,9 +77,16 @@ void launch_check_finite(const float* f, size_t n, int* flag, cudaStream_t s);
 void launch_trace_misfit(const float* syn, const float* obs, const unsigned char* live, const int* shot_rec_ptr,
                          int nshots, int nt, int rtot, double* trace_misfit, double* misfit, cudaStream_t s);
 void launch_fill_f64(double* p, size_t n, double v, cudaStream_t s);
+// cubic-convolution resampling of ntr rows (nin samples at din from oin) to nout samples at dout from oout
+void launch_resample_rows(const float* in, int nin, double din, double oin, float* out, int nout, double dout,
+                          double oout, int ntr, cudaStream_t s);
 // per-shot sums of per-trace misfits, in trace order
 void launch_shot_misfit(const double* trace_misfit, const int* shot_rec_ptr, int nshots, double* misfit,
                         cudaStream_t s);
+// SU records <-> trace rows (su.cu); header: one 240-byte host template; dev: data buffers on the device
+void su_encode(const unsigned char* header, const float* traces, int ntr, int ns, unsigned char* out, bool dev,
+               cudaStream_t s);
+void su_decode(const unsigned char* in, int ntr, int ns, float* traces, bool dev, cudaStream_t s);
 // out[i] = (w[i] != 0) (adjsrc.cu)
 void launch_nonzero(const float* w, int n, unsigned char* out, cudaStream_t s);
 

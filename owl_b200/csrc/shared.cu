@@ -66,6 +66,40 @@ static void launch_transpose(const float* in, float* out, int rows, int cols, cu
     OWL_LAUNCH_CHECK();
 }
 
+// Cubic-convolution resampling of trace rows (Keys' kernel, a = -1/2): output
+// sample i of a row sits at t = oout + i dout, read from the input samples
+// j0-1 .. j0+2 around x = (t - oin) / din (indices clamped to the row; x within
+// 1e-4 of a node snaps to it), zero outside [0, nin - 1]. Linear in the data;
+// exact on input nodes.
+__global__ void k_resample_rows(const float* __restrict__ in, int nin, double din, double oin, float* __restrict__ out,
+                                int nout, double dout, double oout, int ntr) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nout) return;
+    double x = (oout + (double)i * dout - oin) / din;
+    // sampling intervals arrive in single precision: a position within 1e-4 of
+    // an input node is that node (equal samplings copy, the last sample stays inside)
+    if (fabs(x - rint(x)) <= 1.0e-4) x = rint(x);
+    const bool inside = x >= 0.0 && x <= (double)(nin - 1);
+    const int j0 = inside ? (int)floor(x) : 0;
+    const float u = inside ? (float)(x - (double)j0) : 0.f;
+    const float u2 = u * u, u3 = u2 * u;
+    const float w0 = 0.5f * (-u3 + 2.f * u2 - u), w1 = 0.5f * (3.f * u3 - 5.f * u2 + 2.f);
+    const float w2 = 0.5f * (-3.f * u3 + 4.f * u2 + u), w3 = 0.5f * (u3 - u2);
+    const int ja = max(j0 - 1, 0), jb = j0, jc = min(j0 + 1, nin - 1), jd = min(j0 + 2, nin - 1);
+    for (int r = blockIdx.y; r < ntr; r += gridDim.y) {
+        const float* f = in + (size_t)r * nin;
+        out[(size_t)r * nout + i] = inside ? w0 * f[ja] + w1 * f[jb] + w2 * f[jc] + w3 * f[jd] : 0.f;
+    }
+}
+
+void launch_resample_rows(const float* in, int nin, double din, double oin, float* out, int nout, double dout,
+                          double oout, int ntr, cudaStream_t s) {
+    if (ntr <= 0 || nout <= 0) return;
+    dim3 g((nout + 255) / 256, std::min(ntr, 65535));
+    k_resample_rows<<<g, 256, 0, s>>>(in, nin, din, oin, out, nout, dout, oout, ntr);
+    OWL_LAUNCH_CHECK();
+}
+
 void launch_transpose_rec_to_seis(const float* rec, float* seis, int nt, int rtot, cudaStream_t s) {
     launch_transpose(rec, seis, nt, rtot, s);
 }

@@ -589,11 +589,10 @@ void SsgBase::forward(int nshots, const owl_shot* shots, const owl_run_opts& o, 
         OWL_CUDA(cudaMemsetAsync(rec.p, 0, sizeof(float) * nrt, stream));
         forward_batch(S, k, graph, false);
         if (o.check_every > 0) check_nonfinite(st.p, (size_t)S * sst);
-        const size_t n = (size_t)rtot * desc.nt;
+        const size_t n = (size_t)rtot * dnt();
         if (n) {
             seis_tmp.reserve(n);
-            launch_transpose_rec_to_seis(rec.p, seis_tmp.p, desc.nt, rtot, stream);
-            launches++;
+            syn_to_data(seis_tmp.p);
             copy_out(seis + out_off, seis_tmp.p, n * sizeof(float), mem);
         }
         out_off += n;
@@ -628,24 +627,39 @@ void SsgBase::misfit(int nshots, const owl_shot* shots, const float* obs, const 
         OWL_CUDA(cudaMemsetAsync(rec.p, 0, sizeof(float) * nrt, stream));
         forward_batch(S, k, graph, false);
         if (o.check_every > 0) check_nonfinite(st.p, (size_t)S * sst);
-        const size_t n = (size_t)rtot * desc.nt;
+        const int tn = dnt();
+        const size_t n = (size_t)rtot * tn;
         misfit_d.reserve(S);
         trace_d.reserve(std::max(rtot, 1));
+        obs_t.reserve(std::max(nrt, n));
         if (n) {
             seis_tmp.reserve(n);
             OWL_CUDA(cudaMemcpyAsync(seis_tmp.p, obs + data_off, n * sizeof(float),
                                      mem == OWL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
-            launch_transpose_seis_to_rec(seis_tmp.p, obs_t.p, desc.nt, rtot, stream);
+            launch_transpose_seis_to_rec(seis_tmp.p, obs_t.p, tn, rtot, stream);
             launches++;
         }
-        launch_trace_misfit(rec.p, obs_t.p, live.p, rec_shot_ptr.p, S, desc.nt, rtot, trace_d.p, misfit_d.p, stream);
+        const float* syn_i = rec.p;  // synthetics at the data sampling, (tn, rtot)
+        if (resampled() && n) {
+            dat_a.reserve(n);
+            dat_b.reserve(n);
+            syn_to_data(dat_a.p);
+            launch_transpose_seis_to_rec(dat_a.p, dat_b.p, tn, rtot, stream);
+            launches++;
+            syn_i = dat_b.p;
+        }
+        launch_trace_misfit(syn_i, obs_t.p, live.p, rec_shot_ptr.p, S, tn, rtot, trace_d.p, misfit_d.p, stream);
         launches += 2;
         if (misfit) copy_out(misfit + shot0, misfit_d.p, sizeof(double) * S, mem);
         if (trace_misfit && rtot) copy_out(trace_misfit + tr_off, trace_d.p, sizeof(double) * rtot, mem);
         if (seis_out && n) {
-            launch_transpose_rec_to_seis(rec.p, seis_tmp.p, desc.nt, rtot, stream);
-            launches++;
-            copy_out(seis_out + data_off, seis_tmp.p, n * sizeof(float), mem);
+            if (resampled()) {
+                copy_out(seis_out + data_off, dat_a.p, n * sizeof(float), mem);
+            } else {
+                launch_transpose_rec_to_seis(rec.p, seis_tmp.p, desc.nt, rtot, stream);
+                launches++;
+                copy_out(seis_out + data_off, seis_tmp.p, n * sizeof(float), mem);
+            }
         }
         OWL_CUDA(cudaStreamSynchronize(stream));
         data_off += n;
@@ -667,6 +681,69 @@ void SsgBase::fold_out(float* grad, int mem) {
     }
     OWL_LAUNCH_CHECK();
     copy_out(grad, seis_tmp.p, (size_t)nparam * nm * sizeof(float), mem);
+}
+
+void SsgBase::syn_to_data(float* out) {
+    if (!resampled()) {
+        launch_transpose_rec_to_seis(rec.p, out, desc.nt, rtot, stream);
+        launches++;
+        return;
+    }
+    syn_t.reserve((size_t)rtot * desc.nt);
+    launch_transpose_rec_to_seis(rec.p, syn_t.p, desc.nt, rtot, stream);
+    launch_resample_rows(syn_t.p, desc.nt, dt, 0.0, out, data_nt, data_dt, 0.0, rtot, stream);
+    launches += 2;
+}
+
+void SsgBase::data_to_res(const float* rows) {
+    if (!resampled()) {
+        launch_transpose_seis_to_rec(rows, res.p, desc.nt, rtot, stream);
+        launches++;
+        return;
+    }
+    adj_t.reserve((size_t)rtot * desc.nt);
+    launch_resample_rows(rows, data_nt, data_dt, 0.0, adj_t.p, desc.nt, dt, 0.0, rtot, stream);
+    launch_transpose_seis_to_rec(adj_t.p, res.p, desc.nt, rtot, stream);
+    launches += 2;
+}
+
+// Adjoint source of a batch whose data are sampled off the time axis, as the
+// reference orders it: synthetics resampled to the data sampling
+// (submodule_forward_modeling.f90:124-125), the adjoint source computed there,
+// and resampled back to the time axis before injection
+// (submodule_fwi_gradient.f90:46).
+void SsgBase::data_adjoint_source(const float* data, int adj_kind, int mem, int S, float* seis_out) {
+    const int tn = dnt();
+    const size_t n = (size_t)rtot * tn;
+    seis_tmp.reserve(n);
+    OWL_CUDA(cudaMemcpyAsync(seis_tmp.p, data, n * sizeof(float),
+                             mem == OWL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+    dat_a.reserve(n);
+    dat_b.reserve(n);
+    syn_to_data(dat_a.p);
+    if (adj_kind == OWL_ADJ_L2_RESIDUAL) {
+        obs_t.reserve(n);
+        syn_t.reserve(std::max(n, (size_t)rtot * desc.nt));
+        launch_transpose_seis_to_rec(seis_tmp.p, obs_t.p, tn, rtot, stream);
+        launch_transpose_seis_to_rec(dat_a.p, dat_b.p, tn, rtot, stream);
+        launch_residual_l2(dat_b.p, obs_t.p, syn_t.p, live.p, rec_shot_ptr.p, S, tn, rtot, misfit_d.p, stream);
+        launch_transpose_rec_to_seis(syn_t.p, dat_b.p, tn, rtot, stream);
+        launches += 4;
+        data_to_res(dat_b.p);
+    } else if (adj_kind == ADJ_MISFIT) {
+        owl_misfit_opts mo = mopts;
+        mo.dt = data_dt;
+        trace_d.reserve(std::max(rtot, 1));
+        adjsrc.launches = 0;
+        adjsrc.run(mo, (int)h_gather_ptr.size() - 1, h_gather_ptr.data(), tn, dat_a.p, seis_tmp.p, live.p, dat_b.p,
+                   trace_d.p, nullptr, stream);
+        launch_shot_misfit(trace_d.p, rec_shot_ptr.p, S, misfit_d.p, stream);
+        launches += adjsrc.launches + 1;
+        data_to_res(dat_b.p);
+    } else {
+        data_to_res(seis_tmp.p);
+    }
+    if (seis_out) copy_out(seis_out, dat_a.p, n * sizeof(float), mem);
 }
 
 void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data, int adj_kind, const owl_run_opts& o,
@@ -715,10 +792,12 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
         forward_batch(S, k, graph, true);
         if (o.check_every > 0) check_nonfinite(st.p, (size_t)S * sst);
         // 2. adjoint source and misfit
-        const size_t n = (size_t)rtot * nt;
+        const size_t n = (size_t)rtot * dnt();
         misfit_d.reserve(S);
         OWL_CUDA(cudaMemsetAsync(misfit_d.p, 0, sizeof(double) * S, stream));
-        if (n) {
+        if (n && resampled()) {
+            data_adjoint_source(data + data_off, adj_kind, mem, S, seis_out ? seis_out + data_off : nullptr);
+        } else if (n) {
             seis_tmp.reserve(n);
             OWL_CUDA(cudaMemcpyAsync(seis_tmp.p, data + data_off, n * sizeof(float),
                                      mem == OWL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));

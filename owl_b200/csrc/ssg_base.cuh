@@ -104,6 +104,16 @@ struct SsgBase : Engine {
     std::vector<int> h_gather_ptr;  // trace ranges of the (shot, component) gathers of the batch
     AdjointSource adjsrc;
     DevBuf<float> syn_t, adj_t;     // trace-major synthetics / adjoint source (data-domain misfits)
+    DevBuf<float> dat_a, dat_b;     // traces at the data sampling (resampled runs)
+    // seismograms at a sampling other than the time axis (resample_su, src/lib/module_su.f90:426-470)
+    bool resampled() const { return data_nt > 0 && (data_nt != desc.nt || data_dt != dt); }
+    int dnt() const { return data_nt > 0 ? data_nt : desc.nt; }
+    // synthetics of the batch (rec, (nt, rtot)) -> rows of dnt() samples at the data sampling
+    void syn_to_data(float* out);
+    // rows of dnt() samples at the data sampling -> adjoint source on the time axis in res ((nt, rtot))
+    void data_to_res(const float* rows);
+    // adjoint source of the batch from data at the data sampling (forward already run)
+    void data_adjoint_source(const float* data, int adj_kind, int mem, int S, float* seis_out);
 
     SsgBase(const owl_ssg_desc& d, int dim_);
     ~SsgBase() override;

@@ -82,6 +82,22 @@ class MisfitOpts:
         return o
 
 
+def resample_traces(rows, din: float, dout: float, nout: int, oin: float = 0.0, oout: float = 0.0):
+    """Cubic-convolution resampling of trace rows (ntr, nin) on the GPU
+    (owl_resample_traces); numpy in -> numpy out, CUDA tensor in -> CUDA tensor out."""
+    lib = L.load()
+    ntr, nin = int(rows.shape[0]), int(rows.shape[1])
+    if hasattr(rows, "is_cuda") and rows.is_cuda:
+        import torch
+        out = torch.empty((ntr, nout), dtype=torch.float32, device=rows.device)
+        _ready(rows, out)
+    else:
+        rows = np.ascontiguousarray(rows, dtype=f32)
+        out = np.empty((ntr, nout), dtype=f32)
+    L.check(lib.owl_resample_traces(ntr, nin, din, oin, _ptr(rows), nout, dout, oout, _ptr(out), _mem_kind(rows)))
+    return out
+
+
 def adjoint_source(mopts: MisfitOpts, gather_ptr, syn, obs, weight=None, adj=None, trace_misfit=None,
                    gather_misfit=None):
     """compute_adjoint_source on the GPU for traces given as rows (ntr, nt) of
@@ -158,6 +174,7 @@ class SSGSolver:
         self.ncomp = self.lib.owl_ssg_ncomp(medium)
         self.nparam = self.lib.owl_ssg_desc_nparam(C.byref(d))
         self.last_info = L.OwlRunInfo()
+        self.data_nt, self.data_dt = 0, 0.0
 
     def close(self):
         if getattr(self, "h", None):
@@ -195,13 +212,23 @@ class SSGSolver:
         return PreparedShots(shots, self.grid, self.desc.dt, f0factor,
                              0 if time_integration is None else time_integration)
 
+    def set_data_sampling(self, data_nt: int, data_dt: float) -> None:
+        """Traces in and out at data_nt samples of data_dt (data_nt <= 0: the time axis)."""
+        L.check(self.lib.owl_ssg_set_data_sampling(self.h, int(data_nt), float(data_dt)))
+        self.data_nt, self.data_dt = (int(data_nt), float(data_dt)) if data_nt > 0 else (0, 0.0)
+
+    @property
+    def trace_nt(self) -> int:
+        """samples per trace of the seismograms the solver takes and returns"""
+        return self.data_nt if self.data_nt > 0 else self.desc.nt
+
     def seis_size(self, ps: PreparedShots) -> int:
-        return sum(ps.nrec(s) for s in range(ps.nshots)) * self.ncomp * self.desc.nt
+        return sum(ps.nrec(s) for s in range(ps.nshots)) * self.ncomp * self.trace_nt
 
     def split(self, ps: PreparedShots, flat) -> List:
         """flat seismogram buffer -> per-shot (ncomp, nrec, nt) views"""
         out, off = [], 0
-        nt = self.desc.nt
+        nt = self.trace_nt
         for s in range(ps.nshots):
             n = ps.nrec(s) * self.ncomp * nt
             out.append(flat[off:off + n].reshape(self.ncomp, ps.nrec(s), nt))

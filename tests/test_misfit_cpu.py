@@ -105,3 +105,22 @@ def test_discard_rule():
     # a negative threshold keeps the tiny trace, not the zero one
     _, tm2, _ = M.adjoint_source(M.WAVEFORM, [0, 4], rows_s, rows_o, w, discard_threshold=-1.0)
     assert tm2[2] > 0 and tm2[3] == 0
+
+
+def test_resample_oracle_properties():
+    """cubic convolution: identity on the same sampling, exact for quadratics
+    away from the ends, linear in the data"""
+    import oracle.oracle_resample as R
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((3, 50))
+    assert np.allclose(R.resample_rows(x, 1e-3, 1e-3, 50), x, atol=0)
+    t_in = np.arange(50) * 2e-3
+    q = 1.0 + 3.0 * t_in - 40.0 * t_in ** 2
+    t_out = np.arange(120) * 0.7e-3
+    got = R.resample_rows(q, 2e-3, 0.7e-3, 120)[0]
+    inner = (t_out >= 2e-3) & (t_out <= 47 * 2e-3)
+    assert np.allclose(got[inner], (1.0 + 3.0 * t_out - 40.0 * t_out ** 2)[inner], atol=1e-12)
+    y = rng.standard_normal((3, 50))
+    a = R.resample_rows(2 * x - y, 1e-3, 2.5e-3, 20)
+    assert np.allclose(a, 2 * R.resample_rows(x, 1e-3, 2.5e-3, 20) - R.resample_rows(y, 1e-3, 2.5e-3, 20))
+    assert np.all(R.resample_rows(x, 1e-3, 1e-3, 60)[:, 50:] == 0)
