@@ -245,6 +245,41 @@ int owl_su_encode(int ntr, int ns, const unsigned char *header, const float *tra
                   int mem_kind);
 int owl_su_decode(int ntr, int ns, const unsigned char *in, float *traces, int mem_kind);
 
+/* ---- search directions and gradient processing ----------------------- */
+
+/* search_method (src/inverse/module_inversion_search_direction.f90) */
+#define OWL_SEARCH_SD 0    /* steepest descent: -g */
+#define OWL_SEARCH_CG 1    /* Polak-Ribiere conjugate gradient (:38-86) */
+#define OWL_SEARCH_LBFGS 2 /* two-loop L-BFGS (:91-246) */
+
+/* Search direction of one parameter field of n floats. models / grads: nm
+ * pointers each, oldest first, the last one the current iteration: the models
+ * the gradients were computed at (the reference's updated_<name>.bin of
+ * iterations k-nm+1 .. k, its <name>.bin at iteration 0) and those gradients.
+ * L-BFGS uses the nm - 1 newest pairs (the reference keeps nstep_lbfgs = 10);
+ * CG uses the last two gradients and prev_srch; nm = 1 (the first iteration)
+ * gives -g for every method. Dot products are FP64 sums in a fixed order.
+ * All arrays host (OWL_MEM_HOST) or device (OWL_MEM_DEVICE) memory. */
+int owl_search_direction(int method, long long n, int nm, const float *const *models, const float *const *grads,
+                         const float *prev_srch, float *srch, int mem_kind);
+
+/* gradient processing operations (process_model_single_parameter,
+ * src/inverse/2d/module_gradient.f90:733-892) on a field of n1 x n2 x n3
+ * floats, n1 fastest (z, then x, then y as OWL's model files):
+ *   OWL_GRAD_SMOOTH       Gaussian, param[0..2] = standard deviation in cells per axis (0: axis untouched)
+ *   OWL_GRAD_TAPER        Blackman ramps, param[0..5] = ramp lengths in cells (axis 1 start, end, axis 2 ...)
+ *   OWL_GRAD_MASK         multiply by mask (n1 x n2 x n3)
+ *   OWL_GRAD_SCALE        multiply by param[0]
+ *   OWL_GRAD_MAX_BALANCE  divide by the field's maximum when it is not 0
+ * param is host memory; field and mask host or device (mem_kind). */
+#define OWL_GRAD_SMOOTH 0
+#define OWL_GRAD_TAPER 1
+#define OWL_GRAD_MASK 2
+#define OWL_GRAD_SCALE 3
+#define OWL_GRAD_MAX_BALANCE 4
+int owl_grad_process(int op, int n1, int n2, int n3, const float *param, const float *mask, float *field,
+                     int mem_kind);
+
 /* Forward modelling of nshots shots (batched by opts->shots_per_launch).
  * Replaces compute_forward (src/solver/acoustic_iso_2d/submodule_forward_modeling.f90:31-132).
  * seis: per shot, ncomp x nrec x nt float32 (trace-major, the SU trace order),

@@ -172,7 +172,21 @@ EXPORTED = [
     "owl_ssg_dt_stable", "owl_ssg_nparam", "owl_ssg_ncomp", "owl_ssg_device_ok", "owl_ssg_kernel_time",
     "owl_ssg_forward_noalloc", "owl_ssg_desc_nparam", "owl_ssg_misfit", "owl_ssg_gradient_misfit",
     "owl_adjoint_source", "owl_ssg_set_data_sampling", "owl_resample_traces", "owl_su_encode", "owl_su_decode",
+    "owl_search_direction", "owl_grad_process",
 ]
+
+OWL_SEARCH_SD = 0
+OWL_SEARCH_CG = 1
+OWL_SEARCH_LBFGS = 2
+#: search_method names of the reference's parameter file
+SEARCH_NAMES = {"sd": OWL_SEARCH_SD, "steepest-descent": OWL_SEARCH_SD, "cg": OWL_SEARCH_CG,
+                "conjugate-gradient": OWL_SEARCH_CG, "l-bfgs": OWL_SEARCH_LBFGS}
+
+OWL_GRAD_SMOOTH = 0
+OWL_GRAD_TAPER = 1
+OWL_GRAD_MASK = 2
+OWL_GRAD_SCALE = 3
+OWL_GRAD_MAX_BALANCE = 4
 
 OWL_K_FWD_P = 0
 OWL_K_FWD_V = 1
@@ -228,11 +242,15 @@ def load() -> C.CDLL:
                                         C.c_float, C.c_void_p, C.c_int]
     lib.owl_su_encode.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     lib.owl_su_decode.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+    lib.owl_search_direction.argtypes = [C.c_int, C.c_longlong, C.c_int, P(C.c_void_p), P(C.c_void_p), C.c_void_p,
+                                         C.c_void_p, C.c_int]
+    lib.owl_grad_process.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_float), C.c_void_p, C.c_void_p,
+                                     C.c_int]
     for fn in ("owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
                "owl_ssg_source_gradient", "owl_ssg_abi_version", "owl_ssg_nparam", "owl_ssg_ncomp",
                "owl_ssg_device_ok", "owl_ssg_desc_nparam", "owl_ssg_misfit", "owl_ssg_gradient_misfit",
                "owl_adjoint_source", "owl_ssg_set_data_sampling", "owl_resample_traces", "owl_su_encode",
-               "owl_su_decode"):
+               "owl_su_decode", "owl_search_direction", "owl_grad_process"):
         getattr(lib, fn).restype = C.c_int
     _lib = lib
     return lib

@@ -272,6 +272,83 @@ int owl_su_decode(int ntr, int ns, const unsigned char* in, float* traces, int m
     });
 }
 
+int owl_search_direction(int method, long long n, int nm, const float* const* models, const float* const* grads,
+                         const float* prev_srch, float* srch, int mem_kind) {
+    return guarded([&] {
+        check_device();
+        OWL_CHECK(method >= OWL_SEARCH_SD && method <= OWL_SEARCH_LBFGS, OWL_ERR_INVALID, "bad search method");
+        OWL_CHECK(n >= 0 && nm >= 1 && models && grads && srch, OWL_ERR_INVALID, "bad search-direction arguments");
+        OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
+        for (int i = 0; i < nm; ++i) OWL_CHECK(grads[i] && (models[i] || method != OWL_SEARCH_LBFGS),
+                                                 OWL_ERR_INVALID, "null model / gradient");
+        if (n == 0) return;
+        struct Ctx {
+            cudaStream_t s = nullptr;
+            ~Ctx() {
+                if (s) cudaStreamDestroy(s);
+            }
+        } c;
+        OWL_CUDA(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+        std::vector<const float*> x(nm), g(nm);
+        const float* ps = prev_srch;
+        float* out = srch;
+        std::vector<std::unique_ptr<DevBuf<float>>> keep;
+        auto dev = [&](const float* h) -> const float* {
+            if (!h || mem_kind == OWL_MEM_DEVICE) return h;
+            keep.emplace_back(new DevBuf<float>());
+            keep.back()->upload(h, (size_t)n, c.s);
+            return keep.back()->p;
+        };
+        for (int i = 0; i < nm; ++i) {
+            x[i] = dev(models[i]);
+            g[i] = dev(grads[i]);
+        }
+        ps = dev(prev_srch);
+        DevBuf<float> dsrch;
+        if (mem_kind == OWL_MEM_HOST) {
+            dsrch.reserve((size_t)n);
+            out = dsrch.p;
+        }
+        search_direction(method, n, nm, x.data(), g.data(), ps, out, c.s);
+        if (mem_kind == OWL_MEM_HOST)
+            OWL_CUDA(cudaMemcpyAsync(srch, out, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, c.s));
+        OWL_CUDA(cudaStreamSynchronize(c.s));
+    });
+}
+
+int owl_grad_process(int op, int n1, int n2, int n3, const float* param, const float* mask, float* field,
+                     int mem_kind) {
+    return guarded([&] {
+        check_device();
+        OWL_CHECK(op >= OWL_GRAD_SMOOTH && op <= OWL_GRAD_MAX_BALANCE, OWL_ERR_INVALID, "bad gradient processing op");
+        OWL_CHECK(n1 >= 1 && n2 >= 1 && n3 >= 1 && field, OWL_ERR_INVALID, "bad field");
+        OWL_CHECK(param || op == OWL_GRAD_MASK || op == OWL_GRAD_MAX_BALANCE, OWL_ERR_INVALID, "null param");
+        OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
+        struct Ctx {
+            cudaStream_t s = nullptr;
+            ~Ctx() {
+                if (s) cudaStreamDestroy(s);
+            }
+        } c;
+        OWL_CUDA(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+        const size_t n = (size_t)n1 * n2 * n3;
+        DevBuf<float> df, dm;
+        float* f = field;
+        const float* m = mask;
+        if (mem_kind == OWL_MEM_HOST) {
+            df.upload(field, n, c.s);
+            f = df.p;
+            if (mask) {
+                dm.upload(mask, n, c.s);
+                m = dm.p;
+            }
+        }
+        grad_process(op, n1, n2, n3, param, m, f, c.s);
+        if (mem_kind == OWL_MEM_HOST) OWL_CUDA(cudaMemcpyAsync(field, f, n * sizeof(float), cudaMemcpyDeviceToHost, c.s));
+        OWL_CUDA(cudaStreamSynchronize(c.s));
+    });
+}
+
 int owl_adjoint_source(const owl_misfit_opts* mopts, int ngather, const int* gather_ptr, int nt, const float* syn,
                        const float* obs, const float* weight, float* adj, double* trace_misfit,
                        double* gather_misfit, int mem_kind) {

@@ -87,6 +87,10 @@ void launch_shot_misfit(const double* trace_misfit, const int* shot_rec_ptr, int
 void su_encode(const unsigned char* header, const float* traces, int ntr, int ns, unsigned char* out, bool dev,
                cudaStream_t s);
 void su_decode(const unsigned char* in, int ntr, int ns, float* traces, bool dev, cudaStream_t s);
+// search directions / gradient processing (optim.cu), device pointers
+void search_direction(int method, long long n, int nm, const float* const* x, const float* const* g,
+                      const float* prev_srch, float* srch, cudaStream_t s);
+void grad_process(int op, int n1, int n2, int n3, const float* param, const float* mask, float* f, cudaStream_t s);
 // out[i] = (w[i] != 0) (adjsrc.cu)
 void launch_nonzero(const float* w, int n, unsigned char* out, cudaStream_t s);
 
