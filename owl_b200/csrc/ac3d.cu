@@ -22,6 +22,10 @@
 
 #include "ssg_base.cuh"
 
+#ifndef OWL_AC3_ZCHUNK_MIN
+#define OWL_AC3_ZCHUNK_MIN 16  // shortest z chunk of a forward CTA
+#endif
+
 namespace owl {
 
 __constant__ float c_fd3[8];
@@ -643,7 +647,7 @@ struct Ac3dEngine : SsgBase {
     void pick_zchunk(int tyo) {
         const long long xy = (long long)((NXp + 31) / 32) * ((NYp + tyo - 1) / tyo);
         long long want = std::max<long long>(1, (148LL * 128 + xy - 1) / xy);
-        zchunk = (int)std::max<long long>(16, (NZp + want - 1) / want);
+        zchunk = (int)std::max<long long>(OWL_AC3_ZCHUNK_MIN, (NZp + want - 1) / want);
     }
 
     template <int RR, int RY>

@@ -10,7 +10,10 @@
 #pragma once
 // (no namespace block: ac3d.cu includes this inside namespace owl)
 
-constexpr int AC3_NS = 4;  // ring stages
+#ifndef OWL_AC3_STAGES
+#define OWL_AC3_STAGES 4
+#endif
+constexpr int AC3_NS = OWL_AC3_STAGES;  // ring stages
 
 __device__ __forceinline__ void cp16(void* smem, const void* gmem, bool pred) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -21,18 +24,34 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// copy a rows x (4*chunks) float tile starting at storage (x0, y0) of plane zo;
-// rows beyond NYs or chunks beyond the row pitch are zero-filled
+// The copies of a tile are the same on every plane but for the plane offset:
+// thread t owns elements e = t + 256 k of a ROWS x CH grid of 16-byte chunks,
+// stored at dst + 4 e. Their in-plane offsets (-1: outside the field, zero
+// fill) are computed once per CTA, so a plane costs one cp.async per element.
 template <int ROWS, int CH>
-__device__ __forceinline__ void cp_tile(float* dst, const float* src, long long zo, int x0, int y0, int pitch, int NYs) {
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    for (int e = tid; e < ROWS * CH; e += 256) {
-        const int r = e / CH, c = e - r * CH;
-        const int xx = x0 + 4 * c, yy = y0 + r;
-        const bool ok = yy >= 0 && yy < NYs && xx >= 0 && xx + 3 < pitch;
-        cp16(dst + r * (4 * CH) + 4 * c, ok ? src + zo + (long long)yy * pitch + xx : src, ok);
+struct TileSlots {
+    static constexpr int N = (ROWS * CH + 255) / 256;
+    int off[N];
+    __device__ __forceinline__ void init(int x0, int y0, int pitch, int NYs) {
+        const int tid = threadIdx.y * 32 + threadIdx.x;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const int e = tid + 256 * k;
+            const int r = e / CH, c = e - r * CH;
+            const int xx = x0 + 4 * c, yy = y0 + r;
+            const bool ok = e < ROWS * CH && yy >= 0 && yy < NYs && xx >= 0 && xx + 3 < pitch;
+            off[k] = ok ? yy * pitch + xx : -1;
+        }
     }
-}
+    __device__ __forceinline__ void copy(float* dst, const float* plane) const {
+        const int tid = threadIdx.y * 32 + threadIdx.x;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const int e = tid + 256 * k;
+            if (e < ROWS * CH) cp16(dst + 4 * e, off[k] >= 0 ? plane + off[k] : plane, off[k] >= 0);
+        }
+    }
+};
 
 template <int R, int RY>
 struct RingP {
@@ -66,6 +85,12 @@ __global__ void __launch_bounds__(256) k_ac3d_fwd_p(Ac3dDev a) {
         valid[r] = x < a.x1 && y < a.y1;
         oxy[r] = y * a.pitch + x;
     }
+    TileSlots<T::TYO, T::CHX> sx_;
+    TileSlots<T::TYO + 2 * R, 8> sy_;
+    TileSlots<T::TYO, 8> sc_;
+    sx_.init(bx0 - R, by0, a.pitch, a.NYs);
+    sy_.init(bx0, by0 - R, a.pitch, a.NYs);
+    sc_.init(bx0, by0, a.pitch, a.NYs);
     for (int s = s0; s < s1; ++s) {
         const long long so = s * a.sst;
         const float* vx = a.vx + so;
@@ -75,12 +100,12 @@ __global__ void __launch_bounds__(256) k_ac3d_fwd_p(Ac3dDev a) {
         auto issue = [&](int z, int stage) {
             float* st = ring + stage * T::STAGE;
             const long long zo = (long long)z * pl;
-            cp_tile<T::TYO, T::CHX>(st + T::OX, vx, zo, bx0 - R, by0, a.pitch, a.NYs);
-            cp_tile<T::TYO + 2 * R, 8>(st + T::OY, vy, zo, bx0, by0 - R, a.pitch, a.NYs);
+            sx_.copy(st + T::OX, vx + zo);
+            sy_.copy(st + T::OY, vy + zo);
             const long long za = (long long)min(z + 1 + R, a.NZs - 1) * pl;
-            cp_tile<T::TYO, 8>(st + T::OZ, vz, za, bx0, by0, a.pitch, a.NYs);
-            cp_tile<T::TYO, 8>(st + T::OP, pp, zo, bx0, by0, a.pitch, a.NYs);
-            cp_tile<T::TYO, 8>(st + T::OB, a.dtbk, zo, bx0, by0, a.pitch, a.NYs);
+            sc_.copy(st + T::OZ, vz + za);
+            sc_.copy(st + T::OP, pp + zo);
+            sc_.copy(st + T::OB, a.dtbk + zo);
         };
         float q[RY][2 * R];  // q[r][j] = vz(z - R + 1 + j)
 #pragma unroll
@@ -177,20 +202,24 @@ __global__ void __launch_bounds__(256) k_ac3d_fwd_v(Ac3dDev a) {
         valid[r] = x < a.x1 && y < a.y1;
         oxy[r] = y * a.pitch + x;
     }
+    TileSlots<T::HY, T::CHX> sp_;
+    TileSlots<T::TYO, 8> sc_;
+    sp_.init(bx0 - R, by0 - R, a.pitch, a.NYs);
+    sc_.init(bx0, by0, a.pitch, a.NYs);
     for (int s = s0; s < s1; ++s) {
         const long long so = s * a.sst;
         const float* p = a.p + so;
         auto issue = [&](int z, int stage) {
             float* st = ring + stage * T::STAGE;
             const long long zo = (long long)z * pl;
-            cp_tile<T::HY, T::CHX>(st + T::OP, p, zo, bx0 - R, by0 - R, a.pitch, a.NYs);
-            cp_tile<T::TYO, 8>(st + T::OQ, p, (long long)min(z + R, a.NZs - 1) * pl, bx0, by0, a.pitch, a.NYs);
-            cp_tile<T::TYO, 8>(st + T::OV, a.vx + so, zo, bx0, by0, a.pitch, a.NYs);
-            cp_tile<T::TYO, 8>(st + T::OV + T::TYO * 32, a.vy + so, zo, bx0, by0, a.pitch, a.NYs);
-            cp_tile<T::TYO, 8>(st + T::OV + 2 * T::TYO * 32, a.vz + so, zo, bx0, by0, a.pitch, a.NYs);
-            cp_tile<T::TYO, 8>(st + T::OV + 3 * T::TYO * 32, a.dtbx, zo, bx0, by0, a.pitch, a.NYs);
-            cp_tile<T::TYO, 8>(st + T::OV + 4 * T::TYO * 32, a.dtby, zo, bx0, by0, a.pitch, a.NYs);
-            cp_tile<T::TYO, 8>(st + T::OV + 5 * T::TYO * 32, a.dtbz, zo, bx0, by0, a.pitch, a.NYs);
+            sp_.copy(st + T::OP, p + zo);
+            sc_.copy(st + T::OQ, p + (long long)min(z + R, a.NZs - 1) * pl);
+            sc_.copy(st + T::OV, a.vx + so + zo);
+            sc_.copy(st + T::OV + T::TYO * 32, a.vy + so + zo);
+            sc_.copy(st + T::OV + 2 * T::TYO * 32, a.vz + so + zo);
+            sc_.copy(st + T::OV + 3 * T::TYO * 32, a.dtbx + zo);
+            sc_.copy(st + T::OV + 4 * T::TYO * 32, a.dtby + zo);
+            sc_.copy(st + T::OV + 5 * T::TYO * 32, a.dtbz + zo);
         };
         float q[RY][2 * R];  // q[r][j] = p(z - R + j)
 #pragma unroll
