@@ -51,6 +51,7 @@ __device__ __forceinline__ bool pml_half(int x, int pr, int n) { return x <= pr 
 // ------------------------------- forward ------------------------------------
 template <int R, bool STORE>
 __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
+    pdl_prologue();
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = a.zp0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
@@ -95,6 +96,7 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
 
 template <int R, bool STORE>
 __global__ void __launch_bounds__(512) k_ac2d_fwd_v(Ac2dDev a) {
+    pdl_prologue();
     const int zr0 = min(a.zvx0, a.zvz0);
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -159,6 +161,7 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_v(Ac2dDev a) {
 // outside a field's update range stay zero.
 template <int R>
 __global__ void __launch_bounds__(512) k_ac2d_adj_p(Ac2dDev a) {
+    pdl_prologue();
     const int zr0 = min(min(a.zvx0, a.zvz0), a.zp0);
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -225,6 +228,7 @@ __global__ void __launch_bounds__(512) k_ac2d_adj_p(Ac2dDev a) {
 
 template <int R>
 __global__ void __launch_bounds__(512) k_ac2d_adj_v(Ac2dDev a) {
+    pdl_prologue();
     const int zr0 = min(a.zvx0, a.zvz0);
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -486,17 +490,17 @@ struct Ac2dEngine : SsgBase {
             a.spt = spt_f;
             dim3 b(tile_x, tz_f);
             if (id == OWL_K_FWD_P) {
-                if (store) k_ac2d_fwd_p<RR, true><<<grid_for(rows_p, S, spt_f, tz_f), b, 0, stream>>>(a);
-                else k_ac2d_fwd_p<RR, false><<<grid_for(rows_p, S, spt_f, tz_f), b, 0, stream>>>(a);
+                if (store) launch_pdl(k_ac2d_fwd_p<RR, true>, grid_for(rows_p, S, spt_f, tz_f), b, 0, stream, a);
+                else launch_pdl(k_ac2d_fwd_p<RR, false>, grid_for(rows_p, S, spt_f, tz_f), b, 0, stream, a);
             } else {
-                if (store) k_ac2d_fwd_v<RR, true><<<grid_for(rows_v, S, spt_f, tz_f), b, 0, stream>>>(a);
-                else k_ac2d_fwd_v<RR, false><<<grid_for(rows_v, S, spt_f, tz_f), b, 0, stream>>>(a);
+                if (store) launch_pdl(k_ac2d_fwd_v<RR, true>, grid_for(rows_v, S, spt_f, tz_f), b, 0, stream, a);
+                else launch_pdl(k_ac2d_fwd_v<RR, false>, grid_for(rows_v, S, spt_f, tz_f), b, 0, stream, a);
             }
         } else {
             a.spt = spt_a;
             dim3 b(tile_x, tz_a);
-            if (id == OWL_K_ADJ_P) k_ac2d_adj_p<RR><<<grid_for(rows_a, S, spt_a, tz_a), b, 0, stream>>>(a);
-            else k_ac2d_adj_v<RR><<<grid_for(rows_v, S, spt_a, tz_a), b, 0, stream>>>(a);
+            if (id == OWL_K_ADJ_P) launch_pdl(k_ac2d_adj_p<RR>, grid_for(rows_a, S, spt_a, tz_a), b, 0, stream, a);
+            else launch_pdl(k_ac2d_adj_v<RR>, grid_for(rows_v, S, spt_a, tz_a), b, 0, stream, a);
         }
     }
     void launch_kernel(int id, int S, bool store) override {

@@ -43,6 +43,35 @@ void set_last_error(const std::string& msg);
 #define OWL_LAUNCH_CHECK() OWL_CUDA(cudaGetLastError())
 
 // ----------------------------------------------------------------------------
+// Programmatic dependent launch: a kernel launched with launch_pdl may start
+// while the kernel before it on the stream drains; it must call pdl_prologue()
+// before its first global read (griddepcontrol.wait returns once the previous
+// grid has completed and its writes are visible), and the call also lets the
+// next kernel be scheduled. OWL_NO_PDL=1 in the environment launches plainly.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_prologue() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+bool pdl_enabled();
+
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    OWL_CUDA(cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...));
+}
+
+// ----------------------------------------------------------------------------
 // grow-only device buffer. Keeping the pointer stable across calls lets the
 // captured CUDA graphs be replayed without re-instantiation.
 // ----------------------------------------------------------------------------

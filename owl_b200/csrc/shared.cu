@@ -4,7 +4,18 @@
 
 #include "engine.cuh"
 
+#include <cstdlib>
+
 namespace owl {
+
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("OWL_NO_PDL");
+        return !(e && e[0] == '1');
+    }();
+    return on;
+}
+
 
 int nint_f(float v) { return (int)std::lround(v); }
 

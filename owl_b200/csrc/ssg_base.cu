@@ -18,6 +18,7 @@ namespace owl {
 // (the sampling must see every injected tap). The last CTA to finish advances
 // the device step counter, so one captured graph serves every segment.
 __global__ void k_point_fwd(PointDev a, int mode) {
+    pdl_prologue();
     const int s = blockIdx.x;
     const int cur = *a.d_step;
     const int t = cur + 1;
@@ -53,6 +54,7 @@ __global__ void k_point_fwd(PointDev a, int mode) {
 // then the source-side adjoint taps . lambda_{t-1}; the last CTA steps back.
 // Same split as the forward when a shot has many target nodes.
 __global__ void k_point_adj(PointDev a, int mode) {
+    pdl_prologue();
     const int s = blockIdx.x;
     const int t = *a.d_step;
     if (mode & PA_SCATTER) {
@@ -88,10 +90,10 @@ __global__ void k_point_adj(PointDev a, int mode) {
 }
 
 void launch_point_fwd(const PointDev& q, int S, int nb, int mode, cudaStream_t s) {
-    k_point_fwd<<<dim3(S, nb), 256, 0, s>>>(q, mode);
+    launch_pdl(k_point_fwd, dim3(S, nb), dim3(256), 0, s, q, mode);
 }
 void launch_point_adj(const PointDev& q, int S, int nb, int mode, cudaStream_t s) {
-    k_point_adj<<<dim3(S, nb), 256, 0, s>>>(q, mode);
+    launch_pdl(k_point_adj, dim3(S, nb), dim3(256), 0, s, q, mode);
 }
 
 // ------------------------- compressed checkpoints ---------------------------
