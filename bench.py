@@ -42,6 +42,7 @@ def parse():
                    help="profiling target: one gradient step of --nshots shots, nothing else, no JSON line")
     p.add_argument("--no-3d", action="store_true", help="skip the 3D acoustic forward roofline block")
     p.add_argument("--no-misfits", action="store_true", help="skip the data-domain misfit block")
+    p.add_argument("--rows", type=int, default=1, help="rows per thread of the --profile3d forward kernels")
     p.add_argument("--profile3d", type=int, default=0, metavar="N",
                    help="profiling target: 12-step 3D acoustic forward of an N^3 model, no JSON line")
     p.add_argument("--no-elastic", action="store_true", help="skip the 2D elastic VTI block")
@@ -52,9 +53,9 @@ def parse():
     return p.parse_args()
 
 
-def profile_3d(n):
+def profile_3d(n, rows=1):
     """Small 3D forward for kernel captures: N^3 layered model, one shot, 12 steps,
-    forward tiles fixed at one row per thread (no autotuning launches)."""
+    forward tiles fixed at `rows` rows per thread (no autotuning launches)."""
     from owl_b200 import _lib as L
     from owl_b200 import configs
     from owl_b200.geometry import Receiver, Shot, Source
@@ -65,7 +66,7 @@ def profile_3d(n):
     shots = [Shot(1, [Source(x=c, y=c, z=20.0, f0=12.0)], [Receiver(x=20.0 * i, y=c, z=20.0) for i in range(n // 2)])]
     s = SSGSolver(L.OWL_ACOUSTIC_ISO_3D, n, n, 10.0, 10.0, 1e-3, 12, pml=20, f0_max=12.0, ny=n, dy=10.0)
     s.set_model(vp, rho)
-    s.forward(s.prepare(shots), RunOpts(shots_per_cta=1, tile_z=1, use_graph=-1))
+    s.forward(s.prepare(shots), RunOpts(shots_per_cta=1, tile_z=rows, use_graph=-1))
     print(f"profile3d: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
     s.close()
 
@@ -397,7 +398,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.profile3d:
-        return profile_3d(args.profile3d)
+        return profile_3d(args.profile3d, args.rows)
     if args.profile_el:
         return profile_elastic(args.profile_el)
     if args.profile_el3:
