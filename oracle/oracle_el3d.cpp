@@ -9,8 +9,13 @@
 //                                src/solver/elastic_vhtiort_3d/module_wavefield.f90:52-537
 //   add_source                   src/solver/elastic_vhtiort_3d/module_wavefield.f90:1095-1333
 //   sampling                     src/solver/elastic_vhtiort_3d/submodule_forward_modeling.f90:82-145
-// without a free surface, plus the exact discrete adjoint and the chain rule
-// to the model parameters. The M-PML damping ratios of the six faces are zero:
+//   update_wavefield_free_surface (flat free surface on the uniform grid,
+//   free_surface_dz_refine = 1): zero velocities above the surface, the row-1
+//   traction condition pdzvz = -c13/c33 pdxvx - c23/c33 pdyvy, sigma_zz(1) = 0
+//   and the odd stress images      module_wavefield.f90:549-1090
+//   surface images before sampling submodule_forward_modeling.f90:66-82
+//   sources above row 2 skipped    module_wavefield.f90:1107-1315
+// plus the exact discrete adjoint and the chain rule to the model parameters. The M-PML damping ratios of the six faces are zero:
 // that is the reference's value for the isotropic parameterisation
 // (module_cfspml.f90:448-465); for anisotropic media the reference derives them
 // from LAPACK eigenvectors of a 27 x 27 split-field system, which is not
@@ -113,6 +118,7 @@ enum { M_XVX = 0, M_YVY, M_ZVZ, M_ZVY, M_YVZ, M_ZVX, M_XVZ, M_YVX, M_XVY, M_XXX,
 template <typename T>
 struct El3 {
     int nx, ny, nz, P, R, nt, aniso, np;
+    bool fs;
     float dx, dy, dz, dt, idx, idy, idz;
     const float* c;
     E3<T> C[10];              // c11 c12 c13 c22 c23 c33 c44 c55 c66 rho, padded by pml+1
@@ -125,7 +131,7 @@ struct El3 {
     El3(const owl_ssg_desc& d, const T* const* fields) {
         nx = d.nx; ny = d.ny; nz = d.nz; P = d.pml; R = d.fdhalf; nt = d.nt; aniso = d.aniso;
         dx = d.dx; dy = d.dy; dz = d.dz; dt = d.dt;
-        if (d.free_surface) throw std::runtime_error("3D elastic free surface not restated");
+        fs = d.free_surface != 0;
         np = el3_nparam(aniso);
         if (np < 0) throw std::runtime_error("bad aniso");
         idx = (float)(1.0 / (double)dx); idy = (float)(1.0 / (double)dy); idz = (float)(1.0 / (double)dz);
@@ -244,10 +250,16 @@ struct El3 {
         return q + T(a) * u;
     }
 
+    // first z index a field is updated at: with a free surface, the nodes at
+    // integer depth from row 1, those at half depth (syz, sxz, vz) from row 2
+    int kmin(int f) const {
+        if (!fs) return -P + 1;
+        return (f == F_YZ || f == F_XZ || f == F_VZ) ? 2 : 1;
+    }
     template <class Fn>
-    void each(Fn fn) const {
+    void each(Fn fn, int k0) const {
 #pragma omp parallel for collapse(2) schedule(static)
-        for (int k = -P + 1; k <= nz + P; ++k)
+        for (int k = k0; k <= nz + P; ++k)
             for (int j = -P + 1; j <= ny + P; ++j)
                 for (int i = -P + 1; i <= nx + P; ++i) fn(i, j, k);
     }
@@ -255,22 +267,41 @@ struct El3 {
     // forward update; S (optional, 9 planes): Dx', Dy', Dz' at sigma nodes, the
     // shear sums at syz / sxz / sxy, the velocity sums at vx / vy / vz
     void update(El3State<T>& s, E3<T>* S) const {
-        // normal stresses (module_wavefield.f90:93-163)
+        if (fs) {
+            // particle velocities above the free surface are zero (module_wavefield.f90:582-593)
+            for (int q = 1; q <= R; ++q)
+                for (int j = lo[1]; j <= hi[1]; ++j)
+                    for (int i = lo[0]; i <= hi[0]; ++i) {
+                        s.f[F_VX](i, j, 1 - q) = T(0);
+                        s.f[F_VY](i, j, 1 - q) = T(0);
+                        s.f[F_VZ](i, j, 2 - q) = T(0);
+                    }
+        }
+        // normal stresses (module_wavefield.f90:93-163; free surface :602-711)
         each([&](int i, int j, int k) {
             const float fdt = dt;
-            T dX = T(idx) * stP(s.f[F_VX], i, j, k, 0), dY = T(idy) * stP(s.f[F_VY], i, j, k, 1),
-              dZ = T(idz) * stP(s.f[F_VZ], i, j, k, 2);
-            if (shell(i, j, k, false, false, false)) {
-                float ca, cb;
-                coef(0, i, false, ca, cb); dX = pml_f(dX, ca, cb, s.m[M_XVX](i, j, k));
-                coef(1, j, false, ca, cb); dY = pml_f(dY, ca, cb, s.m[M_YVY](i, j, k));
-                coef(2, k, false, ca, cb); dZ = pml_f(dZ, ca, cb, s.m[M_ZVZ](i, j, k));
+            T dX = T(idx) * stP(s.f[F_VX], i, j, k, 0), dY = T(idy) * stP(s.f[F_VY], i, j, k, 1), dZ;
+            if (fs && k == 1) {
+                if (i <= 0 || i >= nx + 1 || j <= 0 || j >= ny + 1) {
+                    float ca, cb;
+                    coef(0, i, false, ca, cb); dX = pml_f(dX, ca, cb, s.m[M_XVX](i, j, k));
+                    coef(1, j, false, ca, cb); dY = pml_f(dY, ca, cb, s.m[M_YVY](i, j, k));
+                }
+                dZ = -(C[2](i, j, k) / C[5](i, j, k)) * dX - (C[4](i, j, k) / C[5](i, j, k)) * dY;
+            } else {
+                dZ = T(idz) * stP(s.f[F_VZ], i, j, k, 2);
+                if (shell(i, j, k, false, false, false)) {
+                    float ca, cb;
+                    coef(0, i, false, ca, cb); dX = pml_f(dX, ca, cb, s.m[M_XVX](i, j, k));
+                    coef(1, j, false, ca, cb); dY = pml_f(dY, ca, cb, s.m[M_YVY](i, j, k));
+                    coef(2, k, false, ca, cb); dZ = pml_f(dZ, ca, cb, s.m[M_ZVZ](i, j, k));
+                }
             }
             s.f[F_XX](i, j, k) = s.f[F_XX](i, j, k) + T(fdt) * (C[0](i, j, k) * dX + C[1](i, j, k) * dY + C[2](i, j, k) * dZ);
             s.f[F_YY](i, j, k) = s.f[F_YY](i, j, k) + T(fdt) * (C[1](i, j, k) * dX + C[3](i, j, k) * dY + C[4](i, j, k) * dZ);
             s.f[F_ZZ](i, j, k) = s.f[F_ZZ](i, j, k) + T(fdt) * (C[2](i, j, k) * dX + C[4](i, j, k) * dY + C[5](i, j, k) * dZ);
             if (S) { S[0](i, j, k) = dX; S[1](i, j, k) = dY; S[2](i, j, k) = dZ; }
-        });
+        }, kmin(F_XX));
         // syz at (i, j-1/2, k-1/2) (:171-221)
         each([&](int i, int n, int p) {
             T dzvy = T(idz) * stM(s.f[F_VY], i, n, p, 2), dyvz = T(idy) * stM(s.f[F_VZ], i, n, p, 1);
@@ -281,7 +312,7 @@ struct El3 {
             }
             s.f[F_YZ](i, n, p) = s.f[F_YZ](i, n, p) + T(dt) * c44e(i, n, p) * (dzvy + dyvz);
             if (S) S[3](i, n, p) = dzvy + dyvz;
-        });
+        }, kmin(F_YZ));
         // sxz at (i-1/2, j, k-1/2) (:228-278)
         each([&](int m, int j, int p) {
             T dzvx = T(idz) * stM(s.f[F_VX], m, j, p, 2), dxvz = T(idx) * stM(s.f[F_VZ], m, j, p, 0);
@@ -292,7 +323,7 @@ struct El3 {
             }
             s.f[F_XZ](m, j, p) = s.f[F_XZ](m, j, p) + T(dt) * c55e(m, j, p) * (dzvx + dxvz);
             if (S) S[4](m, j, p) = dzvx + dxvz;
-        });
+        }, kmin(F_XZ));
         // sxy at (i-1/2, j-1/2, k) (:285-335)
         each([&](int m, int n, int k) {
             T dyvx = T(idy) * stM(s.f[F_VX], m, n, k, 1), dxvy = T(idx) * stM(s.f[F_VY], m, n, k, 0);
@@ -303,7 +334,22 @@ struct El3 {
             }
             s.f[F_XY](m, n, k) = s.f[F_XY](m, n, k) + T(dt) * c66e(m, n, k) * (dyvx + dxvy);
             if (S) S[5](m, n, k) = dyvx + dxvy;
-        });
+        }, kmin(F_XY));
+        if (fs) {
+            // stress images (module_wavefield.f90:871-903): odd about row 1 for the
+            // integer-depth stresses, sigma_zz(1) = 0, odd about row 3/2 for syz, sxz
+            for (int q = 1; q <= R; ++q)
+                for (int j = lo[1]; j <= hi[1]; ++j)
+                    for (int i = lo[0]; i <= hi[0]; ++i) {
+                        s.f[F_ZZ](i, j, 1 - q) = -s.f[F_ZZ](i, j, 1 + q);
+                        s.f[F_ZZ](i, j, 1) = T(0);
+                        s.f[F_XX](i, j, 1 - q) = -s.f[F_XX](i, j, 1 + q);
+                        s.f[F_YY](i, j, 1 - q) = -s.f[F_YY](i, j, 1 + q);
+                        s.f[F_XY](i, j, 1 - q) = -s.f[F_XY](i, j, 1 + q);
+                        s.f[F_YZ](i, j, 2 - q) = -s.f[F_YZ](i, j, 1 + q);
+                        s.f[F_XZ](i, j, 2 - q) = -s.f[F_XZ](i, j, 1 + q);
+                    }
+        }
         // vx at (i-1/2, j, k) (:350-410)
         each([&](int m, int j, int k) {
             T hx = T(idx) * stM(s.f[F_XX], m, j, k, 0), hy = T(idy) * stP(s.f[F_XY], m, j, k, 1),
@@ -317,7 +363,7 @@ struct El3 {
             const T re = T(0.5f) * (C[9](m - 1, j, k) + C[9](m, j, k));
             s.f[F_VX](m, j, k) = s.f[F_VX](m, j, k) + T(dt) / re * (hx + hy + hz);
             if (S) S[6](m, j, k) = hx + hy + hz;
-        });
+        }, kmin(F_VX));
         // vy at (i, j-1/2, k) (:416-476)
         each([&](int i, int n, int k) {
             T hx = T(idx) * stP(s.f[F_XY], i, n, k, 0), hy = T(idy) * stM(s.f[F_YY], i, n, k, 1),
@@ -331,7 +377,7 @@ struct El3 {
             const T re = T(0.5f) * (C[9](i, n - 1, k) + C[9](i, n, k));
             s.f[F_VY](i, n, k) = s.f[F_VY](i, n, k) + T(dt) / re * (hx + hy + hz);
             if (S) S[7](i, n, k) = hx + hy + hz;
-        });
+        }, kmin(F_VY));
         // vz at (i, j, k-1/2) (:482-542)
         each([&](int i, int j, int p) {
             T hx = T(idx) * stP(s.f[F_XZ], i, j, p, 0), hy = T(idy) * stP(s.f[F_YZ], i, j, p, 1),
@@ -345,7 +391,7 @@ struct El3 {
             const T re = T(0.5f) * (C[9](i, j, p - 1) + C[9](i, j, p));
             s.f[F_VZ](i, j, p) = s.f[F_VZ](i, j, p) + T(dt) / re * (hx + hy + hz);
             if (S) S[8](i, j, p) = hx + hy + hz;
-        });
+        }, kmin(F_VZ));
     }
 
     // source taps of one source: (field, i, j, k, weight without the STF amplitude)
@@ -380,6 +426,23 @@ struct El3 {
                             out.emplace_back(F_YZ, q.gx + irx, q.hy + iry, q.hz + irz, -inv * T(q.mt[5]) * T(ix[a]) * T(hy[b]) * T(hz[cc]));
                         }
                     }
+                }
+        // with a free surface, no source tap above row 2 (module_wavefield.f90:1147-1315)
+        if (fs)
+            out.erase(std::remove_if(out.begin(), out.end(), [](const std::tuple<int, int, int, int, T>& tp) {
+                          return std::get<3>(tp) < 2;
+                      }), out.end());
+    }
+
+    // surface images of the velocities before sampling (submodule_forward_modeling.f90:66-82),
+    // over the interpolation half-width nkw = 4 (module_source_receiver.f90:146)
+    void images(El3State<T>& s) const {
+        for (int q = 1; q <= 4; ++q)
+            for (int j = lo[1]; j <= hi[1]; ++j)
+                for (int i = lo[0]; i <= hi[0]; ++i) {
+                    s.f[F_VX](i, j, 1 - q) = s.f[F_VX](i, j, 1 + q);
+                    s.f[F_VY](i, j, 1 - q) = s.f[F_VY](i, j, 1 + q);
+                    s.f[F_VZ](i, j, 2 - q) = s.f[F_VZ](i, j, 1 + q);
                 }
     }
 
@@ -427,6 +490,7 @@ struct El3 {
         std::fill(seis, seis + (size_t)3 * sh.nrec * nt, T(0));
         for (int t = 1; t <= nt; ++t) {
             if (ckpt && (t - 1) % k == 0) ckpt->push_back(s);
+            if (fs) images(s);
             sample(t, sh, s, seis);
             update(s, nullptr);
             add_source(t, sh, s);
@@ -476,14 +540,17 @@ struct El3 {
             }
             return std::array<T, 3>{T(idx) * ex, T(idy) * ey, T(idz) * ez};
         };
-        for (int k = -P + 1; k <= nz + P; ++k)
+        for (int k = kmin(F_VX); k <= nz + P; ++k)
             for (int j = -P + 1; j <= ny + P; ++j)
                 for (int i = -P + 1; i <= nx + P; ++i) {
-                    // vz (i, j, k-1/2): reads sxz (P,x), syz (P,y), szz (M,z)
-                    auto e = vrev(F_VZ, i, j, k, 0, 0, 1, 8, S, false, false, true, M_XXZ, M_YYZ, M_ZZZ);
-                    scP(a.f[F_XZ], i, j, k, 0, e[0]);
-                    scP(a.f[F_YZ], i, j, k, 1, e[1]);
-                    scM(a.f[F_ZZ], i, j, k, 2, e[2]);
+                    std::array<T, 3> e;
+                    if (k >= kmin(F_VZ)) {
+                        // vz (i, j, k-1/2): reads sxz (P,x), syz (P,y), szz (M,z)
+                        e = vrev(F_VZ, i, j, k, 0, 0, 1, 8, S, false, false, true, M_XXZ, M_YYZ, M_ZZZ);
+                        scP(a.f[F_XZ], i, j, k, 0, e[0]);
+                        scP(a.f[F_YZ], i, j, k, 1, e[1]);
+                        scM(a.f[F_ZZ], i, j, k, 2, e[2]);
+                    }
                     // vy (i, j-1/2, k): sxy (P,x), syy (M,y), syz (P,z)
                     e = vrev(F_VY, i, j, k, 0, 1, 0, 7, S, false, true, false, M_XXY, M_YYY, M_ZYZ);
                     scP(a.f[F_XY], i, j, k, 0, e[0]);
@@ -495,6 +562,23 @@ struct El3 {
                     scP(a.f[F_XY], i, j, k, 1, e[1]);
                     scP(a.f[F_XZ], i, j, k, 2, e[2]);
                 }
+        if (fs) {
+            // reverse the stress images and sigma_zz(1) = 0: an image's adjoint
+            // folds onto the row it copies, with the image's sign
+            for (int q = R; q >= 1; --q)
+                for (int j = lo[1]; j <= hi[1]; ++j)
+                    for (int i = lo[0]; i <= hi[0]; ++i) {
+                        for (int f : {F_YZ, F_XZ}) {
+                            a.f[f](i, j, 1 + q) = a.f[f](i, j, 1 + q) - a.f[f](i, j, 2 - q);
+                            a.f[f](i, j, 2 - q) = T(0);
+                        }
+                        a.f[F_ZZ](i, j, 1) = T(0);
+                        for (int f : {F_ZZ, F_XX, F_YY, F_XY}) {
+                            a.f[f](i, j, 1 + q) = a.f[f](i, j, 1 + q) - a.f[f](i, j, 1 - q);
+                            a.f[f](i, j, 1 - q) = T(0);
+                        }
+                    }
+        }
         // reverse the shear updates; c_e = 4 / sum(1 / c) over the 4 cells
         auto shear = [&](int fs, E3<T>& ce, int cq, int i, int j, int k, int si, const int (&cells)[4][3], int ax1, int ax2,
                          bool h1, bool h2, int m1, int m2, int fa, int fb) {
@@ -521,26 +605,49 @@ struct El3 {
             scM(a.f[fa], i, j, k, ax1, T(id[ax1]) * e1);
             scM(a.f[fb], i, j, k, ax2, T(id[ax2]) * e2);
         };
-        for (int k = -P + 1; k <= nz + P; ++k)
+        for (int k = kmin(F_XY); k <= nz + P; ++k)
             for (int j = -P + 1; j <= ny + P; ++j)
                 for (int i = -P + 1; i <= nx + P; ++i) {
+                    if (k >= kmin(F_YZ)) {
                     // syz (i, n, p): dt c44e (Dz vy + Dy vz)
                     { const int cl[4][3] = {{i, j - 1, k - 1}, {i, j, k - 1}, {i, j - 1, k}, {i, j, k}};
                       shear(F_YZ, const_cast<E3<T>&>(c44e), 6, i, j, k, 3, cl, 2, 1, true, true, M_ZVY, M_YVZ, F_VY, F_VZ); }
                     // sxz (m, j, p): dt c55e (Dz vx + Dx vz)
                     { const int cl[4][3] = {{i - 1, j, k - 1}, {i, j, k - 1}, {i - 1, j, k}, {i, j, k}};
                       shear(F_XZ, const_cast<E3<T>&>(c55e), 7, i, j, k, 4, cl, 2, 0, true, true, M_ZVX, M_XVZ, F_VX, F_VZ); }
+                    }
                     // sxy (m, n, k): dt c66e (Dy vx + Dx vy)
                     { const int cl[4][3] = {{i - 1, j - 1, k}, {i, j - 1, k}, {i - 1, j, k}, {i, j, k}};
                       shear(F_XY, const_cast<E3<T>&>(c66e), 8, i, j, k, 5, cl, 1, 0, true, true, M_YVX, M_XVY, F_VX, F_VY); }
                 }
         // reverse the normal-stress update
-        for (int k = -P + 1; k <= nz + P; ++k)
+        for (int k = kmin(F_XX); k <= nz + P; ++k)
             for (int j = -P + 1; j <= ny + P; ++j)
                 for (int i = -P + 1; i <= nx + P; ++i) {
                     const T xh = a.f[F_XX](i, j, k), yh = a.f[F_YY](i, j, k), zh = a.f[F_ZZ](i, j, k);
                     const T dX = S[0](i, j, k), dY = S[1](i, j, k), dZ = S[2](i, j, k);
                     const T tt = T(dt);
+                    if (fs && k == 1) {
+                        // row 1: dZ = -(c13 dX + c23 dY) / c33 and sigma_zz(1) overwritten by 0
+                        const T r13 = C[2](i, j, k) / C[5](i, j, k), r23 = C[4](i, j, k) / C[5](i, j, k);
+                        g.g[0](i, j, k) = g.g[0](i, j, k) + tt * xh * dX;
+                        g.g[1](i, j, k) = g.g[1](i, j, k) + tt * (xh * dY + yh * dX);
+                        g.g[2](i, j, k) = g.g[2](i, j, k) + tt * (xh * (dZ - r13 * dX) - yh * r23 * dX);
+                        g.g[3](i, j, k) = g.g[3](i, j, k) + tt * yh * dY;
+                        g.g[4](i, j, k) = g.g[4](i, j, k) + tt * (yh * (dZ - r23 * dY) - xh * r13 * dY);
+                        g.g[5](i, j, k) = g.g[5](i, j, k) - tt * (xh * r13 + yh * r23) * dZ;
+                        const T w = tt * (C[2](i, j, k) * xh + C[4](i, j, k) * yh);
+                        T qx = tt * (C[0](i, j, k) * xh + C[1](i, j, k) * yh) - r13 * w;
+                        T qy = tt * (C[1](i, j, k) * xh + C[3](i, j, k) * yh) - r23 * w;
+                        if (i <= 0 || i >= nx + 1 || j <= 0 || j >= ny + 1) {
+                            float ca, cb;
+                            coef(0, i, false, ca, cb); qx = pml_e(qx, ca, cb, a.m[M_XVX](i, j, k));
+                            coef(1, j, false, ca, cb); qy = pml_e(qy, ca, cb, a.m[M_YVY](i, j, k));
+                        }
+                        scP(a.f[F_VX], i, j, k, 0, T(idx) * qx);
+                        scP(a.f[F_VY], i, j, k, 1, T(idy) * qy);
+                        continue;
+                    }
                     g.g[0](i, j, k) = g.g[0](i, j, k) + tt * xh * dX;
                     g.g[1](i, j, k) = g.g[1](i, j, k) + tt * (xh * dY + yh * dX);
                     g.g[2](i, j, k) = g.g[2](i, j, k) + tt * (xh * dZ + zh * dX);
@@ -579,6 +686,19 @@ struct El3 {
                         v2 = v2 + r2 * T(q.interp_ix[a0]) * T(q.interp_iy[b0]) * T(q.interp_hz[c0]) * T(q.weight);
                     }
         }
+        if (fs) {
+            // the sampled images fold onto the rows they copy
+            for (int q = 4; q >= 1; --q)
+                for (int j = lo[1]; j <= hi[1]; ++j)
+                    for (int i = lo[0]; i <= hi[0]; ++i) {
+                        a.f[F_VX](i, j, 1 + q) = a.f[F_VX](i, j, 1 + q) + a.f[F_VX](i, j, 1 - q);
+                        a.f[F_VX](i, j, 1 - q) = T(0);
+                        a.f[F_VY](i, j, 1 + q) = a.f[F_VY](i, j, 1 + q) + a.f[F_VY](i, j, 1 - q);
+                        a.f[F_VY](i, j, 1 - q) = T(0);
+                        a.f[F_VZ](i, j, 1 + q) = a.f[F_VZ](i, j, 1 + q) + a.f[F_VZ](i, j, 2 - q);
+                        a.f[F_VZ](i, j, 2 - q) = T(0);
+                    }
+        }
         clear_outside(a);
     }
 
@@ -588,7 +708,8 @@ struct El3 {
             for (int k = lo[2]; k <= hi[2]; ++k)
                 for (int j = lo[1]; j <= hi[1]; ++j)
                     for (int i = lo[0]; i <= hi[0]; ++i) {
-                        const bool in = i >= -P + 1 && i <= nx + P && j >= -P + 1 && j <= ny + P && k >= -P + 1 && k <= nz + P;
+                        const bool in = i >= -P + 1 && i <= nx + P && j >= -P + 1 && j <= ny + P && k >= kmin(q) &&
+                                        k <= nz + P;
                         if (!in) f(i, j, k) = T(0);
                     }
         }
@@ -607,6 +728,7 @@ struct El3 {
             const int n0 = sg * k, n1 = std::min(nt, n0 + k);
             El3State<T> s = ck[sg];
             for (int t = n0 + 1; t <= n1; ++t) {
+                if (fs) images(s);
                 update(s, Sbuf[t - n0 - 1].data());
                 add_source(t, sh, s);
             }

@@ -3,7 +3,12 @@
 // Forward (replaces update_wavefield, add_source and the sampling of
 // compute_forward, src/solver/elastic_vhtiort_3d/module_wavefield.f90:52-537,
 // :1095-1333 and submodule_forward_modeling.f90:82-145) without a free surface,
-// and the exact discrete adjoint with every-k-step checkpoints, Kahan FP32
+// with or without a flat free surface on the uniform grid
+// (update_wavefield_free_surface, module_wavefield.f90:549-1090: zero velocities
+// above the surface, the traction condition pdzvz = -c13/c33 pdxvx - c23/c33
+// pdyvy at row 1, sigma_zz(1) = 0 and odd images of sigma_zz, sigma_yz,
+// sigma_xz; the images of sigma_xx, sigma_yy, sigma_xy are never read and are
+// not stored), and the exact discrete adjoint with every-k-step checkpoints, Kahan FP32
 // correlations for the nine Cij and the three buoyancies, and the FP64 chain
 // rule to the model parameters (replaces compute_adjoint / compute_gradient,
 // submodule_fwi_gradient.f90).
@@ -12,6 +17,10 @@
 // normal stresses at (i, j, k); syz at (i, j-1/2, k-1/2); sxz at (i-1/2, j,
 // k-1/2); sxy at (i-1/2, j-1/2, k); vx at (i-1/2, j, k); vy at (i, j-1/2, k);
 // vz at (i, j, k-1/2). State per shot: 9 fields + 18 CFS-MPML memory volumes.
+// With a free surface, the integer-depth nodes are updated from row 1 and the
+// half-depth ones (syz, sxz, vz) from row 2; velocity taps of the receivers on
+// the surface images (vx, vy (1-k) = (1+k), vz (2-k) = (1+k), k <= 4) are
+// mapped onto the rows they copy.
 //
 // Damping. The reference damps a derivative along axis a of a node in the PML
 // shell with d = d_a(pos_a) + sum of ratio * d_b(pos_b) over the other axes
@@ -44,7 +53,7 @@ constexpr int E3_NAD = 9 + 18 + 18;
 struct El3dDev {
     int nx, ny, nz, P, R, pr, pitch;
     long long plane, fs, sst, sad;
-    int x0, x1, y0, y1, z0, z1, nzb;
+    int x0, x1, y0, y1, z0, z1, nzb, fsurf;
     float idx, idy, idz, dt;
     int nshots, spt;
     const float *c11, *c12, *c13, *c22, *c23, *c33, *c44e, *c55e, *c66e, *bx, *by, *bz;
@@ -120,7 +129,7 @@ __device__ __forceinline__ bool e3_cell(const El3dDev& a, E3Cell& c) {
 }
 
 // ------------------------------- forward ------------------------------------
-template <int R, bool STORE>
+template <int R, bool STORE, bool FS>
 __global__ void __launch_bounds__(256) k_el3d_fwd_s(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
@@ -139,35 +148,62 @@ __global__ void __launch_bounds__(256) k_el3d_fwd_s(El3dDev a) {
     const float g44 = a.dt * __ldg(a.c44e + o), g55 = a.dt * __ldg(a.c55e + o), g66 = a.dt * __ldg(a.c66e + o);
     const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
+    // free surface: row 1, whether the half-depth stresses exist at this row,
+    // and the image rows of sigma_zz (2 pr - z) and of syz / sxz (2 pr + 1 - z)
+    const bool row1 = FS && z == a.pr, hz_ok = !FS || z > a.pr;
+    const bool mir = FS && z > a.pr && z <= a.pr + a.R;
+    const long long dzz = (long long)(2 * a.pr - 2 * z) * sz, dsh = dzz + sz;
     for (int s = s0; s < s1; ++s) {
         float* st = a.st + s * a.sst;
         const float* vx = st + E3_VX * a.fs + o;
         const float* vy = st + E3_VY * a.fs + o;
         const float* vz = st + E3_VZ * a.fs + o;
         float* m = st + E3_M0 * a.fs + o;
-        float dX = a.idx * stP<R>(vx, 1), dY = a.idy * stP<R>(vy, sy), dZ = a.idz * stP<R>(vz, sz);
-        if (sh_n) {
+        float dX = a.idx * stP<R>(vx, 1), dY = a.idy * stP<R>(vy, sy), dZ;
+        if (row1) {
             if (axi != 0.f) dX = pml_fw(dX, axi, bxi, m + N_XVX * a.fs);
             if (ayi != 0.f) dY = pml_fw(dY, ayi, byi, m + N_YVY * a.fs);
-            if (azi != 0.f) dZ = pml_fw(dZ, azi, bzi, m + N_ZVZ * a.fs);
+            dZ = -(c13 / c33) * dX - (c23 / c33) * dY;
+        } else {
+            dZ = a.idz * stP<R>(vz, sz);
+            if (sh_n) {
+                if (axi != 0.f) dX = pml_fw(dX, axi, bxi, m + N_XVX * a.fs);
+                if (ayi != 0.f) dY = pml_fw(dY, ayi, byi, m + N_YVY * a.fs);
+                if (azi != 0.f) dZ = pml_fw(dZ, azi, bzi, m + N_ZVZ * a.fs);
+            }
         }
         st[E3_XX * a.fs + o] += a.dt * (c11 * dX + c12 * dY + c13 * dZ);
         st[E3_YY * a.fs + o] += a.dt * (c12 * dX + c22 * dY + c23 * dZ);
-        st[E3_ZZ * a.fs + o] += a.dt * (c13 * dX + c23 * dY + c33 * dZ);
-        // syz: dz vy + dy vz
-        float dzvy = a.idz * stM<R>(vy, sz), dyvz = a.idy * stM<R>(vz, sy);
-        if (sh_yz) {
-            if (ayh != 0.f) dyvz = pml_fw(dyvz, ayh, byh, m + N_YVZ * a.fs);
-            if (azh != 0.f) dzvy = pml_fw(dzvy, azh, bzh, m + N_ZVY * a.fs);
+        if (row1) {
+            st[E3_ZZ * a.fs + o] = 0.f;
+        } else {
+            const float zn = st[E3_ZZ * a.fs + o] + a.dt * (c13 * dX + c23 * dY + c33 * dZ);
+            st[E3_ZZ * a.fs + o] = zn;
+            if (mir) st[E3_ZZ * a.fs + o + dzz] = -zn;
         }
-        st[E3_YZ * a.fs + o] += g44 * (dzvy + dyvz);
-        // sxz: dz vx + dx vz
-        float dzvx = a.idz * stM<R>(vx, sz), dxvz = a.idx * stM<R>(vz, 1);
-        if (sh_xz) {
-            if (axh != 0.f) dxvz = pml_fw(dxvz, axh, bxh, m + N_XVZ * a.fs);
-            if (azh != 0.f) dzvx = pml_fw(dzvx, azh, bzh, m + N_ZVX * a.fs);
+        float dzvy = 0.f, dyvz = 0.f, dzvx = 0.f, dxvz = 0.f;
+        if (hz_ok) {
+            // syz: dz vy + dy vz
+            dzvy = a.idz * stM<R>(vy, sz);
+            dyvz = a.idy * stM<R>(vz, sy);
+            if (sh_yz) {
+                if (ayh != 0.f) dyvz = pml_fw(dyvz, ayh, byh, m + N_YVZ * a.fs);
+                if (azh != 0.f) dzvy = pml_fw(dzvy, azh, bzh, m + N_ZVY * a.fs);
+            }
+            const float yzn = st[E3_YZ * a.fs + o] + g44 * (dzvy + dyvz);
+            st[E3_YZ * a.fs + o] = yzn;
+            if (mir) st[E3_YZ * a.fs + o + dsh] = -yzn;
+            // sxz: dz vx + dx vz
+            dzvx = a.idz * stM<R>(vx, sz);
+            dxvz = a.idx * stM<R>(vz, 1);
+            if (sh_xz) {
+                if (axh != 0.f) dxvz = pml_fw(dxvz, axh, bxh, m + N_XVZ * a.fs);
+                if (azh != 0.f) dzvx = pml_fw(dzvx, azh, bzh, m + N_ZVX * a.fs);
+            }
+            const float xzn = st[E3_XZ * a.fs + o] + g55 * (dzvx + dxvz);
+            st[E3_XZ * a.fs + o] = xzn;
+            if (mir) st[E3_XZ * a.fs + o + dsh] = -xzn;
         }
-        st[E3_XZ * a.fs + o] += g55 * (dzvx + dxvz);
         // sxy: dy vx + dx vy
         float dyvx = a.idy * stM<R>(vx, sy), dxvy = a.idx * stM<R>(vy, 1);
         if (sh_xy) {
@@ -178,12 +214,13 @@ __global__ void __launch_bounds__(256) k_el3d_fwd_s(El3dDev a) {
         if (STORE) {
             float* S = a.S + slot + s * a.fs + o;
             S[0] = dX; S[a.sterm] = dY; S[2 * a.sterm] = dZ;
-            S[3 * a.sterm] = dzvy + dyvz; S[4 * a.sterm] = dzvx + dxvz; S[5 * a.sterm] = dyvx + dxvy;
+            if (hz_ok) { S[3 * a.sterm] = dzvy + dyvz; S[4 * a.sterm] = dzvx + dxvz; }
+            S[5 * a.sterm] = dyvx + dxvy;
         }
     }
 }
 
-template <int R, bool STORE>
+template <int R, bool STORE, bool FS>
 __global__ void __launch_bounds__(256) k_el3d_fwd_v(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
@@ -226,15 +263,18 @@ __global__ void __launch_bounds__(256) k_el3d_fwd_v(El3dDev a) {
         }
         const float hy = h1 + h2 + h3;
         st[E3_VY * a.fs + o] += by * hy;
-        // vz: dx sxz (P) + dy syz (P) + dz szz (M)
-        h1 = a.idx * stP<R>(sxz, 1); h2 = a.idy * stP<R>(syz, sy); h3 = a.idz * stM<R>(szz, sz);
-        if (sh_vz) {
-            if (axi != 0.f) h1 = pml_fw(h1, axi, bxi, m + N_XXZ * a.fs);
-            if (ayi != 0.f) h2 = pml_fw(h2, ayi, byi, m + N_YYZ * a.fs);
-            if (azh != 0.f) h3 = pml_fw(h3, azh, bzh, m + N_ZZZ * a.fs);
+        // vz: dx sxz (P) + dy syz (P) + dz szz (M); with a free surface from row 2
+        float hz = 0.f;
+        if (!FS || z > a.pr) {
+            h1 = a.idx * stP<R>(sxz, 1); h2 = a.idy * stP<R>(syz, sy); h3 = a.idz * stM<R>(szz, sz);
+            if (sh_vz) {
+                if (axi != 0.f) h1 = pml_fw(h1, axi, bxi, m + N_XXZ * a.fs);
+                if (ayi != 0.f) h2 = pml_fw(h2, ayi, byi, m + N_YYZ * a.fs);
+                if (azh != 0.f) h3 = pml_fw(h3, azh, bzh, m + N_ZZZ * a.fs);
+            }
+            hz = h1 + h2 + h3;
+            st[E3_VZ * a.fs + o] += bz * hz;
         }
-        const float hz = h1 + h2 + h3;
-        st[E3_VZ * a.fs + o] += bz * hz;
         if (STORE) {
             float* S = a.S + slot + s * a.fs + o;
             S[6 * a.sterm] = hx; S[7 * a.sterm] = hy; S[8 * a.sterm] = hz;
@@ -251,7 +291,7 @@ __device__ __forceinline__ void e3_kahan(float* G, long long gg, long long go, i
     G[(12 + q) * gg + go] = c;
 }
 
-template <int R>
+template <int R, bool FS>
 __global__ void __launch_bounds__(256) k_el3d_adj_v(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
@@ -299,18 +339,20 @@ __global__ void __launch_bounds__(256) k_el3d_adj_v(El3dDev a) {
             if (azi != 0.f) e3 = pml_ad(q, azi, bzi, mh + N_ZYZ * a.fs);
         }
         ew[N_XXY * a.fs] = e1; ew[N_YYY * a.fs] = e2; ew[N_ZYZ * a.fs] = e3;
-        // vz^ += Dz^T e_zvz (P) + Dy^T e_yvz (M) + Dx^T e_xvz (M)
-        v = ad[E3_VZ * a.fs + o] + a.idz * tP<R>(e + N_ZVZ * a.fs, sz) + a.idy * tM<R>(e + N_YVZ * a.fs, sy) +
-            a.idx * tM<R>(e + N_XVZ * a.fs, 1);
-        ad[E3_VZ * a.fs + o] = v;
-        gz += v * __ldg(a.S + 8 * a.sterm + so);
-        q = bz * v; e1 = q; e2 = q; e3 = q;
-        if (sh_vz) {
-            if (axi != 0.f) e1 = pml_ad(q, axi, bxi, mh + N_XXZ * a.fs);
-            if (ayi != 0.f) e2 = pml_ad(q, ayi, byi, mh + N_YYZ * a.fs);
-            if (azh != 0.f) e3 = pml_ad(q, azh, bzh, mh + N_ZZZ * a.fs);
+        // vz^ += Dz^T e_zvz (P) + Dy^T e_yvz (M) + Dx^T e_xvz (M); with a free surface from row 2
+        if (!FS || z > a.pr) {
+            v = ad[E3_VZ * a.fs + o] + a.idz * tP<R>(e + N_ZVZ * a.fs, sz) + a.idy * tM<R>(e + N_YVZ * a.fs, sy) +
+                a.idx * tM<R>(e + N_XVZ * a.fs, 1);
+            ad[E3_VZ * a.fs + o] = v;
+            gz += v * __ldg(a.S + 8 * a.sterm + so);
+            q = bz * v; e1 = q; e2 = q; e3 = q;
+            if (sh_vz) {
+                if (axi != 0.f) e1 = pml_ad(q, axi, bxi, mh + N_XXZ * a.fs);
+                if (ayi != 0.f) e2 = pml_ad(q, ayi, byi, mh + N_YYZ * a.fs);
+                if (azh != 0.f) e3 = pml_ad(q, azh, bzh, mh + N_ZZZ * a.fs);
+            }
+            ew[N_XXZ * a.fs] = e1; ew[N_YYZ * a.fs] = e2; ew[N_ZZZ * a.fs] = e3;
         }
-        ew[N_XXZ * a.fs] = e1; ew[N_YYZ * a.fs] = e2; ew[N_ZZZ * a.fs] = e3;
     }
     const long long go = (long long)c.grp * a.fs + o;
     e3_kahan(a.G, a.gg, go, 9, gx);
@@ -318,7 +360,7 @@ __global__ void __launch_bounds__(256) k_el3d_adj_v(El3dDev a) {
     e3_kahan(a.G, a.gg, go, 11, gz);
 }
 
-template <int R>
+template <int R, bool FS>
 __global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
@@ -337,6 +379,13 @@ __global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
                 c23 = __ldg(a.c23 + o), c33 = __ldg(a.c33 + o);
     const float g44 = a.dt * __ldg(a.c44e + o), g55 = a.dt * __ldg(a.c55e + o), g66 = a.dt * __ldg(a.c66e + o);
     const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
+    // free surface: row 1 (traction condition, sigma_zz overwritten by 0), the
+    // half-depth stresses from row 2, and the image rows whose adjoint folds back
+    // onto this node with the image's minus (sigma_zz: 2 pr - z, syz / sxz: 2 pr + 1 - z)
+    const bool row1 = FS && z == a.pr, hz_ok = !FS || z > a.pr;
+    const bool mir = FS && z > a.pr && z <= a.pr + a.R;
+    const long long dzz = (long long)(2 * a.pr - 2 * z) * sz, dsh = dzz + sz;
+    const float r13 = c13 / c33, r23 = c23 / c33;
     float G[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (int s = s0; s < s1; ++s) {
         float* ad = a.ad + s * a.sad;
@@ -346,43 +395,91 @@ __global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
         const float* S = a.S + slot + s * a.fs + o;
         const float xh = ad[E3_XX * a.fs + o] + a.idx * tM<R>(e + N_XXX * a.fs, 1);
         const float yh = ad[E3_YY * a.fs + o] + a.idy * tM<R>(e + N_YYY * a.fs, sy);
-        const float zh = ad[E3_ZZ * a.fs + o] + a.idz * tM<R>(e + N_ZZZ * a.fs, sz);
-        const float yzh = ad[E3_YZ * a.fs + o] + a.idz * tP<R>(e + N_ZYZ * a.fs, sz) + a.idy * tP<R>(e + N_YYZ * a.fs, sy);
-        const float xzh = ad[E3_XZ * a.fs + o] + a.idz * tP<R>(e + N_ZXZ * a.fs, sz) + a.idx * tP<R>(e + N_XXZ * a.fs, 1);
+        float zh = 0.f, yzh = 0.f, xzh = 0.f;
+        if (!row1) {
+            float dzz_s = a.idz * tM<R>(e + N_ZZZ * a.fs, sz);
+            if (mir) {
+                const float* em = e + N_ZZZ * a.fs + dzz;
+                float f = 0.f;
+#pragma unroll
+                for (int q = 1; q <= R; ++q) f = f + c_fd3e[q - 1] * __ldg(em + q * sz);
+                dzz_s = dzz_s + a.idz * f;
+            }
+            zh = ad[E3_ZZ * a.fs + o] + dzz_s;
+        }
+        if (hz_ok) {
+            float dyz = a.idz * tP<R>(e + N_ZYZ * a.fs, sz) + a.idy * tP<R>(e + N_YYZ * a.fs, sy);
+            float dxz = a.idz * tP<R>(e + N_ZXZ * a.fs, sz) + a.idx * tP<R>(e + N_XXZ * a.fs, 1);
+            if (mir) {
+                const float* ey = e + N_ZYZ * a.fs + dsh;
+                const float* ex = e + N_ZXZ * a.fs + dsh;
+                float fy = 0.f, fx = 0.f;
+#pragma unroll
+                for (int q = 1; q <= R; ++q) {
+                    fy = fy + c_fd3e[q - 1] * __ldg(ey + (q - 1) * sz);
+                    fx = fx + c_fd3e[q - 1] * __ldg(ex + (q - 1) * sz);
+                }
+                dyz = dyz + a.idz * fy;
+                dxz = dxz + a.idz * fx;
+            }
+            yzh = ad[E3_YZ * a.fs + o] + dyz;
+            xzh = ad[E3_XZ * a.fs + o] + dxz;
+            ad[E3_YZ * a.fs + o] = yzh;
+            ad[E3_XZ * a.fs + o] = xzh;
+        }
         const float xyh = ad[E3_XY * a.fs + o] + a.idy * tP<R>(e + N_YXY * a.fs, sy) + a.idx * tP<R>(e + N_XXY * a.fs, 1);
         ad[E3_XX * a.fs + o] = xh; ad[E3_YY * a.fs + o] = yh; ad[E3_ZZ * a.fs + o] = zh;
-        ad[E3_YZ * a.fs + o] = yzh; ad[E3_XZ * a.fs + o] = xzh; ad[E3_XY * a.fs + o] = xyh;
+        ad[E3_XY * a.fs + o] = xyh;
         const float dX = __ldg(S), dY = __ldg(S + a.sterm), dZ = __ldg(S + 2 * a.sterm);
-        G[0] += xh * dX;
-        G[1] += xh * dY + yh * dX;
-        G[2] += xh * dZ + zh * dX;
-        G[3] += yh * dY;
-        G[4] += yh * dZ + zh * dY;
-        G[5] += zh * dZ;
-        G[6] += yzh * __ldg(S + 3 * a.sterm);
-        G[7] += xzh * __ldg(S + 4 * a.sterm);
-        G[8] += xyh * __ldg(S + 5 * a.sterm);
-        float qx = a.dt * (c11 * xh + c12 * yh + c13 * zh);
-        float qy = a.dt * (c12 * xh + c22 * yh + c23 * zh);
-        float qz = a.dt * (c13 * xh + c23 * yh + c33 * zh);
-        if (sh_n) {
+        float qx, qy, qz = 0.f;
+        if (row1) {
+            // dZ = -(c13 dX + c23 dY) / c33 and sigma_zz(1) = 0
+            G[0] += xh * dX;
+            G[1] += xh * dY + yh * dX;
+            G[2] += xh * (dZ - r13 * dX) - yh * r23 * dX;
+            G[3] += yh * dY;
+            G[4] += yh * (dZ - r23 * dY) - xh * r13 * dY;
+            G[5] += -(xh * r13 + yh * r23) * dZ;
+            const float w = a.dt * (c13 * xh + c23 * yh);
+            qx = a.dt * (c11 * xh + c12 * yh) - r13 * w;
+            qy = a.dt * (c12 * xh + c22 * yh) - r23 * w;
             if (axi != 0.f) qx = pml_ad(qx, axi, bxi, mh + N_XVX * a.fs);
             if (ayi != 0.f) qy = pml_ad(qy, ayi, byi, mh + N_YVY * a.fs);
-            if (azi != 0.f) qz = pml_ad(qz, azi, bzi, mh + N_ZVZ * a.fs);
+        } else {
+            G[0] += xh * dX;
+            G[1] += xh * dY + yh * dX;
+            G[2] += xh * dZ + zh * dX;
+            G[3] += yh * dY;
+            G[4] += yh * dZ + zh * dY;
+            G[5] += zh * dZ;
+            qx = a.dt * (c11 * xh + c12 * yh + c13 * zh);
+            qy = a.dt * (c12 * xh + c22 * yh + c23 * zh);
+            qz = a.dt * (c13 * xh + c23 * yh + c33 * zh);
+            if (sh_n) {
+                if (axi != 0.f) qx = pml_ad(qx, axi, bxi, mh + N_XVX * a.fs);
+                if (ayi != 0.f) qy = pml_ad(qy, ayi, byi, mh + N_YVY * a.fs);
+                if (azi != 0.f) qz = pml_ad(qz, azi, bzi, mh + N_ZVZ * a.fs);
+            }
         }
         ew[N_XVX * a.fs] = qx; ew[N_YVY * a.fs] = qy; ew[N_ZVZ * a.fs] = qz;
-        float q = g44 * yzh, e1 = q, e2 = q;
-        if (sh_yz) {
-            if (azh != 0.f) e1 = pml_ad(q, azh, bzh, mh + N_ZVY * a.fs);
-            if (ayh != 0.f) e2 = pml_ad(q, ayh, byh, mh + N_YVZ * a.fs);
+        float q, e1, e2;
+        if (hz_ok) {
+            G[6] += yzh * __ldg(S + 3 * a.sterm);
+            G[7] += xzh * __ldg(S + 4 * a.sterm);
+            q = g44 * yzh; e1 = q; e2 = q;
+            if (sh_yz) {
+                if (azh != 0.f) e1 = pml_ad(q, azh, bzh, mh + N_ZVY * a.fs);
+                if (ayh != 0.f) e2 = pml_ad(q, ayh, byh, mh + N_YVZ * a.fs);
+            }
+            ew[N_ZVY * a.fs] = e1; ew[N_YVZ * a.fs] = e2;
+            q = g55 * xzh; e1 = q; e2 = q;
+            if (sh_xz) {
+                if (azh != 0.f) e1 = pml_ad(q, azh, bzh, mh + N_ZVX * a.fs);
+                if (axh != 0.f) e2 = pml_ad(q, axh, bxh, mh + N_XVZ * a.fs);
+            }
+            ew[N_ZVX * a.fs] = e1; ew[N_XVZ * a.fs] = e2;
         }
-        ew[N_ZVY * a.fs] = e1; ew[N_YVZ * a.fs] = e2;
-        q = g55 * xzh; e1 = q; e2 = q;
-        if (sh_xz) {
-            if (azh != 0.f) e1 = pml_ad(q, azh, bzh, mh + N_ZVX * a.fs);
-            if (axh != 0.f) e2 = pml_ad(q, axh, bxh, mh + N_XVZ * a.fs);
-        }
-        ew[N_ZVX * a.fs] = e1; ew[N_XVZ * a.fs] = e2;
+        G[8] += xyh * __ldg(S + 5 * a.sterm);
         q = g66 * xyh; e1 = q; e2 = q;
         if (sh_xy) {
             if (ayh != 0.f) e1 = pml_ad(q, ayh, byh, mh + N_YVX * a.fs);
@@ -463,7 +560,9 @@ __global__ void k_el3d_chain(El3dDev a, int ngroups, int iso, const float* __res
 namespace {
 // per-axis damping tables (module_cfspml.f90:517-600 profiles, damp_coef macro of
 // module_wavefield.f90:40-43, kappa = 1, zero M-PML ratio)
-void e3_axis(int n, int pml, int R, int len, float d, float dt, float pmlvp, float alphamax, std::vector<float>& out) {
+// (low = false: no damping at the low end, the free-surface top, module_cfspml.f90:573-585)
+void e3_axis(int n, int pml, int R, int len, float d, float dt, float pmlvp, float alphamax, std::vector<float>& out,
+             bool low = true) {
     out.assign(4 * (size_t)len, 0.f);  // ai, bi, ah, bh
     const float R0 = 1.0e-5f, adt = std::fabs(dt);
     auto ab = [&](float dd, float al, float& a, float& b) {
@@ -474,6 +573,7 @@ void e3_axis(int n, int pml, int R, int len, float d, float dt, float pmlvp, flo
     for (int i = -pml + 1; i <= n + pml; ++i) {
         float nd, ndh;
         if (i <= 1) {
+            if (!low) continue;
             nd = (float)std::abs(i - 1) * 1.0f / (float)pml;
             ndh = std::fabs((float)(i - 1) - 0.5f) * 1.0f / (float)pml;
         } else if (i >= n) {
@@ -500,7 +600,6 @@ struct El3dEngine : SsgBase {
         aniso = d.aniso;
         OWL_CHECK(aniso == OWL_ANISO_ISO || aniso == OWL_ANISO_CIJ, OWL_ERR_UNSUPPORTED,
                   "elastic 3D takes the iso (vp, vs, rho) or cij (nine moduli, rho) parameterisation");
-        OWL_CHECK(!d.free_surface, OWL_ERR_UNSUPPORTED, "elastic 3D free surface not built");
         idx = (float)(1.0 / (double)d.dx);
         idy = (float)(1.0 / (double)d.dy);
         idz = (float)(1.0 / (double)d.dz);
@@ -599,7 +698,7 @@ struct El3dEngine : SsgBase {
         std::vector<float> tx, ty, tz;
         e3_axis(nx, P, R, pitch, desc.dx, dt, pmlvp, alphamax, tx);
         e3_axis(ny, P, R, NYs, desc.dy, dt, pmlvp, alphamax, ty);
-        e3_axis(nz, P, R, NZs, desc.dz, dt, pmlvp, alphamax, tz);
+        e3_axis(nz, P, R, NZs, desc.dz, dt, pmlvp, alphamax, tz, desc.free_surface == 0);
         c11.upload(hc[0].data(), fs, stream); c12.upload(hc[1].data(), fs, stream); c13.upload(hc[2].data(), fs, stream);
         c22.upload(hc[3].data(), fs, stream); c23.upload(hc[4].data(), fs, stream); c33.upload(hc[5].data(), fs, stream);
         c44e.upload(h44.data(), fs, stream); c55e.upload(h55.data(), fs, stream); c66e.upload(h66.data(), fs, stream);
@@ -622,7 +721,14 @@ struct El3dEngine : SsgBase {
                   OWL_ERR_UNSUPPORTED, "unknown source mechanism");
         return q.mechanism == OWL_SRC_FORCE ? 3 : 1;
     }
+    // with a free surface, no tap above row 2 (module_wavefield.f90:1147-1315)
     void src_taps(const owl_source& q, int comp, std::vector<TapPt>& taps, long long& rc, float& rv) const override {
+        const size_t n0 = taps.size();
+        src_taps_all(q, comp, taps, rc, rv);
+        if (desc.free_surface)
+            taps.erase(std::remove_if(taps.begin() + n0, taps.end(), [](const TapPt& t) { return t.k < 2; }), taps.end());
+    }
+    void src_taps_all(const owl_source& q, int comp, std::vector<TapPt>& taps, long long& rc, float& rv) const {
         const float* ix = q.interp_ix; const float* iy = q.interp_iy; const float* iz = q.interp_iz;
         const float* hx = q.interp_hx; const float* hy = q.interp_hy; const float* hz = q.interp_hz;
         if (q.mechanism == OWL_SRC_FORCE) {
@@ -658,20 +764,33 @@ struct El3dEngine : SsgBase {
                     }
                 }
     }
+    // with a free surface the sampling reads the velocity images vx, vy (1-k) =
+    // (1+k) and vz (2-k) = (1+k), k = 1..4 (submodule_forward_modeling.f90:66-82):
+    // those taps go to the rows they copy; rows above the images hold zero
     void rec_taps(const owl_receiver& q, int comp, std::vector<TapPt>& taps) const override {
+        const bool fsf = desc.free_surface != 0;
         for (int irz = -4; irz <= 4; ++irz)
             for (int iry = -4; iry <= 4; ++iry)
                 for (int irx = -4; irx <= 4; ++irx) {
                     const int a = irx + 4, b = iry + 4, c = irz + 4;
+                    TapPt t;
                     if (comp == 0)
-                        taps.push_back(TapPt{E3_VX, q.hx + irx, q.gy + iry, q.gz + irz,
-                                             q.interp_hx[a] * q.interp_iy[b] * q.interp_iz[c] * q.weight});
+                        t = TapPt{E3_VX, q.hx + irx, q.gy + iry, q.gz + irz,
+                                  q.interp_hx[a] * q.interp_iy[b] * q.interp_iz[c] * q.weight};
                     else if (comp == 1)
-                        taps.push_back(TapPt{E3_VY, q.gx + irx, q.hy + iry, q.gz + irz,
-                                             q.interp_ix[a] * q.interp_hy[b] * q.interp_iz[c] * q.weight});
+                        t = TapPt{E3_VY, q.gx + irx, q.hy + iry, q.gz + irz,
+                                  q.interp_ix[a] * q.interp_hy[b] * q.interp_iz[c] * q.weight};
                     else
-                        taps.push_back(TapPt{E3_VZ, q.gx + irx, q.gy + iry, q.hz + irz,
-                                             q.interp_ix[a] * q.interp_iy[b] * q.interp_hz[c] * q.weight});
+                        t = TapPt{E3_VZ, q.gx + irx, q.gy + iry, q.hz + irz,
+                                  q.interp_ix[a] * q.interp_iy[b] * q.interp_hz[c] * q.weight};
+                    if (fsf) {
+                        const int top = comp == 2 ? 1 : 0;  // last image row: vz images rows <= 1
+                        if (t.k <= top) {
+                            if (t.k < top - 3) continue;
+                            t.k = top + 2 - t.k;  // vx, vy: 2 - k; vz: 3 - k
+                        }
+                    }
+                    taps.push_back(t);
                 }
     }
 
@@ -679,8 +798,10 @@ struct El3dEngine : SsgBase {
         El3dDev a{};
         a.nx = nx; a.ny = ny; a.nz = nz; a.P = P; a.R = R; a.pr = pr; a.pitch = pitch;
         a.plane = plane; a.fs = fs; a.sst = sst; a.sad = sad;
-        a.x0 = R; a.x1 = R + NXp; a.y0 = R; a.y1 = R + NYp; a.z0 = R; a.z1 = R + NZp;
-        a.nzb = (NZp + 1) / 2;
+        a.x0 = R; a.x1 = R + NXp; a.y0 = R; a.y1 = R + NYp; a.z1 = R + NZp;
+        a.fsurf = desc.free_surface != 0;
+        a.z0 = a.fsurf ? pr : R;  // with a free surface nothing above row 1 is updated
+        a.nzb = (a.z1 - a.z0 + 1) / 2;
         a.idx = idx; a.idy = idy; a.idz = idz; a.dt = dt;
         a.nshots = S;
         a.c11 = c11.p; a.c12 = c12.p; a.c13 = c13.p; a.c22 = c22.p; a.c23 = c23.p; a.c33 = c33.p;
@@ -708,6 +829,7 @@ struct El3dEngine : SsgBase {
     template <int RR>
     void launch_r(int id, int S, bool store) {
         El3dDev a = dev(S);
+        const bool FF = a.fsurf != 0;  // free-surface variants of the kernels
         const bool fwd = id == OWL_K_FWD_P || id == OWL_K_FWD_V;
         a.spt = fwd ? spt_f : spt_a;
         const int groups = (S + a.spt - 1) / a.spt;
@@ -716,16 +838,18 @@ struct El3dEngine : SsgBase {
         if (fwd) {
             OWL_CHECK(!store || a.S, OWL_ERR_INVALID, "stencil-term buffer not allocated");
             if (id == OWL_K_FWD_P) {
-                if (store) k_el3d_fwd_s<RR, true><<<g, b, 0, stream>>>(a);
-                else k_el3d_fwd_s<RR, false><<<g, b, 0, stream>>>(a);
+                auto k = store ? (FF ? k_el3d_fwd_s<RR, true, true> : k_el3d_fwd_s<RR, true, false>)
+                               : (FF ? k_el3d_fwd_s<RR, false, true> : k_el3d_fwd_s<RR, false, false>);
+                k<<<g, b, 0, stream>>>(a);
             } else {
-                if (store) k_el3d_fwd_v<RR, true><<<g, b, 0, stream>>>(a);
-                else k_el3d_fwd_v<RR, false><<<g, b, 0, stream>>>(a);
+                auto k = store ? (FF ? k_el3d_fwd_v<RR, true, true> : k_el3d_fwd_v<RR, true, false>)
+                               : (FF ? k_el3d_fwd_v<RR, false, true> : k_el3d_fwd_v<RR, false, false>);
+                k<<<g, b, 0, stream>>>(a);
             }
         } else {
             OWL_CHECK(a.ad && a.S && a.G, OWL_ERR_INVALID, "adjoint buffers not allocated");
-            if (id == OWL_K_ADJ_P) k_el3d_adj_v<RR><<<g, b, 0, stream>>>(a);
-            else k_el3d_adj_s<RR><<<g, b, 0, stream>>>(a);
+            if (id == OWL_K_ADJ_P) (FF ? k_el3d_adj_v<RR, true> : k_el3d_adj_v<RR, false>)<<<g, b, 0, stream>>>(a);
+            else (FF ? k_el3d_adj_s<RR, true> : k_el3d_adj_s<RR, false>)<<<g, b, 0, stream>>>(a);
         }
     }
     void launch_kernel(int id, int S, bool store) override {

@@ -1,6 +1,6 @@
-"""GPU parity tests of the 3D elastic path through the C ABI: forward (vx, vy, vz)
-vs the FP32 oracle at 1e-5 relative L2; gradient vs the FP64 exact-adjoint oracle
-at 1e-4; source-side gradient."""
+"""GPU parity tests of the 3D elastic path through the C ABI, with and without
+the free surface: forward (vx, vy, vz) vs the FP32 oracle at 1e-5 relative L2;
+gradient vs the FP64 exact-adjoint oracle at 1e-4; source-side gradient."""
 import numpy as np
 import pytest
 
@@ -19,18 +19,20 @@ GRAD_TOL = 1e-4
 
 def make(d, f):
     s = SSGSolver(L.OWL_ELASTIC_VHTIORT_3D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
-                  f0_max=d.f0_max, max_shots=d.max_shots, ny=d.ny, dy=d.dy, aniso=d.aniso)
+                  free_surface=bool(d.free_surface), f0_max=d.f0_max, max_shots=d.max_shots, ny=d.ny, dy=d.dy,
+                  aniso=d.aniso)
     s.set_model(*f)
     return s
 
 
+@pytest.mark.parametrize("fs", [0, 1])
 @pytest.mark.parametrize("R", [4, 8])
 @pytest.mark.parametrize("aniso", [L.OWL_ANISO_ISO, L.OWL_ANISO_CIJ])
-def test_el3d_forward_parity(R, aniso):
-    d = el3_desc(aniso, R=R)
+def test_el3d_forward_parity(R, aniso, fs):
+    d = el3_desc(aniso, R=R, fs=fs)
     f = el3_model(aniso)
     s = make(d, f)
-    ps = s.prepare(el3_shots() * 2)
+    ps = s.prepare(el3_shots(fs) * 2)
     ref = oracle.el3d_forward(d, f, ps, "f32")
     for opts in (RunOpts(), RunOpts(shots_per_launch=1, use_graph=-1), RunOpts(shots_per_cta=2)):
         got = s.forward(ps, opts)
@@ -38,12 +40,13 @@ def test_el3d_forward_parity(R, aniso):
     assert abs(s.dt_stable - oracle.el3d_dt_stable(d, f)) <= 1e-6 * s.dt_stable
 
 
+@pytest.mark.parametrize("fs", [0, 1])
 @pytest.mark.parametrize("aniso", [L.OWL_ANISO_ISO, L.OWL_ANISO_CIJ])
-def test_el3d_gradient_parity(aniso):
-    d = el3_desc(aniso)
+def test_el3d_gradient_parity(aniso, fs):
+    d = el3_desc(aniso, fs=fs)
     f = el3_model(aniso)
     s = make(d, f)
-    ps = s.prepare(el3_shots() * 2)
+    ps = s.prepare(el3_shots(fs) * 2)
     obs = oracle.el3d_forward(d, el3_model(aniso, seed=2), ps, "f64").astype(np.float32)
     mref, gref, _ = oracle.el3d_gradient(d, f, ps, obs, adj_kind=L.OWL_ADJ_L2_RESIDUAL, k=7)
     for opts in (RunOpts(checkpoint_interval=7), RunOpts(checkpoint_interval=7, shots_per_launch=1, use_graph=-1)):
@@ -52,11 +55,12 @@ def test_el3d_gradient_parity(aniso):
         assert np.allclose(misfit, mref, rtol=1e-4)
 
 
-def test_el3d_source_gradient_parity():
-    d = el3_desc(L.OWL_ANISO_ISO)
+@pytest.mark.parametrize("fs", [0, 1])
+def test_el3d_source_gradient_parity(fs):
+    d = el3_desc(L.OWL_ANISO_ISO, fs=fs)
     f = el3_model(L.OWL_ANISO_ISO)
     s = make(d, f)
-    ps = s.prepare(el3_shots())
+    ps = s.prepare(el3_shots(fs))
     adj = np.random.default_rng(5).standard_normal(s.seis_size(ps)).astype(np.float32)
     _, _, sref = oracle.el3d_gradient(d, f, ps, adj, adj_kind=L.OWL_ADJ_GIVEN, k=7, stf_grad=True)
     got = s.source_gradient(ps, adj, RunOpts(checkpoint_interval=7))
