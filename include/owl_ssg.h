@@ -205,8 +205,9 @@ int owl_ssg_create(const owl_ssg_desc *desc, owl_ssg **out);
  *     OWL_ANISO_THOMSEN  vp, vs, epsilon, delta, theta, rho     (nparam = 6)
  *     OWL_ANISO_AT       vp, vs, epsilon, eta, theta, rho       (nparam = 6)
  *     OWL_ANISO_CIJ      c11, c13, c33, c55, rho                (nparam = 5)
- *   elastic 3D, by desc.aniso (no free surface):
+ *   elastic 3D, by desc.aniso (theta, phi: tilt and azimuth, radians):
  *     OWL_ANISO_ISO      vp, vs, rho                            (nparam = 3)
+ *     OWL_ANISO_THOMSEN  vp, vs, epsilon, delta, gamma, theta, phi, rho (nparam = 8)
  *     OWL_ANISO_CIJ      c11, c12, c13, c22, c23, c33, c44, c55, c66, rho (nparam = 10)
  * Replaces the transpose / pad_array / bk = rho*vp^2 part of prepare_modeling
  * (src/solver/acoustic_iso_2d/module_vars.f90:109-115) and, for elastic 2D, the

@@ -49,12 +49,74 @@ struct E3 {
     }
 };
 
-inline int el3_nparam(int aniso) { return aniso == OWL_ANISO_ISO ? 3 : (aniso == OWL_ANISO_CIJ ? 10 : -1); }
+inline int el3_nparam(int aniso) {
+    return aniso == OWL_ANISO_ISO ? 3 : aniso == OWL_ANISO_THOMSEN ? 8 : (aniso == OWL_ANISO_CIJ ? 10 : -1);
+}
 
-// Cij of one cell, order c11 c12 c13 c22 c23 c33 c44 c55 c66 rho (module_vars.f90:278-296, :362-375)
+template <typename T>
+inline double el3_re(const T& v) { return std::real(v); }
+
+// Thomsen parameters (vp, vs, eps, del, gam, the, phi, rho) to the ORT moduli:
+// thomsen_to_cij3d (src/lib/module_anisotropy.f90:336-381); the tilt is
+// cij_rotate_3d (:233-291) with rotation_matrix([0, -the, -phi], 'xyz') of FLIT,
+// restated as R = Rz(-phi) Ry(-the), and bond_matrix (:127-170); the VHTIORT
+// solver keeps the nine ORT entries of the rotated tensor (module_vars.f90:317-325).
+template <typename T>
+void el3_thomsen(const T* p, T* c) {
+    const T vp = p[0], vs = p[1], eps = p[2], del = p[3], gam = p[4], the = p[5], phi = p[6], rho = p[7];
+    const T c33 = vp * vp * rho, c44 = vs * vs * rho;
+    const T c11 = c33 * (T(1) + T(2) * eps), c66 = c44 * (T(1) + T(2) * gam);
+    const T c12 = c11 - T(2) * c66;
+    const T tmp = T(2) * c33 * (c33 - c44) * del + (c33 - c44) * (c33 - c44);
+    const T c13 = std::sqrt(el3_re(tmp) < 0 ? -tmp : tmp) - c44;
+    T C[6][6] = {};
+    C[0][0] = c11; C[0][1] = C[1][0] = c12; C[0][2] = C[2][0] = c13; C[1][1] = c11; C[1][2] = C[2][1] = c13;
+    C[2][2] = c33; C[3][3] = c44; C[4][4] = c44; C[5][5] = c66;
+    if ((el3_re(the) != 0 || el3_re(phi) != 0) && !(el3_re(eps) == 0 && el3_re(del) == 0 && el3_re(gam) == 0)) {
+        const T cb = std::cos(-the), sb = std::sin(-the), cg = std::cos(-phi), sg = std::sin(-phi);
+        const T Rz[3][3] = {{cg, -sg, T(0)}, {sg, cg, T(0)}, {T(0), T(0), T(1)}};
+        const T Ry[3][3] = {{cb, T(0), sb}, {T(0), T(1), T(0)}, {-sb, T(0), cb}};
+        T r[3][3];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                r[i][j] = T(0);
+                for (int k = 0; k < 3; ++k) r[i][j] = r[i][j] + Rz[i][k] * Ry[k][j];
+            }
+        // Bond matrix rows as bond_matrix writes them
+        const T b[6][6] = {
+            {r[0][0] * r[0][0], r[0][1] * r[0][1], r[0][2] * r[0][2], T(2) * r[0][1] * r[0][2], T(2) * r[0][0] * r[0][2],
+             T(2) * r[0][0] * r[0][1]},
+            {r[1][0] * r[1][0], r[1][1] * r[1][1], r[1][2] * r[1][2], T(2) * r[1][1] * r[1][2], T(2) * r[1][0] * r[1][2],
+             T(2) * r[1][0] * r[1][1]},
+            {r[2][0] * r[2][0], r[2][1] * r[2][1], r[2][2] * r[2][2], T(2) * r[2][1] * r[2][2], T(2) * r[2][0] * r[2][2],
+             T(2) * r[2][0] * r[2][1]},
+            {r[1][0] * r[2][0], r[1][1] * r[2][1], r[1][2] * r[2][2], r[1][1] * r[2][2] + r[1][2] * r[2][1],
+             r[1][0] * r[2][2] + r[1][2] * r[2][0], r[1][0] * r[2][1] + r[1][1] * r[2][0]},
+            {r[0][0] * r[2][0], r[0][1] * r[2][1], r[0][2] * r[2][2], r[0][1] * r[2][2] + r[0][2] * r[2][1],
+             r[0][0] * r[2][2] + r[0][2] * r[2][0], r[0][0] * r[2][1] + r[0][1] * r[2][0]},
+            {r[0][0] * r[1][0], r[0][1] * r[1][1], r[0][2] * r[1][2], r[0][1] * r[1][2] + r[0][2] * r[1][1],
+             r[0][0] * r[1][2] + r[0][2] * r[1][0], r[0][0] * r[1][1] + r[0][1] * r[1][0]}};
+        T out[6][6];
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j < 6; ++j) {
+                T acc = T(0);
+                for (int k = 0; k < 6; ++k)
+                    for (int l = 0; l < 6; ++l) acc = acc + b[i][k] * C[k][l] * b[j][l];
+                out[i][j] = acc;
+            }
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j < 6; ++j) C[i][j] = out[i][j];
+    }
+    c[0] = C[0][0]; c[1] = C[0][1]; c[2] = C[0][2]; c[3] = C[1][1]; c[4] = C[1][2]; c[5] = C[2][2];
+    c[6] = C[3][3]; c[7] = C[4][4]; c[8] = C[5][5]; c[9] = rho;
+}
+
+// Cij of one cell, order c11 c12 c13 c22 c23 c33 c44 c55 c66 rho (module_vars.f90:278-375)
 template <typename T>
 void el3_cij(int aniso, const T* p, T* c) {
-    if (aniso == OWL_ANISO_ISO) {
+    if (aniso == OWL_ANISO_THOMSEN) {
+        el3_thomsen(p, c);
+    } else if (aniso == OWL_ANISO_ISO) {
         const T vp = p[0], vs = p[1], rho = p[2];
         const T c11 = rho * (vp * vp), c44 = rho * (vs * vs);
         const T c12 = c11 - T(2) * c44;

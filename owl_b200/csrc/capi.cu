@@ -70,7 +70,7 @@ int owl_ssg_nparam(int medium) {
 int owl_ssg_desc_nparam(const owl_ssg_desc* d) {
     if (!d) return -1;
     if (d->medium == OWL_ELASTIC_VHTIORT_3D)
-        return d->aniso == OWL_ANISO_ISO ? 3 : d->aniso == OWL_ANISO_CIJ ? 10 : -1;
+        return d->aniso == OWL_ANISO_ISO ? 3 : d->aniso == OWL_ANISO_THOMSEN ? 8 : d->aniso == OWL_ANISO_CIJ ? 10 : -1;
     if (d->medium != OWL_ELASTIC_VHTIORT_2D) return owl_ssg_nparam(d->medium);
     switch (d->aniso) {
         case OWL_ANISO_ISO: return 3;

@@ -492,9 +492,90 @@ __global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
     for (int q = 0; q < 9; ++q) e3_kahan(a.G, a.gg, go, q, G[q]);
 }
 
+// ---- Thomsen parameterisation (thomsen_to_cij3d, src/lib/module_anisotropy.f90:336-381) ----
+// Dual numbers (value, derivative) for the forward-mode derivatives of the Cij
+// set-up in the chain rule; float / double evaluate the same code.
+struct Dual {
+    double v, d;
+};
+__host__ __device__ inline Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__host__ __device__ inline Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__host__ __device__ inline Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__host__ __device__ inline Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__host__ __device__ inline double tval(Dual a) { return a.v; }
+__host__ __device__ inline double tval(double a) { return a; }
+__host__ __device__ inline double tval(float a) { return a; }
+__host__ __device__ inline Dual tsqrt(Dual a) {
+    const double r = sqrt(a.v);
+    return {r, a.d / (2.0 * r)};
+}
+__host__ __device__ inline Dual tabs(Dual a) { return a.v < 0 ? -a : a; }
+__host__ __device__ inline Dual tcos(Dual a) { return {cos(a.v), -a.d * sin(a.v)}; }
+__host__ __device__ inline Dual tsin(Dual a) { return {sin(a.v), a.d * cos(a.v)}; }
+__host__ __device__ inline double tsqrt(double a) { return sqrt(a); }
+__host__ __device__ inline double tabs(double a) { return fabs(a); }
+__host__ __device__ inline double tcos(double a) { return cos(a); }
+__host__ __device__ inline double tsin(double a) { return sin(a); }
+__host__ __device__ inline float tsqrt(float a) { return sqrtf(a); }
+__host__ __device__ inline float tabs(float a) { return fabsf(a); }
+__host__ __device__ inline float tcos(float a) { return cosf(a); }
+__host__ __device__ inline float tsin(float a) { return sinf(a); }
+template <typename T>
+__host__ __device__ inline T tc(double v) { return T(v); }
+template <>
+__host__ __device__ inline Dual tc<Dual>(double v) { return Dual{v, 0.0}; }
+
+// p: vp, vs, epsilon, delta, gamma, theta, phi, rho -> c: the nine ORT moduli
+// (c11 c12 c13 c22 c23 c33 c44 c55 c66) and rho. A tilt rotates the tensor by
+// rotation_matrix([0, -theta, -phi], 'xyz') and bond_matrix (:127-170,
+// :233-291): restated as r = Rz(-phi) Ry(-theta), C' = M C M^T with the Bond
+// matrix M of r; the solver keeps the nine ORT entries of C'.
+template <typename T>
+__host__ __device__ void thomsen3d_cij(const T* p, T* c) {
+    const T vp = p[0], vs = p[1], eps = p[2], del = p[3], gam = p[4], the = p[5], phi = p[6], rho = p[7];
+    const T c33 = vp * vp * rho, c44 = vs * vs * rho;
+    const T c11 = c33 * (tc<T>(1) + tc<T>(2) * eps), c66 = c44 * (tc<T>(1) + tc<T>(2) * gam);
+    const T c12 = c11 - tc<T>(2) * c66;
+    const T tmp = tc<T>(2) * c33 * (c33 - c44) * del + (c33 - c44) * (c33 - c44);
+    const T c13 = tsqrt(tabs(tmp)) - c44;
+    c[0] = c11; c[1] = c12; c[2] = c13; c[3] = c11; c[4] = c13; c[5] = c33; c[6] = c44; c[7] = c44; c[8] = c66;
+    c[9] = rho;
+    if ((tval(the) != 0.0 || tval(phi) != 0.0) && !(tval(eps) == 0.0 && tval(del) == 0.0 && tval(gam) == 0.0)) {
+        const T cb = tcos(-the), sb = tsin(-the), cg = tcos(-phi), sg = tsin(-phi);
+        const T z0 = tc<T>(0);
+        const T r[3][3] = {{cg * cb, -sg, cg * sb}, {sg * cb, cg, sg * sb}, {-sb, z0, cb}};
+        T M[6][6];
+        const int pi[6] = {0, 1, 2, 1, 0, 0}, pj[6] = {0, 1, 2, 2, 2, 1};  // Voigt index pairs
+        for (int a = 0; a < 6; ++a)
+            for (int b = 0; b < 6; ++b) {
+                const int i = pi[a], j = pj[a], k = pi[b], l = pj[b];
+                if (a < 3) M[a][b] = b < 3 ? r[i][k] * r[i][k] : tc<T>(2) * r[i][k] * r[i][l];
+                else M[a][b] = b < 3 ? r[i][k] * r[j][k] : r[i][k] * r[j][l] + r[i][l] * r[j][k];
+            }
+        const T C6[6][6] = {{c11, c12, c13, z0, z0, z0}, {c12, c11, c13, z0, z0, z0}, {c13, c13, c33, z0, z0, z0},
+                            {z0, z0, z0, c44, z0, z0},   {z0, z0, z0, z0, c44, z0},   {z0, z0, z0, z0, z0, c66}};
+        T MC[6][6];
+        for (int a = 0; a < 6; ++a)
+            for (int b = 0; b < 6; ++b) {
+                T acc = tc<T>(0);
+                for (int q = 0; q < 6; ++q) acc = acc + M[a][q] * C6[q][b];
+                MC[a][b] = acc;
+            }
+        auto rot = [&](int a, int b) {
+            T acc = tc<T>(0);
+            for (int q = 0; q < 6; ++q) acc = acc + MC[a][q] * M[b][q];
+            return acc;
+        };
+        c[0] = rot(0, 0); c[1] = rot(0, 1); c[2] = rot(0, 2); c[3] = rot(1, 1); c[4] = rot(1, 2); c[5] = rot(2, 2);
+        c[6] = rot(3, 3); c[7] = rot(4, 4); c[8] = rot(5, 5);
+    }
+}
+
 // FP64 chain rule on the padded model grid: d J / d (c11 c12 c13 c22 c23 c33 c44 c55 c66 rho),
-// then the parameters (iso: vp, vs, rho; cij: the nine moduli and rho)
+// then the parameters (iso: vp, vs, rho; cij: the nine moduli and rho; thomsen:
+// the eight parameters through dual-number derivatives of thomsen3d_cij)
 __global__ void k_el3d_chain(El3dDev a, int ngroups, int iso, const float* __restrict__ p0, const float* __restrict__ p1,
+                             const float* __restrict__ tpar,
                              const float* __restrict__ c44p, const float* __restrict__ c55p,
                              const float* __restrict__ c66p, const float* __restrict__ rhop, double* __restrict__ gpad,
                              int nxq, int nyq, int nzq) {
@@ -542,7 +623,18 @@ __global__ void k_el3d_chain(El3dDev a, int ngroups, int iso, const float* __res
             }
         }
         const long long npad = n;
-        if (iso) {
+        if (tpar) {
+            double pv[8];
+            for (int q = 0; q < 8; ++q) pv[q] = tpar[q * a.fs + o];
+            for (int q = 0; q < 8; ++q) {
+                Dual pd[8], cd[10];
+                for (int r = 0; r < 8; ++r) pd[r] = Dual{pv[r], r == q ? 1.0 : 0.0};
+                thomsen3d_cij(pd, cd);
+                double g = 0.0;
+                for (int r = 0; r < 10; ++r) g += dc[r] * cd[r].d;
+                gpad[q * npad + cell] += g;
+            }
+        } else if (iso) {
             const double vp = p0[o], vs = p1[o], rho = rhop[o];
             const double sn = dc[0] + dc[3] + dc[5], so = dc[1] + dc[2] + dc[4], ss = dc[6] + dc[7] + dc[8];
             gpad[cell] += 2.0 * rho * vp * (sn + so);
@@ -594,12 +686,13 @@ struct El3dEngine : SsgBase {
     int aniso;
     float idx, idy, idz;
     DevBuf<float> c11, c12, c13, c22, c23, c33, c44e, c55e, c66e, bxp, byp, bzp;
-    DevBuf<float> c44p, c55p, c66p, rhop, p0p, p1p, tabx, taby, tabz;
+    DevBuf<float> c44p, c55p, c66p, rhop, p0p, p1p, tabx, taby, tabz, tparp;
 
     explicit El3dEngine(const owl_ssg_desc& d) : SsgBase(d, 3) {
         aniso = d.aniso;
-        OWL_CHECK(aniso == OWL_ANISO_ISO || aniso == OWL_ANISO_CIJ, OWL_ERR_UNSUPPORTED,
-                  "elastic 3D takes the iso (vp, vs, rho) or cij (nine moduli, rho) parameterisation");
+        OWL_CHECK(aniso == OWL_ANISO_ISO || aniso == OWL_ANISO_CIJ || aniso == OWL_ANISO_THOMSEN, OWL_ERR_UNSUPPORTED,
+                  "elastic 3D takes the iso (vp, vs, rho), thomsen (vp, vs, epsilon, delta, gamma, theta, phi, rho) "
+                  "or cij (nine moduli, rho) parameterisation");
         idx = (float)(1.0 / (double)d.dx);
         idy = (float)(1.0 / (double)d.dy);
         idz = (float)(1.0 / (double)d.dz);
@@ -608,7 +701,7 @@ struct El3dEngine : SsgBase {
         sad = E3_NAD * fs;
         nS = 9;
         ngrad = 12;
-        nparam = aniso == OWL_ANISO_ISO ? 3 : 10;
+        nparam = aniso == OWL_ANISO_ISO ? 3 : aniso == OWL_ANISO_THOMSEN ? 8 : 10;
         ncomp = 3;
         for (int f = 0; f < E3_NST; ++f) st_segments.push_back({f * fs, fs});
     }
@@ -629,8 +722,9 @@ struct El3dEngine : SsgBase {
         for (int q = 0; q < np; ++q) OWL_CHECK(f[q], OWL_ERR_INVALID, "null model parameter");
         std::vector<float> hc[10];
         for (auto& v : hc) v.assign(fs, 0.f);
-        std::vector<float> hp0, hp1;
+        std::vector<float> hp0, hp1, htp;
         if (aniso == OWL_ANISO_ISO) { hp0.assign(fs, 0.f); hp1.assign(fs, 0.f); }
+        if (aniso == OWL_ANISO_THOMSEN) htp.assign((size_t)8 * fs, 0.f);
         // Cij of the padded model (module_vars.f90:278-296, 362-375; padding by pml+1, :409-418)
         for (int k = -P; k <= nz + P + 1; ++k)
             for (int j = -P; j <= ny + P + 1; ++j)
@@ -647,6 +741,10 @@ struct El3dEngine : SsgBase {
                         std::copy(w, w + 10, v);
                         hp0[o] = vp;
                         hp1[o] = vs;
+                    } else if (aniso == OWL_ANISO_THOMSEN) {
+                        float pp[8];
+                        for (int q = 0; q < 8; ++q) htp[(size_t)q * fs + o] = pp[q] = f[q][src];
+                        thomsen3d_cij(pp, v);
                     } else {
                         for (int q = 0; q < 10; ++q) v[q] = f[q][src];
                     }
@@ -706,6 +804,7 @@ struct El3dEngine : SsgBase {
         c44p.upload(hc[6].data(), fs, stream); c55p.upload(hc[7].data(), fs, stream); c66p.upload(hc[8].data(), fs, stream);
         rhop.upload(r.data(), fs, stream);
         if (aniso == OWL_ANISO_ISO) { p0p.upload(hp0.data(), fs, stream); p1p.upload(hp1.data(), fs, stream); }
+        if (aniso == OWL_ANISO_THOMSEN) tparp.upload(htp.data(), htp.size(), stream);
         tabx.upload(tx.data(), tx.size(), stream);
         taby.upload(ty.data(), ty.size(), stream);
         tabz.upload(tz.data(), tz.size(), stream);
@@ -901,7 +1000,8 @@ struct El3dEngine : SsgBase {
         const long long n = (long long)nxq() * nyq() * nzq();
         const int nb = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
         const bool iso = aniso == OWL_ANISO_ISO;
-        k_el3d_chain<<<nb, 256, 0, stream>>>(a, groups, iso ? 1 : 0, iso ? p0p.p : nullptr, iso ? p1p.p : nullptr, c44p.p,
+        k_el3d_chain<<<nb, 256, 0, stream>>>(a, groups, iso ? 1 : 0, iso ? p0p.p : nullptr, iso ? p1p.p : nullptr,
+                                             aniso == OWL_ANISO_THOMSEN ? tparp.p : nullptr, c44p.p,
                                              c55p.p, c66p.p, rhop.p, gpad.p, nxq(), nyq(), nzq());
         OWL_LAUNCH_CHECK();
         launches++;

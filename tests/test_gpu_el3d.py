@@ -27,7 +27,7 @@ def make(d, f):
 
 @pytest.mark.parametrize("fs", [0, 1])
 @pytest.mark.parametrize("R", [4, 8])
-@pytest.mark.parametrize("aniso", [L.OWL_ANISO_ISO, L.OWL_ANISO_CIJ])
+@pytest.mark.parametrize("aniso", [L.OWL_ANISO_ISO, L.OWL_ANISO_CIJ, L.OWL_ANISO_THOMSEN])
 def test_el3d_forward_parity(R, aniso, fs):
     d = el3_desc(aniso, R=R, fs=fs)
     f = el3_model(aniso)
@@ -41,7 +41,7 @@ def test_el3d_forward_parity(R, aniso, fs):
 
 
 @pytest.mark.parametrize("fs", [0, 1])
-@pytest.mark.parametrize("aniso", [L.OWL_ANISO_ISO, L.OWL_ANISO_CIJ])
+@pytest.mark.parametrize("aniso", [L.OWL_ANISO_ISO, L.OWL_ANISO_CIJ, L.OWL_ANISO_THOMSEN])
 def test_el3d_gradient_parity(aniso, fs):
     d = el3_desc(aniso, fs=fs)
     f = el3_model(aniso)

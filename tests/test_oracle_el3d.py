@@ -2,7 +2,7 @@
 
 Pinned by properties (the reference ships no elastic test): the exact adjoint
 passes the dot-product test against complex-step directional derivatives for the
-isotropic and the orthorhombic (nine Cij) parameterisations with explosion,
+isotropic, tilted-Thomsen and orthorhombic (nine Cij) parameterisations with explosion,
 force and moment-tensor sources, with and without the free surface; the misfit
 gradient matches the complex-step derivative of J; FP32 and FP64 forwards agree.
 """
@@ -37,6 +37,14 @@ def el3_model(aniso, seed=1):
     rho = 1000 + 200 * rng.random((N, N, N))
     if aniso == L.OWL_ANISO_ISO:
         return [vp, vs, rho]
+    if aniso == L.OWL_ANISO_THOMSEN:
+        # tilted orthorhombic-free TI: epsilon, delta, gamma, tilt theta and azimuth phi (radians)
+        eps = 0.05 + 0.15 * rng.random((N, N, N))
+        dlt = -0.05 + 0.15 * rng.random((N, N, N))
+        gam = 0.1 * rng.random((N, N, N))
+        the = 0.4 * rng.random((N, N, N))
+        phi = rng.random((N, N, N))
+        return [vp, vs, eps, dlt, gam, the, phi, rho]
     c11, c44 = rho * vp ** 2, rho * vs ** 2
     return [1.1 * c11, c11 - 2 * c44, 0.9 * (c11 - 2 * c44), c11, c11 - 2 * c44, 0.95 * c11, c44, 1.05 * c44,
             0.9 * c44, rho]
@@ -67,7 +75,7 @@ def _dot(g, dm):
 
 
 @pytest.mark.parametrize("aniso,fs", [(L.OWL_ANISO_ISO, 0), (L.OWL_ANISO_CIJ, 0), (L.OWL_ANISO_ISO, 1),
-                                      (L.OWL_ANISO_CIJ, 1)])
+                                      (L.OWL_ANISO_CIJ, 1), (L.OWL_ANISO_THOMSEN, 0), (L.OWL_ANISO_THOMSEN, 1)])
 def test_el3d_adjoint_dot_product(aniso, fs):
     d = el3_desc(aniso, fs=fs)
     f = el3_model(aniso)
