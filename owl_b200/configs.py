@@ -197,13 +197,14 @@ def elastic_3d_ort_model(n=256, dx=10.0):
 def config5(nshots=16, nt=2500, n=256, nrec=128):
     """3D elastic orthorhombic: n^3 (256^3), dx 10 m, dt 0.8 ms, PML 20, 8th order,
     nine-Cij parameterisation; vertical-force 10 Hz shots on a line at 20 m depth;
-    nrec x nrec three-component receivers every 2 cells at 20 m depth."""
+    nrec x nrec three-component receivers every 2 cells at 20 m depth, centred and
+    on grid nodes (their interpolation taps collapse to one node)."""
     dx, dt = 10.0, 8e-4
     d = _desc(L.OWL_ELASTIC_VHTIORT_3D, n, n, dx, dt, nt, pml=20, f0=10.0, max_shots=nshots, ny=n)
     d.aniso = L.OWL_ANISO_CIJ
     step = 2 * dx
     nr = min(nrec, n // 2)
-    x0 = (n - 1) * dx / 2 - step * (nr - 1) / 2
+    x0 = dx * float(int(((n - 1) * dx / 2 - step * (nr - 1) / 2) / dx))
     recs = [Receiver(x=x0 + step * i, y=x0 + step * j, z=20.0) for j in range(nr) for i in range(nr)]
     shots = []
     for k in range(nshots):

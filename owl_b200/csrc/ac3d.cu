@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "ring.cuh"
 #include "ssg_base.cuh"
 
 #ifndef OWL_AC3_ZCHUNK_MIN

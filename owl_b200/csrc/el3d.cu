@@ -37,6 +37,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "ring.cuh"
 #include "ssg_base.cuh"
 
 namespace owl {
@@ -54,6 +55,7 @@ struct El3dDev {
     int nx, ny, nz, P, R, pr, pitch;
     long long plane, fs, sst, sad;
     int x0, x1, y0, y1, z0, z1, nzb, fsurf;
+    int NYs, NZs, zchunk;  // storage planes / rows, z chunk of the ring kernels
     float idx, idy, idz, dt;
     int nshots, spt;
     const float *c11, *c12, *c13, *c22, *c23, *c33, *c44e, *c55e, *c66e, *bx, *by, *bz;
@@ -127,6 +129,8 @@ __device__ __forceinline__ bool e3_cell(const El3dDev& a, E3Cell& c) {
     c.o = (long long)c.z * a.plane + (long long)c.y * a.pitch + c.x;
     return c.x < a.x1 && c.y < a.y1 && c.z < a.z1;
 }
+
+#include "el3d_ring.cuh"
 
 // ------------------------------- forward ------------------------------------
 template <int R, bool STORE, bool FS>
@@ -710,10 +714,17 @@ struct El3dEngine : SsgBase {
     float* ad_field(int f) const override { return f < 9 ? ad.p + f * fs : nullptr; }
     int rho_param() const override { return nparam - 1; }
     std::vector<int> tune_spt(int) const override { return {1, 2, 4}; }
-    std::vector<int> tune_tz(int) const override { return {2}; }
-    void launch_params(const owl_run_opts&) override {
+    // forward pass: 2 = thread per cell (2 planes per block), 1 = the z-marching
+    // ring kernels (half-width 4, no free surface)
+    std::vector<int> tune_tz(int pass) const override {
+        if (pass == 0 && R == 4 && !desc.free_surface) return {2, 1};
+        return {2};
+    }
+    // tile_z = 1 asks for the ring forward kernels (where they apply), anything else the per-cell ones
+    void launch_params(const owl_run_opts& o) override {
         tile_x = 32;
-        tz_f = tz_a = 2;
+        tz_f = (o.tile_z == 1 && R == 4 && !desc.free_surface) ? 1 : 2;
+        tz_a = 2;
     }
 
     void set_model(int np, const float* const* f) override {
@@ -901,6 +912,8 @@ struct El3dEngine : SsgBase {
         a.fsurf = desc.free_surface != 0;
         a.z0 = a.fsurf ? pr : R;  // with a free surface nothing above row 1 is updated
         a.nzb = (a.z1 - a.z0 + 1) / 2;
+        a.NYs = NYs;
+        a.NZs = NZs;
         a.idx = idx; a.idy = idy; a.idz = idz; a.dt = dt;
         a.nshots = S;
         a.c11 = c11.p; a.c12 = c12.p; a.c13 = c13.p; a.c22 = c22.p; a.c23 = c23.p; a.c33 = c33.p;
@@ -934,6 +947,28 @@ struct El3dEngine : SsgBase {
         const int groups = (S + a.spt - 1) / a.spt;
         OWL_CHECK((long long)a.nzb * groups < 65536, OWL_ERR_UNSUPPORTED, "too many z blocks x shot groups");
         const dim3 b(32, 4, 2), g((NXp + 31) / 32, (NYp + 3) / 4, a.nzb * groups);
+        if (fwd && tz_f == 1 && RR == 4 && !FF) {
+            OWL_CHECK(!store || a.S, OWL_ERR_INVALID, "stencil-term buffer not allocated");
+            const int rows = a.z1 - a.z0;
+            const long long xy = (long long)((NXp + 31) / 32) * ((NYp + 7) / 8);
+            const long long want = std::max<long long>(1, (148LL * 64 + xy - 1) / xy);
+            a.zchunk = (int)std::max<long long>(16, (rows + want - 1) / want);
+            const int nzc = (rows + a.zchunk - 1) / a.zchunk;
+            OWL_CHECK((long long)nzc * groups < 65536, OWL_ERR_UNSUPPORTED, "too many z chunks x shot groups");
+            const dim3 br(32, 8), gr((NXp + 31) / 32, (NYp + 7) / 8, nzc * groups);
+            if (id == OWL_K_FWD_P) {
+                constexpr int sm = e3r_bytes_s<4>();
+                auto k = store ? k_el3d_fwd_s_ring<4, true> : k_el3d_fwd_s_ring<4, false>;
+                OWL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+                k<<<gr, br, sm, stream>>>(a);
+            } else {
+                constexpr int sm = e3r_bytes_v<4>();
+                auto k = store ? k_el3d_fwd_v_ring<4, true> : k_el3d_fwd_v_ring<4, false>;
+                OWL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+                k<<<gr, br, sm, stream>>>(a);
+            }
+            return;
+        }
         if (fwd) {
             OWL_CHECK(!store || a.S, OWL_ERR_INVALID, "stencil-term buffer not allocated");
             if (id == OWL_K_FWD_P) {

@@ -34,7 +34,9 @@ def test_el3d_forward_parity(R, aniso, fs):
     s = make(d, f)
     ps = s.prepare(el3_shots(fs) * 2)
     ref = oracle.el3d_forward(d, f, ps, "f32")
-    for opts in (RunOpts(), RunOpts(shots_per_launch=1, use_graph=-1), RunOpts(shots_per_cta=2)):
+    # tile_z=1: the z-marching ring kernels (half-width 4, no free surface; else the per-cell ones)
+    for opts in (RunOpts(), RunOpts(shots_per_launch=1, use_graph=-1), RunOpts(shots_per_cta=2),
+                 RunOpts(tile_z=1), RunOpts(tile_z=1, shots_per_cta=2)):
         got = s.forward(ps, opts)
         assert rel(got, ref) < FWD_TOL, (opts, rel(got, ref))
     assert abs(s.dt_stable - oracle.el3d_dt_stable(d, f)) <= 1e-6 * s.dt_stable
@@ -49,7 +51,8 @@ def test_el3d_gradient_parity(aniso, fs):
     ps = s.prepare(el3_shots(fs) * 2)
     obs = oracle.el3d_forward(d, el3_model(aniso, seed=2), ps, "f64").astype(np.float32)
     mref, gref, _ = oracle.el3d_gradient(d, f, ps, obs, adj_kind=L.OWL_ADJ_L2_RESIDUAL, k=7)
-    for opts in (RunOpts(checkpoint_interval=7), RunOpts(checkpoint_interval=7, shots_per_launch=1, use_graph=-1)):
+    for opts in (RunOpts(checkpoint_interval=7), RunOpts(checkpoint_interval=7, shots_per_launch=1, use_graph=-1),
+                 RunOpts(checkpoint_interval=7, tile_z=1)):
         misfit, g = s.gradient(ps, obs, opts=opts)
         assert rel(g, gref) < GRAD_TOL, (opts, rel(g, gref))
         assert np.allclose(misfit, mref, rtol=1e-4)
