@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--no-elastic", action="store_true", help="skip the 2D elastic VTI block")
     p.add_argument("--profile-el", type=int, default=0, metavar="S",
                    help="profiling target: one 2D elastic VTI gradient of S shots, 60 steps, no JSON line")
+    p.add_argument("--ring", action="store_true", help="--profile-el3 with the ring forward kernels")
     p.add_argument("--profile-el3", type=int, default=0, metavar="N",
                    help="profiling target: one 3D elastic ORT gradient of 1 shot on an N^3 model, 40 steps")
     return p.parse_args()
@@ -127,8 +128,9 @@ def profile_elastic(nshots):
     s.close()
 
 
-def profile_elastic3(n):
-    """Small 3D elastic gradient for kernel captures: the ORT model on n^3, 1 shot, 40 steps."""
+def profile_elastic3(n, ring=False):
+    """Small 3D elastic gradient for kernel captures: the ORT model on n^3, 1 shot, 40 steps;
+    forward kernels thread per cell, or the z-marching ring kernels with ring=True."""
     import numpy as np
     from owl_b200 import _lib as L
     from owl_b200 import configs
@@ -140,7 +142,7 @@ def profile_elastic3(n):
     s.set_model(*f)
     ps = s.prepare(shots)
     obs = np.zeros(s.seis_size(ps), dtype=np.float32)
-    s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=20, shots_per_cta=1, tile_z=2, use_graph=-1))
+    s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=20, shots_per_cta=1, tile_z=1 if ring else 2, use_graph=-1))
     print(f"profile-el3: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
     s.close()
 
@@ -402,7 +404,7 @@ def main():
     if args.profile_el:
         return profile_elastic(args.profile_el)
     if args.profile_el3:
-        return profile_elastic3(args.profile_el3)
+        return profile_elastic3(args.profile_el3, args.ring)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 

@@ -579,12 +579,18 @@ struct Ac3dEngine : SsgBase {
                     taps.push_back(t);
                 }
     }
+    // taps with a zero factor are dropped here (the table keeps none of them)
     void rec_taps(const owl_receiver& q, int, std::vector<TapPt>& taps) const override {
-        for (int irz = -4; irz <= 4; ++irz)
-            for (int iry = -4; iry <= 4; ++iry)
+        for (int irz = -4; irz <= 4; ++irz) {
+            if (q.interp_iz[irz + 4] == 0.f) continue;
+            for (int iry = -4; iry <= 4; ++iry) {
+                if (q.interp_iy[iry + 4] == 0.f) continue;
                 for (int irx = -4; irx <= 4; ++irx)
-                    taps.push_back(TapPt{0, q.gx + irx, q.gy + iry, q.gz + irz,
-                                         q.interp_ix[irx + 4] * q.interp_iy[iry + 4] * q.interp_iz[irz + 4] * q.weight});
+                    if (q.interp_ix[irx + 4] != 0.f)
+                        taps.push_back(TapPt{0, q.gx + irx, q.gy + iry, q.gz + irz,
+                                             q.interp_ix[irx + 4] * q.interp_iy[iry + 4] * q.interp_iz[irz + 4] * q.weight});
+            }
+        }
     }
     void scatter_map(const TapPt& t, std::vector<TapPt>& out) const override {
         if (!desc.free_surface) { out.push_back(t); return; }

@@ -105,14 +105,16 @@ __device__ __forceinline__ float tM(const float* e, long long s) {
     return a;
 }
 
-__device__ __forceinline__ float pml_fw(float D, float a, float b, float* psi) {
-    const float m = a * D + b * *psi;
-    *psi = m;
+// CPML step with the memory value read ahead: psi' = a D + b psi, D + psi'
+__device__ __forceinline__ float pml_up(float D, float a, float b, float psi, float* dst) {
+    const float m = a * D + b * psi;
+    *dst = m;
     return D + m;
 }
-__device__ __forceinline__ float pml_ad(float q, float a, float b, float* psih) {
-    const float u = q + *psih;
-    *psih = b * u;
+// adjoint CPML step with the memory value read ahead: u = q + psih, psih' = b u, q + a u
+__device__ __forceinline__ float pml_adr(float q, float a, float b, float psih, float* dst) {
+    const float u = q + psih;
+    *dst = b * u;
     return q + a * u;
 }
 
@@ -134,7 +136,7 @@ __device__ __forceinline__ bool e3_cell(const El3dDev& a, E3Cell& c) {
 
 // ------------------------------- forward ------------------------------------
 template <int R, bool STORE, bool FS>
-__global__ void __launch_bounds__(256) k_el3d_fwd_s(El3dDev a) {
+__global__ void __launch_bounds__(256, 3) k_el3d_fwd_s(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
     const long long o = c.o, sy = a.pitch, sz = a.plane;
@@ -163,25 +165,35 @@ __global__ void __launch_bounds__(256) k_el3d_fwd_s(El3dDev a) {
         const float* vy = st + E3_VY * a.fs + o;
         const float* vz = st + E3_VZ * a.fs + o;
         float* m = st + E3_M0 * a.fs + o;
+        // the cell's old stresses and CPML memories are read ahead of its first
+        // store (same buffer: no later plain read could move above a store)
+        const float xx0 = st[E3_XX * a.fs + o], yy0 = st[E3_YY * a.fs + o];
+        const float zz0 = row1 ? 0.f : st[E3_ZZ * a.fs + o];
+        const float yz0 = hz_ok ? st[E3_YZ * a.fs + o] : 0.f, xz0 = hz_ok ? st[E3_XZ * a.fs + o] : 0.f;
+        const float xy0 = st[E3_XY * a.fs + o];
+        const bool p0 = (row1 || sh_n) && axi != 0.f, p1 = (row1 || sh_n) && ayi != 0.f, p2 = !row1 && sh_n && azi != 0.f;
+        const bool p3 = hz_ok && sh_yz && ayh != 0.f, p4 = hz_ok && sh_yz && azh != 0.f;
+        const bool p5 = hz_ok && sh_xz && axh != 0.f, p6 = hz_ok && sh_xz && azh != 0.f;
+        const bool p7 = sh_xy && axh != 0.f, p8 = sh_xy && ayh != 0.f;
+        const float m0 = p0 ? m[N_XVX * a.fs] : 0.f, m1 = p1 ? m[N_YVY * a.fs] : 0.f, m2 = p2 ? m[N_ZVZ * a.fs] : 0.f;
+        const float m3 = p3 ? m[N_YVZ * a.fs] : 0.f, m4 = p4 ? m[N_ZVY * a.fs] : 0.f;
+        const float m5 = p5 ? m[N_XVZ * a.fs] : 0.f, m6 = p6 ? m[N_ZVX * a.fs] : 0.f;
+        const float m7 = p7 ? m[N_XVY * a.fs] : 0.f, m8 = p8 ? m[N_YVX * a.fs] : 0.f;
         float dX = a.idx * stP<R>(vx, 1), dY = a.idy * stP<R>(vy, sy), dZ;
+        if (p0) dX = pml_up(dX, axi, bxi, m0, m + N_XVX * a.fs);
+        if (p1) dY = pml_up(dY, ayi, byi, m1, m + N_YVY * a.fs);
         if (row1) {
-            if (axi != 0.f) dX = pml_fw(dX, axi, bxi, m + N_XVX * a.fs);
-            if (ayi != 0.f) dY = pml_fw(dY, ayi, byi, m + N_YVY * a.fs);
             dZ = -(c13 / c33) * dX - (c23 / c33) * dY;
         } else {
             dZ = a.idz * stP<R>(vz, sz);
-            if (sh_n) {
-                if (axi != 0.f) dX = pml_fw(dX, axi, bxi, m + N_XVX * a.fs);
-                if (ayi != 0.f) dY = pml_fw(dY, ayi, byi, m + N_YVY * a.fs);
-                if (azi != 0.f) dZ = pml_fw(dZ, azi, bzi, m + N_ZVZ * a.fs);
-            }
+            if (p2) dZ = pml_up(dZ, azi, bzi, m2, m + N_ZVZ * a.fs);
         }
-        st[E3_XX * a.fs + o] += a.dt * (c11 * dX + c12 * dY + c13 * dZ);
-        st[E3_YY * a.fs + o] += a.dt * (c12 * dX + c22 * dY + c23 * dZ);
+        st[E3_XX * a.fs + o] = xx0 + a.dt * (c11 * dX + c12 * dY + c13 * dZ);
+        st[E3_YY * a.fs + o] = yy0 + a.dt * (c12 * dX + c22 * dY + c23 * dZ);
         if (row1) {
             st[E3_ZZ * a.fs + o] = 0.f;
         } else {
-            const float zn = st[E3_ZZ * a.fs + o] + a.dt * (c13 * dX + c23 * dY + c33 * dZ);
+            const float zn = zz0 + a.dt * (c13 * dX + c23 * dY + c33 * dZ);
             st[E3_ZZ * a.fs + o] = zn;
             if (mir) st[E3_ZZ * a.fs + o + dzz] = -zn;
         }
@@ -190,31 +202,25 @@ __global__ void __launch_bounds__(256) k_el3d_fwd_s(El3dDev a) {
             // syz: dz vy + dy vz
             dzvy = a.idz * stM<R>(vy, sz);
             dyvz = a.idy * stM<R>(vz, sy);
-            if (sh_yz) {
-                if (ayh != 0.f) dyvz = pml_fw(dyvz, ayh, byh, m + N_YVZ * a.fs);
-                if (azh != 0.f) dzvy = pml_fw(dzvy, azh, bzh, m + N_ZVY * a.fs);
-            }
-            const float yzn = st[E3_YZ * a.fs + o] + g44 * (dzvy + dyvz);
+            if (p3) dyvz = pml_up(dyvz, ayh, byh, m3, m + N_YVZ * a.fs);
+            if (p4) dzvy = pml_up(dzvy, azh, bzh, m4, m + N_ZVY * a.fs);
+            const float yzn = yz0 + g44 * (dzvy + dyvz);
             st[E3_YZ * a.fs + o] = yzn;
             if (mir) st[E3_YZ * a.fs + o + dsh] = -yzn;
             // sxz: dz vx + dx vz
             dzvx = a.idz * stM<R>(vx, sz);
             dxvz = a.idx * stM<R>(vz, 1);
-            if (sh_xz) {
-                if (axh != 0.f) dxvz = pml_fw(dxvz, axh, bxh, m + N_XVZ * a.fs);
-                if (azh != 0.f) dzvx = pml_fw(dzvx, azh, bzh, m + N_ZVX * a.fs);
-            }
-            const float xzn = st[E3_XZ * a.fs + o] + g55 * (dzvx + dxvz);
+            if (p5) dxvz = pml_up(dxvz, axh, bxh, m5, m + N_XVZ * a.fs);
+            if (p6) dzvx = pml_up(dzvx, azh, bzh, m6, m + N_ZVX * a.fs);
+            const float xzn = xz0 + g55 * (dzvx + dxvz);
             st[E3_XZ * a.fs + o] = xzn;
             if (mir) st[E3_XZ * a.fs + o + dsh] = -xzn;
         }
         // sxy: dy vx + dx vy
         float dyvx = a.idy * stM<R>(vx, sy), dxvy = a.idx * stM<R>(vy, 1);
-        if (sh_xy) {
-            if (axh != 0.f) dxvy = pml_fw(dxvy, axh, bxh, m + N_XVY * a.fs);
-            if (ayh != 0.f) dyvx = pml_fw(dyvx, ayh, byh, m + N_YVX * a.fs);
-        }
-        st[E3_XY * a.fs + o] += g66 * (dyvx + dxvy);
+        if (p7) dxvy = pml_up(dxvy, axh, bxh, m7, m + N_XVY * a.fs);
+        if (p8) dyvx = pml_up(dyvx, ayh, byh, m8, m + N_YVX * a.fs);
+        st[E3_XY * a.fs + o] = xy0 + g66 * (dyvx + dxvy);
         if (STORE) {
             float* S = a.S + slot + s * a.fs + o;
             S[0] = dX; S[a.sterm] = dY; S[2 * a.sterm] = dZ;
@@ -225,7 +231,7 @@ __global__ void __launch_bounds__(256) k_el3d_fwd_s(El3dDev a) {
 }
 
 template <int R, bool STORE, bool FS>
-__global__ void __launch_bounds__(256) k_el3d_fwd_v(El3dDev a) {
+__global__ void __launch_bounds__(256, 3) k_el3d_fwd_v(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
     const long long o = c.o, sy = a.pitch, sz = a.plane;
@@ -249,35 +255,41 @@ __global__ void __launch_bounds__(256) k_el3d_fwd_v(El3dDev a) {
         const float* sxz = st + E3_XZ * a.fs + o;
         const float* sxy = st + E3_XY * a.fs + o;
         float* m = st + E3_M0 * a.fs + o;
+        // the cell's old velocities and CPML memories are read ahead of its
+        // first store (same buffer: no later plain read could move above a store)
+        const bool vz_ok = !FS || z > a.pr;
+        const float vx0 = st[E3_VX * a.fs + o], vy0 = st[E3_VY * a.fs + o];
+        const float vz0 = vz_ok ? st[E3_VZ * a.fs + o] : 0.f;
+        const bool p0 = sh_vx && axh != 0.f, p1 = sh_vx && ayi != 0.f, p2 = sh_vx && azi != 0.f;
+        const bool p3 = sh_vy && axi != 0.f, p4 = sh_vy && ayh != 0.f, p5 = sh_vy && azi != 0.f;
+        const bool p6 = vz_ok && sh_vz && axi != 0.f, p7 = vz_ok && sh_vz && ayi != 0.f,
+                   p8 = vz_ok && sh_vz && azh != 0.f;
+        const float m0 = p0 ? m[N_XXX * a.fs] : 0.f, m1 = p1 ? m[N_YXY * a.fs] : 0.f, m2 = p2 ? m[N_ZXZ * a.fs] : 0.f;
+        const float m3 = p3 ? m[N_XXY * a.fs] : 0.f, m4 = p4 ? m[N_YYY * a.fs] : 0.f, m5 = p5 ? m[N_ZYZ * a.fs] : 0.f;
+        const float m6 = p6 ? m[N_XXZ * a.fs] : 0.f, m7 = p7 ? m[N_YYZ * a.fs] : 0.f, m8 = p8 ? m[N_ZZZ * a.fs] : 0.f;
         // vx: dx sxx (M) + dy sxy (P) + dz sxz (P)
         float h1 = a.idx * stM<R>(sxx, 1), h2 = a.idy * stP<R>(sxy, sy), h3 = a.idz * stP<R>(sxz, sz);
-        if (sh_vx) {
-            if (axh != 0.f) h1 = pml_fw(h1, axh, bxh, m + N_XXX * a.fs);
-            if (ayi != 0.f) h2 = pml_fw(h2, ayi, byi, m + N_YXY * a.fs);
-            if (azi != 0.f) h3 = pml_fw(h3, azi, bzi, m + N_ZXZ * a.fs);
-        }
+        if (p0) h1 = pml_up(h1, axh, bxh, m0, m + N_XXX * a.fs);
+        if (p1) h2 = pml_up(h2, ayi, byi, m1, m + N_YXY * a.fs);
+        if (p2) h3 = pml_up(h3, azi, bzi, m2, m + N_ZXZ * a.fs);
         const float hx = h1 + h2 + h3;
-        st[E3_VX * a.fs + o] += bx * hx;
+        st[E3_VX * a.fs + o] = vx0 + bx * hx;
         // vy: dx sxy (P) + dy syy (M) + dz syz (P)
         h1 = a.idx * stP<R>(sxy, 1); h2 = a.idy * stM<R>(syy, sy); h3 = a.idz * stP<R>(syz, sz);
-        if (sh_vy) {
-            if (axi != 0.f) h1 = pml_fw(h1, axi, bxi, m + N_XXY * a.fs);
-            if (ayh != 0.f) h2 = pml_fw(h2, ayh, byh, m + N_YYY * a.fs);
-            if (azi != 0.f) h3 = pml_fw(h3, azi, bzi, m + N_ZYZ * a.fs);
-        }
+        if (p3) h1 = pml_up(h1, axi, bxi, m3, m + N_XXY * a.fs);
+        if (p4) h2 = pml_up(h2, ayh, byh, m4, m + N_YYY * a.fs);
+        if (p5) h3 = pml_up(h3, azi, bzi, m5, m + N_ZYZ * a.fs);
         const float hy = h1 + h2 + h3;
-        st[E3_VY * a.fs + o] += by * hy;
+        st[E3_VY * a.fs + o] = vy0 + by * hy;
         // vz: dx sxz (P) + dy syz (P) + dz szz (M); with a free surface from row 2
         float hz = 0.f;
-        if (!FS || z > a.pr) {
+        if (vz_ok) {
             h1 = a.idx * stP<R>(sxz, 1); h2 = a.idy * stP<R>(syz, sy); h3 = a.idz * stM<R>(szz, sz);
-            if (sh_vz) {
-                if (axi != 0.f) h1 = pml_fw(h1, axi, bxi, m + N_XXZ * a.fs);
-                if (ayi != 0.f) h2 = pml_fw(h2, ayi, byi, m + N_YYZ * a.fs);
-                if (azh != 0.f) h3 = pml_fw(h3, azh, bzh, m + N_ZZZ * a.fs);
-            }
+            if (p6) h1 = pml_up(h1, axi, bxi, m6, m + N_XXZ * a.fs);
+            if (p7) h2 = pml_up(h2, ayi, byi, m7, m + N_YYZ * a.fs);
+            if (p8) h3 = pml_up(h3, azh, bzh, m8, m + N_ZZZ * a.fs);
             hz = h1 + h2 + h3;
-            st[E3_VZ * a.fs + o] += bz * hz;
+            st[E3_VZ * a.fs + o] = vz0 + bz * hz;
         }
         if (STORE) {
             float* S = a.S + slot + s * a.fs + o;
@@ -296,7 +308,7 @@ __device__ __forceinline__ void e3_kahan(float* G, long long gg, long long go, i
 }
 
 template <int R, bool FS>
-__global__ void __launch_bounds__(256) k_el3d_adj_v(El3dDev a) {
+__global__ void __launch_bounds__(256, 3) k_el3d_adj_v(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
     const long long o = c.o, sy = a.pitch, sz = a.plane;
@@ -319,42 +331,49 @@ __global__ void __launch_bounds__(256) k_el3d_adj_v(El3dDev a) {
         float* mh = ad + 9 * a.fs + o;
         float* ew = ad + 27 * a.fs + o;
         const long long so = slot + s * a.fs + o;
+        // the cell's old values and CPML memories are read ahead of its first
+        // store: the stores go to the same buffer, so no later plain read could
+        // be moved above them and every read would cost its own round trip
+        const bool vz_ok = !FS || z > a.pr;
+        const float vx0 = ad[E3_VX * a.fs + o], vy0 = ad[E3_VY * a.fs + o];
+        const float vz0 = vz_ok ? ad[E3_VZ * a.fs + o] : 0.f;
+        const bool p0 = sh_vx && axh != 0.f, p1 = sh_vx && ayi != 0.f, p2 = sh_vx && azi != 0.f;
+        const bool p3 = sh_vy && axi != 0.f, p4 = sh_vy && ayh != 0.f, p5 = sh_vy && azi != 0.f;
+        const bool p6 = vz_ok && sh_vz && axi != 0.f, p7 = vz_ok && sh_vz && ayi != 0.f,
+                   p8 = vz_ok && sh_vz && azh != 0.f;
+        const float m0 = p0 ? mh[N_XXX * a.fs] : 0.f, m1 = p1 ? mh[N_YXY * a.fs] : 0.f, m2 = p2 ? mh[N_ZXZ * a.fs] : 0.f;
+        const float m3 = p3 ? mh[N_XXY * a.fs] : 0.f, m4 = p4 ? mh[N_YYY * a.fs] : 0.f, m5 = p5 ? mh[N_ZYZ * a.fs] : 0.f;
+        const float m6 = p6 ? mh[N_XXZ * a.fs] : 0.f, m7 = p7 ? mh[N_YYZ * a.fs] : 0.f, m8 = p8 ? mh[N_ZZZ * a.fs] : 0.f;
         // vx^ += Dx^T e_xvx (P) + Dz^T e_zvx (M) + Dy^T e_yvx (M)
-        float v = ad[E3_VX * a.fs + o] + a.idx * tP<R>(e + N_XVX * a.fs, 1) + a.idz * tM<R>(e + N_ZVX * a.fs, sz) +
+        float v = vx0 + a.idx * tP<R>(e + N_XVX * a.fs, 1) + a.idz * tM<R>(e + N_ZVX * a.fs, sz) +
                   a.idy * tM<R>(e + N_YVX * a.fs, sy);
         ad[E3_VX * a.fs + o] = v;
         gx += v * __ldg(a.S + 6 * a.sterm + so);
         float q = bx * v, e1 = q, e2 = q, e3 = q;
-        if (sh_vx) {
-            if (axh != 0.f) e1 = pml_ad(q, axh, bxh, mh + N_XXX * a.fs);
-            if (ayi != 0.f) e2 = pml_ad(q, ayi, byi, mh + N_YXY * a.fs);
-            if (azi != 0.f) e3 = pml_ad(q, azi, bzi, mh + N_ZXZ * a.fs);
-        }
+        if (p0) e1 = pml_adr(q, axh, bxh, m0, mh + N_XXX * a.fs);
+        if (p1) e2 = pml_adr(q, ayi, byi, m1, mh + N_YXY * a.fs);
+        if (p2) e3 = pml_adr(q, azi, bzi, m2, mh + N_ZXZ * a.fs);
         ew[N_XXX * a.fs] = e1; ew[N_YXY * a.fs] = e2; ew[N_ZXZ * a.fs] = e3;
         // vy^ += Dy^T e_yvy (P) + Dz^T e_zvy (M) + Dx^T e_xvy (M)
-        v = ad[E3_VY * a.fs + o] + a.idy * tP<R>(e + N_YVY * a.fs, sy) + a.idz * tM<R>(e + N_ZVY * a.fs, sz) +
+        v = vy0 + a.idy * tP<R>(e + N_YVY * a.fs, sy) + a.idz * tM<R>(e + N_ZVY * a.fs, sz) +
             a.idx * tM<R>(e + N_XVY * a.fs, 1);
         ad[E3_VY * a.fs + o] = v;
         gy += v * __ldg(a.S + 7 * a.sterm + so);
         q = by * v; e1 = q; e2 = q; e3 = q;
-        if (sh_vy) {
-            if (axi != 0.f) e1 = pml_ad(q, axi, bxi, mh + N_XXY * a.fs);
-            if (ayh != 0.f) e2 = pml_ad(q, ayh, byh, mh + N_YYY * a.fs);
-            if (azi != 0.f) e3 = pml_ad(q, azi, bzi, mh + N_ZYZ * a.fs);
-        }
+        if (p3) e1 = pml_adr(q, axi, bxi, m3, mh + N_XXY * a.fs);
+        if (p4) e2 = pml_adr(q, ayh, byh, m4, mh + N_YYY * a.fs);
+        if (p5) e3 = pml_adr(q, azi, bzi, m5, mh + N_ZYZ * a.fs);
         ew[N_XXY * a.fs] = e1; ew[N_YYY * a.fs] = e2; ew[N_ZYZ * a.fs] = e3;
         // vz^ += Dz^T e_zvz (P) + Dy^T e_yvz (M) + Dx^T e_xvz (M); with a free surface from row 2
-        if (!FS || z > a.pr) {
-            v = ad[E3_VZ * a.fs + o] + a.idz * tP<R>(e + N_ZVZ * a.fs, sz) + a.idy * tM<R>(e + N_YVZ * a.fs, sy) +
+        if (vz_ok) {
+            v = vz0 + a.idz * tP<R>(e + N_ZVZ * a.fs, sz) + a.idy * tM<R>(e + N_YVZ * a.fs, sy) +
                 a.idx * tM<R>(e + N_XVZ * a.fs, 1);
             ad[E3_VZ * a.fs + o] = v;
             gz += v * __ldg(a.S + 8 * a.sterm + so);
             q = bz * v; e1 = q; e2 = q; e3 = q;
-            if (sh_vz) {
-                if (axi != 0.f) e1 = pml_ad(q, axi, bxi, mh + N_XXZ * a.fs);
-                if (ayi != 0.f) e2 = pml_ad(q, ayi, byi, mh + N_YYZ * a.fs);
-                if (azh != 0.f) e3 = pml_ad(q, azh, bzh, mh + N_ZZZ * a.fs);
-            }
+            if (p6) e1 = pml_adr(q, axi, bxi, m6, mh + N_XXZ * a.fs);
+            if (p7) e2 = pml_adr(q, ayi, byi, m7, mh + N_YYZ * a.fs);
+            if (p8) e3 = pml_adr(q, azh, bzh, m8, mh + N_ZZZ * a.fs);
             ew[N_XXZ * a.fs] = e1; ew[N_YYZ * a.fs] = e2; ew[N_ZZZ * a.fs] = e3;
         }
     }
@@ -365,7 +384,7 @@ __global__ void __launch_bounds__(256) k_el3d_adj_v(El3dDev a) {
 }
 
 template <int R, bool FS>
-__global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
+__global__ void __launch_bounds__(256, 3) k_el3d_adj_s(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
     const long long o = c.o, sy = a.pitch, sz = a.plane;
@@ -397,8 +416,22 @@ __global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
         float* ew = ad + 27 * a.fs + o;
         float* mh = ad + 9 * a.fs + o;
         const float* S = a.S + slot + s * a.fs + o;
-        const float xh = ad[E3_XX * a.fs + o] + a.idx * tM<R>(e + N_XXX * a.fs, 1);
-        const float yh = ad[E3_YY * a.fs + o] + a.idy * tM<R>(e + N_YYY * a.fs, sy);
+        // the cell's old values and CPML memories are read ahead of its first
+        // store (same buffer: no later plain read could move above a store)
+        const float xx0 = ad[E3_XX * a.fs + o], yy0 = ad[E3_YY * a.fs + o];
+        const float zz0 = row1 ? 0.f : ad[E3_ZZ * a.fs + o];
+        const float yz0 = hz_ok ? ad[E3_YZ * a.fs + o] : 0.f, xz0 = hz_ok ? ad[E3_XZ * a.fs + o] : 0.f;
+        const float xy0 = ad[E3_XY * a.fs + o];
+        const bool p0 = (row1 || sh_n) && axi != 0.f, p1 = (row1 || sh_n) && ayi != 0.f, p2 = !row1 && sh_n && azi != 0.f;
+        const bool p3 = hz_ok && sh_yz && azh != 0.f, p4 = hz_ok && sh_yz && ayh != 0.f;
+        const bool p5 = hz_ok && sh_xz && azh != 0.f, p6 = hz_ok && sh_xz && axh != 0.f;
+        const bool p7 = sh_xy && ayh != 0.f, p8 = sh_xy && axh != 0.f;
+        const float m0 = p0 ? mh[N_XVX * a.fs] : 0.f, m1 = p1 ? mh[N_YVY * a.fs] : 0.f, m2 = p2 ? mh[N_ZVZ * a.fs] : 0.f;
+        const float m3 = p3 ? mh[N_ZVY * a.fs] : 0.f, m4 = p4 ? mh[N_YVZ * a.fs] : 0.f;
+        const float m5 = p5 ? mh[N_ZVX * a.fs] : 0.f, m6 = p6 ? mh[N_XVZ * a.fs] : 0.f;
+        const float m7 = p7 ? mh[N_YVX * a.fs] : 0.f, m8 = p8 ? mh[N_XVY * a.fs] : 0.f;
+        const float xh = xx0 + a.idx * tM<R>(e + N_XXX * a.fs, 1);
+        const float yh = yy0 + a.idy * tM<R>(e + N_YYY * a.fs, sy);
         float zh = 0.f, yzh = 0.f, xzh = 0.f;
         if (!row1) {
             float dzz_s = a.idz * tM<R>(e + N_ZZZ * a.fs, sz);
@@ -409,7 +442,7 @@ __global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
                 for (int q = 1; q <= R; ++q) f = f + c_fd3e[q - 1] * __ldg(em + q * sz);
                 dzz_s = dzz_s + a.idz * f;
             }
-            zh = ad[E3_ZZ * a.fs + o] + dzz_s;
+            zh = zz0 + dzz_s;
         }
         if (hz_ok) {
             float dyz = a.idz * tP<R>(e + N_ZYZ * a.fs, sz) + a.idy * tP<R>(e + N_YYZ * a.fs, sy);
@@ -426,12 +459,12 @@ __global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
                 dyz = dyz + a.idz * fy;
                 dxz = dxz + a.idz * fx;
             }
-            yzh = ad[E3_YZ * a.fs + o] + dyz;
-            xzh = ad[E3_XZ * a.fs + o] + dxz;
+            yzh = yz0 + dyz;
+            xzh = xz0 + dxz;
             ad[E3_YZ * a.fs + o] = yzh;
             ad[E3_XZ * a.fs + o] = xzh;
         }
-        const float xyh = ad[E3_XY * a.fs + o] + a.idy * tP<R>(e + N_YXY * a.fs, sy) + a.idx * tP<R>(e + N_XXY * a.fs, 1);
+        const float xyh = xy0 + a.idy * tP<R>(e + N_YXY * a.fs, sy) + a.idx * tP<R>(e + N_XXY * a.fs, 1);
         ad[E3_XX * a.fs + o] = xh; ad[E3_YY * a.fs + o] = yh; ad[E3_ZZ * a.fs + o] = zh;
         ad[E3_XY * a.fs + o] = xyh;
         const float dX = __ldg(S), dY = __ldg(S + a.sterm), dZ = __ldg(S + 2 * a.sterm);
@@ -447,8 +480,8 @@ __global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
             const float w = a.dt * (c13 * xh + c23 * yh);
             qx = a.dt * (c11 * xh + c12 * yh) - r13 * w;
             qy = a.dt * (c12 * xh + c22 * yh) - r23 * w;
-            if (axi != 0.f) qx = pml_ad(qx, axi, bxi, mh + N_XVX * a.fs);
-            if (ayi != 0.f) qy = pml_ad(qy, ayi, byi, mh + N_YVY * a.fs);
+            if (p0) qx = pml_adr(qx, axi, bxi, m0, mh + N_XVX * a.fs);
+            if (p1) qy = pml_adr(qy, ayi, byi, m1, mh + N_YVY * a.fs);
         } else {
             G[0] += xh * dX;
             G[1] += xh * dY + yh * dX;
@@ -459,11 +492,9 @@ __global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
             qx = a.dt * (c11 * xh + c12 * yh + c13 * zh);
             qy = a.dt * (c12 * xh + c22 * yh + c23 * zh);
             qz = a.dt * (c13 * xh + c23 * yh + c33 * zh);
-            if (sh_n) {
-                if (axi != 0.f) qx = pml_ad(qx, axi, bxi, mh + N_XVX * a.fs);
-                if (ayi != 0.f) qy = pml_ad(qy, ayi, byi, mh + N_YVY * a.fs);
-                if (azi != 0.f) qz = pml_ad(qz, azi, bzi, mh + N_ZVZ * a.fs);
-            }
+            if (p0) qx = pml_adr(qx, axi, bxi, m0, mh + N_XVX * a.fs);
+            if (p1) qy = pml_adr(qy, ayi, byi, m1, mh + N_YVY * a.fs);
+            if (p2) qz = pml_adr(qz, azi, bzi, m2, mh + N_ZVZ * a.fs);
         }
         ew[N_XVX * a.fs] = qx; ew[N_YVY * a.fs] = qy; ew[N_ZVZ * a.fs] = qz;
         float q, e1, e2;
@@ -471,24 +502,18 @@ __global__ void __launch_bounds__(256) k_el3d_adj_s(El3dDev a) {
             G[6] += yzh * __ldg(S + 3 * a.sterm);
             G[7] += xzh * __ldg(S + 4 * a.sterm);
             q = g44 * yzh; e1 = q; e2 = q;
-            if (sh_yz) {
-                if (azh != 0.f) e1 = pml_ad(q, azh, bzh, mh + N_ZVY * a.fs);
-                if (ayh != 0.f) e2 = pml_ad(q, ayh, byh, mh + N_YVZ * a.fs);
-            }
+            if (p3) e1 = pml_adr(q, azh, bzh, m3, mh + N_ZVY * a.fs);
+            if (p4) e2 = pml_adr(q, ayh, byh, m4, mh + N_YVZ * a.fs);
             ew[N_ZVY * a.fs] = e1; ew[N_YVZ * a.fs] = e2;
             q = g55 * xzh; e1 = q; e2 = q;
-            if (sh_xz) {
-                if (azh != 0.f) e1 = pml_ad(q, azh, bzh, mh + N_ZVX * a.fs);
-                if (axh != 0.f) e2 = pml_ad(q, axh, bxh, mh + N_XVZ * a.fs);
-            }
+            if (p5) e1 = pml_adr(q, azh, bzh, m5, mh + N_ZVX * a.fs);
+            if (p6) e2 = pml_adr(q, axh, bxh, m6, mh + N_XVZ * a.fs);
             ew[N_ZVX * a.fs] = e1; ew[N_XVZ * a.fs] = e2;
         }
         G[8] += xyh * __ldg(S + 5 * a.sterm);
         q = g66 * xyh; e1 = q; e2 = q;
-        if (sh_xy) {
-            if (ayh != 0.f) e1 = pml_ad(q, ayh, byh, mh + N_YVX * a.fs);
-            if (axh != 0.f) e2 = pml_ad(q, axh, bxh, mh + N_XVY * a.fs);
-        }
+        if (p7) e1 = pml_adr(q, ayh, byh, m7, mh + N_YVX * a.fs);
+        if (p8) e2 = pml_adr(q, axh, bxh, m8, mh + N_XVY * a.fs);
         ew[N_YVX * a.fs] = e1; ew[N_XVY * a.fs] = e2;
     }
     const long long go = (long long)c.grp * a.fs + o;
@@ -879,20 +904,21 @@ struct El3dEngine : SsgBase {
     // those taps go to the rows they copy; rows above the images hold zero
     void rec_taps(const owl_receiver& q, int comp, std::vector<TapPt>& taps) const override {
         const bool fsf = desc.free_surface != 0;
-        for (int irz = -4; irz <= 4; ++irz)
-            for (int iry = -4; iry <= 4; ++iry)
+        // the staggered axis of the component uses the half-node weights; taps
+        // with a zero factor are dropped here (the table keeps none of them),
+        // which keeps a node-centred receiver at 8 taps instead of 9^3
+        const float* fx = comp == 0 ? q.interp_hx : q.interp_ix;
+        const float* fy = comp == 1 ? q.interp_hy : q.interp_iy;
+        const float* fz = comp == 2 ? q.interp_hz : q.interp_iz;
+        const int i0 = comp == 0 ? q.hx : q.gx, j0 = comp == 1 ? q.hy : q.gy, k0 = comp == 2 ? q.hz : q.gz;
+        const int field = comp == 0 ? E3_VX : comp == 1 ? E3_VY : E3_VZ;
+        for (int irz = -4; irz <= 4; ++irz) {
+            if (fz[irz + 4] == 0.f) continue;
+            for (int iry = -4; iry <= 4; ++iry) {
+                if (fy[iry + 4] == 0.f) continue;
                 for (int irx = -4; irx <= 4; ++irx) {
-                    const int a = irx + 4, b = iry + 4, c = irz + 4;
-                    TapPt t;
-                    if (comp == 0)
-                        t = TapPt{E3_VX, q.hx + irx, q.gy + iry, q.gz + irz,
-                                  q.interp_hx[a] * q.interp_iy[b] * q.interp_iz[c] * q.weight};
-                    else if (comp == 1)
-                        t = TapPt{E3_VY, q.gx + irx, q.hy + iry, q.gz + irz,
-                                  q.interp_ix[a] * q.interp_hy[b] * q.interp_iz[c] * q.weight};
-                    else
-                        t = TapPt{E3_VZ, q.gx + irx, q.gy + iry, q.hz + irz,
-                                  q.interp_ix[a] * q.interp_iy[b] * q.interp_hz[c] * q.weight};
+                    if (fx[irx + 4] == 0.f) continue;
+                    TapPt t{field, i0 + irx, j0 + iry, k0 + irz, fx[irx + 4] * fy[iry + 4] * fz[irz + 4] * q.weight};
                     if (fsf) {
                         const int top = comp == 2 ? 1 : 0;  // last image row: vz images rows <= 1
                         if (t.k <= top) {
@@ -902,6 +928,8 @@ struct El3dEngine : SsgBase {
                     }
                     taps.push_back(t);
                 }
+            }
+        }
     }
 
     El3dDev dev(int S) const {

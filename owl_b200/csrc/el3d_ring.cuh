@@ -6,8 +6,10 @@
 // chunk of z planes. Every in-plane operand -- the neighbour tiles with their R
 // halo, the cell's own fields and its moduli / buoyancies -- arrives in an
 // NS-stage shared-memory ring by 16-byte cp.async copies issued NS-1 planes
-// ahead (copy slots computed once per CTA, ring.cuh). z derivatives come from a
-// register queue of 2R values per field, fed from the ring's "ahead" tiles.
+// ahead (copy slots computed once per CTA, ring.cuh), right after the plane's
+// one barrier. z derivatives come from a register queue of 2R values per field,
+// fed from the ring's "ahead" tiles. The CPML memories of a cell are read
+// before the ring wait and written back after the update.
 // The arithmetic and its order are those of k_el3d_fwd_s / k_el3d_fwd_v.
 #pragma once
 
@@ -104,17 +106,30 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
             cp_commit();
         }
         for (int z = zb, i = 0; z < ze; ++z, ++i) {
+            // the plane's z coefficients and the cell's CPML memories, loaded
+            // before the ring wait so that their latency overlaps it
+            const long long o = (long long)z * pl + oxy;
+            float* mo = m + o;
+            const bool ozi = e3_out(z, a.pr, a.nz, false), ozh = e3_out(z, a.pr, a.nz, true);
+            const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
+            const bool sh_n = valid && (oxi || oyi || ozi), sh_yz = valid && (oxi || oyh || ozh),
+                       sh_xz = valid && (oxh || oyi || ozh), sh_xy = valid && (oxh || oyh || ozi);
+            const bool p0 = sh_n && axi != 0.f, p1 = sh_n && ayi != 0.f, p2 = sh_n && azi != 0.f;
+            const bool p3 = sh_yz && ayh != 0.f, p4 = sh_yz && azh != 0.f;
+            const bool p5 = sh_xz && axh != 0.f, p6 = sh_xz && azh != 0.f;
+            const bool p7 = sh_xy && axh != 0.f, p8 = sh_xy && ayh != 0.f;
+            const float m0 = p0 ? mo[N_XVX * fs] : 0.f, m1 = p1 ? mo[N_YVY * fs] : 0.f, m2 = p2 ? mo[N_ZVZ * fs] : 0.f;
+            const float m3 = p3 ? mo[N_YVZ * fs] : 0.f, m4 = p4 ? mo[N_ZVY * fs] : 0.f;
+            const float m5 = p5 ? mo[N_XVZ * fs] : 0.f, m6 = p6 ? mo[N_ZVX * fs] : 0.f;
+            const float m7 = p7 ? mo[N_XVY * fs] : 0.f, m8 = p8 ? mo[N_YVX * fs] : 0.f;
+            // plane z's group is complete once at most NS-2 later groups are pending; the
+            // barrier also retires every read of the stage refilled next (plane z-1's)
+            cp_wait<E3R_NS - 2>();
+            __syncthreads();
             if (z + E3R_NS - 1 < ze) issue(z + E3R_NS - 1, (i + E3R_NS - 1) % E3R_NS);
             cp_commit();
-            cp_wait<E3R_NS - 1>();
-            __syncthreads();
             const float* st = ring + (i % E3R_NS) * T::STAGE;
             if (valid) {
-                const long long o = (long long)z * pl + oxy;
-                const bool ozi = e3_out(z, a.pr, a.nz, false), ozh = e3_out(z, a.pr, a.nz, true);
-                const bool sh_n = oxi || oyi || ozi, sh_yz = oxi || oyh || ozh, sh_xz = oxh || oyi || ozh,
-                           sh_xy = oxh || oyh || ozi;
-                const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
                 const float* tvx = st + T::OVX + (ty + R) * T::WX + tx + R;
                 const float* tvy = st + T::OVY + (ty + R) * T::WX + tx + R;
                 const float* tvz = st + T::OVZ + (ty + R) * T::WX + tx + R;
@@ -130,12 +145,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
                     sZ = sZ + c_fd3e[q - 1] * (qz[R - 1 + q] - qz[R - q]);
                 }
                 float dX = a.idx * sX, dY = a.idy * sY, dZ = a.idz * sZ;
-                float* mo = m + o;
-                if (sh_n) {
-                    if (axi != 0.f) dX = pml_fw(dX, axi, bxi, mo + N_XVX * fs);
-                    if (ayi != 0.f) dY = pml_fw(dY, ayi, byi, mo + N_YVY * fs);
-                    if (azi != 0.f) dZ = pml_fw(dZ, azi, bzi, mo + N_ZVZ * fs);
-                }
+                if (p0) dX = pml_up(dX, axi, bxi, m0, mo + N_XVX * fs);
+                if (p1) dY = pml_up(dY, ayi, byi, m1, mo + N_YVY * fs);
+                if (p2) dZ = pml_up(dZ, azi, bzi, m2, mo + N_ZVZ * fs);
                 const float* so = st + T::OS + lo;
                 stp[E3_XX * fs + o] = so[0] + a.dt * (c11 * dX + c12 * dY + c13 * dZ);
                 stp[E3_YY * fs + o] = so[T::T] + a.dt * (c12 * dX + c22 * dY + c23 * dZ);
@@ -148,10 +160,8 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
                     a2 = a2 + c_fd3e[q - 1] * (tvz[(q - 1) * T::WX] - tvz[-q * T::WX]);
                 }
                 float dzvy = a.idz * a1, dyvz = a.idy * a2;
-                if (sh_yz) {
-                    if (ayh != 0.f) dyvz = pml_fw(dyvz, ayh, byh, mo + N_YVZ * fs);
-                    if (azh != 0.f) dzvy = pml_fw(dzvy, azh, bzh, mo + N_ZVY * fs);
-                }
+                if (p3) dyvz = pml_up(dyvz, ayh, byh, m3, mo + N_YVZ * fs);
+                if (p4) dzvy = pml_up(dzvy, azh, bzh, m4, mo + N_ZVY * fs);
                 stp[E3_YZ * fs + o] = so[3 * T::T] + g44 * (dzvy + dyvz);
                 // sxz: dz vx + dx vz
                 a1 = 0.f; a2 = 0.f;
@@ -161,10 +171,8 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
                     a2 = a2 + c_fd3e[q - 1] * (tvz[q - 1] - tvz[-q]);
                 }
                 float dzvx = a.idz * a1, dxvz = a.idx * a2;
-                if (sh_xz) {
-                    if (axh != 0.f) dxvz = pml_fw(dxvz, axh, bxh, mo + N_XVZ * fs);
-                    if (azh != 0.f) dzvx = pml_fw(dzvx, azh, bzh, mo + N_ZVX * fs);
-                }
+                if (p5) dxvz = pml_up(dxvz, axh, bxh, m5, mo + N_XVZ * fs);
+                if (p6) dzvx = pml_up(dzvx, azh, bzh, m6, mo + N_ZVX * fs);
                 stp[E3_XZ * fs + o] = so[4 * T::T] + g55 * (dzvx + dxvz);
                 // sxy: dy vx + dx vy
                 a1 = 0.f; a2 = 0.f;
@@ -174,10 +182,8 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
                     a2 = a2 + c_fd3e[q - 1] * (tvy[q - 1] - tvy[-q]);
                 }
                 float dyvx = a.idy * a1, dxvy = a.idx * a2;
-                if (sh_xy) {
-                    if (axh != 0.f) dxvy = pml_fw(dxvy, axh, bxh, mo + N_XVY * fs);
-                    if (ayh != 0.f) dyvx = pml_fw(dyvx, ayh, byh, mo + N_YVX * fs);
-                }
+                if (p7) dxvy = pml_up(dxvy, axh, bxh, m7, mo + N_XVY * fs);
+                if (p8) dyvx = pml_up(dyvx, ayh, byh, m8, mo + N_YVX * fs);
                 stp[E3_XY * fs + o] = so[5 * T::T] + g66 * (dyvx + dxvy);
                 if (STORE) {
                     float* S = a.S + slot + s * fs + o;
@@ -194,7 +200,6 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
             qx[2 * R - 1] = st[T::OA + lo];
             qy[2 * R - 1] = st[T::OA + T::T + lo];
             qz[2 * R - 1] = st[T::OA + 2 * T::T + lo];
-            __syncthreads();
         }
         cp_wait<0>();
         __syncthreads();
@@ -272,22 +277,31 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_v_ring(El3dDev a) {
             cp_commit();
         }
         for (int z = zb, i = 0; z < ze; ++z, ++i) {
+            // the plane's z coefficients and the cell's CPML memories, loaded
+            // before the ring wait so that their latency overlaps it
+            const long long o = (long long)z * pl + oxy;
+            float* mo = m + o;
+            const bool ozi = e3_out(z, a.pr, a.nz, false), ozh = e3_out(z, a.pr, a.nz, true);
+            const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
+            const bool sh_vx = valid && (oxh || oyi || ozi), sh_vy = valid && (oxi || oyh || ozi),
+                       sh_vz = valid && (oxi || oyi || ozh);
+            const bool p0 = sh_vx && axh != 0.f, p1 = sh_vx && ayi != 0.f, p2 = sh_vx && azi != 0.f;
+            const bool p3 = sh_vy && axi != 0.f, p4 = sh_vy && ayh != 0.f, p5 = sh_vy && azi != 0.f;
+            const bool p6 = sh_vz && axi != 0.f, p7 = sh_vz && ayi != 0.f, p8 = sh_vz && azh != 0.f;
+            const float m0 = p0 ? mo[N_XXX * fs] : 0.f, m1 = p1 ? mo[N_YXY * fs] : 0.f, m2 = p2 ? mo[N_ZXZ * fs] : 0.f;
+            const float m3 = p3 ? mo[N_XXY * fs] : 0.f, m4 = p4 ? mo[N_YYY * fs] : 0.f, m5 = p5 ? mo[N_ZYZ * fs] : 0.f;
+            const float m6 = p6 ? mo[N_XXZ * fs] : 0.f, m7 = p7 ? mo[N_YYZ * fs] : 0.f, m8 = p8 ? mo[N_ZZZ * fs] : 0.f;
+            cp_wait<E3R_NS - 2>();
+            __syncthreads();
             if (z + E3R_NS - 1 < ze) issue(z + E3R_NS - 1, (i + E3R_NS - 1) % E3R_NS);
             cp_commit();
-            cp_wait<E3R_NS - 1>();
-            __syncthreads();
             const float* st = ring + (i % E3R_NS) * T::STAGE;
             if (valid) {
-                const long long o = (long long)z * pl + oxy;
-                const bool ozi = e3_out(z, a.pr, a.nz, false), ozh = e3_out(z, a.pr, a.nz, true);
-                const bool sh_vx = oxh || oyi || ozi, sh_vy = oxi || oyh || ozi, sh_vz = oxi || oyi || ozh;
-                const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
                 const float* txx = st + T::OXX + ty * T::WX + tx + R;
                 const float* tyy = st + T::OYY + (ty + R) * 32 + tx;
                 const float* txy = st + T::OXY + (ty + R) * T::WX + tx + R;
                 const float* txz = st + T::OXZ + ty * T::WX + tx + R;
                 const float* tyz = st + T::OYZ + (ty + R) * 32 + tx;
-                float* mo = m + o;
                 // vx: dx sxx (M) + dy sxy (P) + dz sxz (P)
                 float h1 = 0.f, h2 = 0.f, h3 = 0.f;
 #pragma unroll
@@ -297,11 +311,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_v_ring(El3dDev a) {
                     h3 = h3 + c_fd3e[q - 1] * (qxz[R - 1 + q] - qxz[R - q]);
                 }
                 h1 = a.idx * h1; h2 = a.idy * h2; h3 = a.idz * h3;
-                if (sh_vx) {
-                    if (axh != 0.f) h1 = pml_fw(h1, axh, bxh, mo + N_XXX * fs);
-                    if (ayi != 0.f) h2 = pml_fw(h2, ayi, byi, mo + N_YXY * fs);
-                    if (azi != 0.f) h3 = pml_fw(h3, azi, bzi, mo + N_ZXZ * fs);
-                }
+                if (p0) h1 = pml_up(h1, axh, bxh, m0, mo + N_XXX * fs);
+                if (p1) h2 = pml_up(h2, ayi, byi, m1, mo + N_YXY * fs);
+                if (p2) h3 = pml_up(h3, azi, bzi, m2, mo + N_ZXZ * fs);
                 const float hx = h1 + h2 + h3;
                 stp[E3_VX * fs + o] = st[T::OV + lo] + st[T::OB + lo] * hx;
                 // vy: dx sxy (P) + dy syy (M) + dz syz (P)
@@ -313,11 +325,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_v_ring(El3dDev a) {
                     h3 = h3 + c_fd3e[q - 1] * (qyz[R - 1 + q] - qyz[R - q]);
                 }
                 h1 = a.idx * h1; h2 = a.idy * h2; h3 = a.idz * h3;
-                if (sh_vy) {
-                    if (axi != 0.f) h1 = pml_fw(h1, axi, bxi, mo + N_XXY * fs);
-                    if (ayh != 0.f) h2 = pml_fw(h2, ayh, byh, mo + N_YYY * fs);
-                    if (azi != 0.f) h3 = pml_fw(h3, azi, bzi, mo + N_ZYZ * fs);
-                }
+                if (p3) h1 = pml_up(h1, axi, bxi, m3, mo + N_XXY * fs);
+                if (p4) h2 = pml_up(h2, ayh, byh, m4, mo + N_YYY * fs);
+                if (p5) h3 = pml_up(h3, azi, bzi, m5, mo + N_ZYZ * fs);
                 const float hy = h1 + h2 + h3;
                 stp[E3_VY * fs + o] = st[T::OV + T::T + lo] + st[T::OB + T::T + lo] * hy;
                 // vz: dx sxz (P) + dy syz (P) + dz szz (M)
@@ -329,11 +339,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_v_ring(El3dDev a) {
                     h3 = h3 + c_fd3e[q - 1] * (qzz[R + q - 1] - qzz[R - q]);
                 }
                 h1 = a.idx * h1; h2 = a.idy * h2; h3 = a.idz * h3;
-                if (sh_vz) {
-                    if (axi != 0.f) h1 = pml_fw(h1, axi, bxi, mo + N_XXZ * fs);
-                    if (ayi != 0.f) h2 = pml_fw(h2, ayi, byi, mo + N_YYZ * fs);
-                    if (azh != 0.f) h3 = pml_fw(h3, azh, bzh, mo + N_ZZZ * fs);
-                }
+                if (p6) h1 = pml_up(h1, axi, bxi, m6, mo + N_XXZ * fs);
+                if (p7) h2 = pml_up(h2, ayi, byi, m7, mo + N_YYZ * fs);
+                if (p8) h3 = pml_up(h3, azh, bzh, m8, mo + N_ZZZ * fs);
                 const float hz = h1 + h2 + h3;
                 stp[E3_VZ * fs + o] = st[T::OV + 2 * T::T + lo] + st[T::OB + 2 * T::T + lo] * hz;
                 if (STORE) {
@@ -350,7 +358,6 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_v_ring(El3dDev a) {
             qxz[2 * R - 1] = st[T::OA + lo];
             qyz[2 * R - 1] = st[T::OA + T::T + lo];
             qzz[2 * R - 1] = st[T::OA + 2 * T::T + lo];
-            __syncthreads();
         }
         cp_wait<0>();
         __syncthreads();
