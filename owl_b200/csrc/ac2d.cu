@@ -70,24 +70,29 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
         const long long so = s * a.sst + o;
         const float* vx = a.vx + so;
         const float* vz = a.vz + so;
+        // the cell's own values are read ahead of its stores: the arrays share
+        // one allocation, so no plain read could move above a store; the
+        // neighbours' fields, which this launch does not write, are read
+        // through the read-only path
+        const float p0 = a.p[so], m1 = px ? a.m1[so] : 0.f, m2 = pz ? a.m2[so] : 0.f;
         float sx = 0.f, sz = 0.f;
 #pragma unroll
-        for (int k = 1; k <= R; ++k) sx = sx + c_fd2[k - 1] * (vx[k] - vx[1 - k]);
+        for (int k = 1; k <= R; ++k) sx = sx + c_fd2[k - 1] * (__ldg(vx + k) - __ldg(vx + 1 - k));
 #pragma unroll
-        for (int k = 1; k <= R; ++k) sz = sz + c_fd2[k - 1] * (vz[k * pt] - vz[(1 - k) * pt]);
+        for (int k = 1; k <= R; ++k) sz = sz + c_fd2[k - 1] * (__ldg(vz + k * pt) - __ldg(vz + (1 - k) * pt));
         float gx = a.idx * sx, gz = a.idz * sz;
         if (px) {
-            float m = ax * gx + bx * a.m1[so];
+            float m = ax * gx + bx * m1;
             a.m1[so] = m;
             gx = gx + m;
         }
         if (pz) {
-            float m = az * gz + bz * a.m2[so];
+            float m = az * gz + bz * m2;
             a.m2[so] = m;
             gz = gz + m;
         }
         const float g = gx + gz;
-        const float pn = a.p[so] - dtbk * g;
+        const float pn = p0 - dtbk * g;
         a.p[so] = pn;
         if (mirror) a.p[s * a.sst + omir] = -pn;
         if (STORE) a.Sp[slot + s * a.fs + o] = g;
@@ -114,30 +119,33 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_v(Ac2dDev a) {
     for (int s = s0; s < s1; ++s) {
         const long long so = s * a.sst + o;
         const float* p = a.p + so;
+        // the cell's own values are read ahead of its stores (see k_ac2d_fwd_p)
+        const float vx0 = dox ? a.vx[so] : 0.f, m3 = dox && px ? a.m3[so] : 0.f;
+        const float vz0 = doz ? a.vz[so] : 0.f, m4 = doz && pz ? a.m4[so] : 0.f;
         if (dox) {
             float sx = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sx = sx + c_fd2[k - 1] * (p[k - 1] - p[-k]);
+            for (int k = 1; k <= R; ++k) sx = sx + c_fd2[k - 1] * (__ldg(p + k - 1) - __ldg(p - k));
             float h = a.idx * sx;
             if (px) {
-                float m = ax * h + bx * a.m3[so];
+                float m = ax * h + bx * m3;
                 a.m3[so] = m;
                 h = h + m;
             }
-            a.vx[so] = a.vx[so] - bxc * h;
+            a.vx[so] = vx0 - bxc * h;
             if (STORE) a.Svx[slot + s * a.fs + o] = h;
         }
         if (doz) {
             float sz = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sz = sz + c_fd2[k - 1] * (p[(k - 1) * pt] - p[-k * pt]);
+            for (int k = 1; k <= R; ++k) sz = sz + c_fd2[k - 1] * (__ldg(p + (k - 1) * pt) - __ldg(p - k * pt));
             float h = a.idz * sz;
             if (pz) {
-                float m = az * h + bz * a.m4[so];
+                float m = az * h + bz * m4;
                 a.m4[so] = m;
                 h = h + m;
             }
-            a.vz[so] = a.vz[so] - bzc * h;
+            a.vz[so] = vz0 - bzc * h;
             if (STORE) a.Svz[slot + s * a.fs + o] = h;
         }
     }
@@ -182,37 +190,47 @@ __global__ void __launch_bounds__(512) k_ac2d_adj_p(Ac2dDev a) {
     float gbk = 0.f, gbx = 0.f, gbz = 0.f;
     for (int s = s0; s < s1; ++s) {
         const long long sa = s * a.sad + o, ss = slot + s * a.fs + o;
-        if (ownx) gbx += a.avx[sa] * a.Svx[ss];
-        if (ownz) gbz += a.avz[sa] * a.Svz[ss];
+        // every read of the shot's cell is issued ahead of its stores: the
+        // arrays share one allocation, so no plain read could move above a
+        // store and each would cost its own round trip. Arrays that no thread
+        // of this launch writes (the e terms of the neighbours, the stored
+        // stencil terms) are read through the read-only path, which the
+        // compiler may schedule freely.
+        const float vx = ownx ? a.avx[sa] : 0.f, svx = ownx ? __ldg(a.Svx + ss) : 0.f;
+        const float vz = ownz ? a.avz[sa] : 0.f, svz = ownz ? __ldg(a.Svz + ss) : 0.f;
+        const float p0 = dop ? a.ap[sa] : 0.f, sp = dop ? __ldg(a.Sp + ss) : 0.f;
+        const float m1 = dop && px ? a.am1[sa] : 0.f, m2 = dop && pz ? a.am2[sa] : 0.f;
+        if (ownx) gbx += vx * svx;
+        if (ownz) gbz += vz * svz;
         if (!dop) continue;
         const float* ex = a.aex + sa;
         const float* ez = a.aez + sa;
         float sx = 0.f, sz = 0.f;
 #pragma unroll
-        for (int k = 1; k <= R; ++k) sx = sx + c_fd2[k - 1] * (ex[1 - k] - ex[k]);
+        for (int k = 1; k <= R; ++k) sx = sx + c_fd2[k - 1] * (__ldg(ex + 1 - k) - __ldg(ex + k));
 #pragma unroll
-        for (int k = 1; k <= R; ++k) sz = sz + c_fd2[k - 1] * (ez[(1 - k) * pt] - ez[k * pt]);
+        for (int k = 1; k <= R; ++k) sz = sz + c_fd2[k - 1] * (__ldg(ez + (1 - k) * pt) - __ldg(ez + k * pt));
         float dP = a.idx * sx + a.idz * sz;
         if (mirror) {
             // p(i, 2-j) = -p(i, j), j <= 0: the adjoint landing on the mirror row folds back with a minus
             const float* em = a.aez + s * a.sad + om;
             float sm = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sm = sm + c_fd2[k - 1] * (em[(1 - k) * pt] - em[k * pt]);
+            for (int k = 1; k <= R; ++k) sm = sm + c_fd2[k - 1] * (__ldg(em + (1 - k) * pt) - __ldg(em + k * pt));
             dP = dP - a.idz * sm;
         }
-        const float ph = a.ap[sa] + dP;
+        const float ph = p0 + dP;
         a.ap[sa] = ph;
-        gbk += ph * a.Sp[ss];
+        gbk += ph * sp;
         const float q = -bk * ph;
         float epx = q, epz = q;
         if (px) {
-            float u = q + a.am1[sa];
+            float u = q + m1;
             a.am1[sa] = bxi * u;
             epx = q + axi * u;
         }
         if (pz) {
-            float u = q + a.am2[sa];
+            float u = q + m2;
             a.am2[sa] = bzi * u;
             epz = q + azi * u;
         }
@@ -244,17 +262,20 @@ __global__ void __launch_bounds__(512) k_ac2d_adj_v(Ac2dDev a) {
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     for (int s = s0; s < s1; ++s) {
         const long long sa = s * a.sad + o;
+        // the shot's cell values are read ahead of its stores (see k_ac2d_adj_p)
+        const float vx = dox ? a.avx[sa] : 0.f, m3 = dox && px ? a.am3[sa] : 0.f;
+        const float vz = doz ? a.avz[sa] : 0.f, m4 = doz && pz ? a.am4[sa] : 0.f;
         if (dox) {
             const float* ep = a.aepx + sa;
             float sx = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sx = sx + c_fd2[k - 1] * (ep[-k] - ep[k - 1]);
-            const float xh = a.avx[sa] + a.idx * sx;
+            for (int k = 1; k <= R; ++k) sx = sx + c_fd2[k - 1] * (__ldg(ep - k) - __ldg(ep + k - 1));
+            const float xh = vx + a.idx * sx;
             a.avx[sa] = xh;
             const float q = -bxc * xh;
             float e = q;
             if (px) {
-                float u = q + a.am3[sa];
+                float u = q + m3;
                 a.am3[sa] = bxh * u;
                 e = q + axh * u;
             }
@@ -264,13 +285,13 @@ __global__ void __launch_bounds__(512) k_ac2d_adj_v(Ac2dDev a) {
             const float* ep = a.aepz + sa;
             float sz = 0.f;
 #pragma unroll
-            for (int k = 1; k <= R; ++k) sz = sz + c_fd2[k - 1] * (ep[-k * pt] - ep[(k - 1) * pt]);
-            const float zh = a.avz[sa] + a.idz * sz;
+            for (int k = 1; k <= R; ++k) sz = sz + c_fd2[k - 1] * (__ldg(ep - k * pt) - __ldg(ep + (k - 1) * pt));
+            const float zh = vz + a.idz * sz;
             a.avz[sa] = zh;
             const float q = -bzc * zh;
             float e = q;
             if (pz) {
-                float u = q + a.am4[sa];
+                float u = q + m4;
                 a.am4[sa] = bzh * u;
                 e = q + azh * u;
             }
