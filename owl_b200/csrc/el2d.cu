@@ -70,9 +70,9 @@ __device__ __forceinline__ bool el_pml_int(int x, int pr, int n) { return x < pr
 __device__ __forceinline__ bool el_pml_half(int x, int pr, int n) { return x <= pr || x >= pr + n; }
 
 // adjoint of psi_new = a D + b psi_old, D' = D + psi_new, given q = adjoint of D'
-__device__ __forceinline__ float pml_e(float q, float a, float b, float& psih) {
+__device__ __forceinline__ float pml_e(float q, float a, float b, float psih, float* dst) {
     const float u = q + psih;
-    psih = b * u;
+    *dst = b * u;
     return q + a * u;
 }
 
@@ -101,6 +101,16 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_s(El2dDev a) {
         const float* vx = st + EL_VX * a.fs + o;
         const float* vz = st + EL_VZ * a.fs + o;
         float* mem = st + EL_M0 * a.fs + o;
+        float* sxx = st + EL_SXX * a.fs + o;
+        float* szz = st + EL_SZZ * a.fs + o;
+        float* sxzp = st + EL_SXZ * a.fs + o;
+        // the cell's own stresses and memories are read ahead of its stores:
+        // the fields share one allocation, so no plain read could move above a
+        // store and each would cost its own round trip
+        const float xx0 = *sxx, zz0 = row1 ? 0.f : *szz, xz0 = dxz ? *sxzp : 0.f;
+        const float mxv = (row1 ? px_i : pii) ? mem[M_DXVX * a.fs] : 0.f;
+        const float mzv = !row1 && pii ? mem[M_DZVZ * a.fs] : 0.f;
+        const float mxz = dxz && phh ? mem[M_DXVZ * a.fs] : 0.f, mzx = dxz && phh ? mem[M_DZVX * a.fs] : 0.f;
         // sigma_xx, sigma_zz
         float sx = 0.f;
 #pragma unroll
@@ -108,7 +118,7 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_s(El2dDev a) {
         float dxv = a.idx * sx, dzv;
         if (row1) {
             if (px_i) {
-                const float m = cii.x * dxv + cii.y * mem[M_DXVX * a.fs];
+                const float m = cii.x * dxv + cii.y * mxv;
                 mem[M_DXVX * a.fs] = m;
                 dxv = dxv + m;
             }
@@ -119,21 +129,19 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_s(El2dDev a) {
             for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(vz + (k * pt)) - __ldg(vz + ((1 - k) * pt)));
             dzv = a.idz * sz;
             if (pii) {
-                const float m1 = cii.x * dxv + cii.y * mem[M_DXVX * a.fs];
+                const float m1 = cii.x * dxv + cii.y * mxv;
                 mem[M_DXVX * a.fs] = m1;
                 dxv = dxv + m1;
-                const float m2 = cii.z * dzv + cii.w * mem[M_DZVZ * a.fs];
+                const float m2 = cii.z * dzv + cii.w * mzv;
                 mem[M_DZVZ * a.fs] = m2;
                 dzv = dzv + m2;
             }
         }
-        float* sxx = st + EL_SXX * a.fs + o;
-        float* szz = st + EL_SZZ * a.fs + o;
-        *sxx = *sxx + a.dt * (c11 * dxv + c13 * dzv);
+        *sxx = xx0 + a.dt * (c11 * dxv + c13 * dzv);
         if (row1) {
             *szz = 0.f;
         } else {
-            const float zn = *szz + a.dt * (c13 * dxv + c33 * dzv);
+            const float zn = zz0 + a.dt * (c13 * dxv + c33 * dzv);
             *szz = zn;
             if (mir) st[EL_SZZ * a.fs + (long long)(2 * a.pr - z) * pt + x] = -zn;
         }
@@ -150,16 +158,15 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_s(El2dDev a) {
             for (int k = 1; k <= R; ++k) sxz = sxz + c_fde[k - 1] * (__ldg(vz + (k - 1)) - __ldg(vz + (-k)));
             float dzvx = a.idz * szx, dxvz = a.idx * sxz;
             if (phh) {
-                const float m3 = chh.x * dxvz + chh.y * mem[M_DXVZ * a.fs];
+                const float m3 = chh.x * dxvz + chh.y * mxz;
                 mem[M_DXVZ * a.fs] = m3;
                 dxvz = dxvz + m3;
-                const float m4 = chh.z * dzvx + chh.w * mem[M_DZVX * a.fs];
+                const float m4 = chh.z * dzvx + chh.w * mzx;
                 mem[M_DZVX * a.fs] = m4;
                 dzvx = dzvx + m4;
             }
             const float g = dzvx + dxvz;
-            float* sxzp = st + EL_SXZ * a.fs + o;
-            const float xn = *sxzp + c55dt * g;
+            const float xn = xz0 + c55dt * g;
             *sxzp = xn;
             if (mir) st[EL_SXZ * a.fs + (long long)(2 * a.pr + 1 - z) * pt + x] = -xn;
             if (STORE) a.S[2 * a.sterm + slot + s * a.fs + o] = g;
@@ -188,6 +195,10 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
         const float* szz = st + EL_SZZ * a.fs + o;
         const float* sxz = st + EL_SXZ * a.fs + o;
         float* mem = st + EL_M0 * a.fs + o;
+        // own velocities and memories ahead of the stores (see k_el2d_fwd_s)
+        const float vx0 = st[EL_VX * a.fs + o], vz0 = dvz ? st[EL_VZ * a.fs + o] : 0.f;
+        const float m_xxx = phi ? mem[M_DXXX * a.fs] : 0.f, m_zxz = phi ? mem[M_DZXZ * a.fs] : 0.f;
+        const float m_xxz = dvz && pih ? mem[M_DXXZ * a.fs] : 0.f, m_zzz = dvz && pih ? mem[M_DZZZ * a.fs] : 0.f;
         {
             float sx = 0.f, sz = 0.f;
 #pragma unroll
@@ -196,16 +207,15 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
             for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(sxz + (k * pt)) - __ldg(sxz + ((1 - k) * pt)));
             float hx = a.idx * sx, hz = a.idz * sz;
             if (phi) {
-                const float m1 = chi.x * hx + chi.y * mem[M_DXXX * a.fs];
+                const float m1 = chi.x * hx + chi.y * m_xxx;
                 mem[M_DXXX * a.fs] = m1;
                 hx = hx + m1;
-                const float m2 = chi.z * hz + chi.w * mem[M_DZXZ * a.fs];
+                const float m2 = chi.z * hz + chi.w * m_zxz;
                 mem[M_DZXZ * a.fs] = m2;
                 hz = hz + m2;
             }
             const float h = hx + hz;
-            float* v = st + EL_VX * a.fs + o;
-            *v = *v + bx * h;
+            st[EL_VX * a.fs + o] = vx0 + bx * h;
             if (STORE) a.S[3 * a.sterm + slot + s * a.fs + o] = h;
         }
         if (dvz) {
@@ -216,16 +226,15 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
             for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(szz + ((k - 1) * pt)) - __ldg(szz + (-k * pt)));
             float hx = a.idx * sx, hz = a.idz * sz;
             if (pih) {
-                const float m1 = cih.x * hx + cih.y * mem[M_DXXZ * a.fs];
+                const float m1 = cih.x * hx + cih.y * m_xxz;
                 mem[M_DXXZ * a.fs] = m1;
                 hx = hx + m1;
-                const float m2 = cih.z * hz + cih.w * mem[M_DZZZ * a.fs];
+                const float m2 = cih.z * hz + cih.w * m_zzz;
                 mem[M_DZZZ * a.fs] = m2;
                 hz = hz + m2;
             }
             const float h = hx + hz;
-            float* v = st + EL_VZ * a.fs + o;
-            *v = *v + bz * h;
+            st[EL_VZ * a.fs + o] = vz0 + bz * h;
             if (STORE) a.S[4 * a.sterm + slot + s * a.fs + o] = h;
         }
     }
@@ -268,6 +277,10 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
         float* e = ad + 13 * a.fs + o;
         float* mh = ad + 5 * a.fs + o;
         const long long so = slot + s * a.fs + o;
+        // own adjoint velocities and memories ahead of the stores (see k_el2d_fwd_s)
+        const float vx0 = ad[EL_VX * a.fs + o], vz0 = dvz ? ad[EL_VZ * a.fs + o] : 0.f;
+        const float m_xxx = phi ? mh[M_DXXX * a.fs] : 0.f, m_zxz = phi ? mh[M_DZXZ * a.fs] : 0.f;
+        const float m_xxz = dvz && pih ? mh[M_DXXZ * a.fs] : 0.f, m_zzz = dvz && pih ? mh[M_DZZZ * a.fs] : 0.f;
         {
             const float* e1 = e + M_DXVX * a.fs;
             const float* e2 = e + M_DZVX * a.fs;
@@ -276,15 +289,14 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
             for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (__ldg(e1 + (-k)) - __ldg(e1 + (k - 1)));
 #pragma unroll
             for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(e2 + ((1 - k) * pt)) - __ldg(e2 + (k * pt)));
-            float* vh = ad + EL_VX * a.fs + o;
-            const float v = *vh + (a.idx * sx + a.idz * sz);
-            *vh = v;
+            const float v = vx0 + (a.idx * sx + a.idz * sz);
+            ad[EL_VX * a.fs + o] = v;
             gbx += v * __ldg(a.S + 3 * a.sterm + so);
             const float q = bx * v;
             float ex = q, ez = q;
             if (phi) {
-                ex = pml_e(q, chi.x, chi.y, mh[M_DXXX * a.fs]);
-                ez = pml_e(q, chi.z, chi.w, mh[M_DZXZ * a.fs]);
+                ex = pml_e(q, chi.x, chi.y, m_xxx, mh + M_DXXX * a.fs);
+                ez = pml_e(q, chi.z, chi.w, m_zxz, mh + M_DZXZ * a.fs);
             }
             e[M_DXXX * a.fs] = ex;
             e[M_DZXZ * a.fs] = ez;
@@ -297,15 +309,14 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
             for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(e4 + (-k * pt)) - __ldg(e4 + ((k - 1) * pt)));
 #pragma unroll
             for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (__ldg(e3 + (1 - k)) - __ldg(e3 + (k)));
-            float* vh = ad + EL_VZ * a.fs + o;
-            const float v = *vh + (a.idz * sz + a.idx * sx);
-            *vh = v;
+            const float v = vz0 + (a.idz * sz + a.idx * sx);
+            ad[EL_VZ * a.fs + o] = v;
             gbz += v * __ldg(a.S + 4 * a.sterm + so);
             const float q = bz * v;
             float ex = q, ez = q;
             if (pih) {
-                ex = pml_e(q, cih.x, cih.y, mh[M_DXXZ * a.fs]);
-                ez = pml_e(q, cih.z, cih.w, mh[M_DZZZ * a.fs]);
+                ex = pml_e(q, cih.x, cih.y, m_xxz, mh + M_DXXZ * a.fs);
+                ez = pml_e(q, cih.z, cih.w, m_zzz, mh + M_DZZZ * a.fs);
             }
             e[M_DXXZ * a.fs] = ex;
             e[M_DZZZ * a.fs] = ez;
@@ -349,6 +360,14 @@ __global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
         float* e = ad + 13 * a.fs;
         float* mh = ad + 5 * a.fs + o;
         const long long so = slot + s * a.fs + o;
+        float* xhp = ad + EL_SXX * a.fs + o;
+        float* zhp = ad + EL_SZZ * a.fs + o;
+        float* shp = ad + EL_SXZ * a.fs + o;
+        // own adjoint stresses and memories ahead of the stores (see k_el2d_fwd_s)
+        const float xx0 = *xhp, zz0 = row1 ? 0.f : *zhp, xz0 = dxz ? *shp : 0.f;
+        const float m_xvx = (row1 ? px_i : pii) ? mh[M_DXVX * a.fs] : 0.f;
+        const float m_zvz = !row1 && pii ? mh[M_DZVZ * a.fs] : 0.f;
+        const float m_xvz = dxz && phh ? mh[M_DXVZ * a.fs] : 0.f, m_zvx = dxz && phh ? mh[M_DZVX * a.fs] : 0.f;
         // sigma_xx, sigma_zz
         const float* e5 = e + M_DXXX * a.fs + o;
         const float* e8 = e + M_DZZZ * a.fs + o;
@@ -357,9 +376,7 @@ __global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
         for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (__ldg(e5 + (1 - k)) - __ldg(e5 + (k)));
 #pragma unroll
         for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(e8 + ((1 - k) * pt)) - __ldg(e8 + (k * pt)));
-        float* xhp = ad + EL_SXX * a.fs + o;
-        float* zhp = ad + EL_SZZ * a.fs + o;
-        const float xh = *xhp + a.idx * sx;
+        const float xh = xx0 + a.idx * sx;
         float zh = 0.f;
         if (!row1) {
             float dz = a.idz * sz;
@@ -372,7 +389,7 @@ __global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
                 for (int k = 1; k <= R; ++k) sm = sm + c_fde[k - 1] * __ldg(em + (k * pt));
                 dz = dz + a.idz * sm;
             }
-            zh = *zhp + dz;
+            zh = zz0 + dz;
         }
         *xhp = xh;
         *zhp = zh;
@@ -383,7 +400,7 @@ __global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
             g13 += -2.f * r13 * xh * S0;
             g33 += r13 * r13 * xh * S0;
             const float q = a.dt * c11 * xh - r13 * (a.dt * c13 * xh);
-            ex = px_i ? pml_e(q, cii.x, cii.y, mh[M_DXVX * a.fs]) : q;
+            ex = px_i ? pml_e(q, cii.x, cii.y, m_xvx, mh + M_DXVX * a.fs) : q;
         } else {
             g11 += xh * S0;
             g13 += xh * S1 + zh * S0;
@@ -393,8 +410,8 @@ __global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
             ex = qx;
             ez = qz;
             if (pii) {
-                ex = pml_e(qx, cii.x, cii.y, mh[M_DXVX * a.fs]);
-                ez = pml_e(qz, cii.z, cii.w, mh[M_DZVZ * a.fs]);
+                ex = pml_e(qx, cii.x, cii.y, m_xvx, mh + M_DXVX * a.fs);
+                ez = pml_e(qz, cii.z, cii.w, m_zvz, mh + M_DZVZ * a.fs);
             }
             e[M_DZVZ * a.fs + o] = ez;
         }
@@ -419,15 +436,14 @@ __global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
                 for (int k = 1; k <= R; ++k) mz = mz + c_fde[k - 1] * __ldg(em6 + ((k - 1) * pt));
                 dsum = dsum + a.idz * mz;
             }
-            float* shp = ad + EL_SXZ * a.fs + o;
-            const float sh = *shp + dsum;
+            const float sh = xz0 + dsum;
             *shp = sh;
             g55 += sh * __ldg(a.S + 2 * a.sterm + so);
             const float q = c55dt * sh;
             float ezx = q, exz = q;
             if (phh) {
-                exz = pml_e(q, chh.x, chh.y, mh[M_DXVZ * a.fs]);
-                ezx = pml_e(q, chh.z, chh.w, mh[M_DZVX * a.fs]);
+                exz = pml_e(q, chh.x, chh.y, m_xvz, mh + M_DXVZ * a.fs);
+                ezx = pml_e(q, chh.z, chh.w, m_zvx, mh + M_DZVX * a.fs);
             }
             e[M_DZVX * a.fs + o] = ezx;
             e[M_DXVZ * a.fs + o] = exz;
