@@ -213,7 +213,11 @@ def elastic_3d_block(peak, peak_kind, nshots=4, nt=500):
     out = {"workload": f"3D elastic ORT (nine Cij), 256^3 model (296^3 padded), dt 0.8 ms, {nt} of 2500 steps, "
                        f"{nshots} of 16 vertical-force shots, 128 x 128 three-component receivers",
            "forward_ms": fms, "forward_gcells_per_s": cells * nt * nshots / (fms / 1e3) / 1e9, "kernels": {}}
-    for kid, name in ((L.OWL_K_FWD_P, "k_el3d_fwd_s"), (L.OWL_K_FWD_V, "k_el3d_fwd_v")):
+    # the autotuner's forward kernels: z-marching ring (tile_z 1) or thread per cell
+    ring = s.last_info.tile_z == 1
+    out["forward_kernels"] = "z-marching ring" if ring else "thread per cell"
+    for kid, name in ((L.OWL_K_FWD_P, "k_el3d_fwd_s_ring" if ring else "k_el3d_fwd_s"),
+                      (L.OWL_K_FWD_V, "k_el3d_fwd_v_ring" if ring else "k_el3d_fwd_v")):
         kms, b = s.kernel_time(kid, 10)
         ach = b / (kms / 1e3) / 1e9
         out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,

@@ -322,47 +322,55 @@ __global__ void __launch_bounds__(32 * TY) k_ac3d_adj_v(Ac3dDev a) {
             load_xy_tiles<R, TY>(sx, sy, a.aepx + sa, a.aepy + sa, zo, bx0, by0, a, -1, -1);
             __syncthreads();
             if (valid) {
-                if (z >= a.zvx0) {
+                // the cell's own values are read ahead of its stores (the arrays
+                // share one allocation: no plain read could move above a store);
+                // what this launch does not write goes through the read-only path
+                const bool ox = z >= a.zvx0, oz = z >= a.zvz0;
+                const bool pzz = (!a.fsurf && z <= a.pr) || z >= a.pr + a.nz;
+                const float vx0 = ox ? a.avx[sa + o] : 0.f, vy0 = ox ? a.avy[sa + o] : 0.f;
+                const float vz0 = oz ? a.avz[sa + o] : 0.f;
+                float* m3p = a.am3 + sa + xslab(a, x, y, z);
+                float* m4p = a.am4 + sa + yslab(a, x, y, z);
+                float* m5p = a.am5 + sa + zslab(a, x, y, z);
+                const float m3 = ox && px ? *m3p : 0.f, m4 = ox && py ? *m4p : 0.f, m5 = oz && pzz ? *m5p : 0.f;
+                if (ox) {
                     float h = 0.f, hy = 0.f;
                     // sx col c <-> cell bx0 - R - 1 + c; node x needs cells x-k (col tx+R+1-k) and x+k-1 (col tx+R+k)
 #pragma unroll
                     for (int k = 1; k <= R; ++k) h = h + c_fd3[k - 1] * (sx[ty][tx + R + 1 - k] - sx[ty][tx + R + k]);
 #pragma unroll
                     for (int k = 1; k <= R; ++k) hy = hy + c_fd3[k - 1] * (sy[ty + R + 1 - k][tx] - sy[ty + R + k][tx]);
-                    const float xh = a.avx[sa + o] + a.idx * h;
-                    const float yh = a.avy[sa + o] + a.idy * hy;
+                    const float xh = vx0 + a.idx * h;
+                    const float yh = vy0 + a.idy * hy;
                     a.avx[sa + o] = xh;
                     a.avy[sa + o] = yh;
-                    float qx = -a.dtbx[o] * xh, qy = -a.dtby[o] * yh;
+                    float qx = -__ldg(a.dtbx + o) * xh, qy = -__ldg(a.dtby + o) * yh;
                     float ex = qx, ey = qy;
                     if (px) {
-                        float* m = a.am3 + sa + xslab(a, x, y, z);
-                        float u = qx + *m; *m = bxh * u; ex = qx + axh * u;
+                        float u = qx + m3; *m3p = bxh * u; ex = qx + axh * u;
                     }
                     if (py) {
-                        float* m = a.am4 + sa + yslab(a, x, y, z);
-                        float u = qy + *m; *m = byh * u; ey = qy + ayh * u;
+                        float u = qy + m4; *m4p = byh * u; ey = qy + ayh * u;
                     }
                     a.aex[sa + o] = ex;
                     a.aey[sa + o] = ey;
                 }
-                if (z >= a.zvz0) {
+                if (oz) {
                     float h = 0.f;
 #pragma unroll
                     for (int k = 1; k <= R; ++k) h = h + c_fd3[k - 1] * (q[R - k] - q[R + k - 1]);
-                    const float zh = a.avz[sa + o] + a.idz * h;
+                    const float zh = vz0 + a.idz * h;
                     a.avz[sa + o] = zh;
-                    float qz = -a.dtbz[o] * zh, ez = qz;
-                    if ((!a.fsurf && z <= a.pr) || z >= a.pr + a.nz) {
-                        float* m = a.am5 + sa + zslab(a, x, y, z);
-                        float u = qz + *m; *m = a.bzh[z] * u; ez = qz + a.azh[z] * u;
+                    float qz = -__ldg(a.dtbz + o) * zh, ez = qz;
+                    if (pzz) {
+                        float u = qz + m5; *m5p = a.bzh[z] * u; ez = qz + a.azh[z] * u;
                     }
                     a.aez[sa + o] = ez;
                 }
             }
 #pragma unroll
             for (int j = 0; j < 2 * R - 1; ++j) q[j] = q[j + 1];
-            q[2 * R - 1] = (valid && z + R < a.NZs) ? epz[(long long)(z + R) * a.plane] : 0.f;
+            q[2 * R - 1] = (valid && z + R < a.NZs) ? __ldg(epz + (long long)(z + R) * a.plane) : 0.f;
             __syncthreads();
         }
     }
