@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define OWL_SSG_ABI_VERSION 3
+#define OWL_SSG_ABI_VERSION 4
 
 /* status codes */
 #define OWL_OK 0
@@ -93,6 +93,12 @@ extern "C" {
 #define OWL_MISFIT_ENVELOPE 2 /* compute_adjsrc_envelope :424-451 */
 #define OWL_MISFIT_PHASE 3    /* compute_adjsrc_phase :459-482 (instantaneous phase) */
 #define OWL_MISFIT_ADAPTIVE 4 /* compute_adjsrc_adaptive :490-537 (adaptive waveform inversion) */
+#define OWL_MISFIT_DTW 5      /* compute_adjsrc_dtw :715-980, solve_gdtw :73-234 (dynamic time warping) */
+
+/* form of the DTW misfit (dtw_form) */
+#define OWL_DTW_PHASE 0     /* misfit sum q tau^2, adjoint q tau d/dt(warped obs) / dt */
+#define OWL_DTW_AMP 1       /* misfit and adjoint of syn - warped obs */
+#define OWL_DTW_PHASE_AMP 2 /* both, the amplitude term weighted by dtw_amp_weight */
 
 /* penalty of the adaptive misfit (xcorr_penalty :321-363) */
 #define OWL_PENALTY_LINEAR 0
@@ -105,15 +111,29 @@ extern "C" {
  * these defaults: tlag_max 0 -> 0.1 * (nt - 1) * dt, deconv_eps 0 -> 0.1,
  * penalty_power 0 -> 1, discard_threshold 0 -> 1e-6 (a negative value turns
  * the relative threshold off; traces of weight 0 or with a zero norm are
- * always dropped). */
+ * always dropped). DTW fields (:270-280, 559-569): dtw_niter 0 -> 5,
+ * dtw_rinst 0 -> 0.1, dtw_rcuml 0 -> 1, dtw_epsabs 0 -> 1e-2, dtw_epsrel
+ * 0 -> 1e-3 (a negative value of these four means 0), dtw_loss_power 0 -> 0.5
+ * (the reference's 'l0.5'), dtw_amp_weight 0 -> 1, dtw_trc traces on each side
+ * of a trace that enter its distance (0), dtw_form OWL_DTW_*. DTW takes the
+ * traces at their own sampling; the shifts are not smoothed across traces. */
 typedef struct {
     int misfit;              /* OWL_MISFIT_* */
     float dt;                /* sample interval of the traces (s) */
-    float tlag_max;          /* adaptive: largest penalised lag (s) */
+    float tlag_max;          /* adaptive: largest penalised lag; DTW: the candidate shifts are 2 tlag_max / dt + 1 (s) */
     int penalty;             /* OWL_PENALTY_* */
     float penalty_power;     /* exponent of the power / gaussian / exp penalties */
     float deconv_eps;        /* adaptive: water level, relative to max |D|^2 */
     float discard_threshold; /* trace_discard_threshold (relative to the gather's largest trace norm) */
+    int dtw_form;            /* OWL_DTW_* */
+    int dtw_niter;           /* refinements of the DTW search band */
+    int dtw_trc;             /* neighbouring traces in the DTW distance */
+    float dtw_rinst;         /* weight of the squared slope of the warping path */
+    float dtw_rcuml;         /* weight of the squared shift */
+    float dtw_epsabs;        /* absolute stop tolerance of the path cost */
+    float dtw_epsrel;        /* relative stop tolerance of the path cost */
+    float dtw_loss_power;    /* p of the distance sum |obs(t + tau) - syn(t)|^p */
+    float dtw_amp_weight;    /* weight of the amplitude term of OWL_DTW_PHASE_AMP */
 } owl_misfit_opts;
 
 typedef struct owl_ssg owl_ssg;
@@ -356,10 +376,20 @@ void owl_ssg_destroy(owl_ssg *h);
  * syn, obs, adj, weight, trace_misfit and gather_misfit are all host memory
  * (OWL_MEM_HOST) or all device memory of the current device (OWL_MEM_DEVICE).
  * Trace length: nt <= 8192 (envelope, phase) or next_power_235(2 nt) <= 8192
- * (adaptive), else OWL_ERR_INVALID. */
+ * (adaptive), 3 <= nt <= 16384 with 3 <= 2 tlag_max / dt + 1 <= 4095 (DTW),
+ * else OWL_ERR_INVALID. */
 int owl_adjoint_source(const owl_misfit_opts *mopts, int ngather, const int *gather_ptr, int nt,
                        const float *syn, const float *obs, const float *weight, float *adj,
                        double *trace_misfit, double *gather_misfit, int mem_kind);
+
+/* Time shifts tau(t) of the DTW misfit, obs(t + tau) ~ syn(t), in seconds, one
+ * row per trace like syn (zero on dropped traces): the reference's
+ * shot_<id>_time_shift_<comp>.su output (compute_adjoint_source :1238-1246).
+ * Same arguments and limits as owl_adjoint_source with mopts->misfit =
+ * OWL_MISFIT_DTW. DTW limits: 3 <= nt <= 16384 and 3 <= 2 tlag_max / dt + 1
+ * <= 4095. */
+int owl_dtw_time_shifts(const owl_misfit_opts *mopts, int ngather, const int *gather_ptr, int nt,
+                        const float *syn, const float *obs, const float *weight, float *tau, int mem_kind);
 
 /* ---- diagnostics (no counterpart in the reference) ------------------------ */
 

@@ -51,6 +51,11 @@ OWL_MISFIT_CORR = 1
 OWL_MISFIT_ENVELOPE = 2
 OWL_MISFIT_PHASE = 3
 OWL_MISFIT_ADAPTIVE = 4
+OWL_MISFIT_DTW = 5
+
+OWL_DTW_PHASE = 0
+OWL_DTW_AMP = 1
+OWL_DTW_PHASE_AMP = 2
 
 OWL_PENALTY_LINEAR = 0
 OWL_PENALTY_POWER = 1
@@ -59,7 +64,9 @@ OWL_PENALTY_EXP = 3
 
 #: misfit_type names of the reference's parameter file
 MISFIT_NAMES = {"waveform": OWL_MISFIT_WAVEFORM, "corr": OWL_MISFIT_CORR, "envelope": OWL_MISFIT_ENVELOPE,
-                "phase": OWL_MISFIT_PHASE, "adaptive": OWL_MISFIT_ADAPTIVE}
+                "phase": OWL_MISFIT_PHASE, "adaptive": OWL_MISFIT_ADAPTIVE, "dtw": OWL_MISFIT_DTW}
+#: dtw_form names of the reference's parameter file
+DTW_FORM_NAMES = {"phase": OWL_DTW_PHASE, "amp": OWL_DTW_AMP, "phase+amp": OWL_DTW_PHASE_AMP}
 PENALTY_NAMES = {"linear": OWL_PENALTY_LINEAR, "power": OWL_PENALTY_POWER, "gaussian": OWL_PENALTY_GAUSSIAN,
                  "exp": OWL_PENALTY_EXP}
 
@@ -149,6 +156,15 @@ class OwlMisfitOpts(C.Structure):
         ("penalty_power", C.c_float),
         ("deconv_eps", C.c_float),
         ("discard_threshold", C.c_float),
+        ("dtw_form", C.c_int),
+        ("dtw_niter", C.c_int),
+        ("dtw_trc", C.c_int),
+        ("dtw_rinst", C.c_float),
+        ("dtw_rcuml", C.c_float),
+        ("dtw_epsabs", C.c_float),
+        ("dtw_epsrel", C.c_float),
+        ("dtw_loss_power", C.c_float),
+        ("dtw_amp_weight", C.c_float),
     ]
 
 
@@ -171,8 +187,8 @@ EXPORTED = [
     "owl_ssg_source_gradient", "owl_ssg_destroy", "owl_last_error", "owl_ssg_abi_version",
     "owl_ssg_dt_stable", "owl_ssg_nparam", "owl_ssg_ncomp", "owl_ssg_device_ok", "owl_ssg_kernel_time",
     "owl_ssg_forward_noalloc", "owl_ssg_desc_nparam", "owl_ssg_misfit", "owl_ssg_gradient_misfit",
-    "owl_adjoint_source", "owl_ssg_set_data_sampling", "owl_resample_traces", "owl_su_encode", "owl_su_decode",
-    "owl_search_direction", "owl_grad_process",
+    "owl_adjoint_source", "owl_dtw_time_shifts", "owl_ssg_set_data_sampling", "owl_resample_traces",
+    "owl_su_encode", "owl_su_decode", "owl_search_direction", "owl_grad_process",
 ]
 
 OWL_SEARCH_SD = 0
@@ -237,6 +253,8 @@ def load() -> C.CDLL:
                                             P(OwlRunInfo)]
     lib.owl_adjoint_source.argtypes = [P(OwlMisfitOpts), C.c_int, P(C.c_int), C.c_int, C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    lib.owl_dtw_time_shifts.argtypes = [P(OwlMisfitOpts), C.c_int, P(C.c_int), C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_int]
     lib.owl_ssg_set_data_sampling.argtypes = [C.c_void_p, C.c_int, C.c_float]
     lib.owl_resample_traces.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p, C.c_int, C.c_float,
                                         C.c_float, C.c_void_p, C.c_int]
@@ -249,8 +267,8 @@ def load() -> C.CDLL:
     for fn in ("owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
                "owl_ssg_source_gradient", "owl_ssg_abi_version", "owl_ssg_nparam", "owl_ssg_ncomp",
                "owl_ssg_device_ok", "owl_ssg_desc_nparam", "owl_ssg_misfit", "owl_ssg_gradient_misfit",
-               "owl_adjoint_source", "owl_ssg_set_data_sampling", "owl_resample_traces", "owl_su_encode",
-               "owl_su_decode", "owl_search_direction", "owl_grad_process"):
+               "owl_adjoint_source", "owl_dtw_time_shifts", "owl_ssg_set_data_sampling", "owl_resample_traces",
+               "owl_su_encode", "owl_su_decode", "owl_search_direction", "owl_grad_process"):
         getattr(lib, fn).restype = C.c_int
     _lib = lib
     return lib

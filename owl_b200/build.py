@@ -7,7 +7,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "lib", "libowl_ssg.so")
-SOURCES = ["shared.cu", "ssg_base.cu", "ac2d.cu", "ac3d.cu", "el2d.cu", "el3d.cu", "adjsrc.cu", "su.cu", "optim.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["shared.cu", "ssg_base.cu", "ac2d.cu", "ac3d.cu", "el2d.cu", "el3d.cu", "adjsrc.cu", "dtw.cu", "su.cu", "optim.cu", "capi.cu", "noalloc.cu"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-cudart", "static"]
 

@@ -430,8 +430,8 @@ void DftTables::build(int n, cudaStream_t s) {
 
 void AdjointSource::run(const owl_misfit_opts& o, int ngather, const int* h_gather_ptr, int nt, const float* syn,
                         const float* obs, const unsigned char* weight_live, float* adj, double* tm, double* gm,
-                        cudaStream_t s) {
-    OWL_CHECK(o.misfit >= OWL_MISFIT_WAVEFORM && o.misfit <= OWL_MISFIT_ADAPTIVE, OWL_ERR_INVALID, "bad misfit type");
+                        cudaStream_t s, float* tau) {
+    OWL_CHECK(o.misfit >= OWL_MISFIT_WAVEFORM && o.misfit <= OWL_MISFIT_DTW, OWL_ERR_INVALID, "bad misfit type");
     OWL_CHECK(nt >= 1 && ngather >= 0 && (ngather == 0 || h_gather_ptr), OWL_ERR_INVALID, "bad trace layout");
     OWL_CHECK(ngather == 0 || h_gather_ptr[0] == 0, OWL_ERR_INVALID, "gather_ptr[0] must be 0");
     for (int g = 0; g < ngather; ++g)
@@ -451,6 +451,21 @@ void AdjointSource::run(const owl_misfit_opts& o, int ngather, const int* h_gath
     OWL_LAUNCH_CHECK();
     launches += 2;
 
+    if (o.misfit == OWL_MISFIT_DTW) {
+        DevBuf<double> tmp;
+        if (!tm && gm) {
+            tmp.reserve(ntr);
+            tm = tmp.p;
+        }
+        run_dtw(o, ngather, nt, ntr, syn, obs, adj, tm, tau, s);
+        if (gm) {
+            k_gather_sum<<<(ngather + 127) / 128, 128, 0, s>>>(tm, gptr.p, ngather, gm);
+            OWL_LAUNCH_CHECK();
+            launches++;
+        }
+        OWL_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
     AdjArgs a{};
     a.kind = o.misfit;
     a.nt = nt;

@@ -22,15 +22,22 @@ struct AdjointSource {
     DevBuf<double> nrm, gmax;
     DevBuf<float> pen, ramp, scratch;
     DevBuf<float2> cscratch;
+    DevBuf<double> dsn, dob, band;  // DTW: normalised traces, per-CTA search bands
+    DevBuf<float> qw, warp;         // DTW: quality weights, warped traces
+    DevBuf<unsigned short> path;    // DTW: per-CTA back-pointers of the dynamic program
     long long launches = 0;
 
     // Misfit and adjoint source of every trace (rows of nt samples) of ngather
     // contiguous gathers, all pointers on the device except h_gather_ptr.
     // weight_live: per-trace 0 / 1 (or nullptr = all live) before the discard
-    // rule. adj, tm (per trace), gm (per gather) may be nullptr.
+    // rule. adj, tm (per trace), gm (per gather) may be nullptr; tau (DTW only,
+    // may be nullptr) receives the time shifts in seconds, rows like syn.
     void run(const owl_misfit_opts& o, int ngather, const int* h_gather_ptr, int nt, const float* syn,
              const float* obs, const unsigned char* weight_live, float* adj, double* tm, double* gm,
-             cudaStream_t s);
+             cudaStream_t s, float* tau = nullptr);
+    // the DTW part of run (dtw.cu), after the norms and the discard rule
+    void run_dtw(const owl_misfit_opts& o, int ngather, int nt, int ntr, const float* syn, const float* obs,
+                 float* adj, double* tm, float* tau, cudaStream_t s);
 };
 
 // smallest m >= n with no prime factor above 5 (FLIT next_power_235)

@@ -184,7 +184,7 @@ int owl_ssg_gradient_misfit(owl_ssg* h, int nshots, const owl_shot* shots, const
         OWL_CHECK(nshots >= 0 && (nshots == 0 || shots), OWL_ERR_INVALID, "bad shots");
         OWL_CHECK(obs || nshots == 0, OWL_ERR_INVALID, "null data buffer");
         OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
-        OWL_CHECK(mopts->misfit >= OWL_MISFIT_WAVEFORM && mopts->misfit <= OWL_MISFIT_ADAPTIVE, OWL_ERR_INVALID,
+        OWL_CHECK(mopts->misfit >= OWL_MISFIT_WAVEFORM && mopts->misfit <= OWL_MISFIT_DTW, OWL_ERR_INVALID,
                   "bad misfit type");
         h->eng->mopts = *mopts;
         if (h->eng->mopts.dt <= 0.f) h->eng->mopts.dt = h->eng->desc.dt;
@@ -349,9 +349,11 @@ int owl_grad_process(int op, int n1, int n2, int n3, const float* param, const f
     });
 }
 
-int owl_adjoint_source(const owl_misfit_opts* mopts, int ngather, const int* gather_ptr, int nt, const float* syn,
-                       const float* obs, const float* weight, float* adj, double* trace_misfit,
-                       double* gather_misfit, int mem_kind) {
+// owl_adjoint_source and owl_dtw_time_shifts: host or device traces in, the
+// requested outputs back in the same memory kind
+static int adjoint_source_impl(const owl_misfit_opts* mopts, int ngather, const int* gather_ptr, int nt,
+                               const float* syn, const float* obs, const float* weight, float* adj,
+                               double* trace_misfit, double* gather_misfit, float* tau, int mem_kind) {
     return guarded([&] {
         check_device();
         OWL_CHECK(mopts, OWL_ERR_INVALID, "null misfit options");
@@ -368,7 +370,7 @@ int owl_adjoint_source(const owl_misfit_opts* mopts, int ngather, const int* gat
         OWL_CUDA(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
         AdjointSource as;
         const size_t n = (size_t)ntr * nt;
-        DevBuf<float> dsyn, dobs, dadj, dw;
+        DevBuf<float> dsyn, dobs, dadj, dw, dtau;
         DevBuf<double> dtm, dgm;
         DevBuf<unsigned char> dlive;
         const bool dev = mem_kind == OWL_MEM_DEVICE;
@@ -377,6 +379,7 @@ int owl_adjoint_source(const owl_misfit_opts* mopts, int ngather, const int* gat
         float* pa = adj;
         double* ptm = trace_misfit;
         double* pgm = gather_misfit;
+        float* ptau = tau;
         if (!dev && ntr) {
             dsyn.upload(syn, n, c.s);
             dobs.upload(obs, n, c.s);
@@ -384,6 +387,7 @@ int owl_adjoint_source(const owl_misfit_opts* mopts, int ngather, const int* gat
             po = dobs.p;
             if (adj) { dadj.reserve(n); pa = dadj.p; }
             if (trace_misfit) { dtm.reserve(ntr); ptm = dtm.p; }
+            if (tau) { dtau.reserve(n); ptau = dtau.p; }
         }
         if (!dev && gather_misfit && ngather) { dgm.reserve(ngather); pgm = dgm.p; }
         const unsigned char* wl = nullptr;
@@ -394,9 +398,10 @@ int owl_adjoint_source(const owl_misfit_opts* mopts, int ngather, const int* gat
             launch_nonzero(pw, ntr, dlive.p, c.s);
             wl = dlive.p;
         }
-        as.run(*mopts, ngather, gather_ptr, nt, ps, po, wl, pa, ptm, pgm, c.s);
+        as.run(*mopts, ngather, gather_ptr, nt, ps, po, wl, pa, ptm, pgm, c.s, ptau);
         if (!dev) {
             if (adj && ntr) OWL_CUDA(cudaMemcpyAsync(adj, pa, n * sizeof(float), cudaMemcpyDeviceToHost, c.s));
+            if (tau && ntr) OWL_CUDA(cudaMemcpyAsync(tau, ptau, n * sizeof(float), cudaMemcpyDeviceToHost, c.s));
             if (trace_misfit && ntr)
                 OWL_CUDA(cudaMemcpyAsync(trace_misfit, ptm, ntr * sizeof(double), cudaMemcpyDeviceToHost, c.s));
             if (gather_misfit && ngather)
@@ -404,6 +409,21 @@ int owl_adjoint_source(const owl_misfit_opts* mopts, int ngather, const int* gat
         }
         OWL_CUDA(cudaStreamSynchronize(c.s));
     });
+}
+
+int owl_adjoint_source(const owl_misfit_opts* mopts, int ngather, const int* gather_ptr, int nt, const float* syn,
+                       const float* obs, const float* weight, float* adj, double* trace_misfit,
+                       double* gather_misfit, int mem_kind) {
+    return adjoint_source_impl(mopts, ngather, gather_ptr, nt, syn, obs, weight, adj, trace_misfit, gather_misfit,
+                               nullptr, mem_kind);
+}
+
+int owl_dtw_time_shifts(const owl_misfit_opts* mopts, int ngather, const int* gather_ptr, int nt, const float* syn,
+                        const float* obs, const float* weight, float* tau, int mem_kind) {
+    if (!mopts || mopts->misfit != OWL_MISFIT_DTW || !tau)
+        return guarded([&] { OWL_CHECK(false, OWL_ERR_INVALID, "owl_dtw_time_shifts needs the DTW misfit and a tau buffer"); });
+    return adjoint_source_impl(mopts, ngather, gather_ptr, nt, syn, obs, weight, nullptr, nullptr, nullptr, tau,
+                               mem_kind);
 }
 
 int owl_ssg_kernel_time(owl_ssg* h, int kernel_id, int nlaunch, double* avg_ms, double* alg_bytes) {

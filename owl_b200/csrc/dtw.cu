@@ -1,0 +1,500 @@
+// dtw.cu -- dynamic-time-warping misfit and adjoint source on the GPU
+// (compute_adjsrc_dtw and solve_gdtw, src/inverse/module_inversion_adjoint_source.f90:73-234, 715-980).
+//
+// Per gather (one shot's one component), for every kept trace:
+//   1. obs and syn are normalised by their own L2 norms (single precision);
+//   2. the generalized DTW of Deriso & Boyd finds the shift tau(t) with
+//      obs(t + tau) ~ syn(t): a dynamic program over n samples x m candidate
+//      shifts per iteration, the candidate band shrinking around the previous
+//      path (dtw_niter iterations at most). One CTA per trace, one thread per
+//      candidate; the double-precision arithmetic of the program uses
+//      explicitly rounded operations (no fused multiply-add) so that every
+//      comparison matches the FP64 restatement in the oracle;
+//   3. a quality weight q(t) from the windowed normalised correlation of syn and
+//      the warped obs (|q|^0.2, 7-sample median, Gaussian of 3 samples,
+//      normalised, rescaled to [0, 1]);
+//   4. misfit sum q tau^2 and adjoint q tau d/dt(warped obs) ('phase'), the
+//      warped residual ('amp'), or both ('phase+amp').
+#include <algorithm>
+#include <cmath>
+
+#include "adjsrc.cuh"
+
+namespace owl {
+
+namespace {
+
+constexpr double DTW_SMIN = 1.0e-8, DTW_SMAX = 1.0e2, DTW_ETA = 0.15, DTW_DELTA = 1.0e-10;
+constexpr double DTW_HUGE = 1.7976931348623157e308;
+
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+
+struct DtwArgs {
+    int n, m, ntr, ngather, niter, trc, form;
+    const int* gptr;
+    const unsigned char* live;
+    const float* syn;
+    const float* obs;
+    const double* nrm;    // per trace: obs norm, syn norm
+    double* dsn;          // normalised syn (ntr x n)
+    double* dob;          // normalised obs
+    float* tau;           // shift in seconds (ntr x n)
+    float* q;             // quality weight
+    float* dw;            // warped normalised obs (ntr x n)
+    unsigned short* path; // per CTA: n x m back-pointers
+    double* band;         // per CTA: l, u, tau (3 n)
+    double rinst, rcuml, epsabs, epsrel, power;
+    float dd, amp_weight, tlag;
+    float* adj;
+    double* tm;
+};
+
+// gather of trace r (gptr ascending)
+__device__ int gather_of(const DtwArgs& a, int r) {
+    int lo = 0, hi = a.ngather - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (a.gptr[mid] <= r) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ double block_sum_d(double v, double* red) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    __syncthreads();
+    return t;
+}
+
+__device__ double block_minmax_d(double v, double* red, bool is_max) {
+    for (int o = 16; o; o >>= 1) {
+        const double w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = is_max ? fmax(v, w) : fmin(v, w);
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = red[0];
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) t = is_max ? fmax(t, red[i]) : fmin(t, red[i]);
+    __syncthreads();
+    return t;
+}
+
+// normalised traces (:761-775): obs / norm2(obs), syn / norm2(syn) in single
+// precision, stored as doubles; discarded traces stay zero
+__global__ void k_dtw_normalise(DtwArgs a) {
+    const size_t tot = (size_t)a.ntr * a.n;
+    for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < tot; o += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(o / a.n);
+        const bool lv = a.live[r] != 0;
+        const float no = (float)a.nrm[2 * r], ns = (float)a.nrm[2 * r + 1];
+        a.dob[o] = lv ? (double)(a.obs[o] / no) : 0.0;
+        a.dsn[o] = lv ? (double)(a.syn[o] / ns) : 0.0;
+    }
+}
+
+__device__ __forceinline__ double grid_t(int i, int n) { return (double)i / (double)(n - 1); }
+
+// linear interpolation of column x (uniform grid i / (n-1)) at q, clamped to the ends
+__device__ double interp_clamped(const double* x, int n, double q) {
+    if (q <= 0.0) return x[0];
+    if (q >= grid_t(n - 1, n)) return x[n - 1];
+    int i0 = min((int)floor(dmul(q, (double)(n - 1))), n - 2);
+    i0 = max(i0, 0);
+    while (i0 > 0 && grid_t(i0, n) > q) --i0;
+    while (i0 < n - 2 && grid_t(i0 + 1, n) <= q) ++i0;
+    const double t0 = grid_t(i0, n), t1 = grid_t(i0 + 1, n);
+    const double w = dsub(q, t0) / dsub(t1, t0);
+    return dadd(dmul(x[i0], dsub(1.0, w)), dmul(x[i0 + 1], w));
+}
+
+__device__ __forceinline__ double powabs(double d, double p) {
+    const double v = fabs(d);
+    if (p == 0.5) return __dsqrt_rn(v);
+    if (p == 1.0) return v;
+    if (p == 2.0) return dmul(v, v);
+    return pow(v, p);
+}
+
+// solve_gdtw (:73-234), one CTA per kept trace (grid-strided over traces)
+__global__ void __launch_bounds__(256) k_dtw_solve(DtwArgs a) {
+    extern __shared__ double sh[];
+    const int n = a.n, m = a.m, jc = (m - 1) / 2;
+    double* lin = sh;
+    double* fa = sh + m;
+    double* fb = sh + 2 * m;
+    __shared__ double s_cost;
+    unsigned short* path = a.path + (size_t)blockIdx.x * n * m;
+    double* L = a.band + (size_t)blockIdx.x * 3 * n;
+    double* U = L + n;
+    double* T = U + n;
+    const double dt = 1.0 / ((double)n - 1.0);
+    for (int j = threadIdx.x; j < m; j += blockDim.x) lin[j] = (double)j / (double)(m - 1);
+    for (int r = blockIdx.x; r < a.ntr; r += gridDim.x) {
+        float* tau_out = a.tau + (size_t)r * n;
+        if (!a.live[r]) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) tau_out[i] = 0.f;
+            continue;
+        }
+        const int g = gather_of(a, r);
+        const int c0 = r - a.trc, nc = 2 * a.trc + 1, g0 = a.gptr[g], g1 = a.gptr[g + 1];
+        double cost_prev = 1.1754943508222875e-38;  // single-precision tiny
+        __syncthreads();
+        for (int it = 0; it < a.niter; ++it) {
+            // search band (:112-130)
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const double t = grid_t(i, n);
+                const double u0 = fmin(fmin(0.0 + dmul(DTW_SMAX, t), dsub(1.0, dmul(DTW_SMIN, dsub(1.0, t)))), 1.0);
+                const double l0 = fmax(fmax(dmul(DTW_SMIN, t), dsub(1.0, dmul(DTW_SMAX, dsub(1.0, t)))), 0.0);
+                if (it == 0) {
+                    U[i] = u0;
+                    L[i] = l0;
+                } else {
+                    const double rng = dmul(DTW_ETA, dsub(U[i], L[i])) / 2.0;
+                    U[i] = fmin(dadd(T[i], rng), u0);
+                    L[i] = fmax(dsub(T[i], rng), l0);
+                }
+            }
+            __syncthreads();
+            // row 0: only the centre candidate (bc_start_stop)
+            for (int k = threadIdx.x; k < m; k += blockDim.x) {
+                double v = DTW_HUGE;
+                if (k == jc) {
+                    const double tg = dadd(L[0], dmul(dsub(U[0], L[0]), lin[k]));
+                    double dist = 0.0;
+                    for (int c = 0; c < nc; ++c) {
+                        const int rc = c0 + c;
+                        const bool in = rc >= g0 && rc < g1;
+                        const double xv = in ? interp_clamped(a.dob + (size_t)rc * n, n, tg) : 0.0;
+                        const double yv = in ? a.dsn[(size_t)rc * n] : 0.0;
+                        dist = dadd(dist, powabs(dsub(xv, yv), a.power));
+                    }
+                    const double d = dsub(tg, 0.0);
+                    v = dadd(dist, dmul(a.rcuml, dmul(d, d)));
+                }
+                fa[k] = v;
+            }
+            __syncthreads();
+            double* fcur = fa;
+            double* fnext = fb;
+            for (int i = 0; i < n - 1; ++i) {
+                const double li = L[i], dui = dsub(U[i], L[i]);
+                const double ln = L[i + 1], dun = dsub(U[i + 1], L[i + 1]);
+                const double tn = grid_t(i + 1, n);
+                for (int k = threadIdx.x; k < m; k += blockDim.x) {
+                    const double tgk = dadd(ln, dmul(dun, lin[k]));
+                    double dist = 0.0;
+                    for (int c = 0; c < nc; ++c) {
+                        const int rc = c0 + c;
+                        const bool in = rc >= g0 && rc < g1;
+                        const double xv = in ? interp_clamped(a.dob + (size_t)rc * n, n, tgk) : 0.0;
+                        const double yv = in ? a.dsn[(size_t)rc * n + i + 1] : 0.0;
+                        dist = dadd(dist, powabs(dsub(xv, yv), a.power));
+                    }
+                    const double d = dsub(tgk, tn);
+                    const double nu = dadd(dist, dmul(a.rcuml, dmul(d, d)));
+                    // candidates j with s_min - delta <= slope <= s_max + delta form one run
+                    // (the slope falls as j grows); walk it in ascending j as the reference does
+                    auto slope_of = [&](int j) { return dsub(tgk, dadd(li, dmul(dui, lin[j]))) / dt; };
+                    int j = 0;
+                    if (dui > 0.0) {
+                        const double est = (tgk - (DTW_SMAX + DTW_DELTA) * dt - li) / dui * (double)(m - 1);
+                        j = est <= 0.0 ? 0 : (est >= (double)(m - 1) ? m - 1 : (int)est);
+                        j = max(0, j - 2);
+                        while (j > 0 && !(slope_of(j - 1) > DTW_SMAX + DTW_DELTA)) --j;
+                    }
+                    while (j < m && slope_of(j) > DTW_SMAX + DTW_DELTA) ++j;
+                    double best = DTW_HUGE;
+                    int bj = 0;
+                    for (; j < m; ++j) {
+                        const double s = slope_of(j);
+                        if (s < DTW_SMIN - DTW_DELTA) break;
+                        const double fj = fcur[j];
+                        if (!(fj < DTW_HUGE)) continue;
+                        const double pc = dadd(fj, dmul(dt, dadd(dmul(a.rinst, dmul(s, s)), nu)));
+                        if (pc < best) {
+                            best = pc;
+                            bj = j;
+                        }
+                    }
+                    fnext[k] = best;
+                    path[(size_t)(i + 1) * m + k] = (unsigned short)bj;
+                }
+                __syncthreads();
+                double* tmp = fcur;
+                fcur = fnext;
+                fnext = tmp;
+            }
+            // traceback (:196-209)
+            if (threadIdx.x == 0) {
+                const double cost = fcur[jc];
+                int j = jc;
+                for (int i = n - 1; i >= 0; --i) {
+                    T[i] = dadd(L[i], dmul(dsub(U[i], L[i]), lin[j]));
+                    if (i > 0) j = path[(size_t)i * m + j];
+                }
+                s_cost = cost;
+            }
+            __syncthreads();
+            const double cost = s_cost;
+            if (fabs(cost - cost_prev) <= a.epsabs + a.epsrel * cost_prev) break;
+            cost_prev = cost;
+            __syncthreads();
+        }
+        // tau = (tau - linspace(0, 1, n)) (n - 1), in seconds (:232, :810)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const double lin32 = (double)((float)i / (float)(n - 1));
+            tau_out[i] = (float)dmul(dmul(dsub(T[i], lin32), (double)(n - 1)), (double)a.dd);
+        }
+        __syncthreads();
+    }
+}
+
+// single-precision linear interpolation on the grid i dd, zero outside
+__device__ float interp_zero_f(const double* x, int n, float dd, float q) {
+    const float tl = (float)(n - 1) * dd;
+    if (q < 0.f || q > tl) return 0.f;
+    int i0 = min(max((int)floorf(q / dd), 0), n - 2);
+    while (i0 > 0 && (float)i0 * dd > q) --i0;
+    while (i0 < n - 2 && (float)(i0 + 1) * dd <= q) ++i0;
+    const float t0 = (float)i0 * dd, t1 = (float)(i0 + 1) * dd;
+    const float w = (q - t0) / (t1 - t0);
+    return (float)x[i0] * (1.f - w) + (float)x[i0 + 1] * w;
+}
+
+// quality weights (:838-905), one CTA per trace
+__global__ void __launch_bounds__(256) k_dtw_quality(DtwArgs a) {
+    __shared__ double red[32];
+    const int r = blockIdx.x, n = a.n;
+    float* q = a.q + (size_t)r * n;
+    if (!a.live[r] || a.form == 1) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) q[i] = 1.f;
+        return;
+    }
+    const double* ds = a.dsn + (size_t)r * n;
+    const double* dob = a.dob + (size_t)r * n;
+    const float* tau = a.tau + (size_t)r * n;
+    float* dw = a.dw + (size_t)r * n;
+    double s1 = 0.0, s2 = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float tg = (float)i * a.dd;
+        const float v = interp_zero_f(dob, n, a.dd, tau[i] + tg);
+        dw[i] = v;
+        s1 += ds[i] * ds[i];
+        s2 += (double)v * (double)v;
+    }
+    s1 = block_sum_d(s1, red);
+    s2 = block_sum_d(s2, red);
+    float eta = (float)(fmax(sqrt(s1), sqrt(s2)) * (double)1.0e-2f);
+    if (eta == 0.f) eta = 1.0e-9f;
+    const int nw = (int)floor(fabs((double)(a.tlag / a.dd)) + 0.5);  // nint(tlag_max / dd)
+    __syncthreads();
+    // windowed normalised correlation, then |q|^0.2
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const int lo = max(0, j - nw), hi = min(n - 1, j + nw);
+        double uv = 0.0, uu = 0.0, vv = 0.0;
+        for (int i = lo; i <= hi; ++i) {
+            const double u = (double)(float)ds[i], v = (double)dw[i];
+            uv += u * v;
+            uu += u * u;
+            vv += v * v;
+        }
+        const float c = (float)(uv / (sqrt(uu) * sqrt(vv) + (double)eta));
+        q[j] = powf(fabsf(c), 0.2f);
+    }
+    __syncthreads();
+    // 7-sample median (truncated at the ends) into dw
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        float w[7];
+        const int lo = max(0, j - 3), hi = min(n - 1, j + 3), c = hi - lo + 1;
+        for (int i = 0; i < c; ++i) w[i] = q[lo + i];
+        for (int i = 1; i < c; ++i) {
+            const float v = w[i];
+            int k = i - 1;
+            while (k >= 0 && w[k] > v) { w[k + 1] = w[k]; --k; }
+            w[k + 1] = v;
+        }
+        dw[j] = (c & 1) ? w[c / 2] : 0.5f * (w[c / 2 - 1] + w[c / 2]);
+    }
+    __syncthreads();
+    // Gaussian of 3 samples truncated at 9, end samples replicated (double),
+    // normalised by its L2 norm, rescaled to [0, 1]; NaN / Inf -> 0
+    double wsum = 0.0;
+    for (int k = -9; k <= 9; ++k) wsum += exp(-0.5 * (double)(k * k) / 9.0);
+    auto gauss = [&](int j) {
+        double acc = 0.0;
+        for (int k = -9; k <= 9; ++k) acc += exp(-0.5 * (double)(k * k) / 9.0) / wsum * (double)dw[min(max(j + k, 0), n - 1)];
+        return acc;
+    };
+    double sq = 0.0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const double g = gauss(j);
+        sq += g * g;
+    }
+    const double nrm = sqrt(block_sum_d(sq, red));
+    double lo = DTW_HUGE, hi = -DTW_HUGE;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const double v = gauss(j) / nrm;
+        lo = fmin(lo, v);
+        hi = fmax(hi, v);
+    }
+    lo = block_minmax_d(lo, red, false);
+    hi = block_minmax_d(hi, red, true);
+    double qmax = 0.0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double v = (gauss(j) / nrm - lo) / (hi - lo);
+        if (!isfinite(v)) v = 0.0;
+        const float f = (float)v;
+        q[j] = f;
+        qmax = fmax(qmax, (double)fabsf(f));
+    }
+    __syncthreads();
+    qmax = block_minmax_d(qmax, red, true);
+    if (qmax == 0.0)
+        for (int j = threadIdx.x; j < n; j += blockDim.x) q[j] = 1.f;
+}
+
+__device__ __forceinline__ double keys_at(const float* x, int n, double p) {
+    if (fabs(p - rint(p)) <= 1e-4) p = rint(p);
+    if (p < 0.0 || p > (double)(n - 1)) return 0.0;
+    const int j0 = (int)floor(p);
+    const double u = p - j0, u2 = u * u, u3 = u2 * u;
+    const double w0 = 0.5 * (-u3 + 2 * u2 - u), w1 = 0.5 * (3 * u3 - 5 * u2 + 2);
+    const double w2 = 0.5 * (-3 * u3 + 4 * u2 + u), w3 = 0.5 * (u3 - u2);
+    return w0 * x[max(j0 - 1, 0)] + w1 * x[j0] + w2 * x[min(j0 + 1, n - 1)] + w3 * x[min(j0 + 2, n - 1)];
+}
+
+// adjoint source and misfit (:917-978), one CTA per trace; warped obs staged in dw
+__global__ void __launch_bounds__(256) k_dtw_adjoint(DtwArgs a) {
+    __shared__ double red[32];
+    const int r = blockIdx.x, n = a.n;
+    float* adj = a.adj ? a.adj + (size_t)r * n : nullptr;
+    if (!a.live[r]) {
+        if (adj)
+            for (int i = threadIdx.x; i < n; i += blockDim.x) adj[i] = 0.f;
+        if (threadIdx.x == 0 && a.tm) a.tm[r] = 0.0;
+        return;
+    }
+    const float* obs = a.obs + (size_t)r * n;
+    const float* syn = a.syn + (size_t)r * n;
+    const float* tau = a.tau + (size_t)r * n;
+    const float* q = a.q + (size_t)r * n;
+    float* dw = a.dw + (size_t)r * n;
+    double mph = 0.0, ma = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float pos = (tau[i] + (float)i * a.dd) / a.dd;
+        const double w = keys_at(obs, n, (double)pos);
+        dw[i] = (float)w;
+        const double ti = tau[i];
+        mph += (double)q[i] * ti * ti;
+        const double rr = (double)syn[i] - w;
+        ma += rr * rr;
+    }
+    mph = block_sum_d(mph, red);
+    ma = block_sum_d(ma, red);
+    if (threadIdx.x == 0 && a.tm)
+        a.tm[r] = a.form == 0 ? mph : a.form == 1 ? ma : mph * (1.0 + (double)a.amp_weight);
+    if (!adj) return;
+    const double dd = a.dd;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        // the warped trace is recomputed in double for the derivative's neighbours
+        auto wv = [&](int k) {
+            const float pos = (tau[k] + (float)k * a.dd) / a.dd;
+            return keys_at(obs, n, (double)pos);
+        };
+        double der;
+        if (i == 0) der = wv(1) - wv(0);
+        else if (i == n - 1) der = wv(n - 1) - wv(n - 2);
+        else der = (wv(i + 1) - wv(i - 1)) * 0.5;
+        const double ph = (double)q[i] * (double)tau[i] * der / dd;
+        const double res = (double)syn[i] - wv(i);
+        double v;
+        if (a.form == 0) v = ph;
+        else if (a.form == 1) v = res;
+        else v = ph + (double)a.amp_weight * mph / (ma + 1.1754943508222875e-38) * res;
+        adj[i] = (float)v;
+    }
+}
+
+}  // namespace
+
+void AdjointSource::run_dtw(const owl_misfit_opts& o, int ngather, int nt, int ntr, const float* syn, const float* obs,
+                            float* adj, double* tm, float* tau_out, cudaStream_t s) {
+    OWL_CHECK(o.dt > 0.f, OWL_ERR_INVALID, "the DTW misfit needs the sample interval dt");
+    OWL_CHECK(nt >= 3 && nt <= 16384, OWL_ERR_INVALID, "DTW traces must have 3 .. 16384 samples");
+    const float tlag = o.tlag_max > 0.f ? o.tlag_max : 0.1f * (float)(nt - 1) * o.dt;
+    // m = nint(2 tlag_max / dd) + 1, odd (:795, solve_gdtw :92-96)
+    const float x = (2.0f * tlag) / o.dt;
+    int m = (int)std::floor(std::fabs((double)x) + 0.5) + 1;
+    if (m % 2 == 0) ++m;
+    OWL_CHECK(m >= 3 && m <= 4095, OWL_ERR_INVALID, "DTW: 2 tlag_max / dt + 1 must lie in 3 .. 4095 candidates");
+    OWL_CHECK(o.dtw_form >= 0 && o.dtw_form <= 2, OWL_ERR_INVALID, "bad dtw_form");
+    OWL_CHECK(o.dtw_trc >= 0 && o.dtw_niter >= 0, OWL_ERR_INVALID, "bad DTW options");
+    DtwArgs a{};
+    a.n = nt;
+    a.m = m;
+    a.ntr = ntr;
+    a.ngather = ngather;
+    a.niter = o.dtw_niter > 0 ? o.dtw_niter : 5;
+    a.trc = o.dtw_trc;
+    a.form = o.dtw_form;
+    a.gptr = gptr.p;
+    a.live = live.p;
+    a.syn = syn;
+    a.obs = obs;
+    a.nrm = nrm.p;
+    auto dflt = [](float v, float d) { return v == 0.f ? (double)d : (v < 0.f ? 0.0 : (double)v); };
+    a.rinst = dflt(o.dtw_rinst, 0.1f);
+    a.rcuml = dflt(o.dtw_rcuml, 1.0f);
+    a.epsabs = dflt(o.dtw_epsabs, 1.0e-2f);
+    a.epsrel = dflt(o.dtw_epsrel, 1.0e-3f);
+    a.power = o.dtw_loss_power > 0.f ? (double)o.dtw_loss_power : 0.5;
+    a.amp_weight = o.dtw_amp_weight != 0.f ? std::max(0.f, o.dtw_amp_weight) : 1.0f;
+    a.dd = o.dt;
+    a.tlag = tlag;
+    const size_t nn = (size_t)ntr * nt;
+    dsn.reserve(nn);
+    dob.reserve(nn);
+    qw.reserve(nn);
+    warp.reserve(nn);
+    DevBuf<float> tmp_tau;
+    if (!tau_out) {
+        tmp_tau.reserve(nn);
+        tau_out = tmp_tau.p;
+    }
+    a.dsn = dsn.p;
+    a.dob = dob.p;
+    a.q = qw.p;
+    a.dw = warp.p;
+    a.tau = tau_out;
+    a.adj = adj;
+    a.tm = tm;
+    int dev_id = 0, nsm = 0;
+    OWL_CUDA(cudaGetDevice(&dev_id));
+    OWL_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev_id));
+    // back-pointer tables of the traces solved at once: at most 2 GiB
+    const size_t per = (size_t)nt * m * sizeof(unsigned short);
+    const size_t cap = std::max<size_t>(1, ((size_t)2 << 30) / per);
+    const int grid = (int)std::max<size_t>(1, std::min<size_t>({(size_t)ntr, (size_t)nsm * 4, cap}));
+    path.reserve((size_t)grid * nt * m);
+    band.reserve((size_t)grid * 3 * nt);
+    a.path = path.p;
+    a.band = band.p;
+    k_dtw_normalise<<<(int)std::min<size_t>((nn + 255) / 256, (size_t)nsm * 32), 256, 0, s>>>(a);
+    const size_t smem = (size_t)3 * m * sizeof(double);
+    OWL_CUDA(cudaFuncSetAttribute(k_dtw_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_dtw_solve<<<grid, 256, smem, s>>>(a);
+    k_dtw_quality<<<ntr, 256, 0, s>>>(a);
+    k_dtw_adjoint<<<ntr, 256, 0, s>>>(a);
+    OWL_LAUNCH_CHECK();
+    launches += 4;
+    OWL_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace owl

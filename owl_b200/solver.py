@@ -72,12 +72,22 @@ class MisfitOpts:
     penalty_power: float = 0.0
     deconv_eps: float = 0.0
     discard_threshold: float = 0.0
+    dtw_form: int = L.OWL_DTW_PHASE
+    dtw_niter: int = 0
+    dtw_trc: int = 0
+    dtw_rinst: float = 0.0
+    dtw_rcuml: float = 0.0
+    dtw_epsabs: float = 0.0
+    dtw_epsrel: float = 0.0
+    dtw_loss_power: float = 0.0
+    dtw_amp_weight: float = 0.0
 
     def c(self) -> L.OwlMisfitOpts:
         o = L.OwlMisfitOpts()
-        for k in ("misfit", "penalty"):
+        for k in ("misfit", "penalty", "dtw_form", "dtw_niter", "dtw_trc"):
             setattr(o, k, int(getattr(self, k)))
-        for k in ("dt", "tlag_max", "penalty_power", "deconv_eps", "discard_threshold"):
+        for k in ("dt", "tlag_max", "penalty_power", "deconv_eps", "discard_threshold", "dtw_rinst", "dtw_rcuml",
+                  "dtw_epsabs", "dtw_epsrel", "dtw_loss_power", "dtw_amp_weight"):
             setattr(o, k, float(getattr(self, k)))
         return o
 
@@ -126,6 +136,29 @@ def adjoint_source(mopts: MisfitOpts, gather_ptr, syn, obs, weight=None, adj=Non
                                    _ptr(weight) if weight is not None else None, _ptr(adj), _ptr(trace_misfit),
                                    _ptr(gather_misfit), _mem_kind(syn)))
     return adj, trace_misfit, gather_misfit
+
+
+def dtw_time_shifts(mopts: MisfitOpts, gather_ptr, syn, obs, weight=None, tau=None):
+    """Time shifts tau(t) of the DTW misfit (owl_dtw_time_shifts), obs(t + tau) ~
+    syn(t), in seconds, rows like syn; numpy in -> numpy out, CUDA tensors in ->
+    CUDA tensor out."""
+    lib = L.load()
+    gp = np.ascontiguousarray(np.asarray(gather_ptr, dtype=np.int32))
+    ng = gp.size - 1
+    if hasattr(syn, "is_cuda") and syn.is_cuda:
+        import torch
+        tau = torch.empty_like(syn) if tau is None else tau
+        _ready(syn, obs, weight, tau)
+    else:
+        syn = np.ascontiguousarray(syn, dtype=f32)
+        obs = np.ascontiguousarray(obs, dtype=f32)
+        weight = None if weight is None else np.ascontiguousarray(weight, dtype=f32)
+        tau = np.empty_like(syn) if tau is None else tau
+    o = mopts.c()
+    L.check(lib.owl_dtw_time_shifts(C.byref(o), ng, gp.ctypes.data_as(C.POINTER(C.c_int)), int(syn.shape[1]),
+                                    _ptr(syn), _ptr(obs), _ptr(weight) if weight is not None else None, _ptr(tau),
+                                    _mem_kind(syn)))
+    return tau
 
 
 def elastic_time_integration(mechanism: str) -> int:

@@ -1,0 +1,95 @@
+"""GPU dynamic-time-warping misfit (OWL_MISFIT_DTW) against the oracle's
+restatement (oracle/oracle_dtw.py).
+
+* time shifts (owl_dtw_time_shifts): the GPU's dynamic program uses the
+  oracle's double-precision operations rounded the same way, so the shifts
+  agree to single-precision rounding (1e-6 s) on every trace;
+* adjoint sources and trace misfits of the 'phase', 'amp' and 'phase+amp'
+  forms, with and without neighbouring traces in the distance, host and
+  device buffers, gathers with a weight-0 trace, a trace below the discard
+  threshold and a zero trace: 1e-4 relative L2;
+* the gradient of the DTW misfit through owl_ssg_gradient_misfit equals the
+  FP64 exact-adjoint oracle gradient driven by the oracle's DTW adjoint source
+  of the same synthetics (2e-4);
+* the documented size limits are errors.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import oracle_dtw as D
+from owl_b200 import _lib as L
+from owl_b200.solver import MisfitOpts, RunOpts, adjoint_source, dtw_time_shifts
+
+from cases import desc, prepare, random_model, rel, small_shots
+from test_gpu_ac2d import make_solver
+from test_gpu_misfits import _gathers
+
+pytestmark = pytest.mark.gpu
+
+DT, TLAG = 1e-3, 0.02
+
+
+def _mo(form=L.OWL_DTW_PHASE, trc=0, **kw):
+    return MisfitOpts(misfit=L.OWL_MISFIT_DTW, dt=DT, tlag_max=TLAG, dtw_form=form, dtw_trc=trc, **kw)
+
+
+@pytest.mark.parametrize("form,trc", [(L.OWL_DTW_PHASE, 0), (L.OWL_DTW_AMP, 0), (L.OWL_DTW_PHASE_AMP, 0),
+                                      (L.OWL_DTW_PHASE, 1)])
+def test_dtw_matches_oracle(form, trc):
+    import torch
+    gp, syn, obs, w = _gathers(300)
+    kw = dict(form=form, trc=trc, amp_weight=0.5 if form == L.OWL_DTW_PHASE_AMP else 1.0)
+    ref_adj, ref_tm, ref_gm, ref_tau = D.adjoint_source(gp, syn, obs, w, dt=DT, tlag_max=TLAG, **kw)
+    mo = _mo(form, trc, dtw_amp_weight=kw["amp_weight"])
+    tau = dtw_time_shifts(mo, gp, syn, obs, w)
+    assert np.max(np.abs(tau - ref_tau)) <= 1e-6, np.max(np.abs(tau - ref_tau))
+    assert np.all(tau[[1, 6, 8]] == 0)
+    adj, tm, gm = adjoint_source(mo, gp, syn, obs, w)
+    assert np.all(tm[[1, 6, 8]] == 0) and np.all(adj[[1, 6, 8]] == 0)
+    assert rel(adj, ref_adj) < 1e-4, rel(adj, ref_adj)
+    assert rel(tm, ref_tm) < 1e-4, (tm, ref_tm)
+    assert np.allclose(gm, [tm[:5].sum(), tm[5:].sum()], rtol=1e-12)
+    # device buffers give the same bytes
+    dadj, dtm, _ = adjoint_source(mo, gp, torch.from_numpy(syn).cuda(), torch.from_numpy(obs).cuda(),
+                                  torch.from_numpy(w).cuda())
+    assert np.array_equal(dadj.cpu().numpy(), adj)
+    assert np.array_equal(dtm.cpu().numpy(), tm)
+    dtau = dtw_time_shifts(mo, gp, torch.from_numpy(syn).cuda(), torch.from_numpy(obs).cuda(),
+                           torch.from_numpy(w).cuda())
+    assert np.array_equal(dtau.cpu().numpy(), tau)
+
+
+def test_dtw_gradient_matches_oracle():
+    nx, nz, dx, dt, nt = 48, 40, 10.0, 1e-3, 240
+    d = desc(nx, nz, dx, dt, nt)
+    vp, rho = random_model(nx, nz)
+    ps = prepare(small_shots(nx, nz, dx), nx, nz, dx, dt)
+    obs = oracle.ac2d_forward(d, vp, rho, ps, "f64").astype(np.float32)
+    vp0 = (vp * np.float32(1.03)).astype(np.float32)
+    s = make_solver(d, vp0, rho)
+    mo = MisfitOpts(misfit=L.OWL_MISFIT_DTW, dt=dt, tlag_max=0.02)
+    seis = np.zeros(s.seis_size(ps), dtype=np.float32)
+    mf, g = s.gradient_misfit(ps, obs, mo, RunOpts(checkpoint_interval=30), seis_out=seis)
+    # the oracle's DTW adjoint source of the GPU's own synthetics, then its exact-adjoint gradient
+    gp = s.gather_ptr(ps)
+    live = np.concatenate([[r.weight != 0 for r in sh.receivers] for sh in ps.shots]).astype(np.float64)
+    adj, tm, gm, _ = D.adjoint_source(gp, seis.reshape(-1, nt), obs.reshape(-1, nt), live, dt=dt, tlag_max=0.02)
+    _, g_ref, _ = oracle.ac2d_gradient(d, vp0, rho, ps, adj.ravel().astype(np.float32), adj_kind=1, k=30,
+                                       precision="f64")
+    assert rel(g, g_ref) < 2e-4, rel(g, g_ref)
+    assert rel(mf, gm) < 1e-4
+    assert np.all(mf > 0)
+
+
+def test_dtw_limits():
+    gp, syn, obs, w = _gathers(300)
+    with pytest.raises(L.OwlError):  # 2 tlag_max / dt + 1 > 4095 candidates
+        adjoint_source(MisfitOpts(misfit=L.OWL_MISFIT_DTW, dt=1e-5, tlag_max=0.03), gp, syn, obs, w)
+    with pytest.raises(L.OwlError):  # no sample interval
+        adjoint_source(MisfitOpts(misfit=L.OWL_MISFIT_DTW, tlag_max=0.02), gp, syn, obs, w)
+    long = np.zeros((9, 16385), dtype=np.float32)
+    with pytest.raises(L.OwlError):
+        adjoint_source(_mo(), gp, long, long, w)
+    with pytest.raises(L.OwlError):  # time shifts of another misfit
+        dtw_time_shifts(MisfitOpts(misfit=L.OWL_MISFIT_WAVEFORM, dt=DT), gp, syn, obs, w)
