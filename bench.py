@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--rows", type=int, default=1, help="rows per thread of the --profile3d forward kernels")
     p.add_argument("--profile3d", type=int, default=0, metavar="N",
                    help="profiling target: 12-step 3D acoustic forward of an N^3 model, no JSON line")
+    p.add_argument("--profile3d-grad", type=int, default=0, metavar="N",
+                   help="profiling target: one 3D acoustic gradient of an N^3 model, 1 shot, 60 steps, no JSON line")
     p.add_argument("--no-elastic", action="store_true", help="skip the 2D elastic VTI block")
     p.add_argument("--profile-el", type=int, default=0, metavar="S",
                    help="profiling target: one 2D elastic VTI gradient of S shots, 60 steps, no JSON line")
@@ -69,6 +71,25 @@ def profile_3d(n, rows=1):
     s.set_model(vp, rho)
     s.forward(s.prepare(shots), RunOpts(shots_per_cta=1, tile_z=rows, use_graph=-1))
     print(f"profile3d: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
+    s.close()
+
+
+def profile_3d_grad(n):
+    """Small 3D acoustic gradient for kernel captures: N^3 layered model, one
+    shot, 60 steps, checkpoints every 20 steps."""
+    import numpy as np
+    from owl_b200 import _lib as L
+    from owl_b200 import configs
+    from owl_b200.solver import RunOpts, SSGSolver
+
+    d, vp, rho, shots = configs.config3(n, nt=60)
+    s = SSGSolver(L.OWL_ACOUSTIC_ISO_3D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
+                  f0_max=d.f0_max, ny=d.ny, dy=d.dy)
+    s.set_model(vp, rho)
+    ps = s.prepare(shots)
+    obs = np.zeros(s.seis_size(ps), dtype=np.float32)
+    s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=20, shots_per_cta=1, use_graph=-1))
+    print(f"profile3d-grad: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
     s.close()
 
 
@@ -102,6 +123,28 @@ def forward_3d_block(peak, peak_kind):
                                 "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
                                 "traffic": profile_traffic(name)}
     s.close()
+    # gradient of the same model and shot over 500 of the 1500 steps (FP16 checkpoints
+    # every 50 steps), observed data from a 3 % faster model
+    import numpy as np
+    dg, vpg, rhog, shg = configs.config3(400, nt=500)
+    g = SSGSolver(L.OWL_ACOUSTIC_ISO_3D, dg.nx, dg.nz, dg.dx, dg.dz, dg.dt, dg.nt, pml=dg.pml, fdhalf=dg.fdhalf,
+                  f0_max=dg.f0_max, ny=dg.ny, dy=dg.dy)
+    pg = g.prepare(shg)
+    g.set_model((vpg * np.float32(1.03)).astype(np.float32), rhog)
+    obs = g.forward(pg, RunOpts())
+    g.set_model(vpg, rhog)
+    go = RunOpts(checkpoint_precision=L.OWL_CKPT_FP16)
+    g.gradient(pg, obs, opts=go)
+    g.gradient(pg, obs, opts=go)
+    out["gradient_workload"] = "the same model and shot, 500 of the 1500 steps, FP16 checkpoints every 50 steps"
+    out["gradient_s_per_shot"] = g.last_info.elapsed_ms / 1e3
+    for kid, name in ((L.OWL_K_ADJ_P, "k_ac3d_adj_p"), (L.OWL_K_ADJ_V, "k_ac3d_adj_v")):
+        kms, b = g.kernel_time(kid, 10)
+        ach = b / (kms / 1e3) / 1e9
+        out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
+                                "traffic": profile_traffic(name)}
+    g.close()
     return out
 
 
@@ -423,6 +466,8 @@ def main():
         return profile_elastic(args.profile_el)
     if args.profile_el3:
         return profile_elastic3(args.profile_el3, args.ring)
+    if args.profile3d_grad:
+        return profile_3d_grad(args.profile3d_grad)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 

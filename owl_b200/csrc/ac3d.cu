@@ -376,6 +376,8 @@ __global__ void __launch_bounds__(32 * TY) k_ac3d_adj_v(Ac3dDev a) {
     }
 }
 
+#include "ac3d_adj_ring.cuh"
+
 // ------------------------- FP64 chain rule ---------------------------------
 __global__ void k_ac3d_chain(Ac3dDev a, int ngroups, const float* __restrict__ vpp, const float* __restrict__ rhop,
                              double dt, double* __restrict__ gvp, double* __restrict__ grho, int nxq, int nyq, int nzq) {
@@ -446,8 +448,9 @@ struct Ac3dEngine : SsgBase {
         // state: p, vx, vy, vz, then slabs m0 (x), m1 (y), m2 (z), m3 (x), m4 (y), m5 (z)
         // shot strides rounded to 64 floats: every field of every shot starts 16-byte aligned
         sst = (4 * fs + 2 * (sx_n + sy_n + sz_n) + 63) / 64 * 64;
-        // adjoint: p^, vx^, vy^, vz^, 6 memory slabs, e_x, e_y, e_z, e_px, e_py, e_pz
-        sad = (10 * fs + 2 * (sx_n + sy_n + sz_n) + 63) / 64 * 64;
+        // adjoint: p^, vx^, vy^, vz^, 6 memory slabs, e_x, e_y, e_z, e_px, e_py, e_pz; the
+        // slabs rounded to 64 floats so that the e arrays start 16-byte aligned too
+        sad = (10 * fs + slab_span() + 63) / 64 * 64;
         nS = 4;
         ngrad = 4;
         nparam = 2;
@@ -465,10 +468,11 @@ struct Ac3dEngine : SsgBase {
         for (int i = 0; i < f - 4; ++i) off += sl[i];
         return off;
     }
+    long long slab_span() const { return (2 * (sx_n + sy_n + sz_n) + 63) / 64 * 64; }
     long long ad_off(int f) const {  // 0..3 fields, 4..9 slabs, 10..15 e arrays
         if (f < 4) return f * fs;
         if (f < 10) return st_off(f);
-        return 4 * fs + 2 * (sx_n + sy_n + sz_n) + (long long)(f - 10) * fs;
+        return 4 * fs + slab_span() + (long long)(f - 10) * fs;
     }
     float* st_field(int f) const override { return f < 4 ? st.p + st_off(f) : nullptr; }
     float* ad_field(int f) const override { return f < 4 ? ad.p + ad_off(f) : nullptr; }
@@ -686,6 +690,32 @@ struct Ac3dEngine : SsgBase {
         }
     }
 
+    // the ring adjoint kernels (tile_z 1 of the adjoint pass)
+    template <int RR>
+    void launch_adj_ring(int id, int S) {
+        Ac3dDev a = dev(S);
+        a.spt = spt_a;
+        pick_zchunk(8);
+        a.zchunk = zchunk;
+        auto al = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+        OWL_CHECK(al(a.aex) && al(a.aey) && al(a.aez) && al(a.aepx) && al(a.aepy) && al(a.aepz) && al(a.ap) &&
+                      al(a.Sp) && al(a.Svx) && al(a.Svy) && al(a.Svz) && sad % 4 == 0 && a.sslot % 4 == 0 &&
+                      fs % 4 == 0 && pitch % 4 == 0,
+                  OWL_ERR_UNSUPPORTED, "ring adjoint operands not 16-byte aligned");
+        const int rows_v = a.z1 - std::min(a.zvx0, a.zvz0);
+        const int rows_a = a.z1 - std::min(std::min(a.zvx0, a.zvz0), a.zp0);
+        dim3 b(32, 8);
+        if (id == OWL_K_ADJ_P) {
+            constexpr int sm = ring_bytes_ap<RR>();
+            OWL_CUDA(cudaFuncSetAttribute(k_ac3d_adj_p_ring<RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            k_ac3d_adj_p_ring<RR><<<grid3(rows_a, S, spt_a, 8), b, sm, stream>>>(a);
+        } else {
+            constexpr int sm = ring_bytes_av<RR>();
+            OWL_CUDA(cudaFuncSetAttribute(k_ac3d_adj_v_ring<RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            k_ac3d_adj_v_ring<RR><<<grid3(rows_v, S, spt_a, 8), b, sm, stream>>>(a);
+        }
+    }
+
     template <int RR, int TY>
     void launch_adj(int id, int S) {
         Ac3dDev a = dev(S);
@@ -760,7 +790,8 @@ struct Ac3dEngine : SsgBase {
             else if (tz == 1) launch_fwd<RR, 1>(id, S, store);
             else launch_fwd<RR, 4>(id, S, store);
         } else {
-            if (tz_a == 2) launch_adj<RR, 2>(id, S);
+            if (tz_a == 1) launch_adj_ring<RR>(id, S);
+            else if (tz_a == 2) launch_adj<RR, 2>(id, S);
             else if (tz_a == 8) launch_adj<RR, 8>(id, S);
             else launch_adj<RR, 4>(id, S);
         }

@@ -448,9 +448,10 @@ void SsgBase::launch_params(const owl_run_opts& o) {
 
 std::vector<int> SsgBase::tune_spt(int) const { return {1, 2, 4, 8, 16, 32}; }
 
-// 3D forward kernels take rows per thread (1, 2, 4; 0 = the per-cell kernel); other kernels a tile height
+// 3D forward kernels take rows per thread (1, 2, 4; 0 = the per-cell kernel), 3D adjoint kernels a
+// tile height (2, 4, 8; 1 = the ring kernels); 2D kernels a tile height
 std::vector<int> SsgBase::tune_tz(int pass) const {
-    if (dim == 3) return pass == 0 ? std::vector<int>{0, 1, 2, 4} : std::vector<int>{2, 4, 8};
+    if (dim == 3) return pass == 0 ? std::vector<int>{0, 1, 2, 4} : std::vector<int>{1, 2, 4, 8};
     return {4, 8, 16};
 }
 

@@ -57,10 +57,27 @@ def test_gradient_parity_3d(fs):
     vp0 = vp * np.float32(1.02)
     mf_ref, g_ref = oracle.ac3d_gradient(d, vp0, rho, ps, obs, adj_kind=0, k=30)
     s = solver3(d, vp0, rho)
-    for opts in (RunOpts(checkpoint_interval=30), RunOpts(checkpoint_interval=40, use_graph=-1, tile_z=8)):
+    # tile_z 1: the ring kernels in both passes
+    for opts in (RunOpts(checkpoint_interval=30), RunOpts(checkpoint_interval=40, use_graph=-1, tile_z=8),
+                 RunOpts(checkpoint_interval=30, tile_z=1)):
         mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, opts)
         assert rel(mf, mf_ref) < 1e-4
         assert rel(g, g_ref) < 1e-4, (opts, rel(g, g_ref))
+
+
+@pytest.mark.parametrize("fs", [0, 1])
+def test_ring_adjoint_matches_tiled(fs):
+    """two shots in one CTA: the ring adjoint (one Kahan update per shot) and the
+    tiled adjoint (shots summed, then one update) agree to FP32 rounding"""
+    d, vp, rho, ps = case3(fs)
+    ps = PreparedShots(ps.shots[:2], GridSpec(nx=d.nx, nz=d.nz, dx=d.dx, dz=d.dz, ny=d.ny, dy=d.dy), d.dt)
+    obs = oracle.ac3d_forward(d, vp, rho, ps, "f32").astype(np.float32)
+    s = solver3(d, vp * np.float32(1.02), rho)
+    mf1, g1 = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=30, tile_z=1, shots_per_cta=2))
+    g1 = g1.copy()
+    mf4, g4 = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=30, tile_z=4, shots_per_cta=2))
+    assert rel(g1, g4) < 1e-5, rel(g1, g4)
+    assert np.allclose(mf1, mf4, rtol=1e-6)
 
 
 _REF3 = {}
