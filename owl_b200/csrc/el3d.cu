@@ -521,6 +521,8 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_s(El3dDev a) {
     for (int q = 0; q < 9; ++q) e3_kahan(a.G, a.gg, go, q, G[q]);
 }
 
+#include "el3d_ring_adj.cuh"
+
 // ---- Thomsen parameterisation (thomsen_to_cij3d, src/lib/module_anisotropy.f90:336-381) ----
 // Dual numbers (value, derivative) for the forward-mode derivatives of the Cij
 // set-up in the chain rule; float / double evaluate the same code.
@@ -741,15 +743,16 @@ struct El3dEngine : SsgBase {
     std::vector<int> tune_spt(int) const override { return {1, 2, 4}; }
     // forward pass: 2 = thread per cell (2 planes per block), 1 = the z-marching
     // ring kernels (half-width 4, no free surface)
-    std::vector<int> tune_tz(int pass) const override {
-        if (pass == 0 && R == 4 && !desc.free_surface) return {2, 1};
+    // (the adjoint pass likewise, with the ring adjoint kernels)
+    std::vector<int> tune_tz(int) const override {
+        if (R == 4 && !desc.free_surface) return {2, 1};
         return {2};
     }
-    // tile_z = 1 asks for the ring forward kernels (where they apply), anything else the per-cell ones
+    // tile_z = 1 asks for the ring kernels of both passes (where they apply), anything else the per-cell ones
     void launch_params(const owl_run_opts& o) override {
         tile_x = 32;
         tz_f = (o.tile_z == 1 && R == 4 && !desc.free_surface) ? 1 : 2;
-        tz_a = 2;
+        tz_a = tz_f;
     }
 
     void set_model(int np, const float* const* f) override {
@@ -975,8 +978,8 @@ struct El3dEngine : SsgBase {
         const int groups = (S + a.spt - 1) / a.spt;
         OWL_CHECK((long long)a.nzb * groups < 65536, OWL_ERR_UNSUPPORTED, "too many z blocks x shot groups");
         const dim3 b(32, 4, 2), g((NXp + 31) / 32, (NYp + 3) / 4, a.nzb * groups);
-        if (fwd && tz_f == 1 && RR == 4 && !FF) {
-            OWL_CHECK(!store || a.S, OWL_ERR_INVALID, "stencil-term buffer not allocated");
+        if ((fwd ? tz_f : tz_a) == 1 && RR == 4 && !FF) {
+            OWL_CHECK(fwd ? (!store || a.S) : (a.ad && a.S && a.G), OWL_ERR_INVALID, "buffers not allocated");
             const int rows = a.z1 - a.z0;
             const long long xy = (long long)((NXp + 31) / 32) * ((NYp + 7) / 8);
             const long long want = std::max<long long>(1, (148LL * 64 + xy - 1) / xy);
@@ -984,7 +987,15 @@ struct El3dEngine : SsgBase {
             const int nzc = (rows + a.zchunk - 1) / a.zchunk;
             OWL_CHECK((long long)nzc * groups < 65536, OWL_ERR_UNSUPPORTED, "too many z chunks x shot groups");
             const dim3 br(32, 8), gr((NXp + 31) / 32, (NYp + 7) / 8, nzc * groups);
-            if (id == OWL_K_FWD_P) {
+            if (id == OWL_K_ADJ_P) {
+                constexpr int sm = e3ra_bytes_v<4>();
+                OWL_CUDA(cudaFuncSetAttribute(k_el3d_adj_v_ring<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+                k_el3d_adj_v_ring<4><<<gr, br, sm, stream>>>(a);
+            } else if (id == OWL_K_ADJ_V) {
+                constexpr int sm = e3ra_bytes_s<4>();
+                OWL_CUDA(cudaFuncSetAttribute(k_el3d_adj_s_ring<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+                k_el3d_adj_s_ring<4><<<gr, br, sm, stream>>>(a);
+            } else if (id == OWL_K_FWD_P) {
                 constexpr int sm = e3r_bytes_s<4>();
                 auto k = store ? k_el3d_fwd_s_ring<4, true> : k_el3d_fwd_s_ring<4, false>;
                 OWL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
