@@ -3,6 +3,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <map>
 
@@ -130,7 +131,9 @@ __global__ void k_pack(const float* __restrict__ st, long long sstride, SegDev s
     unsigned short* q = out + s * sstride + sg.off[g];
     const long long n = sg.len[g];
     const float sc = scale[s * sg.nseg + g];
-    const float inv = sc > 0.f ? 1.0f / sc : 0.f;
+    // a field whose largest value is below the smallest normal float is stored as
+    // zero: 1 / sc would overflow and turn its zeros into NaN
+    const float inv = sc >= FLT_MIN ? 1.0f / sc : 0.f;
     for (long long i = blockIdx.z * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.z * blockDim.x) {
         float v = p[i] * inv;
         if (BF16) {
@@ -156,7 +159,7 @@ __global__ void k_unpack(const unsigned short* __restrict__ in, long long sstrid
         float v;
         if (BF16) v = __bfloat162float(*reinterpret_cast<__nv_bfloat16*>(&u));
         else v = __half2float(*reinterpret_cast<__half*>(&u));
-        p[i] = v * sc;
+        p[i] = sc >= FLT_MIN ? v * sc : 0.f;
     }
 }
 

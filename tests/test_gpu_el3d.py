@@ -76,3 +76,26 @@ def test_el3d_source_gradient_parity(fs):
                 mask[off + t - 1] = True
             off += d.nt
     assert rel(got[mask], sref[mask]) < GRAD_TOL
+
+
+def test_el3d_half_checkpoints_of_tiny_fields():
+    """the orthorhombic c5 model on 96^3 (136^3 padded), 300 steps: its force
+    source gives wavefields some of whose checkpointed fields have a largest
+    value below the smallest normal float; FP16 / BF16 checkpoints keep the
+    gradient finite and within 1e-3 of the FP32-checkpoint gradient (a
+    reciprocal of such a scale overflowed and turned the field's zeros into
+    NaN)."""
+    from owl_b200 import configs
+    d, f, shots = configs.config5(1, nt=300, n=96, nrec=32)
+    s = SSGSolver(L.OWL_ELASTIC_VHTIORT_3D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
+                  f0_max=d.f0_max, max_shots=1, ny=d.ny, dy=d.dy, aniso=d.aniso)
+    s.set_model(*f)
+    ps = s.prepare(shots)
+    obs = np.zeros(s.seis_size(ps), dtype=np.float32)
+    _, g32 = s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=50))
+    g32 = np.array(g32, copy=True)
+    assert np.all(np.isfinite(g32))
+    for prec in (L.OWL_CKPT_FP16, L.OWL_CKPT_BF16):
+        _, g = s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=50, checkpoint_precision=prec))
+        assert np.all(np.isfinite(g)), prec
+        assert rel(g, g32) < 1e-3, (prec, rel(g, g32))
