@@ -135,9 +135,10 @@ def forward_3d_block(peak, peak_kind):
     g.set_model(vpg, rhog)
     go = RunOpts(checkpoint_precision=L.OWL_CKPT_FP16)
     g.gradient(pg, obs, opts=go)
-    g.gradient(pg, obs, opts=go)
+    _, gr = g.gradient(pg, obs, opts=go)
     out["gradient_workload"] = "the same model and shot, 500 of the 1500 steps, FP16 checkpoints every 50 steps"
     out["gradient_s_per_shot"] = g.last_info.elapsed_ms / 1e3
+    out["gradient_finite"] = bool(np.all(np.isfinite(np.asarray(gr))))
     for kid, name in ((L.OWL_K_ADJ_P, "k_ac3d_adj_p"), (L.OWL_K_ADJ_V, "k_ac3d_adj_v")):
         kms, b = g.kernel_time(kid, 10)
         ach = b / (kms / 1e3) / 1e9
@@ -216,8 +217,9 @@ def elastic_2d_block(peak, peak_kind, ngrad=16):
     s.gradient(sub, obs, opts=opts)
     gms = []
     for _ in range(2):
-        s.gradient(sub, obs, opts=opts)
+        _, gr = s.gradient(sub, obs, opts=opts)
         gms.append(s.last_info.elapsed_ms)
+    out["gradient_finite"] = bool(np.all(np.isfinite(np.asarray(gr))))
     out["gradient_shots"] = ngrad
     out["gradient_s_per_shot"] = sum(gms) / len(gms) / 1e3 / ngrad
     out["gradient_checkpoints"] = "fp16, per-field scale, every 50 steps"
@@ -276,7 +278,8 @@ def elastic_3d_block(peak, peak_kind, nshots=4, nt=500):
     pg = g.prepare(shg)
     obs = np.zeros(g.seis_size(pg), dtype=np.float32)
     g.gradient(pg, obs, opts=RunOpts(checkpoint_precision=L.OWL_CKPT_FP16))
-    g.gradient(pg, obs, opts=RunOpts(checkpoint_precision=L.OWL_CKPT_FP16))
+    _, gr = g.gradient(pg, obs, opts=RunOpts(checkpoint_precision=L.OWL_CKPT_FP16))
+    out["gradient_finite"] = bool(np.all(np.isfinite(np.asarray(gr))))
     out["gradient_workload"] = "96^3 model of the same kind (136^3 padded), 300 steps, 1 shot, FP16 checkpoints"
     out["gradient_s_per_shot"] = g.last_info.elapsed_ms / 1e3
     for kid, name in ((L.OWL_K_ADJ_P, "k_el3d_adj_v"), (L.OWL_K_ADJ_V, "k_el3d_adj_s")):
