@@ -76,7 +76,8 @@ def profile_3d(n, rows=1):
 
 def profile_3d_grad(n):
     """Small 3D acoustic gradient for kernel captures: N^3 layered model, one
-    shot, 60 steps, checkpoints every 20 steps."""
+    shot, 60 steps, checkpoints every 20 steps, the ring kernels of both passes
+    (tile_z 1: no autotuning launches)."""
     import numpy as np
     from owl_b200 import _lib as L
     from owl_b200 import configs
@@ -88,7 +89,7 @@ def profile_3d_grad(n):
     s.set_model(vp, rho)
     ps = s.prepare(shots)
     obs = np.zeros(s.seis_size(ps), dtype=np.float32)
-    s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=20, shots_per_cta=1, use_graph=-1))
+    s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=20, shots_per_cta=1, tile_z=1, use_graph=-1))
     print(f"profile3d-grad: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
     s.close()
 
@@ -139,7 +140,11 @@ def forward_3d_block(peak, peak_kind):
     out["gradient_workload"] = "the same model and shot, 500 of the 1500 steps, FP16 checkpoints every 50 steps"
     out["gradient_s_per_shot"] = g.last_info.elapsed_ms / 1e3
     out["gradient_finite"] = bool(np.all(np.isfinite(np.asarray(gr))))
-    for kid, name in ((L.OWL_K_ADJ_P, "k_ac3d_adj_p"), (L.OWL_K_ADJ_V, "k_ac3d_adj_v")):
+    # the autotuner's adjoint kernels: z-marching ring (tile 1) or tiled
+    ring = g.last_info.tile_z == 1
+    out["adjoint_kernels"] = "z-marching ring" if ring else f"tiled, {g.last_info.tile_z} rows"
+    for kid, name in ((L.OWL_K_ADJ_P, "k_ac3d_adj_p_ring" if ring else "k_ac3d_adj_p"),
+                      (L.OWL_K_ADJ_V, "k_ac3d_adj_v_ring" if ring else "k_ac3d_adj_v")):
         kms, b = g.kernel_time(kid, 10)
         ach = b / (kms / 1e3) / 1e9
         out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
@@ -282,7 +287,10 @@ def elastic_3d_block(peak, peak_kind, nshots=4, nt=500):
     out["gradient_finite"] = bool(np.all(np.isfinite(np.asarray(gr))))
     out["gradient_workload"] = "96^3 model of the same kind (136^3 padded), 300 steps, 1 shot, FP16 checkpoints"
     out["gradient_s_per_shot"] = g.last_info.elapsed_ms / 1e3
-    for kid, name in ((L.OWL_K_ADJ_P, "k_el3d_adj_v"), (L.OWL_K_ADJ_V, "k_el3d_adj_s")):
+    ring_a = g.last_info.tile_z == 1
+    out["adjoint_kernels"] = "z-marching ring" if ring_a else "thread per cell"
+    for kid, name in ((L.OWL_K_ADJ_P, "k_el3d_adj_v_ring" if ring_a else "k_el3d_adj_v"),
+                      (L.OWL_K_ADJ_V, "k_el3d_adj_s_ring" if ring_a else "k_el3d_adj_s")):
         kms, b = g.kernel_time(kid, 10)
         ach = b / (kms / 1e3) / 1e9
         out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
