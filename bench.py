@@ -362,10 +362,11 @@ def misfit_block(s, ps, obs_dev, opts, l2_ms):
                        f"{ntr} traces of {nt} samples; adaptive: linear penalty, tlag_max 0.2 s, deconv_eps 0.1"}
     for name, kind in L.MISFIT_NAMES.items():
         mo = MisfitOpts(misfit=kind, dt=s.desc.dt, tlag_max=0.2)
-        if kind == L.OWL_MISFIT_DTW:
+        if kind in (L.OWL_MISFIT_DTW, L.OWL_MISFIT_LOCAL_ADAPTIVE):
             # DTW's dynamic program costs O(nt m^2) double-precision steps per trace
-            # (m = 2 tlag_max / dt + 1 = 401 candidate shifts here): its adjoint
-            # source is timed on the first 4 gathers, without a gradient
+            # (m = 2 tlag_max / dt + 1 = 401 candidate shifts here), the local
+            # adaptive misfit five length-2 nt transforms per sample: their adjoint
+            # sources are timed on the first 4 gathers, without a gradient
             g4 = gp[:5]
             n4 = int(g4[-1])
             adjoint_source(mo, g4, syn2[:n4], obs2[:n4])
@@ -373,7 +374,8 @@ def misfit_block(s, ps, obs_dev, opts, l2_ms):
             t0 = time.perf_counter()
             adjoint_source(mo, g4, syn2[:n4], obs2[:n4])
             ams = (time.perf_counter() - t0) * 1e3
-            out[name] = {"sample": f"4 gathers, {n4} traces of {nt} samples, 401 candidate shifts",
+            what = "401 candidate shifts" if kind == L.OWL_MISFIT_DTW else "Gaussian windows of 0.25 s"
+            out[name] = {"sample": f"4 gathers, {n4} traces of {nt} samples, {what}",
                          "adjoint_source_ms": ams, "traces_per_s": n4 / (ams / 1e3)}
             continue
         s.gradient_misfit(ps, obs_dev, mo, opts)

@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define OWL_SSG_ABI_VERSION 4
+#define OWL_SSG_ABI_VERSION 5
 
 /* status codes */
 #define OWL_OK 0
@@ -94,6 +94,8 @@ extern "C" {
 #define OWL_MISFIT_PHASE 3    /* compute_adjsrc_phase :459-482 (instantaneous phase) */
 #define OWL_MISFIT_ADAPTIVE 4 /* compute_adjsrc_adaptive :490-537 (adaptive waveform inversion) */
 #define OWL_MISFIT_DTW 5      /* compute_adjsrc_dtw :715-980, solve_gdtw :73-234 (dynamic time warping) */
+#define OWL_MISFIT_LOCAL_ADAPTIVE 6     /* compute_adjsrc_local_adaptive :545-625 (Gaussian-windowed AWI) */
+#define OWL_MISFIT_ADAPTIVE_SPACETIME 7 /* compute_adjsrc_adaptive_spacetime :630-700 (AWI over neighbouring traces) */
 
 /* form of the DTW misfit (dtw_form) */
 #define OWL_DTW_PHASE 0     /* misfit sum q tau^2, adjoint q tau d/dt(warped obs) / dt */
@@ -116,7 +118,8 @@ extern "C" {
  * 0 -> 1e-3 (a negative value of these four means 0), dtw_loss_power 0 -> 0.5
  * (the reference's 'l0.5'), dtw_amp_weight 0 -> 1, dtw_trc traces on each side
  * of a trace that enter its distance (0), dtw_form OWL_DTW_*. DTW takes the
- * traces at their own sampling; the shifts are not smoothed across traces. */
+ * traces at their own sampling; the shifts are not smoothed across traces.
+ * lawi_sigma 0 -> 0.25 (s), adaptive_half_window 0 -> 3 (traces). */
 typedef struct {
     int misfit;              /* OWL_MISFIT_* */
     float dt;                /* sample interval of the traces (s) */
@@ -134,6 +137,8 @@ typedef struct {
     float dtw_epsrel;        /* relative stop tolerance of the path cost */
     float dtw_loss_power;    /* p of the distance sum |obs(t + tau) - syn(t)|^p */
     float dtw_amp_weight;    /* weight of the amplitude term of OWL_DTW_PHASE_AMP */
+    float lawi_sigma;        /* local adaptive: standard deviation of the Gaussian time window (s) */
+    int adaptive_half_window; /* space-time adaptive: neighbouring traces on each side */
 } owl_misfit_opts;
 
 typedef struct owl_ssg owl_ssg;
@@ -375,8 +380,9 @@ void owl_ssg_destroy(owl_ssg *h);
  *   gather_misfit: one double per gather (may be NULL).
  * syn, obs, adj, weight, trace_misfit and gather_misfit are all host memory
  * (OWL_MEM_HOST) or all device memory of the current device (OWL_MEM_DEVICE).
- * Trace length: nt <= 8192 (envelope, phase) or next_power_235(2 nt) <= 8192
- * (adaptive), 3 <= nt <= 16384 with 3 <= 2 tlag_max / dt + 1 <= 4095 (DTW),
+ * Trace length: nt <= 8192 (envelope, phase), next_power_235(2 nt) <= 8192
+ * (adaptive, local adaptive), next_power_235(4 nt) <= 8192 (space-time
+ * adaptive), 3 <= nt <= 16384 with 3 <= 2 tlag_max / dt + 1 <= 4095 (DTW),
  * else OWL_ERR_INVALID. */
 int owl_adjoint_source(const owl_misfit_opts *mopts, int ngather, const int *gather_ptr, int nt,
                        const float *syn, const float *obs, const float *weight, float *adj,

@@ -392,6 +392,225 @@ __global__ void __launch_bounds__(256) k_adjsrc(AdjArgs g) {
     }
 }
 
+// spectra products of the adaptive misfits: a conj(b) / (|b|^2 + eps) and a b / (|b|^2 + eps)
+__device__ __forceinline__ float2 deconv_conj(float2 a, float2 b, float eps) {
+    const float q = 1.f / (b.x * b.x + b.y * b.y + eps);
+    return make_float2((a.x * b.x + a.y * b.y) * q, (a.y * b.x - a.x * b.y) * q);
+}
+__device__ __forceinline__ float2 deconv_mul(float2 a, float2 b, float eps) {
+    const float q = 1.f / (b.x * b.x + b.y * b.y + eps);
+    return make_float2((a.x * b.x - a.y * b.y) * q, (a.x * b.y + a.y * b.x) * q);
+}
+
+struct LocArgs {
+    int nt, ntr, ngather, hw;
+    const int* gptr;
+    const float* syn;
+    const float* obs;
+    const unsigned char* live;
+    float* adj;
+    double* tm;
+    DftDev dft;         // length next_power_235(2 nt) (local) or next_power_235(4 nt) (space-time)
+    const float* pen;   // penalty per circular lag bin (dft.N)
+    const float* ramp;  // Hann ramp of tl samples
+    int tl;
+    float deconv_eps, sigma;  // sigma: Gaussian window in samples (local)
+    float* scratch;           // per CTA: 4 N floats (local)
+    float2* cscratch;         // per CTA: 2 N (local) or 3 N (space-time) complex
+};
+
+__device__ __forceinline__ float ramp_l(const LocArgs& g, int i) { return i < g.tl ? g.ramp[i] : 1.f; }
+
+// compute_adjsrc_local_adaptive (:545-625): the adaptive matching filter of the
+// trace under a Gaussian window centred on each sample; misfit sum of the
+// squared window misfits, adjoint the window adjoints weighted by the window and
+// normalised by the sum of the squared windows. One CTA per trace.
+__global__ void __launch_bounds__(256) k_adjsrc_local(LocArgs g) {
+    extern __shared__ float2 work[];
+    __shared__ double redd[32];
+    __shared__ float redf[32];
+    const int tid = threadIdx.x, nth = blockDim.x, nt = g.nt, N = g.dft.N;
+    float* u = g.scratch + (size_t)blockIdx.x * 4 * N;
+    float* d = u + N;
+    float* acc = d + N;
+    float* sac = acc + N;
+    float2* cd = g.cscratch + (size_t)blockIdx.x * 2 * N;
+    float2* cu = cd + N;
+    for (int r = blockIdx.x; r < g.ntr; r += gridDim.x) {
+        float* ad = g.adj ? g.adj + (size_t)r * nt : nullptr;
+        if (!g.live[r]) {
+            if (ad)
+                for (int t = tid; t < nt; t += nth) ad[t] = 0.f;
+            if (tid == 0 && g.tm) g.tm[r] = 0.0;
+            continue;
+        }
+        const float* sy = g.syn + (size_t)r * nt;
+        const float* ob = g.obs + (size_t)r * nt;
+        for (int k = tid; k < N; k += nth) {
+            const float rp = k < nt ? ramp_l(g, k) * ramp_l(g, nt - 1 - k) : 0.f;
+            u[k] = k < nt ? sy[k] * rp : 0.f;
+            d[k] = k < nt ? ob[k] * rp : 0.f;
+            acc[k] = 0.f;
+            sac[k] = 0.f;
+        }
+        __syncthreads();
+        // eps from the whole trace's spectrum, eta from its matching filter
+        for (int k = tid; k < N; k += nth) work[k] = make_float2(d[k], 0.f);
+        dft(work, g.dft, false);
+        float mx = 0.f;
+        for (int k = tid; k < N; k += nth) {
+            cd[k] = work[k];
+            mx = fmaxf(mx, work[k].x * work[k].x + work[k].y * work[k].y);
+        }
+        mx = block_max(mx, redf);
+        float eps = g.deconv_eps * mx;
+        if (eps == 0.f) eps = 1.0e-30f;
+        for (int k = tid; k < N; k += nth) work[k] = make_float2(u[k], 0.f);
+        dft(work, g.dft, false);
+        for (int k = tid; k < N; k += nth) work[k] = deconv_conj(work[k], cd[k], eps);
+        dft(work, g.dft, true);
+        float mxx = 0.f;
+        for (int k = tid; k < N; k += nth) mxx = fmaxf(mxx, work[k].x * work[k].x);
+        mxx = block_max(mxx, redf);
+        float eta = g.deconv_eps * mxx;
+        if (eta == 0.f) eta = 1.0e-30f;
+        const float inv2s2 = 1.f / (2.f * g.sigma * g.sigma);
+        double m = 0.0;
+        for (int i = 1; i <= nt; ++i) {
+            // window spectra: U = F(u g), D = F(d g), a_k = k + 1
+            for (int k = tid; k < N; k += nth) {
+                const float x = (float)(k + 1 - i);
+                work[k] = make_float2(u[k] * expf(-x * x * inv2s2), 0.f);
+            }
+            dft(work, g.dft, false);
+            for (int k = tid; k < N; k += nth) cu[k] = work[k];
+            for (int k = tid; k < N; k += nth) {
+                const float x = (float)(k + 1 - i);
+                work[k] = make_float2(d[k] * expf(-x * x * inv2s2), 0.f);
+            }
+            dft(work, g.dft, false);
+            for (int k = tid; k < N; k += nth) {
+                cd[k] = work[k];
+                work[k] = deconv_conj(cu[k], work[k], eps);
+            }
+            dft(work, g.dft, true);
+            double sxx = 0.0, swx = 0.0;
+            for (int k = tid; k < N; k += nth) {
+                const double xc = work[k].x, wx = (double)g.pen[k] * xc;
+                sxx += xc * xc;
+                swx += wx * wx;
+            }
+            sxx = block_sum(sxx, redd) + (double)eta;
+            swx = block_sum(swx, redd);
+            const double vt = swx / sxx;
+            m += vt * vt;
+            for (int k = tid; k < N; k += nth) {
+                const double w = g.pen[k];
+                work[k] = make_float2((float)(vt * (w * w - vt) * (double)work[k].x / sxx), 0.f);
+            }
+            dft(work, g.dft, false);
+            for (int k = tid; k < N; k += nth) work[k] = deconv_mul(work[k], cd[k], eps);
+            dft(work, g.dft, true);
+            for (int k = tid; k < N; k += nth) {
+                const float x = (float)(k + 1 - i), gw = expf(-x * x * inv2s2);
+                acc[k] += work[k].x * gw;
+                sac[k] += gw * gw;
+            }
+        }
+        __syncthreads();
+        if (ad)
+            for (int t = tid; t < nt; t += nth) ad[t] = acc[t] / sac[t] * ramp_l(g, nt - 1 - t);
+        if (tid == 0 && g.tm) g.tm[r] = m;
+        __syncthreads();
+    }
+}
+
+// gather of trace r (gptr ascending)
+__device__ int gather_index(const int* gptr, int ngather, int r) {
+    int lo = 0, hi = ngather - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (gptr[mid] <= r) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// compute_adjsrc_adaptive_spacetime (:630-700): the matching filter averaged
+// over the trace and its hw neighbours on each side within the gather (dropped
+// traces count as zero traces and are left out of the average), misfit as the
+// adaptive one, adjoint through the centre trace's spectrum. One CTA per trace.
+__global__ void __launch_bounds__(256) k_adjsrc_spacetime(LocArgs g) {
+    extern __shared__ float2 work[];
+    __shared__ double redd[32];
+    __shared__ float redf[32];
+    const int tid = threadIdx.x, nth = blockDim.x, nt = g.nt, N = g.dft.N;
+    float2* cs = g.cscratch + (size_t)blockIdx.x * 3 * N;  // summed filter spectra
+    float2* cd = cs + N;                                   // a neighbour's D
+    float2* cc = cd + N;                                   // the centre trace's D
+    for (int r = blockIdx.x; r < g.ntr; r += gridDim.x) {
+        float* ad = g.adj ? g.adj + (size_t)r * nt : nullptr;
+        if (!g.live[r]) {
+            if (ad)
+                for (int t = tid; t < nt; t += nth) ad[t] = 0.f;
+            if (tid == 0 && g.tm) g.tm[r] = 0.0;
+            continue;
+        }
+        const int gi = gather_index(g.gptr, g.ngather, r), g0 = g.gptr[gi], g1 = g.gptr[gi + 1];
+        for (int k = tid; k < N; k += nth) cs[k] = make_float2(0.f, 0.f);
+        int l = 0;
+        float eps_c = 0.f;
+        for (int q = r - g.hw; q <= r + g.hw; ++q) {
+            if (q < g0 || q >= g1 || !g.live[q]) continue;
+            const float* sy = g.syn + (size_t)q * nt;
+            const float* ob = g.obs + (size_t)q * nt;
+            for (int k = tid; k < N; k += nth)
+                work[k] = make_float2(k < nt ? ob[k] * ramp_l(g, k) * ramp_l(g, nt - 1 - k) : 0.f, 0.f);
+            dft(work, g.dft, false);
+            float mx = 0.f;
+            for (int k = tid; k < N; k += nth) {
+                cd[k] = work[k];
+                if (q == r) cc[k] = work[k];
+                mx = fmaxf(mx, work[k].x * work[k].x + work[k].y * work[k].y);
+            }
+            mx = block_max(mx, redf);
+            const float eps = g.deconv_eps * mx;
+            if (q == r) eps_c = eps;
+            if (!(eps > 0.f)) continue;
+            for (int k = tid; k < N; k += nth)
+                work[k] = make_float2(k < nt ? sy[k] * ramp_l(g, k) * ramp_l(g, nt - 1 - k) : 0.f, 0.f);
+            dft(work, g.dft, false);
+            for (int k = tid; k < N; k += nth) {
+                const float2 v = deconv_conj(work[k], cd[k], eps);
+                cs[k] = make_float2(cs[k].x + v.x, cs[k].y + v.y);
+            }
+            ++l;
+        }
+        for (int k = tid; k < N; k += nth) work[k] = cs[k];
+        dft(work, g.dft, true);
+        double sxx = 0.0, swx = 0.0;
+        const float il = l > 0 ? 1.f / (float)l : 0.f;
+        for (int k = tid; k < N; k += nth) {
+            const double xc = (double)(work[k].x * il), wx = (double)g.pen[k] * xc;
+            sxx += xc * xc;
+            swx += wx * wx;
+        }
+        sxx = block_sum(sxx, redd);
+        swx = block_sum(swx, redd);
+        const double m = l > 0 ? 0.5 * swx / sxx : 0.0;
+        for (int k = tid; k < N; k += nth) {
+            const double w = g.pen[k];
+            work[k] = make_float2((float)((w * w - 2.0 * m) * (double)(work[k].x * il) / sxx), 0.f);
+        }
+        dft(work, g.dft, false);
+        for (int k = tid; k < N; k += nth) work[k] = deconv_mul(work[k], cc[k], eps_c);
+        dft(work, g.dft, true);
+        if (ad)
+            for (int t = tid; t < nt; t += nth) ad[t] = work[t].x * ramp_l(g, nt - 1 - t);
+        if (tid == 0 && g.tm) g.tm[r] = m;
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 void DftTables::build(int n, cudaStream_t s) {
@@ -428,10 +647,42 @@ void DftTables::build(int n, cudaStream_t s) {
     logM = lg;
 }
 
+// xcorr_penalty (:321-363) laid out on the nnt circular lags of an adaptive
+// misfit: maxlag = ceiling(tlag_max / dt) (at most (nnt - 1) / 2), lag i at
+// bin i, lag -i at bin nnt - i
+static std::vector<float> awi_penalty(const owl_misfit_opts& o, float tlag, int nnt) {
+    int maxlag = (int)std::ceil(tlag / o.dt);
+    maxlag = std::max(0, std::min(maxlag, (nnt - 1) / 2));
+    const double pw = std::fabs(o.penalty_power != 0.f ? (double)o.penalty_power : 1.0);
+    std::vector<double> p(2 * maxlag + 1);
+    const double sc = 1.0 / std::sqrt(2.0 * std::log(100.0));
+    for (int i = -maxlag; i <= maxlag; ++i) {
+        const double t = (double)i * (double)o.dt;
+        double w;
+        switch (o.penalty) {
+            case OWL_PENALTY_POWER: w = std::pow(std::fabs(t / tlag), pw); break;
+            case OWL_PENALTY_GAUSSIAN: w = std::exp(-t * t / (sc * (double)tlag * (double)tlag)); break;
+            case OWL_PENALTY_EXP: w = std::exp(-std::fabs(t) / (sc * (double)tlag)); break;
+            default: w = std::fabs(t / tlag); break;
+        }
+        p[i + maxlag] = w;
+    }
+    if (o.penalty == OWL_PENALTY_GAUSSIAN || o.penalty == OWL_PENALTY_EXP) {
+        // rescale to [0, 1], power, 1 - w
+        const double lo = *std::min_element(p.begin(), p.end()), hi = *std::max_element(p.begin(), p.end());
+        for (double& w : p) w = 1.0 - std::pow(hi > lo ? (w - lo) / (hi - lo) : 0.0, pw);
+    }
+    std::vector<float> hp(nnt, 0.f);
+    for (int i = 0; i <= maxlag; ++i) hp[i] = (float)p[maxlag + i];
+    for (int i = 1; i <= maxlag; ++i) hp[nnt - i] = (float)p[maxlag - i];
+    return hp;
+}
+
 void AdjointSource::run(const owl_misfit_opts& o, int ngather, const int* h_gather_ptr, int nt, const float* syn,
                         const float* obs, const unsigned char* weight_live, float* adj, double* tm, double* gm,
                         cudaStream_t s, float* tau) {
-    OWL_CHECK(o.misfit >= OWL_MISFIT_WAVEFORM && o.misfit <= OWL_MISFIT_DTW, OWL_ERR_INVALID, "bad misfit type");
+    OWL_CHECK(o.misfit >= OWL_MISFIT_WAVEFORM && o.misfit <= OWL_MISFIT_ADAPTIVE_SPACETIME, OWL_ERR_INVALID,
+              "bad misfit type");
     OWL_CHECK(nt >= 1 && ngather >= 0 && (ngather == 0 || h_gather_ptr), OWL_ERR_INVALID, "bad trace layout");
     OWL_CHECK(ngather == 0 || h_gather_ptr[0] == 0, OWL_ERR_INVALID, "gather_ptr[0] must be 0");
     for (int g = 0; g < ngather; ++g)
@@ -458,6 +709,63 @@ void AdjointSource::run(const owl_misfit_opts& o, int ngather, const int* h_gath
             tm = tmp.p;
         }
         run_dtw(o, ngather, nt, ntr, syn, obs, adj, tm, tau, s);
+        if (gm) {
+            k_gather_sum<<<(ngather + 127) / 128, 128, 0, s>>>(tm, gptr.p, ngather, gm);
+            OWL_LAUNCH_CHECK();
+            launches++;
+        }
+        OWL_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    if (o.misfit == OWL_MISFIT_LOCAL_ADAPTIVE || o.misfit == OWL_MISFIT_ADAPTIVE_SPACETIME) {
+        OWL_CHECK(o.dt > 0.f, OWL_ERR_INVALID, "the adaptive misfits need the sample interval dt");
+        const bool loc = o.misfit == OWL_MISFIT_LOCAL_ADAPTIVE;
+        const int nnt = next_power_235(loc ? 2 * nt : 4 * nt);
+        awl.build(nnt, s);
+        const float tlag = o.tlag_max > 0.f ? o.tlag_max : 0.1f * (float)(nt - 1) * o.dt;
+        const std::vector<float> hp = awi_penalty(o, tlag, nnt);
+        pen.upload(hp.data(), hp.size(), s);
+        const int tl = (int)std::floor(0.025f * (float)nt + 0.5f);
+        std::vector<float> hramp(std::max(tl, 1));
+        for (int i = 0; i < tl; ++i) hramp[i] = (float)(0.5 * (1.0 - std::cos(M_PI * (double)i / (double)tl)));
+        ramp.upload(hramp.data(), hramp.size(), s);
+        DevBuf<double> tmp;
+        if (!tm && gm) {
+            tmp.reserve(ntr);
+            tm = tmp.p;
+        }
+        LocArgs la{};
+        la.nt = nt;
+        la.ntr = ntr;
+        la.ngather = ngather;
+        la.hw = o.adaptive_half_window > 0 ? o.adaptive_half_window : 3;
+        la.gptr = gptr.p;
+        la.syn = syn;
+        la.obs = obs;
+        la.live = live.p;
+        la.adj = adj;
+        la.tm = tm;
+        la.dft = dev(awl);
+        la.pen = pen.p;
+        la.ramp = ramp.p;
+        la.tl = tl;
+        la.deconv_eps = o.deconv_eps > 0.f ? o.deconv_eps : 0.1f;
+        la.sigma = (o.lawi_sigma > 0.f ? o.lawi_sigma : 0.25f) / o.dt;
+        const size_t smem = (size_t)awl.M * sizeof(float2);
+        auto k = loc ? k_adjsrc_local : k_adjsrc_spacetime;
+        OWL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0, nsm = 0, dev_id = 0;
+        OWL_CUDA(cudaGetDevice(&dev_id));
+        OWL_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev_id));
+        OWL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
+        const int grid = std::max(1, std::min(ntr, nsm * std::max(1, per_sm)));
+        scratch.reserve(loc ? (size_t)grid * 4 * nnt : 1);
+        cscratch.reserve((size_t)grid * (loc ? 2 : 3) * nnt);
+        la.scratch = scratch.p;
+        la.cscratch = cscratch.p;
+        k<<<grid, 256, smem, s>>>(la);
+        OWL_LAUNCH_CHECK();
+        launches++;
         if (gm) {
             k_gather_sum<<<(ngather + 127) / 128, 128, 0, s>>>(tm, gptr.p, ngather, gm);
             OWL_LAUNCH_CHECK();
@@ -493,33 +801,9 @@ void AdjointSource::run(const owl_misfit_opts& o, int ngather, const int* h_gath
         awi.build(nnt, s);
         a.awi = dev(awi);
         M = awi.M;
-        // maxlag = ceiling(tlag_max / dt), tl = nint(0.025 n) in single precision (:502-505)
         const float tlag = o.tlag_max > 0.f ? o.tlag_max : 0.1f * (float)(nt - 1) * o.dt;
-        int maxlag = (int)std::ceil(tlag / o.dt);
-        maxlag = std::max(0, std::min(maxlag, (nnt - 1) / 2));
+        hp = awi_penalty(o, tlag, nnt);
         const int tl = (int)std::floor(0.025f * (float)nt + 0.5f);
-        const double pw = std::fabs(o.penalty_power != 0.f ? (double)o.penalty_power : 1.0);
-        std::vector<double> p(2 * maxlag + 1);
-        const double sc = 1.0 / std::sqrt(2.0 * std::log(100.0));
-        for (int i = -maxlag; i <= maxlag; ++i) {
-            const double t = (double)i * (double)o.dt;
-            double w;
-            switch (o.penalty) {
-                case OWL_PENALTY_POWER: w = std::pow(std::fabs(t / tlag), pw); break;
-                case OWL_PENALTY_GAUSSIAN: w = std::exp(-t * t / (sc * (double)tlag * (double)tlag)); break;
-                case OWL_PENALTY_EXP: w = std::exp(-std::fabs(t) / (sc * (double)tlag)); break;
-                default: w = std::fabs(t / tlag); break;
-            }
-            p[i + maxlag] = w;
-        }
-        if (o.penalty == OWL_PENALTY_GAUSSIAN || o.penalty == OWL_PENALTY_EXP) {
-            // rescale to [0, 1], power, 1 - w
-            const double lo = *std::min_element(p.begin(), p.end()), hi = *std::max_element(p.begin(), p.end());
-            for (double& w : p) w = 1.0 - std::pow(hi > lo ? (w - lo) / (hi - lo) : 0.0, pw);
-        }
-        hp.assign(nnt, 0.f);
-        for (int i = 0; i <= maxlag; ++i) hp[i] = (float)p[maxlag + i];
-        for (int i = 1; i <= maxlag; ++i) hp[nnt - i] = (float)p[maxlag - i];
         pen.upload(hp.data(), hp.size(), s);
         a.pen = pen.p;
         hramp.resize(std::max(tl, 1));

@@ -16,7 +16,7 @@ struct DftTables {
 };
 
 struct AdjointSource {
-    DftTables hil, awi;
+    DftTables hil, awi, awl;  // awl: the local and space-time adaptive misfits
     DevBuf<int> gptr;
     DevBuf<unsigned char> live;
     DevBuf<double> nrm, gmax;

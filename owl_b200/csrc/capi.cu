@@ -184,7 +184,7 @@ int owl_ssg_gradient_misfit(owl_ssg* h, int nshots, const owl_shot* shots, const
         OWL_CHECK(nshots >= 0 && (nshots == 0 || shots), OWL_ERR_INVALID, "bad shots");
         OWL_CHECK(obs || nshots == 0, OWL_ERR_INVALID, "null data buffer");
         OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
-        OWL_CHECK(mopts->misfit >= OWL_MISFIT_WAVEFORM && mopts->misfit <= OWL_MISFIT_DTW, OWL_ERR_INVALID,
+        OWL_CHECK(mopts->misfit >= OWL_MISFIT_WAVEFORM && mopts->misfit <= OWL_MISFIT_ADAPTIVE_SPACETIME, OWL_ERR_INVALID,
                   "bad misfit type");
         h->eng->mopts = *mopts;
         if (h->eng->mopts.dt <= 0.f) h->eng->mopts.dt = h->eng->desc.dt;

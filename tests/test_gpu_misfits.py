@@ -23,7 +23,7 @@ from test_gpu_ac2d import make_solver
 pytestmark = pytest.mark.gpu
 
 KINDS = [L.OWL_MISFIT_WAVEFORM, L.OWL_MISFIT_CORR, L.OWL_MISFIT_ENVELOPE, L.OWL_MISFIT_PHASE,
-         L.OWL_MISFIT_ADAPTIVE]
+         L.OWL_MISFIT_ADAPTIVE, L.OWL_MISFIT_LOCAL_ADAPTIVE, L.OWL_MISFIT_ADAPTIVE_SPACETIME]
 
 
 def _gathers(nt, seed=3):

@@ -124,3 +124,23 @@ def test_resample_oracle_properties():
     a = R.resample_rows(2 * x - y, 1e-3, 2.5e-3, 20)
     assert np.allclose(a, 2 * R.resample_rows(x, 1e-3, 2.5e-3, 20) - R.resample_rows(y, 1e-3, 2.5e-3, 20))
     assert np.all(R.resample_rows(x, 1e-3, 1e-3, 60)[:, 50:] == 0)
+
+
+def test_local_and_spacetime_adaptive_properties():
+    """the local adaptive misfit of a trace with itself (not zero: the water
+    level spreads the matching filter) is well below that of a shifted copy;
+    the space-time misfit of a trace flanked by copies of itself equals that of
+    the trace alone"""
+    import oracle.oracle_misfit as M
+    n, dt = 256, 2e-3
+    t = np.arange(n) * dt
+    a = (np.pi * 12.0 * (t - 0.25)) ** 2
+    syn = (1 - 2 * a) * np.exp(-a)
+    a2 = (np.pi * 12.0 * (t - 0.27)) ** 2
+    obs = (1 - 2 * a2) * np.exp(-a2)
+    m0, _ = M.local_adaptive(syn, syn, dt, 0.08)
+    m1, adj1 = M.local_adaptive(obs, syn, dt, 0.08)
+    assert m0 < 0.5 * m1 and np.all(np.isfinite(adj1))
+    s1, a1 = M.adaptive_spacetime(obs[None], syn[None], 0, dt, 0.08)
+    s3, a3 = M.adaptive_spacetime(np.stack([obs, obs, obs]), np.stack([syn, syn, syn]), 1, dt, 0.08)
+    assert s3 == pytest.approx(s1, rel=1e-10) and np.allclose(a3, a1, rtol=1e-9, atol=1e-12)
