@@ -361,6 +361,8 @@ def misfit_block(s, ps, obs_dev, opts, l2_ms):
     out = {"workload": f"the gradient workload ({ps.nshots} shots); adjoint sources of its {len(gp) - 1} gathers, "
                        f"{ntr} traces of {nt} samples; adaptive: linear penalty, tlag_max 0.2 s, deconv_eps 0.1"}
     for name, kind in L.MISFIT_NAMES.items():
+        if kind == L.OWL_MISFIT_DTW_VECTOR:
+            continue  # one component per shot here: the same as dtw
         mo = MisfitOpts(misfit=kind, dt=s.desc.dt, tlag_max=0.2)
         if kind in (L.OWL_MISFIT_DTW, L.OWL_MISFIT_LOCAL_ADAPTIVE):
             # DTW's dynamic program costs O(nt m^2) double-precision steps per trace

@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define OWL_SSG_ABI_VERSION 5
+#define OWL_SSG_ABI_VERSION 6
 
 /* status codes */
 #define OWL_OK 0
@@ -96,6 +96,7 @@ extern "C" {
 #define OWL_MISFIT_DTW 5      /* compute_adjsrc_dtw :715-980, solve_gdtw :73-234 (dynamic time warping) */
 #define OWL_MISFIT_LOCAL_ADAPTIVE 6     /* compute_adjsrc_local_adaptive :545-625 (Gaussian-windowed AWI) */
 #define OWL_MISFIT_ADAPTIVE_SPACETIME 7 /* compute_adjsrc_adaptive_spacetime :630-700 (AWI over neighbouring traces) */
+#define OWL_MISFIT_DTW_VECTOR 8         /* compute_adjsrc_dtw on all components of a shot together (:1232-1236) */
 
 /* form of the DTW misfit (dtw_form) */
 #define OWL_DTW_PHASE 0     /* misfit sum q tau^2, adjoint q tau d/dt(warped obs) / dt */
@@ -119,7 +120,13 @@ extern "C" {
  * (the reference's 'l0.5'), dtw_amp_weight 0 -> 1, dtw_trc traces on each side
  * of a trace that enter its distance (0), dtw_form OWL_DTW_*. DTW takes the
  * traces at their own sampling; the shifts are not smoothed across traces.
- * lawi_sigma 0 -> 0.25 (s), adaptive_half_window 0 -> 3 (traces). */
+ * lawi_sigma 0 -> 0.25 (s), adaptive_half_window 0 -> 3 (traces).
+ * OWL_MISFIT_DTW_VECTOR: consecutive groups of ncomp gathers of equal length
+ * are one shot's components; a receiver has one shift, one quality weight and
+ * the norms over its kept components; its misfit is shared by its component
+ * rows ('phase': equally; 'amp': each row its own; 'phase+amp': each row the
+ * phase term and its own amplitude term). The gradient driver fills ncomp
+ * (0) with the medium's component count. */
 typedef struct {
     int misfit;              /* OWL_MISFIT_* */
     float dt;                /* sample interval of the traces (s) */
@@ -139,6 +146,7 @@ typedef struct {
     float dtw_amp_weight;    /* weight of the amplitude term of OWL_DTW_PHASE_AMP */
     float lawi_sigma;        /* local adaptive: standard deviation of the Gaussian time window (s) */
     int adaptive_half_window; /* space-time adaptive: neighbouring traces on each side */
+    int ncomp;               /* dtw-vector: components (gathers) per shot */
 } owl_misfit_opts;
 
 typedef struct owl_ssg owl_ssg;
@@ -389,10 +397,11 @@ int owl_adjoint_source(const owl_misfit_opts *mopts, int ngather, const int *gat
                        double *trace_misfit, double *gather_misfit, int mem_kind);
 
 /* Time shifts tau(t) of the DTW misfit, obs(t + tau) ~ syn(t), in seconds, one
- * row per trace like syn (zero on dropped traces): the reference's
+ * row per trace like syn (zero on dropped traces; dtw-vector: the receiver's
+ * shift on each of its component rows): the reference's
  * shot_<id>_time_shift_<comp>.su output (compute_adjoint_source :1238-1246).
  * Same arguments and limits as owl_adjoint_source with mopts->misfit =
- * OWL_MISFIT_DTW. DTW limits: 3 <= nt <= 16384 and 3 <= 2 tlag_max / dt + 1
+ * OWL_MISFIT_DTW or OWL_MISFIT_DTW_VECTOR. DTW limits: 3 <= nt <= 16384 and 3 <= 2 tlag_max / dt + 1
  * <= 4095. */
 int owl_dtw_time_shifts(const owl_misfit_opts *mopts, int ngather, const int *gather_ptr, int nt,
                         const float *syn, const float *obs, const float *weight, float *tau, int mem_kind);

@@ -7,7 +7,8 @@ Follows src/inverse/module_inversion_adjoint_source.f90:
   compute_adjsrc_dtw   :715-980 per-gather normalisation, GDTW time shifts,
                                 windowed-correlation quality weights, adjoint
                                 source of the 'phase', 'amp' and 'phase+amp' forms
-  compute_adjoint_source :1224-1230 ('dtw': one call per gather and component)
+  compute_adjoint_source :1224-1236 ('dtw': one call per gather and component;
+                         'dtw-vector': one call on all components of a shot)
 with the defaults of src/lib/module_parameters.f90:270-280, 559-569
 (dtw_niter 5, dtw_rinst 0.1, dtw_rcuml 1, dtw_epsabs 1e-2, dtw_epsrel 1e-3,
 dtw_loss 'l0.5', dtw_form 'phase', dtw_amp_weight 1, dtw_trc 0, no smoothing of
@@ -335,4 +336,145 @@ def adjoint_source(gather_ptr, syn, obs, weight=None, dt=1e-3, tlag_max=0.0, dis
         tm[r0:r1] = t_m
         tau[r0:r1] = ta
         gm[g] = tm[r0:r1].sum()
+    return adj, tm, gm, tau
+
+
+def dtw_vector(syn, obs, live, dd, tlag_max, form=PHASE, niter=5, rinst=0.1, rcuml=1.0, epsabs=1.0e-2,
+               epsrel=1.0e-3, power=0.5, amp_weight=1.0, trc=0):
+    """compute_adjsrc_dtw on the components of one shot together ('dtw-vector',
+    :1232-1236): syn, obs (nc, nr, n), live (nc, nr) after the discard rule.
+    A receiver is kept when any component is; traces are normalised by the
+    norm over the receiver's kept components; one shift and one quality weight
+    per receiver (the components' windowed correlations summed); the adjoint per
+    component. Returns (adj (nc, nr, n), trace misfits (nc, nr), tau (nc, nr, n))
+    with a receiver's misfit shared by its component rows: 'phase' equally,
+    'amp' each row its own, 'phase+amp' each row the phase term (times
+    1 + amp_weight) -- their sum is the reference's err_trc."""
+    syn = np.asarray(syn, dtype=f32)
+    obs = np.asarray(obs, dtype=f32)
+    nc, nr, n = syn.shape
+    live = np.asarray(live, dtype=bool)
+    dd = float(f32(dd))
+    lv = live.any(axis=0)
+    dsyn = np.zeros((nc, nr, n))
+    dobs = np.zeros((nc, nr, n))
+    for i in range(nr):
+        if not lv[i]:
+            continue
+        ns = f32(np.sqrt(sum(np.linalg.norm(syn[c, i].astype(np.float64)) ** 2 for c in range(nc) if live[c, i])))
+        no = f32(np.sqrt(sum(np.linalg.norm(obs[c, i].astype(np.float64)) ** 2 for c in range(nc) if live[c, i])))
+        for c in range(nc):
+            if live[c, i]:
+                dsyn[c, i] = (syn[c, i] / ns).astype(np.float64)
+                dobs[c, i] = (obs[c, i] / no).astype(np.float64)
+    m = lag_count(tlag_max, dd)
+    tau = np.zeros((nc, nr, n), dtype=f32)
+    for i in range(nr):
+        if not lv[i]:
+            continue
+        cols = [(c, q) for c in range(nc) for q in range(i - trc, i + trc + 1)]
+        X = np.stack([dobs[c, q] if 0 <= q < nr else np.zeros(n) for c, q in cols], axis=1)
+        Y = np.stack([dsyn[c, q] if 0 <= q < nr else np.zeros(n) for c, q in cols], axis=1)
+        ts, _ = gdtw(X, Y, m, niter, float(f32(rinst)), float(f32(rcuml)), float(f32(epsabs)), float(f32(epsrel)),
+                     float(f32(power)))
+        tau[:, i] = (ts * float(f32(dd))).astype(f32)
+    q = np.zeros((nr, n), dtype=f32)
+    if form == AMP:
+        q[:] = 1.0
+    else:
+        nw = nint(float(f32(tlag_max) / f32(dd)))
+        tg = np.arange(n, dtype=f32) * f32(dd)
+        for i in range(nr):
+            if not lv[i]:
+                continue
+            acc = np.zeros(n, dtype=f32)
+            for c in range(nc):
+                if not live[c, i]:
+                    continue
+                dw = _lin_interp_zero(tg, dobs[c, i].astype(f32), (tau[c, i] + tg).astype(f32)).astype(np.float64)
+                eta = f32(max(np.linalg.norm(dsyn[c, i]), np.linalg.norm(dw)) * float(f32(1.0e-2)))
+                if eta == 0:
+                    eta = f32(1.0e-9)
+                for j in range(n):
+                    lo, hi = max(0, j - nw), min(n - 1, j + nw)
+                    uu = dsyn[c, i, lo:hi + 1].astype(f32).astype(np.float64)
+                    vv = dw[lo:hi + 1].astype(f32).astype(np.float64)
+                    acc[j] = f32(acc[j] + f32(np.dot(uu, vv) / (np.linalg.norm(uu) * np.linalg.norm(vv) + float(eta))))
+            qi = np.abs(acc) ** f32(0.2)
+            qi = median7(qi.astype(f32))
+            qd = gauss3(qi.astype(np.float64))
+            qd = qd / np.linalg.norm(qd)
+            with np.errstate(invalid="ignore", divide="ignore"):
+                qd = (qd - qd.min()) / (qd.max() - qd.min())
+            q[i] = _normal(qd).astype(f32)
+        for i in range(nr):
+            if np.max(np.abs(q[i])) == 0:
+                q[i] = 1.0
+    adj = np.zeros((nc, nr, n))
+    tm = np.zeros((nc, nr))
+    td = np.arange(n, dtype=f32) * f32(dd)
+    for i in range(nr):
+        if not lv[i]:
+            continue
+        qi = q[i].astype(np.float64)
+        for c in range(nc):
+            ti = tau[c, i].astype(np.float64)
+            mph = float(np.sum(qi * ti * ti))
+            if not live[c, i]:
+                tm[c, i] = mph / nc if form == PHASE else (0.0 if form == AMP else mph * (1.0 + amp_weight))
+                continue
+            pos = ((tau[c, i] + td).astype(f32) / f32(dd)).astype(np.float64)
+            warped = _cubic_warp(obs[c, i].astype(np.float64), pos)
+            r = syn[c, i].astype(np.float64) - warped
+            if form == PHASE:
+                tm[c, i] = mph / nc
+                adj[c, i] = qi * ti * deriv(warped) / dd
+            elif form == AMP:
+                tm[c, i] = float(np.sum(r * r))
+                adj[c, i] = r
+            else:
+                ma = float(np.sum(r * r))
+                tm[c, i] = mph * (1.0 + amp_weight)
+                adj[c, i] = qi * ti * deriv(warped) / dd + amp_weight * mph / (ma + F32_TINY) * r
+    return adj, tm, tau
+
+
+def adjoint_source_vector(gather_ptr, syn, obs, ncomp, weight=None, dt=1e-3, tlag_max=0.0, discard_threshold=0.0,
+                          **kw):
+    """'dtw-vector' over gathers of rows: consecutive groups of ncomp gathers
+    (equal lengths) are one shot's components; the discard rule per gather,
+    then dtw_vector per shot. Returns (adj, trace misfits, gather misfits, tau)."""
+    syn = np.asarray(syn, dtype=f32)
+    obs = np.asarray(obs, dtype=f32)
+    ntr, nt = syn.shape
+    tlag = tlag_max if tlag_max > 0 else float(f32(0.1) * f32(nt - 1) * f32(dt))
+    thr = discard_threshold if discard_threshold != 0 else 1.0e-6
+    thr = max(thr, 0.0)
+    w = np.ones(ntr) if weight is None else np.asarray(weight, dtype=np.float64)
+    ng = len(gather_ptr) - 1
+    live = np.zeros(ntr, dtype=bool)
+    for g in range(ng):
+        r0, r1 = gather_ptr[g], gather_ptr[g + 1]
+        if r1 <= r0:
+            continue
+        no = np.linalg.norm(obs[r0:r1].astype(np.float64), axis=1)
+        ns = np.linalg.norm(syn[r0:r1].astype(np.float64), axis=1)
+        mo, ms = no.max(), ns.max()
+        for r in range(r0, r1):
+            i = r - r0
+            live[r] = not (w[r] == 0 or no[i] < thr * mo or ns[i] < thr * ms or no[i] * ns[i] == 0)
+    adj = np.zeros((ntr, nt))
+    tm = np.zeros(ntr)
+    tau = np.zeros((ntr, nt), dtype=f32)
+    for g0 in range(0, ng, ncomp):
+        rows = [list(range(gather_ptr[g0 + c], gather_ptr[g0 + c + 1])) for c in range(ncomp)]
+        S = np.stack([np.where(live[rs][:, None], syn[rs], 0) for rs in rows]).astype(f32)
+        O = np.stack([np.where(live[rs][:, None], obs[rs], 0) for rs in rows]).astype(f32)
+        Lv = np.stack([live[rs] for rs in rows])
+        a, t_m, ta = dtw_vector(S, O, Lv, dt, tlag, **kw)
+        for c, rs in enumerate(rows):
+            adj[rs] = a[c]
+            tm[rs] = t_m[c]
+            tau[rs] = ta[c]
+    gm = np.array([tm[gather_ptr[g]:gather_ptr[g + 1]].sum() for g in range(ng)])
     return adj, tm, gm, tau

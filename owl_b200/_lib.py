@@ -54,6 +54,7 @@ OWL_MISFIT_ADAPTIVE = 4
 OWL_MISFIT_DTW = 5
 OWL_MISFIT_LOCAL_ADAPTIVE = 6
 OWL_MISFIT_ADAPTIVE_SPACETIME = 7
+OWL_MISFIT_DTW_VECTOR = 8
 
 OWL_DTW_PHASE = 0
 OWL_DTW_AMP = 1
@@ -67,7 +68,8 @@ OWL_PENALTY_EXP = 3
 #: misfit_type names of the reference's parameter file
 MISFIT_NAMES = {"waveform": OWL_MISFIT_WAVEFORM, "corr": OWL_MISFIT_CORR, "envelope": OWL_MISFIT_ENVELOPE,
                 "phase": OWL_MISFIT_PHASE, "adaptive": OWL_MISFIT_ADAPTIVE, "dtw": OWL_MISFIT_DTW,
-                "local-adaptive": OWL_MISFIT_LOCAL_ADAPTIVE, "adaptive-spacetime": OWL_MISFIT_ADAPTIVE_SPACETIME}
+                "local-adaptive": OWL_MISFIT_LOCAL_ADAPTIVE, "adaptive-spacetime": OWL_MISFIT_ADAPTIVE_SPACETIME,
+                "dtw-vector": OWL_MISFIT_DTW_VECTOR}
 #: dtw_form names of the reference's parameter file
 DTW_FORM_NAMES = {"phase": OWL_DTW_PHASE, "amp": OWL_DTW_AMP, "phase+amp": OWL_DTW_PHASE_AMP}
 PENALTY_NAMES = {"linear": OWL_PENALTY_LINEAR, "power": OWL_PENALTY_POWER, "gaussian": OWL_PENALTY_GAUSSIAN,
@@ -170,6 +172,7 @@ class OwlMisfitOpts(C.Structure):
         ("dtw_amp_weight", C.c_float),
         ("lawi_sigma", C.c_float),
         ("adaptive_half_window", C.c_int),
+        ("ncomp", C.c_int),
     ]
 
 

@@ -681,7 +681,7 @@ static std::vector<float> awi_penalty(const owl_misfit_opts& o, float tlag, int 
 void AdjointSource::run(const owl_misfit_opts& o, int ngather, const int* h_gather_ptr, int nt, const float* syn,
                         const float* obs, const unsigned char* weight_live, float* adj, double* tm, double* gm,
                         cudaStream_t s, float* tau) {
-    OWL_CHECK(o.misfit >= OWL_MISFIT_WAVEFORM && o.misfit <= OWL_MISFIT_ADAPTIVE_SPACETIME, OWL_ERR_INVALID,
+    OWL_CHECK(o.misfit >= OWL_MISFIT_WAVEFORM && o.misfit <= OWL_MISFIT_DTW_VECTOR, OWL_ERR_INVALID,
               "bad misfit type");
     OWL_CHECK(nt >= 1 && ngather >= 0 && (ngather == 0 || h_gather_ptr), OWL_ERR_INVALID, "bad trace layout");
     OWL_CHECK(ngather == 0 || h_gather_ptr[0] == 0, OWL_ERR_INVALID, "gather_ptr[0] must be 0");
@@ -702,7 +702,15 @@ void AdjointSource::run(const owl_misfit_opts& o, int ngather, const int* h_gath
     OWL_LAUNCH_CHECK();
     launches += 2;
 
-    if (o.misfit == OWL_MISFIT_DTW) {
+    if (o.misfit == OWL_MISFIT_DTW || o.misfit == OWL_MISFIT_DTW_VECTOR) {
+        if (o.misfit == OWL_MISFIT_DTW_VECTOR) {
+            const int vc = std::max(1, o.ncomp);
+            OWL_CHECK(ngather % vc == 0, OWL_ERR_INVALID, "dtw-vector: the gathers must come in groups of ncomp");
+            for (int g = 0; g < ngather; g += vc)
+                for (int c = 1; c < vc; ++c)
+                    OWL_CHECK(h_gather_ptr[g + c + 1] - h_gather_ptr[g + c] == h_gather_ptr[g + 1] - h_gather_ptr[g],
+                              OWL_ERR_INVALID, "dtw-vector: the component gathers of a shot must hold equal trace counts");
+        }
         DevBuf<double> tmp;
         if (!tm && gm) {
             tmp.reserve(ntr);

@@ -22,7 +22,7 @@ struct AdjointSource {
     DevBuf<double> nrm, gmax;
     DevBuf<float> pen, ramp, scratch;
     DevBuf<float2> cscratch;
-    DevBuf<double> dsn, dob, band;  // DTW: normalised traces, per-CTA search bands
+    DevBuf<double> dsn, dob, band, vnrm;  // DTW: normalised traces, per-CTA search bands, receiver norms
     DevBuf<float> qw, warp;         // DTW: quality weights, warped traces
     DevBuf<unsigned short> path;    // DTW: per-CTA back-pointers of the dynamic program
     long long launches = 0;

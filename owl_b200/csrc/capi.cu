@@ -184,7 +184,7 @@ int owl_ssg_gradient_misfit(owl_ssg* h, int nshots, const owl_shot* shots, const
         OWL_CHECK(nshots >= 0 && (nshots == 0 || shots), OWL_ERR_INVALID, "bad shots");
         OWL_CHECK(obs || nshots == 0, OWL_ERR_INVALID, "null data buffer");
         OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");
-        OWL_CHECK(mopts->misfit >= OWL_MISFIT_WAVEFORM && mopts->misfit <= OWL_MISFIT_ADAPTIVE_SPACETIME, OWL_ERR_INVALID,
+        OWL_CHECK(mopts->misfit >= OWL_MISFIT_WAVEFORM && mopts->misfit <= OWL_MISFIT_DTW_VECTOR, OWL_ERR_INVALID,
                   "bad misfit type");
         h->eng->mopts = *mopts;
         if (h->eng->mopts.dt <= 0.f) h->eng->mopts.dt = h->eng->desc.dt;
@@ -420,7 +420,7 @@ int owl_adjoint_source(const owl_misfit_opts* mopts, int ngather, const int* gat
 
 int owl_dtw_time_shifts(const owl_misfit_opts* mopts, int ngather, const int* gather_ptr, int nt, const float* syn,
                         const float* obs, const float* weight, float* tau, int mem_kind) {
-    if (!mopts || mopts->misfit != OWL_MISFIT_DTW || !tau)
+    if (!mopts || (mopts->misfit != OWL_MISFIT_DTW && mopts->misfit != OWL_MISFIT_DTW_VECTOR) || !tau)
         return guarded([&] { OWL_CHECK(false, OWL_ERR_INVALID, "owl_dtw_time_shifts needs the DTW misfit and a tau buffer"); });
     return adjoint_source_impl(mopts, ngather, gather_ptr, nt, syn, obs, weight, nullptr, nullptr, nullptr, tau,
                                mem_kind);

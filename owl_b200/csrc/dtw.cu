@@ -33,6 +33,8 @@ __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a,
 
 struct DtwArgs {
     int n, m, ntr, ngather, niter, trc, form;
+    int vc;               // components per receiver: 1, or the ncomp consecutive gathers of a shot (dtw-vector)
+    const double* vnrm;   // per row: obs and syn norms over the receiver's kept components
     const int* gptr;
     const unsigned char* live;
     const float* syn;
@@ -59,6 +61,33 @@ __device__ int gather_of(const DtwArgs& a, int r) {
         if (a.gptr[mid] <= r) lo = mid; else hi = mid - 1;
     }
     return lo;
+}
+
+// row of component c of the receiver of row r (dtw-vector; c = the row's own
+// component when vc = 1), and the gather bounds of that component
+__device__ __forceinline__ int comp_row(const DtwArgs& a, int g, int r, int c, int& lo, int& hi) {
+    const int sg = g / a.vc, gc = sg * a.vc + c;
+    lo = a.gptr[gc];
+    hi = a.gptr[gc + 1];
+    return lo + (r - a.gptr[g]);
+}
+
+// obs / syn norms of each row's receiver over its kept components
+__global__ void k_dtw_vnorm(DtwArgs a, double* vn) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.ntr) return;
+    const int g = gather_of(a, r);
+    double so = 0.0, ss = 0.0;
+    for (int c = 0; c < a.vc; ++c) {
+        int lo, hi;
+        const int rc = comp_row(a, g, r, c, lo, hi);
+        if (rc < hi && a.live[rc]) {
+            so += a.nrm[2 * rc] * a.nrm[2 * rc];
+            ss += a.nrm[2 * rc + 1] * a.nrm[2 * rc + 1];
+        }
+    }
+    vn[2 * r] = sqrt(so);
+    vn[2 * r + 1] = sqrt(ss);
 }
 
 __device__ double block_sum_d(double v, double* red) {
@@ -93,7 +122,8 @@ __global__ void k_dtw_normalise(DtwArgs a) {
     for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < tot; o += (size_t)gridDim.x * blockDim.x) {
         const int r = (int)(o / a.n);
         const bool lv = a.live[r] != 0;
-        const float no = (float)a.nrm[2 * r], ns = (float)a.nrm[2 * r + 1];
+        const double* nr = a.vc > 1 ? a.vnrm : a.nrm;
+        const float no = (float)nr[2 * r], ns = (float)nr[2 * r + 1];
         a.dob[o] = lv ? (double)(a.obs[o] / no) : 0.0;
         a.dsn[o] = lv ? (double)(a.syn[o] / ns) : 0.0;
     }
@@ -137,13 +167,32 @@ __global__ void __launch_bounds__(256) k_dtw_solve(DtwArgs a) {
     const double dt = 1.0 / ((double)n - 1.0);
     for (int j = threadIdx.x; j < m; j += blockDim.x) lin[j] = (double)j / (double)(m - 1);
     for (int r = blockIdx.x; r < a.ntr; r += gridDim.x) {
-        float* tau_out = a.tau + (size_t)r * n;
-        if (!a.live[r]) {
-            for (int i = threadIdx.x; i < n; i += blockDim.x) tau_out[i] = 0.f;
+        const int g = gather_of(a, r);
+        if (g % a.vc != 0) continue;  // dtw-vector: the receiver is solved from its first component's row
+        bool lv = false;
+        for (int c = 0; c < a.vc; ++c) {
+            int lo, hi;
+            const int rc = comp_row(a, g, r, c, lo, hi);
+            lv = lv || (rc < hi && a.live[rc]);
+        }
+        if (!lv) {
+            for (int c = 0; c < a.vc; ++c) {
+                int lo, hi;
+                const int rc = comp_row(a, g, r, c, lo, hi);
+                if (rc < hi)
+                    for (int i = threadIdx.x; i < n; i += blockDim.x) a.tau[(size_t)rc * n + i] = 0.f;
+            }
             continue;
         }
-        const int g = gather_of(a, r);
-        const int c0 = r - a.trc, nc = 2 * a.trc + 1, g0 = a.gptr[g], g1 = a.gptr[g + 1];
+        // distance columns: components outer, the trc neighbours on each side inner
+        // (the reference's reshape of (nn, 2 trc + 1, nc))
+        const int nc = (2 * a.trc + 1) * a.vc;
+        auto col_row = [&](int c, int& rc) {
+            const int comp = c / (2 * a.trc + 1), off = c - comp * (2 * a.trc + 1) - a.trc;
+            int lo, hi;
+            rc = comp_row(a, g, r, comp, lo, hi) + off;
+            return rc >= lo && rc < hi;
+        };
         double cost_prev = 1.1754943508222875e-38;  // single-precision tiny
         __syncthreads();
         for (int it = 0; it < a.niter; ++it) {
@@ -169,8 +218,8 @@ __global__ void __launch_bounds__(256) k_dtw_solve(DtwArgs a) {
                     const double tg = dadd(L[0], dmul(dsub(U[0], L[0]), lin[k]));
                     double dist = 0.0;
                     for (int c = 0; c < nc; ++c) {
-                        const int rc = c0 + c;
-                        const bool in = rc >= g0 && rc < g1;
+                        int rc;
+                        const bool in = col_row(c, rc);
                         const double xv = in ? interp_clamped(a.dob + (size_t)rc * n, n, tg) : 0.0;
                         const double yv = in ? a.dsn[(size_t)rc * n] : 0.0;
                         dist = dadd(dist, powabs(dsub(xv, yv), a.power));
@@ -191,8 +240,8 @@ __global__ void __launch_bounds__(256) k_dtw_solve(DtwArgs a) {
                     const double tgk = dadd(ln, dmul(dun, lin[k]));
                     double dist = 0.0;
                     for (int c = 0; c < nc; ++c) {
-                        const int rc = c0 + c;
-                        const bool in = rc >= g0 && rc < g1;
+                        int rc;
+                        const bool in = col_row(c, rc);
                         const double xv = in ? interp_clamped(a.dob + (size_t)rc * n, n, tgk) : 0.0;
                         const double yv = in ? a.dsn[(size_t)rc * n + i + 1] : 0.0;
                         dist = dadd(dist, powabs(dsub(xv, yv), a.power));
@@ -247,10 +296,15 @@ __global__ void __launch_bounds__(256) k_dtw_solve(DtwArgs a) {
             cost_prev = cost;
             __syncthreads();
         }
-        // tau = (tau - linspace(0, 1, n)) (n - 1), in seconds (:232, :810)
+        // tau = (tau - linspace(0, 1, n)) (n - 1), in seconds (:232, :810), on every component's row
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             const double lin32 = (double)((float)i / (float)(n - 1));
-            tau_out[i] = (float)dmul(dmul(dsub(T[i], lin32), (double)(n - 1)), (double)a.dd);
+            const float v = (float)dmul(dmul(dsub(T[i], lin32), (double)(n - 1)), (double)a.dd);
+            for (int c = 0; c < a.vc; ++c) {
+                int lo, hi;
+                const int rc = comp_row(a, g, r, c, lo, hi);
+                if (rc < hi) a.tau[(size_t)rc * n + i] = v;
+            }
         }
         __syncthreads();
     }
@@ -268,46 +322,73 @@ __device__ float interp_zero_f(const double* x, int n, float dd, float q) {
     return (float)x[i0] * (1.f - w) + (float)x[i0 + 1] * w;
 }
 
-// quality weights (:838-905), one CTA per trace
+// quality weights (:838-905), one CTA per trace (dtw-vector: per receiver, the
+// components' windowed correlations summed before |q|^0.2, q on every component's row)
 __global__ void __launch_bounds__(256) k_dtw_quality(DtwArgs a) {
     __shared__ double red[32];
     const int r = blockIdx.x, n = a.n;
+    const int g = gather_of(a, r);
+    if (g % a.vc != 0) return;
+    bool lv = false;
+    for (int c = 0; c < a.vc; ++c) {
+        int lo, hi;
+        const int rc = comp_row(a, g, r, c, lo, hi);
+        lv = lv || (rc < hi && a.live[rc]);
+    }
     float* q = a.q + (size_t)r * n;
-    if (!a.live[r] || a.form == 1) {
+    float* dw = a.dw + (size_t)r * n;
+    auto spread = [&]() {  // copy q to the other components' rows
+        __syncthreads();
+        for (int c = 1; c < a.vc; ++c) {
+            int lo, hi;
+            const int rc = comp_row(a, g, r, c, lo, hi);
+            if (rc < hi)
+                for (int i = threadIdx.x; i < n; i += blockDim.x) a.q[(size_t)rc * n + i] = q[i];
+        }
+    };
+    if (!lv || a.form == 1) {
         for (int i = threadIdx.x; i < n; i += blockDim.x) q[i] = 1.f;
+        spread();
         return;
     }
-    const double* ds = a.dsn + (size_t)r * n;
-    const double* dob = a.dob + (size_t)r * n;
-    const float* tau = a.tau + (size_t)r * n;
-    float* dw = a.dw + (size_t)r * n;
-    double s1 = 0.0, s2 = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const float tg = (float)i * a.dd;
-        const float v = interp_zero_f(dob, n, a.dd, tau[i] + tg);
-        dw[i] = v;
-        s1 += ds[i] * ds[i];
-        s2 += (double)v * (double)v;
-    }
-    s1 = block_sum_d(s1, red);
-    s2 = block_sum_d(s2, red);
-    float eta = (float)(fmax(sqrt(s1), sqrt(s2)) * (double)1.0e-2f);
-    if (eta == 0.f) eta = 1.0e-9f;
     const int nw = (int)floor(fabs((double)(a.tlag / a.dd)) + 0.5);  // nint(tlag_max / dd)
-    __syncthreads();
-    // windowed normalised correlation, then |q|^0.2
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        const int lo = max(0, j - nw), hi = min(n - 1, j + nw);
-        double uv = 0.0, uu = 0.0, vv = 0.0;
-        for (int i = lo; i <= hi; ++i) {
-            const double u = (double)(float)ds[i], v = (double)dw[i];
-            uv += u * v;
-            uu += u * u;
-            vv += v * v;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) q[i] = 0.f;
+    for (int c = 0; c < a.vc; ++c) {
+        int lo, hi;
+        const int rc = comp_row(a, g, r, c, lo, hi);
+        if (rc >= hi || !a.live[rc]) continue;  // a dropped component is a zero trace: it adds nothing
+        const double* ds = a.dsn + (size_t)rc * n;
+        const double* dob = a.dob + (size_t)rc * n;
+        const float* tau = a.tau + (size_t)rc * n;
+        float* dwc = a.dw + (size_t)rc * n;
+        double s1 = 0.0, s2 = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float tg = (float)i * a.dd;
+            const float v = interp_zero_f(dob, n, a.dd, tau[i] + tg);
+            dwc[i] = v;
+            s1 += ds[i] * ds[i];
+            s2 += (double)v * (double)v;
         }
-        const float c = (float)(uv / (sqrt(uu) * sqrt(vv) + (double)eta));
-        q[j] = powf(fabsf(c), 0.2f);
+        s1 = block_sum_d(s1, red);
+        s2 = block_sum_d(s2, red);
+        float eta = (float)(fmax(sqrt(s1), sqrt(s2)) * (double)1.0e-2f);
+        if (eta == 0.f) eta = 1.0e-9f;
+        __syncthreads();
+        // windowed normalised correlation, summed over the components
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const int l0 = max(0, j - nw), l1 = min(n - 1, j + nw);
+            double uv = 0.0, uu = 0.0, vv = 0.0;
+            for (int i = l0; i <= l1; ++i) {
+                const double u = (double)(float)ds[i], v = (double)dwc[i];
+                uv += u * v;
+                uu += u * u;
+                vv += v * v;
+            }
+            q[j] += (float)(uv / (sqrt(uu) * sqrt(vv) + (double)eta));
+        }
+        __syncthreads();
     }
+    for (int j = threadIdx.x; j < n; j += blockDim.x) q[j] = powf(fabsf(q[j]), 0.2f);
     __syncthreads();
     // 7-sample median (truncated at the ends) into dw
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
@@ -358,6 +439,7 @@ __global__ void __launch_bounds__(256) k_dtw_quality(DtwArgs a) {
     qmax = block_minmax_d(qmax, red, true);
     if (qmax == 0.0)
         for (int j = threadIdx.x; j < n; j += blockDim.x) q[j] = 1.f;
+    spread();
 }
 
 __device__ __forceinline__ double keys_at(const float* x, int n, double p) {
@@ -375,10 +457,27 @@ __global__ void __launch_bounds__(256) k_dtw_adjoint(DtwArgs a) {
     __shared__ double red[32];
     const int r = blockIdx.x, n = a.n;
     float* adj = a.adj ? a.adj + (size_t)r * n : nullptr;
+    const int g = gather_of(a, r);
+    bool lv = false;
+    for (int c = 0; c < a.vc; ++c) {
+        int lo, hi;
+        const int rc = comp_row(a, g, r, c, lo, hi);
+        lv = lv || (rc < hi && a.live[rc]);
+    }
     if (!a.live[r]) {
+        // a dropped trace (dtw-vector: a dropped component of a kept receiver is a
+        // zero trace: no adjoint, its share of the receiver's phase misfit)
         if (adj)
             for (int i = threadIdx.x; i < n; i += blockDim.x) adj[i] = 0.f;
-        if (threadIdx.x == 0 && a.tm) a.tm[r] = 0.0;
+        double mph = 0.0;
+        if (lv && a.form != 1) {
+            const float* tau = a.tau + (size_t)r * n;
+            const float* q = a.q + (size_t)r * n;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) mph += (double)q[i] * (double)tau[i] * (double)tau[i];
+            mph = block_sum_d(mph, red);
+        }
+        if (threadIdx.x == 0 && a.tm)
+            a.tm[r] = !lv ? 0.0 : a.form == 0 ? mph / a.vc : a.form == 1 ? 0.0 : mph * (1.0 + (double)a.amp_weight);
         return;
     }
     const float* obs = a.obs + (size_t)r * n;
@@ -398,8 +497,9 @@ __global__ void __launch_bounds__(256) k_dtw_adjoint(DtwArgs a) {
     }
     mph = block_sum_d(mph, red);
     ma = block_sum_d(ma, red);
+    // dtw-vector: the receiver's phase misfit is shared by its component rows
     if (threadIdx.x == 0 && a.tm)
-        a.tm[r] = a.form == 0 ? mph : a.form == 1 ? ma : mph * (1.0 + (double)a.amp_weight);
+        a.tm[r] = a.form == 0 ? mph / a.vc : a.form == 1 ? ma : mph * (1.0 + (double)a.amp_weight);
     if (!adj) return;
     const double dd = a.dd;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -449,6 +549,7 @@ void AdjointSource::run_dtw(const owl_misfit_opts& o, int ngather, int nt, int n
     a.syn = syn;
     a.obs = obs;
     a.nrm = nrm.p;
+    a.vc = o.misfit == OWL_MISFIT_DTW_VECTOR ? std::max(1, o.ncomp) : 1;
     auto dflt = [](float v, float d) { return v == 0.f ? (double)d : (v < 0.f ? 0.0 : (double)v); };
     a.rinst = dflt(o.dtw_rinst, 0.1f);
     a.rcuml = dflt(o.dtw_rcuml, 1.0f);
@@ -486,6 +587,12 @@ void AdjointSource::run_dtw(const owl_misfit_opts& o, int ngather, int nt, int n
     band.reserve((size_t)grid * 3 * nt);
     a.path = path.p;
     a.band = band.p;
+    if (a.vc > 1) {
+        vnrm.reserve(2 * (size_t)ntr);
+        k_dtw_vnorm<<<(ntr + 127) / 128, 128, 0, s>>>(a, vnrm.p);
+        a.vnrm = vnrm.p;
+        launches++;
+    }
     k_dtw_normalise<<<(int)std::min<size_t>((nn + 255) / 256, (size_t)nsm * 32), 256, 0, s>>>(a);
     const size_t smem = (size_t)3 * m * sizeof(double);
     OWL_CUDA(cudaFuncSetAttribute(k_dtw_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -739,6 +739,7 @@ void SsgBase::data_adjoint_source(const float* data, int adj_kind, int mem, int 
     } else if (adj_kind == ADJ_MISFIT) {
         owl_misfit_opts mo = mopts;
         mo.dt = data_dt;
+        if (mo.ncomp <= 0) mo.ncomp = ncomp;  // dtw-vector: the components of a shot are its ncomp gathers
         trace_d.reserve(std::max(rtot, 1));
         adjsrc.launches = 0;
         adjsrc.run(mo, (int)h_gather_ptr.size() - 1, h_gather_ptr.data(), tn, dat_a.p, seis_tmp.p, live.p, dat_b.p,
@@ -820,7 +821,9 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
                 trace_d.reserve(rtot);
                 launch_transpose_rec_to_seis(rec.p, syn_t.p, nt, rtot, stream);
                 adjsrc.launches = 0;
-                adjsrc.run(mopts, (int)h_gather_ptr.size() - 1, h_gather_ptr.data(), nt, syn_t.p, seis_tmp.p,
+                owl_misfit_opts mo = mopts;
+                if (mo.ncomp <= 0) mo.ncomp = ncomp;  // dtw-vector: the components of a shot are its ncomp gathers
+                adjsrc.run(mo, (int)h_gather_ptr.size() - 1, h_gather_ptr.data(), nt, syn_t.p, seis_tmp.p,
                            live.p, adj_t.p, trace_d.p, nullptr, stream);
                 launch_shot_misfit(trace_d.p, rec_shot_ptr.p, S, misfit_d.p, stream);
                 launch_transpose_seis_to_rec(adj_t.p, res.p, nt, rtot, stream);

@@ -11,6 +11,10 @@ restatement (oracle/oracle_dtw.py).
 * the gradient of the DTW misfit through owl_ssg_gradient_misfit equals the
   FP64 exact-adjoint oracle gradient driven by the oracle's DTW adjoint source
   of the same synthetics (2e-4);
+* dtw-vector (OWL_MISFIT_DTW_VECTOR): two shots of two components, a dropped
+  component of a kept receiver and a dropped receiver: shifts to 1e-6 s, one
+  per receiver on both component rows, adjoints and misfits 1e-4; gather
+  layouts that are not groups of equal component gathers are errors;
 * the documented size limits are errors.
 """
 import numpy as np
@@ -93,3 +97,56 @@ def test_dtw_limits():
         adjoint_source(_mo(), gp, long, long, w)
     with pytest.raises(L.OwlError):  # time shifts of another misfit
         dtw_time_shifts(MisfitOpts(misfit=L.OWL_MISFIT_WAVEFORM, dt=DT), gp, syn, obs, w)
+
+
+def _vector_gathers(nt=300, seed=7):
+    """two shots x two components, four receivers each: component c of
+    receiver i shifted by (2 + i) samples; shot 0's component 1 of receiver 2
+    has weight 0 (a dropped component of a kept receiver) and shot 1's
+    receiver 3 has weight 0 on both components (a dropped receiver)"""
+    rng = np.random.default_rng(seed)
+    t = np.arange(nt)
+    syn, obs = [], []
+    for s in range(2):
+        for c in range(2):
+            for i in range(4):
+                ctr = nt * (0.3 + 0.08 * i + 0.05 * s)
+                f = 0.09 + 0.01 * c
+                sh = 2.0 + i
+                pol = 1.0 if c == 0 else -0.6
+                obs.append(pol * np.exp(-((t - ctr) / (0.04 * nt)) ** 2) * np.cos(f * (t - ctr))
+                           + 0.02 * rng.standard_normal(nt))
+                syn.append(0.9 * pol * np.exp(-((t - ctr - sh) / (0.04 * nt)) ** 2) * np.cos(f * (t - ctr - sh))
+                           + 0.02 * rng.standard_normal(nt))
+    w = np.ones(16, dtype=np.float32)
+    w[4 + 2] = 0.0          # shot 0, component 1, receiver 2
+    w[8 + 3] = w[12 + 3] = 0.0  # shot 1, receiver 3, both components
+    return [0, 4, 8, 12, 16], np.array(syn, dtype=np.float32), np.array(obs, dtype=np.float32), w
+
+
+@pytest.mark.parametrize("form", [L.OWL_DTW_PHASE, L.OWL_DTW_AMP, L.OWL_DTW_PHASE_AMP])
+def test_dtw_vector_matches_oracle(form):
+    gp, syn, obs, w = _vector_gathers()
+    kw = dict(form=form, amp_weight=0.5 if form == L.OWL_DTW_PHASE_AMP else 1.0)
+    ref_adj, ref_tm, ref_gm, ref_tau = D.adjoint_source_vector(gp, syn, obs, 2, w, dt=DT, tlag_max=TLAG, **kw)
+    mo = MisfitOpts(misfit=L.OWL_MISFIT_DTW_VECTOR, dt=DT, tlag_max=TLAG, dtw_form=form, ncomp=2,
+                    dtw_amp_weight=kw["amp_weight"])
+    tau = dtw_time_shifts(mo, gp, syn, obs, w)
+    assert np.max(np.abs(tau - ref_tau)) <= 1e-6, np.max(np.abs(tau - ref_tau))
+    # one shift per receiver, on both component rows; none for the dropped receiver
+    assert np.array_equal(tau[0:4], tau[4:8]) and np.array_equal(tau[8:12], tau[12:16])
+    assert np.all(tau[[11, 15]] == 0) and np.any(tau[6] != 0)
+    adj, tm, gm = adjoint_source(mo, gp, syn, obs, w)
+    assert np.all(adj[[6, 11, 15]] == 0)
+    assert rel(adj, ref_adj) < 1e-4, rel(adj, ref_adj)
+    assert rel(tm, ref_tm) < 1e-4, (tm, ref_tm)
+    assert np.allclose(gm, ref_gm, rtol=1e-4)
+
+
+def test_dtw_vector_layout_checks():
+    gp, syn, obs, w = _vector_gathers()
+    with pytest.raises(L.OwlError):  # 4 gathers are not groups of 3
+        adjoint_source(MisfitOpts(misfit=L.OWL_MISFIT_DTW_VECTOR, dt=DT, tlag_max=TLAG, ncomp=3), gp, syn, obs, w)
+    with pytest.raises(L.OwlError):  # component gathers of unequal length
+        adjoint_source(MisfitOpts(misfit=L.OWL_MISFIT_DTW_VECTOR, dt=DT, tlag_max=TLAG, ncomp=2),
+                       [0, 4, 7, 12, 16], syn, obs, w)
