@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define OWL_SSG_ABI_VERSION 6
+#define OWL_SSG_ABI_VERSION 7
 
 /* status codes */
 #define OWL_OK 0
@@ -147,6 +147,9 @@ typedef struct {
     float lawi_sigma;        /* local adaptive: standard deviation of the Gaussian time window (s) */
     int adaptive_half_window; /* space-time adaptive: neighbouring traces on each side */
     int ncomp;               /* dtw-vector: components (gathers) per shot */
+    int adj_nt;              /* samples the traces are resampled to (cubic) before the misfit, the adjoint
+                                resampled back; 0: owl_adjoint_source none, the gradient driver the time
+                                axis' nt, as the reference (DTW: none; other values rejected) */
 } owl_misfit_opts;
 
 typedef struct owl_ssg owl_ssg;

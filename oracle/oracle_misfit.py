@@ -267,13 +267,38 @@ def trace_misfit(kind, obs, syn, dt=1e-3, tlag_max=0.1, penalty_method=LINEAR, p
 
 def adjoint_source(kind, gather_ptr, syn, obs, weight=None, dt=1e-3, tlag_max=0.0, penalty_method=LINEAR,
                    penalty_power=0.0, deconv_eps=0.0, discard_threshold=0.0, lawi_sigma=0.0,
-                   adaptive_half_window=0):
+                   adaptive_half_window=0, adj_nt=0):
     """compute_adjoint_source (:985-1277) over gathers of rows: returns
     (adj, trace misfits, gather misfits). Zero-valued options take the
-    reference's defaults (module_parameters.f90:550-570)."""
+    reference's defaults (module_parameters.f90:550-570). adj_nt (:1082-1152):
+    the traces kept by the discard rule are resampled to adj_nt samples over
+    the same span (cubic, FLIT interp_to restated as the Keys cubic convolution
+    of oracle_resample) before the misfit, the adjoint resampled back."""
     syn = np.asarray(syn, dtype=np.float64)
     obs = np.asarray(obs, dtype=np.float64)
     ntr, nt = syn.shape
+    if adj_nt > 0 and adj_nt != nt:
+        from oracle.oracle_resample import resample_rows
+        f32 = np.float32
+        dd = float(f32(f32(nt - 1) * f32(dt)) / f32(adj_nt - 1))
+        thr = discard_threshold if discard_threshold != 0 else 1.0e-6
+        thr = max(thr, 0.0)
+        w0 = np.ones(ntr) if weight is None else np.asarray(weight, dtype=np.float64)
+        keep = np.zeros(ntr)
+        for g in range(len(gather_ptr) - 1):
+            r0, r1 = gather_ptr[g], gather_ptr[g + 1]
+            if r1 <= r0:
+                continue
+            no = np.linalg.norm(obs[r0:r1], axis=1)
+            ns = np.linalg.norm(syn[r0:r1], axis=1)
+            for r in range(r0, r1):
+                i = r - r0
+                keep[r] = not (w0[r] == 0 or no[i] < thr * no.max() or ns[i] < thr * ns.max() or no[i] * ns[i] == 0)
+        ts = resample_rows(syn, float(f32(dt)), dd, adj_nt)
+        to = resample_rows(obs, float(f32(dt)), dd, adj_nt)
+        a, tm, gm = adjoint_source(kind, gather_ptr, ts, to, keep, dd, tlag_max, penalty_method, penalty_power,
+                                   deconv_eps, -1.0, lawi_sigma, adaptive_half_window)
+        return resample_rows(a, dd, float(f32(dt)), nt), tm, gm
     tlag = tlag_max if tlag_max > 0 else float(np.float32(0.1) * np.float32(nt - 1) * np.float32(dt))
     pp = penalty_power if penalty_power != 0 else 1.0
     eps = deconv_eps if deconv_eps > 0 else 0.1

@@ -173,6 +173,7 @@ class OwlMisfitOpts(C.Structure):
         ("lawi_sigma", C.c_float),
         ("adaptive_half_window", C.c_int),
         ("ncomp", C.c_int),
+        ("adj_nt", C.c_int),
     ]
 
 

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "adjsrc.cuh"
+#include "engine.cuh"  // launch_resample_rows
 
 namespace owl {
 
@@ -702,6 +703,33 @@ void AdjointSource::run(const owl_misfit_opts& o, int ngather, const int* h_gath
     OWL_LAUNCH_CHECK();
     launches += 2;
 
+    if (o.adj_nt > 0 && o.adj_nt != nt) {
+        // adj_nt (:1082-1089, :1111-1152): the misfit on the traces resampled to
+        // adj_nt samples over the same span (cubic), the adjoint resampled back;
+        // the trace selection is that of the traces as given
+        OWL_CHECK(o.misfit != OWL_MISFIT_DTW && o.misfit != OWL_MISFIT_DTW_VECTOR, OWL_ERR_UNSUPPORTED,
+                  "adj_nt resampling of the DTW misfits is not built");
+        OWL_CHECK(o.dt > 0.f && o.adj_nt >= 2, OWL_ERR_INVALID, "adj_nt needs dt and at least 2 samples");
+        const int nn = o.adj_nt;
+        const float dd = ((float)(nt - 1) * o.dt) / (float)(nn - 1);
+        DevBuf<float> rs, ro, ra;
+        DevBuf<unsigned char> keep;
+        rs.reserve((size_t)ntr * nn);
+        ro.reserve((size_t)ntr * nn);
+        keep.reserve(ntr);
+        OWL_CUDA(cudaMemcpyAsync(keep.p, live.p, ntr, cudaMemcpyDeviceToDevice, s));
+        launch_resample_rows(syn, nt, o.dt, 0.0, rs.p, nn, dd, 0.0, ntr, s);
+        launch_resample_rows(obs, nt, o.dt, 0.0, ro.p, nn, dd, 0.0, ntr, s);
+        if (adj) ra.reserve((size_t)ntr * nn);
+        owl_misfit_opts o2 = o;
+        o2.adj_nt = 0;
+        o2.dt = dd;
+        o2.discard_threshold = -1.f;  // the selection made above; zero traces stay zero
+        run(o2, ngather, h_gather_ptr, nn, rs.p, ro.p, keep.p, adj ? ra.p : nullptr, tm, gm, s);
+        if (adj) launch_resample_rows(ra.p, nn, dd, 0.0, adj, nt, o.dt, 0.0, ntr, s);
+        OWL_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
     if (o.misfit == OWL_MISFIT_DTW || o.misfit == OWL_MISFIT_DTW_VECTOR) {
         if (o.misfit == OWL_MISFIT_DTW_VECTOR) {
             const int vc = std::max(1, o.ncomp);

@@ -84,10 +84,11 @@ class MisfitOpts:
     lawi_sigma: float = 0.0
     adaptive_half_window: int = 0
     ncomp: int = 0
+    adj_nt: int = 0
 
     def c(self) -> L.OwlMisfitOpts:
         o = L.OwlMisfitOpts()
-        for k in ("misfit", "penalty", "dtw_form", "dtw_niter", "dtw_trc", "adaptive_half_window", "ncomp"):
+        for k in ("misfit", "penalty", "dtw_form", "dtw_niter", "dtw_trc", "adaptive_half_window", "ncomp", "adj_nt"):
             setattr(o, k, int(getattr(self, k)))
         for k in ("dt", "tlag_max", "penalty_power", "deconv_eps", "discard_threshold", "dtw_rinst", "dtw_rcuml",
                   "dtw_epsabs", "dtw_epsrel", "dtw_loss_power", "dtw_amp_weight", "lawi_sigma"):

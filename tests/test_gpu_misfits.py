@@ -119,3 +119,19 @@ def test_gradient_misfit_matches_oracle(kind):
     if kind == L.OWL_MISFIT_WAVEFORM:
         mf2, g2 = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=30))
         assert rel(g, g2) < 1e-6 and rel(mf, mf2) < 1e-6
+
+
+@pytest.mark.parametrize("kind", [L.OWL_MISFIT_WAVEFORM, L.OWL_MISFIT_ENVELOPE, L.OWL_MISFIT_ADAPTIVE])
+def test_adjoint_source_resampled_to_adj_nt(kind):
+    """adj_nt: the misfit on the kept traces resampled (cubic) to adj_nt samples
+    over the same span, the adjoint resampled back"""
+    gp, syn, obs, w = _gathers(400)
+    for nn in (300, 613):
+        mo = MisfitOpts(misfit=kind, dt=1e-3, tlag_max=0.04, adj_nt=nn)
+        adj, tm, gm = adjoint_source(mo, gp, syn, obs, w)
+        ref_adj, ref_tm, ref_gm = M.adjoint_source(kind, gp, syn, obs, w, dt=1e-3, tlag_max=0.04, adj_nt=nn)
+        assert np.all(tm[[1, 6, 8]] == 0)
+        assert rel(adj, ref_adj) < 1e-4, (nn, rel(adj, ref_adj))
+        assert rel(tm, ref_tm) < 1e-4, (nn, tm, ref_tm)
+    with pytest.raises(L.OwlError):  # not built for DTW
+        adjoint_source(MisfitOpts(misfit=L.OWL_MISFIT_DTW, dt=1e-3, tlag_max=0.02, adj_nt=300), gp, syn, obs, w)

@@ -77,7 +77,9 @@ def test_gradient_at_data_sampling(kind):
         _, g = s.gradient(ps, adj_d.ravel(), L.OWL_ADJ_GIVEN, opts)
     else:
         mf, g = s.gradient_misfit(ps, obs.ravel(), MisfitOpts(misfit=kind), opts)
-        adj_d, _, gm = M.adjoint_source(kind, s.gather_ptr(ps), syn_d, obs, live.astype(np.float64), dt=DDT)
+        # the misfit is taken on the traces resampled to the time axis' NT samples (adj_nt's default)
+        adj_d, _, gm = M.adjoint_source(kind, s.gather_ptr(ps), syn_d, obs, live.astype(np.float64), dt=DDT,
+                                        adj_nt=NT)
         assert rel(mf, gm) < 2e-4
     adj_t = R.resample_rows(adj_d, DDT, DT, NT).astype(np.float32)
     _, g_ref, _ = oracle.ac2d_gradient(d, vp0, rho, ps, adj_t.ravel(), adj_kind=1, k=30, precision="f64")
