@@ -308,12 +308,22 @@ int owl_search_direction(int method, long long n, int nm, const float *const *mo
  *   OWL_GRAD_MASK         multiply by mask (n1 x n2 x n3)
  *   OWL_GRAD_SCALE        multiply by param[0]
  *   OWL_GRAD_MAX_BALANCE  divide by the field's maximum when it is not 0
+ *   OWL_GRAD_RMS_BALANCE  divide by the field's root-mean-square when it is not 0 (rms_balance)
+ *   OWL_GRAD_RMS_BALANCE_AXIS  rms_balance_z / _x (/ _y): each slice j along axis param[0] (1, 2, 3)
+ *                         divided by the L2 norm of the slices j - (w-1)/2 .. j + (w-1)/2, w =
+ *                         param[1] cells rounded and made odd (zero slices beyond the ends); NaN / Inf -> 0
+ *   OWL_GRAD_MEDIAN       median_filt: median of the window of half-widths param[0..2] cells per axis,
+ *                         truncated at the ends (the mean of the two middle values of an even count);
+ *                         the window holds at most 343 cells
  * param is host memory; field and mask host or device (mem_kind). */
 #define OWL_GRAD_SMOOTH 0
 #define OWL_GRAD_TAPER 1
 #define OWL_GRAD_MASK 2
 #define OWL_GRAD_SCALE 3
 #define OWL_GRAD_MAX_BALANCE 4
+#define OWL_GRAD_RMS_BALANCE 5
+#define OWL_GRAD_RMS_BALANCE_AXIS 6
+#define OWL_GRAD_MEDIAN 7
 int owl_grad_process(int op, int n1, int n2, int n3, const float *param, const float *mask, float *field,
                      int mem_kind);
 

@@ -6,7 +6,12 @@ compute_search_direction (src/inverse/module_inversion_search_direction.f90):
   L-BFGS two-loop recursion :91-246 over s_i = x_{i+1} - x_i, y_i = g_{i+1} - g_i.
 process_model_single_parameter (src/inverse/2d/module_gradient.f90:733-892):
   smooth (FLIT gauss_filt), taper (FLIT taper, Blackman ramps), mask, scale,
-  max_balance. FLIT is not vendored (no version pinned) and no reference test
+  max_balance, rms_balance (FLIT mean(w, 2), restated as the root mean
+  square), rms_balance_z / _x (:795-823, restated as written: each slice
+  divided by the L2 norm of the odd window of slices around it, NaN / Inf -> 0),
+  median_filt (FLIT, restated as the median of the window of the given
+  half-widths, truncated at the ends, the mean of the two middle values of an
+  even count). FLIT is not vendored (no version pinned) and no reference test
   pins gauss_filt or taper -- parity unpinned: restated as a Gaussian of the
   given standard deviation in cells truncated at ceil(3 sigma), normalised,
   edge samples replicated; Blackman ramps 0.42 - 0.5 cos(pi i / l) +
@@ -20,6 +25,7 @@ import numpy as np
 
 SD, CG, LBFGS = 0, 1, 2
 SMOOTH, TAPER, MASK, SCALE, MAX_BALANCE = 0, 1, 2, 3, 4
+RMS_BALANCE, RMS_BALANCE_AXIS, MEDIAN = 5, 6, 7
 
 
 def search_direction(method, models, grads, prev_srch=None):
@@ -99,4 +105,32 @@ def process(op, field, param=None, mask=None):
     if op == MAX_BALANCE:
         m = f.max()
         return f / m if m != 0 else f
+    if op == RMS_BALANCE:
+        r = math.sqrt(float(np.mean(f * f)))
+        return f / r if r != 0 else f
+    if op == RMS_BALANCE_AXIS:
+        axis = f.ndim - int(round(param[0]))
+        wn = int(round(param[1]))
+        if wn % 2 == 0:
+            wn -= 1
+        hw = (wn - 1) // 2
+        fm = np.moveaxis(f, axis, 0)
+        ss = np.array([np.sum(fm[j] ** 2) for j in range(fm.shape[0])])
+        nrm = np.array([math.sqrt(ss[max(0, j - hw):j + hw + 1].sum()) for j in range(fm.shape[0])])
+        with np.errstate(invalid="ignore", divide="ignore"):
+            out = fm / nrm.reshape((-1,) + (1,) * (fm.ndim - 1))
+        out = np.where(np.isfinite(out), out, 0.0)
+        return np.moveaxis(out, 0, axis)
+    if op == MEDIAN:
+        h = [int(round(param[a])) for a in range(3)]
+        out = np.empty_like(f)
+        for idx in np.ndindex(*f.shape):
+            sl = []
+            for d, i in enumerate(idx):
+                hh = h[f.ndim - 1 - d] if f.shape[d] > 1 else 0
+                sl.append(slice(max(0, i - hh), min(f.shape[d], i + hh + 1)))
+            w = np.sort(f[tuple(sl)].ravel())
+            c = w.size
+            out[idx] = w[c // 2] if c % 2 else 0.5 * (w[c // 2 - 1] + w[c // 2])
+        return out
     raise ValueError(op)

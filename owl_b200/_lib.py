@@ -212,6 +212,9 @@ OWL_GRAD_TAPER = 1
 OWL_GRAD_MASK = 2
 OWL_GRAD_SCALE = 3
 OWL_GRAD_MAX_BALANCE = 4
+OWL_GRAD_RMS_BALANCE = 5
+OWL_GRAD_RMS_BALANCE_AXIS = 6
+OWL_GRAD_MEDIAN = 7
 
 OWL_K_FWD_P = 0
 OWL_K_FWD_V = 1

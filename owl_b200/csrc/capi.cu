@@ -320,7 +320,7 @@ int owl_grad_process(int op, int n1, int n2, int n3, const float* param, const f
                      int mem_kind) {
     return guarded([&] {
         check_device();
-        OWL_CHECK(op >= OWL_GRAD_SMOOTH && op <= OWL_GRAD_MAX_BALANCE, OWL_ERR_INVALID, "bad gradient processing op");
+        OWL_CHECK(op >= OWL_GRAD_SMOOTH && op <= OWL_GRAD_MEDIAN, OWL_ERR_INVALID, "bad gradient processing op");
         OWL_CHECK(n1 >= 1 && n2 >= 1 && n3 >= 1 && field, OWL_ERR_INVALID, "bad field");
         OWL_CHECK(param || op == OWL_GRAD_MASK || op == OWL_GRAD_MAX_BALANCE, OWL_ERR_INVALID, "null param");
         OWL_CHECK(mem_kind == OWL_MEM_HOST || mem_kind == OWL_MEM_DEVICE, OWL_ERR_INVALID, "bad mem_kind");

@@ -135,6 +135,83 @@ __global__ void k_max_part(const float* __restrict__ f, long long n, float* __re
     }
 }
 
+// sum of squares of each slice along an axis (one CTA per slice, FP64)
+__global__ void k_slice_sumsq(const float* __restrict__ f, int n1, int n2, int n3, int axis, double* __restrict__ out) {
+    const int j = blockIdx.x;
+    const long long m = axis == 0 ? (long long)n2 * n3 : axis == 1 ? (long long)n1 * n3 : (long long)n1 * n2;
+    double acc = 0.0;
+    for (long long e = threadIdx.x; e < m; e += blockDim.x) {
+        long long i1, i2, i3;
+        if (axis == 0) { i1 = j; i2 = e % n2; i3 = e / n2; }
+        else if (axis == 1) { i1 = e % n1; i2 = j; i3 = e / n1; }
+        else { i1 = e % n1; i2 = e / n1; i3 = j; }
+        const double v = f[(i3 * n2 + i2) * n1 + i1];
+        acc += v * v;
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[j] = red[0];
+}
+
+// each element divided by the norm of its slice's window; NaN / Inf -> 0
+__global__ void k_div_slice(float* __restrict__ f, long long n, int n1, int n2, int axis, const float* __restrict__ nrm) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long j = axis == 0 ? i % n1 : axis == 1 ? (i / n1) % n2 : i / ((long long)n1 * n2);
+        const float v = f[i] / nrm[j];
+        f[i] = isfinite(v) ? v : 0.f;
+    }
+}
+
+// median of the (2 h1 + 1) x (2 h2 + 1) x (2 h3 + 1) window, truncated at the ends
+__device__ float select_kth(float* a, int n, int k) {  // k-th smallest (0-based), a is reordered
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const float piv = a[(lo + hi) / 2];
+        int i = lo, j = hi;
+        while (i <= j) {
+            while (a[i] < piv) ++i;
+            while (a[j] > piv) --j;
+            if (i <= j) {
+                const float t = a[i]; a[i] = a[j]; a[j] = t;
+                ++i; --j;
+            }
+        }
+        if (k <= j) hi = j;
+        else if (k >= i) lo = i;
+        else return a[k];
+    }
+    return a[k];
+}
+
+__global__ void k_median(const float* __restrict__ in, float* __restrict__ out, int n1, int n2, int n3, int h1, int h2,
+                         int h3) {
+    const long long n = (long long)n1 * n2 * n3;
+    float w[343];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int i1 = (int)(i % n1), i2 = (int)((i / n1) % n2), i3 = (int)(i / ((long long)n1 * n2));
+        int c = 0;
+        for (int a3 = max(0, i3 - h3); a3 <= min(n3 - 1, i3 + h3); ++a3)
+            for (int a2 = max(0, i2 - h2); a2 <= min(n2 - 1, i2 + h2); ++a2)
+                for (int a1 = max(0, i1 - h1); a1 <= min(n1 - 1, i1 + h1); ++a1)
+                    w[c++] = in[((long long)a3 * n2 + a2) * n1 + a1];
+        float v;
+        if (c & 1) {
+            v = select_kth(w, c, c / 2);
+        } else {
+            const float hi = select_kth(w, c, c / 2);
+            float lo = w[0];  // after the selection, the largest of w[0 .. c/2 - 1] is the (c/2 - 1)-th
+            for (int k = 1; k < c / 2; ++k) lo = fmaxf(lo, w[k]);
+            v = 0.5f * (lo + hi);
+        }
+        out[i] = v;
+    }
+}
+
 int blocks_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, RED_BLOCKS)); }
 
 // (s.q, y.s, y.y) on the device, returned to the host
@@ -261,6 +338,65 @@ void grad_process(int op, int n1, int n2, int n3, const float* param, const floa
                 k_mul<<<nb, 256, 0, s>>>(f, n, nullptr, 1.f / m);
                 OWL_LAUNCH_CHECK();
             }
+            break;
+        }
+        case OWL_GRAD_RMS_BALANCE: {
+            DevBuf<double> part, tot;
+            part.reserve(1);
+            k_slice_sumsq<<<1, 256, 0, s>>>(f, 1, (int)n, 1, 0, part.p);  // the whole field as one slice
+            OWL_LAUNCH_CHECK();
+            double ss = 0.0;
+            OWL_CUDA(cudaMemcpyAsync(&ss, part.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+            OWL_CUDA(cudaStreamSynchronize(s));
+            const double rms = std::sqrt(ss / (double)n);
+            if (rms != 0.0) {
+                k_mul<<<nb, 256, 0, s>>>(f, n, nullptr, (float)(1.0 / rms));
+                OWL_LAUNCH_CHECK();
+            }
+            break;
+        }
+        case OWL_GRAD_RMS_BALANCE_AXIS: {
+            const int axis = (int)std::lround(param[0]) - 1;
+            OWL_CHECK(axis >= 0 && axis <= 2, OWL_ERR_INVALID, "rms balance axis must be 1, 2 or 3");
+            int wn = (int)std::lround(param[1]);
+            if (wn % 2 == 0) --wn;
+            OWL_CHECK(wn >= 1, OWL_ERR_INVALID, "rms balance window must be at least 1 cell");
+            const int len[3] = {n1, n2, n3};
+            const int L = len[axis];
+            DevBuf<double> ss;
+            ss.reserve(L);
+            k_slice_sumsq<<<L, 256, 0, s>>>(f, n1, n2, n3, axis, ss.p);
+            OWL_LAUNCH_CHECK();
+            std::vector<double> hs(L);
+            OWL_CUDA(cudaMemcpyAsync(hs.data(), ss.p, L * sizeof(double), cudaMemcpyDeviceToHost, s));
+            OWL_CUDA(cudaStreamSynchronize(s));
+            std::vector<float> hn(L);
+            const int hw = (wn - 1) / 2;
+            for (int j = 0; j < L; ++j) {
+                double acc = 0.0;
+                for (int k = std::max(0, j - hw); k <= std::min(L - 1, j + hw); ++k) acc += hs[k];
+                hn[j] = (float)std::sqrt(acc);
+            }
+            DevBuf<float> dn;
+            dn.upload(hn.data(), L, s);
+            k_div_slice<<<nb, 256, 0, s>>>(f, n, n1, n2, axis, dn.p);
+            OWL_LAUNCH_CHECK();
+            OWL_CUDA(cudaStreamSynchronize(s));
+            break;
+        }
+        case OWL_GRAD_MEDIAN: {
+            int h[3];
+            for (int i = 0; i < 3; ++i) h[i] = std::max(0, (int)std::lround(param[i]));
+            if (n1 == 1) h[0] = 0;
+            if (n2 == 1) h[1] = 0;
+            if (n3 == 1) h[2] = 0;
+            OWL_CHECK((2 * h[0] + 1) * (2 * h[1] + 1) * (2 * h[2] + 1) <= 343, OWL_ERR_INVALID,
+                      "median window above 343 cells");
+            DevBuf<float> tmp;
+            tmp.reserve(n);
+            k_median<<<nb, 256, 0, s>>>(f, tmp.p, n1, n2, n3, h[0], h[1], h[2]);
+            OWL_LAUNCH_CHECK();
+            OWL_CUDA(cudaMemcpyAsync(f, tmp.p, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
             break;
         }
         default:

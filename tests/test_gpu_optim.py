@@ -49,7 +49,10 @@ def test_processing_matches_oracle(shape):
     # the oracle takes the field with the fastest (z) axis last
     to_o = lambda a: np.ascontiguousarray(np.transpose(a))  # noqa: E731
     for op, par in ((L.OWL_GRAD_SMOOTH, [1.5, 2.5, 1.0]), (L.OWL_GRAD_TAPER, [3, 4, 5, 2, 2, 3]),
-                    (L.OWL_GRAD_MASK, None), (L.OWL_GRAD_SCALE, [2.5]), (L.OWL_GRAD_MAX_BALANCE, None)):
+                    (L.OWL_GRAD_MASK, None), (L.OWL_GRAD_SCALE, [2.5]), (L.OWL_GRAD_MAX_BALANCE, None),
+                    (L.OWL_GRAD_RMS_BALANCE, None), (L.OWL_GRAD_RMS_BALANCE_AXIS, [1, 5]),
+                    (L.OWL_GRAD_RMS_BALANCE_AXIS, [2, 4]), (L.OWL_GRAD_RMS_BALANCE_AXIS, [len(shape), 1]),
+                    (L.OWL_GRAD_MEDIAN, [1, 1, 1]), (L.OWL_GRAD_MEDIAN, [2, 1, 0])):
         got = process(f.copy(), op, par, m if op == L.OWL_GRAD_MASK else None)
         ref = np.transpose(O.process(op, to_o(f), par, to_o(m)))
         assert rel(got, ref) < 1e-6, (op, rel(got, ref))

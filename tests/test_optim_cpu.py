@@ -47,3 +47,19 @@ def test_processing_properties():
     assert np.array_equal(t[7:-7, 5:-5], g[7:-7, 5:-5])
     assert np.allclose(t[:, 0], 0, atol=1e-12) and np.allclose(t[0, :], 0, atol=1e-12)
     assert np.isclose(O.process(O.MAX_BALANCE, g).max(), 1.0)
+
+
+def test_balance_and_median_properties():
+    """rms_balance leaves unit root mean square; the windowed balance of a
+    field constant along its axis is the field over sqrt(window slices);
+    the median of a field with one spike removes it"""
+    rng = np.random.default_rng(2)
+    f = rng.standard_normal((9, 12))
+    g = O.process(O.RMS_BALANCE, f)
+    assert abs(np.sqrt(np.mean(g * g)) - 1.0) < 1e-12
+    c = np.ones((7, 10))  # axis 1 (n1, the last numpy axis) has 10 slices of 7 ones
+    b = O.process(O.RMS_BALANCE_AXIS, c, [1, 3])
+    assert np.allclose(b[:, 1:-1], 1.0 / np.sqrt(21.0)) and np.allclose(b[:, 0], 1.0 / np.sqrt(14.0))
+    sp = np.zeros((5, 6))
+    sp[2, 3] = 100.0
+    assert np.all(O.process(O.MEDIAN, sp, [1, 1, 0]) == 0.0)
