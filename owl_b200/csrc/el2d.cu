@@ -77,8 +77,9 @@ __device__ __forceinline__ float pml_e(float q, float a, float b, float psih, fl
 }
 
 // ------------------------------- forward ------------------------------------
+// 48 registers at R = 4 (no spills): five 256-thread CTAs per SM instead of four
 template <int R, bool STORE>
-__global__ void __launch_bounds__(512) k_el2d_fwd_s(El2dDev a) {
+__global__ void __maxnreg__(R == 4 ? 48 : 128) k_el2d_fwd_s(El2dDev a) {
     const int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int z = a.zs0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
@@ -331,8 +332,11 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
 // (sigma^ += D^T e of the velocity nodes, free-surface images folded back with
 // a minus), correlate sigma^ with the stored terms of step t (Cij gradients),
 // then the adjoint PML terms of the stress update of step t
+// 64 registers at R = 4 (a few bytes spilled) instead of the 128 that a
+// 512-thread bound allows: four 256-thread CTAs per SM instead of two, which
+// hides more of the load latency this kernel is bound by
 template <int R>
-__global__ void __launch_bounds__(512) k_el2d_adj_s(El2dDev a) {
+__global__ void __maxnreg__(R == 4 ? 64 : 128) k_el2d_adj_s(El2dDev a) {
     const int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int z = a.zs0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
