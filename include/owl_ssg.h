@@ -148,8 +148,9 @@ typedef struct {
     int adaptive_half_window; /* space-time adaptive: neighbouring traces on each side */
     int ncomp;               /* dtw-vector: components (gathers) per shot */
     int adj_nt;              /* samples the traces are resampled to (cubic) before the misfit, the adjoint
-                                resampled back; 0: owl_adjoint_source none, the gradient driver the time
-                                axis' nt, as the reference (DTW: none; other values rejected) */
+                                resampled back (DTW: the shifts and quality weights are computed at adj_nt
+                                samples and interpolated back, pchip); 0: owl_adjoint_source none, the
+                                gradient driver the time axis' nt, as the reference */
 } owl_misfit_opts;
 
 typedef struct owl_ssg owl_ssg;

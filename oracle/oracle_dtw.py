@@ -12,8 +12,11 @@ Follows src/inverse/module_inversion_adjoint_source.f90:
 with the defaults of src/lib/module_parameters.f90:270-280, 559-569
 (dtw_niter 5, dtw_rinst 0.1, dtw_rcuml 1, dtw_epsabs 1e-2, dtw_epsrel 1e-3,
 dtw_loss 'l0.5', dtw_form 'phase', dtw_amp_weight 1, dtw_trc 0, no smoothing of
-the shifts across traces). The data are taken at their own sampling (adj_nt
-equal to the trace length, no resampling).
+the shifts across traces). With adj_nt (:744-750, :765-771, :907-911) the
+normalised traces are resampled to adj_nt samples over the same span (cubic,
+single precision), the shifts and quality weights are computed at that
+sampling and interpolated back to the trace length with 'pchip'; the adjoint
+is taken on the traces as given.
 
 The dynamic program is evaluated in the order of the reference's loops (for each
 row, candidates j ascending, strict improvement), in float64 without fused
@@ -35,7 +38,17 @@ unpinned. They are restated as:
   gauss_filt(q,3)  Gaussian of standard deviation 3 samples truncated at 9,
                    normalised, end samples replicated;
   deriv(x)         centred difference inside, one-sided at the ends;
-  rescale(q,[0,1]) (q - min) / (max - min);  return_normal: NaN / Inf -> 0.
+  rescale(q,[0,1]) (q - min) / (max - min);  return_normal: NaN / Inf -> 0;
+  interp_to cubic  the trace resampling restatement (oracle_resample), evaluated
+                   in float64 and rounded to single precision;
+  interp_to pchip  monotone piecewise cubic Hermite interpolation (Fritsch and
+                   Carlson 1980) on the unit sample grid: interior slopes the
+                   harmonic mean of the neighbouring secants (zero where they
+                   differ in sign or one is zero), end slopes the three-point
+                   formula (3 s0 - s1) / 2 limited to keep the secant's sign and
+                   at most 3 |s0|; output sample i at x = i dout / din (1e-4
+                   snap to a node), clamped to the grid; float64, rounded to
+                   single precision.
 """
 from __future__ import annotations
 
@@ -214,13 +227,72 @@ def deriv(x):
     return d
 
 
+def resample_f32(rows, din, dout, nout):
+    """interp_to(x, nout, method='cubic') of single-precision rows (:767-768)."""
+    from .oracle_resample import resample_rows
+    shp = np.shape(rows)
+    out = resample_rows(np.reshape(rows, (-1, shp[-1])), din, dout, nout)
+    return out.astype(f32).astype(np.float64).reshape(shp[:-1] + (nout,))
+
+
+def _pchip_slope(r, k):
+    nn = len(r)
+    if nn == 2:
+        return r[1] - r[0]
+    if k == 0 or k == nn - 1:
+        a, b = (r[1] - r[0], r[2] - r[1]) if k == 0 else (r[nn - 1] - r[nn - 2], r[nn - 2] - r[nn - 3])
+        d = (3.0 * a - b) / 2.0
+        if np.sign(d) != np.sign(a):
+            return 0.0
+        if np.sign(a) != np.sign(b) and abs(d) > abs(3.0 * a):
+            return 3.0 * a
+        return d
+    a, b = r[k] - r[k - 1], r[k + 1] - r[k]
+    if a == 0 or b == 0 or (a > 0) != (b > 0):
+        return 0.0
+    return 2.0 / (1.0 / a + 1.0 / b)
+
+
+def pchip_rows(rows, din, dout, nout):
+    """interp_to(x, [nout, nr], method=['pchip', 'nearest']) (:909-910) of
+    single-precision rows sampled at din onto nout samples at dout."""
+    shp = np.shape(rows)
+    R = np.reshape(np.asarray(rows, dtype=np.float64), (-1, shp[-1]))
+    nn = R.shape[1]
+    out = np.zeros((R.shape[0], nout))
+    for i in range(nout):
+        x = (i * dout) / din
+        if abs(x - np.rint(x)) <= 1e-4:
+            x = float(np.rint(x))
+        x = min(max(x, 0.0), float(nn - 1))
+        j0 = min(int(math.floor(x)), nn - 2)
+        u = x - j0
+        w = 1.0 - u
+        h00, h10 = (1.0 + 2.0 * u) * (w * w), u * (w * w)
+        h01, h11 = (u * u) * (3.0 - 2.0 * u), (u * u) * (u - 1.0)
+        for t in range(R.shape[0]):
+            r = R[t]
+            out[t, i] = h00 * r[j0] + h10 * _pchip_slope(r, j0) + h01 * r[j0 + 1] + h11 * _pchip_slope(r, j0 + 1)
+    return out.astype(f32).reshape(shp[:-1] + (nout,))
+
+
+def _adj_sampling(dsyn, dobs, dd, adj_nt):
+    """(n, dd, dsyn, dobs) of the shift computation: the normalised traces
+    resampled to adj_nt samples over the same span (:744-750, :765-768)."""
+    n = np.shape(dsyn)[-1]
+    if adj_nt <= 0 or adj_nt == n:
+        return n, dd, dsyn, dobs
+    ddn = float(f32(f32(n - 1) * f32(dd)) / f32(adj_nt - 1))
+    return adj_nt, ddn, resample_f32(dsyn, dd, ddn, adj_nt), resample_f32(dobs, dd, ddn, adj_nt)
+
+
 def _normal(a):
     a = np.asarray(a, dtype=np.float64)
     return np.where(np.isfinite(a), a, 0.0)
 
 
 def dtw_gather(syn, obs, live, dd, tlag_max, form=PHASE, niter=5, rinst=0.1, rcuml=1.0, epsabs=1.0e-2,
-               epsrel=1.0e-3, power=0.5, amp_weight=1.0, trc=0):
+               epsrel=1.0e-3, power=0.5, amp_weight=1.0, trc=0, adj_nt=0):
     """compute_adjsrc_dtw (:715-980) on one gather (nr, n): returns
     (adj, trace misfits, tau in seconds, quality weights)."""
     syn = np.asarray(syn, dtype=f32)
@@ -235,6 +307,8 @@ def dtw_gather(syn, obs, live, dd, tlag_max, form=PHASE, niter=5, rinst=0.1, rcu
         if live[i]:
             dsyn[i] = (syn[i] / f32(np.linalg.norm(syn[i].astype(np.float64)))).astype(np.float64)
             dobs[i] = (obs[i] / f32(np.linalg.norm(obs[i].astype(np.float64)))).astype(np.float64)
+    n0, dd0 = n, dd
+    n, dd, dsyn, dobs = _adj_sampling(dsyn, dobs, dd, adj_nt)
     m = lag_count(tlag_max, dd)
     tau = np.zeros((nr, n), dtype=f32)
     for i in range(nr):
@@ -278,6 +352,9 @@ def dtw_gather(syn, obs, live, dd, tlag_max, form=PHASE, niter=5, rinst=0.1, rcu
         for i in range(nr):
             if np.max(np.abs(q[i])) == 0:
                 q[i] = 1.0
+    if n != n0:  # shifts and weights back to the trace length (:907-911)
+        tau, q = pchip_rows(tau, dd, dd0, n0), pchip_rows(q, dd, dd0, n0)
+        n, dd = n0, dd0
     # adjoint source (:917-978)
     adj = np.zeros((nr, n))
     tm = np.zeros(nr)
@@ -340,7 +417,7 @@ def adjoint_source(gather_ptr, syn, obs, weight=None, dt=1e-3, tlag_max=0.0, dis
 
 
 def dtw_vector(syn, obs, live, dd, tlag_max, form=PHASE, niter=5, rinst=0.1, rcuml=1.0, epsabs=1.0e-2,
-               epsrel=1.0e-3, power=0.5, amp_weight=1.0, trc=0):
+               epsrel=1.0e-3, power=0.5, amp_weight=1.0, trc=0, adj_nt=0):
     """compute_adjsrc_dtw on the components of one shot together ('dtw-vector',
     :1232-1236): syn, obs (nc, nr, n), live (nc, nr) after the discard rule.
     A receiver is kept when any component is; traces are normalised by the
@@ -367,6 +444,8 @@ def dtw_vector(syn, obs, live, dd, tlag_max, form=PHASE, niter=5, rinst=0.1, rcu
             if live[c, i]:
                 dsyn[c, i] = (syn[c, i] / ns).astype(np.float64)
                 dobs[c, i] = (obs[c, i] / no).astype(np.float64)
+    n0, dd0 = n, dd
+    n, dd, dsyn, dobs = _adj_sampling(dsyn, dobs, dd, adj_nt)
     m = lag_count(tlag_max, dd)
     tau = np.zeros((nc, nr, n), dtype=f32)
     for i in range(nr):
@@ -410,6 +489,9 @@ def dtw_vector(syn, obs, live, dd, tlag_max, form=PHASE, niter=5, rinst=0.1, rcu
         for i in range(nr):
             if np.max(np.abs(q[i])) == 0:
                 q[i] = 1.0
+    if n != n0:
+        tau, q = pchip_rows(tau, dd, dd0, n0), pchip_rows(q, dd, dd0, n0)
+        n, dd = n0, dd0
     adj = np.zeros((nc, nr, n))
     tm = np.zeros((nc, nr))
     td = np.arange(n, dtype=f32) * f32(dd)

@@ -703,12 +703,12 @@ void AdjointSource::run(const owl_misfit_opts& o, int ngather, const int* h_gath
     OWL_LAUNCH_CHECK();
     launches += 2;
 
-    if (o.adj_nt > 0 && o.adj_nt != nt) {
+    const bool dtw = o.misfit == OWL_MISFIT_DTW || o.misfit == OWL_MISFIT_DTW_VECTOR;
+    if (o.adj_nt > 0 && o.adj_nt != nt && !dtw) {
         // adj_nt (:1082-1089, :1111-1152): the misfit on the traces resampled to
         // adj_nt samples over the same span (cubic), the adjoint resampled back;
-        // the trace selection is that of the traces as given
-        OWL_CHECK(o.misfit != OWL_MISFIT_DTW && o.misfit != OWL_MISFIT_DTW_VECTOR, OWL_ERR_UNSUPPORTED,
-                  "adj_nt resampling of the DTW misfits is not built");
+        // the trace selection is that of the traces as given (DTW resamples
+        // only its shift computation: run_dtw)
         OWL_CHECK(o.dt > 0.f && o.adj_nt >= 2, OWL_ERR_INVALID, "adj_nt needs dt and at least 2 samples");
         const int nn = o.adj_nt;
         const float dd = ((float)(nt - 1) * o.dt) / (float)(nn - 1);
@@ -730,7 +730,7 @@ void AdjointSource::run(const owl_misfit_opts& o, int ngather, const int* h_gath
         OWL_CUDA(cudaStreamSynchronize(s));
         return;
     }
-    if (o.misfit == OWL_MISFIT_DTW || o.misfit == OWL_MISFIT_DTW_VECTOR) {
+    if (dtw) {
         if (o.misfit == OWL_MISFIT_DTW_VECTOR) {
             const int vc = std::max(1, o.ncomp);
             OWL_CHECK(ngather % vc == 0, OWL_ERR_INVALID, "dtw-vector: the gathers must come in groups of ncomp");

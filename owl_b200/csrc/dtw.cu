@@ -442,6 +442,80 @@ __global__ void __launch_bounds__(256) k_dtw_quality(DtwArgs a) {
     spread();
 }
 
+// interp_to(x, nn, 'cubic') of the normalised traces (:765-768): Keys cubic
+// convolution (a = -1/2; indices clamped to the trace, zero outside it, 1e-4
+// snap to a node) in float64 without fused multiply-adds, rounded to single
+// precision as the reference's traces are
+__global__ void k_dtw_resample(const double* __restrict__ in, int n, double din, double* __restrict__ out, int nn,
+                               double dout, int ntr) {
+    const size_t tot = (size_t)ntr * nn;
+    for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < tot; o += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(o / nn), i = (int)(o % nn);
+        double x = __ddiv_rn(dmul((double)i, dout), din);
+        const double xr = rint(x);
+        if (fabs(dsub(x, xr)) <= 1e-4) x = xr;
+        double v = 0.0;
+        if (x >= 0.0 && x <= (double)(n - 1)) {
+            const int j0 = (int)floor(x);
+            const double u = dsub(x, (double)j0), u2 = dmul(u, u), u3 = dmul(u2, u);
+            const double w0 = dmul(0.5, dsub(dadd(-u3, dmul(2.0, u2)), u));
+            const double w1 = dmul(0.5, dadd(dsub(dmul(3.0, u3), dmul(5.0, u2)), 2.0));
+            const double w2 = dmul(0.5, dadd(dadd(dmul(-3.0, u3), dmul(4.0, u2)), u));
+            const double w3 = dmul(0.5, dsub(u3, u2));
+            const double* row = in + (size_t)r * n;
+            v = dadd(dadd(dadd(dmul(w0, row[max(j0 - 1, 0)]), dmul(w1, row[j0])), dmul(w2, row[min(j0 + 1, n - 1)])),
+                     dmul(w3, row[min(j0 + 2, n - 1)]));
+        }
+        out[o] = (double)(float)v;
+    }
+}
+
+__device__ __forceinline__ int sgn(double v) { return (v > 0.0) - (v < 0.0); }
+
+// slope of the monotone cubic at node k of a row on the unit grid: the harmonic
+// mean of the neighbouring secants inside (zero where they differ in sign or one
+// is zero), the three-point formula at the ends limited to keep the secant's
+// sign and at most three times it (Fritsch and Carlson 1980)
+__device__ double pchip_slope(const float* r, int nn, int k) {
+    if (nn == 2) return dsub((double)r[1], (double)r[0]);
+    if (k == 0 || k == nn - 1) {
+        const double a = k == 0 ? dsub((double)r[1], (double)r[0]) : dsub((double)r[nn - 1], (double)r[nn - 2]);
+        const double b = k == 0 ? dsub((double)r[2], (double)r[1]) : dsub((double)r[nn - 2], (double)r[nn - 3]);
+        const double a3 = dmul(3.0, a);
+        const double d = __ddiv_rn(dsub(a3, b), 2.0);
+        if (sgn(d) != sgn(a)) return 0.0;
+        if (sgn(a) != sgn(b) && fabs(d) > fabs(a3)) return a3;
+        return d;
+    }
+    const double a = dsub((double)r[k], (double)r[k - 1]), b = dsub((double)r[k + 1], (double)r[k]);
+    if (a == 0.0 || b == 0.0 || (a > 0.0) != (b > 0.0)) return 0.0;
+    return __ddiv_rn(2.0, dadd(__ddiv_rn(1.0, a), __ddiv_rn(1.0, b)));
+}
+
+// interp_to(x, [n, nr], method=['pchip', 'nearest']) (:907-911): rows of nn
+// samples at din onto n samples at dout (x = i dout / din, 1e-4 snap to a node,
+// clamped to the grid), float64 without fused multiply-adds, single-precision out
+__global__ void k_dtw_pchip(const float* __restrict__ in, int nn, double din, float* __restrict__ out, int n,
+                            double dout, int ntr) {
+    const size_t tot = (size_t)ntr * n;
+    for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < tot; o += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(o / n), i = (int)(o % n);
+        double x = __ddiv_rn(dmul((double)i, dout), din);
+        const double xr = rint(x);
+        if (fabs(dsub(x, xr)) <= 1e-4) x = xr;
+        x = fmin(fmax(x, 0.0), (double)(nn - 1));
+        const int j0 = min((int)floor(x), nn - 2);
+        const double u = dsub(x, (double)j0), w = dsub(1.0, u), ww = dmul(w, w), uu = dmul(u, u);
+        const double h00 = dmul(dadd(1.0, dmul(2.0, u)), ww), h10 = dmul(u, ww);
+        const double h01 = dmul(uu, dsub(3.0, dmul(2.0, u))), h11 = dmul(uu, dsub(u, 1.0));
+        const float* row = in + (size_t)r * nn;
+        const double v = dadd(dadd(dadd(dmul(h00, (double)row[j0]), dmul(h10, pchip_slope(row, nn, j0))),
+                                   dmul(h01, (double)row[j0 + 1])),
+                              dmul(h11, pchip_slope(row, nn, j0 + 1)));
+        out[o] = (float)v;
+    }
+}
+
 __device__ __forceinline__ double keys_at(const float* x, int n, double p) {
     if (fabs(p - rint(p)) <= 1e-4) p = rint(p);
     if (p < 0.0 || p > (double)(n - 1)) return 0.0;
@@ -529,8 +603,14 @@ void AdjointSource::run_dtw(const owl_misfit_opts& o, int ngather, int nt, int n
     OWL_CHECK(o.dt > 0.f, OWL_ERR_INVALID, "the DTW misfit needs the sample interval dt");
     OWL_CHECK(nt >= 3 && nt <= 16384, OWL_ERR_INVALID, "DTW traces must have 3 .. 16384 samples");
     const float tlag = o.tlag_max > 0.f ? o.tlag_max : 0.1f * (float)(nt - 1) * o.dt;
+    // adj_nt (:744-750): the shifts and quality weights are computed on the
+    // normalised traces resampled to ns samples over the same span
+    const bool rs = o.adj_nt > 0 && o.adj_nt != nt;
+    const int ns = rs ? o.adj_nt : nt;
+    OWL_CHECK(ns >= 3 && ns <= 16384, OWL_ERR_INVALID, "DTW: adj_nt must lie in 3 .. 16384");
+    const float dds = rs ? ((float)(nt - 1) * o.dt) / (float)(ns - 1) : o.dt;
     // m = nint(2 tlag_max / dd) + 1, odd (:795, solve_gdtw :92-96)
-    const float x = (2.0f * tlag) / o.dt;
+    const float x = (2.0f * tlag) / dds;
     int m = (int)std::floor(std::fabs((double)x) + 0.5) + 1;
     if (m % 2 == 0) ++m;
     OWL_CHECK(m >= 3 && m <= 4095, OWL_ERR_INVALID, "DTW: 2 tlag_max / dt + 1 must lie in 3 .. 4095 candidates");
@@ -563,7 +643,7 @@ void AdjointSource::run_dtw(const owl_misfit_opts& o, int ngather, int nt, int n
     dsn.reserve(nn);
     dob.reserve(nn);
     qw.reserve(nn);
-    warp.reserve(nn);
+    warp.reserve((size_t)ntr * std::max(nt, ns));
     DevBuf<float> tmp_tau;
     if (!tau_out) {
         tmp_tau.reserve(nn);
@@ -580,11 +660,11 @@ void AdjointSource::run_dtw(const owl_misfit_opts& o, int ngather, int nt, int n
     OWL_CUDA(cudaGetDevice(&dev_id));
     OWL_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev_id));
     // back-pointer tables of the traces solved at once: at most 2 GiB
-    const size_t per = (size_t)nt * m * sizeof(unsigned short);
+    const size_t per = (size_t)ns * m * sizeof(unsigned short);
     const size_t cap = std::max<size_t>(1, ((size_t)2 << 30) / per);
     const int grid = (int)std::max<size_t>(1, std::min<size_t>({(size_t)ntr, (size_t)nsm * 4, cap}));
-    path.reserve((size_t)grid * nt * m);
-    band.reserve((size_t)grid * 3 * nt);
+    path.reserve((size_t)grid * ns * m);
+    band.reserve((size_t)grid * 3 * ns);
     a.path = path.p;
     a.band = band.p;
     if (a.vc > 1) {
@@ -594,10 +674,38 @@ void AdjointSource::run_dtw(const owl_misfit_opts& o, int ngather, int nt, int n
         launches++;
     }
     k_dtw_normalise<<<(int)std::min<size_t>((nn + 255) / 256, (size_t)nsm * 32), 256, 0, s>>>(a);
+    // the shift computation's view: ns samples at dds
+    DtwArgs b = a;
+    DevBuf<double> rsn, rob;
+    DevBuf<float> rtau, rq;
+    if (rs) {
+        const size_t nr = (size_t)ntr * ns;
+        rsn.reserve(nr);
+        rob.reserve(nr);
+        rtau.reserve(nr);
+        rq.reserve(nr);
+        const int gr = (int)std::min<size_t>((nr + 255) / 256, (size_t)nsm * 32);
+        k_dtw_resample<<<gr, 256, 0, s>>>(dsn.p, nt, (double)o.dt, rsn.p, ns, (double)dds, ntr);
+        k_dtw_resample<<<gr, 256, 0, s>>>(dob.p, nt, (double)o.dt, rob.p, ns, (double)dds, ntr);
+        launches += 2;
+        b.n = ns;
+        b.dd = dds;
+        b.dsn = rsn.p;
+        b.dob = rob.p;
+        b.tau = rtau.p;
+        b.q = rq.p;
+    }
     const size_t smem = (size_t)3 * m * sizeof(double);
     OWL_CUDA(cudaFuncSetAttribute(k_dtw_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_dtw_solve<<<grid, 256, smem, s>>>(a);
-    k_dtw_quality<<<ntr, 256, 0, s>>>(a);
+    k_dtw_solve<<<grid, 256, smem, s>>>(b);
+    k_dtw_quality<<<ntr, 256, 0, s>>>(b);
+    if (rs) {
+        // shifts and weights back to the trace length (:907-911)
+        const int gr = (int)std::min<size_t>((nn + 255) / 256, (size_t)nsm * 32);
+        k_dtw_pchip<<<gr, 256, 0, s>>>(rtau.p, ns, (double)dds, a.tau, nt, (double)o.dt, ntr);
+        k_dtw_pchip<<<gr, 256, 0, s>>>(rq.p, ns, (double)dds, a.q, nt, (double)o.dt, ntr);
+        launches += 2;
+    }
     k_dtw_adjoint<<<ntr, 256, 0, s>>>(a);
     OWL_LAUNCH_CHECK();
     launches += 4;

@@ -741,8 +741,8 @@ void SsgBase::data_adjoint_source(const float* data, int adj_kind, int mem, int 
         mo.dt = data_dt;
         if (mo.ncomp <= 0) mo.ncomp = ncomp;  // dtw-vector: the components of a shot are its ncomp gathers
         // adj_nt defaults to the time axis' nt (module_parameters.f90:552): the misfit of data
-        // sampled differently is taken on traces resampled to nt samples (DTW: at the data sampling)
-        if (mo.adj_nt <= 0 && mo.misfit != OWL_MISFIT_DTW && mo.misfit != OWL_MISFIT_DTW_VECTOR) mo.adj_nt = desc.nt;
+        // sampled differently is taken on traces resampled to nt samples (DTW: its shifts)
+        if (mo.adj_nt <= 0) mo.adj_nt = desc.nt;
         trace_d.reserve(std::max(rtot, 1));
         adjsrc.launches = 0;
         adjsrc.run(mo, (int)h_gather_ptr.size() - 1, h_gather_ptr.data(), tn, dat_a.p, seis_tmp.p, live.p, dat_b.p,

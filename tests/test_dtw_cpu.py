@@ -119,3 +119,48 @@ def test_lag_count_is_odd():
     for tl, dd in ((0.04, 2e-3), (0.05, 2e-3), (0.1, 1e-3), (0.0105, 1e-3)):
         m = D.lag_count(tl, dd)
         assert m % 2 == 1 and m >= 3
+
+
+def test_pchip_matches_scipy():
+    """The pchip restatement is the published monotone cubic (Fritsch and
+    Carlson): it agrees with SciPy's independent implementation to single
+    precision, keeps monotone rows monotone and reproduces linear rows."""
+    from scipy.interpolate import PchipInterpolator
+    rng = np.random.default_rng(5)
+    for nn, nout in ((30, 71), (57, 20), (3, 11), (2, 9)):
+        x = rng.standard_normal((4, nn)).astype(np.float32)
+        x[1] = np.cumsum(np.abs(x[1]))
+        x[2, nn // 2:] = x[2, nn // 2]  # a flat stretch
+        dout = (nn - 1) / (nout - 1)
+        got = D.pchip_rows(x, 1.0, dout, nout)
+        pos = np.minimum(np.arange(nout) * dout, nn - 1)
+        for r in range(4):
+            ref = PchipInterpolator(np.arange(nn), x[r].astype(np.float64))(pos)
+            assert np.max(np.abs(got[r] - ref)) <= 1e-6 * max(1.0, np.abs(ref).max()), (nn, r)
+        assert np.all(np.diff(got[1]) >= 0)
+    lin = (np.arange(12) * 0.25).astype(np.float32)
+    assert np.allclose(D.pchip_rows(lin, 2.0, 0.5, 45), np.arange(45) * 0.0625, atol=1e-6)
+
+
+def test_adj_nt_shift_computation():
+    """adj_nt: shifts computed on traces resampled to adj_nt samples and brought
+    back by pchip recover the planted shifts at the trace sampling; adj_nt equal
+    to the trace length is no resampling."""
+    n, dd = 300, 2e-3
+    t = np.arange(n) * dd
+    centres, shifts = [0.25, 0.30], [0.012, -0.010]
+    syn = np.stack([_ricker(t, c) for c in centres]).astype(np.float32)
+    obs = np.stack([_ricker(t, c + s) for c, s in zip(centres, shifts)]).astype(np.float32)
+    live = np.ones(2, bool)
+    base = D.dtw_gather(syn, obs, live, dd, 0.04)
+    same = D.dtw_gather(syn, obs, live, dd, 0.04, adj_nt=n)
+    for a, b in zip(base, same):
+        assert np.array_equal(a, b)
+    for nn in (451, 200):
+        adj, tm, tau, q = D.dtw_gather(syn, obs, live, dd, 0.04, adj_nt=nn)
+        assert tau.shape == (2, n) and q.shape == (2, n) and adj.shape == (2, n)
+        ddn = (n - 1) * dd / (nn - 1)
+        for i, s in enumerate(shifts):
+            j = int(np.argmax(np.abs(syn[i])))
+            assert abs(tau[i, j] - s) <= 1.5 * ddn, (nn, i, tau[i, j], s)
+        assert np.all((q >= -1e-6) & (q <= 1 + 1e-6))

@@ -15,6 +15,10 @@ restatement (oracle/oracle_dtw.py).
   component of a kept receiver and a dropped receiver: shifts to 1e-6 s, one
   per receiver on both component rows, adjoints and misfits 1e-4; gather
   layouts that are not groups of equal component gathers are errors;
+* adj_nt: shifts and quality weights computed on the normalised traces
+  resampled to adj_nt samples and brought back by pchip, scalar and vector:
+  shifts to 1e-6 s, adjoints 1e-4; the gradient driver with data sampled off
+  the time axis (adj_nt's default, the time axis' nt) against the FP64 oracle;
 * the documented size limits are errors.
 """
 import numpy as np
@@ -150,3 +154,68 @@ def test_dtw_vector_layout_checks():
     with pytest.raises(L.OwlError):  # component gathers of unequal length
         adjoint_source(MisfitOpts(misfit=L.OWL_MISFIT_DTW_VECTOR, dt=DT, tlag_max=TLAG, ncomp=2),
                        [0, 4, 7, 12, 16], syn, obs, w)
+
+
+@pytest.mark.parametrize("form,nn", [(L.OWL_DTW_PHASE, 451), (L.OWL_DTW_PHASE_AMP, 200), (L.OWL_DTW_AMP, 451)])
+def test_dtw_adj_nt_matches_oracle(form, nn):
+    """adj_nt: the shifts and weights computed on the normalised traces
+    resampled to adj_nt samples (float64 cubic, single-precision result, as the
+    oracle) and interpolated back by pchip; shifts to 1e-6 s."""
+    gp, syn, obs, w = _gathers(300)
+    kw = dict(form=form, amp_weight=0.5 if form == L.OWL_DTW_PHASE_AMP else 1.0, adj_nt=nn)
+    ref_adj, ref_tm, ref_gm, ref_tau = D.adjoint_source(gp, syn, obs, w, dt=DT, tlag_max=TLAG, **kw)
+    mo = _mo(form, dtw_amp_weight=kw["amp_weight"], adj_nt=nn)
+    tau = dtw_time_shifts(mo, gp, syn, obs, w)
+    assert tau.shape == syn.shape
+    assert np.max(np.abs(tau - ref_tau)) <= 1e-6, np.max(np.abs(tau - ref_tau))
+    adj, tm, gm = adjoint_source(mo, gp, syn, obs, w)
+    assert np.all(tm[[1, 6, 8]] == 0) and np.all(adj[[1, 6, 8]] == 0)
+    assert rel(adj, ref_adj) < 1e-4, rel(adj, ref_adj)
+    assert rel(tm, ref_tm) < 1e-4, (tm, ref_tm)
+    # adj_nt equal to the trace length is no resampling
+    t0 = dtw_time_shifts(_mo(form, dtw_amp_weight=kw["amp_weight"]), gp, syn, obs, w)
+    t1 = dtw_time_shifts(_mo(form, dtw_amp_weight=kw["amp_weight"], adj_nt=300), gp, syn, obs, w)
+    assert np.array_equal(t0, t1)
+
+
+def test_dtw_vector_adj_nt_matches_oracle():
+    gp, syn, obs, w = _vector_gathers()
+    ref_adj, ref_tm, ref_gm, ref_tau = D.adjoint_source_vector(gp, syn, obs, 2, w, dt=DT, tlag_max=TLAG,
+                                                               adj_nt=401)
+    mo = MisfitOpts(misfit=L.OWL_MISFIT_DTW_VECTOR, dt=DT, tlag_max=TLAG, ncomp=2, adj_nt=401)
+    tau = dtw_time_shifts(mo, gp, syn, obs, w)
+    assert np.max(np.abs(tau - ref_tau)) <= 1e-6, np.max(np.abs(tau - ref_tau))
+    assert np.array_equal(tau[0:4], tau[4:8]) and np.array_equal(tau[8:12], tau[12:16])
+    adj, tm, gm = adjoint_source(mo, gp, syn, obs, w)
+    assert rel(adj, ref_adj) < 1e-4, rel(adj, ref_adj)
+    assert np.allclose(gm, ref_gm, rtol=1e-4)
+
+
+def test_dtw_gradient_at_data_sampling():
+    """Data sampled at 2.5 ms on a 1 ms time axis: the gradient driver's DTW
+    shifts are computed at the time axis' nt samples (adj_nt's default), the
+    adjoint at the data sampling, resampled back before injection."""
+    import oracle.oracle_resample as R
+    nx, nz, dx, dt, nt = 48, 40, 10.0, 1e-3, 241
+    ddt = 2.5e-3
+    dnt = int(round((nt - 1) * dt / ddt)) + 1
+    d = desc(nx, nz, dx, dt, nt)
+    vp, rho = random_model(nx, nz)
+    ps = prepare(small_shots(nx, nz, dx), nx, nz, dx, dt)
+    obs = R.resample_rows(oracle.ac2d_forward(d, vp, rho, ps, "f64").reshape(-1, nt), dt, ddt, dnt)
+    obs = obs.astype(np.float32)
+    vp0 = (vp * np.float32(1.03)).astype(np.float32)
+    s = make_solver(d, vp0, rho)
+    s.set_data_sampling(dnt, ddt)
+    seis = np.zeros(s.seis_size(ps), dtype=np.float32)
+    mf, g = s.gradient_misfit(ps, obs.ravel(), MisfitOpts(misfit=L.OWL_MISFIT_DTW, tlag_max=0.02),
+                              RunOpts(checkpoint_interval=30), seis_out=seis)
+    # the oracle's DTW adjoint source (adj_nt = nt) of the GPU's own resampled synthetics
+    gp = s.gather_ptr(ps)
+    live = np.concatenate([[r.weight != 0 for r in sh.receivers] for sh in ps.shots]).astype(np.float64)
+    syn_d = seis.reshape(-1, dnt)
+    adj_d, tm, gm, _ = D.adjoint_source(gp, syn_d, obs, live, dt=ddt, tlag_max=0.02, adj_nt=nt)
+    assert rel(mf, gm) < 1e-4, (mf, gm)
+    adj_t = R.resample_rows(adj_d, ddt, dt, nt).astype(np.float32)
+    _, g_ref, _ = oracle.ac2d_gradient(d, vp0, rho, ps, adj_t.ravel(), adj_kind=1, k=30, precision="f64")
+    assert rel(g, g_ref) < 2e-4, rel(g, g_ref)
