@@ -208,7 +208,10 @@ typedef struct {
 /* Per-call execution options. Zero-initialised means defaults. */
 typedef struct {
     int shots_per_launch;     /* shots per batched launch; 0 = max_shots; 1 = plain per-shot path */
-    int checkpoint_interval;  /* k of every-k-step checkpoints; 0 = 50 */
+    int checkpoint_interval;  /* k of every-k-step checkpoints; 0 = 50; < 0: the whole run when the stored
+                                 stencil terms of every step fit in 60 % of the free device memory, else the
+                                 longest interval that fits. The forward stores the last segment's terms
+                                 itself, so k >= nt recomputes nothing */
     int checkpoint_precision; /* OWL_CKPT_* */
     int use_graph;            /* 1: capture the time loop in CUDA graphs (default when 0 is -1) */
     int shots_per_cta;        /* shots handled per CTA; 0 = autotuned */

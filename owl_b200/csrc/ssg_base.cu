@@ -223,6 +223,7 @@ void SsgBase::invalidate_graphs() {
     g_fwd.reset();
     g_rec.reset();
     g_adj.reset();
+    g_fst.reset();
 }
 
 DevBuf<long long>& SsgBase::seg_off() {
@@ -354,12 +355,15 @@ PointDev SsgBase::pdev(int S, bool adjoint, bool want_src_adj) {
     return q;
 }
 
+// kind 0: forward step; 1: recomputed step storing the stencil terms; 2:
+// adjoint step; 3: forward step storing the stencil terms (the last segment of
+// a gradient's forward, whose recompute it replaces)
 void SsgBase::launch_step(int kind, int S, const PointDev& q) {
     // point operators of shots with more than 1024 traces / target nodes use
     // NB CTAs per shot and a separate launch for the dependent phase
-    if (kind == 0 || kind == 1) {
-        launch_kernel(OWL_K_FWD_P, S, kind == 1);
-        launch_kernel(OWL_K_FWD_V, S, kind == 1);
+    if (kind != 2) {
+        launch_kernel(OWL_K_FWD_P, S, kind == 1 || kind == 3);
+        launch_kernel(OWL_K_FWD_V, S, kind == 1 || kind == 3);
         if (kind == 1) {
             launch_point_fwd(q, S, 1, PT_INJECT | PT_TICK, stream);
             launches += 3;
@@ -392,7 +396,7 @@ void SsgBase::run_steps(int kind, int n, int S, const PointDev& q, bool graph) {
         OWL_LAUNCH_CHECK();
         return;
     }
-    GraphCache& gc = kind == 0 ? g_fwd : (kind == 1 ? g_rec : g_adj);
+    GraphCache& gc = kind == 0 ? g_fwd : kind == 1 ? g_rec : kind == 3 ? g_fst : g_adj;
     std::vector<uintptr_t> sig = {(uintptr_t)n, (uintptr_t)S, (uintptr_t)spt_f, (uintptr_t)spt_a, (uintptr_t)tz_f,
                                   (uintptr_t)tz_a, (uintptr_t)cur_k, (uintptr_t)tile_x, (uintptr_t)st.p,
                                   (uintptr_t)ad.p, (uintptr_t)Sbuf.p, (uintptr_t)G.p, (uintptr_t)rec.p,
@@ -418,7 +422,7 @@ void SsgBase::run_steps(int kind, int n, int S, const PointDev& q, bool graph) {
         gc.sig = sig;
     }
     OWL_CUDA(cudaGraphLaunch(gc.exec, stream));
-    launches += (long long)n * (kind == 1 ? 3 : kind == 0 ? (nb_rec <= 4 ? 3 : 4) : (nb_sct <= 4 ? 3 : 4));
+    launches += (long long)n * (kind == 1 ? 3 : kind != 2 ? (nb_rec <= 4 ? 3 : 4) : (nb_sct <= 4 ? 3 : 4));
 }
 
 void SsgBase::resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bool& graph) {
@@ -428,6 +432,16 @@ void SsgBase::resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bo
     B = o.shots_per_launch > 0 ? o.shots_per_launch : std::max(1, desc.max_shots);
     B = std::min(B, std::max(1, nshots));
     k = o.checkpoint_interval > 0 ? o.checkpoint_interval : 50;
+    if (o.checkpoint_interval < 0) {
+        // the whole run as one segment when the stencil terms of every step fit
+        // in 60 % of the free device memory (the forward then stores them and
+        // nothing is recomputed), else the longest segment that fits
+        size_t fr = 0, tot = 0;
+        OWL_CUDA(cudaMemGetInfo(&fr, &tot));
+        const double per_step = 4.0 * nS * B * (double)fs;
+        const double room = 0.6 * (double)fr + (double)Sbuf.n * 4.0;  // the buffer held now is reused
+        k = per_step > 0 ? (int)std::max(1.0, std::min((double)desc.nt, std::floor(room / per_step))) : desc.nt;
+    }
     k = std::min(k, desc.nt);
     spt_f = spt_a = std::min(o.shots_per_cta > 0 ? o.shots_per_cta : 1, B);
     graph = o.use_graph >= 0;
@@ -531,7 +545,10 @@ void SsgBase::restore_ckpt(int slot, int S) {
     launches += 1;
 }
 
-void SsgBase::forward_batch(int S, int k, bool graph, bool save) {
+// save: a checkpoint at the start of every segment; store_last: the last
+// segment's steps store their stencil terms (slot t % k, as its recompute
+// would) and get no checkpoint
+void SsgBase::forward_batch(int S, int k, bool graph, bool save, bool store_last) {
     const int nt = desc.nt;
     cur_k = k;
     PointDev q = pdev(S, false, false);
@@ -542,9 +559,10 @@ void SsgBase::forward_batch(int S, int k, bool graph, bool save) {
     launches++;
     const int nseg = (nt + k - 1) / k;
     for (int sg = 0; sg < nseg; ++sg) {
-        if (save) save_ckpt(sg, S);
+        const bool last = store_last && sg == nseg - 1;
+        if (save && !last) save_ckpt(sg, S);
         const int n = std::min(k, nt - sg * k);
-        run_steps(0, n, S, q, graph && n == k);
+        run_steps(last ? 3 : 0, n, S, q, graph && n == k);
     }
 }
 
@@ -798,8 +816,8 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
         const size_t nitems = item_src.size();
         src_adj.reserve(std::max<size_t>(1, nitems * nt));
         if (want_src) OWL_CUDA(cudaMemsetAsync(src_adj.p, 0, sizeof(float) * std::max<size_t>(1, nitems * nt), stream));
-        // 1. forward with checkpoints
-        forward_batch(S, k, graph, true);
+        // 1. forward with checkpoints; the last segment stores its stencil terms
+        forward_batch(S, k, graph, true, true);
         if (o.check_every > 0) check_nonfinite(st.p, (size_t)S * sst);
         // 2. adjoint source and misfit
         const size_t n = (size_t)rtot * dnt();
@@ -842,16 +860,21 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
         }
         if (misfit) copy_out(misfit + shot0, misfit_d.p, sizeof(double) * S, mem);
         // 3. reverse sweep: restore a checkpoint, recompute its segment storing
-        //    the stencil terms, run the exact adjoint back through it
+        //    the stencil terms, run the exact adjoint back through it (the last
+        //    segment's terms are already stored by the forward)
         OWL_CUDA(cudaMemsetAsync(ad.p, 0, sizeof(float) * sad * S, stream));
         OWL_CUDA(cudaMemsetAsync(G.p, 0, sizeof(float) * 2 * ngrad * groups * fs, stream));
         PointDev qf = pdev(S, false, false);
         PointDev qa = pdev(S, true, want_src);
         for (int sg = nseg - 1; sg >= 0; --sg) {
             const int n0 = sg * k, nn = std::min(k, nt - n0);
-            restore_ckpt(sg, S);
-            set_step(n0);
-            run_steps(1, nn, S, qf, graph && nn == k);
+            if (sg == nseg - 1) {
+                set_step(nt);
+            } else {
+                restore_ckpt(sg, S);
+                set_step(n0);
+                run_steps(1, nn, S, qf, graph && nn == k);
+            }
             run_steps(2, nn, S, qa, graph && nn == k);
         }
         if (o.check_every > 0) check_nonfinite(ad.p, (size_t)S * sad);

@@ -87,7 +87,7 @@ struct SsgBase : Engine {
     DevBuf<int> inj_shot_ptr, rec_shot_ptr, sct_shot_ptr;
     DevBuf<unsigned char> live;
     DevBuf<long long> segbuf;  // st_segments offsets then lengths, on the device
-    GraphCache g_fwd, g_rec, g_adj;
+    GraphCache g_fwd, g_rec, g_adj, g_fst;
 
     long long launches = 0;
     int cur_k = 0, cur_S = 0, tile_x = 32;
@@ -173,7 +173,7 @@ struct SsgBase : Engine {
     void autotune(int S, int k, bool grad);
     void save_ckpt(int slot, int S);
     void restore_ckpt(int slot, int S);
-    void forward_batch(int S, int k, bool graph, bool save);
+    void forward_batch(int S, int k, bool graph, bool save, bool store_last = false);
     void check_nonfinite(const float* f, size_t n);
     void copy_out(void* dst, const void* src, size_t bytes, int mem);
     void fold_out(float* grad, int mem);

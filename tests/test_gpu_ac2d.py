@@ -64,8 +64,10 @@ def test_gradient_parity_small(fs):
     obs = oracle.ac2d_forward(d, vp, rho, ps, "f64").astype(np.float32)
     mf_ref, g_ref, _ = oracle.ac2d_gradient(d, vp0, rho, ps, obs, adj_kind=0, k=37, precision="f64")
     s = make_solver(d, vp0, rho)
+    # k >= nt and the memory-sized choice (-1): one segment, stored by the forward, no recompute
     for opts in (RunOpts(checkpoint_interval=37), RunOpts(checkpoint_interval=50, shots_per_launch=1, use_graph=-1),
-                 RunOpts(checkpoint_interval=20, shots_per_cta=3)):
+                 RunOpts(checkpoint_interval=20, shots_per_cta=3), RunOpts(checkpoint_interval=-1),
+                 RunOpts(checkpoint_interval=100000, use_graph=-1)):
         mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, opts)
         assert rel(mf, mf_ref) < 1e-4
         e = rel(g, g_ref)
