@@ -555,7 +555,9 @@ def main():
     shots_job = nshots * world
     value = ms_step / 1e3 / shots_job
     cells = (d.nx + 2 * d.pml) * (d.nz + 2 * d.pml)
-    gcells = 3.0 * cells * d.nt * shots_job / (ms_step / 1e3) / 1e9
+    kk = opts.checkpoint_interval
+    passes = 2.0 + (-(-d.nt // kk) - 1) * kk / d.nt  # forward, recompute of all but the last segment, adjoint
+    gcells = passes * cells * d.nt * shots_job / (ms_step / 1e3) / 1e9
 
     # e2e: same call through the C ABI with pinned host buffers (H2D of the
     # observed data and D2H of gradient + misfit inside the timed region)

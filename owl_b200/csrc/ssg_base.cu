@@ -583,7 +583,10 @@ void SsgBase::copy_out(void* dst, const void* src, size_t bytes, int mem) {
 
 void SsgBase::fill_info(owl_run_info& info, int nshots, int batches, bool grad) {
     info.gpu_launches = launches;
-    info.steps_cell_updates = (grad ? 3.0 : 1.0) * (double)NXp * NYp * NZp * desc.nt * nshots;
+    // a gradient: forward, recompute of all but the last segment, adjoint
+    const int kk = std::max(1, std::min(cur_k, desc.nt));
+    const double passes = grad ? 2.0 + (double)((desc.nt + kk - 1) / kk - 1) * kk / desc.nt : 1.0;
+    info.steps_cell_updates = passes * (double)NXp * NYp * NZp * desc.nt * nshots;
     info.dt_used = dt;
     info.dt_stable = dt_stable_;
     info.shots_per_cta = grad ? spt_a : spt_f;
