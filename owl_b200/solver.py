@@ -21,7 +21,7 @@ f32 = np.float32
 @dataclass
 class RunOpts:
     shots_per_launch: int = 0      # 0 = all shots of the call in one launch (<= max_shots)
-    checkpoint_interval: int = 50
+    checkpoint_interval: int = 50  # >= nt: one segment, stored by the forward, no recompute; -1: sized to free memory
     checkpoint_precision: int = L.OWL_CKPT_FP32
     use_graph: int = 0             # 0 / 1: CUDA graphs on; -1: plain launches
     shots_per_cta: int = 0
