@@ -93,7 +93,14 @@ struct DevBuf {
         if (count <= n && p) return false;
         release();
         size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-        OWL_CUDA(cudaMalloc(&p, bytes));
+        const cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            // a failed allocation leaves the handle usable: clear the runtime's
+            // last error so that the next launch check does not report it again
+            p = nullptr;
+            (void)cudaGetLastError();
+            OWL_CUDA(e);
+        }
         n = std::max<size_t>(count, 1);
         return true;
     }
