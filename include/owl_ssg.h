@@ -447,19 +447,22 @@ int owl_ssg_kernel_time(owl_ssg *h, int kernel_id, int nlaunch, double *avg_ms, 
 #define OWL_NOALLOC_MAX_FLOATS (16 * 1024 * 1024)
 
 /* One 2D acoustic shot (explosion sources, no free surface) modelled without
- * any device allocation, for callers that cannot call cudaMalloc: code running
- * while a stream is captured into a CUDA graph, or applications whose device
- * memory is reserved up front by another allocator. Materials, PML
+ * any device allocation (no counterpart in the reference), for callers that
+ * cannot call cudaMalloc where they model a shot: applications whose device
+ * memory is owned by another allocator or reserved up front as a fixed budget,
+ * where one more cudaMalloc fails or breaks the budget. Materials, PML
  * coefficients, wavefields and traces live in a static device array of
  * OWL_NOALLOC_MAX_FLOATS floats. Inputs and outputs are host memory: vp, rho as
  * for owl_ssg_set_model (nparam = 2), seis = nrec x nt floats in the layout of
  * owl_ssg_forward. The same seismograms as owl_ssg_forward. Returns
  * OWL_ERR_INVALID when the run needs more than OWL_NOALLOC_MAX_FLOATS floats.
- * The first call on a device looks up the array's device address; make it
- * before any stream capture starts. All calls share the array, which keeps the
- * last call's contents (each call clears what must start at zero); calls whose
- * GPU work overlapped would race on it, so the call holds a process-wide lock
- * and returns only after its GPU work has finished. */
+ * The first call on a device looks up the array's device address and keeps it
+ * for the process; make that first call before any stream capture starts. A
+ * call after cudaDeviceReset on that device is not supported. All calls share
+ * the array, which keeps the last call's contents (each call clears what must
+ * start at zero); calls whose GPU work overlapped would race on it, so the
+ * call holds a process-wide lock and returns only after its GPU work has
+ * finished. */
 int owl_ssg_forward_noalloc(const owl_ssg_desc *desc, int nparam, const float *const *fields,
                             const owl_shot *shot, float *seis);
 

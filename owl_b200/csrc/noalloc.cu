@@ -2,13 +2,12 @@
 // device memory.
 //
 // Who needs it: callers that cannot call cudaMalloc at the point where they
-// model a shot. Two common cases: code that runs while a stream is being
-// captured into a CUDA graph (cudaMalloc is not a stream operation and is not
-// allowed in a global-mode capture), and host applications whose device memory
-// is owned by another allocator or reserved up front as a fixed budget (for
-// instance a framework's caching allocator holding all of HBM), where an extra
-// cudaMalloc either fails or breaks the budget. The regular entry points
-// (owl_ssg_create / owl_ssg_forward) allocate their buffers on the handle.
+// model a shot -- host applications whose device memory is owned by another
+// allocator or reserved up front as a fixed budget (for instance a framework's
+// caching allocator holding all of HBM, or a service with a fixed per-process
+// device-memory quota), where one more cudaMalloc either fails or breaks the
+// budget. The regular entry points (owl_ssg_create / owl_ssg_forward) allocate
+// their buffers on the handle.
 //
 // How: every buffer of the run (padded materials, CFS-PML coefficients,
 // wavefields, PML memory, trace buffer, source and receiver descriptions)
@@ -17,8 +16,10 @@
 // array until the process exits. In host code the array's name is a host-side
 // stand-in, not a device address, so its device address is looked up with
 // cudaGetSymbolAddress once per device (with that device current) on the
-// first call made on that device, and cached. Make that first call before any
-// stream capture starts. All calls share the array and it keeps the last call's
+// first call made on that device, and kept for the life of the process. Make
+// that first call before any stream capture starts. A call made after
+// cudaDeviceReset on that device is not supported: the kept address dates from
+// before the reset. All calls share the array and it keeps the last call's
 // contents: each call clears what must start at zero. Calls whose GPU work
 // overlapped would race on the array; this entry point therefore holds a
 // process-wide lock for the whole call and returns only after its GPU work has

@@ -1,6 +1,6 @@
 """GPU test of owl_ssg_forward_noalloc, the forward entry point that allocates
-no device memory (for callers that cannot call cudaMalloc, e.g. code running
-under CUDA-graph stream capture or inside a fixed device-memory budget).
+no device memory (for callers that cannot call cudaMalloc because their
+device memory is owned by another allocator or reserved as a fixed budget).
 
 The file name sorts last so that pytest collects it after every other test:
 the entry point shares one static device array across calls and keeps the
