@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define OWL_SSG_ABI_VERSION 7
+#define OWL_SSG_ABI_VERSION 8
 
 /* status codes */
 #define OWL_OK 0
@@ -430,13 +430,18 @@ int owl_dtw_time_shifts(const owl_misfit_opts *mopts, int ngather, const int *ga
 #define OWL_K_FWD_V 1   /* velocity update with fused CFS-PML */
 #define OWL_K_ADJ_P 2   /* adjoint of the velocity update (writes p^) */
 #define OWL_K_ADJ_V 3   /* adjoint of the pressure update (writes v^) */
+#define OWL_K_FWD_P_STORE 4 /* OWL_K_FWD_P also writing the step's stencil terms (recomputed and last
+                               forward segments of a gradient) */
+#define OWL_K_FWD_V_STORE 5 /* OWL_K_FWD_V also writing the step's stencil terms */
 
 /* Times nlaunch back-to-back standalone launches of one kernel on the state of
  * the last batch of the last forward / gradient call (CUDA events on the
  * handle's stream). avg_ms: mean duration of one launch. alg_bytes: compulsory
  * HBM bytes of one launch (each state field read / written once per shot,
- * materials once per launch, PML memory only inside the PML). Leaves the
- * wavefields in an unspecified state. */
+ * materials once per launch, PML memory only inside the PML, the stored
+ * stencil terms of the _STORE variants once). The _STORE variants and the
+ * adjoint kernels need a gradient call first. Leaves the wavefields in an
+ * unspecified state. */
 int owl_ssg_kernel_time(owl_ssg *h, int kernel_id, int nlaunch, double *avg_ms, double *alg_bytes);
 
 /* ---- forward without device allocation (no counterpart in the reference) -- */

@@ -220,6 +220,8 @@ OWL_K_FWD_P = 0
 OWL_K_FWD_V = 1
 OWL_K_ADJ_P = 2
 OWL_K_ADJ_V = 3
+OWL_K_FWD_P_STORE = 4
+OWL_K_FWD_V_STORE = 5
 
 
 class OwlError(RuntimeError):

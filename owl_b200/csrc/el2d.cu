@@ -982,6 +982,8 @@ struct El2dEngine : SsgBase {
     // written once per shot, e terms written once and read once, materials once
     // per launch, PML memory and coefficients only inside the PML, gradient
     // accumulators (sum + compensation) once per shot group
+    int n_store_p() const override { return 3; }
+
     double alg_bytes(int id, int S, int groups) const override {
         const bool fsf = desc.free_surface != 0;
         const double rows_s = NZp - (fsf ? P : 0), rows_v = rows_s;

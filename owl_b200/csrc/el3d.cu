@@ -1058,6 +1058,8 @@ struct El3dEngine : SsgBase {
     // compulsory bytes per launch (fields once per shot, materials once per
     // launch, memories and e terms once, Kahan sums once per shot group);
     // PML memory traffic is not counted (it is a fraction of the shell)
+    int n_store_p() const override { return 6; }
+
     double alg_bytes(int id, int S, int groups) const override {
         const double cells = (double)NXp * NYp * NZp;
         switch (id) {

@@ -948,19 +948,25 @@ void SsgBase::source_gradient(int nshots, const owl_shot* shots, const float* ad
 
 void SsgBase::kernel_time(int id, int nlaunch, double* avg_ms, double* bytes) {
     OWL_CHECK(cur_S > 0, OWL_ERR_INVALID, "no batch has run on this handle");
-    OWL_CHECK(id >= OWL_K_FWD_P && id <= OWL_K_ADJ_V, OWL_ERR_INVALID, "bad kernel id");
+    OWL_CHECK(id >= OWL_K_FWD_P && id <= OWL_K_FWD_V_STORE, OWL_ERR_INVALID, "bad kernel id");
     const int S = cur_S;
-    OWL_CHECK(id < OWL_K_ADJ_P || (ad.p && G.p && Sbuf.p && ad.n >= (size_t)sad * S &&
-                                   Sbuf.n >= (size_t)nS * cur_k * S * fs),
-              OWL_ERR_INVALID, "adjoint kernels need a gradient call first");
+    const bool store = id == OWL_K_FWD_P_STORE || id == OWL_K_FWD_V_STORE;
+    const int kid = store ? id - OWL_K_FWD_P_STORE : id;
+    OWL_CHECK((kid < OWL_K_ADJ_P && !store) ||
+                  (ad.p && G.p && Sbuf.p && ad.n >= (size_t)sad * S && Sbuf.n >= (size_t)nS * cur_k * S * fs),
+              OWL_ERR_INVALID, "adjoint kernels and store variants need a gradient call first");
     set_step(cur_k);
-    for (int i = 0; i < 3; ++i) launch_kernel(id, S, false);
+    for (int i = 0; i < 3; ++i) launch_kernel(kid, S, store);
     OWL_LAUNCH_CHECK();
     EventTimer tm(stream);
-    for (int i = 0; i < nlaunch; ++i) launch_kernel(id, S, false);
+    for (int i = 0; i < nlaunch; ++i) launch_kernel(kid, S, store);
     OWL_LAUNCH_CHECK();
     *avg_ms = tm.stop_ms() / nlaunch;
-    *bytes = alg_bytes(id, S, (S + spt_a - 1) / spt_a);
+    *bytes = alg_bytes(kid, S, (S + spt_a - 1) / spt_a);
+    if (store) {
+        const int terms = kid == OWL_K_FWD_P ? n_store_p() : nS - n_store_p();
+        *bytes += 4.0 * terms * (double)S * NXp * NYp * NZp;
+    }
 }
 
 }  // namespace owl

@@ -127,6 +127,9 @@ struct SsgBase : Engine {
     virtual void scatter_map(const TapPt& t, std::vector<TapPt>& out) const { out.push_back(t); }
     virtual void launch_kernel(int id, int S, bool store) = 0;
     virtual double alg_bytes(int id, int S, int groups) const = 0;
+    // stencil terms written per cell by the store variant of the p / stress kernel
+    // (the velocity kernel writes the other nS - n_store_p)
+    virtual int n_store_p() const { return 1; }
     virtual void chain_rule(int S, int groups) = 0;  // += into gpad
     virtual int rho_param() const = 0;
     virtual float* st_field(int f) const = 0;  // base pointer (shot 0) of forward field f

@@ -1,7 +1,9 @@
-"""Shot sharding and the gradient all-reduce with world size 2 on gloo (CPU):
-the summed per-rank gradients equal the single-process gradient over all shots.
-The per-shot gradients come from the FP64 oracle here (no GPU needed); on GPUs
-the same rank logic runs with NCCL in bench.py."""
+"""Shot sharding and the FP64 gradient / misfit all-reduce with world size 2 on
+gloo (CPU), through owl_b200.dist.ShotSharding -- the rank logic bench.py runs
+with NCCL: the summed per-rank gradients equal the single-process gradient over
+all shots, and every shot's misfit lands at its index. The shards are uneven
+(3 shots: 2 on one rank, 1 on the other). The per-shot gradients come from the
+FP64 oracle here (no GPU needed)."""
 import os
 import socket
 
@@ -39,7 +41,7 @@ def _worker(rank, world, port, out, fail_rank):
     import torch.distributed as dist
     import oracle
     from cases import prepare
-    from owl_b200.dist import allreduce_sum, shard_shots
+    from owl_b200.dist import ShotSharding
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=20))
@@ -47,13 +49,15 @@ def _worker(rank, world, port, out, fail_rank):
         if rank == fail_rank:
             raise RuntimeError("injected rank failure")
         d, vp, rho, shots, (nx, nz, dx, dt) = _case()
-        mine = shard_shots(shots, rank, world)
-        ps = prepare([shots[i] for i in mine], nx, nz, dx, dt)
+        sh = ShotSharding(shots, rank, world)
+        ps = prepare(sh.local(shots), nx, nz, dx, dt)
         obs = oracle.ac2d_forward(d, vp * 1.03, rho, ps, "f64")
-        _, g, _ = oracle.ac2d_gradient(d, vp, rho, ps, obs, adj_kind=0, k=30)
-        t = torch.from_numpy(g.copy())
-        allreduce_sum(t)
-        out[rank] = t.numpy().tolist()
+        mf, g, _ = oracle.ac2d_gradient(d, vp, rho, ps, obs, adj_kind=0, k=30)
+        # the rank's FP32 gradient, as the library returns it, summed in FP64
+        g64, m64 = sh.reduce(torch.from_numpy(g.astype(np.float32)), torch.from_numpy(mf))
+        oom_anywhere = sh.any_rank(rank == 1)
+        out[rank] = {"mine": sh.mine, "g": g64.numpy().tolist(), "m": m64.numpy().tolist(),
+                     "dtype": str(g64.dtype), "any": oom_anywhere}
     except Exception as e:  # the failing rank leaves between steps; the peer's collective errors out
         out[rank] = repr(e)
     finally:
@@ -92,13 +96,20 @@ def test_allreduce_gradient_world2():
     from cases import prepare
     res = _run(2)
     assert set(res) == {0, 1}
-    g0, g1 = np.array(res[0]), np.array(res[1])
+    r0, r1 = res[0], res[1]
+    assert isinstance(r0, dict) and isinstance(r1, dict), (r0, r1)
+    assert sorted(r0["mine"] + r1["mine"]) == [0, 1, 2] and len(r0["mine"]) != len(r1["mine"])
+    assert r0["dtype"] == "torch.float64" and r0["any"] and r1["any"]
+    g0, g1 = np.array(r0["g"]), np.array(r1["g"])
+    assert np.array_equal(g0, g1) and np.array_equal(np.array(r0["m"]), np.array(r1["m"]))
     d, vp, rho, shots, (nx, nz, dx, dt) = _case()
     ps = prepare(shots, nx, nz, dx, dt)
     obs = oracle.ac2d_forward(d, vp * 1.03, rho, ps, "f64")
-    _, g, _ = oracle.ac2d_gradient(d, vp, rho, ps, obs, adj_kind=0, k=30)
-    assert np.allclose(g0, g1, rtol=0, atol=0)
-    assert np.linalg.norm(g0 - g) <= 1e-12 * np.linalg.norm(g)
+    mf, g, _ = oracle.ac2d_gradient(d, vp, rho, ps, obs, adj_kind=0, k=30)
+    # per-rank FP32 gradients summed in FP64: within FP32 rounding of the FP64 total
+    assert np.linalg.norm(g0 - g) <= 1e-6 * np.linalg.norm(g)
+    # misfits are per shot, each computed by one rank: exact at their global index
+    assert np.allclose(np.array(r0["m"]), mf, rtol=1e-12, atol=0)
 
 
 def test_rank_failure_surfaces_as_error():
