@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--profile3d-grad", type=int, default=0, metavar="N",
                    help="profiling target: one 3D acoustic gradient of an N^3 model, 1 shot, 60 steps, no JSON line")
     p.add_argument("--no-elastic", action="store_true", help="skip the 2D elastic VTI block")
+    p.add_argument("--el3-grad-shots", type=int, default=16,
+                   help="shots of the 3D elastic gradient at the workload's size (0: none)")
     p.add_argument("--profile-el", type=int, default=0, metavar="S",
                    help="profiling target: one 2D elastic VTI gradient of S shots, 60 steps, no JSON line")
     p.add_argument("--ring", action="store_true", help="--profile-el3 with the ring forward kernels")
@@ -243,12 +245,14 @@ def elastic_2d_block(peak, peak_kind, ngrad=16):
     return out
 
 
-def elastic_3d_block(peak, peak_kind, nshots=4, nt=500):
-    """3D elastic orthorhombic (nine Cij) on the 256^3 model (296^3 padded cells),
-    `nshots` vertical-force shots and `nt` steps of the 2500-step workload:
-    forward Gcell-updates/s and the HBM roofline of the four stencil kernels
-    (after a gradient of one shot of a 96^3 model, 300 steps, which sets up the
-    adjoint state the adjoint kernels are timed on)."""
+def elastic_3d_block(peak, peak_kind, nshots=4, nt=500, grad_shots=16):
+    """3D elastic orthorhombic (nine Cij) on the 256^3 model (296^3 padded cells):
+    forward of `nshots` of the 16 vertical-force shots over `nt` of the 2500
+    steps (Gcell-updates/s, HBM roofline of the two forward stencil kernels),
+    then the gradient w.r.t. the nine Cij and rho of `grad_shots` shots over all
+    2500 steps with FP16 checkpoints, shots per batch and checkpoint interval
+    chosen by the memory planner (s/shot, HBM roofline of the two adjoint
+    kernels on that gradient's state)."""
     import numpy as np
     from owl_b200 import _lib as L
     from owl_b200 import configs
@@ -277,28 +281,36 @@ def elastic_3d_block(peak, peak_kind, nshots=4, nt=500):
                                 "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
                                 "shots_per_launch": nshots, "traffic": profile_traffic(name)}
     s.close()
-    # gradient of one shot on a 96^3 model (the full model's checkpoints would not fit)
-    m = 96
-    dg, fg, shg = configs.config5(1, nt=300, n=m, nrec=32)
+    if grad_shots <= 0:
+        return out
+    # the gradient at the workload's size: all 2500 steps, FP16 checkpoints
+    dg, fg, shg = configs.config5(16, nt=2500)
+    shg = shg[:grad_shots]
     g = SSGSolver(L.OWL_ELASTIC_VHTIORT_3D, dg.nx, dg.nz, dg.dx, dg.dz, dg.dt, dg.nt, pml=dg.pml, fdhalf=dg.fdhalf,
-                  f0_max=dg.f0_max, max_shots=1, ny=dg.ny, dy=dg.dy, aniso=dg.aniso)
+                  f0_max=dg.f0_max, max_shots=len(shg), ny=dg.ny, dy=dg.dy, aniso=dg.aniso)
     g.set_model(*fg)
     pg = g.prepare(shg)
     obs = np.zeros(g.seis_size(pg), dtype=np.float32)
-    g.gradient(pg, obs, opts=RunOpts(checkpoint_precision=L.OWL_CKPT_FP16))
-    _, gr = g.gradient(pg, obs, opts=RunOpts(checkpoint_precision=L.OWL_CKPT_FP16))
+    go = RunOpts(checkpoint_precision=L.OWL_CKPT_FP16, checkpoint_interval=-1)
+    _, gr = g.gradient(pg, obs, opts=go)
+    info = g.last_info
     out["gradient_finite"] = bool(np.all(np.isfinite(np.asarray(gr))))
-    out["gradient_workload"] = "96^3 model of the same kind (136^3 padded), 300 steps, 1 shot, FP16 checkpoints"
-    out["gradient_s_per_shot"] = g.last_info.elapsed_ms / 1e3
-    ring_a = g.last_info.tile_z == 1
+    out["gradient_workload"] = (f"{grad_shots} of the 16 shots, all 2500 steps, 256^3 model (296^3 padded), "
+                                f"gradient w.r.t. c11, c12, c13, c22, c23, c33, c44, c55, c66, rho, FP16 checkpoints, "
+                                f"L2 misfit against zero data")
+    out["gradient_s_per_shot"] = info.elapsed_ms / 1e3 / len(shg)
+    out["gradient_plan"] = {"shots_per_batch": info.shots_per_launch, "checkpoint_interval": info.checkpoint_interval,
+                            "batches": info.batches}
+    ring_a = info.tile_z == 1
     out["adjoint_kernels"] = "z-marching ring" if ring_a else "thread per cell"
     for kid, name in ((L.OWL_K_ADJ_P, "k_el3d_adj_v_ring" if ring_a else "k_el3d_adj_v"),
                       (L.OWL_K_ADJ_V, "k_el3d_adj_s_ring" if ring_a else "k_el3d_adj_s")):
-        kms, b = g.kernel_time(kid, 10)
+        kms, b = g.kernel_time(kid, 5)
         ach = b / (kms / 1e3) / 1e9
         out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                                 "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
-                                "shots_per_launch": 1, "model": "96^3", "traffic": profile_traffic(name)}
+                                "shots_per_launch": info.shots_per_launch, "model": "256^3",
+                                "traffic": profile_traffic(name)}
     g.close()
     return out
 
@@ -753,7 +765,7 @@ def main():
         line["forward_3d"] = forward_3d_block(peak, peak_kind)
     if extras and not args.no_elastic:
         line["elastic_2d"] = elastic_2d_block(peak, peak_kind)
-        line["elastic_3d"] = elastic_3d_block(peak, peak_kind)
+        line["elastic_3d"] = elastic_3d_block(peak, peak_kind, grad_shots=args.el3_grad_shots)
 
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -230,6 +230,8 @@ module owl_ssg_c
         integer(c_int) :: tile_x
         integer(c_int) :: tile_z
         integer(c_int) :: batches
+        integer(c_int) :: checkpoint_interval
+        integer(c_int) :: shots_per_launch
     end type
 
     interface

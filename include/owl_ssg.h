@@ -207,11 +207,12 @@ typedef struct {
 
 /* Per-call execution options. Zero-initialised means defaults. */
 typedef struct {
-    int shots_per_launch;     /* shots per batched launch; 0 = max_shots; 1 = plain per-shot path */
-    int checkpoint_interval;  /* k of every-k-step checkpoints; 0 = 50; < 0: the whole run when the stored
-                                 stencil terms of every step fit in 60 % of the free device memory, else the
-                                 longest interval that fits. The forward stores the last segment's terms
-                                 itself, so k >= nt recomputes nothing */
+    int shots_per_launch;     /* shots per batched launch; 0 = the most up to max_shots whose buffers fit
+                                 the free device memory; 1 = plain per-shot path */
+    int checkpoint_interval;  /* k of every-k-step checkpoints; 0 = 50; < 0: the whole run when every
+                                 buffer of the batch fits the free device memory with the stored stencil
+                                 terms of every step, else the longest interval that fits. The forward
+                                 stores the last segment's terms itself, so k >= nt recomputes nothing */
     int checkpoint_precision; /* OWL_CKPT_* */
     int use_graph;            /* 1: capture the time loop in CUDA graphs (default when 0 is -1) */
     int shots_per_cta;        /* shots handled per CTA; 0 = autotuned */
@@ -229,6 +230,8 @@ typedef struct {
     int shots_per_cta;
     int tile_x, tile_z;
     int batches;
+    int checkpoint_interval;  /* gradients: the interval used (opts, or chosen from free device memory) */
+    int shots_per_launch;     /* shots per batched launch used (opts, or the most that fit the device) */
 } owl_run_info;
 
 /* ---- lifecycle ---------------------------------------------------------- */

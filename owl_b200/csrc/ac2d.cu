@@ -14,10 +14,18 @@
 // only inside the PML), shot-major. Material coefficients shared by all shots:
 // dtbk = dt*rho*vp^2, dtbx = dt/rho_eff_x, dtbz = dt/rho_eff_z.
 //
-// One time step is three launches over all shots of a batch:
-//   k_ac2d_fwd_p : p -= dtbk * (dx vx + dz vz), CFS-PML memory fused
-//   k_ac2d_fwd_v : vx -= dtbx * dx p ; vz -= dtbz * dz p, CFS-PML memory fused
-//   point kernel : add_source(t), receivers of step t+1, step counter (ssg_base.cu)
+// One time step is two launches over all shots of a batch:
+//   k_ac2d_fwd_p : the explosion sources of step t-1 added by the owner of each
+//                  tap node (deferred from the end of step t-1, where the
+//                  reference adds them after the velocity update), then
+//                  p -= dtbk * (dx vx + dz vz), CFS-PML memory fused
+//   k_ac2d_fwd_v : vx -= dtbx * dx p ; vz -= dtbz * dz p, CFS-PML memory fused,
+//                  force sources of step t added by the tap nodes' owners; extra
+//                  CTAs record the receivers of step t+1 from p plus the pending
+//                  explosion taps; the last CTA advances the step counter
+// The values are those of the reference's order (update, add_source, sample)
+// to the bit. A batch whose taps fall outside the nodes a kernel updates keeps
+// the separate point kernel of ssg_base.cu (three launches per step).
 #include <algorithm>
 #include <cmath>
 
@@ -26,6 +34,22 @@
 namespace owl {
 
 __constant__ float c_fd2[8];
+
+// point work fused into the stencil kernels (FZ_* modes of ssg_base.cuh)
+struct Ac2dPt {
+    const int* item_ptr;  // injection items of shot s: [item_ptr[s], item_ptr[s + 1])
+    const int4* box;      // per item: field, x0, -, z0 (storage coordinates of its 9 x 9 box)
+    const float* bw;      // per item: 81 weights [z][x]
+    const float* amp;     // per item: nt amplitudes (stf * amp * dt)
+    int nt, rtot, nb, mode, rows_blk;
+    const int* rec_ptr;   // receivers (traces) of shot s: [rec_ptr[s], rec_ptr[s + 1])
+    CSRView smp;
+    float* rec;
+    const int* sct_shot_ptr;  // scatter targets of shot s
+    CSRView sct;
+    const float* res;
+    int* d_done;
+};
 
 struct Ac2dDev {
     int nx, nz, P, R, pr, pitch;
@@ -43,18 +67,38 @@ struct Ac2dDev {
     float *ap, *avx, *avz, *am1, *am2, *am3, *am4;
     float *aex, *aez, *aepx, *aepz;
     float *Gbk, *Gbx, *Gbz, *Cbk, *Cbx, *Cbz;
+    Ac2dPt pt;
 };
 
 __device__ __forceinline__ bool pml_int(int x, int pr, int n) { return x < pr || x >= pr + n; }
 __device__ __forceinline__ bool pml_half(int x, int pr, int n) { return x <= pr || x >= pr + n; }
 
+// v + the injection of step index ti (0-based) of shot s's sources on field f
+// at storage node (x, z), items in order as add_source loops them; taps of
+// weight 0 are not taps
+__device__ __forceinline__ float ac2d_inj(const Ac2dPt& q, int s, int f, int x, int z, int ti, float v) {
+    if ((unsigned)ti >= (unsigned)q.nt) return v;
+    const int i1 = q.item_ptr[s + 1];
+    for (int it = q.item_ptr[s]; it < i1; ++it) {
+        const int4 b = q.box[it];
+        const unsigned dx = (unsigned)(x - b.y), dz = (unsigned)(z - b.w);
+        if (b.x == f && dx < (unsigned)BOX_W && dz < (unsigned)BOX_W) {
+            const float A = q.amp[(size_t)it * q.nt + ti];
+            const float w = q.bw[(size_t)it * (BOX_W * BOX_W) + dz * BOX_W + dx];
+            if (A != 0.f && w != 0.f) v = v + A * w;
+        }
+    }
+    return v;
+}
+
 // ------------------------------- forward ------------------------------------
-template <int R, bool STORE>
+template <int R, bool STORE, bool FUSE>
 __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
     pdl_prologue();
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = a.zp0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
+    const int cur = FUSE ? *a.d_step : 0;
     const long long o = (long long)z * a.pitch + x;
     const float dtbk = a.dtbk[o];
     const bool px = pml_int(x, a.pr, a.nx);
@@ -74,7 +118,10 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
         // one allocation, so no plain read could move above a store; the
         // neighbours' fields, which this launch does not write, are read
         // through the read-only path
-        const float p0 = a.p[so], m1 = px ? a.m1[so] : 0.f, m2 = pz ? a.m2[so] : 0.f;
+        float p0 = a.p[so];
+        const float m1 = px ? a.m1[so] : 0.f, m2 = pz ? a.m2[so] : 0.f;
+        // explosion sources of step t-1 (cur), added where add_source would have
+        if (FUSE && (a.pt.mode & FZ_INJ)) p0 = ac2d_inj(a.pt, s, 0, x, z, cur - 1, p0);
         float sx = 0.f, sz = 0.f;
 #pragma unroll
         for (int k = 1; k <= R; ++k) sx = sx + c_fd2[k - 1] * (__ldg(vx + k) - __ldg(vx + 1 - k));
@@ -99,9 +146,29 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
     }
 }
 
-template <int R, bool STORE>
-__global__ void __launch_bounds__(512) k_ac2d_fwd_v(Ac2dDev a) {
-    pdl_prologue();
+// receivers of step t+1 (cur + 2) of shot s from p and the pending explosion
+// taps of step t (cur), each trace a sequential sum over its taps (the
+// sampling of submodule_forward_modeling.f90:58-79 after add_source)
+__device__ __forceinline__ void ac2d_sample(const Ac2dDev& a, int cur) {
+    const Ac2dPt& q = a.pt;
+    const int cta = (blockIdx.y - q.rows_blk) * gridDim.x + blockIdx.x;
+    const int s = cta / q.nb, part = cta % q.nb, tr = cur + 2;
+    if (blockIdx.z != 0 || s >= a.nshots || tr > q.nt) return;
+    const int nthr = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const float* p = a.p + s * a.sst;
+    for (int r = q.rec_ptr[s] + part * nthr + tid; r < q.rec_ptr[s + 1]; r += q.nb * nthr) {
+        float acc = 0.f;
+        for (int j = q.smp.ptr[r]; j < q.smp.ptr[r + 1]; ++j) {
+            const long long off = q.smp.off[j];
+            const int zz = (int)(off / a.pitch), xx = (int)(off - (long long)zz * a.pitch);
+            acc = acc + ac2d_inj(q, s, 0, xx, zz, cur, p[off]) * q.smp.w[j];
+        }
+        q.rec[(size_t)(tr - 1) * q.rtot + r] = acc;
+    }
+}
+
+template <int R, bool STORE, bool FUSE>
+__device__ __forceinline__ void ac2d_fwd_v_cells(const Ac2dDev& a, int cur) {
     const int zr0 = min(a.zvx0, a.zvz0);
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -132,7 +199,9 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_v(Ac2dDev a) {
                 a.m3[so] = m;
                 h = h + m;
             }
-            a.vx[so] = vx0 - bxc * h;
+            float vn = vx0 - bxc * h;
+            if (FUSE && (a.pt.mode & FZ_INJ)) vn = ac2d_inj(a.pt, s, 1, x, z, cur, vn);  // force sources of step t
+            a.vx[so] = vn;
             if (STORE) a.Svx[slot + s * a.fs + o] = h;
         }
         if (doz) {
@@ -145,10 +214,24 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_v(Ac2dDev a) {
                 a.m4[so] = m;
                 h = h + m;
             }
-            a.vz[so] = vz0 - bzc * h;
+            float vn = vz0 - bzc * h;
+            if (FUSE && (a.pt.mode & FZ_INJ)) vn = ac2d_inj(a.pt, s, 2, x, z, cur, vn);
+            a.vz[so] = vn;
             if (STORE) a.Svz[slot + s * a.fs + o] = h;
         }
     }
+}
+
+template <int R, bool STORE, bool FUSE>
+__global__ void __launch_bounds__(512) k_ac2d_fwd_v(Ac2dDev a) {
+    pdl_prologue();
+    const int cur = FUSE ? *a.d_step : 0;
+    if (FUSE && (int)blockIdx.y >= a.pt.rows_blk) {
+        if (a.pt.mode & FZ_SMP) ac2d_sample(a, cur);
+    } else {
+        ac2d_fwd_v_cells<R, STORE, FUSE>(a, cur);
+    }
+    if (FUSE && (a.pt.mode & FZ_TICK)) tick_last_block(a.d_step, a.pt.d_done, 1);
 }
 
 // ------------------------------- adjoint ------------------------------------
@@ -244,9 +327,26 @@ __global__ void __launch_bounds__(512) k_ac2d_adj_p(Ac2dDev a) {
     if (ownz) { sm = a.Gbz[go]; c = a.Cbz[go]; kahan_add(sm, c, gbz); a.Gbz[go] = sm; a.Cbz[go] = c; }
 }
 
+// adjoint of the sampling of step t: the residual of step t into p^ at the
+// receivers' tap nodes, one thread per target node, its contributions summed in
+// a fixed order (k_point_adj's scatter phase)
+__device__ __forceinline__ void ac2d_scatter(const Ac2dDev& a, int t) {
+    const Ac2dPt& q = a.pt;
+    const int cta = (blockIdx.y - q.rows_blk) * gridDim.x + blockIdx.x;
+    const int s = cta / q.nb, part = cta % q.nb;
+    if (blockIdx.z != 0 || s >= a.nshots || t < 1) return;
+    const int nthr = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int it = q.sct_shot_ptr[s] + part * nthr + tid; it < q.sct_shot_ptr[s + 1]; it += q.nb * nthr) {
+        float acc = 0.f;
+        const int j0 = q.sct.ptr[it], j1 = q.sct.ptr[it + 1];
+        for (int j = j0; j < j1; ++j) acc = acc + q.res[(size_t)(t - 1) * q.rtot + q.sct.item[j]] * q.sct.w[j];
+        float* f = a.ap + s * a.sad + q.sct.off[j0];
+        *f = *f + acc;
+    }
+}
+
 template <int R>
-__global__ void __launch_bounds__(512) k_ac2d_adj_v(Ac2dDev a) {
-    pdl_prologue();
+__device__ __forceinline__ void ac2d_adj_v_cells(const Ac2dDev& a) {
     const int zr0 = min(a.zvx0, a.zvz0);
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -298,6 +398,17 @@ __global__ void __launch_bounds__(512) k_ac2d_adj_v(Ac2dDev a) {
             a.aez[sa] = e;
         }
     }
+}
+
+template <int R, bool FUSE>
+__global__ void __launch_bounds__(512) k_ac2d_adj_v(Ac2dDev a) {
+    pdl_prologue();
+    if (FUSE && (int)blockIdx.y >= a.pt.rows_blk) {
+        if (a.pt.mode & FZ_SCT) ac2d_scatter(a, *a.d_step);
+    } else {
+        ac2d_adj_v_cells<R>(a);
+    }
+    if (FUSE && (a.pt.mode & FZ_TICK)) tick_last_block(a.d_step, a.pt.d_done, -1);
 }
 
 // ------------------------- FP64 chain rule ---------------------------------
@@ -359,6 +470,18 @@ struct Ac2dEngine : SsgBase {
         nparam = 2;
         ncomp = 1;
         for (int f = 0; f < 7; ++f) st_segments.push_back({f * fs, fs});
+    }
+
+    // injection, sampling and the residual scatter run inside the stencil
+    // kernels when every source tap lies on a node its kernel updates and the
+    // receivers sample p
+    bool fuse_supported() const override { return true; }
+    bool fuse_tap_ok(int field, int x, int, int z, bool sampling) const override {
+        const bool fsf = desc.free_surface != 0;
+        if (sampling) return field == 0;
+        const int x0 = R, x1 = R + NXp, z1 = R + NZp;
+        const int z0 = field == 0 ? (fsf ? pr + 1 : R) : field == 1 ? (fsf ? pr : R) : (fsf ? pr + 1 : R);
+        return field >= 0 && field <= 2 && x >= x0 && x < x1 && z >= z0 && z < z1;
     }
 
     float* st_field(int f) const override { return f < 3 ? st.p + f * fs : nullptr; }
@@ -499,6 +622,12 @@ struct Ac2dEngine : SsgBase {
             a.Gbk = G.p; a.Gbx = G.p + gg; a.Gbz = G.p + 2 * gg;
             a.Cbk = G.p + 3 * gg; a.Cbx = G.p + 4 * gg; a.Cbz = G.p + 5 * gg;
         }
+        Ac2dPt& q = a.pt;
+        q.item_ptr = inj_shot_ptr.p; q.box = inj_box.p; q.bw = inj_bw.p; q.amp = amp.p;
+        q.nt = desc.nt; q.rtot = rtot; q.nb = 1; q.mode = fz_mode; q.rows_blk = 1 << 30;
+        q.rec_ptr = rec_shot_ptr.p; q.smp = view(smp); q.rec = rec.p;
+        q.sct_shot_ptr = sct_shot_ptr.p; q.sct = view(sct); q.res = res.p;
+        q.d_done = ctr.p + 1;
         return a;
     }
 
@@ -507,21 +636,47 @@ struct Ac2dEngine : SsgBase {
         Ac2dDev a = dev(S);
         const int rows_p = a.z1 - a.zp0, rows_v = a.z1 - std::min(a.zvx0, a.zvz0);
         const int rows_a = a.z1 - std::min(std::min(a.zvx0, a.zvz0), a.zp0);
+        const bool fz = fz_mode != 0;
+        // extra CTA rows after the stencil rows for the sampling / scatter work, nb CTAs per shot
+        auto add_point_rows = [&](dim3& g, int nb) {
+            a.pt.rows_blk = (int)g.y;
+            a.pt.nb = nb;
+            g.y += (S * nb + g.x - 1) / g.x;
+        };
         if (id == OWL_K_FWD_P || id == OWL_K_FWD_V) {
             a.spt = spt_f;
             dim3 b(tile_x, tz_f);
             if (id == OWL_K_FWD_P) {
-                if (store) launch_pdl(k_ac2d_fwd_p<RR, true>, grid_for(rows_p, S, spt_f, tz_f), b, 0, stream, a);
-                else launch_pdl(k_ac2d_fwd_p<RR, false>, grid_for(rows_p, S, spt_f, tz_f), b, 0, stream, a);
+                dim3 g = grid_for(rows_p, S, spt_f, tz_f);
+                if (store) {
+                    if (fz) launch_pdl(k_ac2d_fwd_p<RR, true, true>, g, b, 0, stream, a);
+                    else launch_pdl(k_ac2d_fwd_p<RR, true, false>, g, b, 0, stream, a);
+                } else {
+                    if (fz) launch_pdl(k_ac2d_fwd_p<RR, false, true>, g, b, 0, stream, a);
+                    else launch_pdl(k_ac2d_fwd_p<RR, false, false>, g, b, 0, stream, a);
+                }
             } else {
-                if (store) launch_pdl(k_ac2d_fwd_v<RR, true>, grid_for(rows_v, S, spt_f, tz_f), b, 0, stream, a);
-                else launch_pdl(k_ac2d_fwd_v<RR, false>, grid_for(rows_v, S, spt_f, tz_f), b, 0, stream, a);
+                dim3 g = grid_for(rows_v, S, spt_f, tz_f);
+                if (fz && (fz_mode & FZ_SMP)) add_point_rows(g, nb_rec);
+                if (store) {
+                    if (fz) launch_pdl(k_ac2d_fwd_v<RR, true, true>, g, b, 0, stream, a);
+                    else launch_pdl(k_ac2d_fwd_v<RR, true, false>, g, b, 0, stream, a);
+                } else {
+                    if (fz) launch_pdl(k_ac2d_fwd_v<RR, false, true>, g, b, 0, stream, a);
+                    else launch_pdl(k_ac2d_fwd_v<RR, false, false>, g, b, 0, stream, a);
+                }
             }
         } else {
             a.spt = spt_a;
             dim3 b(tile_x, tz_a);
-            if (id == OWL_K_ADJ_P) launch_pdl(k_ac2d_adj_p<RR>, grid_for(rows_a, S, spt_a, tz_a), b, 0, stream, a);
-            else launch_pdl(k_ac2d_adj_v<RR>, grid_for(rows_v, S, spt_a, tz_a), b, 0, stream, a);
+            if (id == OWL_K_ADJ_P) {
+                launch_pdl(k_ac2d_adj_p<RR>, grid_for(rows_a, S, spt_a, tz_a), b, 0, stream, a);
+            } else {
+                dim3 g = grid_for(rows_v, S, spt_a, tz_a);
+                if (fz && (fz_mode & FZ_SCT)) add_point_rows(g, nb_sct);
+                if (fz) launch_pdl(k_ac2d_adj_v<RR, true>, g, b, 0, stream, a);
+                else launch_pdl(k_ac2d_adj_v<RR, false>, g, b, 0, stream, a);
+            }
         }
     }
     void launch_kernel(int id, int S, bool store) override {

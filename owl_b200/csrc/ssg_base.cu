@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 #include <map>
 
 #include "ssg_base.cuh"
@@ -247,6 +248,10 @@ void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
     h_gather_ptr.assign(1, 0);
     std::vector<float> hamp;
     std::vector<unsigned char> hlive;
+    std::vector<int4> hbox;
+    std::vector<float> hbw;
+    const size_t boxn = dim == 3 ? (size_t)BOX_W * BOX_W * BOX_W : (size_t)BOX_W * BOX_W;
+    bool fuse = fuse_supported();
     item_src.clear(); item_comp.clear(); item_shot.clear(); item_rho_cell.clear(); item_rho.clear();
     const int nt = desc.nt;
     std::vector<TapPt> taps, mapped;
@@ -264,12 +269,29 @@ void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
                 long long rc = -1;
                 float rv = 0.f;
                 src_taps(q, comp, taps, rc, rv);
+                int bi = 1 << 30, bj = 1 << 30, bk = 1 << 30, bf = -1;
                 for (const TapPt& t : taps) {
                     if (t.w == 0.f) continue;
                     OWL_CHECK(in_wavefield(t.i, t.j, t.k), OWL_ERR_INVALID, "source tap outside the padded grid");
                     hinj.push(Tap{t.field, s, soff(t.i, t.j, t.k), t.w, 0});
+                    bi = std::min(bi, t.i); bj = std::min(bj, t.j); bk = std::min(bk, t.k);
+                    if (bf < 0) bf = t.field;
+                    if (bf != t.field) fuse = false;
                 }
                 hinj.close_item();
+                {
+                    const size_t base = hbw.size();
+                    hbw.resize(base + boxn, 0.f);
+                    if (bf < 0) { bi = bj = bk = -(1 << 20); bf = 0; }
+                    hbox.push_back(int4{bf, bi + pr - 1, dim == 3 ? bj + pr - 1 : 0, bk + pr - 1});
+                    for (const TapPt& t : taps) {
+                        if (t.w == 0.f) continue;
+                        const int dx = t.i - bi, dy = dim == 3 ? t.j - bj : 0, dz = t.k - bk;
+                        if (dx >= BOX_W || dy >= BOX_W || dz >= BOX_W) { fuse = false; continue; }
+                        hbw[base + ((size_t)dz * (dim == 3 ? BOX_W : 1) + dy) * BOX_W + dx] = t.w;
+                        fuse &= fuse_tap_ok(t.field, t.i + pr - 1, dim == 3 ? t.j + pr - 1 : 0, t.k + pr - 1, false);
+                    }
+                }
                 item_src.push_back(kk); item_comp.push_back(comp); item_shot.push_back(s);
                 item_rho_cell.push_back(rc); item_rho.push_back(rv);
                 size_t base = hamp.size();
@@ -292,11 +314,15 @@ void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
                         if (t.w == 0.f) continue;
                         OWL_CHECK(in_wavefield(t.i, t.j, t.k), OWL_ERR_INVALID, "receiver tap outside the padded grid");
                         hsmp.push(Tap{t.field, s, soff(t.i, t.j, t.k), t.w, rg});
+                        fuse &= fuse_tap_ok(t.field, t.i + pr - 1, dim == 3 ? t.j + pr - 1 : 0, t.k + pr - 1, true);
                         if (need_sct) {
                             mapped.clear();
                             scatter_map(t, mapped);
-                            for (const TapPt& m : mapped)
+                            for (const TapPt& m : mapped) {
                                 cells[{m.field, soff(m.i, m.j, m.k)}].push_back({rg, m.w});
+                                fuse &= fuse_tap_ok(m.field, m.i + pr - 1, dim == 3 ? m.j + pr - 1 : 0, m.k + pr - 1,
+                                                    true);
+                            }
                         }
                     }
                 }
@@ -325,6 +351,10 @@ void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
     sct_shot_ptr.upload(hsct_ptr.data(), hsct_ptr.size(), stream);
     amp.upload(hamp.data(), hamp.size(), stream);
     live.upload(hlive.data(), hlive.size(), stream);
+    if (hbox.empty()) { hbox.push_back(int4{-1, 0, 0, 0}); hbw.resize(boxn, 0.f); }
+    inj_box.upload(hbox.data(), hbox.size(), stream);
+    inj_bw.upload(hbw.data(), hbw.size(), stream);
+    fuse_on = fuse && std::getenv("OWL_NO_FUSE") == nullptr;
 }
 
 void SsgBase::ensure_state(int S, int k, bool grad) {
@@ -358,7 +388,30 @@ PointDev SsgBase::pdev(int S, bool adjoint, bool want_src_adj) {
 // kind 0: forward step; 1: recomputed step storing the stencil terms; 2:
 // adjoint step; 3: forward step storing the stencil terms (the last segment of
 // a gradient's forward, whose recompute it replaces)
+int SsgBase::step_launches(int kind) const {
+    if (fuse_on) return kind == 2 && want_src_now ? 3 : 2;
+    if (kind == 1) return 3;
+    if (kind != 2) return nb_rec <= 4 ? 3 : 4;
+    return nb_sct <= 4 ? 3 : 4;
+}
+
 void SsgBase::launch_step(int kind, int S, const PointDev& q) {
+    if (fuse_on) {
+        // the stencil kernels inject, sample / scatter and advance the step counter
+        if (kind != 2) {
+            fz_mode = FZ_INJ | FZ_TICK | (kind == 1 ? 0 : FZ_SMP);
+            launch_kernel(OWL_K_FWD_P, S, kind == 1 || kind == 3);
+            launch_kernel(OWL_K_FWD_V, S, kind == 1 || kind == 3);
+        } else {
+            fz_mode = FZ_SCT | (want_src_now ? 0 : FZ_TICK);
+            launch_kernel(OWL_K_ADJ_P, S, false);
+            launch_kernel(OWL_K_ADJ_V, S, false);
+            if (want_src_now) launch_point_adj(q, S, 1, PA_SRC | PA_TICK, stream);
+        }
+        fz_mode = 0;
+        launches += step_launches(kind);
+        return;
+    }
     // point operators of shots with more than 1024 traces / target nodes use
     // NB CTAs per shot and a separate launch for the dependent phase
     if (kind != 2) {
@@ -404,7 +457,8 @@ void SsgBase::run_steps(int kind, int n, int S, const PointDev& q, bool graph) {
                                   (uintptr_t)inj.off.p, (uintptr_t)smp.ptr.p, (uintptr_t)smp.w.p, (uintptr_t)smp.off.p,
                                   (uintptr_t)sct.ptr.p, (uintptr_t)sct.w.p, (uintptr_t)sct.off.p, (uintptr_t)amp.p,
                                   (uintptr_t)inj_shot_ptr.p, (uintptr_t)rec_shot_ptr.p, (uintptr_t)sct_shot_ptr.p,
-                                  (uintptr_t)q.rtot, (uintptr_t)nb_rec, (uintptr_t)nb_sct};
+                                  (uintptr_t)q.rtot, (uintptr_t)nb_rec, (uintptr_t)nb_sct, (uintptr_t)inj_box.p,
+                                  (uintptr_t)inj_bw.p, (uintptr_t)fuse_on, (uintptr_t)want_src_now};
     if (!gc.exec || gc.sig != sig) {
         gc.reset();
         cudaGraph_t g;
@@ -422,33 +476,87 @@ void SsgBase::run_steps(int kind, int n, int S, const PointDev& q, bool graph) {
         gc.sig = sig;
     }
     OWL_CUDA(cudaGraphLaunch(gc.exec, stream));
-    launches += (long long)n * (kind == 1 ? 3 : kind != 2 ? (nb_rec <= 4 ? 3 : 4) : (nb_sct <= 4 ? 3 : 4));
+    launches += (long long)n * step_launches(kind);
 }
 
-void SsgBase::resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bool& graph) {
+double SsgBase::batch_bytes(int S, int k, bool grad, int rec_per_shot) const {
+    const double f4 = 4.0, nt = desc.nt;
+    const double rtotS = (double)rec_per_shot * ncomp * S;
+    double b = f4 * sst * S + f4 * nt * std::max(rtotS, 1.0) * (grad ? 5.0 : 2.0) + f4 * nparam * (double)nx * ny * nz;
+    if (grad) {
+        const int kk = std::max(1, std::min(k, desc.nt));
+        const double nseg = std::ceil(nt / kk);
+        const double ck = ckpt_prec == OWL_CKPT_FP32 ? 4.0 : 2.0;
+        b += f4 * sad * S                          // adjoint state
+             + f4 * 2.0 * ngrad * S * (double)fs   // Kahan sums, one group per shot at most
+             + f4 * nS * (double)kk * S * fs       // stencil terms of a segment
+             + nseg * ck * sst * S                 // checkpoints
+             + 8.0 * nparam * (double)npad();      // FP64 padded gradient
+    }
+    return b;
+}
+
+double SsgBase::held_bytes() const {
+    return 4.0 * ((double)st.n + ad.n + G.n + Sbuf.n + ckpt.n + rec.n + res.n + obs_t.n + seis_tmp.n) +
+           2.0 * (double)ckpt16.n + 8.0 * (double)gpad.n;
+}
+
+// Options of one call. Shots per batch: opts.shots_per_launch, else the
+// largest count up to max_shots whose buffers fit the device. Checkpoint
+// interval: opts.checkpoint_interval (0: 50); < 0 the whole run when the
+// stored stencil terms of every step fit (nothing is recomputed), else the
+// longest interval that fits. "Fit" counts every buffer of the batch (state,
+// adjoint state, Kahan sums, the segment's stencil terms, checkpoints, traces)
+// against 92 % of the free device memory plus what the handle already holds
+// (OWL_MEM_BUDGET_MB in the environment caps that figure).
+void SsgBase::resolve_opts(const owl_run_opts& o, int nshots, const owl_shot* shots, bool grad, int& B, int& k,
+                           bool& graph) {
     // tile_z: 0 = autotuned; > 0 explicit tile height (3D forward: rows per
     // thread); < 0 in 3D: one thread per cell for the forward kernels
     tune = o.shots_per_cta <= 0 && o.tile_z == 0;
-    B = o.shots_per_launch > 0 ? o.shots_per_launch : std::max(1, desc.max_shots);
-    B = std::min(B, std::max(1, nshots));
-    k = o.checkpoint_interval > 0 ? o.checkpoint_interval : 50;
-    if (o.checkpoint_interval < 0) {
-        // the whole run as one segment when the stencil terms of every step fit
-        // in 60 % of the free device memory (the forward then stores them and
-        // nothing is recomputed), else the longest segment that fits
-        size_t fr = 0, tot = 0;
-        OWL_CUDA(cudaMemGetInfo(&fr, &tot));
-        const double per_step = 4.0 * nS * B * (double)fs;
-        const double room = 0.6 * (double)fr + (double)Sbuf.n * 4.0;  // the buffer held now is reused
-        k = per_step > 0 ? (int)std::max(1.0, std::min((double)desc.nt, std::floor(room / per_step))) : desc.nt;
-    }
-    k = std::min(k, desc.nt);
-    spt_f = spt_a = std::min(o.shots_per_cta > 0 ? o.shots_per_cta : 1, B);
-    graph = o.use_graph >= 0;
-    launch_params(o);
     OWL_CHECK(o.checkpoint_precision >= OWL_CKPT_FP32 && o.checkpoint_precision <= OWL_CKPT_BF16, OWL_ERR_INVALID,
               "bad checkpoint precision");
     ckpt_prec = o.checkpoint_precision;
+    const int Bmax = std::min(o.shots_per_launch > 0 ? o.shots_per_launch : std::max(1, desc.max_shots),
+                              std::max(1, nshots));
+    int recs = 1;
+    for (int i = 0; i < nshots && shots; ++i) recs = std::max(recs, shots[i].nrec);
+    size_t fr = 0, tot = 0;
+    OWL_CUDA(cudaMemGetInfo(&fr, &tot));
+    double budget = 0.92 * (double)fr + held_bytes();
+    if (const char* e = std::getenv("OWL_MEM_BUDGET_MB")) budget = std::min(budget, std::atof(e) * 1048576.0);
+    const bool auto_k = o.checkpoint_interval < 0;
+    const int k_fixed = std::min(o.checkpoint_interval > 0 ? o.checkpoint_interval : 50, desc.nt);
+    // the longest interval that fits S shots, 0 if none
+    auto fit_k = [&](int S) {
+        if (!auto_k) return batch_bytes(S, k_fixed, grad, recs) <= budget ? k_fixed : 0;
+        if (!grad) return batch_bytes(S, desc.nt, false, recs) <= budget ? desc.nt : 0;
+        for (int kk = desc.nt; kk >= 1; --kk)
+            if (batch_bytes(S, kk, true, recs) <= budget) return kk;
+        return 0;
+    };
+    B = Bmax;
+    k = fit_k(B);
+    if (o.shots_per_launch <= 0) {
+        while (k == 0 && B > 1) k = fit_k(--B);
+    }
+    if (k == 0) {
+        // nothing fits: the interval of least memory (the allocation reports OWL_ERR_OOM)
+        k = k_fixed;
+        if (auto_k && grad) {
+            double best = 1e300;
+            for (int kk = 1; kk <= desc.nt; ++kk) {
+                const double b = batch_bytes(B, kk, true, recs);
+                if (b < best) { best = b; k = kk; }
+            }
+        }
+    }
+    k = std::max(1, std::min(k, desc.nt));
+    plan_k = k;
+    plan_B = B;
+    spt_f = spt_a = std::min(o.shots_per_cta > 0 ? o.shots_per_cta : 1, B);
+    graph = o.use_graph >= 0;
+    launch_params(o);
 }
 
 // Times the stencil kernels of one step for each (shots per CTA, tile height)
@@ -593,6 +701,8 @@ void SsgBase::fill_info(owl_run_info& info, int nshots, int batches, bool grad) 
     info.tile_x = tile_x;
     info.tile_z = grad ? tz_a : tz_f;
     info.batches = batches;
+    info.checkpoint_interval = grad ? plan_k : 0;
+    info.shots_per_launch = plan_B;
 }
 
 void SsgBase::forward(int nshots, const owl_shot* shots, const owl_run_opts& o, float* seis, int mem,
@@ -600,7 +710,7 @@ void SsgBase::forward(int nshots, const owl_shot* shots, const owl_run_opts& o, 
     OWL_CHECK(model_set, OWL_ERR_INVALID, "set_model must be called first");
     int B, k;
     bool graph;
-    resolve_opts(o, nshots, B, k, graph);
+    resolve_opts(o, nshots, shots, false, B, k, graph);
     launches = 0;
     EventTimer tm(stream);
     size_t out_off = 0;
@@ -637,7 +747,7 @@ void SsgBase::misfit(int nshots, const owl_shot* shots, const float* obs, const 
     OWL_CHECK(model_set, OWL_ERR_INVALID, "set_model must be called first");
     int B, k;
     bool graph;
-    resolve_opts(o, nshots, B, k, graph);
+    resolve_opts(o, nshots, shots, false, B, k, graph);
     launches = 0;
     EventTimer tm(stream);
     size_t data_off = 0, tr_off = 0;
@@ -785,7 +895,7 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
               OWL_ERR_INVALID, "bad adj_kind");
     int B, k;
     bool graph;
-    resolve_opts(o, nshots, B, k, graph);
+    resolve_opts(o, nshots, shots, true, B, k, graph);
     launches = 0;
     const int nt = desc.nt;
     EventTimer tm(stream);
@@ -869,6 +979,7 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
         OWL_CUDA(cudaMemsetAsync(G.p, 0, sizeof(float) * 2 * ngrad * groups * fs, stream));
         PointDev qf = pdev(S, false, false);
         PointDev qa = pdev(S, true, want_src);
+        want_src_now = want_src;
         for (int sg = nseg - 1; sg >= 0; --sg) {
             const int n0 = sg * k, nn = std::min(k, nt - n0);
             if (sg == nseg - 1) {
@@ -880,6 +991,7 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
             }
             run_steps(2, nn, S, qa, graph && nn == k);
         }
+        want_src_now = false;
         if (o.check_every > 0) check_nonfinite(ad.p, (size_t)S * sad);
         // 4. chain rule (FP64) into the padded accumulators
         chain_rule(S, groups);
@@ -956,10 +1068,14 @@ void SsgBase::kernel_time(int id, int nlaunch, double* avg_ms, double* bytes) {
                   (ad.p && G.p && Sbuf.p && ad.n >= (size_t)sad * S && Sbuf.n >= (size_t)nS * cur_k * S * fs),
               OWL_ERR_INVALID, "adjoint kernels and store variants need a gradient call first");
     set_step(cur_k);
+    // the variant the time loop launches, without advancing the step counter
+    const int fz = fuse_on ? (kid < OWL_K_ADJ_P ? FZ_INJ : FZ_SCT) : 0;
+    fz_mode = fz;
     for (int i = 0; i < 3; ++i) launch_kernel(kid, S, store);
     OWL_LAUNCH_CHECK();
     EventTimer tm(stream);
     for (int i = 0; i < nlaunch; ++i) launch_kernel(kid, S, store);
+    fz_mode = 0;
     OWL_LAUNCH_CHECK();
     *avg_ms = tm.stop_ms() / nlaunch;
     *bytes = alg_bytes(kid, S, (S + spt_a - 1) / spt_a);

@@ -47,6 +47,13 @@ struct PointDev {
 };
 
 enum { PT_INJECT = 1, PT_SAMPLE = 2, PT_TICK = 4, PT_NEXT = 8 };  // forward point kernel phases
+// point work fused into a medium's stencil kernels (media that support it):
+// FZ_INJ source injection by the owner of each tap node, FZ_SMP receiver
+// sampling by extra CTAs of the velocity kernel, FZ_TICK the step counter
+// advanced by the last CTA, FZ_SCT the residual scatter by extra CTAs of the
+// adjoint velocity-node kernel
+enum { FZ_INJ = 1, FZ_SMP = 2, FZ_TICK = 4, FZ_SCT = 8 };
+constexpr int BOX_W = 9;  // taps of a source along each axis (the 9-tap Kaiser sinc)
 // adjoint point kernel phases. PA_SRC records the source-side adjoint of step
 // t-1 after the scatter; PA_SRC_NOW records that of step t from the fields as
 // they are (media whose adjoint kernels interleave with the source terms)
@@ -85,6 +92,13 @@ struct SsgBase : Engine {
     DevBuf<int> pt_idx;
     DevCSR inj, smp, sct;
     DevBuf<int> inj_shot_ptr, rec_shot_ptr, sct_shot_ptr;
+    // each injection item's taps as a dense BOX_W^dim box: (field, x0, y0, z0)
+    // storage coordinates of its lowest corner, weights [z][y][x] (0 off the taps)
+    DevBuf<int4> inj_box;
+    DevBuf<float> inj_bw;
+    bool fuse_on = false;  // this batch's point work runs inside the stencil kernels
+    bool want_src_now = false;  // the adjoint sweep records the source-side adjoint
+    int fz_mode = 0;       // FZ_* work of the next stencil launches
     DevBuf<unsigned char> live;
     DevBuf<long long> segbuf;  // st_segments offsets then lengths, on the device
     GraphCache g_fwd, g_rec, g_adj, g_fst;
@@ -141,6 +155,16 @@ struct SsgBase : Engine {
     virtual std::vector<int> tune_tz(int pass) const;
     // tile_x / tile_z of the run options (validated), spt_f / spt_a already set
     virtual void launch_params(const owl_run_opts& o);
+    // point work inside the stencil kernels: whether the medium's kernels do it,
+    // and whether an injection / sampling tap of `field` at storage (x, y, z)
+    // lies in the nodes its kernel updates (else the batch keeps the point kernels)
+    virtual bool fuse_supported() const { return false; }
+    virtual bool fuse_tap_ok(int field, int x, int y, int z, bool sampling) const {
+        (void)field; (void)x; (void)y; (void)z; (void)sampling;
+        return false;
+    }
+    // launches of one time step of `kind` (launch_step)
+    int step_launches(int kind) const;
     // medium-specific tuning after the shared autotuner (S shots per launch)
     virtual void tune_extra(int S, int k, bool grad) { (void)S; (void)k; (void)grad; }
 
@@ -172,7 +196,13 @@ struct SsgBase : Engine {
     PointDev pdev(int S, bool adjoint, bool want_src_adj);
     virtual void launch_step(int kind, int S, const PointDev& q);
     void run_steps(int kind, int n, int S, const PointDev& q, bool graph);
-    void resolve_opts(const owl_run_opts& o, int nshots, int& B, int& k, bool& graph);
+    void resolve_opts(const owl_run_opts& o, int nshots, const owl_shot* shots, bool grad, int& B, int& k,
+                      bool& graph);
+    // device bytes one batch of S shots needs (k: checkpoint interval of a gradient)
+    double batch_bytes(int S, int k, bool grad, int rec_per_shot) const;
+    // bytes of the buffers a new batch would reuse or replace
+    double held_bytes() const;
+    int plan_k = 0, plan_B = 0;  // the last call's checkpoint interval and shots per batch
     void autotune(int S, int k, bool grad);
     void save_ckpt(int slot, int S);
     void restore_ckpt(int slot, int S);

@@ -156,3 +156,61 @@ def test_unstable_dt_rejected():
     with pytest.raises(L.OwlError) as e:
         s.set_model(vp, rho)
     assert e.value.code == L.OWL_ERR_UNSTABLE
+
+
+@pytest.mark.parametrize("fs", [0, 1])
+def test_fused_point_work_matches_point_kernels(fs):
+    """Injection, sampling and the residual scatter inside the stencil kernels
+    give the seismograms, misfits and gradients of the separate point kernel
+    (OWL_NO_FUSE=1) to the bit: explosion and force sources, two overlapping
+    sources in one shot, off-grid receivers sharing taps, a zero-weight trace."""
+    import os
+    nx, nz, dx, dt, nt = 48, 40, 10.0, 1e-3, 300
+    d = desc(nx, nz, dx, dt, nt, fs=fs)
+    vp, rho = random_model(nx, nz)
+    ps = prepare(small_shots(nx, nz, dx, bool(fs)), nx, nz, dx, dt)
+    obs = oracle.ac2d_forward(d, vp, rho, ps, "f64").astype(np.float32)
+    s = make_solver(d, vp * np.float32(1.02), rho)
+    out = {}
+    for off in (False, True):
+        if off:
+            os.environ["OWL_NO_FUSE"] = "1"
+        try:
+            seis = s.forward(ps, RunOpts())
+            mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=40))
+            launches = s.last_info.gpu_launches
+            gs = s.source_gradient(ps, obs, RunOpts(checkpoint_interval=40))
+        finally:
+            os.environ.pop("OWL_NO_FUSE", None)
+        out[off] = (seis, mf, g, gs, launches)
+    for a, b in zip(out[False][:4], out[True][:4]):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+    assert out[False][4] < out[True][4]  # fewer launches with the fused point work
+
+
+def test_memory_planner_picks_batch_and_interval():
+    """With the device budget capped (OWL_MEM_BUDGET_MB), the planner splits the
+    shots into smaller batches and picks a checkpoint interval below nt; the
+    gradient still matches the FP64 oracle, and the run reports its plan."""
+    import os
+    nx, nz, dx, dt, nt = 48, 40, 10.0, 1e-3, 300
+    d = desc(nx, nz, dx, dt, nt)
+    vp, rho = random_model(nx, nz)
+    ps = prepare(small_shots(nx, nz, dx), nx, nz, dx, dt)
+    obs = oracle.ac2d_forward(d, vp, rho, ps, "f64").astype(np.float32)
+    vp0 = vp * np.float32(1.02)
+    _, g_ref, _ = oracle.ac2d_gradient(d, vp0, rho, ps, obs, adj_kind=0, k=37, precision="f64")
+    s = make_solver(d, vp0, rho)
+    _, g_free = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=-1))
+    assert s.last_info.checkpoint_interval == nt and s.last_info.shots_per_launch == 3
+    os.environ["OWL_MEM_BUDGET_MB"] = "10"
+    try:
+        _, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=-1))
+        info = s.last_info
+    finally:
+        os.environ.pop("OWL_MEM_BUDGET_MB", None)
+    print("planned", info.shots_per_launch, "shots per batch, interval", info.checkpoint_interval,
+          "batches", info.batches)
+    assert info.shots_per_launch < 3 and info.batches >= 2
+    assert 1 <= info.checkpoint_interval < nt
+    assert rel(g, g_ref) < GRAD_TOL and rel(g_free, g_ref) < GRAD_TOL
