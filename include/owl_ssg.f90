@@ -419,6 +419,19 @@ module owl_ssg_c
             type(c_ptr), value :: seis
         end function
 
+        ! damp_ratio (module_cfspml.f90:193-248) of one face cell, host computation
+        real(c_float) function owl_mpml_damp_ratio(c, axis) bind(c, name='owl_mpml_damp_ratio')
+            import :: c_float, c_int
+            real(c_float), intent(in) :: c(*)
+            integer(c_int), value :: axis
+        end function
+
+        ! the six M-PML face-ratio arrays of an elastic 3D handle
+        integer(c_int) function owl_ssg_mpml_ratios(h, faces) bind(c, name='owl_ssg_mpml_ratios')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, faces
+        end function
+
         ! returns a NUL-terminated C string (c_f_pointer it to a character array)
         type(c_ptr) function owl_last_error() bind(c, name='owl_last_error')
             import :: c_ptr

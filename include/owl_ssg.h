@@ -474,6 +474,23 @@ int owl_ssg_kernel_time(owl_ssg *h, int kernel_id, int nlaunch, double *avg_ms, 
 int owl_ssg_forward_noalloc(const owl_ssg_desc *desc, int nparam, const float *const *fields,
                             const owl_shot *shot, float *seis);
 
+/* ---- M-PML damping ratios of the 3D anisotropic elastic solver ---------- */
+
+/* damp_ratio (src/solver/elastic_vhtiort_3d/module_cfspml.f90:193-248): the
+ * M-PML ratio of one PML face cell, c = (c11, c12, c13, c22, c23, c33, c44,
+ * c55, c66) of the cell, axis 0 / 1 / 2 the damped axis (x, y, z faces).
+ * Host computation, no device needed; -1 on bad arguments. */
+float owl_mpml_damp_ratio(const float *c, int axis);
+
+/* The six face-ratio arrays an elastic 3D handle uses after set_model
+ * (compute_damping_profile_ratio, module_cfspml.f90:253-421; all zero for the
+ * iso parameterisation, as the reference's): faces = left, right (x low /
+ * high: (nz + 2 pml) x (ny + 2 pml), y fastest), front, back (y: (nz + 2 pml) x
+ * (nx + 2 pml), x fastest), top, bottom (z: (ny + 2 pml) x (nx + 2 pml), x
+ * fastest), concatenated; index 0 of each axis is the reference's -pml + 1.
+ * With a free surface the x / y faces hold zeros above row 1. */
+int owl_ssg_mpml_ratios(const owl_ssg *h, float *faces);
+
 /* ---- queries ------------------------------------------------------------ */
 
 const char *owl_last_error(void);

@@ -48,6 +48,8 @@ def load():
         _lib.oracle_el3d_jvp_c128.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp]
         _lib.oracle_el3d_gradient_f64.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp, vp]
         _lib.oracle_el3d_setup.argtypes = [vp, vp, vp]
+        _lib.oracle_el3d_set_mpml.argtypes = [vp, C.c_longlong]
+        _lib.oracle_el3d_set_mpml.restype = None
     return _lib
 
 
@@ -223,6 +225,17 @@ def el2d_damp_ratio(c11, c13, c33, c55, rho, direction="x"):
 # ------------------------------- elastic 3D ----------------------------------
 def _nseis_el3(ps, nt):
     return 3 * sum(ps.arr[s].nrec for s in range(ps.nshots)) * nt
+
+
+def el3d_set_mpml(faces=None):
+    """M-PML face ratios (the layout of owl_ssg_mpml_ratios) for the following
+    elastic 3D oracle runs; None: all zero."""
+    lib = load()
+    if faces is None:
+        lib.oracle_el3d_set_mpml(None, 0)
+        return
+    f = np.ascontiguousarray(faces, dtype=np.float32)
+    lib.oracle_el3d_set_mpml(f.ctypes.data, f.size)
 
 
 def el3d_forward(desc, fields, ps, precision="f32"):

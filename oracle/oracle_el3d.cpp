@@ -15,11 +15,13 @@
 //   and the odd stress images      module_wavefield.f90:549-1090
 //   surface images before sampling submodule_forward_modeling.f90:66-82
 //   sources above row 2 skipped    module_wavefield.f90:1107-1315
-// plus the exact discrete adjoint and the chain rule to the model parameters. The M-PML damping ratios of the six faces are zero:
-// that is the reference's value for the isotropic parameterisation
-// (module_cfspml.f90:448-465); for anisotropic media the reference derives them
-// from LAPACK eigenvectors of a 27 x 27 split-field system, which is not
-// restated here.
+// plus the exact discrete adjoint and the chain rule to the model parameters.
+// M-PML damping ratios of the six faces: zero -- the reference's value for the
+// isotropic parameterisation (module_cfspml.f90:448-465) -- unless face arrays
+// are set with oracle_el3d_set_mpml (anisotropic media: the reference's
+// eigen-derivative search, module_cfspml.f90:51-421, is restated literally in
+// oracle_mpml.py, which checks the library's face arrays; the tests pass those
+// arrays here).
 //
 // Templated on T: float (forward parity), double (gradient), complex<double>
 // (complex-step Jacobian-vector products).
@@ -177,6 +179,10 @@ enum { F_XX = 0, F_YY, F_ZZ, F_YZ, F_XZ, F_XY, F_VX, F_VY, F_VZ };
 enum { M_XVX = 0, M_YVY, M_ZVZ, M_ZVY, M_YVZ, M_ZVX, M_XVZ, M_YVX, M_XVY, M_XXX, M_YXY, M_ZXZ, M_XXY, M_YYY,
        M_ZYZ, M_XXZ, M_YYZ, M_ZZZ };
 
+// M-PML face ratios for the next oracle runs (the layout of owl_ssg_mpml_ratios);
+// empty: all zero, the reference's value for the iso parameterisation
+static std::vector<float> g_el3_faces;
+
 template <typename T>
 struct El3 {
     int nx, ny, nz, P, R, nt, aniso, np;
@@ -248,15 +254,50 @@ struct El3 {
         px.build(nx, P, dx, pmlvp, alphamax);
         py.build(ny, P, dy, pmlvp, alphamax);
         pz.build(nz, P, dz, pmlvp, alphamax);
+        const long long fx = (long long)(ny + 2 * P) * (nz + 2 * P), fy = (long long)(nx + 2 * P) * (nz + 2 * P),
+                        fz = (long long)(nx + 2 * P) * (ny + 2 * P);
+        if (g_el3_faces.size() == (size_t)(2 * (fx + fy + fz))) {
+            faces = g_el3_faces;
+            const long long o[6] = {0, fx, 2 * fx, 2 * fx + fy, 2 * fx + 2 * fy, 2 * fx + 2 * fy + fz};
+            for (int q = 0; q < 6; ++q) ofs[q] = o[q];
+        }
         for (int a = 0; a < 3; ++a) lo[a] = -P - R + 1;
         hi[0] = nx + P + R; hi[1] = ny + P + R; hi[2] = nz + P + R;
     }
 
-    // damping of one derivative of a node: axis 0/1/2, position half or integer
-    void coef(int axis, int pos, bool half, float& a, float& b) const {
-        const Prof3& p = axis == 0 ? px : axis == 1 ? py : pz;
-        el3_ab(dt, half ? p.dh(pos) : p.di(pos), half ? p.ah(pos) : p.ai(pos), a, b);
+    // damping of the derivative along `axis` of the node (i, j, k) staggered by
+    // (hx, hy, hz) (true: half position on that axis), the M-PML blocks of
+    // module_wavefield.f90:101-145 (and their counterparts for the other
+    // nodes): d = own profile + ratio * profile of each other axis, in the
+    // reference's order, the ratio of an axis being its face's value when the
+    // node lies beyond that face (index <= 0, <= 1 at a half position, or >= n + 1)
+    void coef(int axis, int i, int j, int k, bool hx, bool hy, bool hz, float& a, float& b) const {
+        auto beyond = [](int v, int n, bool h) { return (h ? v <= 1 : v <= 0) ? -1 : v >= n + 1 ? 1 : 0; };
+        const int bx = beyond(i, nx, hx), by = beyond(j, ny, hy), bz = beyond(k, nz, hz);
+        const float rx = bx < 0 ? fl(j, k) : bx > 0 ? fr(j, k) : 0.f;
+        const float ry = by < 0 ? ff(i, k) : by > 0 ? fb(i, k) : 0.f;
+        const float rz = bz < 0 ? ft(i, j) : bz > 0 ? fo(i, j) : 0.f;
+        const float dX = hx ? px.dh(i) : px.di(i), dY = hy ? py.dh(j) : py.di(j), dZ = hz ? pz.dh(k) : pz.di(k);
+        float d, al;
+        if (axis == 0) { d = dX + ry * dY + rz * dZ; al = hx ? px.ah(i) : px.ai(i); }
+        else if (axis == 1) { d = dY + rx * dX + rz * dZ; al = hy ? py.ah(j) : py.ai(j); }
+        else { d = dZ + rx * dX + ry * dY; al = hz ? pz.ah(k) : pz.ai(k); }
+        el3_ab(dt, d, al, a, b);
     }
+    // face ratios over the padded ranges (-pml+1 .. n+pml): left / right (j, k),
+    // front / back (i, k), top / bottom (i, j); zero unless set by oracle_el3d_set_mpml
+    std::vector<float> faces;
+    long long ofs[6] = {0, 0, 0, 0, 0, 0};
+    float face(int f, int u, int v, int nu) const {
+        if (faces.empty()) return 0.f;
+        return faces[ofs[f] + (long long)(v + P - 1) * nu + (u + P - 1)];
+    }
+    float fl(int j, int k) const { return face(0, j, k, ny + 2 * P); }
+    float fr(int j, int k) const { return face(1, j, k, ny + 2 * P); }
+    float ff(int i, int k) const { return face(2, i, k, nx + 2 * P); }
+    float fb(int i, int k) const { return face(3, i, k, nx + 2 * P); }
+    float ft(int i, int j) const { return face(4, i, j, nx + 2 * P); }
+    float fo(int i, int j) const { return face(5, i, j, nx + 2 * P); }
     // node in the PML shell: h[a] says whether the node is at a half position on axis a
     bool shell(int i, int j, int k, bool hx, bool hy, bool hz) const {
         auto out = [](int v, int n, bool h) { return h ? (v <= 1 || v >= n + 1) : (v <= 0 || v >= n + 1); };
@@ -346,17 +387,17 @@ struct El3 {
             if (fs && k == 1) {
                 if (i <= 0 || i >= nx + 1 || j <= 0 || j >= ny + 1) {
                     float ca, cb;
-                    coef(0, i, false, ca, cb); dX = pml_f(dX, ca, cb, s.m[M_XVX](i, j, k));
-                    coef(1, j, false, ca, cb); dY = pml_f(dY, ca, cb, s.m[M_YVY](i, j, k));
+                    coef(0, i, j, k, false, false, false, ca, cb); dX = pml_f(dX, ca, cb, s.m[M_XVX](i, j, k));
+                    coef(1, i, j, k, false, false, false, ca, cb); dY = pml_f(dY, ca, cb, s.m[M_YVY](i, j, k));
                 }
                 dZ = -(C[2](i, j, k) / C[5](i, j, k)) * dX - (C[4](i, j, k) / C[5](i, j, k)) * dY;
             } else {
                 dZ = T(idz) * stP(s.f[F_VZ], i, j, k, 2);
                 if (shell(i, j, k, false, false, false)) {
                     float ca, cb;
-                    coef(0, i, false, ca, cb); dX = pml_f(dX, ca, cb, s.m[M_XVX](i, j, k));
-                    coef(1, j, false, ca, cb); dY = pml_f(dY, ca, cb, s.m[M_YVY](i, j, k));
-                    coef(2, k, false, ca, cb); dZ = pml_f(dZ, ca, cb, s.m[M_ZVZ](i, j, k));
+                    coef(0, i, j, k, false, false, false, ca, cb); dX = pml_f(dX, ca, cb, s.m[M_XVX](i, j, k));
+                    coef(1, i, j, k, false, false, false, ca, cb); dY = pml_f(dY, ca, cb, s.m[M_YVY](i, j, k));
+                    coef(2, i, j, k, false, false, false, ca, cb); dZ = pml_f(dZ, ca, cb, s.m[M_ZVZ](i, j, k));
                 }
             }
             s.f[F_XX](i, j, k) = s.f[F_XX](i, j, k) + T(fdt) * (C[0](i, j, k) * dX + C[1](i, j, k) * dY + C[2](i, j, k) * dZ);
@@ -369,8 +410,8 @@ struct El3 {
             T dzvy = T(idz) * stM(s.f[F_VY], i, n, p, 2), dyvz = T(idy) * stM(s.f[F_VZ], i, n, p, 1);
             if (shell(i, n, p, false, true, true)) {
                 float ca, cb;
-                coef(1, n, true, ca, cb); dyvz = pml_f(dyvz, ca, cb, s.m[M_YVZ](i, n, p));
-                coef(2, p, true, ca, cb); dzvy = pml_f(dzvy, ca, cb, s.m[M_ZVY](i, n, p));
+                coef(1, i, n, p, false, true, true, ca, cb); dyvz = pml_f(dyvz, ca, cb, s.m[M_YVZ](i, n, p));
+                coef(2, i, n, p, false, true, true, ca, cb); dzvy = pml_f(dzvy, ca, cb, s.m[M_ZVY](i, n, p));
             }
             s.f[F_YZ](i, n, p) = s.f[F_YZ](i, n, p) + T(dt) * c44e(i, n, p) * (dzvy + dyvz);
             if (S) S[3](i, n, p) = dzvy + dyvz;
@@ -380,8 +421,8 @@ struct El3 {
             T dzvx = T(idz) * stM(s.f[F_VX], m, j, p, 2), dxvz = T(idx) * stM(s.f[F_VZ], m, j, p, 0);
             if (shell(m, j, p, true, false, true)) {
                 float ca, cb;
-                coef(0, m, true, ca, cb); dxvz = pml_f(dxvz, ca, cb, s.m[M_XVZ](m, j, p));
-                coef(2, p, true, ca, cb); dzvx = pml_f(dzvx, ca, cb, s.m[M_ZVX](m, j, p));
+                coef(0, m, j, p, true, false, true, ca, cb); dxvz = pml_f(dxvz, ca, cb, s.m[M_XVZ](m, j, p));
+                coef(2, m, j, p, true, false, true, ca, cb); dzvx = pml_f(dzvx, ca, cb, s.m[M_ZVX](m, j, p));
             }
             s.f[F_XZ](m, j, p) = s.f[F_XZ](m, j, p) + T(dt) * c55e(m, j, p) * (dzvx + dxvz);
             if (S) S[4](m, j, p) = dzvx + dxvz;
@@ -391,8 +432,8 @@ struct El3 {
             T dyvx = T(idy) * stM(s.f[F_VX], m, n, k, 1), dxvy = T(idx) * stM(s.f[F_VY], m, n, k, 0);
             if (shell(m, n, k, true, true, false)) {
                 float ca, cb;
-                coef(0, m, true, ca, cb); dxvy = pml_f(dxvy, ca, cb, s.m[M_XVY](m, n, k));
-                coef(1, n, true, ca, cb); dyvx = pml_f(dyvx, ca, cb, s.m[M_YVX](m, n, k));
+                coef(0, m, n, k, true, true, false, ca, cb); dxvy = pml_f(dxvy, ca, cb, s.m[M_XVY](m, n, k));
+                coef(1, m, n, k, true, true, false, ca, cb); dyvx = pml_f(dyvx, ca, cb, s.m[M_YVX](m, n, k));
             }
             s.f[F_XY](m, n, k) = s.f[F_XY](m, n, k) + T(dt) * c66e(m, n, k) * (dyvx + dxvy);
             if (S) S[5](m, n, k) = dyvx + dxvy;
@@ -418,9 +459,9 @@ struct El3 {
               hz = T(idz) * stP(s.f[F_XZ], m, j, k, 2);
             if (shell(m, j, k, true, false, false)) {
                 float ca, cb;
-                coef(0, m, true, ca, cb); hx = pml_f(hx, ca, cb, s.m[M_XXX](m, j, k));
-                coef(1, j, false, ca, cb); hy = pml_f(hy, ca, cb, s.m[M_YXY](m, j, k));
-                coef(2, k, false, ca, cb); hz = pml_f(hz, ca, cb, s.m[M_ZXZ](m, j, k));
+                coef(0, m, j, k, true, false, false, ca, cb); hx = pml_f(hx, ca, cb, s.m[M_XXX](m, j, k));
+                coef(1, m, j, k, true, false, false, ca, cb); hy = pml_f(hy, ca, cb, s.m[M_YXY](m, j, k));
+                coef(2, m, j, k, true, false, false, ca, cb); hz = pml_f(hz, ca, cb, s.m[M_ZXZ](m, j, k));
             }
             const T re = T(0.5f) * (C[9](m - 1, j, k) + C[9](m, j, k));
             s.f[F_VX](m, j, k) = s.f[F_VX](m, j, k) + T(dt) / re * (hx + hy + hz);
@@ -432,9 +473,9 @@ struct El3 {
               hz = T(idz) * stP(s.f[F_YZ], i, n, k, 2);
             if (shell(i, n, k, false, true, false)) {
                 float ca, cb;
-                coef(0, i, false, ca, cb); hx = pml_f(hx, ca, cb, s.m[M_XXY](i, n, k));
-                coef(1, n, true, ca, cb); hy = pml_f(hy, ca, cb, s.m[M_YYY](i, n, k));
-                coef(2, k, false, ca, cb); hz = pml_f(hz, ca, cb, s.m[M_ZYZ](i, n, k));
+                coef(0, i, n, k, false, true, false, ca, cb); hx = pml_f(hx, ca, cb, s.m[M_XXY](i, n, k));
+                coef(1, i, n, k, false, true, false, ca, cb); hy = pml_f(hy, ca, cb, s.m[M_YYY](i, n, k));
+                coef(2, i, n, k, false, true, false, ca, cb); hz = pml_f(hz, ca, cb, s.m[M_ZYZ](i, n, k));
             }
             const T re = T(0.5f) * (C[9](i, n - 1, k) + C[9](i, n, k));
             s.f[F_VY](i, n, k) = s.f[F_VY](i, n, k) + T(dt) / re * (hx + hy + hz);
@@ -446,9 +487,9 @@ struct El3 {
               hz = T(idz) * stM(s.f[F_ZZ], i, j, p, 2);
             if (shell(i, j, p, false, false, true)) {
                 float ca, cb;
-                coef(0, i, false, ca, cb); hx = pml_f(hx, ca, cb, s.m[M_XXZ](i, j, p));
-                coef(1, j, false, ca, cb); hy = pml_f(hy, ca, cb, s.m[M_YYZ](i, j, p));
-                coef(2, p, true, ca, cb); hz = pml_f(hz, ca, cb, s.m[M_ZZZ](i, j, p));
+                coef(0, i, j, p, false, false, true, ca, cb); hx = pml_f(hx, ca, cb, s.m[M_XXZ](i, j, p));
+                coef(1, i, j, p, false, false, true, ca, cb); hy = pml_f(hy, ca, cb, s.m[M_YYZ](i, j, p));
+                coef(2, i, j, p, false, false, true, ca, cb); hz = pml_f(hz, ca, cb, s.m[M_ZZZ](i, j, p));
             }
             const T re = T(0.5f) * (C[9](i, j, p - 1) + C[9](i, j, p));
             s.f[F_VZ](i, j, p) = s.f[F_VZ](i, j, p) + T(dt) / re * (hx + hy + hz);
@@ -596,9 +637,9 @@ struct El3 {
             T ex = q, ey = q, ez = q;
             if (shell(i, j, k, hxh, hyh, hzh)) {
                 float ca, cb;
-                coef(0, i, hxh, ca, cb); ex = pml_e(q, ca, cb, a.m[mx](i, j, k));
-                coef(1, j, hyh, ca, cb); ey = pml_e(q, ca, cb, a.m[my](i, j, k));
-                coef(2, k, hzh, ca, cb); ez = pml_e(q, ca, cb, a.m[mz](i, j, k));
+                coef(0, i, j, k, hxh, hyh, hzh, ca, cb); ex = pml_e(q, ca, cb, a.m[mx](i, j, k));
+                coef(1, i, j, k, hxh, hyh, hzh, ca, cb); ey = pml_e(q, ca, cb, a.m[my](i, j, k));
+                coef(2, i, j, k, hxh, hyh, hzh, ca, cb); ez = pml_e(q, ca, cb, a.m[mz](i, j, k));
             }
             return std::array<T, 3>{T(idx) * ex, T(idy) * ey, T(idz) * ez};
         };
@@ -660,8 +701,8 @@ struct El3 {
             hh[ax1] = h1; hh[ax2] = h2;
             if (shell(i, j, k, hh[0], hh[1], hh[2])) {
                 float ca, cb;
-                coef(ax1, pos[ax1], h1, ca, cb); e1 = pml_e(q, ca, cb, a.m[m1](i, j, k));
-                coef(ax2, pos[ax2], h2, ca, cb); e2 = pml_e(q, ca, cb, a.m[m2](i, j, k));
+                coef(ax1, i, j, k, hh[0], hh[1], hh[2], ca, cb); e1 = pml_e(q, ca, cb, a.m[m1](i, j, k));
+                coef(ax2, i, j, k, hh[0], hh[1], hh[2], ca, cb); e2 = pml_e(q, ca, cb, a.m[m2](i, j, k));
             }
             const float id[3] = {idx, idy, idz};
             scM(a.f[fa], i, j, k, ax1, T(id[ax1]) * e1);
@@ -703,8 +744,8 @@ struct El3 {
                         T qy = tt * (C[1](i, j, k) * xh + C[3](i, j, k) * yh) - r23 * w;
                         if (i <= 0 || i >= nx + 1 || j <= 0 || j >= ny + 1) {
                             float ca, cb;
-                            coef(0, i, false, ca, cb); qx = pml_e(qx, ca, cb, a.m[M_XVX](i, j, k));
-                            coef(1, j, false, ca, cb); qy = pml_e(qy, ca, cb, a.m[M_YVY](i, j, k));
+                            coef(0, i, j, k, false, false, false, ca, cb); qx = pml_e(qx, ca, cb, a.m[M_XVX](i, j, k));
+                            coef(1, i, j, k, false, false, false, ca, cb); qy = pml_e(qy, ca, cb, a.m[M_YVY](i, j, k));
                         }
                         scP(a.f[F_VX], i, j, k, 0, T(idx) * qx);
                         scP(a.f[F_VY], i, j, k, 1, T(idy) * qy);
@@ -721,9 +762,9 @@ struct El3 {
                     T qz = tt * (C[2](i, j, k) * xh + C[4](i, j, k) * yh + C[5](i, j, k) * zh);
                     if (shell(i, j, k, false, false, false)) {
                         float ca, cb;
-                        coef(0, i, false, ca, cb); qx = pml_e(qx, ca, cb, a.m[M_XVX](i, j, k));
-                        coef(1, j, false, ca, cb); qy = pml_e(qy, ca, cb, a.m[M_YVY](i, j, k));
-                        coef(2, k, false, ca, cb); qz = pml_e(qz, ca, cb, a.m[M_ZVZ](i, j, k));
+                        coef(0, i, j, k, false, false, false, ca, cb); qx = pml_e(qx, ca, cb, a.m[M_XVX](i, j, k));
+                        coef(1, i, j, k, false, false, false, ca, cb); qy = pml_e(qy, ca, cb, a.m[M_YVY](i, j, k));
+                        coef(2, i, j, k, false, false, false, ca, cb); qz = pml_e(qz, ca, cb, a.m[M_ZVZ](i, j, k));
                     }
                     scP(a.f[F_VX], i, j, k, 0, T(idx) * qx);
                     scP(a.f[F_VY], i, j, k, 1, T(idy) * qy);
@@ -923,6 +964,11 @@ extern "C" int oracle_el3d_gradient_f64(const owl_ssg_desc* d, const double* con
         std::fprintf(stderr, "oracle: %s\n", e.what());
         return -1;
     }
+}
+
+extern "C" void oracle_el3d_set_mpml(const float* faces, long long n) {
+    if (faces && n > 0) g_el3_faces.assign(faces, faces + n);
+    else g_el3_faces.clear();
 }
 
 extern "C" int oracle_el3d_setup(const owl_ssg_desc* d, const float* const* f, float* dt_stable) {

@@ -199,6 +199,7 @@ EXPORTED = [
     "owl_ssg_forward_noalloc", "owl_ssg_desc_nparam", "owl_ssg_misfit", "owl_ssg_gradient_misfit",
     "owl_adjoint_source", "owl_dtw_time_shifts", "owl_ssg_set_data_sampling", "owl_resample_traces",
     "owl_su_encode", "owl_su_decode", "owl_search_direction", "owl_grad_process",
+    "owl_mpml_damp_ratio", "owl_ssg_mpml_ratios",
 ]
 
 OWL_SEARCH_SD = 0
@@ -253,6 +254,10 @@ def load() -> C.CDLL:
                                             C.c_void_p, C.c_int, P(OwlRunInfo)]
     lib.owl_ssg_kernel_time.argtypes = [C.c_void_p, C.c_int, C.c_int, P(C.c_double), P(C.c_double)]
     lib.owl_ssg_kernel_time.restype = C.c_int
+    lib.owl_mpml_damp_ratio.argtypes = [P(C.c_float), C.c_int]
+    lib.owl_mpml_damp_ratio.restype = C.c_float
+    lib.owl_ssg_mpml_ratios.argtypes = [C.c_void_p, P(C.c_float)]
+    lib.owl_ssg_mpml_ratios.restype = C.c_int
     lib.owl_ssg_forward_noalloc.argtypes = [P(OwlSsgDesc), C.c_int, P(P(C.c_float)), P(OwlShot), C.c_void_p]
     lib.owl_ssg_forward_noalloc.restype = C.c_int
     lib.owl_ssg_destroy.argtypes = [C.c_void_p]

@@ -11,7 +11,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "lib", "libowl_ssg.so")
 OBJ = os.path.join(HERE, "lib", "obj")
 SOURCES = ["shared.cu", "ssg_base.cu", "ac2d.cu", "ac3d.cu", "el2d.cu", "el3d.cu", "adjsrc.cu", "dtw.cu", "su.cu",
-           "optim.cu", "capi.cu", "noalloc.cu"]
+           "optim.cu", "capi.cu", "noalloc.cu", "mpml.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17"] + ARCH + ["-lineinfo", "-Xcompiler", "-fPIC"]
 

@@ -1,4 +1,5 @@
 // capi.cu -- extern "C" entry points declared in include/owl_ssg.h.
+#include <algorithm>
 #include <memory>
 #include <mutex>
 
@@ -430,6 +431,15 @@ int owl_ssg_kernel_time(owl_ssg* h, int kernel_id, int nlaunch, double* avg_ms, 
     return guarded([&] {
         OWL_CHECK(h && h->eng && avg_ms && alg_bytes && nlaunch > 0, OWL_ERR_INVALID, "bad arguments");
         h->eng->kernel_time(kernel_id, nlaunch, avg_ms, alg_bytes);
+    });
+}
+
+int owl_ssg_mpml_ratios(const owl_ssg* h, float* faces) {
+    return guarded([&] {
+        OWL_CHECK(h && h->eng && faces, OWL_ERR_INVALID, "bad arguments");
+        const std::vector<float>* f = h->eng->mpml_faces();
+        OWL_CHECK(f && h->eng->model_set, OWL_ERR_INVALID, "M-PML ratios exist for an elastic 3D handle after set_model");
+        std::copy(f->begin(), f->end(), faces);
     });
 }
 

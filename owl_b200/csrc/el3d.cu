@@ -23,12 +23,16 @@
 // mapped onto the rows they copy.
 //
 // Damping. The reference damps a derivative along axis a of a node in the PML
-// shell with d = d_a(pos_a) + sum of ratio * d_b(pos_b) over the other axes
-// (module_wavefield.f90:104-145). With the M-PML ratios at zero -- the
-// reference's value for isotropic media, and what this solver uses for every
-// parameterisation -- (a, b) of a derivative depend only on the node's position
-// along that axis, so they are 1D tables per axis (integer and half
-// positions); a memory whose a is 0 stays exactly 0 and is not touched.
+// shell with d = d_a(pos_a) + sum of ratio_b * d_b(pos_b) over the other axes b
+// (module_wavefield.f90:104-145), ratio_b the M-PML ratio of the face of axis b
+// the node lies beyond (0 between them) and alpha_a the axis-a profile inside
+// its PML, alphamax elsewhere in the shell. With the ratios at zero -- the
+// reference's value for the iso parameterisation -- (a, b) of a derivative
+// depend only on the node's position along that axis: 1D tables per axis
+// (integer and half positions), and a memory whose a is 0 stays exactly 0 and is
+// not touched. Anisotropic parameterisations have nonzero ratios (searched on
+// the host, mpml.cu): the MP instances of the per-cell kernels compute each
+// shell node's (a, b) from the per-axis profiles and the six face-ratio arrays.
 //
 // One step = two stencil launches (stresses, velocities) + the point kernel;
 // the adjoint of a step = velocity-node kernel, source adjoint (optional),
@@ -37,6 +41,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "mpml.cuh"
 #include "ring.cuh"
 #include "ssg_base.cuh"
 
@@ -50,6 +55,17 @@ enum { N_XVX = 0, N_YVY, N_ZVZ, N_ZVY, N_YVZ, N_ZVX, N_XVZ, N_YVX, N_XVY, N_XXX,
        N_XXZ, N_YYZ, N_ZZZ };
 constexpr int E3_NST = 9 + 18;
 constexpr int E3_NAD = 9 + 18 + 18;
+
+// M-PML tables: per axis the damping profile d and alpha at integer [0] and
+// half [1] positions (storage index; d = 0 and alpha = alphamax outside the
+// axis' PML), and the face ratios: left / right [z][y] (NYs), front / back
+// [z][x], top / bottom [y][x] (pitch), zero outside the padded model
+struct E3Mp {
+    const float* d[3][2];
+    const float* al[3][2];
+    const float* face[6];
+    float adt;
+};
 
 struct El3dDev {
     int nx, ny, nz, P, R, pr, pitch;
@@ -69,6 +85,7 @@ struct El3dDev {
     float* ad;
     float* G;  // [12][group][fs] sums then [12][group][fs] compensations
     long long gg;
+    E3Mp mp;
 };
 
 __device__ __forceinline__ bool e3_out(int v, int pr, int n, bool half) {
@@ -118,6 +135,33 @@ __device__ __forceinline__ float pml_adr(float q, float a, float b, float psih, 
     return q + a * u;
 }
 
+// (a, b) of the derivative along axis ax at the node at storage (x, y, z),
+// staggered by (hx, hy, hz) (1: half position on that axis): d = own profile +
+// ratio * profile of each other axis in the reference's order, alpha of the own
+// axis, kappa = 1, damp_coef of module_wavefield.f90:40-43 (the M-PML blocks of
+// module_wavefield.f90:101-145 and their counterparts for the other nodes)
+__device__ __forceinline__ void e3_mpml(const El3dDev& a, int ax, int x, int y, int z, int hx, int hy, int hz,
+                                        float& ca, float& cb) {
+    const E3Mp& m = a.mp;
+    // beyond a face: reference index <= 0 (integer position) or <= 1 (half
+    // position), or >= n + 1 -- the node's own shell test on that axis
+    const int lo = a.pr;
+    const float rx = x < lo + hx ? __ldg(m.face[0] + z * a.NYs + y)
+                   : x >= lo + a.nx ? __ldg(m.face[1] + z * a.NYs + y) : 0.f;
+    const float ry = y < lo + hy ? __ldg(m.face[2] + z * a.pitch + x)
+                   : y >= lo + a.ny ? __ldg(m.face[3] + z * a.pitch + x) : 0.f;
+    const float rz = z < lo + hz ? __ldg(m.face[4] + y * a.pitch + x)
+                   : z >= lo + a.nz ? __ldg(m.face[5] + y * a.pitch + x) : 0.f;
+    const float dX = __ldg(m.d[0][hx] + x), dY = __ldg(m.d[1][hy] + y), dZ = __ldg(m.d[2][hz] + z);
+    float d, al;
+    if (ax == 0) { d = dX + ry * dY + rz * dZ; al = __ldg(m.al[0][hx] + x); }
+    else if (ax == 1) { d = dY + rx * dX + rz * dZ; al = __ldg(m.al[1][hy] + y); }
+    else { d = dZ + rx * dX + ry * dY; al = __ldg(m.al[2][hz] + z); }
+    const float b = d + al;
+    ca = -2.0f * m.adt * d / (2.0f + m.adt * b);
+    cb = (2.0f - m.adt * b) / (2.0f + m.adt * b);
+}
+
 struct E3Cell {
     int x, y, z, grp;
     long long o;
@@ -135,8 +179,8 @@ __device__ __forceinline__ bool e3_cell(const El3dDev& a, E3Cell& c) {
 #include "el3d_ring.cuh"
 
 // ------------------------------- forward ------------------------------------
-template <int R, bool STORE, bool FS>
-__global__ void __launch_bounds__(256, 3) k_el3d_fwd_s(El3dDev a) {
+template <int R, bool STORE, bool FS, bool MP>
+__global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_s(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
     const long long o = c.o, sy = a.pitch, sz = a.plane;
@@ -159,6 +203,25 @@ __global__ void __launch_bounds__(256, 3) k_el3d_fwd_s(El3dDev a) {
     const bool row1 = FS && z == a.pr, hz_ok = !FS || z > a.pr;
     const bool mir = FS && z > a.pr && z <= a.pr + a.R;
     const long long dzz = (long long)(2 * a.pr - 2 * z) * sz, dsh = dzz + sz;
+    // MP: the M-PML (a, b) of each derivative of the node (shell nodes only);
+    // otherwise the per-axis 1D tables above
+    float ca[9], cb[9];
+    if (MP) {
+        if (row1 || sh_n || sh_yz || sh_xz || sh_xy) {
+            e3_mpml(a, 0, x, y, z, 0, 0, 0, ca[0], cb[0]);
+            e3_mpml(a, 1, x, y, z, 0, 0, 0, ca[1], cb[1]);
+            e3_mpml(a, 2, x, y, z, 0, 0, 0, ca[2], cb[2]);
+            e3_mpml(a, 1, x, y, z, 0, 1, 1, ca[3], cb[3]);
+            e3_mpml(a, 2, x, y, z, 0, 1, 1, ca[4], cb[4]);
+            e3_mpml(a, 0, x, y, z, 1, 0, 1, ca[5], cb[5]);
+            e3_mpml(a, 2, x, y, z, 1, 0, 1, ca[6], cb[6]);
+            e3_mpml(a, 0, x, y, z, 1, 1, 0, ca[7], cb[7]);
+            e3_mpml(a, 1, x, y, z, 1, 1, 0, ca[8], cb[8]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) ca[q] = cb[q] = 0.f;
+        }
+    }
     for (int s = s0; s < s1; ++s) {
         float* st = a.st + s * a.sst;
         const float* vx = st + E3_VX * a.fs + o;
@@ -171,22 +234,22 @@ __global__ void __launch_bounds__(256, 3) k_el3d_fwd_s(El3dDev a) {
         const float zz0 = row1 ? 0.f : st[E3_ZZ * a.fs + o];
         const float yz0 = hz_ok ? st[E3_YZ * a.fs + o] : 0.f, xz0 = hz_ok ? st[E3_XZ * a.fs + o] : 0.f;
         const float xy0 = st[E3_XY * a.fs + o];
-        const bool p0 = (row1 || sh_n) && axi != 0.f, p1 = (row1 || sh_n) && ayi != 0.f, p2 = !row1 && sh_n && azi != 0.f;
-        const bool p3 = hz_ok && sh_yz && ayh != 0.f, p4 = hz_ok && sh_yz && azh != 0.f;
-        const bool p5 = hz_ok && sh_xz && axh != 0.f, p6 = hz_ok && sh_xz && azh != 0.f;
-        const bool p7 = sh_xy && axh != 0.f, p8 = sh_xy && ayh != 0.f;
+        const bool p0 = (row1 || sh_n) && (MP ? ca[0] : axi) != 0.f, p1 = (row1 || sh_n) && (MP ? ca[1] : ayi) != 0.f, p2 = !row1 && sh_n && (MP ? ca[2] : azi) != 0.f;
+        const bool p3 = hz_ok && sh_yz && (MP ? ca[3] : ayh) != 0.f, p4 = hz_ok && sh_yz && (MP ? ca[4] : azh) != 0.f;
+        const bool p5 = hz_ok && sh_xz && (MP ? ca[5] : axh) != 0.f, p6 = hz_ok && sh_xz && (MP ? ca[6] : azh) != 0.f;
+        const bool p7 = sh_xy && (MP ? ca[7] : axh) != 0.f, p8 = sh_xy && (MP ? ca[8] : ayh) != 0.f;
         const float m0 = p0 ? m[N_XVX * a.fs] : 0.f, m1 = p1 ? m[N_YVY * a.fs] : 0.f, m2 = p2 ? m[N_ZVZ * a.fs] : 0.f;
         const float m3 = p3 ? m[N_YVZ * a.fs] : 0.f, m4 = p4 ? m[N_ZVY * a.fs] : 0.f;
         const float m5 = p5 ? m[N_XVZ * a.fs] : 0.f, m6 = p6 ? m[N_ZVX * a.fs] : 0.f;
         const float m7 = p7 ? m[N_XVY * a.fs] : 0.f, m8 = p8 ? m[N_YVX * a.fs] : 0.f;
         float dX = a.idx * stP<R>(vx, 1), dY = a.idy * stP<R>(vy, sy), dZ;
-        if (p0) dX = pml_up(dX, axi, bxi, m0, m + N_XVX * a.fs);
-        if (p1) dY = pml_up(dY, ayi, byi, m1, m + N_YVY * a.fs);
+        if (p0) dX = pml_up(dX, MP ? ca[0] : axi, MP ? cb[0] : bxi, m0, m + N_XVX * a.fs);
+        if (p1) dY = pml_up(dY, MP ? ca[1] : ayi, MP ? cb[1] : byi, m1, m + N_YVY * a.fs);
         if (row1) {
             dZ = -(c13 / c33) * dX - (c23 / c33) * dY;
         } else {
             dZ = a.idz * stP<R>(vz, sz);
-            if (p2) dZ = pml_up(dZ, azi, bzi, m2, m + N_ZVZ * a.fs);
+            if (p2) dZ = pml_up(dZ, MP ? ca[2] : azi, MP ? cb[2] : bzi, m2, m + N_ZVZ * a.fs);
         }
         st[E3_XX * a.fs + o] = xx0 + a.dt * (c11 * dX + c12 * dY + c13 * dZ);
         st[E3_YY * a.fs + o] = yy0 + a.dt * (c12 * dX + c22 * dY + c23 * dZ);
@@ -202,24 +265,24 @@ __global__ void __launch_bounds__(256, 3) k_el3d_fwd_s(El3dDev a) {
             // syz: dz vy + dy vz
             dzvy = a.idz * stM<R>(vy, sz);
             dyvz = a.idy * stM<R>(vz, sy);
-            if (p3) dyvz = pml_up(dyvz, ayh, byh, m3, m + N_YVZ * a.fs);
-            if (p4) dzvy = pml_up(dzvy, azh, bzh, m4, m + N_ZVY * a.fs);
+            if (p3) dyvz = pml_up(dyvz, MP ? ca[3] : ayh, MP ? cb[3] : byh, m3, m + N_YVZ * a.fs);
+            if (p4) dzvy = pml_up(dzvy, MP ? ca[4] : azh, MP ? cb[4] : bzh, m4, m + N_ZVY * a.fs);
             const float yzn = yz0 + g44 * (dzvy + dyvz);
             st[E3_YZ * a.fs + o] = yzn;
             if (mir) st[E3_YZ * a.fs + o + dsh] = -yzn;
             // sxz: dz vx + dx vz
             dzvx = a.idz * stM<R>(vx, sz);
             dxvz = a.idx * stM<R>(vz, 1);
-            if (p5) dxvz = pml_up(dxvz, axh, bxh, m5, m + N_XVZ * a.fs);
-            if (p6) dzvx = pml_up(dzvx, azh, bzh, m6, m + N_ZVX * a.fs);
+            if (p5) dxvz = pml_up(dxvz, MP ? ca[5] : axh, MP ? cb[5] : bxh, m5, m + N_XVZ * a.fs);
+            if (p6) dzvx = pml_up(dzvx, MP ? ca[6] : azh, MP ? cb[6] : bzh, m6, m + N_ZVX * a.fs);
             const float xzn = xz0 + g55 * (dzvx + dxvz);
             st[E3_XZ * a.fs + o] = xzn;
             if (mir) st[E3_XZ * a.fs + o + dsh] = -xzn;
         }
         // sxy: dy vx + dx vy
         float dyvx = a.idy * stM<R>(vx, sy), dxvy = a.idx * stM<R>(vy, 1);
-        if (p7) dxvy = pml_up(dxvy, axh, bxh, m7, m + N_XVY * a.fs);
-        if (p8) dyvx = pml_up(dyvx, ayh, byh, m8, m + N_YVX * a.fs);
+        if (p7) dxvy = pml_up(dxvy, MP ? ca[7] : axh, MP ? cb[7] : bxh, m7, m + N_XVY * a.fs);
+        if (p8) dyvx = pml_up(dyvx, MP ? ca[8] : ayh, MP ? cb[8] : byh, m8, m + N_YVX * a.fs);
         st[E3_XY * a.fs + o] = xy0 + g66 * (dyvx + dxvy);
         if (STORE) {
             float* S = a.S + slot + s * a.fs + o;
@@ -230,8 +293,8 @@ __global__ void __launch_bounds__(256, 3) k_el3d_fwd_s(El3dDev a) {
     }
 }
 
-template <int R, bool STORE, bool FS>
-__global__ void __launch_bounds__(256, 3) k_el3d_fwd_v(El3dDev a) {
+template <int R, bool STORE, bool FS, bool MP>
+__global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_v(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
     const long long o = c.o, sy = a.pitch, sz = a.plane;
@@ -240,6 +303,25 @@ __global__ void __launch_bounds__(256, 3) k_el3d_fwd_v(El3dDev a) {
     const bool oyi = e3_out(y, a.pr, a.ny, false), oyh = e3_out(y, a.pr, a.ny, true);
     const bool ozi = e3_out(z, a.pr, a.nz, false), ozh = e3_out(z, a.pr, a.nz, true);
     const bool sh_vx = oxh || oyi || ozi, sh_vy = oxi || oyh || ozi, sh_vz = oxi || oyi || ozh;
+    // MP: the M-PML (a, b) of each derivative of the node (shell nodes only);
+    // otherwise the per-axis 1D tables above
+    float ca[9], cb[9];
+    if (MP) {
+        if (sh_vx || sh_vy || sh_vz) {
+            e3_mpml(a, 0, x, y, z, 1, 0, 0, ca[0], cb[0]);
+            e3_mpml(a, 1, x, y, z, 1, 0, 0, ca[1], cb[1]);
+            e3_mpml(a, 2, x, y, z, 1, 0, 0, ca[2], cb[2]);
+            e3_mpml(a, 0, x, y, z, 0, 1, 0, ca[3], cb[3]);
+            e3_mpml(a, 1, x, y, z, 0, 1, 0, ca[4], cb[4]);
+            e3_mpml(a, 2, x, y, z, 0, 1, 0, ca[5], cb[5]);
+            e3_mpml(a, 0, x, y, z, 0, 0, 1, ca[6], cb[6]);
+            e3_mpml(a, 1, x, y, z, 0, 0, 1, ca[7], cb[7]);
+            e3_mpml(a, 2, x, y, z, 0, 0, 1, ca[8], cb[8]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) ca[q] = cb[q] = 0.f;
+        }
+    }
     const float axi = a.axi[x], bxi = a.bxi[x], axh = a.axh[x], bxh = a.bxh[x];
     const float ayi = a.ayi[y], byi = a.byi[y], ayh = a.ayh[y], byh = a.byh[y];
     const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
@@ -260,34 +342,34 @@ __global__ void __launch_bounds__(256, 3) k_el3d_fwd_v(El3dDev a) {
         const bool vz_ok = !FS || z > a.pr;
         const float vx0 = st[E3_VX * a.fs + o], vy0 = st[E3_VY * a.fs + o];
         const float vz0 = vz_ok ? st[E3_VZ * a.fs + o] : 0.f;
-        const bool p0 = sh_vx && axh != 0.f, p1 = sh_vx && ayi != 0.f, p2 = sh_vx && azi != 0.f;
-        const bool p3 = sh_vy && axi != 0.f, p4 = sh_vy && ayh != 0.f, p5 = sh_vy && azi != 0.f;
-        const bool p6 = vz_ok && sh_vz && axi != 0.f, p7 = vz_ok && sh_vz && ayi != 0.f,
-                   p8 = vz_ok && sh_vz && azh != 0.f;
+        const bool p0 = sh_vx && (MP ? ca[0] : axh) != 0.f, p1 = sh_vx && (MP ? ca[1] : ayi) != 0.f, p2 = sh_vx && (MP ? ca[2] : azi) != 0.f;
+        const bool p3 = sh_vy && (MP ? ca[3] : axi) != 0.f, p4 = sh_vy && (MP ? ca[4] : ayh) != 0.f, p5 = sh_vy && (MP ? ca[5] : azi) != 0.f;
+        const bool p6 = vz_ok && sh_vz && (MP ? ca[6] : axi) != 0.f, p7 = vz_ok && sh_vz && (MP ? ca[7] : ayi) != 0.f,
+                   p8 = vz_ok && sh_vz && (MP ? ca[8] : azh) != 0.f;
         const float m0 = p0 ? m[N_XXX * a.fs] : 0.f, m1 = p1 ? m[N_YXY * a.fs] : 0.f, m2 = p2 ? m[N_ZXZ * a.fs] : 0.f;
         const float m3 = p3 ? m[N_XXY * a.fs] : 0.f, m4 = p4 ? m[N_YYY * a.fs] : 0.f, m5 = p5 ? m[N_ZYZ * a.fs] : 0.f;
         const float m6 = p6 ? m[N_XXZ * a.fs] : 0.f, m7 = p7 ? m[N_YYZ * a.fs] : 0.f, m8 = p8 ? m[N_ZZZ * a.fs] : 0.f;
         // vx: dx sxx (M) + dy sxy (P) + dz sxz (P)
         float h1 = a.idx * stM<R>(sxx, 1), h2 = a.idy * stP<R>(sxy, sy), h3 = a.idz * stP<R>(sxz, sz);
-        if (p0) h1 = pml_up(h1, axh, bxh, m0, m + N_XXX * a.fs);
-        if (p1) h2 = pml_up(h2, ayi, byi, m1, m + N_YXY * a.fs);
-        if (p2) h3 = pml_up(h3, azi, bzi, m2, m + N_ZXZ * a.fs);
+        if (p0) h1 = pml_up(h1, MP ? ca[0] : axh, MP ? cb[0] : bxh, m0, m + N_XXX * a.fs);
+        if (p1) h2 = pml_up(h2, MP ? ca[1] : ayi, MP ? cb[1] : byi, m1, m + N_YXY * a.fs);
+        if (p2) h3 = pml_up(h3, MP ? ca[2] : azi, MP ? cb[2] : bzi, m2, m + N_ZXZ * a.fs);
         const float hx = h1 + h2 + h3;
         st[E3_VX * a.fs + o] = vx0 + bx * hx;
         // vy: dx sxy (P) + dy syy (M) + dz syz (P)
         h1 = a.idx * stP<R>(sxy, 1); h2 = a.idy * stM<R>(syy, sy); h3 = a.idz * stP<R>(syz, sz);
-        if (p3) h1 = pml_up(h1, axi, bxi, m3, m + N_XXY * a.fs);
-        if (p4) h2 = pml_up(h2, ayh, byh, m4, m + N_YYY * a.fs);
-        if (p5) h3 = pml_up(h3, azi, bzi, m5, m + N_ZYZ * a.fs);
+        if (p3) h1 = pml_up(h1, MP ? ca[3] : axi, MP ? cb[3] : bxi, m3, m + N_XXY * a.fs);
+        if (p4) h2 = pml_up(h2, MP ? ca[4] : ayh, MP ? cb[4] : byh, m4, m + N_YYY * a.fs);
+        if (p5) h3 = pml_up(h3, MP ? ca[5] : azi, MP ? cb[5] : bzi, m5, m + N_ZYZ * a.fs);
         const float hy = h1 + h2 + h3;
         st[E3_VY * a.fs + o] = vy0 + by * hy;
         // vz: dx sxz (P) + dy syz (P) + dz szz (M); with a free surface from row 2
         float hz = 0.f;
         if (vz_ok) {
             h1 = a.idx * stP<R>(sxz, 1); h2 = a.idy * stP<R>(syz, sy); h3 = a.idz * stM<R>(szz, sz);
-            if (p6) h1 = pml_up(h1, axi, bxi, m6, m + N_XXZ * a.fs);
-            if (p7) h2 = pml_up(h2, ayi, byi, m7, m + N_YYZ * a.fs);
-            if (p8) h3 = pml_up(h3, azh, bzh, m8, m + N_ZZZ * a.fs);
+            if (p6) h1 = pml_up(h1, MP ? ca[6] : axi, MP ? cb[6] : bxi, m6, m + N_XXZ * a.fs);
+            if (p7) h2 = pml_up(h2, MP ? ca[7] : ayi, MP ? cb[7] : byi, m7, m + N_YYZ * a.fs);
+            if (p8) h3 = pml_up(h3, MP ? ca[8] : azh, MP ? cb[8] : bzh, m8, m + N_ZZZ * a.fs);
             hz = h1 + h2 + h3;
             st[E3_VZ * a.fs + o] = vz0 + bz * hz;
         }
@@ -307,8 +389,8 @@ __device__ __forceinline__ void e3_kahan(float* G, long long gg, long long go, i
     G[(12 + q) * gg + go] = c;
 }
 
-template <int R, bool FS>
-__global__ void __launch_bounds__(256, 3) k_el3d_adj_v(El3dDev a) {
+template <int R, bool FS, bool MP>
+__global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_v(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
     const long long o = c.o, sy = a.pitch, sz = a.plane;
@@ -319,6 +401,25 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_v(El3dDev a) {
     const bool oyi = e3_out(y, a.pr, a.ny, false), oyh = e3_out(y, a.pr, a.ny, true);
     const bool ozi = e3_out(z, a.pr, a.nz, false), ozh = e3_out(z, a.pr, a.nz, true);
     const bool sh_vx = oxh || oyi || ozi, sh_vy = oxi || oyh || ozi, sh_vz = oxi || oyi || ozh;
+    // MP: the M-PML (a, b) of each derivative of the node (shell nodes only);
+    // otherwise the per-axis 1D tables above
+    float ca[9], cb[9];
+    if (MP) {
+        if (sh_vx || sh_vy || sh_vz) {
+            e3_mpml(a, 0, x, y, z, 1, 0, 0, ca[0], cb[0]);
+            e3_mpml(a, 1, x, y, z, 1, 0, 0, ca[1], cb[1]);
+            e3_mpml(a, 2, x, y, z, 1, 0, 0, ca[2], cb[2]);
+            e3_mpml(a, 0, x, y, z, 0, 1, 0, ca[3], cb[3]);
+            e3_mpml(a, 1, x, y, z, 0, 1, 0, ca[4], cb[4]);
+            e3_mpml(a, 2, x, y, z, 0, 1, 0, ca[5], cb[5]);
+            e3_mpml(a, 0, x, y, z, 0, 0, 1, ca[6], cb[6]);
+            e3_mpml(a, 1, x, y, z, 0, 0, 1, ca[7], cb[7]);
+            e3_mpml(a, 2, x, y, z, 0, 0, 1, ca[8], cb[8]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) ca[q] = cb[q] = 0.f;
+        }
+    }
     const float axi = a.axi[x], bxi = a.bxi[x], axh = a.axh[x], bxh = a.bxh[x];
     const float ayi = a.ayi[y], byi = a.byi[y], ayh = a.ayh[y], byh = a.byh[y];
     const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
@@ -337,10 +438,10 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_v(El3dDev a) {
         const bool vz_ok = !FS || z > a.pr;
         const float vx0 = ad[E3_VX * a.fs + o], vy0 = ad[E3_VY * a.fs + o];
         const float vz0 = vz_ok ? ad[E3_VZ * a.fs + o] : 0.f;
-        const bool p0 = sh_vx && axh != 0.f, p1 = sh_vx && ayi != 0.f, p2 = sh_vx && azi != 0.f;
-        const bool p3 = sh_vy && axi != 0.f, p4 = sh_vy && ayh != 0.f, p5 = sh_vy && azi != 0.f;
-        const bool p6 = vz_ok && sh_vz && axi != 0.f, p7 = vz_ok && sh_vz && ayi != 0.f,
-                   p8 = vz_ok && sh_vz && azh != 0.f;
+        const bool p0 = sh_vx && (MP ? ca[0] : axh) != 0.f, p1 = sh_vx && (MP ? ca[1] : ayi) != 0.f, p2 = sh_vx && (MP ? ca[2] : azi) != 0.f;
+        const bool p3 = sh_vy && (MP ? ca[3] : axi) != 0.f, p4 = sh_vy && (MP ? ca[4] : ayh) != 0.f, p5 = sh_vy && (MP ? ca[5] : azi) != 0.f;
+        const bool p6 = vz_ok && sh_vz && (MP ? ca[6] : axi) != 0.f, p7 = vz_ok && sh_vz && (MP ? ca[7] : ayi) != 0.f,
+                   p8 = vz_ok && sh_vz && (MP ? ca[8] : azh) != 0.f;
         const float m0 = p0 ? mh[N_XXX * a.fs] : 0.f, m1 = p1 ? mh[N_YXY * a.fs] : 0.f, m2 = p2 ? mh[N_ZXZ * a.fs] : 0.f;
         const float m3 = p3 ? mh[N_XXY * a.fs] : 0.f, m4 = p4 ? mh[N_YYY * a.fs] : 0.f, m5 = p5 ? mh[N_ZYZ * a.fs] : 0.f;
         const float m6 = p6 ? mh[N_XXZ * a.fs] : 0.f, m7 = p7 ? mh[N_YYZ * a.fs] : 0.f, m8 = p8 ? mh[N_ZZZ * a.fs] : 0.f;
@@ -350,9 +451,9 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_v(El3dDev a) {
         ad[E3_VX * a.fs + o] = v;
         gx += v * __ldg(a.S + 6 * a.sterm + so);
         float q = bx * v, e1 = q, e2 = q, e3 = q;
-        if (p0) e1 = pml_adr(q, axh, bxh, m0, mh + N_XXX * a.fs);
-        if (p1) e2 = pml_adr(q, ayi, byi, m1, mh + N_YXY * a.fs);
-        if (p2) e3 = pml_adr(q, azi, bzi, m2, mh + N_ZXZ * a.fs);
+        if (p0) e1 = pml_adr(q, MP ? ca[0] : axh, MP ? cb[0] : bxh, m0, mh + N_XXX * a.fs);
+        if (p1) e2 = pml_adr(q, MP ? ca[1] : ayi, MP ? cb[1] : byi, m1, mh + N_YXY * a.fs);
+        if (p2) e3 = pml_adr(q, MP ? ca[2] : azi, MP ? cb[2] : bzi, m2, mh + N_ZXZ * a.fs);
         ew[N_XXX * a.fs] = e1; ew[N_YXY * a.fs] = e2; ew[N_ZXZ * a.fs] = e3;
         // vy^ += Dy^T e_yvy (P) + Dz^T e_zvy (M) + Dx^T e_xvy (M)
         v = vy0 + a.idy * tP<R>(e + N_YVY * a.fs, sy) + a.idz * tM<R>(e + N_ZVY * a.fs, sz) +
@@ -360,9 +461,9 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_v(El3dDev a) {
         ad[E3_VY * a.fs + o] = v;
         gy += v * __ldg(a.S + 7 * a.sterm + so);
         q = by * v; e1 = q; e2 = q; e3 = q;
-        if (p3) e1 = pml_adr(q, axi, bxi, m3, mh + N_XXY * a.fs);
-        if (p4) e2 = pml_adr(q, ayh, byh, m4, mh + N_YYY * a.fs);
-        if (p5) e3 = pml_adr(q, azi, bzi, m5, mh + N_ZYZ * a.fs);
+        if (p3) e1 = pml_adr(q, MP ? ca[3] : axi, MP ? cb[3] : bxi, m3, mh + N_XXY * a.fs);
+        if (p4) e2 = pml_adr(q, MP ? ca[4] : ayh, MP ? cb[4] : byh, m4, mh + N_YYY * a.fs);
+        if (p5) e3 = pml_adr(q, MP ? ca[5] : azi, MP ? cb[5] : bzi, m5, mh + N_ZYZ * a.fs);
         ew[N_XXY * a.fs] = e1; ew[N_YYY * a.fs] = e2; ew[N_ZYZ * a.fs] = e3;
         // vz^ += Dz^T e_zvz (P) + Dy^T e_yvz (M) + Dx^T e_xvz (M); with a free surface from row 2
         if (vz_ok) {
@@ -371,9 +472,9 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_v(El3dDev a) {
             ad[E3_VZ * a.fs + o] = v;
             gz += v * __ldg(a.S + 8 * a.sterm + so);
             q = bz * v; e1 = q; e2 = q; e3 = q;
-            if (p6) e1 = pml_adr(q, axi, bxi, m6, mh + N_XXZ * a.fs);
-            if (p7) e2 = pml_adr(q, ayi, byi, m7, mh + N_YYZ * a.fs);
-            if (p8) e3 = pml_adr(q, azh, bzh, m8, mh + N_ZZZ * a.fs);
+            if (p6) e1 = pml_adr(q, MP ? ca[6] : axi, MP ? cb[6] : bxi, m6, mh + N_XXZ * a.fs);
+            if (p7) e2 = pml_adr(q, MP ? ca[7] : ayi, MP ? cb[7] : byi, m7, mh + N_YYZ * a.fs);
+            if (p8) e3 = pml_adr(q, MP ? ca[8] : azh, MP ? cb[8] : bzh, m8, mh + N_ZZZ * a.fs);
             ew[N_XXZ * a.fs] = e1; ew[N_YYZ * a.fs] = e2; ew[N_ZZZ * a.fs] = e3;
         }
     }
@@ -383,8 +484,8 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_v(El3dDev a) {
     e3_kahan(a.G, a.gg, go, 11, gz);
 }
 
-template <int R, bool FS>
-__global__ void __launch_bounds__(256, 3) k_el3d_adj_s(El3dDev a) {
+template <int R, bool FS, bool MP>
+__global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_s(El3dDev a) {
     E3Cell c;
     if (!e3_cell(a, c)) return;
     const long long o = c.o, sy = a.pitch, sz = a.plane;
@@ -395,6 +496,25 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_s(El3dDev a) {
     const bool oyi = e3_out(y, a.pr, a.ny, false), oyh = e3_out(y, a.pr, a.ny, true);
     const bool ozi = e3_out(z, a.pr, a.nz, false), ozh = e3_out(z, a.pr, a.nz, true);
     const bool sh_n = oxi || oyi || ozi, sh_yz = oxi || oyh || ozh, sh_xz = oxh || oyi || ozh, sh_xy = oxh || oyh || ozi;
+    // MP: the M-PML (a, b) of each derivative of the node (shell nodes only);
+    // otherwise the per-axis 1D tables above
+    float ca[9], cb[9];
+    if (MP) {
+        if (sh_n || sh_yz || sh_xz || sh_xy) {
+            e3_mpml(a, 0, x, y, z, 0, 0, 0, ca[0], cb[0]);
+            e3_mpml(a, 1, x, y, z, 0, 0, 0, ca[1], cb[1]);
+            e3_mpml(a, 2, x, y, z, 0, 0, 0, ca[2], cb[2]);
+            e3_mpml(a, 2, x, y, z, 0, 1, 1, ca[3], cb[3]);
+            e3_mpml(a, 1, x, y, z, 0, 1, 1, ca[4], cb[4]);
+            e3_mpml(a, 2, x, y, z, 1, 0, 1, ca[5], cb[5]);
+            e3_mpml(a, 0, x, y, z, 1, 0, 1, ca[6], cb[6]);
+            e3_mpml(a, 1, x, y, z, 1, 1, 0, ca[7], cb[7]);
+            e3_mpml(a, 0, x, y, z, 1, 1, 0, ca[8], cb[8]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) ca[q] = cb[q] = 0.f;
+        }
+    }
     const float axi = a.axi[x], bxi = a.bxi[x], axh = a.axh[x], bxh = a.bxh[x];
     const float ayi = a.ayi[y], byi = a.byi[y], ayh = a.ayh[y], byh = a.byh[y];
     const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
@@ -422,10 +542,10 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_s(El3dDev a) {
         const float zz0 = row1 ? 0.f : ad[E3_ZZ * a.fs + o];
         const float yz0 = hz_ok ? ad[E3_YZ * a.fs + o] : 0.f, xz0 = hz_ok ? ad[E3_XZ * a.fs + o] : 0.f;
         const float xy0 = ad[E3_XY * a.fs + o];
-        const bool p0 = (row1 || sh_n) && axi != 0.f, p1 = (row1 || sh_n) && ayi != 0.f, p2 = !row1 && sh_n && azi != 0.f;
-        const bool p3 = hz_ok && sh_yz && azh != 0.f, p4 = hz_ok && sh_yz && ayh != 0.f;
-        const bool p5 = hz_ok && sh_xz && azh != 0.f, p6 = hz_ok && sh_xz && axh != 0.f;
-        const bool p7 = sh_xy && ayh != 0.f, p8 = sh_xy && axh != 0.f;
+        const bool p0 = (row1 || sh_n) && (MP ? ca[0] : axi) != 0.f, p1 = (row1 || sh_n) && (MP ? ca[1] : ayi) != 0.f, p2 = !row1 && sh_n && (MP ? ca[2] : azi) != 0.f;
+        const bool p3 = hz_ok && sh_yz && (MP ? ca[3] : azh) != 0.f, p4 = hz_ok && sh_yz && (MP ? ca[4] : ayh) != 0.f;
+        const bool p5 = hz_ok && sh_xz && (MP ? ca[5] : azh) != 0.f, p6 = hz_ok && sh_xz && (MP ? ca[6] : axh) != 0.f;
+        const bool p7 = sh_xy && (MP ? ca[7] : ayh) != 0.f, p8 = sh_xy && (MP ? ca[8] : axh) != 0.f;
         const float m0 = p0 ? mh[N_XVX * a.fs] : 0.f, m1 = p1 ? mh[N_YVY * a.fs] : 0.f, m2 = p2 ? mh[N_ZVZ * a.fs] : 0.f;
         const float m3 = p3 ? mh[N_ZVY * a.fs] : 0.f, m4 = p4 ? mh[N_YVZ * a.fs] : 0.f;
         const float m5 = p5 ? mh[N_ZVX * a.fs] : 0.f, m6 = p6 ? mh[N_XVZ * a.fs] : 0.f;
@@ -480,8 +600,8 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_s(El3dDev a) {
             const float w = a.dt * (c13 * xh + c23 * yh);
             qx = a.dt * (c11 * xh + c12 * yh) - r13 * w;
             qy = a.dt * (c12 * xh + c22 * yh) - r23 * w;
-            if (p0) qx = pml_adr(qx, axi, bxi, m0, mh + N_XVX * a.fs);
-            if (p1) qy = pml_adr(qy, ayi, byi, m1, mh + N_YVY * a.fs);
+            if (p0) qx = pml_adr(qx, MP ? ca[0] : axi, MP ? cb[0] : bxi, m0, mh + N_XVX * a.fs);
+            if (p1) qy = pml_adr(qy, MP ? ca[1] : ayi, MP ? cb[1] : byi, m1, mh + N_YVY * a.fs);
         } else {
             G[0] += xh * dX;
             G[1] += xh * dY + yh * dX;
@@ -492,9 +612,9 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_s(El3dDev a) {
             qx = a.dt * (c11 * xh + c12 * yh + c13 * zh);
             qy = a.dt * (c12 * xh + c22 * yh + c23 * zh);
             qz = a.dt * (c13 * xh + c23 * yh + c33 * zh);
-            if (p0) qx = pml_adr(qx, axi, bxi, m0, mh + N_XVX * a.fs);
-            if (p1) qy = pml_adr(qy, ayi, byi, m1, mh + N_YVY * a.fs);
-            if (p2) qz = pml_adr(qz, azi, bzi, m2, mh + N_ZVZ * a.fs);
+            if (p0) qx = pml_adr(qx, MP ? ca[0] : axi, MP ? cb[0] : bxi, m0, mh + N_XVX * a.fs);
+            if (p1) qy = pml_adr(qy, MP ? ca[1] : ayi, MP ? cb[1] : byi, m1, mh + N_YVY * a.fs);
+            if (p2) qz = pml_adr(qz, MP ? ca[2] : azi, MP ? cb[2] : bzi, m2, mh + N_ZVZ * a.fs);
         }
         ew[N_XVX * a.fs] = qx; ew[N_YVY * a.fs] = qy; ew[N_ZVZ * a.fs] = qz;
         float q, e1, e2;
@@ -502,18 +622,18 @@ __global__ void __launch_bounds__(256, 3) k_el3d_adj_s(El3dDev a) {
             G[6] += yzh * __ldg(S + 3 * a.sterm);
             G[7] += xzh * __ldg(S + 4 * a.sterm);
             q = g44 * yzh; e1 = q; e2 = q;
-            if (p3) e1 = pml_adr(q, azh, bzh, m3, mh + N_ZVY * a.fs);
-            if (p4) e2 = pml_adr(q, ayh, byh, m4, mh + N_YVZ * a.fs);
+            if (p3) e1 = pml_adr(q, MP ? ca[3] : azh, MP ? cb[3] : bzh, m3, mh + N_ZVY * a.fs);
+            if (p4) e2 = pml_adr(q, MP ? ca[4] : ayh, MP ? cb[4] : byh, m4, mh + N_YVZ * a.fs);
             ew[N_ZVY * a.fs] = e1; ew[N_YVZ * a.fs] = e2;
             q = g55 * xzh; e1 = q; e2 = q;
-            if (p5) e1 = pml_adr(q, azh, bzh, m5, mh + N_ZVX * a.fs);
-            if (p6) e2 = pml_adr(q, axh, bxh, m6, mh + N_XVZ * a.fs);
+            if (p5) e1 = pml_adr(q, MP ? ca[5] : azh, MP ? cb[5] : bzh, m5, mh + N_ZVX * a.fs);
+            if (p6) e2 = pml_adr(q, MP ? ca[6] : axh, MP ? cb[6] : bxh, m6, mh + N_XVZ * a.fs);
             ew[N_ZVX * a.fs] = e1; ew[N_XVZ * a.fs] = e2;
         }
         G[8] += xyh * __ldg(S + 5 * a.sterm);
         q = g66 * xyh; e1 = q; e2 = q;
-        if (p7) e1 = pml_adr(q, ayh, byh, m7, mh + N_YVX * a.fs);
-        if (p8) e2 = pml_adr(q, axh, bxh, m8, mh + N_XVY * a.fs);
+        if (p7) e1 = pml_adr(q, MP ? ca[7] : ayh, MP ? cb[7] : byh, m7, mh + N_YVX * a.fs);
+        if (p8) e2 = pml_adr(q, MP ? ca[8] : axh, MP ? cb[8] : bxh, m8, mh + N_XVY * a.fs);
         ew[N_YVX * a.fs] = e1; ew[N_XVY * a.fs] = e2;
     }
     const long long go = (long long)c.grp * a.fs + o;
@@ -718,6 +838,117 @@ struct El3dEngine : SsgBase {
     float idx, idy, idz;
     DevBuf<float> c11, c12, c13, c22, c23, c33, c44e, c55e, c66e, bxp, byp, bzp;
     DevBuf<float> c44p, c55p, c66p, rhop, p0p, p1p, tabx, taby, tabz, tparp;
+    // M-PML: nonzero face ratios, the faces in the layout of owl_ssg_mpml_ratios,
+    // per-axis profiles (d and alpha at integer and half positions) and the
+    // faces in storage layout
+    bool mpml = false;
+    std::vector<float> h_faces;
+    DevBuf<float> mp_prof, mp_face;
+    const std::vector<float>* mpml_faces() const override { return &h_faces; }
+
+    // the M-PML tables of the model (module_cfspml.f90:421-625): damping and
+    // alpha profiles per axis, and the six faces' ratios (zero for iso)
+    void build_mpml(const std::vector<float>* hc, float pmlvp, float alphamax) {
+        const bool fsf = desc.free_surface != 0;
+        const int len[3] = {pitch, NYs, NZs}, nn[3] = {nx, ny, nz};
+        const float dd[3] = {desc.dx, desc.dy, desc.dz};
+        const float R0 = 1.0e-5f;
+        std::vector<float> prof;
+        for (int ax = 0; ax < 3; ++ax) {
+            const int L = len[ax], n = nn[ax];
+            std::vector<float> t(4 * (size_t)L, 0.f);
+            std::fill(t.begin() + 2 * L, t.end(), alphamax);
+            const bool low = !(ax == 2 && fsf);  // no top PML under a free surface
+            for (int i = -P + 1; i <= n + P; ++i) {
+                float nd, ndh;
+                if (i <= 1) {
+                    if (!low) continue;
+                    nd = (float)std::abs(i - 1) * 1.0f / (float)P;
+                    ndh = std::fabs((float)(i - 1) - 0.5f) * 1.0f / (float)P;
+                } else if (i >= n) {
+                    nd = (float)std::abs(i - n) * 1.0f / (float)P;
+                    ndh = std::fabs((float)(i - n) - 0.5f) * 1.0f / (float)P;
+                } else {
+                    continue;
+                }
+                const float c0 = std::log(1.0f / R0) * 3.0f * pmlvp / (2.0f * (float)P * dd[ax]);
+                const int x = i + pr - 1;
+                t[x] = c0 * (nd * nd);
+                t[L + x] = c0 * (ndh * ndh);
+                t[2 * (size_t)L + x] = std::max(alphamax * (1.0f - nd), 0.25f * alphamax);
+                t[3 * (size_t)L + x] = std::max(alphamax * (1.0f - ndh), 0.25f * alphamax);
+            }
+            prof.insert(prof.end(), t.begin(), t.end());
+        }
+        const size_t fx = (size_t)NYp * NZp, fy = (size_t)NXp * NZp, fz = (size_t)NXp * NYp;
+        h_faces.assign(2 * (fx + fy + fz), 0.f);
+        float* fL = h_faces.data();
+        float* fR = fL + fx;
+        float* fF = fR + fx;
+        float* fB = fF + fy;
+        float* fT = fB + fy;
+        float* fO = fT + fz;
+        if (aniso != OWL_ANISO_ISO) {
+            // the x / y faces span the rows the solver updates: from row 1 under a free surface
+            const int z1 = fsf ? 1 : -P + 1, n2 = nz + P - z1 + 1, zoff = z1 + P - 1;
+            auto cell = [&](int i, int j, int k, float* c) {
+                const long long o = soff(i, j, k);
+                for (int q = 0; q < 9; ++q) c[q] = hc[q][o];
+            };
+            mpml_face(NYp, n2, 0, [&](int a, int b, float* c) { cell(1, -P + 1 + a, z1 + b, c); },
+                      fL + (size_t)zoff * NYp, NYp);
+            mpml_face(NYp, n2, 0, [&](int a, int b, float* c) { cell(nx, -P + 1 + a, z1 + b, c); },
+                      fR + (size_t)zoff * NYp, NYp);
+            mpml_face(NXp, n2, 1, [&](int a, int b, float* c) { cell(-P + 1 + a, 1, z1 + b, c); },
+                      fF + (size_t)zoff * NXp, NXp);
+            mpml_face(NXp, n2, 1, [&](int a, int b, float* c) { cell(-P + 1 + a, ny, z1 + b, c); },
+                      fB + (size_t)zoff * NXp, NXp);
+            mpml_face(NXp, NYp, 2, [&](int a, int b, float* c) { cell(-P + 1 + a, -P + 1 + b, 1, c); }, fT, NXp);
+            mpml_face(NXp, NYp, 2, [&](int a, int b, float* c) { cell(-P + 1 + a, -P + 1 + b, nz, c); }, fO, NXp);
+        }
+        mpml = std::any_of(h_faces.begin(), h_faces.end(), [](float v) { return v != 0.f; });
+        // storage layout: x faces [z][y] (NYs), y faces [z][x], z faces [y][x] (pitch)
+        const size_t sx = (size_t)NZs * NYs, sy = (size_t)NZs * pitch, sz = (size_t)NYs * pitch;
+        std::vector<float> hf(2 * (sx + sy + sz), 0.f);
+        for (int k = 0; k < NZp; ++k)
+            for (int j = 0; j < NYp; ++j) {
+                hf[(size_t)(k + R) * NYs + (j + R)] = fL[(size_t)k * NYp + j];
+                hf[sx + (size_t)(k + R) * NYs + (j + R)] = fR[(size_t)k * NYp + j];
+            }
+        for (int k = 0; k < NZp; ++k)
+            for (int i = 0; i < NXp; ++i) {
+                hf[2 * sx + (size_t)(k + R) * pitch + (i + R)] = fF[(size_t)k * NXp + i];
+                hf[2 * sx + sy + (size_t)(k + R) * pitch + (i + R)] = fB[(size_t)k * NXp + i];
+            }
+        for (int j = 0; j < NYp; ++j)
+            for (int i = 0; i < NXp; ++i) {
+                hf[2 * sx + 2 * sy + (size_t)(j + R) * pitch + (i + R)] = fT[(size_t)j * NXp + i];
+                hf[2 * sx + 2 * sy + sz + (size_t)(j + R) * pitch + (i + R)] = fO[(size_t)j * NXp + i];
+            }
+        mp_prof.upload(prof.data(), prof.size(), stream);
+        mp_face.upload(hf.data(), hf.size(), stream);
+    }
+    E3Mp mp_view() const {
+        E3Mp m{};
+        const int len[3] = {pitch, NYs, NZs};
+        size_t off = 0;
+        for (int ax = 0; ax < 3; ++ax) {
+            m.d[ax][0] = mp_prof.p + off;
+            m.d[ax][1] = mp_prof.p + off + len[ax];
+            m.al[ax][0] = mp_prof.p + off + 2 * (size_t)len[ax];
+            m.al[ax][1] = mp_prof.p + off + 3 * (size_t)len[ax];
+            off += 4 * (size_t)len[ax];
+        }
+        const size_t sx = (size_t)NZs * NYs, sy = (size_t)NZs * pitch, sz = (size_t)NYs * pitch;
+        m.face[0] = mp_face.p;
+        m.face[1] = mp_face.p + sx;
+        m.face[2] = mp_face.p + 2 * sx;
+        m.face[3] = mp_face.p + 2 * sx + sy;
+        m.face[4] = mp_face.p + 2 * sx + 2 * sy;
+        m.face[5] = mp_face.p + 2 * sx + 2 * sy + sz;
+        m.adt = std::fabs(dt);
+        return m;
+    }
 
     explicit El3dEngine(const owl_ssg_desc& d) : SsgBase(d, 3) {
         aniso = d.aniso;
@@ -745,13 +976,15 @@ struct El3dEngine : SsgBase {
     // ring kernels (half-width 4, no free surface)
     // (the adjoint pass likewise, with the ring adjoint kernels)
     std::vector<int> tune_tz(int) const override {
-        if (R == 4 && !desc.free_surface) return {2, 1};
+        if (ring_ok()) return {2, 1};
         return {2};
     }
+    // the ring kernels: half-width 4, no free surface, zero M-PML ratios
+    bool ring_ok() const { return R == 4 && !desc.free_surface && !mpml; }
     // tile_z = 1 asks for the ring kernels of both passes (where they apply), anything else the per-cell ones
     void launch_params(const owl_run_opts& o) override {
         tile_x = 32;
-        tz_f = (o.tile_z == 1 && R == 4 && !desc.free_surface) ? 1 : 2;
+        tz_f = (o.tile_z == 1 && ring_ok()) ? 1 : 2;
         tz_a = tz_f;
     }
 
@@ -836,6 +1069,7 @@ struct El3dEngine : SsgBase {
         e3_axis(nx, P, R, pitch, desc.dx, dt, pmlvp, alphamax, tx);
         e3_axis(ny, P, R, NYs, desc.dy, dt, pmlvp, alphamax, ty);
         e3_axis(nz, P, R, NZs, desc.dz, dt, pmlvp, alphamax, tz, desc.free_surface == 0);
+        build_mpml(hc, pmlvp, alphamax);
         c11.upload(hc[0].data(), fs, stream); c12.upload(hc[1].data(), fs, stream); c13.upload(hc[2].data(), fs, stream);
         c22.upload(hc[3].data(), fs, stream); c23.upload(hc[4].data(), fs, stream); c33.upload(hc[5].data(), fs, stream);
         c44e.upload(h44.data(), fs, stream); c55e.upload(h55.data(), fs, stream); c66e.upload(h66.data(), fs, stream);
@@ -966,6 +1200,7 @@ struct El3dEngine : SsgBase {
             a.G = G.p;
             a.gg = (long long)((S + spt_a - 1) / spt_a) * fs;
         }
+        a.mp = mp_view();
         return a;
     }
 
@@ -978,7 +1213,7 @@ struct El3dEngine : SsgBase {
         const int groups = (S + a.spt - 1) / a.spt;
         OWL_CHECK((long long)a.nzb * groups < 65536, OWL_ERR_UNSUPPORTED, "too many z blocks x shot groups");
         const dim3 b(32, 4, 2), g((NXp + 31) / 32, (NYp + 3) / 4, a.nzb * groups);
-        if ((fwd ? tz_f : tz_a) == 1 && RR == 4 && !FF) {
+        if ((fwd ? tz_f : tz_a) == 1 && RR == 4 && !FF && !mpml) {
             OWL_CHECK(fwd ? (!store || a.S) : (a.ad && a.S && a.G), OWL_ERR_INVALID, "buffers not allocated");
             const int rows = a.z1 - a.z0;
             const long long xy = (long long)((NXp + 31) / 32) * ((NYp + 7) / 8);
@@ -1008,21 +1243,26 @@ struct El3dEngine : SsgBase {
             }
             return;
         }
-        if (fwd) {
-            OWL_CHECK(!store || a.S, OWL_ERR_INVALID, "stencil-term buffer not allocated");
-            if (id == OWL_K_FWD_P) {
-                auto k = store ? (FF ? k_el3d_fwd_s<RR, true, true> : k_el3d_fwd_s<RR, true, false>)
-                               : (FF ? k_el3d_fwd_s<RR, false, true> : k_el3d_fwd_s<RR, false, false>);
-                k<<<g, b, 0, stream>>>(a);
-            } else {
-                auto k = store ? (FF ? k_el3d_fwd_v<RR, true, true> : k_el3d_fwd_v<RR, true, false>)
-                               : (FF ? k_el3d_fwd_v<RR, false, true> : k_el3d_fwd_v<RR, false, false>);
-                k<<<g, b, 0, stream>>>(a);
-            }
+        if (fwd) OWL_CHECK(!store || a.S, OWL_ERR_INVALID, "stencil-term buffer not allocated");
+        else OWL_CHECK(a.ad && a.S && a.G, OWL_ERR_INVALID, "adjoint buffers not allocated");
+        if (mpml) launch_cell<RR, true>(id, store, FF, a, g, b);
+        else launch_cell<RR, false>(id, store, FF, a, g, b);
+    }
+    // the per-cell kernels; MP: M-PML coefficients per shell node
+    template <int RR, bool MP>
+    void launch_cell(int id, bool store, bool FF, const El3dDev& a, dim3 g, dim3 b) {
+        if (id == OWL_K_FWD_P) {
+            auto k = store ? (FF ? k_el3d_fwd_s<RR, true, true, MP> : k_el3d_fwd_s<RR, true, false, MP>)
+                           : (FF ? k_el3d_fwd_s<RR, false, true, MP> : k_el3d_fwd_s<RR, false, false, MP>);
+            k<<<g, b, 0, stream>>>(a);
+        } else if (id == OWL_K_FWD_V) {
+            auto k = store ? (FF ? k_el3d_fwd_v<RR, true, true, MP> : k_el3d_fwd_v<RR, true, false, MP>)
+                           : (FF ? k_el3d_fwd_v<RR, false, true, MP> : k_el3d_fwd_v<RR, false, false, MP>);
+            k<<<g, b, 0, stream>>>(a);
+        } else if (id == OWL_K_ADJ_P) {
+            (FF ? k_el3d_adj_v<RR, true, MP> : k_el3d_adj_v<RR, false, MP>)<<<g, b, 0, stream>>>(a);
         } else {
-            OWL_CHECK(a.ad && a.S && a.G, OWL_ERR_INVALID, "adjoint buffers not allocated");
-            if (id == OWL_K_ADJ_P) (FF ? k_el3d_adj_v<RR, true> : k_el3d_adj_v<RR, false>)<<<g, b, 0, stream>>>(a);
-            else (FF ? k_el3d_adj_s<RR, true> : k_el3d_adj_s<RR, false>)<<<g, b, 0, stream>>>(a);
+            (FF ? k_el3d_adj_s<RR, true, MP> : k_el3d_adj_s<RR, false, MP>)<<<g, b, 0, stream>>>(a);
         }
     }
     void launch_kernel(int id, int S, bool store) override {

@@ -1,6 +1,8 @@
 // engine.cuh -- medium-independent engine interface and shared kernels.
 #pragma once
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace owl {
@@ -31,6 +33,8 @@ struct Engine {
     // sources): data_nt samples at data_dt from t = 0; data_nt <= 0: the time axis
     int data_nt = 0;
     float data_dt = 0.f;
+    // M-PML face ratios of the model (elastic 3D; null elsewhere), the layout of owl_ssg_mpml_ratios
+    virtual const std::vector<float>* mpml_faces() const { return nullptr; }
 };
 
 Engine* make_ac2d_engine(const owl_ssg_desc& d);

@@ -369,6 +369,15 @@ class SSGSolver:
                                         C.byref(self.last_info)))
         return (misfit, tm) if traces else misfit
 
+    def mpml_ratios(self) -> np.ndarray:
+        """The six M-PML face-ratio arrays of an elastic 3D model (left, right,
+        front, back, top, bottom; the layout of owl_ssg_mpml_ratios)."""
+        d = self.desc
+        nx, ny, nz = d.nx + 2 * d.pml, d.ny + 2 * d.pml, d.nz + 2 * d.pml
+        out = np.zeros(2 * (ny * nz + nx * nz + nx * ny), dtype=f32)
+        L.check(self.lib.owl_ssg_mpml_ratios(self.h, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
     def kernel_time(self, kernel_id: int, nlaunch: int = 20) -> Tuple[float, float]:
         """(mean ms per launch, algorithmic bytes per launch) of one kernel on the last batch state."""
         ms, b = C.c_double(), C.c_double()

@@ -1,6 +1,8 @@
 """GPU parity tests of the 3D elastic path through the C ABI, with and without
 the free surface: forward (vx, vy, vz) vs the FP32 oracle at 1e-5 relative L2;
-gradient vs the FP64 exact-adjoint oracle at 1e-4; source-side gradient."""
+gradient vs the FP64 exact-adjoint oracle at 1e-4; source-side gradient. The
+anisotropic parameterisations run with their M-PML damping ratios (nonzero),
+the isotropic one with zero ratios, as the reference."""
 import numpy as np
 import pytest
 
@@ -18,10 +20,15 @@ GRAD_TOL = 1e-4
 
 
 def make(d, f):
+    """The solver of the model; the oracle runs that follow use the M-PML face
+    ratios the library computed for it (all zero for iso), which
+    test_mpml_faces_match_the_restated_search checks separately."""
     s = SSGSolver(L.OWL_ELASTIC_VHTIORT_3D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
                   free_surface=bool(d.free_surface), f0_max=d.f0_max, max_shots=d.max_shots, ny=d.ny, dy=d.dy,
                   aniso=d.aniso)
     s.set_model(*f)
+    faces = s.mpml_ratios()
+    oracle.el3d_set_mpml(faces if np.any(faces) else None)
     return s
 
 
@@ -99,3 +106,55 @@ def test_el3d_half_checkpoints_of_tiny_fields():
         _, g = s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=50, checkpoint_precision=prec))
         assert np.all(np.isfinite(g)), prec
         assert rel(g, g32) < 1e-3, (prec, rel(g, g32))
+
+
+@pytest.mark.parametrize("fs", [0, 1])
+@pytest.mark.parametrize("aniso", [L.OWL_ANISO_ISO, L.OWL_ANISO_CIJ])
+def test_mpml_faces_match_the_restated_search(aniso, fs):
+    """The library's six face-ratio arrays: zero for iso; for anisotropic media
+    the damping-ratio search at every 10th face cell, interpolated, exactly as
+    the oracle's restatement of compute_damping_profile_ratio_face arranges it
+    (fed the library's own single-cell search, which test_mpml_cpu checks
+    against the literal 27 x 27 eigen-derivative form)."""
+    from oracle import oracle_mpml as M
+    d = el3_desc(aniso, fs=fs)
+    f = el3_model(aniso)
+    s = make(d, f)
+    faces = s.mpml_ratios()
+    if aniso == L.OWL_ANISO_ISO:
+        assert not np.any(faces)
+        return
+    assert np.all(faces >= 0) and np.any(faces > 0)
+    lib = L.load()
+    P, n = d.pml, N
+    npad = n + 2 * P
+    # stiffness of a face cell: the model's edge cell (the padded model replicates it)
+    C9 = [np.asarray(f[q], dtype=np.float32) for q in range(9)]
+
+    def c_at(i, j, k):  # reference indices, clamped to the model
+        ii, jj, kk = (min(max(v, 1), n) - 1 for v in (i, j, k))
+        return np.array([c[ii, jj, kk] for c in C9], dtype=np.float32)
+
+    def lib_ratio(c, direction):
+        cc = np.ascontiguousarray(c, dtype=np.float32)
+        return float(lib.owl_mpml_damp_ratio(cc.ctypes.data_as(L.C.POINTER(L.C.c_float)), "xyz".index(direction)))
+
+    z1 = 1 if fs else -P + 1
+    nzf = n + P - z1 + 1
+    fx, fy, fz = npad * npad, npad * npad, npad * npad
+    views = [faces[0:fx].reshape(npad, npad), faces[fx:2 * fx].reshape(npad, npad),
+             faces[2 * fx:2 * fx + fy].reshape(npad, npad), faces[2 * fx + fy:2 * fx + 2 * fy].reshape(npad, npad),
+             faces[2 * fx + 2 * fy:2 * fx + 2 * fy + fz].reshape(npad, npad), faces[2 * fx + 2 * fy + fz:].reshape(npad, npad)]
+    zoff = z1 + P - 1
+    specs = [("x", lambda a, b: c_at(1, -P + 1 + a, z1 + b), npad, nzf, zoff),
+             ("x", lambda a, b: c_at(n, -P + 1 + a, z1 + b), npad, nzf, zoff),
+             ("y", lambda a, b: c_at(-P + 1 + a, 1, z1 + b), npad, nzf, zoff),
+             ("y", lambda a, b: c_at(-P + 1 + a, n, z1 + b), npad, nzf, zoff),
+             ("z", lambda a, b: c_at(-P + 1 + a, -P + 1 + b, 1), npad, npad, 0),
+             ("z", lambda a, b: c_at(-P + 1 + a, -P + 1 + b, n), npad, npad, 0)]
+    for (direction, cell, n1, n2, off), got in zip(specs, views):
+        cf = np.array([[cell(a, b) for b in range(n2)] for a in range(n1)])
+        want = M.face_ratio(cf, direction, ratio_fn=lib_ratio)  # (n1, n2)
+        assert np.allclose(got[off:off + n2, :].T, want, rtol=0, atol=1e-6), direction
+        if off:
+            assert not np.any(got[:off])
