@@ -22,6 +22,7 @@
 
 #include "ring.cuh"
 #include "ssg_base.cuh"
+#include "tma.cuh"
 
 #ifndef OWL_AC3_ZCHUNK_MIN
 #define OWL_AC3_ZCHUNK_MIN 16  // shortest z chunk of a forward CTA
@@ -50,6 +51,7 @@ struct Ac3dDev {
     float *ap, *avx, *avy, *avz, *am0, *am1, *am2, *am3, *am4, *am5;
     float *aex, *aey, *aez, *aepx, *aepy, *aepz;
     float *Gbk, *Gbx, *Gby, *Gbz, *Cbk, *Cbx, *Cby, *Cbz;
+    int* err;  // set by a TMA wait that gave up (OWL_ERR_TIMEOUT on the host)
 };
 
 // slab indices (only called for nodes inside the corresponding PML)
@@ -86,6 +88,7 @@ __device__ __forceinline__ void load_xy_tiles(float (*tx_)[32 + 2 * R], float (*
 
 // ------------------------------- forward ------------------------------------
 #include "ac3d_fwd.cuh"
+#include "ac3d_fwd_tma.cuh"
 
 // One thread per cell, block 32 x 4 x 2, every neighbour an independent
 // read-only load (served by L1 / L2): low register count, full occupancy and
@@ -633,6 +636,7 @@ struct Ac3dEngine : SsgBase {
         a.m3 = s0 + st_off(7); a.m4 = s0 + st_off(8); a.m5 = s0 + st_off(9);
         a.k = std::max(1, cur_k);
         a.d_step = ctr.p;
+        a.err = ctr.p + 3;
         const long long F = (long long)S * fs;
         if (Sbuf.p && Sbuf.n >= (size_t)4 * a.k * F) {
             a.sslot = F;
@@ -687,6 +691,55 @@ struct Ac3dEngine : SsgBase {
             auto k = store ? k_ac3d_fwd_v<RR, RY, true> : k_ac3d_fwd_v<RR, RY, false>;
             OWL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
             k<<<grid3(rows_v, S, spt_f, 8 * RY), b, sm, stream>>>(a);
+        }
+    }
+
+    // tensor maps of the TMA forward kernels: the state as (x, y, z, field, shot)
+    // with one box per tile shape, the coefficients as (x, y, z)
+    Ac3Maps tma_maps(int RY, int S) const {
+        Ac3Maps m;
+        const uint32_t TYO = 8 * RY, WX = 32 + 2 * R, HY = TYO + 2 * R;
+        const uint64_t sd[5] = {(uint64_t)pitch, (uint64_t)NYs, (uint64_t)NZs, 4, (uint64_t)S};
+        const uint64_t ss[4] = {(uint64_t)pitch * 4, (uint64_t)plane * 4, (uint64_t)fs * 4, (uint64_t)sst * 4};
+        auto st5 = [&](uint32_t bx, uint32_t by) {
+            const uint32_t b[5] = {bx, by, 1, 1, 1};
+            return make_tensor_map_f32(st.p, 5, sd, ss, b);
+        };
+        m.sA = st5(WX, TYO);
+        m.sB = st5(32, HY);
+        m.sC = st5(32, TYO);
+        m.sD = st5(WX, HY);
+        const uint64_t md[3] = {(uint64_t)pitch, (uint64_t)NYs, (uint64_t)NZs};
+        const uint64_t ms[2] = {(uint64_t)pitch * 4, (uint64_t)plane * 4};
+        const uint32_t bc[3] = {32, TYO, 1};
+        m.mk = make_tensor_map_f32(dtbk.p, 3, md, ms, bc);
+        m.mx = make_tensor_map_f32(dtbx.p, 3, md, ms, bc);
+        m.my = make_tensor_map_f32(dtby.p, 3, md, ms, bc);
+        m.mz = make_tensor_map_f32(dtbz.p, 3, md, ms, bc);
+        return m;
+    }
+
+    template <int RR, int RY>
+    void launch_fwd_tma(int id, int S, bool store) {
+        Ac3dDev a = dev(S);
+        a.spt = spt_f;
+        pick_zchunk(8 * RY);
+        a.zchunk = zchunk;
+        OWL_CHECK(sst % 4 == 0 && fs % 4 == 0 && pitch % 4 == 0 && ((uintptr_t)st.p & 15) == 0, OWL_ERR_UNSUPPORTED,
+                  "TMA operands not 16-byte aligned");
+        const Ac3Maps mp = tma_maps(RY, S);
+        const int rows_p = a.z1 - a.zp0, rows_v = a.z1 - std::min(a.zvx0, a.zvz0);
+        dim3 b(32, 8);
+        if (id == OWL_K_FWD_P) {
+            constexpr int sm = tma_bytes_p<RR, RY>();
+            auto k = store ? k_ac3d_fwd_p_tma<RR, RY, true> : k_ac3d_fwd_p_tma<RR, RY, false>;
+            OWL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            k<<<grid3(rows_p, S, spt_f, 8 * RY), b, sm, stream>>>(a, mp);
+        } else {
+            constexpr int sm = tma_bytes_v<RR, RY>();
+            auto k = store ? k_ac3d_fwd_v_tma<RR, RY, true> : k_ac3d_fwd_v_tma<RR, RY, false>;
+            OWL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            k<<<grid3(rows_v, S, spt_f, 8 * RY), b, sm, stream>>>(a, mp);
         }
     }
 
@@ -760,7 +813,7 @@ struct Ac3dEngine : SsgBase {
         int best[2] = {tz_f, tz_f};
         for (int kid : {OWL_K_FWD_P, OWL_K_FWD_V}) {
             float bms = 1e30f;
-            for (int tz : {0, 1, 2, 4}) {
+            for (int tz : {0, 1, 2, 4, 11, 12, 14}) {
                 (kid == OWL_K_FWD_P ? tz_fp : tz_fv) = tz;
                 launch_kernel(kid, S, false);
                 OWL_LAUNCH_CHECK();
@@ -785,10 +838,15 @@ struct Ac3dEngine : SsgBase {
         if (id <= OWL_K_FWD_V) {
             const int sel = id == OWL_K_FWD_P ? tz_fp : tz_fv;
             const int tz = sel >= 0 ? sel : tz_f;
+            // 0: per cell; 1, 2, 4: cp.async ring with that many rows per thread;
+            // 11, 12, 14: the TMA ring with 1, 2, 4 rows per thread
             if (tz == 0) launch_naive<RR>(id, S, store);
             else if (tz == 2) launch_fwd<RR, 2>(id, S, store);
             else if (tz == 1) launch_fwd<RR, 1>(id, S, store);
-            else launch_fwd<RR, 4>(id, S, store);
+            else if (tz == 4) launch_fwd<RR, 4>(id, S, store);
+            else if (tz == 11) launch_fwd_tma<RR, 1>(id, S, store);
+            else if (tz == 12) launch_fwd_tma<RR, 2>(id, S, store);
+            else launch_fwd_tma<RR, 4>(id, S, store);
         } else {
             if (tz_a == 1) launch_adj_ring<RR>(id, S);
             else if (tz_a == 2) launch_adj<RR, 2>(id, S);

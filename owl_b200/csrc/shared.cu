@@ -6,6 +6,10 @@
 
 #include <cstdlib>
 
+#include <cudaTypedefs.h>
+
+#include "tma.cuh"
+
 namespace owl {
 
 bool pdl_enabled() {
@@ -18,6 +22,39 @@ bool pdl_enabled() {
 
 
 int nint_f(float v) { return (int)std::lround(v); }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda)
+CUtensorMap make_tensor_map_f32(const float* base, int rank, const uint64_t* dims, const uint64_t* stride_bytes,
+                                const uint32_t* box) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess) fn = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }();
+    OWL_CHECK(encode != nullptr, OWL_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    OWL_CHECK(rank >= 1 && rank <= 5 && ((uintptr_t)base % 16) == 0, OWL_ERR_INVALID, "tensor map base or rank");
+    cuuint64_t gd[5], gs[4];
+    cuuint32_t bx[5], es[5];
+    for (int i = 0; i < rank; ++i) {
+        gd[i] = dims[i];
+        bx[i] = box[i];
+        es[i] = 1;
+        OWL_CHECK(box[i] >= 1 && box[i] <= 256, OWL_ERR_INVALID, "tensor map box extent");
+    }
+    OWL_CHECK((box[0] * 4) % 16 == 0, OWL_ERR_INVALID, "tensor map box row must be a multiple of 16 bytes");
+    for (int i = 0; i + 1 < rank; ++i) {
+        gs[i] = stride_bytes[i];
+        OWL_CHECK(stride_bytes[i] % 16 == 0, OWL_ERR_INVALID, "tensor map strides must be multiples of 16 bytes");
+    }
+    CUtensorMap m;
+    const CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, const_cast<float*>(base), gd, gs,
+                              bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    OWL_CHECK(r == CUDA_SUCCESS, OWL_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
 
 void damp_coef(float bdvp, float d, float dist, int pml, float dt, float alphamax, float& a, float& b) {
     // npower_d = 2, npower_a = 1, kmax = 1, R0 = 1e-5 (module_cfspml.f90:27-30,68-70)

@@ -212,7 +212,19 @@ SsgBase::SsgBase(const owl_ssg_desc& d, int dim_) {
     fs = plane * NZs;
     dt = d.dt;
     OWL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    // step counter, CTA count of the last-block tick, non-finite flag, timeout flag
     ctr.reserve(4);
+    OWL_CUDA(cudaMemsetAsync(ctr.p, 0, 4 * sizeof(int), stream));
+}
+
+void SsgBase::check_timeout() {
+    int flag = 0;
+    OWL_CUDA(cudaMemcpyAsync(&flag, ctr.p + 3, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    OWL_CUDA(cudaStreamSynchronize(stream));
+    if (flag) {
+        OWL_CUDA(cudaMemsetAsync(ctr.p + 3, 0, sizeof(int), stream));
+        throw OwlError(OWL_ERR_TIMEOUT, "a bounded wait for TMA copies gave up; the results are invalid");
+    }
 }
 
 SsgBase::~SsgBase() {
@@ -736,6 +748,7 @@ void SsgBase::forward(int nshots, const owl_shot* shots, const owl_run_opts& o, 
         batches++;
     }
     info.elapsed_ms = tm.stop_ms();
+    check_timeout();
     fill_info(info, nshots, batches, false);
 }
 
@@ -805,6 +818,7 @@ void SsgBase::misfit(int nshots, const owl_shot* shots, const float* obs, const 
         batches++;
     }
     info.elapsed_ms = tm.stop_ms();
+    check_timeout();
     fill_info(info, nshots, batches, false);
 }
 
@@ -1044,6 +1058,7 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
     }
     if (grad) fold_out(grad, mem);
     info.elapsed_ms = tm.stop_ms();
+    check_timeout();
     fill_info(info, nshots, batches, true);
 }
 
@@ -1078,6 +1093,7 @@ void SsgBase::kernel_time(int id, int nlaunch, double* avg_ms, double* bytes) {
     fz_mode = 0;
     OWL_LAUNCH_CHECK();
     *avg_ms = tm.stop_ms() / nlaunch;
+    check_timeout();
     *bytes = alg_bytes(kid, S, (S + spt_a - 1) / spt_a);
     if (store) {
         const int terms = kid == OWL_K_FWD_P ? n_store_p() : nS - n_store_p();

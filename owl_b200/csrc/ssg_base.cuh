@@ -208,6 +208,7 @@ struct SsgBase : Engine {
     void restore_ckpt(int slot, int S);
     void forward_batch(int S, int k, bool graph, bool save, bool store_last = false);
     void check_nonfinite(const float* f, size_t n);
+    void check_timeout();  // OWL_ERR_TIMEOUT if a kernel's bounded wait gave up
     void copy_out(void* dst, const void* src, size_t bytes, int mem);
     void fold_out(float* grad, int mem);
     void invalidate_graphs();
