@@ -42,6 +42,7 @@ struct Ac2dPt {
     const float* bw;      // per item: 81 weights [z][x]
     const float* amp;     // per item: nt amplitudes (stf * amp * dt)
     int nt, rtot, nb, mode, rows_blk;
+    int fmask;            // fields the batch's sources inject into (bit 0 p, 1 vx, 2 vz)
     const int* rec_ptr;   // receivers (traces) of shot s: [rec_ptr[s], rec_ptr[s + 1])
     CSRView smp;
     float* rec;
@@ -91,6 +92,19 @@ __device__ __forceinline__ float ac2d_inj(const Ac2dPt& q, int s, int f, int x, 
     return v;
 }
 
+// whether a source of shot s injecting into a field of `fmask` has a tap in
+// columns [x0, x1) x rows [z0, z1) (storage): the same answer for every thread
+// of a CTA, so the per-node lookups run only in the CTAs around the sources
+__device__ __forceinline__ bool ac2d_inj_near(const Ac2dPt& q, int s, int fmask, int x0, int x1, int z0, int z1) {
+    if (!(q.fmask & fmask)) return false;
+    const int i1 = q.item_ptr[s + 1];
+    for (int it = q.item_ptr[s]; it < i1; ++it) {
+        const int4 b = q.box[it];
+        if (((fmask >> b.x) & 1) && b.y < x1 && b.y + BOX_W > x0 && b.w < z1 && b.w + BOX_W > z0) return true;
+    }
+    return false;
+}
+
 // ------------------------------- forward ------------------------------------
 template <int R, bool STORE, bool FUSE>
 __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
@@ -99,6 +113,7 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
     int z = a.zp0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
     const int cur = FUSE ? *a.d_step : 0;
+    const int cx0 = a.x0 + blockIdx.x * blockDim.x, cz0 = a.zp0 + blockIdx.y * blockDim.y;  // the CTA's tile
     const long long o = (long long)z * a.pitch + x;
     const float dtbk = a.dtbk[o];
     const bool px = pml_int(x, a.pr, a.nx);
@@ -121,7 +136,8 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
         float p0 = a.p[so];
         const float m1 = px ? a.m1[so] : 0.f, m2 = pz ? a.m2[so] : 0.f;
         // explosion sources of step t-1 (cur), added where add_source would have
-        if (FUSE && (a.pt.mode & FZ_INJ)) p0 = ac2d_inj(a.pt, s, 0, x, z, cur - 1, p0);
+        if (FUSE && (a.pt.mode & FZ_INJ) && ac2d_inj_near(a.pt, s, 1, cx0, cx0 + blockDim.x, cz0, cz0 + blockDim.y))
+            p0 = ac2d_inj(a.pt, s, 0, x, z, cur - 1, p0);
         float sx = 0.f, sz = 0.f;
 #pragma unroll
         for (int k = 1; k <= R; ++k) sx = sx + c_fd2[k - 1] * (__ldg(vx + k) - __ldg(vx + 1 - k));
@@ -173,6 +189,7 @@ __device__ __forceinline__ void ac2d_fwd_v_cells(const Ac2dDev& a, int cur) {
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
+    const int cx0 = a.x0 + blockIdx.x * blockDim.x, cz0 = zr0 + blockIdx.y * blockDim.y;  // the CTA's tile
     const long long o = (long long)z * a.pitch + x;
     const bool dox = z >= a.zvx0, doz = z >= a.zvz0;
     const float bxc = a.dtbx[o], bzc = a.dtbz[o];
@@ -200,7 +217,9 @@ __device__ __forceinline__ void ac2d_fwd_v_cells(const Ac2dDev& a, int cur) {
                 h = h + m;
             }
             float vn = vx0 - bxc * h;
-            if (FUSE && (a.pt.mode & FZ_INJ)) vn = ac2d_inj(a.pt, s, 1, x, z, cur, vn);  // force sources of step t
+            // force sources of step t
+            if (FUSE && (a.pt.mode & FZ_INJ) && ac2d_inj_near(a.pt, s, 2, cx0, cx0 + blockDim.x, cz0, cz0 + blockDim.y))
+                vn = ac2d_inj(a.pt, s, 1, x, z, cur, vn);
             a.vx[so] = vn;
             if (STORE) a.Svx[slot + s * a.fs + o] = h;
         }
@@ -215,7 +234,8 @@ __device__ __forceinline__ void ac2d_fwd_v_cells(const Ac2dDev& a, int cur) {
                 h = h + m;
             }
             float vn = vz0 - bzc * h;
-            if (FUSE && (a.pt.mode & FZ_INJ)) vn = ac2d_inj(a.pt, s, 2, x, z, cur, vn);
+            if (FUSE && (a.pt.mode & FZ_INJ) && ac2d_inj_near(a.pt, s, 4, cx0, cx0 + blockDim.x, cz0, cz0 + blockDim.y))
+                vn = ac2d_inj(a.pt, s, 2, x, z, cur, vn);
             a.vz[so] = vn;
             if (STORE) a.Svz[slot + s * a.fs + o] = h;
         }
@@ -410,6 +430,8 @@ __global__ void __launch_bounds__(512) k_ac2d_adj_v(Ac2dDev a) {
     }
     if (FUSE && (a.pt.mode & FZ_TICK)) tick_last_block(a.d_step, a.pt.d_done, -1);
 }
+
+#include "ac2d_vec.cuh"
 
 // ------------------------- FP64 chain rule ---------------------------------
 // Gradient w.r.t. vp and rho on the padded model grid [-P, n+P+1] from the
@@ -624,15 +646,36 @@ struct Ac2dEngine : SsgBase {
         }
         Ac2dPt& q = a.pt;
         q.item_ptr = inj_shot_ptr.p; q.box = inj_box.p; q.bw = inj_bw.p; q.amp = amp.p;
-        q.nt = desc.nt; q.rtot = rtot; q.nb = 1; q.mode = fz_mode; q.rows_blk = 1 << 30;
+        q.nt = desc.nt; q.rtot = rtot; q.nb = 1; q.mode = fz_mode; q.rows_blk = 1 << 30; q.fmask = inj_fmask;
         q.rec_ptr = rec_shot_ptr.p; q.smp = view(smp); q.rec = rec.p;
         q.sct_shot_ptr = sct_shot_ptr.p; q.sct = view(sct); q.res = res.p;
         q.d_done = ctr.p + 1;
         return a;
     }
 
+    // tile heights of the autotuner: 4, 8, 16 rows of one-cell threads (32 x
+    // tz), or 100 + 2, 4, 8 rows of four-cell threads (k_ac2d_*4, 32 x tz
+    // threads covering 128 x tz cells)
+    std::vector<int> tune_tz(int) const override { return {4, 8, 16, 102, 104, 108}; }
+    void launch_params(const owl_run_opts& o) override {
+        const bool vec = o.tile_z >= 100;
+        owl_run_opts q = o;
+        if (vec) q.tile_z = o.tile_z - 100;
+        SsgBase::launch_params(q);
+        if (vec) {
+            OWL_CHECK(tile_x == 32 && q.tile_z <= 8, OWL_ERR_INVALID,
+                      "four-cell tiles: tile_x 32 and tile_z 100 + (1 .. 8)");
+            tz_f = tz_a = o.tile_z;
+        }
+    }
+
     template <int RR>
     void launch_r(int id, int S, bool store) {
+        const int tzv = (id == OWL_K_FWD_P || id == OWL_K_FWD_V) ? tz_f : tz_a;
+        if (tzv >= 100) {
+            launch_v4<RR>(id, S, store, tzv - 100);
+            return;
+        }
         Ac2dDev a = dev(S);
         const int rows_p = a.z1 - a.zp0, rows_v = a.z1 - std::min(a.zvx0, a.zvz0);
         const int rows_a = a.z1 - std::min(std::min(a.zvx0, a.zvz0), a.zp0);
@@ -677,6 +720,54 @@ struct Ac2dEngine : SsgBase {
                 if (fz) launch_pdl(k_ac2d_adj_v<RR, true>, g, b, 0, stream, a);
                 else launch_pdl(k_ac2d_adj_v<RR, false>, g, b, 0, stream, a);
             }
+        }
+    }
+    // the four-cell kernels: 32 x ty threads over 128 x ty cells
+    template <int RR>
+    void launch_v4(int id, int S, bool store, int ty) {
+        Ac2dDev a = dev(S);
+        const int rows_p = a.z1 - a.zp0, rows_v = a.z1 - std::min(a.zvx0, a.zvz0);
+        const int rows_a = a.z1 - std::min(std::min(a.zvx0, a.zvz0), a.zp0);
+        const bool fz = fz_mode != 0;
+        auto grid = [&](int rows, int spt) {
+            return dim3((NXp + 127) / 128, (rows + ty - 1) / ty, (S + spt - 1) / spt);
+        };
+        auto add_point_rows = [&](dim3& g, int nb) {
+            a.pt.rows_blk = (int)g.y;
+            a.pt.nb = nb;
+            g.y += (S * nb + g.x - 1) / g.x;
+        };
+        const dim3 b(32, ty);
+        if (id == OWL_K_FWD_P) {
+            a.spt = spt_f;
+            const dim3 g = grid(rows_p, spt_f);
+            if (store) {
+                if (fz) launch_pdl(k_ac2d_fwd_p4<RR, true, true>, g, b, 0, stream, a);
+                else launch_pdl(k_ac2d_fwd_p4<RR, true, false>, g, b, 0, stream, a);
+            } else {
+                if (fz) launch_pdl(k_ac2d_fwd_p4<RR, false, true>, g, b, 0, stream, a);
+                else launch_pdl(k_ac2d_fwd_p4<RR, false, false>, g, b, 0, stream, a);
+            }
+        } else if (id == OWL_K_FWD_V) {
+            a.spt = spt_f;
+            dim3 g = grid(rows_v, spt_f);
+            if (fz && (fz_mode & FZ_SMP)) add_point_rows(g, nb_rec);
+            if (store) {
+                if (fz) launch_pdl(k_ac2d_fwd_v4<RR, true, true>, g, b, 0, stream, a);
+                else launch_pdl(k_ac2d_fwd_v4<RR, true, false>, g, b, 0, stream, a);
+            } else {
+                if (fz) launch_pdl(k_ac2d_fwd_v4<RR, false, true>, g, b, 0, stream, a);
+                else launch_pdl(k_ac2d_fwd_v4<RR, false, false>, g, b, 0, stream, a);
+            }
+        } else if (id == OWL_K_ADJ_P) {
+            a.spt = spt_a;
+            launch_pdl(k_ac2d_adj_p4<RR>, grid(rows_a, spt_a), b, 0, stream, a);
+        } else {
+            a.spt = spt_a;
+            dim3 g = grid(rows_v, spt_a);
+            if (fz && (fz_mode & FZ_SCT)) add_point_rows(g, nb_sct);
+            if (fz) launch_pdl(k_ac2d_adj_v4<RR, true>, g, b, 0, stream, a);
+            else launch_pdl(k_ac2d_adj_v4<RR, false>, g, b, 0, stream, a);
         }
     }
     void launch_kernel(int id, int S, bool store) override {

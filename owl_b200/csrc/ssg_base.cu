@@ -207,7 +207,9 @@ SsgBase::SsgBase(const owl_ssg_desc& d, int dim_) {
     P = d.pml; R = d.fdhalf; pr = P + R;
     NXp = nx + 2 * P; NYp = dim == 3 ? ny + 2 * P : 1; NZp = nz + 2 * P;
     NXs = NXp + 2 * R; NYs = dim == 3 ? NYp + 2 * R : 1; NZs = NZp + 2 * R;
-    pitch = (NXs + 31) / 32 * 32;
+    // rows of 128-byte multiples; in 2D at least four floats past the last
+    // column, so that the four-cell kernels' float4 windows stay in their row
+    pitch = (NXs + (dim == 2 ? 4 : 0) + 31) / 32 * 32;
     plane = (long long)pitch * NYs;
     fs = plane * NZs;
     dt = d.dt;
@@ -363,6 +365,9 @@ void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
     sct_shot_ptr.upload(hsct_ptr.data(), hsct_ptr.size(), stream);
     amp.upload(hamp.data(), hamp.size(), stream);
     live.upload(hlive.data(), hlive.size(), stream);
+    inj_fmask = 0;
+    for (const int4& b : hbox)
+        if (b.x >= 0 && b.x < 30) inj_fmask |= 1 << b.x;
     if (hbox.empty()) { hbox.push_back(int4{-1, 0, 0, 0}); hbw.resize(boxn, 0.f); }
     inj_box.upload(hbox.data(), hbox.size(), stream);
     inj_bw.upload(hbw.data(), hbw.size(), stream);

@@ -97,6 +97,7 @@ struct SsgBase : Engine {
     DevBuf<int4> inj_box;
     DevBuf<float> inj_bw;
     bool fuse_on = false;  // this batch's point work runs inside the stencil kernels
+    int inj_fmask = 0;     // fields the batch's sources inject into (bit f: field f)
     bool want_src_now = false;  // the adjoint sweep records the source-side adjoint
     int fz_mode = 0;       // FZ_* work of the next stencil launches
     DevBuf<unsigned char> live;

@@ -35,7 +35,9 @@ def test_forward_parity_small(fs, R):
     ps = prepare(small_shots(nx, nz, dx, bool(fs)), nx, nz, dx, dt)
     ref = oracle.ac2d_forward(d, vp, rho, ps, "f32")
     s = make_solver(d, vp, rho)
-    for opts in (RunOpts(), RunOpts(shots_per_launch=1, use_graph=-1), RunOpts(shots_per_cta=2)):
+    # tile_z 100 + h: the four-cell kernels, h rows per CTA
+    for opts in (RunOpts(), RunOpts(shots_per_launch=1, use_graph=-1), RunOpts(shots_per_cta=2),
+                 RunOpts(tile_z=104), RunOpts(tile_z=108, shots_per_cta=2), RunOpts(tile_z=102, use_graph=-1)):
         got = s.forward(ps, opts)
         assert rel(got, ref) < FWD_TOL, (opts, rel(got, ref))
     # zero-weight receiver records zeros
@@ -67,7 +69,8 @@ def test_gradient_parity_small(fs):
     # k >= nt and the memory-sized choice (-1): one segment, stored by the forward, no recompute
     for opts in (RunOpts(checkpoint_interval=37), RunOpts(checkpoint_interval=50, shots_per_launch=1, use_graph=-1),
                  RunOpts(checkpoint_interval=20, shots_per_cta=3), RunOpts(checkpoint_interval=-1),
-                 RunOpts(checkpoint_interval=100000, use_graph=-1)):
+                 RunOpts(checkpoint_interval=100000, use_graph=-1), RunOpts(checkpoint_interval=37, tile_z=104),
+                 RunOpts(checkpoint_interval=20, tile_z=108, shots_per_cta=2)):
         mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, opts)
         assert rel(mf, mf_ref) < 1e-4
         e = rel(g, g_ref)
@@ -158,8 +161,9 @@ def test_unstable_dt_rejected():
     assert e.value.code == L.OWL_ERR_UNSTABLE
 
 
+@pytest.mark.parametrize("tz", [8, 104])
 @pytest.mark.parametrize("fs", [0, 1])
-def test_fused_point_work_matches_point_kernels(fs):
+def test_fused_point_work_matches_point_kernels(fs, tz):
     """Injection, sampling and the residual scatter inside the stencil kernels
     give the seismograms, misfits and gradients of the separate point kernel
     (OWL_NO_FUSE=1) to the bit: explosion and force sources, two overlapping
@@ -176,10 +180,10 @@ def test_fused_point_work_matches_point_kernels(fs):
         if off:
             os.environ["OWL_NO_FUSE"] = "1"
         try:
-            seis = s.forward(ps, RunOpts())
-            mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=40))
+            seis = s.forward(ps, RunOpts(tile_z=tz))
+            mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=40, tile_z=tz))
             launches = s.last_info.gpu_launches
-            gs = s.source_gradient(ps, obs, RunOpts(checkpoint_interval=40))
+            gs = s.source_gradient(ps, obs, RunOpts(checkpoint_interval=40, tile_z=tz))
         finally:
             os.environ.pop("OWL_NO_FUSE", None)
         out[off] = (seis, mf, g, gs, launches)

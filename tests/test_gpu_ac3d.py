@@ -132,3 +132,33 @@ def test_tma_forward_kernels_match_cp_async_ring(fs, R):
     s0 = solver3(d, vp0, rho)
     _, g = s0.gradient(ps1, obs, opts=RunOpts(checkpoint_interval=30, tile_z=12))
     assert rel(g, g_ref) < 1e-4, rel(g, g_ref)
+
+
+_C3 = {}
+
+
+@pytest.mark.parametrize("prec,tol", [(L.OWL_CKPT_FP32, 1e-4), (L.OWL_CKPT_FP16, 2e-3), (L.OWL_CKPT_BF16, 2e-2)])
+def test_c3_kind_checkpoint_precision(prec, tol):
+    """The 3D acoustic workload scaled down to a 48^3 model (its layered model
+    generator with the 5 % lateral perturbation and Gardner rho, dx 10 m, dt
+    1 ms, 20-cell PML, 8th order, the 12 Hz source at the centre, 24 x 24
+    receivers every 20 m at z = 20 m), 300 steps, observed data from a 3 %
+    faster model, checkpoints every 50 steps in FP32 / FP16 / BF16 (per-field,
+    per-shot scale): the vp / rho gradient against the FP64 exact-adjoint
+    oracle of the same stencil."""
+    from owl_b200 import configs
+    if not _C3:
+        d, vp, rho, shots = configs.config3(48, nt=300)
+        ps = PreparedShots(shots, GridSpec(nx=d.nx, nz=d.nz, dx=d.dx, dz=d.dz, ny=d.ny, dy=d.dy), d.dt)
+        obs = oracle.ac3d_forward(d, (vp * np.float32(1.03)).astype(np.float32), rho, ps, "f64").astype(np.float32)
+        _, g_ref = oracle.ac3d_gradient(d, vp, rho, ps, obs, adj_kind=0, k=50)
+        _C3.update(d=d, vp=vp, rho=rho, ps=ps, obs=obs, g=g_ref)
+    r = _C3
+    d = r["d"]
+    s = SSGSolver(L.OWL_ACOUSTIC_ISO_3D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
+                  f0_max=d.f0_max, ny=d.ny, dy=d.dy)
+    s.set_model(r["vp"], r["rho"])
+    _, g = s.gradient(r["ps"], r["obs"], L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=50, checkpoint_precision=prec))
+    e = rel(g, r["g"])
+    print(f"c3-kind 48^3 gradient, checkpoint precision {prec}: rel err vs FP64 oracle {e:.3e}")
+    assert e < tol, e
