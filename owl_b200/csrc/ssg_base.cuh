@@ -165,7 +165,7 @@ struct SsgBase : Engine {
         return false;
     }
     // launches of one time step of `kind` (launch_step)
-    int step_launches(int kind) const;
+    virtual int step_launches(int kind) const;
     // medium-specific tuning after the shared autotuner (S shots per launch)
     virtual void tune_extra(int S, int k, bool grad) { (void)S; (void)k; (void)grad; }
 
