@@ -572,9 +572,14 @@ def headline_roofline(s, d, k, peak, peak_kind):
     # the other segments storing; adjoint every step
     counts = {L.OWL_K_FWD_P: nt - n_last, L.OWL_K_FWD_V: nt - n_last, L.OWL_K_FWD_P_STORE: nt,
               L.OWL_K_FWD_V_STORE: nt, L.OWL_K_ADJ_P: nt, L.OWL_K_ADJ_V: nt}
-    names = {L.OWL_K_FWD_P: "k_ac2d_fwd_p<4,0>", L.OWL_K_FWD_V: "k_ac2d_fwd_v<4,0>",
-             L.OWL_K_FWD_P_STORE: "k_ac2d_fwd_p<4,1>", L.OWL_K_FWD_V_STORE: "k_ac2d_fwd_v<4,1>",
-             L.OWL_K_ADJ_P: "k_ac2d_adj_p<4>", L.OWL_K_ADJ_V: "k_ac2d_adj_v<4>"}
+    # the autotuner's variants: tile codes >= 100 are the four-cell kernels
+    v4f = s.last_info.tile_z_forward >= 100
+    v4a = s.last_info.tile_z >= 100
+    fp, fv = ("k_ac2d_fwd_p4", "k_ac2d_fwd_v4") if v4f else ("k_ac2d_fwd_p", "k_ac2d_fwd_vf")
+    ap, av = ("k_ac2d_adj_p4", "k_ac2d_adj_v4") if v4a else ("k_ac2d_adj_p", "k_ac2d_adj_v")
+    names = {L.OWL_K_FWD_P: fp + "<4,0>", L.OWL_K_FWD_V: fv + "<4,0>",
+             L.OWL_K_FWD_P_STORE: fp + "<4,1>", L.OWL_K_FWD_V_STORE: fv + "<4,1>",
+             L.OWL_K_ADJ_P: ap + "<4>", L.OWL_K_ADJ_V: av + "<4>"}
     kt = {}
     for kid in names:
         if counts[kid] > 0:
@@ -588,7 +593,9 @@ def headline_roofline(s, d, k, peak, peak_kind):
             "alg_bytes_per_launch": bytes_k, "ms_per_launch": ms_k,
             "kernel_ms_per_launch": {names[q]: kt[q][0] for q in kt},
             "launches_per_gradient": {names[q]: counts[q] for q in kt},
-            "kernel_ms_per_gradient": {names[q]: kt[q][0] * counts[q] for q in kt}}
+            "kernel_ms_per_gradient": {names[q]: kt[q][0] * counts[q] for q in kt},
+            "tile_codes": {"forward": s.last_info.tile_z_forward, "adjoint": s.last_info.tile_z,
+                           "shots_per_cta": s.last_info.shots_per_cta}}
 
 
 def main():

@@ -232,6 +232,7 @@ module owl_ssg_c
         integer(c_int) :: batches
         integer(c_int) :: checkpoint_interval
         integer(c_int) :: shots_per_launch
+        integer(c_int) :: tile_z_forward
     end type
 
     interface

@@ -232,6 +232,7 @@ typedef struct {
     int batches;
     int checkpoint_interval;  /* gradients: the interval used (opts, or chosen from free device memory) */
     int shots_per_launch;     /* shots per batched launch used (opts, or the most that fit the device) */
+    int tile_z_forward;       /* the forward kernels' tile code (tile_z is the adjoint kernels' in a gradient) */
 } owl_run_info;
 
 /* ---- lifecycle ---------------------------------------------------------- */

@@ -43,6 +43,7 @@ struct Ac2dPt {
     const float* amp;     // per item: nt amplitudes (stf * amp * dt)
     int nt, rtot, nb, mode, rows_blk;
     int fmask;            // fields the batch's sources inject into (bit 0 p, 1 vx, 2 vz)
+    const int4* bbox;     // per shot: bounding box (x0, x1, z0, z1) of its p taps, then of its vx / vz taps
     const int* rec_ptr;   // receivers (traces) of shot s: [rec_ptr[s], rec_ptr[s + 1])
     CSRView smp;
     float* rec;
@@ -92,17 +93,14 @@ __device__ __forceinline__ float ac2d_inj(const Ac2dPt& q, int s, int f, int x, 
     return v;
 }
 
-// whether a source of shot s injecting into a field of `fmask` has a tap in
-// columns [x0, x1) x rows [z0, z1) (storage): the same answer for every thread
-// of a CTA, so the per-node lookups run only in the CTAs around the sources
+// whether shot s has a tap on p (fmask 1) or on vx / vz (fmask 2 or 4) in
+// columns [x0, x1) x rows [z0, z1) (storage): one read-only load of the shot's
+// bounding box, independent of the stencil loads, and the same answer for every
+// thread of a CTA, so the per-node lookups run only in the CTAs around sources
 __device__ __forceinline__ bool ac2d_inj_near(const Ac2dPt& q, int s, int fmask, int x0, int x1, int z0, int z1) {
     if (!(q.fmask & fmask)) return false;
-    const int i1 = q.item_ptr[s + 1];
-    for (int it = q.item_ptr[s]; it < i1; ++it) {
-        const int4 b = q.box[it];
-        if (((fmask >> b.x) & 1) && b.y < x1 && b.y + BOX_W > x0 && b.w < z1 && b.w + BOX_W > z0) return true;
-    }
-    return false;
+    const int4 b = __ldg(q.bbox + 2 * s + (fmask == 1 ? 0 : 1));
+    return b.x < x1 && b.y > x0 && b.z < z1 && b.w > z0;
 }
 
 // ------------------------------- forward ------------------------------------
@@ -242,16 +240,27 @@ __device__ __forceinline__ void ac2d_fwd_v_cells(const Ac2dDev& a, int cur) {
     }
 }
 
-template <int R, bool STORE, bool FUSE>
+// the fused instance is held to 32 registers (4 CTAs of 512 per SM), the
+// occupancy of the plain kernel: the step is latency bound
+template <int R, bool STORE>
 __global__ void __launch_bounds__(512) k_ac2d_fwd_v(Ac2dDev a) {
     pdl_prologue();
-    const int cur = FUSE ? *a.d_step : 0;
-    if (FUSE && (int)blockIdx.y >= a.pt.rows_blk) {
+    ac2d_fwd_v_cells<R, STORE, false>(a, 0);
+}
+
+// with the fused point work; held to 40 registers (3 CTAs of 512 per SM): at
+// 32 the injection and sampling branches spill, and without a bound the
+// sampling branch raises the count of every CTA further
+template <int R, bool STORE>
+__global__ void __launch_bounds__(512, 3) k_ac2d_fwd_vf(Ac2dDev a) {
+    pdl_prologue();
+    const int cur = *a.d_step;
+    if ((int)blockIdx.y >= a.pt.rows_blk) {
         if (a.pt.mode & FZ_SMP) ac2d_sample(a, cur);
     } else {
-        ac2d_fwd_v_cells<R, STORE, FUSE>(a, cur);
+        ac2d_fwd_v_cells<R, STORE, true>(a, cur);
     }
-    if (FUSE && (a.pt.mode & FZ_TICK)) tick_last_block(a.d_step, a.pt.d_done, 1);
+    if (a.pt.mode & FZ_TICK) tick_last_block(a.d_step, a.pt.d_done, 1);
 }
 
 // ------------------------------- adjoint ------------------------------------
@@ -647,6 +656,7 @@ struct Ac2dEngine : SsgBase {
         Ac2dPt& q = a.pt;
         q.item_ptr = inj_shot_ptr.p; q.box = inj_box.p; q.bw = inj_bw.p; q.amp = amp.p;
         q.nt = desc.nt; q.rtot = rtot; q.nb = 1; q.mode = fz_mode; q.rows_blk = 1 << 30; q.fmask = inj_fmask;
+        q.bbox = inj_bbox.p;
         q.rec_ptr = rec_shot_ptr.p; q.smp = view(smp); q.rec = rec.p;
         q.sct_shot_ptr = sct_shot_ptr.p; q.sct = view(sct); q.res = res.p;
         q.d_done = ctr.p + 1;
@@ -702,11 +712,11 @@ struct Ac2dEngine : SsgBase {
                 dim3 g = grid_for(rows_v, S, spt_f, tz_f);
                 if (fz && (fz_mode & FZ_SMP)) add_point_rows(g, nb_rec);
                 if (store) {
-                    if (fz) launch_pdl(k_ac2d_fwd_v<RR, true, true>, g, b, 0, stream, a);
-                    else launch_pdl(k_ac2d_fwd_v<RR, true, false>, g, b, 0, stream, a);
+                    if (fz) launch_pdl(k_ac2d_fwd_vf<RR, true>, g, b, 0, stream, a);
+                    else launch_pdl(k_ac2d_fwd_v<RR, true>, g, b, 0, stream, a);
                 } else {
-                    if (fz) launch_pdl(k_ac2d_fwd_v<RR, false, true>, g, b, 0, stream, a);
-                    else launch_pdl(k_ac2d_fwd_v<RR, false, false>, g, b, 0, stream, a);
+                    if (fz) launch_pdl(k_ac2d_fwd_vf<RR, false>, g, b, 0, stream, a);
+                    else launch_pdl(k_ac2d_fwd_v<RR, false>, g, b, 0, stream, a);
                 }
             }
         } else {

@@ -219,7 +219,7 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
 }
 
 template <int R, bool STORE, bool FUSE>
-__global__ void __launch_bounds__(256) k_ac2d_fwd_v4(Ac2dDev a) {
+__global__ void __launch_bounds__(256, FUSE ? 3 : 1) k_ac2d_fwd_v4(Ac2dDev a) {
     pdl_prologue();
     const int cur = FUSE ? *a.d_step : 0;
     if (FUSE && (int)blockIdx.y >= a.pt.rows_blk) {

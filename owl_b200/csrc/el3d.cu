@@ -65,6 +65,10 @@ struct E3Mp {
     const float* al[3][2];
     const float* face[6];
     float adt;
+    // (a, b) of every derivative of every node, computed once per model by
+    // k_el3d_mpml_coef: a of entry q at (2 q) fs + o, b at (2 q + 1) fs + o;
+    // q 0..8 the stress nodes' derivatives, q 9..17 the velocity nodes'
+    const float* coef;
 };
 
 struct El3dDev {
@@ -163,6 +167,49 @@ __device__ __forceinline__ void e3_mpml(const El3dDev& a, int ax, int x, int y, 
     cb = (2.0f - m.adt * b) / (2.0f + m.adt * b);
 }
 
+// the derivatives of the precomputed table, in the order of k_el3d_mpml_coef:
+// (axis, hx, hy, hz) of q = 0..8 (stress nodes) and 9..17 (velocity nodes)
+__constant__ int c_e3_coef_node[18][4] = {
+    {0, 0, 0, 0}, {1, 0, 0, 0}, {2, 0, 0, 0}, {1, 0, 1, 1}, {2, 0, 1, 1}, {0, 1, 0, 1}, {2, 1, 0, 1}, {0, 1, 1, 0},
+    {1, 1, 1, 0}, {0, 1, 0, 0}, {1, 1, 0, 0}, {2, 1, 0, 0}, {0, 0, 1, 0}, {1, 0, 1, 0}, {2, 0, 1, 0}, {0, 0, 0, 1},
+    {1, 0, 0, 1}, {2, 0, 0, 1}};
+// the order in which a kernel wants entries q0 + 0..8: the forward stress and
+// both velocity kernels take them as stored, the adjoint stress kernel swaps
+// the two derivatives of each shear node
+constexpr int E3_PERM_S = 0, E3_PERM_AS = 1;
+template <int PERM>
+__device__ __forceinline__ int e3_perm(int q) {
+    return PERM == E3_PERM_S ? q : (q < 3 ? q : (q & 1 ? q + 1 : q - 1));
+}
+// the a of the node's nine derivatives (they decide which memories update);
+// each b is loaded where its update needs it (e3_cb), to hold fewer registers
+template <int PERM>
+__device__ __forceinline__ void e3_coef_load(const El3dDev& a, long long o, int q0, float (&ca)[9]) {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) ca[q] = __ldg(a.mp.coef + (2 * (q0 + e3_perm<PERM>(q))) * a.fs + o);
+}
+template <int PERM>
+__device__ __forceinline__ float e3_cb(const El3dDev& a, long long o, int q0, int q) {
+    return __ldg(a.mp.coef + (2 * (q0 + e3_perm<PERM>(q)) + 1) * a.fs + o);
+}
+
+// one thread per updated cell: the (a, b) of its 18 derivatives (e3_mpml, the
+// same arithmetic the kernels used to repeat every step)
+__global__ void k_el3d_mpml_coef(El3dDev a, float* __restrict__ out) {
+    const int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = a.y0 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = a.z0 + blockIdx.z;
+    if (x >= a.x1 || y >= a.y1 || z >= a.z1) return;
+    const long long o = (long long)z * a.plane + (long long)y * a.pitch + x;
+    for (int q = 0; q < 18; ++q) {
+        float ca, cb;
+        e3_mpml(a, c_e3_coef_node[q][0], x, y, z, c_e3_coef_node[q][1], c_e3_coef_node[q][2], c_e3_coef_node[q][3],
+                ca, cb);
+        out[(2 * q) * a.fs + o] = ca;
+        out[(2 * q + 1) * a.fs + o] = cb;
+    }
+}
+
 struct E3Cell {
     int x, y, z, grp;
     long long o;
@@ -207,21 +254,13 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_s(El3dDev a) {
     const long long dzz = (long long)(2 * a.pr - 2 * z) * sz, dsh = dzz + sz;
     // MP: the M-PML (a, b) of each derivative of the node (shell nodes only);
     // otherwise the per-axis 1D tables above
-    float ca[9], cb[9];
+    float ca[9];
     if (MP) {
         if (row1 || sh_n || sh_yz || sh_xz || sh_xy) {
-            e3_mpml(a, 0, x, y, z, 0, 0, 0, ca[0], cb[0]);
-            e3_mpml(a, 1, x, y, z, 0, 0, 0, ca[1], cb[1]);
-            e3_mpml(a, 2, x, y, z, 0, 0, 0, ca[2], cb[2]);
-            e3_mpml(a, 1, x, y, z, 0, 1, 1, ca[3], cb[3]);
-            e3_mpml(a, 2, x, y, z, 0, 1, 1, ca[4], cb[4]);
-            e3_mpml(a, 0, x, y, z, 1, 0, 1, ca[5], cb[5]);
-            e3_mpml(a, 2, x, y, z, 1, 0, 1, ca[6], cb[6]);
-            e3_mpml(a, 0, x, y, z, 1, 1, 0, ca[7], cb[7]);
-            e3_mpml(a, 1, x, y, z, 1, 1, 0, ca[8], cb[8]);
+            e3_coef_load<E3_PERM_S>(a, o, 0, ca);
         } else {
 #pragma unroll
-            for (int q = 0; q < 9; ++q) ca[q] = cb[q] = 0.f;
+            for (int q = 0; q < 9; ++q) ca[q] = 0.f;
         }
     }
     for (int s = s0; s < s1; ++s) {
@@ -245,13 +284,13 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_s(El3dDev a) {
         const float m5 = p5 ? m[N_XVZ * a.fs] : 0.f, m6 = p6 ? m[N_ZVX * a.fs] : 0.f;
         const float m7 = p7 ? m[N_XVY * a.fs] : 0.f, m8 = p8 ? m[N_YVX * a.fs] : 0.f;
         float dX = a.idx * stP<R>(vx, 1), dY = a.idy * stP<R>(vy, sy), dZ;
-        if (p0) dX = pml_up(dX, MP ? ca[0] : axi, MP ? cb[0] : bxi, m0, m + N_XVX * a.fs);
-        if (p1) dY = pml_up(dY, MP ? ca[1] : ayi, MP ? cb[1] : byi, m1, m + N_YVY * a.fs);
+        if (p0) dX = pml_up(dX, MP ? ca[0] : axi, MP ? e3_cb<E3_PERM_S>(a, o, 0, 0) : bxi, m0, m + N_XVX * a.fs);
+        if (p1) dY = pml_up(dY, MP ? ca[1] : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 0, 1) : byi, m1, m + N_YVY * a.fs);
         if (row1) {
             dZ = -(c13 / c33) * dX - (c23 / c33) * dY;
         } else {
             dZ = a.idz * stP<R>(vz, sz);
-            if (p2) dZ = pml_up(dZ, MP ? ca[2] : azi, MP ? cb[2] : bzi, m2, m + N_ZVZ * a.fs);
+            if (p2) dZ = pml_up(dZ, MP ? ca[2] : azi, MP ? e3_cb<E3_PERM_S>(a, o, 0, 2) : bzi, m2, m + N_ZVZ * a.fs);
         }
         st[E3_XX * a.fs + o] = xx0 + a.dt * (c11 * dX + c12 * dY + c13 * dZ);
         st[E3_YY * a.fs + o] = yy0 + a.dt * (c12 * dX + c22 * dY + c23 * dZ);
@@ -267,24 +306,24 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_s(El3dDev a) {
             // syz: dz vy + dy vz
             dzvy = a.idz * stM<R>(vy, sz);
             dyvz = a.idy * stM<R>(vz, sy);
-            if (p3) dyvz = pml_up(dyvz, MP ? ca[3] : ayh, MP ? cb[3] : byh, m3, m + N_YVZ * a.fs);
-            if (p4) dzvy = pml_up(dzvy, MP ? ca[4] : azh, MP ? cb[4] : bzh, m4, m + N_ZVY * a.fs);
+            if (p3) dyvz = pml_up(dyvz, MP ? ca[3] : ayh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 3) : byh, m3, m + N_YVZ * a.fs);
+            if (p4) dzvy = pml_up(dzvy, MP ? ca[4] : azh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 4) : bzh, m4, m + N_ZVY * a.fs);
             const float yzn = yz0 + g44 * (dzvy + dyvz);
             st[E3_YZ * a.fs + o] = yzn;
             if (mir) st[E3_YZ * a.fs + o + dsh] = -yzn;
             // sxz: dz vx + dx vz
             dzvx = a.idz * stM<R>(vx, sz);
             dxvz = a.idx * stM<R>(vz, 1);
-            if (p5) dxvz = pml_up(dxvz, MP ? ca[5] : axh, MP ? cb[5] : bxh, m5, m + N_XVZ * a.fs);
-            if (p6) dzvx = pml_up(dzvx, MP ? ca[6] : azh, MP ? cb[6] : bzh, m6, m + N_ZVX * a.fs);
+            if (p5) dxvz = pml_up(dxvz, MP ? ca[5] : axh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 5) : bxh, m5, m + N_XVZ * a.fs);
+            if (p6) dzvx = pml_up(dzvx, MP ? ca[6] : azh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 6) : bzh, m6, m + N_ZVX * a.fs);
             const float xzn = xz0 + g55 * (dzvx + dxvz);
             st[E3_XZ * a.fs + o] = xzn;
             if (mir) st[E3_XZ * a.fs + o + dsh] = -xzn;
         }
         // sxy: dy vx + dx vy
         float dyvx = a.idy * stM<R>(vx, sy), dxvy = a.idx * stM<R>(vy, 1);
-        if (p7) dxvy = pml_up(dxvy, MP ? ca[7] : axh, MP ? cb[7] : bxh, m7, m + N_XVY * a.fs);
-        if (p8) dyvx = pml_up(dyvx, MP ? ca[8] : ayh, MP ? cb[8] : byh, m8, m + N_YVX * a.fs);
+        if (p7) dxvy = pml_up(dxvy, MP ? ca[7] : axh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 7) : bxh, m7, m + N_XVY * a.fs);
+        if (p8) dyvx = pml_up(dyvx, MP ? ca[8] : ayh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 8) : byh, m8, m + N_YVX * a.fs);
         st[E3_XY * a.fs + o] = xy0 + g66 * (dyvx + dxvy);
         if (STORE) {
             float* S = a.S + slot + s * a.fs + o;
@@ -307,21 +346,13 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_v(El3dDev a) {
     const bool sh_vx = oxh || oyi || ozi, sh_vy = oxi || oyh || ozi, sh_vz = oxi || oyi || ozh;
     // MP: the M-PML (a, b) of each derivative of the node (shell nodes only);
     // otherwise the per-axis 1D tables above
-    float ca[9], cb[9];
+    float ca[9];
     if (MP) {
         if (sh_vx || sh_vy || sh_vz) {
-            e3_mpml(a, 0, x, y, z, 1, 0, 0, ca[0], cb[0]);
-            e3_mpml(a, 1, x, y, z, 1, 0, 0, ca[1], cb[1]);
-            e3_mpml(a, 2, x, y, z, 1, 0, 0, ca[2], cb[2]);
-            e3_mpml(a, 0, x, y, z, 0, 1, 0, ca[3], cb[3]);
-            e3_mpml(a, 1, x, y, z, 0, 1, 0, ca[4], cb[4]);
-            e3_mpml(a, 2, x, y, z, 0, 1, 0, ca[5], cb[5]);
-            e3_mpml(a, 0, x, y, z, 0, 0, 1, ca[6], cb[6]);
-            e3_mpml(a, 1, x, y, z, 0, 0, 1, ca[7], cb[7]);
-            e3_mpml(a, 2, x, y, z, 0, 0, 1, ca[8], cb[8]);
+            e3_coef_load<E3_PERM_S>(a, o, 9, ca);
         } else {
 #pragma unroll
-            for (int q = 0; q < 9; ++q) ca[q] = cb[q] = 0.f;
+            for (int q = 0; q < 9; ++q) ca[q] = 0.f;
         }
     }
     const float axi = a.axi[x], bxi = a.bxi[x], axh = a.axh[x], bxh = a.bxh[x];
@@ -353,25 +384,25 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_v(El3dDev a) {
         const float m6 = p6 ? m[N_XXZ * a.fs] : 0.f, m7 = p7 ? m[N_YYZ * a.fs] : 0.f, m8 = p8 ? m[N_ZZZ * a.fs] : 0.f;
         // vx: dx sxx (M) + dy sxy (P) + dz sxz (P)
         float h1 = a.idx * stM<R>(sxx, 1), h2 = a.idy * stP<R>(sxy, sy), h3 = a.idz * stP<R>(sxz, sz);
-        if (p0) h1 = pml_up(h1, MP ? ca[0] : axh, MP ? cb[0] : bxh, m0, m + N_XXX * a.fs);
-        if (p1) h2 = pml_up(h2, MP ? ca[1] : ayi, MP ? cb[1] : byi, m1, m + N_YXY * a.fs);
-        if (p2) h3 = pml_up(h3, MP ? ca[2] : azi, MP ? cb[2] : bzi, m2, m + N_ZXZ * a.fs);
+        if (p0) h1 = pml_up(h1, MP ? ca[0] : axh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 0) : bxh, m0, m + N_XXX * a.fs);
+        if (p1) h2 = pml_up(h2, MP ? ca[1] : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 1) : byi, m1, m + N_YXY * a.fs);
+        if (p2) h3 = pml_up(h3, MP ? ca[2] : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 2) : bzi, m2, m + N_ZXZ * a.fs);
         const float hx = h1 + h2 + h3;
         st[E3_VX * a.fs + o] = vx0 + bx * hx;
         // vy: dx sxy (P) + dy syy (M) + dz syz (P)
         h1 = a.idx * stP<R>(sxy, 1); h2 = a.idy * stM<R>(syy, sy); h3 = a.idz * stP<R>(syz, sz);
-        if (p3) h1 = pml_up(h1, MP ? ca[3] : axi, MP ? cb[3] : bxi, m3, m + N_XXY * a.fs);
-        if (p4) h2 = pml_up(h2, MP ? ca[4] : ayh, MP ? cb[4] : byh, m4, m + N_YYY * a.fs);
-        if (p5) h3 = pml_up(h3, MP ? ca[5] : azi, MP ? cb[5] : bzi, m5, m + N_ZYZ * a.fs);
+        if (p3) h1 = pml_up(h1, MP ? ca[3] : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 3) : bxi, m3, m + N_XXY * a.fs);
+        if (p4) h2 = pml_up(h2, MP ? ca[4] : ayh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 4) : byh, m4, m + N_YYY * a.fs);
+        if (p5) h3 = pml_up(h3, MP ? ca[5] : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 5) : bzi, m5, m + N_ZYZ * a.fs);
         const float hy = h1 + h2 + h3;
         st[E3_VY * a.fs + o] = vy0 + by * hy;
         // vz: dx sxz (P) + dy syz (P) + dz szz (M); with a free surface from row 2
         float hz = 0.f;
         if (vz_ok) {
             h1 = a.idx * stP<R>(sxz, 1); h2 = a.idy * stP<R>(syz, sy); h3 = a.idz * stM<R>(szz, sz);
-            if (p6) h1 = pml_up(h1, MP ? ca[6] : axi, MP ? cb[6] : bxi, m6, m + N_XXZ * a.fs);
-            if (p7) h2 = pml_up(h2, MP ? ca[7] : ayi, MP ? cb[7] : byi, m7, m + N_YYZ * a.fs);
-            if (p8) h3 = pml_up(h3, MP ? ca[8] : azh, MP ? cb[8] : bzh, m8, m + N_ZZZ * a.fs);
+            if (p6) h1 = pml_up(h1, MP ? ca[6] : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 6) : bxi, m6, m + N_XXZ * a.fs);
+            if (p7) h2 = pml_up(h2, MP ? ca[7] : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 7) : byi, m7, m + N_YYZ * a.fs);
+            if (p8) h3 = pml_up(h3, MP ? ca[8] : azh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 8) : bzh, m8, m + N_ZZZ * a.fs);
             hz = h1 + h2 + h3;
             st[E3_VZ * a.fs + o] = vz0 + bz * hz;
         }
@@ -405,21 +436,13 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_v(El3dDev a) {
     const bool sh_vx = oxh || oyi || ozi, sh_vy = oxi || oyh || ozi, sh_vz = oxi || oyi || ozh;
     // MP: the M-PML (a, b) of each derivative of the node (shell nodes only);
     // otherwise the per-axis 1D tables above
-    float ca[9], cb[9];
+    float ca[9];
     if (MP) {
         if (sh_vx || sh_vy || sh_vz) {
-            e3_mpml(a, 0, x, y, z, 1, 0, 0, ca[0], cb[0]);
-            e3_mpml(a, 1, x, y, z, 1, 0, 0, ca[1], cb[1]);
-            e3_mpml(a, 2, x, y, z, 1, 0, 0, ca[2], cb[2]);
-            e3_mpml(a, 0, x, y, z, 0, 1, 0, ca[3], cb[3]);
-            e3_mpml(a, 1, x, y, z, 0, 1, 0, ca[4], cb[4]);
-            e3_mpml(a, 2, x, y, z, 0, 1, 0, ca[5], cb[5]);
-            e3_mpml(a, 0, x, y, z, 0, 0, 1, ca[6], cb[6]);
-            e3_mpml(a, 1, x, y, z, 0, 0, 1, ca[7], cb[7]);
-            e3_mpml(a, 2, x, y, z, 0, 0, 1, ca[8], cb[8]);
+            e3_coef_load<E3_PERM_S>(a, o, 9, ca);
         } else {
 #pragma unroll
-            for (int q = 0; q < 9; ++q) ca[q] = cb[q] = 0.f;
+            for (int q = 0; q < 9; ++q) ca[q] = 0.f;
         }
     }
     const float axi = a.axi[x], bxi = a.bxi[x], axh = a.axh[x], bxh = a.bxh[x];
@@ -453,9 +476,9 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_v(El3dDev a) {
         ad[E3_VX * a.fs + o] = v;
         gx += v * __ldg(a.S + 6 * a.sterm + so);
         float q = bx * v, e1 = q, e2 = q, e3 = q;
-        if (p0) e1 = pml_adr(q, MP ? ca[0] : axh, MP ? cb[0] : bxh, m0, mh + N_XXX * a.fs);
-        if (p1) e2 = pml_adr(q, MP ? ca[1] : ayi, MP ? cb[1] : byi, m1, mh + N_YXY * a.fs);
-        if (p2) e3 = pml_adr(q, MP ? ca[2] : azi, MP ? cb[2] : bzi, m2, mh + N_ZXZ * a.fs);
+        if (p0) e1 = pml_adr(q, MP ? ca[0] : axh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 0) : bxh, m0, mh + N_XXX * a.fs);
+        if (p1) e2 = pml_adr(q, MP ? ca[1] : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 1) : byi, m1, mh + N_YXY * a.fs);
+        if (p2) e3 = pml_adr(q, MP ? ca[2] : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 2) : bzi, m2, mh + N_ZXZ * a.fs);
         ew[N_XXX * a.fs] = e1; ew[N_YXY * a.fs] = e2; ew[N_ZXZ * a.fs] = e3;
         // vy^ += Dy^T e_yvy (P) + Dz^T e_zvy (M) + Dx^T e_xvy (M)
         v = vy0 + a.idy * tP<R>(e + N_YVY * a.fs, sy) + a.idz * tM<R>(e + N_ZVY * a.fs, sz) +
@@ -463,9 +486,9 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_v(El3dDev a) {
         ad[E3_VY * a.fs + o] = v;
         gy += v * __ldg(a.S + 7 * a.sterm + so);
         q = by * v; e1 = q; e2 = q; e3 = q;
-        if (p3) e1 = pml_adr(q, MP ? ca[3] : axi, MP ? cb[3] : bxi, m3, mh + N_XXY * a.fs);
-        if (p4) e2 = pml_adr(q, MP ? ca[4] : ayh, MP ? cb[4] : byh, m4, mh + N_YYY * a.fs);
-        if (p5) e3 = pml_adr(q, MP ? ca[5] : azi, MP ? cb[5] : bzi, m5, mh + N_ZYZ * a.fs);
+        if (p3) e1 = pml_adr(q, MP ? ca[3] : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 3) : bxi, m3, mh + N_XXY * a.fs);
+        if (p4) e2 = pml_adr(q, MP ? ca[4] : ayh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 4) : byh, m4, mh + N_YYY * a.fs);
+        if (p5) e3 = pml_adr(q, MP ? ca[5] : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 5) : bzi, m5, mh + N_ZYZ * a.fs);
         ew[N_XXY * a.fs] = e1; ew[N_YYY * a.fs] = e2; ew[N_ZYZ * a.fs] = e3;
         // vz^ += Dz^T e_zvz (P) + Dy^T e_yvz (M) + Dx^T e_xvz (M); with a free surface from row 2
         if (vz_ok) {
@@ -474,9 +497,9 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_v(El3dDev a) {
             ad[E3_VZ * a.fs + o] = v;
             gz += v * __ldg(a.S + 8 * a.sterm + so);
             q = bz * v; e1 = q; e2 = q; e3 = q;
-            if (p6) e1 = pml_adr(q, MP ? ca[6] : axi, MP ? cb[6] : bxi, m6, mh + N_XXZ * a.fs);
-            if (p7) e2 = pml_adr(q, MP ? ca[7] : ayi, MP ? cb[7] : byi, m7, mh + N_YYZ * a.fs);
-            if (p8) e3 = pml_adr(q, MP ? ca[8] : azh, MP ? cb[8] : bzh, m8, mh + N_ZZZ * a.fs);
+            if (p6) e1 = pml_adr(q, MP ? ca[6] : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 6) : bxi, m6, mh + N_XXZ * a.fs);
+            if (p7) e2 = pml_adr(q, MP ? ca[7] : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 7) : byi, m7, mh + N_YYZ * a.fs);
+            if (p8) e3 = pml_adr(q, MP ? ca[8] : azh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 8) : bzh, m8, mh + N_ZZZ * a.fs);
             ew[N_XXZ * a.fs] = e1; ew[N_YYZ * a.fs] = e2; ew[N_ZZZ * a.fs] = e3;
         }
     }
@@ -500,21 +523,13 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_s(El3dDev a) {
     const bool sh_n = oxi || oyi || ozi, sh_yz = oxi || oyh || ozh, sh_xz = oxh || oyi || ozh, sh_xy = oxh || oyh || ozi;
     // MP: the M-PML (a, b) of each derivative of the node (shell nodes only);
     // otherwise the per-axis 1D tables above
-    float ca[9], cb[9];
+    float ca[9];
     if (MP) {
         if (sh_n || sh_yz || sh_xz || sh_xy) {
-            e3_mpml(a, 0, x, y, z, 0, 0, 0, ca[0], cb[0]);
-            e3_mpml(a, 1, x, y, z, 0, 0, 0, ca[1], cb[1]);
-            e3_mpml(a, 2, x, y, z, 0, 0, 0, ca[2], cb[2]);
-            e3_mpml(a, 2, x, y, z, 0, 1, 1, ca[3], cb[3]);
-            e3_mpml(a, 1, x, y, z, 0, 1, 1, ca[4], cb[4]);
-            e3_mpml(a, 2, x, y, z, 1, 0, 1, ca[5], cb[5]);
-            e3_mpml(a, 0, x, y, z, 1, 0, 1, ca[6], cb[6]);
-            e3_mpml(a, 1, x, y, z, 1, 1, 0, ca[7], cb[7]);
-            e3_mpml(a, 0, x, y, z, 1, 1, 0, ca[8], cb[8]);
+            e3_coef_load<E3_PERM_AS>(a, o, 0, ca);
         } else {
 #pragma unroll
-            for (int q = 0; q < 9; ++q) ca[q] = cb[q] = 0.f;
+            for (int q = 0; q < 9; ++q) ca[q] = 0.f;
         }
     }
     const float axi = a.axi[x], bxi = a.bxi[x], axh = a.axh[x], bxh = a.bxh[x];
@@ -602,8 +617,8 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_s(El3dDev a) {
             const float w = a.dt * (c13 * xh + c23 * yh);
             qx = a.dt * (c11 * xh + c12 * yh) - r13 * w;
             qy = a.dt * (c12 * xh + c22 * yh) - r23 * w;
-            if (p0) qx = pml_adr(qx, MP ? ca[0] : axi, MP ? cb[0] : bxi, m0, mh + N_XVX * a.fs);
-            if (p1) qy = pml_adr(qy, MP ? ca[1] : ayi, MP ? cb[1] : byi, m1, mh + N_YVY * a.fs);
+            if (p0) qx = pml_adr(qx, MP ? ca[0] : axi, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 0) : bxi, m0, mh + N_XVX * a.fs);
+            if (p1) qy = pml_adr(qy, MP ? ca[1] : ayi, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 1) : byi, m1, mh + N_YVY * a.fs);
         } else {
             G[0] += xh * dX;
             G[1] += xh * dY + yh * dX;
@@ -614,9 +629,9 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_s(El3dDev a) {
             qx = a.dt * (c11 * xh + c12 * yh + c13 * zh);
             qy = a.dt * (c12 * xh + c22 * yh + c23 * zh);
             qz = a.dt * (c13 * xh + c23 * yh + c33 * zh);
-            if (p0) qx = pml_adr(qx, MP ? ca[0] : axi, MP ? cb[0] : bxi, m0, mh + N_XVX * a.fs);
-            if (p1) qy = pml_adr(qy, MP ? ca[1] : ayi, MP ? cb[1] : byi, m1, mh + N_YVY * a.fs);
-            if (p2) qz = pml_adr(qz, MP ? ca[2] : azi, MP ? cb[2] : bzi, m2, mh + N_ZVZ * a.fs);
+            if (p0) qx = pml_adr(qx, MP ? ca[0] : axi, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 0) : bxi, m0, mh + N_XVX * a.fs);
+            if (p1) qy = pml_adr(qy, MP ? ca[1] : ayi, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 1) : byi, m1, mh + N_YVY * a.fs);
+            if (p2) qz = pml_adr(qz, MP ? ca[2] : azi, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 2) : bzi, m2, mh + N_ZVZ * a.fs);
         }
         ew[N_XVX * a.fs] = qx; ew[N_YVY * a.fs] = qy; ew[N_ZVZ * a.fs] = qz;
         float q, e1, e2;
@@ -624,18 +639,18 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_s(El3dDev a) {
             G[6] += yzh * __ldg(S + 3 * a.sterm);
             G[7] += xzh * __ldg(S + 4 * a.sterm);
             q = g44 * yzh; e1 = q; e2 = q;
-            if (p3) e1 = pml_adr(q, MP ? ca[3] : azh, MP ? cb[3] : bzh, m3, mh + N_ZVY * a.fs);
-            if (p4) e2 = pml_adr(q, MP ? ca[4] : ayh, MP ? cb[4] : byh, m4, mh + N_YVZ * a.fs);
+            if (p3) e1 = pml_adr(q, MP ? ca[3] : azh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 3) : bzh, m3, mh + N_ZVY * a.fs);
+            if (p4) e2 = pml_adr(q, MP ? ca[4] : ayh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 4) : byh, m4, mh + N_YVZ * a.fs);
             ew[N_ZVY * a.fs] = e1; ew[N_YVZ * a.fs] = e2;
             q = g55 * xzh; e1 = q; e2 = q;
-            if (p5) e1 = pml_adr(q, MP ? ca[5] : azh, MP ? cb[5] : bzh, m5, mh + N_ZVX * a.fs);
-            if (p6) e2 = pml_adr(q, MP ? ca[6] : axh, MP ? cb[6] : bxh, m6, mh + N_XVZ * a.fs);
+            if (p5) e1 = pml_adr(q, MP ? ca[5] : azh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 5) : bzh, m5, mh + N_ZVX * a.fs);
+            if (p6) e2 = pml_adr(q, MP ? ca[6] : axh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 6) : bxh, m6, mh + N_XVZ * a.fs);
             ew[N_ZVX * a.fs] = e1; ew[N_XVZ * a.fs] = e2;
         }
         G[8] += xyh * __ldg(S + 5 * a.sterm);
         q = g66 * xyh; e1 = q; e2 = q;
-        if (p7) e1 = pml_adr(q, MP ? ca[7] : ayh, MP ? cb[7] : byh, m7, mh + N_YVX * a.fs);
-        if (p8) e2 = pml_adr(q, MP ? ca[8] : axh, MP ? cb[8] : bxh, m8, mh + N_XVY * a.fs);
+        if (p7) e1 = pml_adr(q, MP ? ca[7] : ayh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 7) : byh, m7, mh + N_YVX * a.fs);
+        if (p8) e2 = pml_adr(q, MP ? ca[8] : axh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 8) : bxh, m8, mh + N_XVY * a.fs);
         ew[N_YVX * a.fs] = e1; ew[N_XVY * a.fs] = e2;
     }
     const long long go = (long long)c.grp * a.fs + o;
@@ -845,7 +860,7 @@ struct El3dEngine : SsgBase {
     // faces in storage layout
     bool mpml = false;
     std::vector<float> h_faces;
-    DevBuf<float> mp_prof, mp_face;
+    DevBuf<float> mp_prof, mp_face, mp_coef;
     const std::vector<float>* mpml_faces() const override { return &h_faces; }
 
     // the M-PML tables of the model (module_cfspml.f90:421-625): damping and
@@ -929,6 +944,18 @@ struct El3dEngine : SsgBase {
             }
         mp_prof.upload(prof.data(), prof.size(), stream);
         mp_face.upload(hf.data(), hf.size(), stream);
+        // the per-node (a, b) of every shell derivative, once per model: the
+        // per-cell kernels load them instead of recomputing 18 damping
+        // coefficients (two divisions each) every step
+        if (!mpml) {
+            mp_coef.release();
+            return;
+        }
+        mp_coef.reserve(36 * (size_t)fs);
+        const El3dDev a = dev(1);
+        const dim3 b(32, 8), g((a.x1 - a.x0 + 31) / 32, (a.y1 - a.y0 + 7) / 8, a.z1 - a.z0);
+        k_el3d_mpml_coef<<<g, b, 0, stream>>>(a, mp_coef.p);
+        OWL_LAUNCH_CHECK();
     }
     E3Mp mp_view() const {
         E3Mp m{};
@@ -949,6 +976,7 @@ struct El3dEngine : SsgBase {
         m.face[4] = mp_face.p + 2 * sx + 2 * sy;
         m.face[5] = mp_face.p + 2 * sx + 2 * sy + sz;
         m.adt = std::fabs(dt);
+        m.coef = mp_coef.p;
         return m;
     }
 
@@ -1220,11 +1248,14 @@ struct El3dEngine : SsgBase {
         El3dDev ab = a;  // the per-cell kernels' view (the shell only, next to the ring kernels of an M-PML model)
         if (ring && mpml) {
             // the ratios act in the PML shell only: the ring kernels take the
-            // interior box (its x start a multiple of 4 from the halo, for the
-            // 16-byte copies), the M-PML per-cell kernels every other cell
-            a.x0 = R + 4 * ((P + 3) / 4); a.x1 = pr + nx;
-            a.y0 = pr; a.y1 = pr + ny;
-            a.z0 = pr; a.z1 = pr + nz;
+            // interior box, the M-PML per-cell kernels every other cell. The
+            // half-position nodes of the first interior cell (index pr) lie in
+            // the shell (e3_out), so the box starts at pr + 1 on every axis,
+            // its x start rounded up to a multiple of 4 from the halo for the
+            // 16-byte copies
+            a.x0 = R + 4 * ((P + 1 + 3) / 4); a.x1 = pr + nx;
+            a.y0 = pr + 1; a.y1 = pr + ny;
+            a.z0 = pr + 1; a.z1 = pr + nz;
             ab.ex0 = a.x0; ab.ex1 = a.x1; ab.ey0 = a.y0; ab.ey1 = a.y1; ab.ez0 = a.z0; ab.ez1 = a.z1;
         }
         if (ring) {

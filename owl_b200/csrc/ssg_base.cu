@@ -368,10 +368,27 @@ void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
     inj_fmask = 0;
     for (const int4& b : hbox)
         if (b.x >= 0 && b.x < 30) inj_fmask |= 1 << b.x;
+    {
+        std::vector<int4> bb(2 * (size_t)std::max(S, 1), int4{0, 0, 0, 0});
+        for (int s = 0; s < S; ++s)
+            for (int it = hinj_ptr[s]; it < hinj_ptr[s + 1]; ++it) {
+                const int4 b = hbox[it];
+                if (b.x < 0 || b.y < -(1 << 19)) continue;  // no taps
+                int4& u = bb[2 * s + (b.x == 0 ? 0 : 1)];
+                const int4 nb{b.y, b.y + BOX_W, b.w, b.w + BOX_W};
+                if (u.x == u.y) u = nb;
+                else u = int4{std::min(u.x, nb.x), std::max(u.y, nb.y), std::min(u.z, nb.z), std::max(u.w, nb.w)};
+            }
+        inj_bbox.upload(bb.data(), bb.size(), stream);
+    }
     if (hbox.empty()) { hbox.push_back(int4{-1, 0, 0, 0}); hbw.resize(boxn, 0.f); }
     inj_box.upload(hbox.data(), hbox.size(), stream);
     inj_bw.upload(hbw.data(), hbw.size(), stream);
-    fuse_on = fuse && std::getenv("OWL_NO_FUSE") == nullptr;
+    // measured slower than the separate point kernel on the 2D workloads (the
+    // extra branches and registers cost the stencil kernels more than the
+    // launch they save): opt-in with OWL_FUSE=1
+    const char* fz = std::getenv("OWL_FUSE");
+    fuse_on = fuse && fz && fz[0] == '1' && fz[1] == 0;
 }
 
 void SsgBase::ensure_state(int S, int k, bool grad) {
@@ -615,16 +632,28 @@ void SsgBase::autotune(int S, int k, bool grad) {
             if (spt > S) break;
             for (int tz : tzs) {
                 if (pass == 0) { spt_f = spt; tz_f = tz; } else { spt_a = spt; tz_a = tz; }
+                // the forward variants the time loop launches (the fused injection,
+                // without the sampling CTAs and the step counter); the adjoint's
+                // fused work is the residual scatter of extra CTAs, whose residual
+                // buffer does not exist yet: its stencil kernels are timed alone
                 auto run = [&]() {
-                    if (pass == 0) { launch_kernel(OWL_K_FWD_P, S, false); launch_kernel(OWL_K_FWD_V, S, false); }
-                    else { launch_kernel(OWL_K_ADJ_P, S, false); launch_kernel(OWL_K_ADJ_V, S, false); }
+                    if (pass == 0) {
+                        fz_mode = fuse_on ? FZ_INJ : 0;
+                        launch_kernel(OWL_K_FWD_P, S, false);
+                        launch_kernel(OWL_K_FWD_V, S, false);
+                    } else {
+                        launch_kernel(OWL_K_ADJ_P, S, false);
+                        launch_kernel(OWL_K_ADJ_V, S, false);
+                    }
+                    fz_mode = 0;
                 };
+                run();
                 run();
                 OWL_LAUNCH_CHECK();
                 EventTimer tm(stream);
-                for (int i = 0; i < 3; ++i) run();
+                for (int i = 0; i < 8; ++i) run();
                 float ms = (float)tm.stop_ms();
-                launches += 8;
+                launches += 20;
                 if (ms < best) { best = ms; bs = spt; bt = tz; }
             }
         }
@@ -720,6 +749,7 @@ void SsgBase::fill_info(owl_run_info& info, int nshots, int batches, bool grad) 
     info.batches = batches;
     info.checkpoint_interval = grad ? plan_k : 0;
     info.shots_per_launch = plan_B;
+    info.tile_z_forward = tz_f;
 }
 
 void SsgBase::forward(int nshots, const owl_shot* shots, const owl_run_opts& o, float* seis, int mem,
@@ -949,7 +979,11 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
         src_adj.reserve(std::max<size_t>(1, nitems * nt));
         if (want_src) OWL_CUDA(cudaMemsetAsync(src_adj.p, 0, sizeof(float) * std::max<size_t>(1, nitems * nt), stream));
         // 1. forward with checkpoints; the last segment stores its stencil terms
-        forward_batch(S, k, graph, true, true);
+        // the forward stores the last segment's stencil terms (no recompute of
+        // it); OWL_NO_STORE_LAST=1 checkpoints and recomputes it like the others
+        // (the tests compare the two)
+        const bool store_last = std::getenv("OWL_NO_STORE_LAST") == nullptr;
+        forward_batch(S, k, graph, true, store_last);
         if (o.check_every > 0) check_nonfinite(st.p, (size_t)S * sst);
         // 2. adjoint source and misfit
         const size_t n = (size_t)rtot * dnt();
@@ -1001,7 +1035,7 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
         want_src_now = want_src;
         for (int sg = nseg - 1; sg >= 0; --sg) {
             const int n0 = sg * k, nn = std::min(k, nt - n0);
-            if (sg == nseg - 1) {
+            if (sg == nseg - 1 && store_last) {
                 set_step(nt);
             } else {
                 restore_ckpt(sg, S);

@@ -96,6 +96,9 @@ struct SsgBase : Engine {
     // storage coordinates of its lowest corner, weights [z][y][x] (0 off the taps)
     DevBuf<int4> inj_box;
     DevBuf<float> inj_bw;
+    // per shot: bounding boxes (x0, x1, z0, z1; storage) of its taps on field 0,
+    // then on every other field (2D media)
+    DevBuf<int4> inj_bbox;
     bool fuse_on = false;  // this batch's point work runs inside the stencil kernels
     int inj_fmask = 0;     // fields the batch's sources inject into (bit f: field f)
     bool want_src_now = false;  // the adjoint sweep records the source-side adjoint

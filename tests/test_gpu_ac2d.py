@@ -166,7 +166,7 @@ def test_unstable_dt_rejected():
 def test_fused_point_work_matches_point_kernels(fs, tz):
     """Injection, sampling and the residual scatter inside the stencil kernels
     give the seismograms, misfits and gradients of the separate point kernel
-    (OWL_NO_FUSE=1) to the bit: explosion and force sources, two overlapping
+    (the default; OWL_FUSE=1 fuses) to the bit: explosion and force sources, two overlapping
     sources in one shot, off-grid receivers sharing taps, a zero-weight trace."""
     import os
     nx, nz, dx, dt, nt = 48, 40, 10.0, 1e-3, 300
@@ -177,15 +177,15 @@ def test_fused_point_work_matches_point_kernels(fs, tz):
     s = make_solver(d, vp * np.float32(1.02), rho)
     out = {}
     for off in (False, True):
-        if off:
-            os.environ["OWL_NO_FUSE"] = "1"
+        if not off:
+            os.environ["OWL_FUSE"] = "1"
         try:
             seis = s.forward(ps, RunOpts(tile_z=tz))
             mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=40, tile_z=tz))
             launches = s.last_info.gpu_launches
             gs = s.source_gradient(ps, obs, RunOpts(checkpoint_interval=40, tile_z=tz))
         finally:
-            os.environ.pop("OWL_NO_FUSE", None)
+            os.environ.pop("OWL_FUSE", None)
         out[off] = (seis, mf, g, gs, launches)
     for a, b in zip(out[False][:4], out[True][:4]):
         assert np.array_equal(np.asarray(a), np.asarray(b))
