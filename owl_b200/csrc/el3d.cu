@@ -75,7 +75,6 @@ struct El3dDev {
     int nx, ny, nz, P, R, pr, pitch;
     long long plane, fs, sst, sad;
     int x0, x1, y0, y1, z0, z1, nzb, fsurf;
-    int ex0, ex1, ey0, ey1, ez0, ez1;  // cells the per-cell kernels skip (the ring kernels' box; empty by default)
     int NYs, NZs, zchunk;  // storage planes / rows, z chunk of the ring kernels
     float idx, idy, idz, dt;
     int nshots, spt;
@@ -189,6 +188,10 @@ __device__ __forceinline__ void e3_coef_load(const El3dDev& a, long long o, int 
     for (int q = 0; q < 9; ++q) ca[q] = __ldg(a.mp.coef + (2 * (q0 + e3_perm<PERM>(q))) * a.fs + o);
 }
 template <int PERM>
+__device__ __forceinline__ float e3_ca(const El3dDev& a, long long o, int q0, int q) {
+    return __ldg(a.mp.coef + (2 * (q0 + e3_perm<PERM>(q))) * a.fs + o);
+}
+template <int PERM>
 __device__ __forceinline__ float e3_cb(const El3dDev& a, long long o, int q0, int q) {
     return __ldg(a.mp.coef + (2 * (q0 + e3_perm<PERM>(q)) + 1) * a.fs + o);
 }
@@ -221,8 +224,7 @@ __device__ __forceinline__ bool e3_cell(const El3dDev& a, E3Cell& c) {
     c.y = a.y0 + blockIdx.y * blockDim.y + threadIdx.y;
     c.z = a.z0 + zb * blockDim.z + threadIdx.z;
     c.o = (long long)c.z * a.plane + (long long)c.y * a.pitch + c.x;
-    const bool skip = c.x >= a.ex0 && c.x < a.ex1 && c.y >= a.ey0 && c.y < a.ey1 && c.z >= a.ez0 && c.z < a.ez1;
-    return c.x < a.x1 && c.y < a.y1 && c.z < a.z1 && !skip;
+    return c.x < a.x1 && c.y < a.y1 && c.z < a.z1;
 }
 
 #include "el3d_ring.cuh"
@@ -1009,8 +1011,8 @@ struct El3dEngine : SsgBase {
         if (ring_ok()) return {2, 1};
         return {2};
     }
-    // the ring kernels: half-width 4, no free surface (with M-PML ratios they
-    // take the interior box only, where the ratios never act)
+    // the ring kernels: half-width 4, no free surface (M-PML ratios: the per-node
+    // coefficient table on the shell nodes)
     bool ring_ok() const { return R == 4 && !desc.free_surface; }
     // tile_z = 1 asks for the ring kernels of both passes (where they apply), anything else the per-cell ones
     void launch_params(const owl_run_opts& o) override {
@@ -1245,19 +1247,6 @@ struct El3dEngine : SsgBase {
         OWL_CHECK((long long)a.nzb * groups < 65536, OWL_ERR_UNSUPPORTED, "too many z blocks x shot groups");
         const dim3 b(32, 4, 2), g((NXp + 31) / 32, (NYp + 3) / 4, a.nzb * groups);
         const bool ring = (fwd ? tz_f : tz_a) == 1 && RR == 4 && !FF;
-        El3dDev ab = a;  // the per-cell kernels' view (the shell only, next to the ring kernels of an M-PML model)
-        if (ring && mpml) {
-            // the ratios act in the PML shell only: the ring kernels take the
-            // interior box, the M-PML per-cell kernels every other cell. The
-            // half-position nodes of the first interior cell (index pr) lie in
-            // the shell (e3_out), so the box starts at pr + 1 on every axis,
-            // its x start rounded up to a multiple of 4 from the halo for the
-            // 16-byte copies
-            a.x0 = R + 4 * ((P + 1 + 3) / 4); a.x1 = pr + nx;
-            a.y0 = pr + 1; a.y1 = pr + ny;
-            a.z0 = pr + 1; a.z1 = pr + nz;
-            ab.ex0 = a.x0; ab.ex1 = a.x1; ab.ey0 = a.y0; ab.ey1 = a.y1; ab.ez0 = a.z0; ab.ez1 = a.z1;
-        }
         if (ring) {
             OWL_CHECK(fwd ? (!store || a.S) : (a.ad && a.S && a.G), OWL_ERR_INVALID, "buffers not allocated");
             const int rows = a.z1 - a.z0;
@@ -1267,40 +1256,41 @@ struct El3dEngine : SsgBase {
             const int nzc = (rows + a.zchunk - 1) / a.zchunk;
             OWL_CHECK((long long)nzc * groups < 65536, OWL_ERR_UNSUPPORTED, "too many z chunks x shot groups");
             const dim3 br(32, 8), gr((NXp + 31) / 32, (NYp + 7) / 8, nzc * groups);
-            if (id == OWL_K_ADJ_P) {
-                constexpr int sm = e3ra_bytes_v<4>();
-                OWL_CUDA(cudaFuncSetAttribute(k_el3d_adj_v_ring<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-                k_el3d_adj_v_ring<4><<<gr, br, sm, stream>>>(a);
-            } else if (id == OWL_K_ADJ_V) {
-                constexpr int sm = e3ra_bytes_s<4>();
-                OWL_CUDA(cudaFuncSetAttribute(k_el3d_adj_s_ring<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-                k_el3d_adj_s_ring<4><<<gr, br, sm, stream>>>(a);
-            } else if (id == OWL_K_FWD_P) {
-                constexpr int sm = e3r_bytes_s<4>();
-                auto k = store ? k_el3d_fwd_s_ring<4, true> : k_el3d_fwd_s_ring<4, false>;
-                OWL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-                k<<<gr, br, sm, stream>>>(a);
-            } else {
-                constexpr int sm = e3r_bytes_v<4>();
-                auto k = store ? k_el3d_fwd_v_ring<4, true> : k_el3d_fwd_v_ring<4, false>;
-                OWL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-                k<<<gr, br, sm, stream>>>(a);
-            }
-            if (!mpml) return;
-            launches++;  // the shell's per-cell launch below
+            if (mpml) launch_ring<true>(id, store, a, gr, br);
+            else launch_ring<false>(id, store, a, gr, br);
+            return;
         }
         if (fwd) OWL_CHECK(!store || a.S, OWL_ERR_INVALID, "stencil-term buffer not allocated");
         else OWL_CHECK(a.ad && a.S && a.G, OWL_ERR_INVALID, "adjoint buffers not allocated");
-        if (mpml) launch_cell<RR, true>(id, store, FF, ab, g, b);
-        else launch_cell<RR, false>(id, store, FF, ab, g, b);
+        if (mpml) launch_cell<RR, true>(id, store, FF, a, g, b);
+        else launch_cell<RR, false>(id, store, FF, a, g, b);
     }
-    // two stencil launches per kernel when the ring kernels of an M-PML model
-    // take the interior and the per-cell kernels the shell
-    bool hybrid() const { return mpml && ring_ok(); }
     int step_launches(int kind) const override {
-        const int extra = hybrid() && (kind == 2 ? tz_a : tz_f) == 1 ? 2 : 0;
-        if (kind != 2) return SsgBase::step_launches(kind) + extra;
-        return 2 + (want_src_now ? 1 : 0) + (nb_sct <= 4 ? 1 : 2) + extra;
+        if (kind != 2) return SsgBase::step_launches(kind);
+        return 2 + (want_src_now ? 1 : 0) + (nb_sct <= 4 ? 1 : 2);
+    }
+    // the z-marching ring kernels (half-width 4); MP: M-PML coefficients per shell node
+    template <bool MP>
+    void launch_ring(int id, bool store, const El3dDev& a, dim3 gr, dim3 br) {
+        if (id == OWL_K_ADJ_P) {
+            constexpr int sm = e3ra_bytes_v<4>();
+            OWL_CUDA(cudaFuncSetAttribute(k_el3d_adj_v_ring<4, MP>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            k_el3d_adj_v_ring<4, MP><<<gr, br, sm, stream>>>(a);
+        } else if (id == OWL_K_ADJ_V) {
+            constexpr int sm = e3ra_bytes_s<4>();
+            OWL_CUDA(cudaFuncSetAttribute(k_el3d_adj_s_ring<4, MP>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            k_el3d_adj_s_ring<4, MP><<<gr, br, sm, stream>>>(a);
+        } else if (id == OWL_K_FWD_P) {
+            constexpr int sm = e3r_bytes_s<4>();
+            auto k = store ? k_el3d_fwd_s_ring<4, true, MP> : k_el3d_fwd_s_ring<4, false, MP>;
+            OWL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            k<<<gr, br, sm, stream>>>(a);
+        } else {
+            constexpr int sm = e3r_bytes_v<4>();
+            auto k = store ? k_el3d_fwd_v_ring<4, true, MP> : k_el3d_fwd_v_ring<4, false, MP>;
+            OWL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            k<<<gr, br, sm, stream>>>(a);
+        }
     }
     // the per-cell kernels; MP: M-PML coefficients per shell node
     template <int RR, bool MP>

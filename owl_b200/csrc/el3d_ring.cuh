@@ -38,7 +38,7 @@ constexpr int e3r_bytes_s() { return E3R_NS * RingE3S<R>::STAGE * 4; }
 template <int R>
 constexpr int e3r_bytes_v() { return E3R_NS * RingE3V<R>::STAGE * 4; }
 
-template <int R, bool STORE>
+template <int R, bool STORE, bool MP>
 __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
     using T = RingE3S<R>;
     extern __shared__ __align__(16) float ring[];
@@ -114,10 +114,10 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
             const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
             const bool sh_n = valid && (oxi || oyi || ozi), sh_yz = valid && (oxi || oyh || ozh),
                        sh_xz = valid && (oxh || oyi || ozh), sh_xy = valid && (oxh || oyh || ozi);
-            const bool p0 = sh_n && axi != 0.f, p1 = sh_n && ayi != 0.f, p2 = sh_n && azi != 0.f;
-            const bool p3 = sh_yz && ayh != 0.f, p4 = sh_yz && azh != 0.f;
-            const bool p5 = sh_xz && axh != 0.f, p6 = sh_xz && azh != 0.f;
-            const bool p7 = sh_xy && axh != 0.f, p8 = sh_xy && ayh != 0.f;
+            const bool p0 = sh_n && (MP || axi != 0.f), p1 = sh_n && (MP || ayi != 0.f), p2 = sh_n && (MP || azi != 0.f);
+            const bool p3 = sh_yz && (MP || ayh != 0.f), p4 = sh_yz && (MP || azh != 0.f);
+            const bool p5 = sh_xz && (MP || axh != 0.f), p6 = sh_xz && (MP || azh != 0.f);
+            const bool p7 = sh_xy && (MP || axh != 0.f), p8 = sh_xy && (MP || ayh != 0.f);
             const float m0 = p0 ? mo[N_XVX * fs] : 0.f, m1 = p1 ? mo[N_YVY * fs] : 0.f, m2 = p2 ? mo[N_ZVZ * fs] : 0.f;
             const float m3 = p3 ? mo[N_YVZ * fs] : 0.f, m4 = p4 ? mo[N_ZVY * fs] : 0.f;
             const float m5 = p5 ? mo[N_XVZ * fs] : 0.f, m6 = p6 ? mo[N_ZVX * fs] : 0.f;
@@ -145,9 +145,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
                     sZ = sZ + c_fd3e[q - 1] * (qz[R - 1 + q] - qz[R - q]);
                 }
                 float dX = a.idx * sX, dY = a.idy * sY, dZ = a.idz * sZ;
-                if (p0) dX = pml_up(dX, axi, bxi, m0, mo + N_XVX * fs);
-                if (p1) dY = pml_up(dY, ayi, byi, m1, mo + N_YVY * fs);
-                if (p2) dZ = pml_up(dZ, azi, bzi, m2, mo + N_ZVZ * fs);
+                if (p0) dX = pml_up(dX, MP ? e3_ca<E3_PERM_S>(a, o, 0, 0) : axi, MP ? e3_cb<E3_PERM_S>(a, o, 0, 0) : bxi, m0, mo + N_XVX * fs);
+                if (p1) dY = pml_up(dY, MP ? e3_ca<E3_PERM_S>(a, o, 0, 1) : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 0, 1) : byi, m1, mo + N_YVY * fs);
+                if (p2) dZ = pml_up(dZ, MP ? e3_ca<E3_PERM_S>(a, o, 0, 2) : azi, MP ? e3_cb<E3_PERM_S>(a, o, 0, 2) : bzi, m2, mo + N_ZVZ * fs);
                 const float* so = st + T::OS + lo;
                 stp[E3_XX * fs + o] = so[0] + a.dt * (c11 * dX + c12 * dY + c13 * dZ);
                 stp[E3_YY * fs + o] = so[T::T] + a.dt * (c12 * dX + c22 * dY + c23 * dZ);
@@ -160,8 +160,8 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
                     a2 = a2 + c_fd3e[q - 1] * (tvz[(q - 1) * T::WX] - tvz[-q * T::WX]);
                 }
                 float dzvy = a.idz * a1, dyvz = a.idy * a2;
-                if (p3) dyvz = pml_up(dyvz, ayh, byh, m3, mo + N_YVZ * fs);
-                if (p4) dzvy = pml_up(dzvy, azh, bzh, m4, mo + N_ZVY * fs);
+                if (p3) dyvz = pml_up(dyvz, MP ? e3_ca<E3_PERM_S>(a, o, 0, 3) : ayh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 3) : byh, m3, mo + N_YVZ * fs);
+                if (p4) dzvy = pml_up(dzvy, MP ? e3_ca<E3_PERM_S>(a, o, 0, 4) : azh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 4) : bzh, m4, mo + N_ZVY * fs);
                 stp[E3_YZ * fs + o] = so[3 * T::T] + g44 * (dzvy + dyvz);
                 // sxz: dz vx + dx vz
                 a1 = 0.f; a2 = 0.f;
@@ -171,8 +171,8 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
                     a2 = a2 + c_fd3e[q - 1] * (tvz[q - 1] - tvz[-q]);
                 }
                 float dzvx = a.idz * a1, dxvz = a.idx * a2;
-                if (p5) dxvz = pml_up(dxvz, axh, bxh, m5, mo + N_XVZ * fs);
-                if (p6) dzvx = pml_up(dzvx, azh, bzh, m6, mo + N_ZVX * fs);
+                if (p5) dxvz = pml_up(dxvz, MP ? e3_ca<E3_PERM_S>(a, o, 0, 5) : axh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 5) : bxh, m5, mo + N_XVZ * fs);
+                if (p6) dzvx = pml_up(dzvx, MP ? e3_ca<E3_PERM_S>(a, o, 0, 6) : azh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 6) : bzh, m6, mo + N_ZVX * fs);
                 stp[E3_XZ * fs + o] = so[4 * T::T] + g55 * (dzvx + dxvz);
                 // sxy: dy vx + dx vy
                 a1 = 0.f; a2 = 0.f;
@@ -182,8 +182,8 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
                     a2 = a2 + c_fd3e[q - 1] * (tvy[q - 1] - tvy[-q]);
                 }
                 float dyvx = a.idy * a1, dxvy = a.idx * a2;
-                if (p7) dxvy = pml_up(dxvy, axh, bxh, m7, mo + N_XVY * fs);
-                if (p8) dyvx = pml_up(dyvx, ayh, byh, m8, mo + N_YVX * fs);
+                if (p7) dxvy = pml_up(dxvy, MP ? e3_ca<E3_PERM_S>(a, o, 0, 7) : axh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 7) : bxh, m7, mo + N_XVY * fs);
+                if (p8) dyvx = pml_up(dyvx, MP ? e3_ca<E3_PERM_S>(a, o, 0, 8) : ayh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 8) : byh, m8, mo + N_YVX * fs);
                 stp[E3_XY * fs + o] = so[5 * T::T] + g66 * (dyvx + dxvy);
                 if (STORE) {
                     float* S = a.S + slot + s * fs + o;
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_s_ring(El3dDev a) {
     }
 }
 
-template <int R, bool STORE>
+template <int R, bool STORE, bool MP>
 __global__ void __launch_bounds__(256, 2) k_el3d_fwd_v_ring(El3dDev a) {
     using T = RingE3V<R>;
     extern __shared__ __align__(16) float ring[];
@@ -285,9 +285,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_v_ring(El3dDev a) {
             const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
             const bool sh_vx = valid && (oxh || oyi || ozi), sh_vy = valid && (oxi || oyh || ozi),
                        sh_vz = valid && (oxi || oyi || ozh);
-            const bool p0 = sh_vx && axh != 0.f, p1 = sh_vx && ayi != 0.f, p2 = sh_vx && azi != 0.f;
-            const bool p3 = sh_vy && axi != 0.f, p4 = sh_vy && ayh != 0.f, p5 = sh_vy && azi != 0.f;
-            const bool p6 = sh_vz && axi != 0.f, p7 = sh_vz && ayi != 0.f, p8 = sh_vz && azh != 0.f;
+            const bool p0 = sh_vx && (MP || axh != 0.f), p1 = sh_vx && (MP || ayi != 0.f), p2 = sh_vx && (MP || azi != 0.f);
+            const bool p3 = sh_vy && (MP || axi != 0.f), p4 = sh_vy && (MP || ayh != 0.f), p5 = sh_vy && (MP || azi != 0.f);
+            const bool p6 = sh_vz && (MP || axi != 0.f), p7 = sh_vz && (MP || ayi != 0.f), p8 = sh_vz && (MP || azh != 0.f);
             const float m0 = p0 ? mo[N_XXX * fs] : 0.f, m1 = p1 ? mo[N_YXY * fs] : 0.f, m2 = p2 ? mo[N_ZXZ * fs] : 0.f;
             const float m3 = p3 ? mo[N_XXY * fs] : 0.f, m4 = p4 ? mo[N_YYY * fs] : 0.f, m5 = p5 ? mo[N_ZYZ * fs] : 0.f;
             const float m6 = p6 ? mo[N_XXZ * fs] : 0.f, m7 = p7 ? mo[N_YYZ * fs] : 0.f, m8 = p8 ? mo[N_ZZZ * fs] : 0.f;
@@ -311,9 +311,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_v_ring(El3dDev a) {
                     h3 = h3 + c_fd3e[q - 1] * (qxz[R - 1 + q] - qxz[R - q]);
                 }
                 h1 = a.idx * h1; h2 = a.idy * h2; h3 = a.idz * h3;
-                if (p0) h1 = pml_up(h1, axh, bxh, m0, mo + N_XXX * fs);
-                if (p1) h2 = pml_up(h2, ayi, byi, m1, mo + N_YXY * fs);
-                if (p2) h3 = pml_up(h3, azi, bzi, m2, mo + N_ZXZ * fs);
+                if (p0) h1 = pml_up(h1, MP ? e3_ca<E3_PERM_S>(a, o, 9, 0) : axh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 0) : bxh, m0, mo + N_XXX * fs);
+                if (p1) h2 = pml_up(h2, MP ? e3_ca<E3_PERM_S>(a, o, 9, 1) : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 1) : byi, m1, mo + N_YXY * fs);
+                if (p2) h3 = pml_up(h3, MP ? e3_ca<E3_PERM_S>(a, o, 9, 2) : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 2) : bzi, m2, mo + N_ZXZ * fs);
                 const float hx = h1 + h2 + h3;
                 stp[E3_VX * fs + o] = st[T::OV + lo] + st[T::OB + lo] * hx;
                 // vy: dx sxy (P) + dy syy (M) + dz syz (P)
@@ -325,9 +325,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_v_ring(El3dDev a) {
                     h3 = h3 + c_fd3e[q - 1] * (qyz[R - 1 + q] - qyz[R - q]);
                 }
                 h1 = a.idx * h1; h2 = a.idy * h2; h3 = a.idz * h3;
-                if (p3) h1 = pml_up(h1, axi, bxi, m3, mo + N_XXY * fs);
-                if (p4) h2 = pml_up(h2, ayh, byh, m4, mo + N_YYY * fs);
-                if (p5) h3 = pml_up(h3, azi, bzi, m5, mo + N_ZYZ * fs);
+                if (p3) h1 = pml_up(h1, MP ? e3_ca<E3_PERM_S>(a, o, 9, 3) : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 3) : bxi, m3, mo + N_XXY * fs);
+                if (p4) h2 = pml_up(h2, MP ? e3_ca<E3_PERM_S>(a, o, 9, 4) : ayh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 4) : byh, m4, mo + N_YYY * fs);
+                if (p5) h3 = pml_up(h3, MP ? e3_ca<E3_PERM_S>(a, o, 9, 5) : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 5) : bzi, m5, mo + N_ZYZ * fs);
                 const float hy = h1 + h2 + h3;
                 stp[E3_VY * fs + o] = st[T::OV + T::T + lo] + st[T::OB + T::T + lo] * hy;
                 // vz: dx sxz (P) + dy syz (P) + dz szz (M)
@@ -339,9 +339,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_fwd_v_ring(El3dDev a) {
                     h3 = h3 + c_fd3e[q - 1] * (qzz[R + q - 1] - qzz[R - q]);
                 }
                 h1 = a.idx * h1; h2 = a.idy * h2; h3 = a.idz * h3;
-                if (p6) h1 = pml_up(h1, axi, bxi, m6, mo + N_XXZ * fs);
-                if (p7) h2 = pml_up(h2, ayi, byi, m7, mo + N_YYZ * fs);
-                if (p8) h3 = pml_up(h3, azh, bzh, m8, mo + N_ZZZ * fs);
+                if (p6) h1 = pml_up(h1, MP ? e3_ca<E3_PERM_S>(a, o, 9, 6) : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 6) : bxi, m6, mo + N_XXZ * fs);
+                if (p7) h2 = pml_up(h2, MP ? e3_ca<E3_PERM_S>(a, o, 9, 7) : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 7) : byi, m7, mo + N_YYZ * fs);
+                if (p8) h3 = pml_up(h3, MP ? e3_ca<E3_PERM_S>(a, o, 9, 8) : azh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 8) : bzh, m8, mo + N_ZZZ * fs);
                 const float hz = h1 + h2 + h3;
                 stp[E3_VZ * fs + o] = st[T::OV + 2 * T::T + lo] + st[T::OB + 2 * T::T + lo] * hz;
                 if (STORE) {

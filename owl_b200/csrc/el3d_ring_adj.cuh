@@ -47,7 +47,7 @@ __device__ __forceinline__ void e3_kahan_rw(float* G, long long gg, long long go
 
 // velocity nodes: v^ += D^T e (stress-derivative e terms), rho correlations,
 // adjoint PML terms of the velocity derivatives
-template <int R>
+template <int R, bool MP>
 __global__ void __launch_bounds__(256, 2) k_el3d_adj_v_ring(El3dDev a) {
     using T = RingA3V<R>;
     constexpr int NS = E3RA_NS_V;
@@ -125,9 +125,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_adj_v_ring(El3dDev a) {
             const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
             const bool sh_vx = valid && (oxh || oyi || ozi), sh_vy = valid && (oxi || oyh || ozi),
                        sh_vz = valid && (oxi || oyi || ozh);
-            const bool p0 = sh_vx && axh != 0.f, p1 = sh_vx && ayi != 0.f, p2 = sh_vx && azi != 0.f;
-            const bool p3 = sh_vy && axi != 0.f, p4 = sh_vy && ayh != 0.f, p5 = sh_vy && azi != 0.f;
-            const bool p6 = sh_vz && axi != 0.f, p7 = sh_vz && ayi != 0.f, p8 = sh_vz && azh != 0.f;
+            const bool p0 = sh_vx && (MP || axh != 0.f), p1 = sh_vx && (MP || ayi != 0.f), p2 = sh_vx && (MP || azi != 0.f);
+            const bool p3 = sh_vy && (MP || axi != 0.f), p4 = sh_vy && (MP || ayh != 0.f), p5 = sh_vy && (MP || azi != 0.f);
+            const bool p6 = sh_vz && (MP || axi != 0.f), p7 = sh_vz && (MP || ayi != 0.f), p8 = sh_vz && (MP || azh != 0.f);
             const float m0 = p0 ? mh[N_XXX * fs + o] : 0.f, m1 = p1 ? mh[N_YXY * fs + o] : 0.f;
             const float m2 = p2 ? mh[N_ZXZ * fs + o] : 0.f, m3 = p3 ? mh[N_XXY * fs + o] : 0.f;
             const float m4 = p4 ? mh[N_YYY * fs + o] : 0.f, m5 = p5 ? mh[N_ZYZ * fs + o] : 0.f;
@@ -166,9 +166,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_adj_v_ring(El3dDev a) {
                 ad[E3_VX * fs + o] = v;
                 e3_kahan_rw(a.G, a.gg, go, 9, g[0], c[0], v * os[0]);
                 float qq = ob[0] * v, e1 = qq, e2 = qq, e3 = qq;
-                if (p0) e1 = pml_adr(qq, axh, bxh, m0, mh + N_XXX * fs + o);
-                if (p1) e2 = pml_adr(qq, ayi, byi, m1, mh + N_YXY * fs + o);
-                if (p2) e3 = pml_adr(qq, azi, bzi, m2, mh + N_ZXZ * fs + o);
+                if (p0) e1 = pml_adr(qq, MP ? e3_ca<E3_PERM_S>(a, o, 9, 0) : axh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 0) : bxh, m0, mh + N_XXX * fs + o);
+                if (p1) e2 = pml_adr(qq, MP ? e3_ca<E3_PERM_S>(a, o, 9, 1) : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 1) : byi, m1, mh + N_YXY * fs + o);
+                if (p2) e3 = pml_adr(qq, MP ? e3_ca<E3_PERM_S>(a, o, 9, 2) : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 2) : bzi, m2, mh + N_ZXZ * fs + o);
                 ew[N_XXX * fs + o] = e1; ew[N_YXY * fs + o] = e2; ew[N_ZXZ * fs + o] = e3;
                 // vy^ += Dy^T e_yvy (P) + Dz^T e_zvy (M) + Dx^T e_xvy (M)
                 tpx = 0.f; tmx = 0.f; tmy = 0.f;
@@ -182,9 +182,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_adj_v_ring(El3dDev a) {
                 ad[E3_VY * fs + o] = v;
                 e3_kahan_rw(a.G, a.gg, go, 10, g[1], c[1], v * os[T::T]);
                 qq = ob[T::T] * v; e1 = qq; e2 = qq; e3 = qq;
-                if (p3) e1 = pml_adr(qq, axi, bxi, m3, mh + N_XXY * fs + o);
-                if (p4) e2 = pml_adr(qq, ayh, byh, m4, mh + N_YYY * fs + o);
-                if (p5) e3 = pml_adr(qq, azi, bzi, m5, mh + N_ZYZ * fs + o);
+                if (p3) e1 = pml_adr(qq, MP ? e3_ca<E3_PERM_S>(a, o, 9, 3) : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 3) : bxi, m3, mh + N_XXY * fs + o);
+                if (p4) e2 = pml_adr(qq, MP ? e3_ca<E3_PERM_S>(a, o, 9, 4) : ayh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 4) : byh, m4, mh + N_YYY * fs + o);
+                if (p5) e3 = pml_adr(qq, MP ? e3_ca<E3_PERM_S>(a, o, 9, 5) : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 5) : bzi, m5, mh + N_ZYZ * fs + o);
                 ew[N_XXY * fs + o] = e1; ew[N_YYY * fs + o] = e2; ew[N_ZYZ * fs + o] = e3;
                 // vz^ += Dz^T e_zvz (P) + Dy^T e_yvz (M) + Dx^T e_xvz (M)
                 tpx = 0.f; tmx = 0.f; tmy = 0.f;
@@ -198,9 +198,9 @@ __global__ void __launch_bounds__(256, 2) k_el3d_adj_v_ring(El3dDev a) {
                 ad[E3_VZ * fs + o] = v;
                 e3_kahan_rw(a.G, a.gg, go, 11, g[2], c[2], v * os[2 * T::T]);
                 qq = ob[2 * T::T] * v; e1 = qq; e2 = qq; e3 = qq;
-                if (p6) e1 = pml_adr(qq, axi, bxi, m6, mh + N_XXZ * fs + o);
-                if (p7) e2 = pml_adr(qq, ayi, byi, m7, mh + N_YYZ * fs + o);
-                if (p8) e3 = pml_adr(qq, azh, bzh, m8, mh + N_ZZZ * fs + o);
+                if (p6) e1 = pml_adr(qq, MP ? e3_ca<E3_PERM_S>(a, o, 9, 6) : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 6) : bxi, m6, mh + N_XXZ * fs + o);
+                if (p7) e2 = pml_adr(qq, MP ? e3_ca<E3_PERM_S>(a, o, 9, 7) : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 7) : byi, m7, mh + N_YYZ * fs + o);
+                if (p8) e3 = pml_adr(qq, MP ? e3_ca<E3_PERM_S>(a, o, 9, 8) : azh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 8) : bzh, m8, mh + N_ZZZ * fs + o);
                 ew[N_XXZ * fs + o] = e1; ew[N_YYZ * fs + o] = e2; ew[N_ZZZ * fs + o] = e3;
             }
 #pragma unroll
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(256, 2) k_el3d_adj_v_ring(El3dDev a) {
 
 // stress nodes: sigma^ += D^T e (velocity-derivative e terms), Cij
 // correlations, adjoint PML terms of the stress derivatives
-template <int R>
+template <int R, bool MP>
 __global__ void __launch_bounds__(256, 2) k_el3d_adj_s_ring(El3dDev a) {
     using T = RingA3S<R>;
     constexpr int NS = E3RA_NS_S;
@@ -303,10 +303,10 @@ __global__ void __launch_bounds__(256, 2) k_el3d_adj_s_ring(El3dDev a) {
             const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
             const bool sh_n = valid && (oxi || oyi || ozi), sh_yz = valid && (oxi || oyh || ozh),
                        sh_xz = valid && (oxh || oyi || ozh), sh_xy = valid && (oxh || oyh || ozi);
-            const bool p0 = sh_n && axi != 0.f, p1 = sh_n && ayi != 0.f, p2 = sh_n && azi != 0.f;
-            const bool p3 = sh_yz && azh != 0.f, p4 = sh_yz && ayh != 0.f;
-            const bool p5 = sh_xz && azh != 0.f, p6 = sh_xz && axh != 0.f;
-            const bool p7 = sh_xy && ayh != 0.f, p8 = sh_xy && axh != 0.f;
+            const bool p0 = sh_n && (MP || axi != 0.f), p1 = sh_n && (MP || ayi != 0.f), p2 = sh_n && (MP || azi != 0.f);
+            const bool p3 = sh_yz && (MP || azh != 0.f), p4 = sh_yz && (MP || ayh != 0.f);
+            const bool p5 = sh_xz && (MP || azh != 0.f), p6 = sh_xz && (MP || axh != 0.f);
+            const bool p7 = sh_xy && (MP || ayh != 0.f), p8 = sh_xy && (MP || axh != 0.f);
             const float m0 = p0 ? mh[N_XVX * fs + o] : 0.f, m1 = p1 ? mh[N_YVY * fs + o] : 0.f;
             const float m2 = p2 ? mh[N_ZVZ * fs + o] : 0.f, m3 = p3 ? mh[N_ZVY * fs + o] : 0.f;
             const float m4 = p4 ? mh[N_YVZ * fs + o] : 0.f, m5 = p5 ? mh[N_ZVX * fs + o] : 0.f;
@@ -373,21 +373,21 @@ __global__ void __launch_bounds__(256, 2) k_el3d_adj_s_ring(El3dDev a) {
                 float qx_ = a.dt * (c11 * xh + c12 * yh + c13 * zh);
                 float qy_ = a.dt * (c12 * xh + c22 * yh + c23 * zh);
                 float qz_ = a.dt * (c13 * xh + c23 * yh + c33 * zh);
-                if (p0) qx_ = pml_adr(qx_, axi, bxi, m0, mh + N_XVX * fs + o);
-                if (p1) qy_ = pml_adr(qy_, ayi, byi, m1, mh + N_YVY * fs + o);
-                if (p2) qz_ = pml_adr(qz_, azi, bzi, m2, mh + N_ZVZ * fs + o);
+                if (p0) qx_ = pml_adr(qx_, MP ? e3_ca<E3_PERM_AS>(a, o, 0, 0) : axi, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 0) : bxi, m0, mh + N_XVX * fs + o);
+                if (p1) qy_ = pml_adr(qy_, MP ? e3_ca<E3_PERM_AS>(a, o, 0, 1) : ayi, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 1) : byi, m1, mh + N_YVY * fs + o);
+                if (p2) qz_ = pml_adr(qz_, MP ? e3_ca<E3_PERM_AS>(a, o, 0, 2) : azi, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 2) : bzi, m2, mh + N_ZVZ * fs + o);
                 ew[N_XVX * fs + o] = qx_; ew[N_YVY * fs + o] = qy_; ew[N_ZVZ * fs + o] = qz_;
                 float q = a.dt * sm[6 * T::T] * yzh, e1 = q, e2 = q;
-                if (p3) e1 = pml_adr(q, azh, bzh, m3, mh + N_ZVY * fs + o);
-                if (p4) e2 = pml_adr(q, ayh, byh, m4, mh + N_YVZ * fs + o);
+                if (p3) e1 = pml_adr(q, MP ? e3_ca<E3_PERM_AS>(a, o, 0, 3) : azh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 3) : bzh, m3, mh + N_ZVY * fs + o);
+                if (p4) e2 = pml_adr(q, MP ? e3_ca<E3_PERM_AS>(a, o, 0, 4) : ayh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 4) : byh, m4, mh + N_YVZ * fs + o);
                 ew[N_ZVY * fs + o] = e1; ew[N_YVZ * fs + o] = e2;
                 q = a.dt * sm[7 * T::T] * xzh; e1 = q; e2 = q;
-                if (p5) e1 = pml_adr(q, azh, bzh, m5, mh + N_ZVX * fs + o);
-                if (p6) e2 = pml_adr(q, axh, bxh, m6, mh + N_XVZ * fs + o);
+                if (p5) e1 = pml_adr(q, MP ? e3_ca<E3_PERM_AS>(a, o, 0, 5) : azh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 5) : bzh, m5, mh + N_ZVX * fs + o);
+                if (p6) e2 = pml_adr(q, MP ? e3_ca<E3_PERM_AS>(a, o, 0, 6) : axh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 6) : bxh, m6, mh + N_XVZ * fs + o);
                 ew[N_ZVX * fs + o] = e1; ew[N_XVZ * fs + o] = e2;
                 q = a.dt * sm[8 * T::T] * xyh; e1 = q; e2 = q;
-                if (p7) e1 = pml_adr(q, ayh, byh, m7, mh + N_YVX * fs + o);
-                if (p8) e2 = pml_adr(q, axh, bxh, m8, mh + N_XVY * fs + o);
+                if (p7) e1 = pml_adr(q, MP ? e3_ca<E3_PERM_AS>(a, o, 0, 7) : ayh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 7) : byh, m7, mh + N_YVX * fs + o);
+                if (p8) e2 = pml_adr(q, MP ? e3_ca<E3_PERM_AS>(a, o, 0, 8) : axh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 8) : bxh, m8, mh + N_XVY * fs + o);
                 ew[N_YVX * fs + o] = e1; ew[N_XVY * fs + o] = e2;
             }
 #pragma unroll
