@@ -572,11 +572,18 @@ def headline_roofline(s, d, k, peak, peak_kind):
     # the other segments storing; adjoint every step
     counts = {L.OWL_K_FWD_P: nt - n_last, L.OWL_K_FWD_V: nt - n_last, L.OWL_K_FWD_P_STORE: nt,
               L.OWL_K_FWD_V_STORE: nt, L.OWL_K_ADJ_P: nt, L.OWL_K_ADJ_V: nt}
-    # the autotuner's variants: tile codes >= 100 are the four-cell kernels
+    # the autotuner's variants: tile codes >= 100 are the four-cell kernels,
+    # >= 200 with the pipelined adjoint p kernel (when a CTA takes several shots)
     v4f = s.last_info.tile_z_forward >= 100
     v4a = s.last_info.tile_z >= 100
-    fp, fv = ("k_ac2d_fwd_p4", "k_ac2d_fwd_v4") if v4f else ("k_ac2d_fwd_p", "k_ac2d_fwd_vf")
+    pfa = s.last_info.tile_z >= 200 and s.last_info.shots_per_cta > 1
+    pff = s.last_info.tile_z_forward >= 200 and s.last_info.shots_per_cta_forward > 1
+    fp, fv = ("k_ac2d_fwd_p4", "k_ac2d_fwd_v4") if v4f else ("k_ac2d_fwd_p", "k_ac2d_fwd_v")
     ap, av = ("k_ac2d_adj_p4", "k_ac2d_adj_v4") if v4a else ("k_ac2d_adj_p", "k_ac2d_adj_v")
+    if pff:
+        fp, fv = fp + "_pf", fv + "_pf"
+    if pfa:
+        ap, av = ap + "_pf", av + "_pf"
     names = {L.OWL_K_FWD_P: fp + "<4,0>", L.OWL_K_FWD_V: fv + "<4,0>",
              L.OWL_K_FWD_P_STORE: fp + "<4,1>", L.OWL_K_FWD_V_STORE: fv + "<4,1>",
              L.OWL_K_ADJ_P: ap + "<4>", L.OWL_K_ADJ_V: av + "<4>"}
@@ -595,7 +602,8 @@ def headline_roofline(s, d, k, peak, peak_kind):
             "launches_per_gradient": {names[q]: counts[q] for q in kt},
             "kernel_ms_per_gradient": {names[q]: kt[q][0] * counts[q] for q in kt},
             "tile_codes": {"forward": s.last_info.tile_z_forward, "adjoint": s.last_info.tile_z,
-                           "shots_per_cta": s.last_info.shots_per_cta}}
+                           "shots_per_cta": s.last_info.shots_per_cta,
+                           "shots_per_cta_forward": s.last_info.shots_per_cta_forward}}
 
 
 def main():

@@ -19,7 +19,7 @@ module owl_ssg_c
     use iso_c_binding
     implicit none
 
-    integer(c_int), parameter :: OWL_SSG_ABI_VERSION = 8
+    integer(c_int), parameter :: OWL_SSG_ABI_VERSION = 9
 
     ! status codes
     integer(c_int), parameter :: OWL_OK = 0
@@ -233,6 +233,7 @@ module owl_ssg_c
         integer(c_int) :: checkpoint_interval
         integer(c_int) :: shots_per_launch
         integer(c_int) :: tile_z_forward
+        integer(c_int) :: shots_per_cta_forward
     end type
 
     interface

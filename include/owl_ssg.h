@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define OWL_SSG_ABI_VERSION 8
+#define OWL_SSG_ABI_VERSION 9
 
 /* status codes */
 #define OWL_OK 0
@@ -233,6 +233,7 @@ typedef struct {
     int checkpoint_interval;  /* gradients: the interval used (opts, or chosen from free device memory) */
     int shots_per_launch;     /* shots per batched launch used (opts, or the most that fit the device) */
     int tile_z_forward;       /* the forward kernels' tile code (tile_z is the adjoint kernels' in a gradient) */
+    int shots_per_cta_forward; /* the forward kernels' shots per CTA (shots_per_cta is the adjoint kernels' in a gradient) */
 } owl_run_info;
 
 /* ---- lifecycle ---------------------------------------------------------- */

@@ -188,6 +188,7 @@ class OwlRunInfo(C.Structure):
         ("tile_x", C.c_int), ("tile_z", C.c_int),
         ("batches", C.c_int),
         ("checkpoint_interval", C.c_int), ("shots_per_launch", C.c_int), ("tile_z_forward", C.c_int),
+        ("shots_per_cta_forward", C.c_int),
     ]
 
 

@@ -665,16 +665,18 @@ struct Ac2dEngine : SsgBase {
 
     // tile heights of the autotuner: 4, 8, 16 rows of one-cell threads (32 x
     // tz), or 100 + 2, 4, 8 rows of four-cell threads (k_ac2d_*4, 32 x tz
-    // threads covering 128 x tz cells)
-    std::vector<int> tune_tz(int) const override { return {4, 8, 16, 102, 104, 108}; }
+    // threads covering 128 x tz cells), or 200 + 2, 4, 8: the four-cell
+    // tiles with each thread loading its next shot's cells ahead (when a CTA
+    // takes several shots)
+    std::vector<int> tune_tz(int) const override { return {4, 8, 16, 102, 104, 108, 202, 204, 208}; }
     void launch_params(const owl_run_opts& o) override {
         const bool vec = o.tile_z >= 100;
         owl_run_opts q = o;
-        if (vec) q.tile_z = o.tile_z - 100;
+        if (vec) q.tile_z = o.tile_z % 100;
         SsgBase::launch_params(q);
         if (vec) {
-            OWL_CHECK(tile_x == 32 && q.tile_z <= 8, OWL_ERR_INVALID,
-                      "four-cell tiles: tile_x 32 and tile_z 100 + (1 .. 8)");
+            OWL_CHECK(tile_x == 32 && q.tile_z >= 1 && q.tile_z <= 8 && o.tile_z < 300, OWL_ERR_INVALID,
+                      "four-cell tiles: tile_x 32 and tile_z 100 + (1 .. 8) or 200 + (1 .. 8)");
             tz_f = tz_a = o.tile_z;
         }
     }
@@ -735,6 +737,9 @@ struct Ac2dEngine : SsgBase {
     // the four-cell kernels: 32 x ty threads over 128 x ty cells
     template <int RR>
     void launch_v4(int id, int S, bool store, int ty) {
+        // tile codes 200 + ty: the same tiles with the next shot's loads issued ahead
+        const bool pf = ty >= 100;
+        ty %= 100;
         Ac2dDev a = dev(S);
         const int rows_p = a.z1 - a.zp0, rows_v = a.z1 - std::min(a.zvx0, a.zvz0);
         const int rows_a = a.z1 - std::min(std::min(a.zvx0, a.zvz0), a.zp0);
@@ -751,32 +756,40 @@ struct Ac2dEngine : SsgBase {
         if (id == OWL_K_FWD_P) {
             a.spt = spt_f;
             const dim3 g = grid(rows_p, spt_f);
+            const bool p2 = pf && !fz && spt_f > 1;
             if (store) {
                 if (fz) launch_pdl(k_ac2d_fwd_p4<RR, true, true>, g, b, 0, stream, a);
+                else if (p2) launch_pdl(k_ac2d_fwd_p4_pf<RR, true>, g, b, 0, stream, a);
                 else launch_pdl(k_ac2d_fwd_p4<RR, true, false>, g, b, 0, stream, a);
             } else {
                 if (fz) launch_pdl(k_ac2d_fwd_p4<RR, false, true>, g, b, 0, stream, a);
+                else if (p2) launch_pdl(k_ac2d_fwd_p4_pf<RR, false>, g, b, 0, stream, a);
                 else launch_pdl(k_ac2d_fwd_p4<RR, false, false>, g, b, 0, stream, a);
             }
         } else if (id == OWL_K_FWD_V) {
             a.spt = spt_f;
             dim3 g = grid(rows_v, spt_f);
             if (fz && (fz_mode & FZ_SMP)) add_point_rows(g, nb_rec);
+            const bool p2 = pf && !fz && spt_f > 1;
             if (store) {
                 if (fz) launch_pdl(k_ac2d_fwd_v4<RR, true, true>, g, b, 0, stream, a);
+                else if (p2) launch_pdl(k_ac2d_fwd_v4_pf<RR, true>, g, b, 0, stream, a);
                 else launch_pdl(k_ac2d_fwd_v4<RR, true, false>, g, b, 0, stream, a);
             } else {
                 if (fz) launch_pdl(k_ac2d_fwd_v4<RR, false, true>, g, b, 0, stream, a);
+                else if (p2) launch_pdl(k_ac2d_fwd_v4_pf<RR, false>, g, b, 0, stream, a);
                 else launch_pdl(k_ac2d_fwd_v4<RR, false, false>, g, b, 0, stream, a);
             }
         } else if (id == OWL_K_ADJ_P) {
             a.spt = spt_a;
-            launch_pdl(k_ac2d_adj_p4<RR>, grid(rows_a, spt_a), b, 0, stream, a);
+            if (pf && spt_a > 1) launch_pdl(k_ac2d_adj_p4_pf<RR>, grid(rows_a, spt_a), b, 0, stream, a);
+            else launch_pdl(k_ac2d_adj_p4<RR>, grid(rows_a, spt_a), b, 0, stream, a);
         } else {
             a.spt = spt_a;
             dim3 g = grid(rows_v, spt_a);
             if (fz && (fz_mode & FZ_SCT)) add_point_rows(g, nb_sct);
             if (fz) launch_pdl(k_ac2d_adj_v4<RR, true>, g, b, 0, stream, a);
+            else if (pf && spt_a > 1) launch_pdl(k_ac2d_adj_v4_pf<RR>, g, b, 0, stream, a);
             else launch_pdl(k_ac2d_adj_v4<RR, false>, g, b, 0, stream, a);
         }
     }

@@ -624,7 +624,14 @@ void SsgBase::autotune(int S, int k, bool grad) {
     }
     cur_k = k;
     set_step(k);
+    // the forward pass's choice is shared by the forward-only and the gradient
+    // entries of S: the forwards of a misfit and of a gradient of one handle
+    // run the same kernels (their seismograms equal to the bit)
+    const auto other = tune_cache.find(std::make_pair(S, grad ? 0 : 1));
+    const bool have_fwd = other != tune_cache.end();
+    if (have_fwd) { spt_f = other->second[0]; tz_f = other->second[1]; }
     for (int pass = 0; pass < (grad ? 2 : 1); ++pass) {
+        if (pass == 0 && have_fwd) continue;
         const std::vector<int> tzs = tune_tz(pass);
         float best = 1e30f;
         int bs = 1, bt = tzs[std::min<size_t>(1, tzs.size() - 1)];
@@ -750,6 +757,7 @@ void SsgBase::fill_info(owl_run_info& info, int nshots, int batches, bool grad) 
     info.checkpoint_interval = grad ? plan_k : 0;
     info.shots_per_launch = plan_B;
     info.tile_z_forward = tz_f;
+    info.shots_per_cta_forward = spt_f;
 }
 
 void SsgBase::forward(int nshots, const owl_shot* shots, const owl_run_opts& o, float* seis, int mem,

@@ -30,7 +30,7 @@ def test_header_symbols_exported():
 
 def test_queries():
     lib = L.load()
-    assert lib.owl_ssg_abi_version() == 8
+    assert lib.owl_ssg_abi_version() == 9
     assert lib.owl_ssg_nparam(L.OWL_ACOUSTIC_ISO_2D) == 2
     assert lib.owl_ssg_ncomp(L.OWL_ELASTIC_VHTIORT_2D) == 2
     assert lib.owl_ssg_nparam(99) == -1
