@@ -43,6 +43,9 @@ def parse():
     p.add_argument("--nshots", type=int, default=NSHOTS, help="shots per GPU (32 for the benchmark)")
     p.add_argument("--profile", action="store_true",
                    help="profiling target: one gradient step of --nshots shots, nothing else, no JSON line")
+    p.add_argument("--tile-z", type=int, default=0,
+                   help="--profile: tile code of the kernels (0: autotuned, which adds the tuning launches)")
+    p.add_argument("--spt", type=int, default=0, help="--profile: shots per CTA with --tile-z")
     p.add_argument("--no-3d", action="store_true", help="skip the 3D acoustic forward roofline block")
     p.add_argument("--no-misfits", action="store_true", help="skip the data-domain misfit block")
     p.add_argument("--rows", type=int, default=1, help="rows per thread of the --profile3d forward kernels")
@@ -56,6 +59,8 @@ def parse():
     p.add_argument("--profile-el", type=int, default=0, metavar="S",
                    help="profiling target: one 2D elastic VTI gradient of S shots, 60 steps, no JSON line")
     p.add_argument("--ring", action="store_true", help="--profile-el3 with the ring forward kernels")
+    p.add_argument("--profile-el3-fwd", type=int, default=0, metavar="N",
+                   help="profiling target: a 10-step 3D elastic ORT forward of 1 shot on an N^3 model")
     p.add_argument("--profile-el3", type=int, default=0, metavar="N",
                    help="profiling target: one 3D elastic ORT gradient of 1 shot on an N^3 model, 40 steps")
     return p.parse_args()
@@ -215,6 +220,23 @@ def profile_elastic3(n, ring=False):
     obs = np.zeros(s.seis_size(ps), dtype=np.float32)
     s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=20, shots_per_cta=1, tile_z=1 if ring else 2, use_graph=-1))
     print(f"profile-el3: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
+    s.close()
+
+
+def profile_elastic3_forward(n, ring=False):
+    """3D elastic forward for DRAM-traffic captures: the ORT model on n^3 (M-PML
+    ratios on), 1 shot, 10 steps, no stored stencil terms; ring or per-cell kernels."""
+    from owl_b200 import _lib as L
+    from owl_b200 import configs
+    from owl_b200.solver import RunOpts, SSGSolver
+
+    d, f, shots = configs.config5(1, nt=10, n=n, nrec=16)
+    s = SSGSolver(L.OWL_ELASTIC_VHTIORT_3D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
+                  f0_max=d.f0_max, max_shots=1, ny=d.ny, dy=d.dy, aniso=d.aniso)
+    s.set_model(*f)
+    ps = s.prepare(shots)
+    s.forward(ps, RunOpts(shots_per_cta=1, tile_z=1 if ring else 2, use_graph=-1))
+    print(f"profile-el3-fwd: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
     s.close()
 
 
@@ -572,18 +594,17 @@ def headline_roofline(s, d, k, peak, peak_kind):
     # the other segments storing; adjoint every step
     counts = {L.OWL_K_FWD_P: nt - n_last, L.OWL_K_FWD_V: nt - n_last, L.OWL_K_FWD_P_STORE: nt,
               L.OWL_K_FWD_V_STORE: nt, L.OWL_K_ADJ_P: nt, L.OWL_K_ADJ_V: nt}
-    # the autotuner's variants: tile codes >= 100 are the four-cell kernels,
-    # >= 200 with the pipelined adjoint p kernel (when a CTA takes several shots)
-    v4f = s.last_info.tile_z_forward >= 100
-    v4a = s.last_info.tile_z >= 100
-    pfa = s.last_info.tile_z >= 200 and s.last_info.shots_per_cta > 1
-    pff = s.last_info.tile_z_forward >= 200 and s.last_info.shots_per_cta_forward > 1
+    # the autotuner's variants: tile codes 100 + h are the four-cell kernels,
+    # 200 + h the same with the pipelined adjoint p kernel, 300 + h the
+    # one-cell kernels with it (pipelined only when a CTA takes several shots)
+    tzf, tza = s.last_info.tile_z_forward, s.last_info.tile_z
+    v4f = 100 <= tzf < 300
+    v4a = 100 <= tza < 300
+    pfa = tza >= 200 and s.last_info.shots_per_cta > 1
     fp, fv = ("k_ac2d_fwd_p4", "k_ac2d_fwd_v4") if v4f else ("k_ac2d_fwd_p", "k_ac2d_fwd_v")
     ap, av = ("k_ac2d_adj_p4", "k_ac2d_adj_v4") if v4a else ("k_ac2d_adj_p", "k_ac2d_adj_v")
-    if pff:
-        fp, fv = fp + "_pf", fv + "_pf"
     if pfa:
-        ap, av = ap + "_pf", av + "_pf"
+        ap = ap + "_pf"
     names = {L.OWL_K_FWD_P: fp + "<4,0>", L.OWL_K_FWD_V: fv + "<4,0>",
              L.OWL_K_FWD_P_STORE: fp + "<4,1>", L.OWL_K_FWD_V_STORE: fv + "<4,1>",
              L.OWL_K_ADJ_P: ap + "<4>", L.OWL_K_ADJ_V: av + "<4>"}
@@ -617,6 +638,8 @@ def main():
         return profile_elastic(args.profile_el)
     if args.profile_el3:
         return profile_elastic3(args.profile_el3, args.ring)
+    if args.profile_el3_fwd:
+        return profile_elastic3_forward(args.profile_el3_fwd, args.ring)
     if args.profile3d_grad:
         return profile_3d_grad(args.profile3d_grad)
     if args.impl == "reference":
@@ -648,6 +671,8 @@ def main():
     obs = s.forward(ps)  # observed data from the true model (not timed)
     s.set_model(vp0, rho0)
     opts = RunOpts(checkpoint_interval=CKPT_K)
+    if args.profile and args.tile_z:
+        opts = RunOpts(checkpoint_interval=CKPT_K, tile_z=args.tile_z, shots_per_cta=max(1, args.spt))
     nm = d.nx * d.nz
     obs_dev = torch.from_numpy(obs).cuda()
     g_dev = torch.zeros(2 * nm, dtype=torch.float32, device="cuda")

@@ -279,9 +279,12 @@ __global__ void __launch_bounds__(512, 3) k_ac2d_fwd_vf(Ac2dDev a) {
 // Every node's e is computed once by its owner and read by its neighbours in
 // the next launch: no double buffering, no halo recomputation. Entries of e
 // outside a field's update range stay zero.
-template <int R>
-__global__ void __launch_bounds__(512) k_ac2d_adj_p(Ac2dDev a) {
-    pdl_prologue();
+//
+// PF: the next shot's cell values are loaded before this shot's stores (they
+// cannot alias: each shot owns its own slices), so two shots' loads are in
+// flight per thread instead of one
+template <int R, bool PF>
+__device__ __forceinline__ void ac2d_adj_p_cells(const Ac2dDev& a) {
     const int zr0 = min(min(a.zvx0, a.zvz0), a.zp0);
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -300,18 +303,37 @@ __global__ void __launch_bounds__(512) k_ac2d_adj_p(Ac2dDev a) {
     const int pt = a.pitch;
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     float gbk = 0.f, gbx = 0.f, gbz = 0.f;
-    for (int s = s0; s < s1; ++s) {
+    // every read of a shot's cell is issued ahead of its stores: the arrays
+    // share one allocation, so no plain read could move above a store and each
+    // would cost its own round trip. Arrays that no thread of this launch
+    // writes (the e terms of the neighbours, the stored stencil terms) are read
+    // through the read-only path, which the compiler may schedule freely.
+    struct Cell {
+        float vx, svx, vz, svz, p0, sp, m1, m2;
+    };
+    auto load = [&](int s, Cell& L) {
         const long long sa = s * a.sad + o, ss = slot + s * a.fs + o;
-        // every read of the shot's cell is issued ahead of its stores: the
-        // arrays share one allocation, so no plain read could move above a
-        // store and each would cost its own round trip. Arrays that no thread
-        // of this launch writes (the e terms of the neighbours, the stored
-        // stencil terms) are read through the read-only path, which the
-        // compiler may schedule freely.
-        const float vx = ownx ? a.avx[sa] : 0.f, svx = ownx ? __ldg(a.Svx + ss) : 0.f;
-        const float vz = ownz ? a.avz[sa] : 0.f, svz = ownz ? __ldg(a.Svz + ss) : 0.f;
-        const float p0 = dop ? a.ap[sa] : 0.f, sp = dop ? __ldg(a.Sp + ss) : 0.f;
-        const float m1 = dop && px ? a.am1[sa] : 0.f, m2 = dop && pz ? a.am2[sa] : 0.f;
+        L.vx = ownx ? a.avx[sa] : 0.f;
+        L.svx = ownx ? __ldg(a.Svx + ss) : 0.f;
+        L.vz = ownz ? a.avz[sa] : 0.f;
+        L.svz = ownz ? __ldg(a.Svz + ss) : 0.f;
+        L.p0 = dop ? a.ap[sa] : 0.f;
+        L.sp = dop ? __ldg(a.Sp + ss) : 0.f;
+        L.m1 = dop && px ? a.am1[sa] : 0.f;
+        L.m2 = dop && pz ? a.am2[sa] : 0.f;
+    };
+    Cell nx_;
+    if (PF && s0 < s1) load(s0, nx_);
+    for (int s = s0; s < s1; ++s) {
+        const long long sa = s * a.sad + o;
+        Cell c_;
+        if (PF) {
+            c_ = nx_;
+            if (s + 1 < s1) load(s + 1, nx_);
+        } else {
+            load(s, c_);
+        }
+        const float vx = c_.vx, svx = c_.svx, vz = c_.vz, svz = c_.svz, p0 = c_.p0, sp = c_.sp, m1 = c_.m1, m2 = c_.m2;
         if (ownx) gbx += vx * svx;
         if (ownz) gbz += vz * svz;
         if (!dop) continue;
@@ -354,6 +376,17 @@ __global__ void __launch_bounds__(512) k_ac2d_adj_p(Ac2dDev a) {
     if (dop) { sm = a.Gbk[go]; c = a.Cbk[go]; kahan_add(sm, c, gbk); a.Gbk[go] = sm; a.Cbk[go] = c; }
     if (ownx) { sm = a.Gbx[go]; c = a.Cbx[go]; kahan_add(sm, c, gbx); a.Gbx[go] = sm; a.Cbx[go] = c; }
     if (ownz) { sm = a.Gbz[go]; c = a.Cbz[go]; kahan_add(sm, c, gbz); a.Gbz[go] = sm; a.Cbz[go] = c; }
+}
+
+template <int R>
+__global__ void __launch_bounds__(512) k_ac2d_adj_p(Ac2dDev a) {
+    pdl_prologue();
+    ac2d_adj_p_cells<R, false>(a);
+}
+template <int R>
+__global__ void __launch_bounds__(512) k_ac2d_adj_p_pf(Ac2dDev a) {
+    pdl_prologue();
+    ac2d_adj_p_cells<R, true>(a);
 }
 
 // adjoint of the sampling of step t: the residual of step t into p^ at the
@@ -665,18 +698,24 @@ struct Ac2dEngine : SsgBase {
 
     // tile heights of the autotuner: 4, 8, 16 rows of one-cell threads (32 x
     // tz), or 100 + 2, 4, 8 rows of four-cell threads (k_ac2d_*4, 32 x tz
-    // threads covering 128 x tz cells), or 200 + 2, 4, 8: the four-cell
-    // tiles with each thread loading its next shot's cells ahead (when a CTA
-    // takes several shots)
-    std::vector<int> tune_tz(int) const override { return {4, 8, 16, 102, 104, 108, 202, 204, 208}; }
+    // threads covering 128 x tz cells); adjoint pass also 200 + 2, 4, 8 and
+    // 300 + 4, 8: the four-cell / one-cell tiles with the adjoint p kernel
+    // loading each thread's next shot ahead (when a CTA takes several shots).
+    // The same for the forward and adjoint velocity-node kernels measured
+    // slower: not built.
+    std::vector<int> tune_tz(int pass) const override {
+        if (pass == 1) return {4, 8, 16, 304, 308, 102, 104, 108, 202, 204, 208};
+        return {4, 8, 16, 102, 104, 108};
+    }
     void launch_params(const owl_run_opts& o) override {
-        const bool vec = o.tile_z >= 100;
+        const bool code = o.tile_z >= 100;
         owl_run_opts q = o;
-        if (vec) q.tile_z = o.tile_z % 100;
+        if (code) q.tile_z = o.tile_z % 100;
         SsgBase::launch_params(q);
-        if (vec) {
-            OWL_CHECK(tile_x == 32 && q.tile_z >= 1 && q.tile_z <= 8 && o.tile_z < 300, OWL_ERR_INVALID,
-                      "four-cell tiles: tile_x 32 and tile_z 100 + (1 .. 8) or 200 + (1 .. 8)");
+        if (code) {
+            OWL_CHECK(o.tile_z < 400 && (o.tile_z >= 300 || (tile_x == 32 && q.tile_z >= 1 && q.tile_z <= 8)),
+                      OWL_ERR_INVALID,
+                      "tile_z: rows, 100 + (1 .. 8) or 200 + (1 .. 8) with tile_x 32, or 300 + rows");
             tz_f = tz_a = o.tile_z;
         }
     }
@@ -684,10 +723,12 @@ struct Ac2dEngine : SsgBase {
     template <int RR>
     void launch_r(int id, int S, bool store) {
         const int tzv = (id == OWL_K_FWD_P || id == OWL_K_FWD_V) ? tz_f : tz_a;
-        if (tzv >= 100) {
+        if (tzv >= 100 && tzv < 300) {
             launch_v4<RR>(id, S, store, tzv - 100);
             return;
         }
+        // codes 300 + h: the one-cell tiles of h rows, the adjoint p kernel loading each thread's next shot ahead
+        const bool pf = tzv >= 300;
         Ac2dDev a = dev(S);
         const int rows_p = a.z1 - a.zp0, rows_v = a.z1 - std::min(a.zvx0, a.zvz0);
         const int rows_a = a.z1 - std::min(std::min(a.zvx0, a.zvz0), a.zp0);
@@ -700,9 +741,10 @@ struct Ac2dEngine : SsgBase {
         };
         if (id == OWL_K_FWD_P || id == OWL_K_FWD_V) {
             a.spt = spt_f;
-            dim3 b(tile_x, tz_f);
+            const int ty = tz_f % 100;
+            dim3 b(tile_x, ty);
             if (id == OWL_K_FWD_P) {
-                dim3 g = grid_for(rows_p, S, spt_f, tz_f);
+                dim3 g = grid_for(rows_p, S, spt_f, ty);
                 if (store) {
                     if (fz) launch_pdl(k_ac2d_fwd_p<RR, true, true>, g, b, 0, stream, a);
                     else launch_pdl(k_ac2d_fwd_p<RR, true, false>, g, b, 0, stream, a);
@@ -711,7 +753,7 @@ struct Ac2dEngine : SsgBase {
                     else launch_pdl(k_ac2d_fwd_p<RR, false, false>, g, b, 0, stream, a);
                 }
             } else {
-                dim3 g = grid_for(rows_v, S, spt_f, tz_f);
+                dim3 g = grid_for(rows_v, S, spt_f, ty);
                 if (fz && (fz_mode & FZ_SMP)) add_point_rows(g, nb_rec);
                 if (store) {
                     if (fz) launch_pdl(k_ac2d_fwd_vf<RR, true>, g, b, 0, stream, a);
@@ -723,11 +765,13 @@ struct Ac2dEngine : SsgBase {
             }
         } else {
             a.spt = spt_a;
-            dim3 b(tile_x, tz_a);
+            const int ty = tz_a % 100;
+            dim3 b(tile_x, ty);
             if (id == OWL_K_ADJ_P) {
-                launch_pdl(k_ac2d_adj_p<RR>, grid_for(rows_a, S, spt_a, tz_a), b, 0, stream, a);
+                if (pf && spt_a > 1) launch_pdl(k_ac2d_adj_p_pf<RR>, grid_for(rows_a, S, spt_a, ty), b, 0, stream, a);
+                else launch_pdl(k_ac2d_adj_p<RR>, grid_for(rows_a, S, spt_a, ty), b, 0, stream, a);
             } else {
-                dim3 g = grid_for(rows_v, S, spt_a, tz_a);
+                dim3 g = grid_for(rows_v, S, spt_a, ty);
                 if (fz && (fz_mode & FZ_SCT)) add_point_rows(g, nb_sct);
                 if (fz) launch_pdl(k_ac2d_adj_v<RR, true>, g, b, 0, stream, a);
                 else launch_pdl(k_ac2d_adj_v<RR, false>, g, b, 0, stream, a);
@@ -737,7 +781,7 @@ struct Ac2dEngine : SsgBase {
     // the four-cell kernels: 32 x ty threads over 128 x ty cells
     template <int RR>
     void launch_v4(int id, int S, bool store, int ty) {
-        // tile codes 200 + ty: the same tiles with the next shot's loads issued ahead
+        // tile codes 200 + ty: the same tiles, the adjoint p kernel loading each thread's next shot ahead
         const bool pf = ty >= 100;
         ty %= 100;
         Ac2dDev a = dev(S);
@@ -756,28 +800,22 @@ struct Ac2dEngine : SsgBase {
         if (id == OWL_K_FWD_P) {
             a.spt = spt_f;
             const dim3 g = grid(rows_p, spt_f);
-            const bool p2 = pf && !fz && spt_f > 1;
             if (store) {
                 if (fz) launch_pdl(k_ac2d_fwd_p4<RR, true, true>, g, b, 0, stream, a);
-                else if (p2) launch_pdl(k_ac2d_fwd_p4_pf<RR, true>, g, b, 0, stream, a);
                 else launch_pdl(k_ac2d_fwd_p4<RR, true, false>, g, b, 0, stream, a);
             } else {
                 if (fz) launch_pdl(k_ac2d_fwd_p4<RR, false, true>, g, b, 0, stream, a);
-                else if (p2) launch_pdl(k_ac2d_fwd_p4_pf<RR, false>, g, b, 0, stream, a);
                 else launch_pdl(k_ac2d_fwd_p4<RR, false, false>, g, b, 0, stream, a);
             }
         } else if (id == OWL_K_FWD_V) {
             a.spt = spt_f;
             dim3 g = grid(rows_v, spt_f);
             if (fz && (fz_mode & FZ_SMP)) add_point_rows(g, nb_rec);
-            const bool p2 = pf && !fz && spt_f > 1;
             if (store) {
                 if (fz) launch_pdl(k_ac2d_fwd_v4<RR, true, true>, g, b, 0, stream, a);
-                else if (p2) launch_pdl(k_ac2d_fwd_v4_pf<RR, true>, g, b, 0, stream, a);
                 else launch_pdl(k_ac2d_fwd_v4<RR, true, false>, g, b, 0, stream, a);
             } else {
                 if (fz) launch_pdl(k_ac2d_fwd_v4<RR, false, true>, g, b, 0, stream, a);
-                else if (p2) launch_pdl(k_ac2d_fwd_v4_pf<RR, false>, g, b, 0, stream, a);
                 else launch_pdl(k_ac2d_fwd_v4<RR, false, false>, g, b, 0, stream, a);
             }
         } else if (id == OWL_K_ADJ_P) {
@@ -789,7 +827,6 @@ struct Ac2dEngine : SsgBase {
             dim3 g = grid(rows_v, spt_a);
             if (fz && (fz_mode & FZ_SCT)) add_point_rows(g, nb_sct);
             if (fz) launch_pdl(k_ac2d_adj_v4<RR, true>, g, b, 0, stream, a);
-            else if (pf && spt_a > 1) launch_pdl(k_ac2d_adj_v4_pf<RR>, g, b, 0, stream, a);
             else launch_pdl(k_ac2d_adj_v4<RR, false>, g, b, 0, stream, a);
         }
     }

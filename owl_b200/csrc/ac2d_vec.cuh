@@ -52,11 +52,9 @@ __device__ __forceinline__ bool ac2d_v4(const Ac2dDev& a, int zr0, Ac2dV4& c) {
     return c.x < a.x1 && c.z < a.z1;
 }
 
-// PF: the next shot's cell values are loaded before this shot's stores (they
-// cannot alias: each shot owns its own slices), so two shots' loads are in
-// flight per thread instead of one (no fused point work)
-template <int R, bool STORE, bool FUSE, bool PF>
-__device__ __forceinline__ void ac2d_fwd_p4_cells(const Ac2dDev& a) {
+template <int R, bool STORE, bool FUSE>
+__global__ void __launch_bounds__(256) k_ac2d_fwd_p4(Ac2dDev a) {
+    pdl_prologue();
     Ac2dV4 c;
     if (!ac2d_v4(a, a.zp0, c)) return;
     const int x = c.x, z = c.z, n = c.n;
@@ -82,30 +80,13 @@ __device__ __forceinline__ void ac2d_fwd_p4_cells(const Ac2dDev& a) {
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
     const int pt = a.pitch;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-    struct Cell {
-        float4 p0, m1, m2;
-    };
-    auto load = [&](int s, Cell& L) {
-        const long long so = s * a.sst + o;
-        L.p0 = ld4(a.p + so);
-        L.m1 = anyx ? ld4(a.m1 + so) : zero;
-        L.m2 = pz ? ld4(a.m2 + so) : zero;
-    };
-    Cell nx_;
-    if (PF && s0 < s1) load(s0, nx_);
     for (int s = s0; s < s1; ++s) {
         const long long so = s * a.sst + o;
         const float* vx = a.vx + so;
         const float* vz = a.vz + so;
         // the cells' own values ahead of their stores (see k_ac2d_fwd_p)
-        Cell c_;
-        if (PF) {
-            c_ = nx_;
-            if (s + 1 < s1) load(s + 1, nx_);
-        } else {
-            load(s, c_);
-        }
-        float4 p0 = c_.p0, m1 = c_.m1, m2 = c_.m2;
+        float4 p0 = ld4(a.p + so);
+        float4 m1 = anyx ? ld4(a.m1 + so) : zero, m2 = pz ? ld4(a.m2 + so) : zero;
         if (FUSE && (a.pt.mode & FZ_INJ) && ac2d_inj_near(a.pt, s, 1, cx0, cx0 + 4 * blockDim.x, cz0, cz0 + blockDim.y)) {
 #pragma unroll
             for (int q = 0; q < 4; ++q)
@@ -151,17 +132,6 @@ __device__ __forceinline__ void ac2d_fwd_p4_cells(const Ac2dDev& a) {
 }
 
 template <int R, bool STORE, bool FUSE>
-__global__ void __launch_bounds__(256) k_ac2d_fwd_p4(Ac2dDev a) {
-    pdl_prologue();
-    ac2d_fwd_p4_cells<R, STORE, FUSE, false>(a);
-}
-template <int R, bool STORE>
-__global__ void __launch_bounds__(256) k_ac2d_fwd_p4_pf(Ac2dDev a) {
-    pdl_prologue();
-    ac2d_fwd_p4_cells<R, STORE, false, true>(a);
-}
-
-template <int R, bool STORE, bool FUSE, bool PF>
 __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
     Ac2dV4 c;
     if (!ac2d_v4(a, min(a.zvx0, a.zvz0), c)) return;
@@ -186,18 +156,6 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
     const int pt = a.pitch;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-    struct Cell {
-        float4 vx0, m3, vz0, m4;
-    };
-    auto load = [&](int s, Cell& L) {
-        const long long so = s * a.sst + o;
-        L.vx0 = dox ? ld4(a.vx + so) : zero;
-        L.m3 = dox && anyx ? ld4(a.m3 + so) : zero;
-        L.vz0 = doz ? ld4(a.vz + so) : zero;
-        L.m4 = doz && pz ? ld4(a.m4 + so) : zero;
-    };
-    Cell nx_;
-    if (PF && s0 < s1) load(s0, nx_);
     for (int s = s0; s < s1; ++s) {
         const long long so = s * a.sst + o;
         const float* p = a.p + so;
@@ -205,14 +163,8 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
         const int cx1 = cx0 + 4 * blockDim.x, cz1 = cz0 + blockDim.y;
         const bool injx = inj && ac2d_inj_near(a.pt, s, 2, cx0, cx1, cz0, cz1);
         const bool injz = inj && ac2d_inj_near(a.pt, s, 4, cx0, cx1, cz0, cz1);
-        Cell c_;
-        if (PF) {
-            c_ = nx_;
-            if (s + 1 < s1) load(s + 1, nx_);
-        } else {
-            load(s, c_);
-        }
-        float4 vx0 = c_.vx0, m3 = c_.m3, vz0 = c_.vz0, m4 = c_.m4;
+        float4 vx0 = dox ? ld4(a.vx + so) : zero, m3 = dox && anyx ? ld4(a.m3 + so) : zero;
+        float4 vz0 = doz ? ld4(a.vz + so) : zero, m4 = doz && pz ? ld4(a.m4 + so) : zero;
         if (dox) {
             float w[2 * R + 4];
             ac2d_win<R>(p, w);
@@ -273,14 +225,9 @@ __global__ void __launch_bounds__(256, FUSE ? 3 : 1) k_ac2d_fwd_v4(Ac2dDev a) {
     if (FUSE && (int)blockIdx.y >= a.pt.rows_blk) {
         if (a.pt.mode & FZ_SMP) ac2d_sample(a, cur);
     } else {
-        ac2d_fwd_v4_cells<R, STORE, FUSE, false>(a, cur);
+        ac2d_fwd_v4_cells<R, STORE, FUSE>(a, cur);
     }
     if (FUSE && (a.pt.mode & FZ_TICK)) tick_last_block(a.d_step, a.pt.d_done, 1);
-}
-template <int R, bool STORE>
-__global__ void __launch_bounds__(256) k_ac2d_fwd_v4_pf(Ac2dDev a) {
-    pdl_prologue();
-    ac2d_fwd_v4_cells<R, STORE, false, true>(a, 0);
 }
 
 // PF: the next shot's cell values are loaded before this shot's stores (they
@@ -430,9 +377,7 @@ __global__ void __launch_bounds__(256, 2) k_ac2d_adj_p4_pf(Ac2dDev a) {
     ac2d_adj_p4_cells<R, true>(a);
 }
 
-// PF: the next shot's cell values are loaded before this shot's stores (see
-// ac2d_adj_p4_cells)
-template <int R, bool PF>
+template <int R>
 __device__ __forceinline__ void ac2d_adj_v4_cells(const Ac2dDev& a) {
     Ac2dV4 c;
     if (!ac2d_v4(a, min(a.zvx0, a.zvz0), c)) return;
@@ -455,28 +400,10 @@ __device__ __forceinline__ void ac2d_adj_v4_cells(const Ac2dDev& a) {
     const int pt = a.pitch;
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-    struct Cell {
-        float4 vx, m3, vz, m4;
-    };
-    auto load = [&](int s, Cell& L) {
-        const long long sa = s * a.sad + o;
-        L.vx = dox ? ld4(a.avx + sa) : zero;
-        L.m3 = dox && anyx ? ld4(a.am3 + sa) : zero;
-        L.vz = doz ? ld4(a.avz + sa) : zero;
-        L.m4 = doz && pz ? ld4(a.am4 + sa) : zero;
-    };
-    Cell nx_;
-    if (PF && s0 < s1) load(s0, nx_);
     for (int s = s0; s < s1; ++s) {
         const long long sa = s * a.sad + o;
-        Cell c_;
-        if (PF) {
-            c_ = nx_;
-            if (s + 1 < s1) load(s + 1, nx_);
-        } else {
-            load(s, c_);
-        }
-        const float4 vx = c_.vx, m3 = c_.m3, vz = c_.vz, m4 = c_.m4;
+        const float4 vx = dox ? ld4(a.avx + sa) : zero, m3 = dox && anyx ? ld4(a.am3 + sa) : zero;
+        const float4 vz = doz ? ld4(a.avz + sa) : zero, m4 = doz && pz ? ld4(a.am4 + sa) : zero;
         if (dox) {
             float w[2 * R + 4];
             ac2d_win<R>(a.aepx + sa, w);
@@ -537,13 +464,7 @@ __global__ void __launch_bounds__(256) k_ac2d_adj_v4(Ac2dDev a) {
     if (FUSE && (int)blockIdx.y >= a.pt.rows_blk) {
         if (a.pt.mode & FZ_SCT) ac2d_scatter(a, *a.d_step);
     } else {
-        ac2d_adj_v4_cells<R, false>(a);
+        ac2d_adj_v4_cells<R>(a);
     }
     if (FUSE && (a.pt.mode & FZ_TICK)) tick_last_block(a.d_step, a.pt.d_done, -1);
-}
-// the pipelined form (no fused point work)
-template <int R>
-__global__ void __launch_bounds__(256) k_ac2d_adj_v4_pf(Ac2dDev a) {
-    pdl_prologue();
-    ac2d_adj_v4_cells<R, true>(a);
 }

@@ -1344,13 +1344,48 @@ struct El3dEngine : SsgBase {
     // PML memory traffic is not counted (it is a fraction of the shell)
     int n_store_p() const override { return 6; }
 
+    // CPML memories read and written per shot by the stress-node (q0 = 0) or
+    // velocity-node (q0 = 9) kernels: a derivative along axis a carries one
+    // where the node lies in the a-PML (per-axis CFS-PML) or anywhere in the
+    // node's PML shell (M-PML: every derivative is damped there)
+    double memory_cells(int q0) const {
+        static const int node[18][4] = {
+            {0, 0, 0, 0}, {1, 0, 0, 0}, {2, 0, 0, 0}, {1, 0, 1, 1}, {2, 0, 1, 1}, {0, 1, 0, 1}, {2, 1, 0, 1}, {0, 1, 1, 0},
+            {1, 1, 1, 0}, {0, 1, 0, 0}, {1, 1, 0, 0}, {2, 1, 0, 0}, {0, 0, 1, 0}, {1, 0, 1, 0}, {2, 0, 1, 0}, {0, 0, 0, 1},
+            {1, 0, 0, 1}, {2, 0, 0, 1}};
+        const double full[3] = {(double)NXp, (double)NYp, (double)NZp};
+        const bool fsf = desc.free_surface != 0;
+        // shell cells along an axis: P on each side, one more on the low side at half positions
+        auto out = [&](int ax, int h) { return (ax == 2 && fsf) ? (double)P : 2.0 * P + h; };
+        double n = 0;
+        for (int q = q0; q < q0 + 9; ++q) {
+            const int ax = node[q][0];
+            if (mpml) {
+                double in = 1;
+                for (int b = 0; b < 3; ++b) in *= full[b] - out(b, node[q][1 + b]);
+                n += full[0] * full[1] * full[2] - in;
+            } else {
+                double f = out(ax, node[q][1 + ax]);
+                for (int b = 0; b < 3; ++b)
+                    if (b != ax) f *= full[b];
+                n += f;
+            }
+        }
+        return n;
+    }
     double alg_bytes(int id, int S, int groups) const override {
         const double cells = (double)NXp * NYp * NZp;
         switch (id) {
-            case OWL_K_FWD_P: return S * cells * (3 * 4.0 + 6 * 8.0) + cells * 9 * 4.0;
-            case OWL_K_FWD_V: return S * cells * (6 * 4.0 + 3 * 8.0) + cells * 3 * 4.0;
-            case OWL_K_ADJ_P: return S * cells * (9 * 4.0 + 3 * 8.0 + 9 * 4.0 + 3 * 4.0) + cells * 3 * 4.0 + groups * cells * 3 * 16.0;
-            case OWL_K_ADJ_V: return S * cells * (9 * 4.0 + 6 * 8.0 + 9 * 4.0 + 6 * 4.0) + cells * 9 * 4.0 + groups * cells * 9 * 16.0;
+            case OWL_K_FWD_P:
+                return S * (cells * (3 * 4.0 + 6 * 8.0) + memory_cells(0) * 8.0) + cells * 9 * 4.0;
+            case OWL_K_FWD_V:
+                return S * (cells * (6 * 4.0 + 3 * 8.0) + memory_cells(9) * 8.0) + cells * 3 * 4.0;
+            case OWL_K_ADJ_P:
+                return S * (cells * (9 * 4.0 + 3 * 8.0 + 9 * 4.0 + 3 * 4.0) + memory_cells(9) * 8.0) + cells * 3 * 4.0 +
+                       groups * cells * 3 * 16.0;
+            case OWL_K_ADJ_V:
+                return S * (cells * (9 * 4.0 + 6 * 8.0 + 9 * 4.0 + 6 * 4.0) + memory_cells(0) * 8.0) + cells * 9 * 4.0 +
+                       groups * cells * 9 * 16.0;
         }
         return 0;
     }

@@ -35,11 +35,9 @@ def test_forward_parity_small(fs, R):
     ps = prepare(small_shots(nx, nz, dx, bool(fs)), nx, nz, dx, dt)
     ref = oracle.ac2d_forward(d, vp, rho, ps, "f32")
     s = make_solver(d, vp, rho)
-    # tile_z 100 + h: the four-cell kernels, h rows per CTA; 200 + h: the same
-    # with each thread's next shot loaded ahead
+    # tile_z 100 + h: the four-cell kernels, h rows per CTA
     for opts in (RunOpts(), RunOpts(shots_per_launch=1, use_graph=-1), RunOpts(shots_per_cta=2),
-                 RunOpts(tile_z=104), RunOpts(tile_z=108, shots_per_cta=2), RunOpts(tile_z=102, use_graph=-1),
-                 RunOpts(tile_z=204, shots_per_cta=3)):
+                 RunOpts(tile_z=104), RunOpts(tile_z=108, shots_per_cta=2), RunOpts(tile_z=102, use_graph=-1)):
         got = s.forward(ps, opts)
         assert rel(got, ref) < FWD_TOL, (opts, rel(got, ref))
     # zero-weight receiver records zeros
@@ -69,13 +67,15 @@ def test_gradient_parity_small(fs):
     mf_ref, g_ref, _ = oracle.ac2d_gradient(d, vp0, rho, ps, obs, adj_kind=0, k=37, precision="f64")
     s = make_solver(d, vp0, rho)
     # k >= nt and the memory-sized choice (-1): one segment, stored by the forward, no recompute;
-    # tile_z 200 + h: the four-cell kernels with each thread's next shot loaded ahead
+    # tile_z 200 + h / 300 + h: four-cell / one-cell tiles, the adjoint p kernel
+    # loading each thread's next shot ahead
     for opts in (RunOpts(checkpoint_interval=37), RunOpts(checkpoint_interval=50, shots_per_launch=1, use_graph=-1),
                  RunOpts(checkpoint_interval=20, shots_per_cta=3), RunOpts(checkpoint_interval=-1),
                  RunOpts(checkpoint_interval=100000, use_graph=-1), RunOpts(checkpoint_interval=37, tile_z=104),
                  RunOpts(checkpoint_interval=20, tile_z=108, shots_per_cta=2),
                  RunOpts(checkpoint_interval=37, tile_z=204, shots_per_cta=3),
-                 RunOpts(checkpoint_interval=20, tile_z=208, shots_per_cta=2, use_graph=-1)):
+                 RunOpts(checkpoint_interval=20, tile_z=208, shots_per_cta=2, use_graph=-1),
+                 RunOpts(checkpoint_interval=37, tile_z=304, shots_per_cta=3)):
         mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, opts)
         assert rel(mf, mf_ref) < 1e-4
         e = rel(g, g_ref)
