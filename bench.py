@@ -44,7 +44,8 @@ def parse():
     p.add_argument("--profile", action="store_true",
                    help="profiling target: one gradient step of --nshots shots, nothing else, no JSON line")
     p.add_argument("--tile-z", type=int, default=0,
-                   help="--profile: tile code of the kernels (0: autotuned, which adds the tuning launches)")
+                   help="--profile / --profile-el: tile code of the kernels (--profile 0: autotuned, which adds "
+                        "the tuning launches; --profile-el 0: 8)")
     p.add_argument("--spt", type=int, default=0, help="--profile: shots per CTA with --tile-z")
     p.add_argument("--no-3d", action="store_true", help="skip the 3D acoustic forward roofline block")
     p.add_argument("--no-misfits", action="store_true", help="skip the data-domain misfit block")
@@ -193,13 +194,14 @@ def elastic_solver(nshots, nt):
     return d, f, s, s.prepare(shots)
 
 
-def profile_elastic(nshots):
-    """Small elastic gradient for kernel captures: the 2D VTI model, S shots, 60 steps."""
+def profile_elastic(nshots, tile_z=8):
+    """Small elastic gradient for kernel captures: the 2D VTI model, S shots, 60
+    steps, tile code tile_z (100 + h: four-cell forward kernels)."""
     import numpy as np
     from owl_b200.solver import RunOpts
     d, f, s, ps = elastic_solver(nshots, 60)
     obs = np.zeros(s.seis_size(ps), dtype=np.float32)
-    s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=20, shots_per_cta=1, tile_z=8, use_graph=-1))
+    s.gradient(ps, obs, opts=RunOpts(checkpoint_interval=20, shots_per_cta=1, tile_z=tile_z, use_graph=-1))
     print(f"profile-el: {s.last_info.elapsed_ms:.2f} ms, {s.last_info.gpu_launches} launches")
     s.close()
 
@@ -242,8 +244,9 @@ def profile_elastic3_forward(n, ring=False):
 
 def elastic_2d_block(peak, peak_kind, ngrad=16):
     """2D elastic VTI with a free surface (301 x 601, dx 5 m, 4000 steps, Thomsen
-    parameters): forward of all 64 shots (Gcell-updates/s), gradient of `ngrad`
-    shots (s/shot), and the HBM roofline of the four stencil kernels."""
+    parameters): forward of all 64 shots (Gcell-updates/s) and the HBM roofline
+    of its two stencil kernels, gradient of `ngrad` shots (s/shot) and the
+    roofline of its two adjoint kernels."""
     import numpy as np
     from owl_b200 import _lib as L
     from owl_b200.solver import RunOpts
@@ -258,7 +261,22 @@ def elastic_2d_block(peak, peak_kind, ngrad=16):
     fms = sum(fwd) / len(fwd)
     out = {"workload": "2D elastic VTI, 301 x 601 model, dx 5 m, dt 0.5 ms, 4000 steps, PML 20, free surface, "
                        "64 shots (explosion / vertical force), 301 two-component receivers",
-           "forward_ms_64_shots": fms, "forward_gcells_per_s": cells * d.nt * 64 / (fms / 1e3) / 1e9}
+           "forward_ms_64_shots": fms, "forward_gcells_per_s": cells * d.nt * 64 / (fms / 1e3) / 1e9,
+           "kernels": {}}
+
+    def roof(kid, name, shots):
+        kms, b = s.kernel_time(kid, 20)
+        ach = b / (kms / 1e3) / 1e9
+        out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
+                                "shots_per_launch": shots, "traffic": profile_traffic(name)}
+
+    # the forward's kernels on its own 64-shot launch (autotuned: tile codes >=
+    # 100 are the four-cell kernels)
+    v4 = s.last_info.tile_z_forward >= 100
+    out["forward_tile_code"] = s.last_info.tile_z_forward
+    roof(L.OWL_K_FWD_P, "k_el2d_fwd_s4" if v4 else "k_el2d_fwd_s", 64)
+    roof(L.OWL_K_FWD_V, "k_el2d_fwd_v4" if v4 else "k_el2d_fwd_v", 64)
     from owl_b200 import configs
     sub = s.prepare(configs.config4_shots(64, d.nx, d.dx)[:ngrad])
     obs = np.zeros(s.seis_size(sub), dtype=np.float32)
@@ -272,14 +290,10 @@ def elastic_2d_block(peak, peak_kind, ngrad=16):
     out["gradient_shots"] = ngrad
     out["gradient_s_per_shot"] = sum(gms) / len(gms) / 1e3 / ngrad
     out["gradient_checkpoints"] = "fp16, per-field scale, every 50 steps"
-    out["kernels"] = {}
-    for kid, name in ((L.OWL_K_FWD_P, "k_el2d_fwd_s"), (L.OWL_K_FWD_V, "k_el2d_fwd_v"),
-                      (L.OWL_K_ADJ_P, "k_el2d_adj_v"), (L.OWL_K_ADJ_V, "k_el2d_adj_s")):
-        kms, b = s.kernel_time(kid, 20)
-        ach = b / (kms / 1e3) / 1e9
-        out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                                "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
-                                "shots_per_launch": ngrad, "traffic": profile_traffic(name)}
+    # the adjoint kernels on the gradient's 16-shot launch
+    out["gradient_tile_codes"] = {"forward": s.last_info.tile_z_forward, "adjoint": s.last_info.tile_z}
+    roof(L.OWL_K_ADJ_P, "k_el2d_adj_v", ngrad)
+    roof(L.OWL_K_ADJ_V, "k_el2d_adj_s", ngrad)
     s.close()
     return out
 
@@ -309,16 +323,19 @@ def elastic_3d_block(peak, peak_kind, nshots=4, nt=500, grad_shots=16):
     out = {"workload": f"3D elastic ORT (nine Cij), 256^3 model (296^3 padded), dt 0.8 ms, {nt} of 2500 steps, "
                        f"{nshots} of 16 vertical-force shots, 128 x 128 three-component receivers",
            "forward_ms": fms, "forward_gcells_per_s": cells * nt * nshots / (fms / 1e3) / 1e9, "kernels": {}}
-    # the autotuner's forward kernels: z-marching ring (tile_z 1) or thread per cell
+    # the autotuner's forward kernels: z-marching ring (tile_z 1) or thread per
+    # cell, timed on one shot per launch (the gradient's batch; the traffic
+    # figure is an ncu capture of that launch)
     ring = s.last_info.tile_z == 1
     out["forward_kernels"] = "z-marching ring" if ring else "thread per cell"
+    s.forward(s.prepare(shots[:1]), RunOpts(tile_z=1 if ring else 2))
     for kid, name in ((L.OWL_K_FWD_P, "k_el3d_fwd_s_ring" if ring else "k_el3d_fwd_s"),
                       (L.OWL_K_FWD_V, "k_el3d_fwd_v_ring" if ring else "k_el3d_fwd_v")):
         kms, b = s.kernel_time(kid, 10)
         ach = b / (kms / 1e3) / 1e9
         out["kernels"][name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                                 "peak_source": peak_kind, "alg_bytes_per_launch": b, "ms_per_launch": kms,
-                                "shots_per_launch": nshots, "traffic": profile_traffic(name)}
+                                "shots_per_launch": 1, "traffic": profile_traffic(name)}
     s.close()
     if grad_shots <= 0:
         return out
@@ -635,7 +652,7 @@ def main():
     if args.profile3d:
         return profile_3d(args.profile3d, args.rows)
     if args.profile_el:
-        return profile_elastic(args.profile_el)
+        return profile_elastic(args.profile_el, args.tile_z or 8)
     if args.profile_el3:
         return profile_elastic3(args.profile_el3, args.ring)
     if args.profile_el3_fwd:

@@ -30,6 +30,7 @@
 #include <cmath>
 
 #include "ssg_base.cuh"
+#include "vec4.cuh"
 
 namespace owl {
 

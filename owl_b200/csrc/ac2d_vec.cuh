@@ -15,30 +15,9 @@
 // fewer than four cells (n < 4): it stores those cells one by one.
 #pragma once
 
+// (vec4.cuh is included by ac2d.cu, outside the namespace)
 template <int R>
-__device__ __forceinline__ void ac2d_win(const float* f, float* w) {
-#pragma unroll
-    for (int q = 0; q < R / 2 + 1; ++q) {
-        const float4 t = __ldg(reinterpret_cast<const float4*>(f - R + 4 * q));
-        w[4 * q] = t.x; w[4 * q + 1] = t.y; w[4 * q + 2] = t.z; w[4 * q + 3] = t.w;
-    }
-}
-__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
-__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
-__device__ __forceinline__ float f4at(const float4& v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
-__device__ __forceinline__ void f4set(float4& v, int c, float s) {
-    if (c == 0) v.x = s; else if (c == 1) v.y = s; else if (c == 2) v.z = s; else v.w = s;
-}
-// all four cells, or the first n one by one
-__device__ __forceinline__ void st4n(float* p, const float4& v, int n) {
-    if (n == 4) {
-        *reinterpret_cast<float4*>(p) = v;
-    } else {
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-            if (c < n) p[c] = f4at(v, c);
-    }
-}
+__device__ __forceinline__ void ac2d_win(const float* f, float* w) { win4<R>(f, w); }
 
 struct Ac2dV4 {  // the thread's four cells
     int x, z, n;

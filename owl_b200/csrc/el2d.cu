@@ -35,6 +35,7 @@
 #include <complex>
 
 #include "ssg_base.cuh"
+#include "vec4.cuh"
 
 namespace owl {
 
@@ -240,6 +241,8 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
         }
     }
 }
+
+#include "el2d_vec.cuh"
 
 // ------------------------------- adjoint ------------------------------------
 // Adjoint state planes of one shot: 0..4 the fields' adjoints (sxx, szz, sxz,
@@ -924,6 +927,25 @@ struct El2dEngine : SsgBase {
         return a;
     }
 
+    // tile heights of the autotuner: 4, 8, 16 rows of one-cell threads (32 x
+    // tz); forward pass also 100 + 2, 4, 8: rows of four-cell threads
+    // (k_el2d_fwd_*4, 32 x tz threads covering 128 x tz cells)
+    std::vector<int> tune_tz(int pass) const override {
+        if (pass == 0) return {4, 8, 16, 102, 104, 108};
+        return {4, 8, 16};
+    }
+    void launch_params(const owl_run_opts& o) override {
+        const bool vec = o.tile_z >= 100;
+        owl_run_opts q = o;
+        if (vec) q.tile_z = o.tile_z - 100;
+        SsgBase::launch_params(q);
+        if (vec) {
+            OWL_CHECK(o.tile_z < 200 && tile_x == 32 && q.tile_z >= 1 && q.tile_z <= 8, OWL_ERR_INVALID,
+                      "four-cell tiles: tile_x 32 and tile_z 100 + (1 .. 8)");
+            tz_f = o.tile_z;  // the adjoint kernels take the rows with one-cell threads
+        }
+    }
+
     template <int RR>
     void launch_r(int id, int S, bool store) {
         El2dDev a = dev(S);
@@ -931,6 +953,22 @@ struct El2dEngine : SsgBase {
         if (id == OWL_K_FWD_P || id == OWL_K_FWD_V) {
             OWL_CHECK(!store || a.S, OWL_ERR_INVALID, "stencil-term buffer not allocated");
             a.spt = spt_f;
+            if (tz_f >= 100) {
+                // four-cell threads: 32 x ty threads over 128 x ty cells
+                const int ty = tz_f - 100;
+                const dim3 b(32, ty);
+                auto grid = [&](int rows) {
+                    return dim3((NXp + 127) / 128, (rows + ty - 1) / ty, (S + spt_f - 1) / spt_f);
+                };
+                if (id == OWL_K_FWD_P) {
+                    if (store) k_el2d_fwd_s4<RR, true><<<grid(rows_s), b, 0, stream>>>(a);
+                    else k_el2d_fwd_s4<RR, false><<<grid(rows_s), b, 0, stream>>>(a);
+                } else {
+                    if (store) k_el2d_fwd_v4<RR, true><<<grid(rows_v), b, 0, stream>>>(a);
+                    else k_el2d_fwd_v4<RR, false><<<grid(rows_v), b, 0, stream>>>(a);
+                }
+                return;
+            }
             const dim3 b(tile_x, tz_f);
             if (id == OWL_K_FWD_P) {
                 if (store) k_el2d_fwd_s<RR, true><<<grid_for(rows_s, S, spt_f, tz_f), b, 0, stream>>>(a);

@@ -36,7 +36,9 @@ def test_el2d_forward_parity(fs, R, aniso):
     s = make(d, f)
     ps = s.prepare(el_shots(fs) * 2)
     ref = oracle.el2d_forward(d, f, ps, "f32")
-    for opts in (RunOpts(), RunOpts(shots_per_launch=1, use_graph=-1), RunOpts(shots_per_cta=2)):
+    # tile_z 100 + h: the four-cell forward kernels, h rows per CTA
+    for opts in (RunOpts(), RunOpts(shots_per_launch=1, use_graph=-1), RunOpts(shots_per_cta=2),
+                 RunOpts(tile_z=104), RunOpts(tile_z=102, shots_per_cta=2, use_graph=-1)):
         got = s.forward(ps, opts)
         assert rel(got, ref) < FWD_TOL, (opts, rel(got, ref))
     assert abs(s.dt_stable - oracle.el2d_dt_stable(d, f)) <= 1e-6 * s.dt_stable
@@ -51,7 +53,8 @@ def test_el2d_gradient_parity(fs, aniso):
     ps = s.prepare(el_shots(fs) * 2)
     obs = oracle.el2d_forward(d, el_model(aniso, seed=2), ps, "f64").astype(np.float32)
     mref, gref, _ = oracle.el2d_gradient(d, f, ps, obs, adj_kind=L.OWL_ADJ_L2_RESIDUAL, k=7)
-    for opts in (RunOpts(checkpoint_interval=7), RunOpts(checkpoint_interval=7, shots_per_launch=1, use_graph=-1)):
+    for opts in (RunOpts(checkpoint_interval=7), RunOpts(checkpoint_interval=7, shots_per_launch=1, use_graph=-1),
+                 RunOpts(checkpoint_interval=7, tile_z=104, shots_per_cta=2)):
         misfit, g = s.gradient(ps, obs, opts=opts)
         assert rel(g, gref) < GRAD_TOL, (opts, rel(g, gref))
         assert np.allclose(misfit, mref, rtol=1e-4)
