@@ -66,8 +66,8 @@ struct E3Mp {
     const float* face[6];
     float adt;
     // (a, b) of every derivative of every node, computed once per model by
-    // k_el3d_mpml_coef: a of entry q at (2 q) fs + o, b at (2 q + 1) fs + o;
-    // q 0..8 the stress nodes' derivatives, q 9..17 the velocity nodes'
+    // k_el3d_mpml_coef: entry q's pair is float2 number q fs + o; q 0..8 the
+    // stress nodes' derivatives, q 9..17 the velocity nodes'
     const float* coef;
 };
 
@@ -183,17 +183,22 @@ __device__ __forceinline__ int e3_perm(int q) {
 // the a of the node's nine derivatives (they decide which memories update);
 // each b is loaded where its update needs it (e3_cb), to hold fewer registers
 template <int PERM>
-__device__ __forceinline__ void e3_coef_load(const El3dDev& a, long long o, int q0, float (&ca)[9]) {
-#pragma unroll
-    for (int q = 0; q < 9; ++q) ca[q] = __ldg(a.mp.coef + (2 * (q0 + e3_perm<PERM>(q))) * a.fs + o);
+__device__ __forceinline__ float2 e3_ab(const El3dDev& a, long long o, int q0, int q) {
+    return __ldg(reinterpret_cast<const float2*>(a.mp.coef) + (q0 + e3_perm<PERM>(q)) * a.fs + o);
 }
 template <int PERM>
+__device__ __forceinline__ void e3_coef_load(const El3dDev& a, long long o, int q0, float (&ca)[9]) {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) ca[q] = e3_ab<PERM>(a, o, q0, q).x;
+}
+// a and b of one entry: one 8-byte load where both are used together
+template <int PERM>
 __device__ __forceinline__ float e3_ca(const El3dDev& a, long long o, int q0, int q) {
-    return __ldg(a.mp.coef + (2 * (q0 + e3_perm<PERM>(q))) * a.fs + o);
+    return e3_ab<PERM>(a, o, q0, q).x;
 }
 template <int PERM>
 __device__ __forceinline__ float e3_cb(const El3dDev& a, long long o, int q0, int q) {
-    return __ldg(a.mp.coef + (2 * (q0 + e3_perm<PERM>(q)) + 1) * a.fs + o);
+    return e3_ab<PERM>(a, o, q0, q).y;
 }
 
 // one thread per updated cell: the (a, b) of its 18 derivatives (e3_mpml, the
@@ -208,8 +213,7 @@ __global__ void k_el3d_mpml_coef(El3dDev a, float* __restrict__ out) {
         float ca, cb;
         e3_mpml(a, c_e3_coef_node[q][0], x, y, z, c_e3_coef_node[q][1], c_e3_coef_node[q][2], c_e3_coef_node[q][3],
                 ca, cb);
-        out[(2 * q) * a.fs + o] = ca;
-        out[(2 * q + 1) * a.fs + o] = cb;
+        reinterpret_cast<float2*>(out)[q * a.fs + o] = make_float2(ca, cb);
     }
 }
 
