@@ -42,7 +42,8 @@ struct Ac2dPt {
     const int4* box;      // per item: field, x0, -, z0 (storage coordinates of its 9 x 9 box)
     const float* bw;      // per item: 81 weights [z][x]
     const float* amp;     // per item: nt amplitudes (stf * amp * dt)
-    int nt, rtot, nb, mode, rows_blk;
+    int nt, rtot, nb, mode;
+    int rows_pt;          // leading grid rows of point-work CTAs (0: none); the stencil rows follow
     int fmask;            // fields the batch's sources inject into (bit 0 p, 1 vx, 2 vz)
     const int4* bbox;     // per shot: bounding box (x0, x1, z0, z1) of its p taps, then of its vx / vz taps
     const int* rec_ptr;   // receivers (traces) of shot s: [rec_ptr[s], rec_ptr[s + 1])
@@ -75,23 +76,34 @@ struct Ac2dDev {
 
 __device__ __forceinline__ bool pml_int(int x, int pr, int n) { return x < pr || x >= pr + n; }
 __device__ __forceinline__ bool pml_half(int x, int pr, int n) { return x <= pr || x >= pr + n; }
+// this CTA's row of stencil tiles: the grid's leading rows are point-work CTAs
+// (receiver sampling, residual scatter), so that they run beside the stencil
+// CTAs instead of after them
+__device__ __forceinline__ int ac2d_row(const Ac2dDev& a) { return (int)blockIdx.y - a.pt.rows_pt; }
 
 // v + the injection of step index ti (0-based) of shot s's sources on field f
 // at storage node (x, z), items in order as add_source loops them; taps of
 // weight 0 are not taps
-__device__ __forceinline__ float ac2d_inj(const Ac2dPt& q, int s, int f, int x, int z, int ti, float v) {
-    if ((unsigned)ti >= (unsigned)q.nt) return v;
-    const int i1 = q.item_ptr[s + 1];
-    for (int it = q.item_ptr[s]; it < i1; ++it) {
-        const int4 b = q.box[it];
+// (not inlined: it runs only in the CTAs around a source, and inlined it
+// raised the registers of every CTA of the stencil kernels)
+__device__ __noinline__ float ac2d_inj_taps(const int* __restrict__ item_ptr, const int4* __restrict__ box,
+                                            const float* __restrict__ bw, const float* __restrict__ amp, int nt, int s,
+                                            int f, int x, int z, int ti, float v) {
+    if ((unsigned)ti >= (unsigned)nt) return v;
+    const int i1 = item_ptr[s + 1];
+    for (int it = item_ptr[s]; it < i1; ++it) {
+        const int4 b = box[it];
         const unsigned dx = (unsigned)(x - b.y), dz = (unsigned)(z - b.w);
         if (b.x == f && dx < (unsigned)BOX_W && dz < (unsigned)BOX_W) {
-            const float A = q.amp[(size_t)it * q.nt + ti];
-            const float w = q.bw[(size_t)it * (BOX_W * BOX_W) + dz * BOX_W + dx];
+            const float A = amp[(size_t)it * nt + ti];
+            const float w = bw[(size_t)it * (BOX_W * BOX_W) + dz * BOX_W + dx];
             if (A != 0.f && w != 0.f) v = v + A * w;
         }
     }
     return v;
+}
+__device__ __forceinline__ float ac2d_inj(const Ac2dPt& q, int s, int f, int x, int z, int ti, float v) {
+    return ac2d_inj_taps(q.item_ptr, q.box, q.bw, q.amp, q.nt, s, f, x, z, ti, v);
 }
 
 // whether shot s has a tap on p (fmask 1) or on vx / vz (fmask 2 or 4) in
@@ -134,14 +146,16 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
         // through the read-only path
         float p0 = a.p[so];
         const float m1 = px ? a.m1[so] : 0.f, m2 = pz ? a.m2[so] : 0.f;
-        // explosion sources of step t-1 (cur), added where add_source would have
-        if (FUSE && (a.pt.mode & FZ_INJ) && ac2d_inj_near(a.pt, s, 1, cx0, cx0 + blockDim.x, cz0, cz0 + blockDim.y))
-            p0 = ac2d_inj(a.pt, s, 0, x, z, cur - 1, p0);
+        // whether this CTA holds explosion taps of shot s (its load overlaps the stencil's)
+        const bool inj = FUSE && (a.pt.mode & FZ_INJ) &&
+                         ac2d_inj_near(a.pt, s, 1, cx0, cx0 + blockDim.x, cz0, cz0 + blockDim.y);
         float sx = 0.f, sz = 0.f;
 #pragma unroll
         for (int k = 1; k <= R; ++k) sx = sx + c_fd2[k - 1] * (__ldg(vx + k) - __ldg(vx + 1 - k));
 #pragma unroll
         for (int k = 1; k <= R; ++k) sz = sz + c_fd2[k - 1] * (__ldg(vz + k * pt) - __ldg(vz + (1 - k) * pt));
+        // explosion sources of step t-1 (cur), added where add_source would have
+        if (inj) p0 = ac2d_inj(a.pt, s, 0, x, z, cur - 1, p0);
         float gx = a.idx * sx, gz = a.idz * sz;
         if (px) {
             float m = ax * gx + bx * m1;
@@ -164,9 +178,9 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
 // receivers of step t+1 (cur + 2) of shot s from p and the pending explosion
 // taps of step t (cur), each trace a sequential sum over its taps (the
 // sampling of submodule_forward_modeling.f90:58-79 after add_source)
-__device__ __forceinline__ void ac2d_sample(const Ac2dDev& a, int cur) {
+__device__ __noinline__ void ac2d_sample(const Ac2dDev& a, int cur) {
     const Ac2dPt& q = a.pt;
-    const int cta = (blockIdx.y - q.rows_blk) * gridDim.x + blockIdx.x;
+    const int cta = blockIdx.y * gridDim.x + blockIdx.x;
     const int s = cta / q.nb, part = cta % q.nb, tr = cur + 2;
     if (blockIdx.z != 0 || s >= a.nshots || tr > q.nt) return;
     const int nthr = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
@@ -186,9 +200,9 @@ template <int R, bool STORE, bool FUSE>
 __device__ __forceinline__ void ac2d_fwd_v_cells(const Ac2dDev& a, int cur) {
     const int zr0 = min(a.zvx0, a.zvz0);
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
-    int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
+    int z = zr0 + ac2d_row(a) * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
-    const int cx0 = a.x0 + blockIdx.x * blockDim.x, cz0 = zr0 + blockIdx.y * blockDim.y;  // the CTA's tile
+    const int cx0 = a.x0 + blockIdx.x * blockDim.x, cz0 = zr0 + ac2d_row(a) * blockDim.y;  // the CTA's tile
     const long long o = (long long)z * a.pitch + x;
     const bool dox = z >= a.zvx0, doz = z >= a.zvz0;
     const float bxc = a.dtbx[o], bzc = a.dtbz[o];
@@ -249,14 +263,13 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_v(Ac2dDev a) {
     ac2d_fwd_v_cells<R, STORE, false>(a, 0);
 }
 
-// with the fused point work; held to 40 registers (3 CTAs of 512 per SM): at
-// 32 the injection and sampling branches spill, and without a bound the
-// sampling branch raises the count of every CTA further
+// with the fused point work; held to 64 registers (2 CTAs of 512 per SM): at
+// 40 the injection call and the sampling branch spill
 template <int R, bool STORE>
-__global__ void __launch_bounds__(512, 3) k_ac2d_fwd_vf(Ac2dDev a) {
+__global__ void __launch_bounds__(512, 2) k_ac2d_fwd_vf(const __grid_constant__ Ac2dDev a) {
     pdl_prologue();
     const int cur = *a.d_step;
-    if ((int)blockIdx.y >= a.pt.rows_blk) {
+    if ((int)blockIdx.y < a.pt.rows_pt) {
         if (a.pt.mode & FZ_SMP) ac2d_sample(a, cur);
     } else {
         ac2d_fwd_v_cells<R, STORE, true>(a, cur);
@@ -288,7 +301,7 @@ template <int R, bool PF>
 __device__ __forceinline__ void ac2d_adj_p_cells(const Ac2dDev& a) {
     const int zr0 = min(min(a.zvx0, a.zvz0), a.zp0);
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
-    int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
+    int z = zr0 + ac2d_row(a) * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
     const int t = *a.d_step;
     const long long slot = (long long)((t - 1) % a.k) * a.sslot;
@@ -393,9 +406,9 @@ __global__ void __launch_bounds__(512) k_ac2d_adj_p_pf(Ac2dDev a) {
 // adjoint of the sampling of step t: the residual of step t into p^ at the
 // receivers' tap nodes, one thread per target node, its contributions summed in
 // a fixed order (k_point_adj's scatter phase)
-__device__ __forceinline__ void ac2d_scatter(const Ac2dDev& a, int t) {
+__device__ __noinline__ void ac2d_scatter(const Ac2dDev& a, int t) {
     const Ac2dPt& q = a.pt;
-    const int cta = (blockIdx.y - q.rows_blk) * gridDim.x + blockIdx.x;
+    const int cta = blockIdx.y * gridDim.x + blockIdx.x;
     const int s = cta / q.nb, part = cta % q.nb;
     if (blockIdx.z != 0 || s >= a.nshots || t < 1) return;
     const int nthr = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
@@ -412,7 +425,7 @@ template <int R>
 __device__ __forceinline__ void ac2d_adj_v_cells(const Ac2dDev& a) {
     const int zr0 = min(a.zvx0, a.zvz0);
     int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
-    int z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
+    int z = zr0 + ac2d_row(a) * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
     const long long o = (long long)z * a.pitch + x;
     const bool dox = z >= a.zvx0, doz = z >= a.zvz0;
@@ -464,9 +477,9 @@ __device__ __forceinline__ void ac2d_adj_v_cells(const Ac2dDev& a) {
 }
 
 template <int R, bool FUSE>
-__global__ void __launch_bounds__(512) k_ac2d_adj_v(Ac2dDev a) {
+__global__ void __launch_bounds__(512) k_ac2d_adj_v(const __grid_constant__ Ac2dDev a) {
     pdl_prologue();
-    if (FUSE && (int)blockIdx.y >= a.pt.rows_blk) {
+    if (FUSE && (int)blockIdx.y < a.pt.rows_pt) {
         if (a.pt.mode & FZ_SCT) ac2d_scatter(a, *a.d_step);
     } else {
         ac2d_adj_v_cells<R>(a);
@@ -689,7 +702,7 @@ struct Ac2dEngine : SsgBase {
         }
         Ac2dPt& q = a.pt;
         q.item_ptr = inj_shot_ptr.p; q.box = inj_box.p; q.bw = inj_bw.p; q.amp = amp.p;
-        q.nt = desc.nt; q.rtot = rtot; q.nb = 1; q.mode = fz_mode; q.rows_blk = 1 << 30; q.fmask = inj_fmask;
+        q.nt = desc.nt; q.rtot = rtot; q.nb = 1; q.mode = fz_mode; q.rows_pt = 0; q.fmask = inj_fmask;
         q.bbox = inj_bbox.p;
         q.rec_ptr = rec_shot_ptr.p; q.smp = view(smp); q.rec = rec.p;
         q.sct_shot_ptr = sct_shot_ptr.p; q.sct = view(sct); q.res = res.p;
@@ -736,9 +749,9 @@ struct Ac2dEngine : SsgBase {
         const bool fz = fz_mode != 0;
         // extra CTA rows after the stencil rows for the sampling / scatter work, nb CTAs per shot
         auto add_point_rows = [&](dim3& g, int nb) {
-            a.pt.rows_blk = (int)g.y;
+            a.pt.rows_pt = (S * nb + (int)g.x - 1) / (int)g.x;
             a.pt.nb = nb;
-            g.y += (S * nb + g.x - 1) / g.x;
+            g.y += a.pt.rows_pt;
         };
         if (id == OWL_K_FWD_P || id == OWL_K_FWD_V) {
             a.spt = spt_f;
@@ -793,9 +806,9 @@ struct Ac2dEngine : SsgBase {
             return dim3((NXp + 127) / 128, (rows + ty - 1) / ty, (S + spt - 1) / spt);
         };
         auto add_point_rows = [&](dim3& g, int nb) {
-            a.pt.rows_blk = (int)g.y;
+            a.pt.rows_pt = (S * nb + (int)g.x - 1) / (int)g.x;
             a.pt.nb = nb;
-            g.y += (S * nb + g.x - 1) / g.x;
+            g.y += a.pt.rows_pt;
         };
         const dim3 b(32, ty);
         if (id == OWL_K_FWD_P) {

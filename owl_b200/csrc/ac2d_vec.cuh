@@ -25,7 +25,7 @@ struct Ac2dV4 {  // the thread's four cells
 };
 __device__ __forceinline__ bool ac2d_v4(const Ac2dDev& a, int zr0, Ac2dV4& c) {
     c.x = a.x0 + 4 * (blockIdx.x * blockDim.x + threadIdx.x);
-    c.z = zr0 + blockIdx.y * blockDim.y + threadIdx.y;
+    c.z = zr0 + ac2d_row(a) * blockDim.y + threadIdx.y;
     c.n = min(4, a.x1 - c.x);
     c.o = (long long)c.z * a.pitch + c.x;
     return c.x < a.x1 && c.z < a.z1;
@@ -66,11 +66,9 @@ __global__ void __launch_bounds__(256) k_ac2d_fwd_p4(Ac2dDev a) {
         // the cells' own values ahead of their stores (see k_ac2d_fwd_p)
         float4 p0 = ld4(a.p + so);
         float4 m1 = anyx ? ld4(a.m1 + so) : zero, m2 = pz ? ld4(a.m2 + so) : zero;
-        if (FUSE && (a.pt.mode & FZ_INJ) && ac2d_inj_near(a.pt, s, 1, cx0, cx0 + 4 * blockDim.x, cz0, cz0 + blockDim.y)) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (q < n) f4set(p0, q, ac2d_inj(a.pt, s, 0, x + q, z, cur - 1, f4at(p0, q)));
-        }
+        // whether this CTA holds explosion taps of shot s (its load overlaps the stencil's)
+        const bool inj = FUSE && (a.pt.mode & FZ_INJ) &&
+                         ac2d_inj_near(a.pt, s, 1, cx0, cx0 + 4 * blockDim.x, cz0, cz0 + blockDim.y);
         float w[2 * R + 4];
         ac2d_win<R>(vx, w);
         float sx[4] = {0.f, 0.f, 0.f, 0.f}, sz[4] = {0.f, 0.f, 0.f, 0.f};
@@ -83,6 +81,12 @@ __global__ void __launch_bounds__(256) k_ac2d_fwd_p4(Ac2dDev a) {
             const float4 up = ldg4(vz + k * pt), dn = ldg4(vz + (1 - k) * pt);
 #pragma unroll
             for (int q = 0; q < 4; ++q) sz[q] = sz[q] + c_fd2[k - 1] * (f4at(up, q) - f4at(dn, q));
+        }
+        // explosion sources of step t-1 (cur), added where add_source would have
+        if (inj) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (q < n) f4set(p0, q, ac2d_inj(a.pt, s, 0, x + q, z, cur - 1, f4at(p0, q)));
         }
         float4 pn = p0, gS = zero;
 #pragma unroll
@@ -116,7 +120,7 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
     if (!ac2d_v4(a, min(a.zvx0, a.zvz0), c)) return;
     const int x = c.x, z = c.z, n = c.n;
     const long long o = c.o;
-    const int cx0 = a.x0 + 4 * blockIdx.x * blockDim.x, cz0 = min(a.zvx0, a.zvz0) + blockIdx.y * blockDim.y;
+    const int cx0 = a.x0 + 4 * blockIdx.x * blockDim.x, cz0 = min(a.zvx0, a.zvz0) + ac2d_row(a) * blockDim.y;
     const bool dox = z >= a.zvx0, doz = z >= a.zvz0;
     const float4 bxc = ldg4(a.dtbx + o), bzc = ldg4(a.dtbz + o);
     bool px[4];
@@ -159,14 +163,19 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
                     f4set(m3, q, m);
                     h = h + m;
                 }
-                float v = f4at(vx0, q) - f4at(bxc, q) * h;
-                if (FUSE && injx && q < n) v = ac2d_inj(a.pt, s, 1, x + q, z, cur, v);
-                f4set(vn, q, v);
+                f4set(vn, q, f4at(vx0, q) - f4at(bxc, q) * h);
                 f4set(hS, q, h);
             }
-            st4n(a.vx + so, vn, n);
             if (anyx) st4n(a.m3 + so, m3, n);
             if (STORE) st4n(a.Svx + slot + s * a.fs + o, hS, n);
+            // force sources of step t, added to the updated cells (out of the
+            // loop above, so that the calls hold no stencil values live)
+            if (FUSE && injx) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (q < n) f4set(vn, q, ac2d_inj(a.pt, s, 1, x + q, z, cur, f4at(vn, q)));
+            }
+            st4n(a.vx + so, vn, n);
         }
         if (doz) {
             float sz[4] = {0.f, 0.f, 0.f, 0.f};
@@ -185,23 +194,26 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
                     f4set(m4, q, m);
                     h = h + m;
                 }
-                float v = f4at(vz0, q) - f4at(bzc, q) * h;
-                if (FUSE && injz && q < n) v = ac2d_inj(a.pt, s, 2, x + q, z, cur, v);
-                f4set(vn, q, v);
+                f4set(vn, q, f4at(vz0, q) - f4at(bzc, q) * h);
                 f4set(hS, q, h);
             }
-            st4n(a.vz + so, vn, n);
             if (pz) st4n(a.m4 + so, m4, n);
             if (STORE) st4n(a.Svz + slot + s * a.fs + o, hS, n);
+            if (FUSE && injz) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (q < n) f4set(vn, q, ac2d_inj(a.pt, s, 2, x + q, z, cur, f4at(vn, q)));
+            }
+            st4n(a.vz + so, vn, n);
         }
     }
 }
 
 template <int R, bool STORE, bool FUSE>
-__global__ void __launch_bounds__(256, FUSE ? 3 : 1) k_ac2d_fwd_v4(Ac2dDev a) {
+__global__ void __launch_bounds__(256) k_ac2d_fwd_v4(const __grid_constant__ Ac2dDev a) {
     pdl_prologue();
     const int cur = FUSE ? *a.d_step : 0;
-    if (FUSE && (int)blockIdx.y >= a.pt.rows_blk) {
+    if (FUSE && (int)blockIdx.y < a.pt.rows_pt) {
         if (a.pt.mode & FZ_SMP) ac2d_sample(a, cur);
     } else {
         ac2d_fwd_v4_cells<R, STORE, FUSE>(a, cur);
@@ -438,9 +450,9 @@ __device__ __forceinline__ void ac2d_adj_v4_cells(const Ac2dDev& a) {
 }
 
 template <int R, bool FUSE>
-__global__ void __launch_bounds__(256) k_ac2d_adj_v4(Ac2dDev a) {
+__global__ void __launch_bounds__(256) k_ac2d_adj_v4(const __grid_constant__ Ac2dDev a) {
     pdl_prologue();
-    if (FUSE && (int)blockIdx.y >= a.pt.rows_blk) {
+    if (FUSE && (int)blockIdx.y < a.pt.rows_pt) {
         if (a.pt.mode & FZ_SCT) ac2d_scatter(a, *a.d_step);
     } else {
         ac2d_adj_v4_cells<R>(a);
