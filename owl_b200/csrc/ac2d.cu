@@ -105,6 +105,33 @@ __device__ __noinline__ float ac2d_inj_taps(const int* __restrict__ item_ptr, co
 __device__ __forceinline__ float ac2d_inj(const Ac2dPt& q, int s, int f, int x, int z, int ti, float v) {
     return ac2d_inj_taps(q.item_ptr, q.box, q.bw, q.amp, q.nt, s, f, x, z, ti, v);
 }
+// the same for the four cells x .. x + 3 (the first n) of one row: one pass
+// over the shot's items, each cell's taps added in item order as above
+__device__ __noinline__ float4 ac2d_inj4_taps(const int* __restrict__ item_ptr, const int4* __restrict__ box,
+                                              const float* __restrict__ bw, const float* __restrict__ amp, int nt,
+                                              int s, int f, int x, int z, int ti, float4 v, int n) {
+    if ((unsigned)ti >= (unsigned)nt) return v;
+    float r[4] = {v.x, v.y, v.z, v.w};
+    const int i1 = item_ptr[s + 1];
+    for (int it = item_ptr[s]; it < i1; ++it) {
+        const int4 b = box[it];
+        const unsigned dz = (unsigned)(z - b.w);
+        if (b.x != f || dz >= (unsigned)BOX_W) continue;
+        const float A = amp[(size_t)it * nt + ti];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const unsigned dx = (unsigned)(x + q - b.y);
+            if (q < n && dx < (unsigned)BOX_W) {
+                const float w = bw[(size_t)it * (BOX_W * BOX_W) + dz * BOX_W + dx];
+                if (A != 0.f && w != 0.f) r[q] = r[q] + A * w;
+            }
+        }
+    }
+    return make_float4(r[0], r[1], r[2], r[3]);
+}
+__device__ __forceinline__ float4 ac2d_inj4(const Ac2dPt& q, int s, int f, int x, int z, int ti, float4 v, int n) {
+    return ac2d_inj4_taps(q.item_ptr, q.box, q.bw, q.amp, q.nt, s, f, x, z, ti, v, n);
+}
 
 // whether shot s has a tap on p (fmask 1) or on vx / vz (fmask 2 or 4) in
 // columns [x0, x1) x rows [z0, z1) (storage): one read-only load of the shot's
@@ -263,16 +290,17 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_v(Ac2dDev a) {
     ac2d_fwd_v_cells<R, STORE, false>(a, 0);
 }
 
-// with the fused point work; held to 64 registers (2 CTAs of 512 per SM): at
-// 40 the injection call and the sampling branch spill
-template <int R, bool STORE>
+// with the fused point work (VINJ: the batch has force sources, injected by
+// the velocity kernel); held to 64 registers (2 CTAs of 512 per SM): at 40
+// the injection call and the sampling branch spill
+template <int R, bool STORE, bool VINJ>
 __global__ void __launch_bounds__(512, 2) k_ac2d_fwd_vf(const __grid_constant__ Ac2dDev a) {
     pdl_prologue();
     const int cur = *a.d_step;
     if ((int)blockIdx.y < a.pt.rows_pt) {
         if (a.pt.mode & FZ_SMP) ac2d_sample(a, cur);
     } else {
-        ac2d_fwd_v_cells<R, STORE, true>(a, cur);
+        ac2d_fwd_v_cells<R, STORE, VINJ>(a, cur);
     }
     if (a.pt.mode & FZ_TICK) tick_last_block(a.d_step, a.pt.d_done, 1);
 }
@@ -769,11 +797,14 @@ struct Ac2dEngine : SsgBase {
             } else {
                 dim3 g = grid_for(rows_v, S, spt_f, ty);
                 if (fz && (fz_mode & FZ_SMP)) add_point_rows(g, nb_rec);
+                const bool vinj = (inj_fmask & 6) != 0;
                 if (store) {
-                    if (fz) launch_pdl(k_ac2d_fwd_vf<RR, true>, g, b, 0, stream, a);
+                    if (fz) launch_pdl(vinj ? k_ac2d_fwd_vf<RR, true, true> : k_ac2d_fwd_vf<RR, true, false>, g, b, 0,
+                                       stream, a);
                     else launch_pdl(k_ac2d_fwd_v<RR, true>, g, b, 0, stream, a);
                 } else {
-                    if (fz) launch_pdl(k_ac2d_fwd_vf<RR, false>, g, b, 0, stream, a);
+                    if (fz) launch_pdl(vinj ? k_ac2d_fwd_vf<RR, false, true> : k_ac2d_fwd_vf<RR, false, false>, g, b, 0,
+                                       stream, a);
                     else launch_pdl(k_ac2d_fwd_v<RR, false>, g, b, 0, stream, a);
                 }
             }
@@ -825,12 +856,15 @@ struct Ac2dEngine : SsgBase {
             a.spt = spt_f;
             dim3 g = grid(rows_v, spt_f);
             if (fz && (fz_mode & FZ_SMP)) add_point_rows(g, nb_rec);
+            const bool vinj = (inj_fmask & 6) != 0;
             if (store) {
-                if (fz) launch_pdl(k_ac2d_fwd_v4<RR, true, true>, g, b, 0, stream, a);
-                else launch_pdl(k_ac2d_fwd_v4<RR, true, false>, g, b, 0, stream, a);
+                if (fz) launch_pdl(vinj ? k_ac2d_fwd_v4<RR, true, true, true> : k_ac2d_fwd_v4<RR, true, true, false>, g, b,
+                                   0, stream, a);
+                else launch_pdl(k_ac2d_fwd_v4<RR, true, false, false>, g, b, 0, stream, a);
             } else {
-                if (fz) launch_pdl(k_ac2d_fwd_v4<RR, false, true>, g, b, 0, stream, a);
-                else launch_pdl(k_ac2d_fwd_v4<RR, false, false>, g, b, 0, stream, a);
+                if (fz) launch_pdl(vinj ? k_ac2d_fwd_v4<RR, false, true, true> : k_ac2d_fwd_v4<RR, false, true, false>, g,
+                                   b, 0, stream, a);
+                else launch_pdl(k_ac2d_fwd_v4<RR, false, false, false>, g, b, 0, stream, a);
             }
         } else if (id == OWL_K_ADJ_P) {
             a.spt = spt_a;

@@ -83,11 +83,7 @@ __global__ void __launch_bounds__(256) k_ac2d_fwd_p4(Ac2dDev a) {
             for (int q = 0; q < 4; ++q) sz[q] = sz[q] + c_fd2[k - 1] * (f4at(up, q) - f4at(dn, q));
         }
         // explosion sources of step t-1 (cur), added where add_source would have
-        if (inj) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (q < n) f4set(p0, q, ac2d_inj(a.pt, s, 0, x + q, z, cur - 1, f4at(p0, q)));
-        }
+        if (inj) p0 = ac2d_inj4(a.pt, s, 0, x, z, cur - 1, p0, n);
         float4 pn = p0, gS = zero;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -170,11 +166,7 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
             if (STORE) st4n(a.Svx + slot + s * a.fs + o, hS, n);
             // force sources of step t, added to the updated cells (out of the
             // loop above, so that the calls hold no stencil values live)
-            if (FUSE && injx) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    if (q < n) f4set(vn, q, ac2d_inj(a.pt, s, 1, x + q, z, cur, f4at(vn, q)));
-            }
+            if (FUSE && injx) vn = ac2d_inj4(a.pt, s, 1, x, z, cur, vn, n);
             st4n(a.vx + so, vn, n);
         }
         if (doz) {
@@ -199,24 +191,21 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
             }
             if (pz) st4n(a.m4 + so, m4, n);
             if (STORE) st4n(a.Svz + slot + s * a.fs + o, hS, n);
-            if (FUSE && injz) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    if (q < n) f4set(vn, q, ac2d_inj(a.pt, s, 2, x + q, z, cur, f4at(vn, q)));
-            }
+            if (FUSE && injz) vn = ac2d_inj4(a.pt, s, 2, x, z, cur, vn, n);
             st4n(a.vz + so, vn, n);
         }
     }
 }
 
-template <int R, bool STORE, bool FUSE>
+// FUSE: the sampling CTAs; VINJ: also the force sources of the batch
+template <int R, bool STORE, bool FUSE, bool VINJ>
 __global__ void __launch_bounds__(256) k_ac2d_fwd_v4(const __grid_constant__ Ac2dDev a) {
     pdl_prologue();
     const int cur = FUSE ? *a.d_step : 0;
     if (FUSE && (int)blockIdx.y < a.pt.rows_pt) {
         if (a.pt.mode & FZ_SMP) ac2d_sample(a, cur);
     } else {
-        ac2d_fwd_v4_cells<R, STORE, FUSE>(a, cur);
+        ac2d_fwd_v4_cells<R, STORE, VINJ>(a, cur);
     }
     if (FUSE && (a.pt.mode & FZ_TICK)) tick_last_block(a.d_step, a.pt.d_done, 1);
 }

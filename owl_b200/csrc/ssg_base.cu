@@ -384,11 +384,10 @@ void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
     if (hbox.empty()) { hbox.push_back(int4{-1, 0, 0, 0}); hbw.resize(boxn, 0.f); }
     inj_box.upload(hbox.data(), hbox.size(), stream);
     inj_bw.upload(hbw.data(), hbw.size(), stream);
-    // measured slower than the separate point kernel on the 2D workloads (the
-    // extra branches and registers cost the stencil kernels more than the
-    // launch they save): opt-in with OWL_FUSE=1
+    // the point work inside the stencil kernels where the medium supports it;
+    // OWL_FUSE=0 keeps the separate point kernel
     const char* fz = std::getenv("OWL_FUSE");
-    fuse_on = fuse && fz && fz[0] == '1' && fz[1] == 0;
+    fuse_on = fuse && !(fz && fz[0] == '0' && fz[1] == 0);
 }
 
 void SsgBase::ensure_state(int S, int k, bool grad) {

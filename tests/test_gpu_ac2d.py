@@ -170,8 +170,7 @@ def test_unstable_dt_rejected():
 @pytest.mark.parametrize("fs", [0, 1])
 def test_fused_point_work_matches_point_kernels(fs, tz):
     """Injection, sampling and the residual scatter inside the stencil kernels
-    give the seismograms, misfits and gradients of the separate point kernel
-    (the default; OWL_FUSE=1 fuses) to the bit: explosion and force sources, two overlapping
+    (OWL_FUSE=0) to the bit: explosion and force sources, two overlapping
     sources in one shot, off-grid receivers sharing taps, a zero-weight trace."""
     import os
     nx, nz, dx, dt, nt = 48, 40, 10.0, 1e-3, 300
@@ -182,8 +181,8 @@ def test_fused_point_work_matches_point_kernels(fs, tz):
     s = make_solver(d, vp * np.float32(1.02), rho)
     out = {}
     for off in (False, True):
-        if not off:
-            os.environ["OWL_FUSE"] = "1"
+        if off:
+            os.environ["OWL_FUSE"] = "0"
         try:
             seis = s.forward(ps, RunOpts(tile_z=tz))
             mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=40, tile_z=tz))

@@ -43,6 +43,6 @@ def test_misfit_matches_forward_and_gradient():
     mg, _ = s.gradient(ps, obs, opts=RunOpts(tile_z=8))
     assert np.allclose(mg, m, rtol=1e-9)
     # the autotuned forward and gradient of one batch size share the forward kernels
-    ma, _ = s.misfit(ps, obs)
+    ma = s.misfit(ps, obs)
     mga, _ = s.gradient(ps, obs)
     assert np.allclose(mga, ma, rtol=1e-9)
