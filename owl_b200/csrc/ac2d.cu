@@ -27,6 +27,7 @@
 // to the bit. A batch whose taps fall outside the nodes a kernel updates keeps
 // the separate point kernel of ssg_base.cu (three launches per step).
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 
 #include "ssg_base.cuh"
@@ -205,11 +206,10 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
 // receivers of step t+1 (cur + 2) of shot s from p and the pending explosion
 // taps of step t (cur), each trace a sequential sum over its taps (the
 // sampling of submodule_forward_modeling.f90:58-79 after add_source)
-__device__ __noinline__ void ac2d_sample(const Ac2dDev& a, int cur) {
+__device__ __noinline__ void ac2d_sample_cta(const Ac2dDev& a, int cta, int cur) {
     const Ac2dPt& q = a.pt;
-    const int cta = blockIdx.y * gridDim.x + blockIdx.x;
     const int s = cta / q.nb, part = cta % q.nb, tr = cur + 2;
-    if (blockIdx.z != 0 || s >= a.nshots || tr > q.nt) return;
+    if (s >= a.nshots || tr > q.nt) return;
     const int nthr = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
     const float* p = a.p + s * a.sst;
     for (int r = q.rec_ptr[s] + part * nthr + tid; r < q.rec_ptr[s + 1]; r += q.nb * nthr) {
@@ -221,6 +221,10 @@ __device__ __noinline__ void ac2d_sample(const Ac2dDev& a, int cur) {
         }
         q.rec[(size_t)(tr - 1) * q.rtot + r] = acc;
     }
+}
+// the launch's sampling CTAs: the leading grid rows of shot group 0
+__device__ __forceinline__ void ac2d_sample(const Ac2dDev& a, int cur) {
+    if (blockIdx.z == 0) ac2d_sample_cta(a, blockIdx.y * gridDim.x + blockIdx.x, cur);
 }
 
 template <int R, bool STORE, bool FUSE>
@@ -881,6 +885,55 @@ struct Ac2dEngine : SsgBase {
     void launch_kernel(int id, int S, bool store) override {
         if (R == 4) launch_r<4>(id, S, store);
         else launch_r<8>(id, S, store);
+    }
+
+    // persistent forward segments (OWL_PERSIST=1): one cooperative launch per
+    // segment of the four-cell forward with the fused point work
+    DevBuf<unsigned> pbar;  // the grid barrier's arrival count and generation
+    int num_sms = 0;
+    bool run_steps_persistent(int kind, int n, int S) override {
+        const char* e = std::getenv("OWL_PERSIST");
+        if (!(e && e[0] == '1' && e[1] == 0) || kind == 2 || !fuse_on || tz_f < 100 || tz_f >= 200) return false;
+        if (R == 4) return persist_r<4>(kind, n, S);
+        return persist_r<8>(kind, n, S);
+    }
+    template <int RR>
+    bool persist_r(int kind, int n, int S) {
+        Ac2dDev a = dev(S);
+        a.spt = spt_f;
+        a.pt.mode = FZ_INJ | (kind == 1 ? 0 : FZ_SMP);
+        a.pt.rows_pt = 0;
+        a.pt.nb = nb_rec;
+        const int ty = tz_f - 100;
+        Ac2dPersist p{};
+        p.n = n;
+        p.gx = (NXp + 127) / 128;
+        p.gy_p = (a.z1 - a.zp0 + ty - 1) / ty;
+        p.gy_v = (a.z1 - std::min(a.zvx0, a.zvz0) + ty - 1) / ty;
+        p.gz = (S + spt_f - 1) / spt_f;
+        p.nsmp = kind == 1 ? 0 : S * nb_rec;
+        if (!pbar.p) pbar.reserve(2);
+        OWL_CUDA(cudaMemsetAsync(pbar.p, 0, 2 * sizeof(unsigned), stream));
+        p.bar = pbar.p;
+        p.err = ctr.p + 3;
+        const bool store = kind == 1 || kind == 3, vinj = (inj_fmask & 6) != 0;
+        void (*k)(Ac2dDev, Ac2dPersist) =
+            store ? (vinj ? k_ac2d_fwd_persist<RR, true, true> : k_ac2d_fwd_persist<RR, true, false>)
+                  : (vinj ? k_ac2d_fwd_persist<RR, false, true> : k_ac2d_fwd_persist<RR, false, false>);
+        if (!num_sms) {
+            int d = 0;
+            OWL_CUDA(cudaGetDevice(&d));
+            OWL_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, d));
+        }
+        int per_sm = 0;
+        OWL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * ty, 0));
+        const int np = p.gx * p.gy_p * p.gz, nv = p.nsmp + p.gx * p.gy_v * p.gz;
+        // every block resident at once (the cooperative launch checks it)
+        const int nblocks = std::max(1, std::min(per_sm * num_sms, std::max(np, nv)));
+        void* args[] = {&a, &p};
+        OWL_CUDA(cudaLaunchCooperativeKernel((void*)k, dim3(nblocks), dim3(32, ty), args, 0, stream));
+        launches += 1;
+        return true;
     }
 
     // compulsory bytes of one launch (each state field read / written once per

@@ -18,28 +18,49 @@
 // (vec4.cuh is included by ac2d.cu, outside the namespace)
 template <int R>
 __device__ __forceinline__ void ac2d_win(const float* f, float* w) { win4<R>(f, w); }
+// COH: plain (coherent) loads, for fields that the same launch writes (the
+// persistent segment kernel); otherwise the read-only path
+template <int R, bool COH>
+__device__ __forceinline__ void ac2d_winc(const float* f, float* w) {
+    if (!COH) {
+        win4<R>(f, w);
+        return;
+    }
+#pragma unroll
+    for (int q = 0; q < R / 2 + 1; ++q) {
+        const float4 t = ld4(f - R + 4 * q);
+        w[4 * q] = t.x; w[4 * q + 1] = t.y; w[4 * q + 2] = t.z; w[4 * q + 3] = t.w;
+    }
+}
+template <bool COH>
+__device__ __forceinline__ float4 ldc4(const float* p) { return COH ? ld4(p) : ldg4(p); }
 
 struct Ac2dV4 {  // the thread's four cells
     int x, z, n;
     long long o;
 };
-__device__ __forceinline__ bool ac2d_v4(const Ac2dDev& a, int zr0, Ac2dV4& c) {
-    c.x = a.x0 + 4 * (blockIdx.x * blockDim.x + threadIdx.x);
-    c.z = zr0 + ac2d_row(a) * blockDim.y + threadIdx.y;
+// the thread's cells in tile (b.x, b.y) of 32 x blockDim.y four-cell threads
+__device__ __forceinline__ bool ac2d_v4t(const Ac2dDev& a, int zr0, uint3 b, Ac2dV4& c) {
+    c.x = a.x0 + 4 * (b.x * blockDim.x + threadIdx.x);
+    c.z = zr0 + b.y * blockDim.y + threadIdx.y;
     c.n = min(4, a.x1 - c.x);
     c.o = (long long)c.z * a.pitch + c.x;
     return c.x < a.x1 && c.z < a.z1;
 }
+// the launch's own tile: blockIdx, past the leading point-work rows
+__device__ __forceinline__ uint3 ac2d_tile(const Ac2dDev& a) {
+    return make_uint3(blockIdx.x, (unsigned)ac2d_row(a), blockIdx.z);
+}
+__device__ __forceinline__ bool ac2d_v4(const Ac2dDev& a, int zr0, Ac2dV4& c) { return ac2d_v4t(a, zr0, ac2d_tile(a), c); }
 
-template <int R, bool STORE, bool FUSE>
-__global__ void __launch_bounds__(256) k_ac2d_fwd_p4(Ac2dDev a) {
-    pdl_prologue();
+// tile b of the pressure update of step cur (the device step counter's value)
+template <int R, bool STORE, bool FUSE, bool COH = false>
+__device__ __forceinline__ void ac2d_fwd_p4_tile(const Ac2dDev& a, uint3 b, int cur) {
     Ac2dV4 c;
-    if (!ac2d_v4(a, a.zp0, c)) return;
+    if (!ac2d_v4t(a, a.zp0, b, c)) return;
     const int x = c.x, z = c.z, n = c.n;
     const long long o = c.o;
-    const int cur = FUSE ? *a.d_step : 0;
-    const int cx0 = a.x0 + 4 * blockIdx.x * blockDim.x, cz0 = a.zp0 + blockIdx.y * blockDim.y;  // the CTA's tile
+    const int cx0 = a.x0 + 4 * b.x * blockDim.x, cz0 = a.zp0 + b.y * blockDim.y;  // the tile's cells
     const float4 dtbk = ldg4(a.dtbk + o);
     bool px[4];
     float ax[4], bx[4];
@@ -55,8 +76,8 @@ __global__ void __launch_bounds__(256) k_ac2d_fwd_p4(Ac2dDev a) {
     const float az = pz ? a.azi[z] : 0.f, bz = pz ? a.bzi[z] : 0.f;
     const bool mirror = a.fsurf && z <= a.pr + a.P;
     const long long omir = (long long)(2 * a.pr - z) * a.pitch + x;
-    const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
-    const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
+    const int s0 = b.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
+    const long long slot = STORE ? (long long)(cur % a.k) * a.sslot : 0;
     const int pt = a.pitch;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int s = s0; s < s1; ++s) {
@@ -70,7 +91,7 @@ __global__ void __launch_bounds__(256) k_ac2d_fwd_p4(Ac2dDev a) {
         const bool inj = FUSE && (a.pt.mode & FZ_INJ) &&
                          ac2d_inj_near(a.pt, s, 1, cx0, cx0 + 4 * blockDim.x, cz0, cz0 + blockDim.y);
         float w[2 * R + 4];
-        ac2d_win<R>(vx, w);
+        ac2d_winc<R, COH>(vx, w);
         float sx[4] = {0.f, 0.f, 0.f, 0.f}, sz[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int q = 0; q < 4; ++q)
@@ -78,7 +99,7 @@ __global__ void __launch_bounds__(256) k_ac2d_fwd_p4(Ac2dDev a) {
             for (int k = 1; k <= R; ++k) sx[q] = sx[q] + c_fd2[k - 1] * (w[R + q + k] - w[R + q + 1 - k]);
 #pragma unroll
         for (int k = 1; k <= R; ++k) {
-            const float4 up = ldg4(vz + k * pt), dn = ldg4(vz + (1 - k) * pt);
+            const float4 up = ldc4<COH>(vz + k * pt), dn = ldc4<COH>(vz + (1 - k) * pt);
 #pragma unroll
             for (int q = 0; q < 4; ++q) sz[q] = sz[q] + c_fd2[k - 1] * (f4at(up, q) - f4at(dn, q));
         }
@@ -111,12 +132,19 @@ __global__ void __launch_bounds__(256) k_ac2d_fwd_p4(Ac2dDev a) {
 }
 
 template <int R, bool STORE, bool FUSE>
-__device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
+__global__ void __launch_bounds__(256) k_ac2d_fwd_p4(Ac2dDev a) {
+    pdl_prologue();
+    ac2d_fwd_p4_tile<R, STORE, FUSE>(a, ac2d_tile(a), (FUSE || STORE) ? *a.d_step : 0);
+}
+
+// tile b of the velocity update of step cur
+template <int R, bool STORE, bool FUSE, bool COH = false>
+__device__ __forceinline__ void ac2d_fwd_v4_tile(const Ac2dDev& a, uint3 b, int cur) {
     Ac2dV4 c;
-    if (!ac2d_v4(a, min(a.zvx0, a.zvz0), c)) return;
+    if (!ac2d_v4t(a, min(a.zvx0, a.zvz0), b, c)) return;
     const int x = c.x, z = c.z, n = c.n;
     const long long o = c.o;
-    const int cx0 = a.x0 + 4 * blockIdx.x * blockDim.x, cz0 = min(a.zvx0, a.zvz0) + ac2d_row(a) * blockDim.y;
+    const int cx0 = a.x0 + 4 * b.x * blockDim.x, cz0 = min(a.zvx0, a.zvz0) + b.y * blockDim.y;
     const bool dox = z >= a.zvx0, doz = z >= a.zvz0;
     const float4 bxc = ldg4(a.dtbx + o), bzc = ldg4(a.dtbz + o);
     bool px[4];
@@ -131,8 +159,8 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
     }
     const bool pz = (!a.fsurf && z <= a.pr) || z >= a.pr + a.nz;
     const float az = pz ? a.azh[z] : 0.f, bz = pz ? a.bzh[z] : 0.f;
-    const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
-    const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
+    const int s0 = b.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
+    const long long slot = STORE ? (long long)(cur % a.k) * a.sslot : 0;
     const int pt = a.pitch;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int s = s0; s < s1; ++s) {
@@ -146,7 +174,7 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
         float4 vz0 = doz ? ld4(a.vz + so) : zero, m4 = doz && pz ? ld4(a.m4 + so) : zero;
         if (dox) {
             float w[2 * R + 4];
-            ac2d_win<R>(p, w);
+            ac2d_winc<R, COH>(p, w);
             float4 vn = vx0, hS = zero;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
@@ -173,7 +201,7 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
             float sz[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
             for (int k = 1; k <= R; ++k) {
-                const float4 up = ldg4(p + (k - 1) * pt), dn = ldg4(p - k * pt);
+                const float4 up = ldc4<COH>(p + (k - 1) * pt), dn = ldc4<COH>(p - k * pt);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) sz[q] = sz[q] + c_fd2[k - 1] * (f4at(up, q) - f4at(dn, q));
             }
@@ -201,11 +229,11 @@ __device__ __forceinline__ void ac2d_fwd_v4_cells(const Ac2dDev& a, int cur) {
 template <int R, bool STORE, bool FUSE, bool VINJ>
 __global__ void __launch_bounds__(256) k_ac2d_fwd_v4(const __grid_constant__ Ac2dDev a) {
     pdl_prologue();
-    const int cur = FUSE ? *a.d_step : 0;
+    const int cur = (FUSE || STORE) ? *a.d_step : 0;
     if (FUSE && (int)blockIdx.y < a.pt.rows_pt) {
         if (a.pt.mode & FZ_SMP) ac2d_sample(a, cur);
     } else {
-        ac2d_fwd_v4_cells<R, STORE, VINJ>(a, cur);
+        ac2d_fwd_v4_tile<R, STORE, VINJ>(a, ac2d_tile(a), cur);
     }
     if (FUSE && (a.pt.mode & FZ_TICK)) tick_last_block(a.d_step, a.pt.d_done, 1);
 }
@@ -447,4 +475,86 @@ __global__ void __launch_bounds__(256) k_ac2d_adj_v4(const __grid_constant__ Ac2
         ac2d_adj_v4_cells<R>(a);
     }
     if (FUSE && (a.pt.mode & FZ_TICK)) tick_last_block(a.d_step, a.pt.d_done, -1);
+}
+
+// ------------------------- persistent forward segment -------------------------
+// All n steps of a forward segment in one cooperative launch: each block loops
+// over the pressure tiles of a step, a grid barrier, the sampling CTAs' work
+// and the velocity tiles, a barrier, the next step. Injection, sampling and
+// the arithmetic are those of the fused step kernels (same tile functions);
+// the fields that the launch itself writes are read with plain (coherent)
+// loads, not through the read-only path, whose cache a barrier does not
+// invalidate.
+
+// bounded barrier of a cooperative launch: bar[0] counts arrivals, bar[1] is
+// the generation. The last block to arrive resets the count and advances the
+// generation; the others poll it (with a pause between polls). A wait that
+// outlasts PERSIST_SPIN_LIMIT polls, or sees another block's failure, records
+// it in *err (the host reports OWL_ERR_TIMEOUT) and returns false, and the
+// block leaves the kernel.
+constexpr unsigned PERSIST_SPIN_LIMIT = 1u << 22;
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) {
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        int ok = 1;
+        volatile unsigned* vgen = bar + 1;
+        const unsigned g = *vgen;
+        __threadfence();
+        const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
+        if (atomicAdd(bar, 1u) == nb - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned i = 0;
+            while (*vgen == g) {
+                if (++i > PERSIST_SPIN_LIMIT || *(volatile int*)err) {
+                    atomicExch(err, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+struct Ac2dPersist {
+    int n;                   // steps of the segment
+    int gx, gy_p, gy_v, gz;  // pressure / velocity tiles: x, rows, shot groups
+    int nsmp;                // sampling work items (shots x CTAs per shot; 0: none)
+    unsigned* bar;
+    int* err;
+};
+
+template <int R, bool STORE, bool VINJ>
+__global__ void __launch_bounds__(256) k_ac2d_fwd_persist(const __grid_constant__ Ac2dDev a, Ac2dPersist p) {
+    // the step counter as the segment starts; no block writes it before every
+    // block has passed the last barrier
+    const int cur0 = *a.d_step;
+    const int np = p.gx * p.gy_p * p.gz, nv = p.nsmp + p.gx * p.gy_v * p.gz;
+    for (int i = 0; i < p.n; ++i) {
+        const int cur = cur0 + i;
+        for (int t = blockIdx.x; t < np; t += gridDim.x) {
+            const uint3 b = make_uint3(t % p.gx, (t / p.gx) % p.gy_p, t / (p.gx * p.gy_p));
+            ac2d_fwd_p4_tile<R, STORE, true, true>(a, b, cur);
+        }
+        if (!grid_barrier(p.bar, p.err)) return;
+        for (int t = blockIdx.x; t < nv; t += gridDim.x) {
+            if (t < p.nsmp) {
+                ac2d_sample_cta(a, t, cur);
+            } else {
+                const int u = t - p.nsmp;
+                const uint3 b = make_uint3(u % p.gx, (u / p.gx) % p.gy_v, u / (p.gx * p.gy_v));
+                ac2d_fwd_v4_tile<R, STORE, VINJ, true>(a, b, cur);
+            }
+        }
+        if (!grid_barrier(p.bar, p.err)) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) *a.d_step = cur0 + p.n;
 }

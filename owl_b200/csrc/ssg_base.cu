@@ -225,7 +225,7 @@ void SsgBase::check_timeout() {
     OWL_CUDA(cudaStreamSynchronize(stream));
     if (flag) {
         OWL_CUDA(cudaMemsetAsync(ctr.p + 3, 0, sizeof(int), stream));
-        throw OwlError(OWL_ERR_TIMEOUT, "a bounded wait for TMA copies gave up; the results are invalid");
+        throw OwlError(OWL_ERR_TIMEOUT, "a bounded wait (TMA copies or a grid barrier) gave up; the results are invalid");
     }
 }
 
@@ -477,6 +477,7 @@ void SsgBase::launch_step(int kind, int S, const PointDev& q) {
 
 void SsgBase::run_steps(int kind, int n, int S, const PointDev& q, bool graph) {
     if (n <= 0) return;
+    if (run_steps_persistent(kind, n, S)) return;
     if (!graph) {
         for (int i = 0; i < n; ++i) launch_step(kind, S, q);
         OWL_LAUNCH_CHECK();

@@ -199,6 +199,12 @@ struct SsgBase : Engine {
     void ensure_state(int S, int k, bool grad);
     PointDev pdev(int S, bool adjoint, bool want_src_adj);
     virtual void launch_step(int kind, int S, const PointDev& q);
+    // all n steps of a segment of kind `kind` as one persistent launch, where
+    // the medium has one and it is selected; false: run_steps launches per step
+    virtual bool run_steps_persistent(int kind, int n, int S) {
+        (void)kind; (void)n; (void)S;
+        return false;
+    }
     void run_steps(int kind, int n, int S, const PointDev& q, bool graph);
     void resolve_opts(const owl_run_opts& o, int nshots, const owl_shot* shots, bool grad, int& B, int& k,
                       bool& graph);

@@ -196,6 +196,38 @@ def test_fused_point_work_matches_point_kernels(fs, tz):
     assert out[False][4] < out[True][4]  # fewer launches with the fused point work
 
 
+@pytest.mark.parametrize("fs", [0, 1])
+def test_persistent_forward_segments_match_step_launches(fs):
+    """A forward segment as one cooperative launch (OWL_PERSIST=1: each block
+    loops over the pressure tiles, a grid barrier, the sampling work and the
+    velocity tiles, a barrier, per step) gives the seismograms, misfits and
+    gradients of the per-step launches to the bit, with and without graphs and
+    with a last segment shorter than the checkpoint interval."""
+    import os
+    nx, nz, dx, dt, nt = 48, 40, 10.0, 1e-3, 300
+    d = desc(nx, nz, dx, dt, nt, fs=fs)
+    vp, rho = random_model(nx, nz)
+    ps = prepare(small_shots(nx, nz, dx, bool(fs)), nx, nz, dx, dt)
+    obs = oracle.ac2d_forward(d, vp, rho, ps, "f64").astype(np.float32)
+    s = make_solver(d, vp * np.float32(1.02), rho)
+    out = {}
+    for persist in (False, True):
+        if persist:
+            os.environ["OWL_PERSIST"] = "1"
+        try:
+            seis = s.forward(ps, RunOpts(tile_z=104, shots_per_cta=2))
+            mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=37, tile_z=104))
+            mf2, g2 = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL,
+                                 RunOpts(checkpoint_interval=37, tile_z=102, use_graph=-1))
+            launches = s.last_info.gpu_launches
+        finally:
+            os.environ.pop("OWL_PERSIST", None)
+        out[persist] = (seis, mf, g, mf2, g2, launches)
+    for a, b in zip(out[False][:5], out[True][:5]):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+    assert out[True][5] < out[False][5]
+
+
 def test_memory_planner_picks_batch_and_interval():
     """With the device budget capped (OWL_MEM_BUDGET_MB), the planner splits the
     shots into smaller batches and picks a checkpoint interval below nt; the
