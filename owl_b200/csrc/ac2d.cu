@@ -914,6 +914,11 @@ struct Ac2dEngine : SsgBase {
         p.nsmp = kind == 1 ? 0 : S * nb_rec;
         if (!pbar.p) pbar.reserve(2);
         OWL_CUDA(cudaMemsetAsync(pbar.p, 0, 2 * sizeof(unsigned), stream));
+        // failure-detection test: OWL_PERSIST_STALL=1 starts the arrival count
+        // past the block count, so no block is ever the last to arrive and
+        // every barrier wait runs out (the call reports OWL_ERR_TIMEOUT)
+        if (const char* st = std::getenv("OWL_PERSIST_STALL"))
+            if (st[0] == '1' && st[1] == 0) OWL_CUDA(cudaMemsetAsync(pbar.p, 0x40, sizeof(unsigned), stream));
         p.bar = pbar.p;
         p.err = ctr.p + 3;
         const bool store = kind == 1 || kind == 3, vinj = (inj_fmask & 6) != 0;

@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(256) k_ac2d_adj_v4(const __grid_constant__ Ac2
 // outlasts PERSIST_SPIN_LIMIT polls, or sees another block's failure, records
 // it in *err (the host reports OWL_ERR_TIMEOUT) and returns false, and the
 // block leaves the kernel.
-constexpr unsigned PERSIST_SPIN_LIMIT = 1u << 22;
+constexpr unsigned PERSIST_SPIN_LIMIT = 1u << 21;  // polls (about a second at most)
 __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) {
     __shared__ int ok_s;
     __syncthreads();
@@ -514,7 +514,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) {
                     ok = 0;
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(32);
             }
         }
         __threadfence();

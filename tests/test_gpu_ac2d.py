@@ -228,6 +228,33 @@ def test_persistent_forward_segments_match_step_launches(fs):
     assert out[True][5] < out[False][5]
 
 
+def test_persistent_barrier_wait_runs_out():
+    """A grid-barrier wait of the persistent forward that nothing releases
+    (OWL_PERSIST_STALL=1: no block is ever the last to arrive) gives up after
+    its poll limit: the call raises OWL_ERR_TIMEOUT instead of hanging, and the
+    handle runs the next call normally."""
+    import os
+    nx, nz, dx, dt, nt = 48, 40, 10.0, 1e-3, 60
+    d = desc(nx, nz, dx, dt, nt)
+    vp, rho = random_model(nx, nz)
+    ps = prepare(small_shots(nx, nz, dx), nx, nz, dx, dt)
+    s = make_solver(d, vp, rho)
+    ref = s.forward(ps, RunOpts(tile_z=104))
+    os.environ["OWL_PERSIST"] = "1"
+    try:
+        os.environ["OWL_PERSIST_STALL"] = "1"
+        try:
+            with pytest.raises(L.OwlError) as e:
+                s.forward(ps, RunOpts(tile_z=104))
+            assert e.value.code == L.OWL_ERR_TIMEOUT
+        finally:
+            os.environ.pop("OWL_PERSIST_STALL", None)
+        got = s.forward(ps, RunOpts(tile_z=104))
+    finally:
+        os.environ.pop("OWL_PERSIST", None)
+    assert np.array_equal(got, ref)
+
+
 def test_memory_planner_picks_batch_and_interval():
     """With the device budget capped (OWL_MEM_BUDGET_MB), the planner splits the
     shots into smaller batches and picks a checkpoint interval below nt; the
