@@ -19,7 +19,7 @@ module owl_ssg_c
     use iso_c_binding
     implicit none
 
-    integer(c_int), parameter :: OWL_SSG_ABI_VERSION = 9
+    integer(c_int), parameter :: OWL_SSG_ABI_VERSION = 10
 
     ! status codes
     integer(c_int), parameter :: OWL_OK = 0
@@ -155,6 +155,9 @@ module owl_ssg_c
         integer(c_int) :: max_shots
         integer(c_int) :: allow_dt_adjust
         integer(c_int) :: aniso
+        real(c_float) :: free_surface_dz_refine
+        real(c_float) :: dz_max
+        integer(c_int) :: free_surface_refine_rows
     end type
 
     ! one source after prepare_geometry / prepare_stf
@@ -456,6 +459,27 @@ module owl_ssg_c
         integer(c_int) function owl_ssg_desc_nparam(desc) bind(c, name='owl_ssg_desc_nparam')
             import :: c_int, owl_ssg_desc
             type(owl_ssg_desc), intent(in) :: desc
+        end function
+
+        ! computational rows of the depth-refined free-surface mesh (host only);
+        ! null arrays (c_null_ptr) size them: nz_mesh + 2 pml + 2 values each
+        integer(c_int) function owl_vertical_mesh(desc, nz_mesh, z_i, z_h, dz_i, dz_h) &
+                bind(c, name='owl_vertical_mesh')
+            import :: c_int, c_ptr, owl_ssg_desc
+            type(owl_ssg_desc), intent(in) :: desc
+            integer(c_int), intent(out) :: nz_mesh
+            type(c_ptr), value :: z_i, z_h, dz_i, dz_h
+        end function
+
+        ! refine_nz from the model's surface row and the lowest source f0 (host only)
+        integer(c_int) function owl_free_surface_refine_rows(desc, nparam, fields, f0_min, refine_rows) &
+                bind(c, name='owl_free_surface_refine_rows')
+            import :: c_int, c_ptr, c_float, owl_ssg_desc
+            type(owl_ssg_desc), intent(in) :: desc
+            integer(c_int), value :: nparam
+            type(c_ptr), intent(in) :: fields(*)
+            real(c_float), value :: f0_min
+            integer(c_int), intent(out) :: refine_rows
         end function
 
         integer(c_int) function owl_ssg_ncomp(medium) bind(c, name='owl_ssg_ncomp')

@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define OWL_SSG_ABI_VERSION 9
+#define OWL_SSG_ABI_VERSION 10
 
 /* status codes */
 #define OWL_OK 0
@@ -170,6 +170,17 @@ typedef struct {
     int max_shots;       /* capacity of one batched launch (>= 1) */
     int allow_dt_adjust; /* 0: dt above the CFL bound is OWL_ERR_UNSTABLE */
     int aniso;           /* OWL_ANISO_*: model parameterisation of elastic media */
+    /* Depth-refined vertical mesh of the elastic 2D solver with a free surface
+     * (free_surface_dz_refine and dz_max of wave_solver_elastic_vhtiort_2d,
+     * elastic_vhtiort_2d/interface.f90:61-62; prepare_modeling,
+     * module_vars.f90:313-376): rows dz / free_surface_dz_refine apart from the
+     * surface down to (free_surface_refine_rows - 1) dz, then 2.5 % wider per
+     * row up to dz_max. The model, the gradient and the geometry's x / z stay on
+     * the regular (nz, nx) grid; owl_vertical_mesh gives the computational rows
+     * that the geometry's gz / hz and taps refer to. All zero: the uniform grid. */
+    float free_surface_dz_refine; /* >= 1; 0 = 1 */
+    float dz_max;                 /* largest row spacing (m); 0 = dz */
+    int free_surface_refine_rows; /* refine_nz (>= 1 when refined): owl_free_surface_refine_rows */
 } owl_ssg_desc;
 
 /* One source after prepare_geometry / prepare_stf. */
@@ -494,6 +505,25 @@ float owl_mpml_damp_ratio(const float *c, int axis);
 int owl_ssg_mpml_ratios(const owl_ssg *h, float *faces);
 
 /* ---- queries ------------------------------------------------------------ */
+
+/* Vertical mesh of a descriptor (host only, no device needed): the
+ * computational rows of the elastic 2D solver with a free surface
+ * (module_vars.f90:313-376). nz_mesh gets the number of rows (desc->nz for the
+ * uniform grid); each non-null array gets nz_mesh + 2 pml + 2 values, rows
+ * -pml .. nz_mesh + pml + 1 of the reference's zz_i, zz_h, dz_i, dz_h (depths
+ * below the model origin, m). Geometry on this mesh (module_source_receiver.f90:
+ * 596-616, 640-680): gz = the row of z_i nearest to z - oz (the first on a tie),
+ * hz likewise on z_h (z = 0 counts as just below the surface), taps
+ * kaiser_sinc((z - oz - z_i(gz)) / dz_i(gz)), the same with z_h, dz_h; with a
+ * free surface, sources above dz_i(1) move to dz_i(1) with 1.2 x amplitude
+ * (module_vars.f90:463-466). Call once with null arrays to size them. */
+int owl_vertical_mesh(const owl_ssg_desc *desc, int *nz_mesh, float *z_i, float *z_h, float *dz_i, float *dz_h);
+/* refine_nz of the refined mesh (module_vars.f90:315-317): ceil(0.5 lambda / dz)
+ * with lambda = sqrt(mean over the padded surface row of c55 / rho) / f0_min,
+ * c55 and rho of the model in desc->aniso's parameterisation (elastic 2D),
+ * f0_min the lowest peak frequency of the sources. Host only. */
+int owl_free_surface_refine_rows(const owl_ssg_desc *desc, int nparam, const float *const *fields, float f0_min,
+                                 int *refine_rows);
 
 const char *owl_last_error(void);
 int owl_ssg_abi_version(void);

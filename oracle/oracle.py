@@ -42,6 +42,7 @@ def load():
         _lib.oracle_el2d_gradient_f64.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, vp, vp, vp]
         _lib.oracle_el2d_setup.argtypes = [vp, vp, vp]
         _lib.oracle_el2d_damp_ratio.argtypes = [C.c_float] * 5 + [C.c_int]
+        _lib.oracle_el2d_mesh.argtypes = [vp, vp, vp, vp, vp, vp]
         _lib.oracle_el2d_damp_ratio.restype = C.c_float
         _lib.oracle_el3d_forward_f32.argtypes = [vp, vp, C.c_int, vp, vp]
         _lib.oracle_el3d_forward_f64.argtypes = [vp, vp, C.c_int, vp, vp]
@@ -216,6 +217,20 @@ def el2d_dt_stable(desc, fields):
     if lib.oracle_el2d_setup(C.byref(desc), arr, C.byref(out)):
         raise RuntimeError("oracle el2d setup failed")
     return out.value
+
+
+def el2d_mesh(desc):
+    """(nz_mesh, z_i, z_h, dz_i, dz_h) of the depth-refined free-surface mesh,
+    rows -pml .. nz_mesh + pml + 1; the arrays are None on the uniform grid."""
+    lib = load()
+    n = C.c_int(0)
+    if lib.oracle_el2d_mesh(C.byref(desc), C.byref(n), None, None, None, None):
+        raise RuntimeError("oracle el2d mesh failed")
+    arr = [np.zeros(n.value + 2 * desc.pml + 2, dtype=np.float32) for _ in range(4)]
+    if lib.oracle_el2d_mesh(C.byref(desc), C.byref(n), *[_p(a) for a in arr]):
+        raise RuntimeError("oracle el2d mesh failed")
+    refined = bool(np.any(arr[2] != 0))
+    return (n.value, *arr) if refined else (n.value, None, None, None, None)
 
 
 def el2d_damp_ratio(c11, c13, c33, c55, rho, direction="x"):

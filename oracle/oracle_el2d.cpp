@@ -12,9 +12,13 @@
 //   add_source                  src/solver/elastic_vhtiort_2d/module_wavefield.f90:294-403
 //   time loop, surface images and sampling
 //                               src/solver/elastic_vhtiort_2d/submodule_forward_modeling.f90:58-197
-// on a uniform grid (free_surface_dz_refine = 1, dz_max = dz, so dz_i = dz and
-// the dz scaling factors are 1), plus the exact discrete adjoint of that loop
-// and the chain rule from (c11, c13, c33, c55, rho) to the model parameters.
+// on the uniform grid and on the depth-refined free-surface mesh
+// (module_vars.f90:313-376: Cij interpolated linearly to the mesh rows, every z
+// derivative scaled by dz / dz_i or dz / dz_h, the z PML and the explosion
+// source on the row's own dz_i), plus the exact discrete adjoint of that loop
+// and the chain rule from (c11, c13, c33, c55, rho) to the model parameters (on
+// the refined mesh through the transpose of the row interpolation, back to the
+// regular rows).
 //
 // Templated on T: float (forward parity oracle), double (FP64 gradient oracle),
 // std::complex<double> (complex-step Jacobian-vector products). The PML
@@ -193,18 +197,21 @@ struct El2dState {
 template <typename T>
 struct El2d {
     int nx, nz, pml, R, nt, aniso, np;
+    int nzm;                          // regular (model) rows; nz: the mesh's rows
     float dx, dz, dt, idx, idz;
     bool fs;
     const float* c;
-    Arr2<T> c11, c13, c33, c55, rho;  // padded by pml+1
+    ZMesh zm;
+    ZLinear zl;
+    Arr2<T> c11, c13, c33, c55, rho;  // padded by pml+1, on the mesh's rows
     Arr2<T> c55e;                     // harmonic c55 at the sigma_xz nodes
-    std::vector<Arr2<T>> par;         // padded model parameters
+    std::vector<Arr2<T>> par;         // padded model parameters, regular rows
     Mp2 ii, hh, hi, ih;
     int lo_x, hi_x, lo_z, hi_z;
     float dt_stable = 0;
 
     El2d(const owl_ssg_desc& d, const T* const* fields) {
-        nx = d.nx; nz = d.nz; pml = d.pml; R = d.fdhalf; nt = d.nt; aniso = d.aniso;
+        nx = d.nx; nzm = d.nz; pml = d.pml; R = d.fdhalf; nt = d.nt; aniso = d.aniso;
         dx = d.dx; dz = d.dz; dt = d.dt; fs = d.free_surface != 0;
         np = aniso_nparam(aniso);
         if (np < 0) throw std::runtime_error("bad aniso");
@@ -212,16 +219,37 @@ struct El2d {
         idz = (float)(1.0 / (double)dz);
         c = fdcoefs(R);
         const int P = pml;
-        for (Arr2<T>* a : {&c11, &c13, &c33, &c55, &rho}) a->init(-P, nx + P + 1, -P, nz + P + 1);
+        zm = zmesh_build(d);
+        nz = zm.n;
+        if (zm.refined) zl = zlinear_build(zm, nzm, dz);
+        // Cij of the regular padded rows
+        Arr2<T> r11(-P, nx + P + 1, -P, nzm + P + 1), r13 = r11, r33 = r11, r55 = r11, rr_ = r11;
         par.resize(np);
-        for (auto& a : par) a.init(-P, nx + P + 1, -P, nz + P + 1);
-        for (int j = -P; j <= nz + P + 1; ++j)
+        for (auto& a : par) a.init(-P, nx + P + 1, -P, nzm + P + 1);
+        for (int j = -P; j <= nzm + P + 1; ++j)
             for (int i = -P; i <= nx + P + 1; ++i) {
-                int ii_ = std::min(std::max(i, 1), nx), jj = std::min(std::max(j, 1), nz);
-                size_t src = (size_t)(ii_ - 1) * nz + (jj - 1);
+                int ii_ = std::min(std::max(i, 1), nx), jj = std::min(std::max(j, 1), nzm);
+                size_t src = (size_t)(ii_ - 1) * nzm + (jj - 1);
                 std::vector<T> p(np);
                 for (int q = 0; q < np; ++q) p[q] = par[q](i, j) = fields[q][src];
-                to_cij(aniso, p.data(), c11(i, j), c13(i, j), c33(i, j), c55(i, j), rho(i, j));
+                to_cij(aniso, p.data(), r11(i, j), r13(i, j), r33(i, j), r55(i, j), rr_(i, j));
+            }
+        // the mesh's rows (map_regular_to_irregular, module_vars.f90:139-169)
+        for (Arr2<T>* a : {&c11, &c13, &c33, &c55, &rho}) a->init(-P, nx + P + 1, -P, nz + P + 1);
+        for (int j = -P; j <= nz + P + 1; ++j)
+            for (int i = -P; i <= nx + P + 1; ++i) {
+                if (!zm.refined) {
+                    c11(i, j) = r11(i, j); c13(i, j) = r13(i, j); c33(i, j) = r33(i, j); c55(i, j) = r55(i, j);
+                    rho(i, j) = rr_(i, j);
+                    continue;
+                }
+                const int j0 = zl.j0(j);
+                const T w = T(zl.w(j));
+                c11(i, j) = r11(i, j0) + w * (r11(i, j0 + 1) - r11(i, j0));
+                c13(i, j) = r13(i, j0) + w * (r13(i, j0 + 1) - r13(i, j0));
+                c33(i, j) = r33(i, j0) + w * (r33(i, j0 + 1) - r33(i, j0));
+                c55(i, j) = r55(i, j0) + w * (r55(i, j0 + 1) - r55(i, j0));
+                rho(i, j) = rr_(i, j0) + w * (rr_(i, j0 + 1) - rr_(i, j0));
             }
         c55e.init(-P + 1, nx + P, -P + 1, nz + P);
         for (int n = -P + 1; n <= nz + P; ++n)
@@ -229,26 +257,40 @@ struct El2d {
                 T s = T(1) / c55(m - 1, n - 1) + T(1) / c55(m, n - 1) + T(1) / c55(m - 1, n) + T(1) / c55(m, n);
                 c55e(m, n) = T(4) / s;
             }
-        // pmlvp (module_vars.f90:289-293) and dt_stable (:408-420)
+        // pmlvp of the regular model's edges (module_vars.f90:298-302) and dt_stable
+        // (:381-420: on the refined mesh the least over the cells, each with its
+        // row's smaller spacing)
         float pv = -1e30f, maxv = 0.f;
-        for (int j = 1; j <= nz; ++j)
+        for (int j = 1; j <= nzm; ++j)
             for (int i : {1, nx}) {
-                pv = std::max(pv, (float)re(c11(i, j)) / (float)re(rho(i, j)));
-                pv = std::max(pv, (float)re(c33(i, j)) / (float)re(rho(i, j)));
+                pv = std::max(pv, (float)re(r11(i, j)) / (float)re(rr_(i, j)));
+                pv = std::max(pv, (float)re(r33(i, j)) / (float)re(rr_(i, j)));
             }
         for (int i = 1; i <= nx; ++i)
-            for (int j : {1, nz}) {
-                pv = std::max(pv, (float)re(c11(i, j)) / (float)re(rho(i, j)));
-                pv = std::max(pv, (float)re(c33(i, j)) / (float)re(rho(i, j)));
+            for (int j : {1, nzm}) {
+                pv = std::max(pv, (float)re(r11(i, j)) / (float)re(rr_(i, j)));
+                pv = std::max(pv, (float)re(r33(i, j)) / (float)re(rr_(i, j)));
             }
         const float pmlvp = std::sqrt(pv);
-        for (int j = 1; j <= nz; ++j)
-            for (int i = 1; i <= nx; ++i)
-                maxv = std::max({maxv, std::sqrt((float)re(c11(i, j)) / (float)re(rho(i, j))),
-                                 std::sqrt((float)re(c33(i, j)) / (float)re(rho(i, j)))});
         float temp = 0.f;
         for (int k = 0; k < R; ++k) temp += std::fabs(c[k]);
-        dt_stable = 1.0f / (temp * maxv * std::sqrt(1.0f / (dx * dx) + 1.0f / (dz * dz)));
+        if (!zm.refined) {
+            for (int j = 1; j <= nz; ++j)
+                for (int i = 1; i <= nx; ++i)
+                    maxv = std::max({maxv, std::sqrt((float)re(c11(i, j)) / (float)re(rho(i, j))),
+                                     std::sqrt((float)re(c33(i, j)) / (float)re(rho(i, j)))});
+            dt_stable = 1.0f / (temp * maxv * std::sqrt(1.0f / (dx * dx) + 1.0f / (dz * dz)));
+        } else {
+            float best = 3.0e38f;
+            for (int j = 1; j <= nz; ++j)
+                for (int i = 1; i <= nx; ++i) {
+                    const float mv = std::max(std::sqrt((float)re(c11(i, j)) / (float)re(rho(i, j))),
+                                              std::sqrt((float)re(c33(i, j)) / (float)re(rho(i, j))));
+                    const float h = std::min(zm.dzi(j), zm.dzh(j));
+                    best = std::min(best, 1.0f / (temp * mv * std::sqrt(1.0f / (dx * dx) + 1.0f / (h * h))));
+                }
+            dt_stable = best;
+        }
         // M-PML ratios (module_cfspml.f90:229-276), zero for the isotropic parameterisation
         Arr1<float> rl, rr, rt, rb;
         rl.init(-P, nz + P + 1, 0.f); rr.init(-P, nz + P + 1, 0.f);
@@ -285,8 +327,10 @@ struct El2d {
                 float rx = 0.f, rz = 0.f;
                 if (i <= 1) rx = rl(j); else if (i >= nx) rx = rr(j);
                 if (j <= 1) rz = rt(i); else if (j >= nz) rz = rb(i);
+                // the row's own dz_i(j) on the refined mesh (module_cfspml.f90:446-473)
+                const float dzj = zm.refined ? zm.dzi(j) : dz;
                 auto set = [&](Mp2& m, float xd, float zd) {
-                    el_damp_coef(pmlvp, xd, zd, dx, dz, P, dt, alphamax, rx, rz, m.ax(i, j), m.bx(i, j), m.az(i, j),
+                    el_damp_coef(pmlvp, xd, zd, dx, dzj, P, dt, alphamax, rx, rz, m.ax(i, j), m.bx(i, j), m.az(i, j),
                                  m.bz(i, j));
                 };
                 set(ii, xdi, zdi);
@@ -297,6 +341,12 @@ struct El2d {
         lo_x = -P - R + 1; hi_x = nx + P + R;
         lo_z = -P - R + 1; hi_z = nz + P + R;
     }
+
+    // dz scalings of the z derivatives at integer / half rows (1 on the uniform grid)
+    T zsi(int j) const { return zm.refined ? T(zm.si(j)) : T(1); }
+    T zsh(int j) const { return zm.refined ? T(zm.sh(j)) : T(1); }
+    // local spacing of an explosion / moment-tensor source's row (dz_s, module_wavefield.f90:305-309)
+    float dz_src(int gz) const { return zm.refined ? zm.dzi(gz) : dz; }
 
     // PML membership of the owner node of each field
     bool in_ii(int i, int j) const { return i <= 0 || i >= nx + 1 || (!fs && j <= 0) || j >= nz + 1; }
@@ -335,7 +385,7 @@ struct El2d {
                     pdzvz = -(c13(i, j) / c33(i, j) * pdxvx);
                 } else {
                     for (int k = 1; k <= R; ++k) sz = sz + T(c[k - 1]) * (s.vz(i, j + k) - s.vz(i, j - k + 1));
-                    pdzvz = T(idz) * sz;
+                    pdzvz = T(idz) * sz * zsi(j);
                     if (in_ii(i, j)) {
                         s.m_dxvx(i, j) = T(ii.ax(i, j)) * pdxvx + T(ii.bx(i, j)) * s.m_dxvx(i, j);
                         pdxvx = pdxvx + s.m_dxvx(i, j);
@@ -354,7 +404,7 @@ struct El2d {
                 T sz = T(0), sx = T(0);
                 for (int k = 1; k <= R; ++k) sz = sz + T(c[k - 1]) * (s.vx(m, n - 1 + k) - s.vx(m, n - k));
                 for (int k = 1; k <= R; ++k) sx = sx + T(c[k - 1]) * (s.vz(m - 1 + k, n) - s.vz(m - k, n));
-                T pdzvx = T(idz) * sz, pdxvz = T(idx) * sx;
+                T pdzvx = T(idz) * sz * zsh(n), pdxvz = T(idx) * sx;
                 if (in_hh(m, n)) {
                     s.m_dxvz(m, n) = T(hh.ax(m, n)) * pdxvz + T(hh.bx(m, n)) * s.m_dxvz(m, n);
                     pdxvz = pdxvz + s.m_dxvz(m, n);
@@ -380,7 +430,7 @@ struct El2d {
                 T sx = T(0), sz = T(0);
                 for (int k = 1; k <= R; ++k) sx = sx + T(c[k - 1]) * (s.sxx(m - 1 + k, j) - s.sxx(m - k, j));
                 for (int k = 1; k <= R; ++k) sz = sz + T(c[k - 1]) * (s.sxz(m, j + k) - s.sxz(m, j - k + 1));
-                T pdxxx = T(idx) * sx, pdzxz = T(idz) * sz;
+                T pdxxx = T(idx) * sx, pdzxz = T(idz) * sz * zsi(j);
                 if (in_hi(m, j)) {
                     s.m_dxxx(m, j) = T(hi.ax(m, j)) * pdxxx + T(hi.bx(m, j)) * s.m_dxxx(m, j);
                     pdxxx = pdxxx + s.m_dxxx(m, j);
@@ -398,7 +448,7 @@ struct El2d {
                 T sx = T(0), sz = T(0);
                 for (int k = 1; k <= R; ++k) sx = sx + T(c[k - 1]) * (s.sxz(i + k, n) - s.sxz(i - k + 1, n));
                 for (int k = 1; k <= R; ++k) sz = sz + T(c[k - 1]) * (s.szz(i, n - 1 + k) - s.szz(i, n - k));
-                T pdxxz = T(idx) * sx, pdzzz = T(idz) * sz;
+                T pdxxz = T(idx) * sx, pdzzz = T(idz) * sz * zsh(n);
                 if (in_ih(i, n)) {
                     s.m_dxxz(i, n) = T(ih.ax(i, n)) * pdxxz + T(ih.bx(i, n)) * s.m_dxxz(i, n);
                     pdxxz = pdxxz + s.m_dxxz(i, n);
@@ -434,7 +484,7 @@ struct El2d {
                                 T(std::cos(q.polar)) * amp / rho(q.gx, q.hz) * T(q.interp_ix[irx + 4]) * T(q.interp_hz[irz + 4]);
                     }
             } else {
-                const T a = amp / (T(dx) * T(dz));
+                const T a = amp / (T(dx) * T(dz_src(q.gz)));
                 const bool mt = q.mechanism == OWL_SRC_MT;
                 const T mxx = mt ? T(q.mt[0]) : T(1), mzz = mt ? T(q.mt[2]) : T(1), mxz = T(q.mt[4]);
                 for (int irz = -4; irz <= 4; ++irz)
@@ -540,7 +590,7 @@ struct El2d {
                         if (mt && (!fs || q.hz + irz >= 2))
                             acc = acc + mxz * a.sxz(q.hx + irx, q.hz + irz) * T(q.interp_hx[irx + 4]) * T(q.interp_hz[irz + 4]);
                     }
-                dstf = -acc * T(q.amp) * T(dt) / (T(dx) * T(dz));
+                dstf = -acc * T(q.amp) * T(dt) / (T(dx) * T(dz_src(q.gz)));
             }
             if (stf_grad) stf_grad[(size_t)kk * nt + (t - 1)] = stf_grad[(size_t)kk * nt + (t - 1)] + dstf;
         }
@@ -559,7 +609,7 @@ struct El2d {
                     ez = pml_e(q, ih.az(i, n), ih.bz(i, n), a.m_dzzz(i, n));
                 }
                 ex = T(idx) * ex;
-                ez = T(idz) * ez;
+                ez = T(idz) * zsh(n) * ez;
                 for (int k = 1; k <= R; ++k) {
                     a.sxz(i + k, n) = a.sxz(i + k, n) + T(c[k - 1]) * ex;
                     a.sxz(i - k + 1, n) = a.sxz(i - k + 1, n) - T(c[k - 1]) * ex;
@@ -582,7 +632,7 @@ struct El2d {
                     ez = pml_e(q, hi.az(m, j), hi.bz(m, j), a.m_dzxz(m, j));
                 }
                 ex = T(idx) * ex;
-                ez = T(idz) * ez;
+                ez = T(idz) * zsi(j) * ez;
                 for (int k = 1; k <= R; ++k) {
                     a.sxx(m - 1 + k, j) = a.sxx(m - 1 + k, j) + T(c[k - 1]) * ex;
                     a.sxx(m - k, j) = a.sxx(m - k, j) - T(c[k - 1]) * ex;
@@ -621,7 +671,7 @@ struct El2d {
                     ex = pml_e(q, hh.ax(m, n), hh.bx(m, n), a.m_dxvz(m, n));
                     ez = pml_e(q, hh.az(m, n), hh.bz(m, n), a.m_dzvx(m, n));
                 }
-                ez = T(idz) * ez;
+                ez = T(idz) * zsh(n) * ez;
                 ex = T(idx) * ex;
                 for (int k = 1; k <= R; ++k) {
                     a.vx(m, n - 1 + k) = a.vx(m, n - 1 + k) + T(c[k - 1]) * ez;
@@ -658,7 +708,7 @@ struct El2d {
                     }
                 }
                 ex = T(idx) * ex;
-                ez = T(idz) * ez;
+                ez = T(idz) * zsi(j) * ez;
                 for (int k = 1; k <= R; ++k) {
                     a.vx(i + k, j) = a.vx(i + k, j) + T(c[k - 1]) * ex;
                     a.vx(i - k + 1, j) = a.vx(i - k + 1, j) - T(c[k - 1]) * ex;
@@ -730,13 +780,31 @@ struct El2d {
 
     // parameter gradients on the padded grid from d J / d (c11, c13, c33, c55, rho):
     // the Jacobian of to_cij by complex-step differentiation of each parameter
+    // (on the refined mesh: first the transpose of the row interpolation, from
+    // the mesh rows to the regular rows)
     void chain(Grad& g) const {
         typedef std::complex<double> C;
         const int P = pml;
-        g.gpar.assign(np, Arr2<T>(-P, nx + P + 1, -P, nz + P + 1));
-        for (int j = -P; j <= nz + P + 1; ++j)
+        std::array<Arr2<T>, 5> rg;
+        const Arr2<T>* src[5] = {&g.g11, &g.g13, &g.g33, &g.g55, &g.grho};
+        if (zm.refined) {
+            for (auto& a : rg) a.init(-P, nx + P + 1, -P, nzm + P + 1);
+            for (int f = -P; f <= nz + P + 1; ++f) {
+                const int j0 = zl.j0(f);
+                const T w = T(zl.w(f));
+                for (int q = 0; q < 5; ++q)
+                    for (int i = -P; i <= nx + P + 1; ++i) {
+                        const T v = (*src[q])(i, f);
+                        rg[q](i, j0) = rg[q](i, j0) + (T(1) - w) * v;
+                        rg[q](i, j0 + 1) = rg[q](i, j0 + 1) + w * v;
+                    }
+            }
+            for (int q = 0; q < 5; ++q) src[q] = &rg[q];
+        }
+        g.gpar.assign(np, Arr2<T>(-P, nx + P + 1, -P, nzm + P + 1));
+        for (int j = -P; j <= nzm + P + 1; ++j)
             for (int i = -P; i <= nx + P + 1; ++i) {
-                const T dc[5] = {g.g11(i, j), g.g13(i, j), g.g33(i, j), g.g55(i, j), g.grho(i, j)};
+                const T dc[5] = {(*src[0])(i, j), (*src[1])(i, j), (*src[2])(i, j), (*src[3])(i, j), (*src[4])(i, j)};
                 for (int q = 0; q < np; ++q) {
                     std::vector<C> p(np);
                     for (int r = 0; r < np; ++r) p[r] = C(re(par[r](i, j)), r == q ? 1e-30 : 0.0);
@@ -750,11 +818,11 @@ struct El2d {
     }
 
     void fold(const Arr2<T>& gp, T* out) const {
-        std::fill(out, out + (size_t)nx * nz, T(0));
+        std::fill(out, out + (size_t)nx * nzm, T(0));
         for (int j = gp.j0; j <= gp.j1; ++j)
             for (int i = gp.i0; i <= gp.i1; ++i) {
-                int ii_ = std::min(std::max(i, 1), nx), jj = std::min(std::max(j, 1), nz);
-                out[(size_t)(ii_ - 1) * nz + (jj - 1)] += gp(i, j);
+                int ii_ = std::min(std::max(i, 1), nx), jj = std::min(std::max(j, 1), nzm);
+                out[(size_t)(ii_ - 1) * nzm + (jj - 1)] += gp(i, j);
             }
     }
 };
@@ -871,6 +939,27 @@ extern "C" int oracle_el2d_setup(const owl_ssg_desc* d, const float* const* f, f
     try {
         El2d<float> m(*d, f);
         *dt_stable = m.dt_stable;
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle: %s\n", e.what());
+        return -1;
+    }
+}
+
+// the refined mesh of a descriptor: nz_mesh, then rows -pml .. nz_mesh + pml + 1
+// of z_i, z_h, dz_i, dz_h (arrays of nz_mesh + 2 pml + 2 floats, or null)
+extern "C" int oracle_el2d_mesh(const owl_ssg_desc* d, int* nz_mesh, float* zi, float* zh, float* dzi, float* dzh) {
+    try {
+        ZMesh m = zmesh_build(*d);
+        *nz_mesh = m.n;
+        if (!m.refined) return 0;
+        for (int j = -d->pml; j <= m.n + d->pml + 1; ++j) {
+            const size_t o = (size_t)(j + d->pml);
+            if (zi) zi[o] = m.zi(j);
+            if (zh) zh[o] = m.zh(j);
+            if (dzi) dzi[o] = m.dzi(j);
+            if (dzh) dzh[o] = m.dzh(j);
+        }
         return 0;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "oracle: %s\n", e.what());

@@ -98,6 +98,9 @@ class OwlSsgDesc(C.Structure):
         ("max_shots", C.c_int),
         ("allow_dt_adjust", C.c_int),
         ("aniso", C.c_int),
+        ("free_surface_dz_refine", C.c_float),
+        ("dz_max", C.c_float),
+        ("free_surface_refine_rows", C.c_int),
     ]
 
 
@@ -200,7 +203,7 @@ EXPORTED = [
     "owl_ssg_forward_noalloc", "owl_ssg_desc_nparam", "owl_ssg_misfit", "owl_ssg_gradient_misfit",
     "owl_adjoint_source", "owl_dtw_time_shifts", "owl_ssg_set_data_sampling", "owl_resample_traces",
     "owl_su_encode", "owl_su_decode", "owl_search_direction", "owl_grad_process",
-    "owl_mpml_damp_ratio", "owl_ssg_mpml_ratios",
+    "owl_mpml_damp_ratio", "owl_ssg_mpml_ratios", "owl_vertical_mesh", "owl_free_surface_refine_rows",
 ]
 
 OWL_SEARCH_SD = 0
@@ -285,7 +288,9 @@ def load() -> C.CDLL:
                                          C.c_void_p, C.c_int]
     lib.owl_grad_process.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_float), C.c_void_p, C.c_void_p,
                                      C.c_int]
-    for fn in ("owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
+    lib.owl_vertical_mesh.argtypes = [P(OwlSsgDesc), P(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.owl_free_surface_refine_rows.argtypes = [P(OwlSsgDesc), C.c_int, P(P(C.c_float)), C.c_float, P(C.c_int)]
+    for fn in ("owl_vertical_mesh", "owl_free_surface_refine_rows", "owl_ssg_create", "owl_ssg_set_model", "owl_ssg_forward", "owl_ssg_gradient",
                "owl_ssg_source_gradient", "owl_ssg_abi_version", "owl_ssg_nparam", "owl_ssg_ncomp",
                "owl_ssg_device_ok", "owl_ssg_desc_nparam", "owl_ssg_misfit", "owl_ssg_gradient_misfit",
                "owl_adjoint_source", "owl_dtw_time_shifts", "owl_ssg_set_data_sampling", "owl_resample_traces",

@@ -5,6 +5,7 @@
 
 #include "adjsrc.cuh"
 #include "engine.cuh"
+#include "vmesh.hpp"
 
 struct owl_ssg {
     std::unique_ptr<owl::Engine> eng;
@@ -90,6 +91,49 @@ int owl_ssg_ncomp(int medium) {
         case OWL_ELASTIC_VHTIORT_3D: return 3;
         default: return -1;
     }
+}
+
+int owl_vertical_mesh(const owl_ssg_desc* desc, int* nz_mesh, float* z_i, float* z_h, float* dz_i, float* dz_h) {
+    return guarded([&] {
+        OWL_CHECK(desc && nz_mesh, OWL_ERR_INVALID, "null argument");
+        OWL_CHECK(desc->nz >= 1 && desc->pml >= 0 && desc->dz > 0, OWL_ERR_INVALID, "bad grid");
+        VMesh m;
+        try {
+            m = build_vmesh(*desc);
+        } catch (const std::invalid_argument& e) {
+            throw OwlError(OWL_ERR_INVALID, e.what());
+        }
+        *nz_mesh = m.nz;
+        const int P = desc->pml;
+        const size_t L = (size_t)m.nz + 2 * P + 2;
+        for (int j = -P; j <= m.nz + P + 1; ++j) {
+            const size_t o = (size_t)(j + P);
+            if (m.refined) {
+                if (z_i) z_i[o] = m.zi[o];
+                if (z_h) z_h[o] = m.zh[o];
+                if (dz_i) dz_i[o] = m.dzi[o];
+                if (dz_h) dz_h[o] = m.dzh[o];
+            } else {
+                // the uniform grid: row j at (j - 1) dz, half row at (j - 1.5) dz
+                if (z_i) z_i[o] = (float)(j - 1) * desc->dz;
+                if (z_h) z_h[o] = ((float)(j - 1) - 0.5f) * desc->dz;
+                if (dz_i) dz_i[o] = desc->dz;
+                if (dz_h) dz_h[o] = desc->dz;
+            }
+        }
+        (void)L;
+    });
+}
+
+int owl_free_surface_refine_rows(const owl_ssg_desc* desc, int nparam, const float* const* fields, float f0_min,
+                                 int* refine_rows) {
+    return guarded([&] {
+        OWL_CHECK(desc && fields && refine_rows, OWL_ERR_INVALID, "null argument");
+        OWL_CHECK(f0_min > 0, OWL_ERR_INVALID, "f0_min must be positive");
+        OWL_CHECK(desc->medium == OWL_ELASTIC_VHTIORT_2D, OWL_ERR_UNSUPPORTED,
+                  "the refined free-surface mesh is built for the elastic 2D medium");
+        *refine_rows = el2d_refine_rows(*desc, nparam, fields, f0_min);
+    });
 }
 
 int owl_ssg_device_ok(void) {

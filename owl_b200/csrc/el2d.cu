@@ -36,6 +36,7 @@
 
 #include "ssg_base.cuh"
 #include "vec4.cuh"
+#include "vmesh.hpp"
 
 namespace owl {
 
@@ -57,6 +58,10 @@ struct El2dDev {
     int nshots, spt;
     const float *c11, *c13, *c33, *c55e, *bx, *bz;
     const float4 *pii, *phh, *phi, *pih;
+    // per storage row: dz / dz_i and dz / dz_h of the depth-refined mesh, the
+    // factors of the z derivatives at integer-z nodes (sigma_xx, sigma_zz, vx)
+    // and half-z nodes (sigma_xz, vz); 1 on the uniform grid
+    const float *zfi, *zfh;
     float* st;   // forward state (shot 0)
     float* S;    // stored stencil terms: [term][slot][shot][fs]
     long long sslot, sterm;
@@ -95,6 +100,8 @@ __global__ void __maxnreg__(R == 4 ? 48 : 128) k_el2d_fwd_s(El2dDev a) {
     const float4 chh = (phh && dxz) ? __ldg(a.phh + o) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float c11 = __ldg(a.c11 + o), c13 = __ldg(a.c13 + o), c33 = __ldg(a.c33 + o);
     const float c55dt = dxz ? a.dt * __ldg(a.c55e + o) : 0.f;
+    // 1/dz times the row's dz scaling (refined mesh; 1/dz exactly on the uniform grid)
+    const float zsi = a.idz * __ldg(a.zfi + z), zsh = a.idz * __ldg(a.zfh + z);
     const bool mir = a.fsurf && z > a.pr && z <= a.pr + a.R;
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
@@ -129,7 +136,7 @@ __global__ void __maxnreg__(R == 4 ? 48 : 128) k_el2d_fwd_s(El2dDev a) {
             float sz = 0.f;
 #pragma unroll
             for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(vz + (k * pt)) - __ldg(vz + ((1 - k) * pt)));
-            dzv = a.idz * sz;
+            dzv = zsi * sz;
             if (pii) {
                 const float m1 = cii.x * dxv + cii.y * mxv;
                 mem[M_DXVX * a.fs] = m1;
@@ -158,7 +165,7 @@ __global__ void __maxnreg__(R == 4 ? 48 : 128) k_el2d_fwd_s(El2dDev a) {
             for (int k = 1; k <= R; ++k) szx = szx + c_fde[k - 1] * (__ldg(vx + ((k - 1) * pt)) - __ldg(vx + (-k * pt)));
 #pragma unroll
             for (int k = 1; k <= R; ++k) sxz = sxz + c_fde[k - 1] * (__ldg(vz + (k - 1)) - __ldg(vz + (-k)));
-            float dzvx = a.idz * szx, dxvz = a.idx * sxz;
+            float dzvx = zsh * szx, dxvz = a.idx * sxz;
             if (phh) {
                 const float m3 = chh.x * dxvz + chh.y * mxz;
                 mem[M_DXVZ * a.fs] = m3;
@@ -189,6 +196,7 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
     const float4 chi = phi ? __ldg(a.phi + o) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 cih = (pih && dvz) ? __ldg(a.pih + o) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float bx = __ldg(a.bx + o), bz = dvz ? __ldg(a.bz + o) : 0.f;
+    const float zsi = a.idz * __ldg(a.zfi + z), zsh = a.idz * __ldg(a.zfh + z);  // see k_el2d_fwd_s
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
     for (int s = s0; s < s1; ++s) {
@@ -207,7 +215,7 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
             for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (__ldg(sxx + (k - 1)) - __ldg(sxx + (-k)));
 #pragma unroll
             for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(sxz + (k * pt)) - __ldg(sxz + ((1 - k) * pt)));
-            float hx = a.idx * sx, hz = a.idz * sz;
+            float hx = a.idx * sx, hz = zsi * sz;
             if (phi) {
                 const float m1 = chi.x * hx + chi.y * m_xxx;
                 mem[M_DXXX * a.fs] = m1;
@@ -226,7 +234,7 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
             for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (__ldg(sxz + (k)) - __ldg(sxz + (1 - k)));
 #pragma unroll
             for (int k = 1; k <= R; ++k) sz = sz + c_fde[k - 1] * (__ldg(szz + ((k - 1) * pt)) - __ldg(szz + (-k * pt)));
-            float hx = a.idx * sx, hz = a.idz * sz;
+            float hx = a.idx * sx, hz = zsh * sz;
             if (pih) {
                 const float m1 = cih.x * hx + cih.y * m_xxz;
                 mem[M_DXXZ * a.fs] = m1;
@@ -274,6 +282,9 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
     const float4 chi = phi ? __ldg(a.phi + o) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 cih = (pih && dvz) ? __ldg(a.pih + o) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float bx = __ldg(a.bx + o), bz = dvz ? __ldg(a.bz + o) : 0.f;
+    // the z-derivative e terms carry the node's dz scaling, so that the
+    // neighbours' transposed stencils stay plain
+    const float zsi = __ldg(a.zfi + z), zsh = __ldg(a.zfh + z);
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     float gbx = 0.f, gbz = 0.f;
     for (int s = s0; s < s1; ++s) {
@@ -303,7 +314,7 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
                 ez = pml_e(q, chi.z, chi.w, m_zxz, mh + M_DZXZ * a.fs);
             }
             e[M_DXXX * a.fs] = ex;
-            e[M_DZXZ * a.fs] = ez;
+            e[M_DZXZ * a.fs] = ez * zsi;
         }
         if (dvz) {
             const float* e4 = e + M_DZVZ * a.fs;
@@ -323,7 +334,7 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
                 ez = pml_e(q, cih.z, cih.w, m_zzz, mh + M_DZZZ * a.fs);
             }
             e[M_DXXZ * a.fs] = ex;
-            e[M_DZZZ * a.fs] = ez;
+            e[M_DZZZ * a.fs] = ez * zsh;
         }
     }
     const long long go = (long long)blockIdx.z * a.fs + o;
@@ -360,6 +371,7 @@ __global__ void __maxnreg__(R == 4 ? 64 : 128) k_el2d_adj_s(El2dDev a) {
     const long long ozz = (long long)(2 * a.pr - z) * pt + x;      // sigma_zz image row
     const long long oxz = (long long)(2 * a.pr + 1 - z) * pt + x;  // sigma_xz image row
     const float r13 = c13 / c33;
+    const float zsi = __ldg(a.zfi + z), zsh = __ldg(a.zfh + z);  // see k_el2d_adj_v
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     float g11 = 0.f, g13 = 0.f, g33 = 0.f, g55 = 0.f;
     for (int s = s0; s < s1; ++s) {
@@ -420,7 +432,7 @@ __global__ void __maxnreg__(R == 4 ? 64 : 128) k_el2d_adj_s(El2dDev a) {
                 ex = pml_e(qx, cii.x, cii.y, m_xvx, mh + M_DXVX * a.fs);
                 ez = pml_e(qz, cii.z, cii.w, m_zvz, mh + M_DZVZ * a.fs);
             }
-            e[M_DZVZ * a.fs + o] = ez;
+            e[M_DZVZ * a.fs + o] = ez * zsi;
         }
         e[M_DXVX * a.fs + o] = ex;
         // sigma_xz
@@ -452,7 +464,7 @@ __global__ void __maxnreg__(R == 4 ? 64 : 128) k_el2d_adj_s(El2dDev a) {
                 exz = pml_e(q, chh.x, chh.y, m_xvz, mh + M_DXVZ * a.fs);
                 ezx = pml_e(q, chh.z, chh.w, m_zvx, mh + M_DZVX * a.fs);
             }
-            e[M_DZVX * a.fs + o] = ezx;
+            e[M_DZVX * a.fs + o] = ezx * zsh;
             e[M_DXVZ * a.fs + o] = exz;
         }
     }
@@ -470,6 +482,9 @@ __global__ void __maxnreg__(R == 4 ? 64 : 128) k_el2d_adj_s(El2dDev a) {
 //   sigma += dt (C . D)           -> dJ/dc   = dt G_c
 //   sigma_xz += dt c55e D         -> dJ/dc55 = dt G_55 c55e^2 / (4 c55^2), 4 nodes
 //   v += (dt / rho_eff) H         -> dJ/drho = -0.5 dt G_b / rho_eff^2, 2 + 2 nodes
+// With jac null (the depth-refined mesh) the five d J / d (c11, c13, c33, c55,
+// rho) of the mesh cells go to gpad's planes 0..4 as they are; k_el2d_zmap
+// carries them to the regular rows and through the Jacobian.
 __global__ void k_el2d_chain(El2dDev a, int ngroups, const float* __restrict__ c55p, const float* __restrict__ rhop,
                              const double* __restrict__ jac, int np, long long npad, double* __restrict__ gpad,
                              int nxq, int nzq) {
@@ -514,10 +529,39 @@ __global__ void k_el2d_chain(El2dDev a, int ngroups, const float* __restrict__ c
         }
     }
     const long long cell = (long long)iz * nxq + ix;
+    if (!jac) {
+        for (int q = 0; q < 5; ++q) gpad[(long long)q * npad + cell] += dc[q];
+        return;
+    }
     for (int p = 0; p < np; ++p) {
         double g = 0;
         for (int q = 0; q < 5; ++q) g += jac[((long long)p * 5 + q) * npad + cell] * dc[q];
         gpad[(long long)p * npad + cell] += g;
+    }
+}
+
+// Gradient of the regular padded rows from the mesh cells' d J / d (c11, c13,
+// c33, c55, rho): the transpose of the row interpolation that maps the regular
+// Cij to the mesh (regular row r gets sum over mesh rows f of w(f, r) g(f), the
+// pairs in zptr / zrow / zw), then the per-cell Jacobian to the model
+// parameters. One thread per regular padded cell, FP64.
+__global__ void k_el2d_zmap(const double* __restrict__ gmesh, long long npad_m, const int* __restrict__ zptr,
+                            const int* __restrict__ zrow, const double* __restrict__ zw,
+                            const double* __restrict__ jac, int np, long long npad_r, double* __restrict__ gout,
+                            int nxq, int nzq_r) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x, iz = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= nxq || iz >= nzq_r) return;
+    double dc[5] = {0, 0, 0, 0, 0};
+    for (int e = zptr[iz]; e < zptr[iz + 1]; ++e) {
+        const long long cm = (long long)zrow[e] * nxq + ix;
+        const double w = zw[e];
+        for (int q = 0; q < 5; ++q) dc[q] += w * gmesh[(long long)q * npad_m + cm];
+    }
+    const long long cell = (long long)iz * nxq + ix;
+    for (int p = 0; p < np; ++p) {
+        double g = 0;
+        for (int q = 0; q < 5; ++q) g += jac[((long long)p * 5 + q) * npad_r + cell] * dc[q];
+        gout[(long long)p * npad_r + cell] = g;
     }
 }
 
@@ -668,19 +712,40 @@ float4 mpml_coef(float vp, float xd, float zd, float dx, float dz, int pml, floa
     return c;
 }
 
+VMesh checked_vmesh(const owl_ssg_desc& d) {
+    try {
+        return build_vmesh(d);
+    } catch (const std::invalid_argument& e) {
+        throw OwlError(OWL_ERR_INVALID, e.what());
+    }
+}
+
+owl_ssg_desc with_rows(owl_ssg_desc d, int nz) {
+    d.nz = nz;
+    return d;
+}
+
 }  // namespace
 
 // ============================================================================
 // host engine
 // ============================================================================
+// With the depth-refined free-surface mesh the engine runs on the mesh's rows
+// (nz of the base = the computational rows); the model and the gradient stay on
+// the regular nz_model rows.
 struct El2dEngine : SsgBase {
     int aniso;
     float idx, idz;
-    DevBuf<float> c11, c13, c33, c55e, bxp, bzp, c55p, rhop;
+    VMesh vm;
+    int nz_model;
+    ZInterp zt;
+    DevBuf<float> c11, c13, c33, c55e, bxp, bzp, c55p, rhop, zfi, zfh;
     DevBuf<float4> pii, phh, phi, pih;
-    DevBuf<double> jac;
+    DevBuf<double> jac, zw, gzmap;
+    DevBuf<int> zptr, zrow;
 
-    explicit El2dEngine(const owl_ssg_desc& d) : SsgBase(d, 2) {
+    explicit El2dEngine(const owl_ssg_desc& d) : El2dEngine(d, checked_vmesh(d)) {}
+    El2dEngine(const owl_ssg_desc& d, VMesh m) : SsgBase(with_rows(d, m.nz), 2), vm(std::move(m)), nz_model(d.nz) {
         aniso = d.aniso;
         OWL_CHECK(el_nparam(aniso) > 0, OWL_ERR_INVALID, "unknown elastic parameterisation (aniso)");
         idx = (float)(1.0 / (double)d.dx);
@@ -693,27 +758,64 @@ struct El2dEngine : SsgBase {
         nparam = el_nparam(aniso);
         ncomp = 2;
         for (int f = 0; f < EL_NST; ++f) st_segments.push_back({f * fs, fs});
+        // dz scalings of the storage rows (1 outside the mesh arrays and on the uniform grid)
+        std::vector<float> hi(NZs, 1.f), hh(NZs, 1.f);
+        if (vm.refined) {
+            for (int z = 0; z < NZs; ++z) {
+                const int j = z - pr + 1;
+                if (j < -P || j > nz + P + 1) continue;
+                hi[z] = vm.get(vm.si, j);
+                hh[z] = vm.get(vm.sh, j);
+            }
+            zt = build_zinterp(vm, nz_model, d.dz);
+            // transpose of the row interpolation, per regular padded row
+            const int nzr = nz_model + 2 * P + 2;
+            std::vector<std::vector<std::pair<int, double>>> by(nzr);
+            for (int f = -P; f <= nz + P + 1; ++f) {
+                const int r0 = zt.r0[(size_t)(f + P)];
+                const double w = zt.w[(size_t)(f + P)];
+                by[(size_t)(r0 + P)].push_back({f + P, 1.0 - w});
+                by[(size_t)(r0 + 1 + P)].push_back({f + P, w});
+            }
+            std::vector<int> hp(1, 0), hr;
+            std::vector<double> hw;
+            for (auto& v : by) {
+                for (auto& e : v) { hr.push_back(e.first); hw.push_back(e.second); }
+                hp.push_back((int)hr.size());
+            }
+            zptr.upload(hp.data(), hp.size(), stream);
+            zrow.upload(hr.data(), hr.size(), stream);
+            zw.upload(hw.data(), hw.size(), stream);
+        }
+        zfi.upload(hi.data(), hi.size(), stream);
+        zfh.upload(hh.data(), hh.size(), stream);
+        OWL_CUDA(cudaStreamSynchronize(stream));
     }
+
+    // refined mesh: gpad holds the mesh cells' d J / d (c11, c13, c33, c55, rho)
+    int grad_planes() const override { return vm.refined ? 5 : nparam; }
 
     float* st_field(int f) const override { return f < 5 ? st.p + f * fs : nullptr; }
     float* ad_field(int f) const override { return f < 5 ? ad.p + f * fs : nullptr; }
-    int rho_param() const override { return nparam - 1; }
+    int rho_param() const override { return vm.refined ? 4 : nparam - 1; }
 
     void set_model(int np, const float* const* f) override {
         OWL_CHECK(np == nparam && f, OWL_ERR_INVALID,
                   "elastic 2D model needs " + std::to_string(nparam) + " parameters for this parameterisation");
         for (int q = 0; q < np; ++q) OWL_CHECK(f[q], OWL_ERR_INVALID, "null model parameter");
-        const int nxq_ = nxq(), nzq_ = nzq();
-        const size_t np_ = npad();
-        // padded parameters and Cij (padding by pml+1 with edge values, module_vars.f90:297-301)
-        std::vector<float> hc11(fs, 0.f), hc13(fs, 0.f), hc33(fs, 0.f), hc55(fs, 0.f), hrho(fs, 0.f);
-        std::vector<double> hjac((size_t)np * 5 * np_, 0.0);
+        const int nxq_ = nxq(), nzr = nz_model;
+        const size_t npr = (size_t)nxq_ * (nzr + 2 * P + 2);  // regular padded cells
+        // padded parameters and Cij of the regular rows (padding by pml+1 with
+        // edge values, module_vars.f90:297-301)
+        std::vector<float> r11(npr), r13(npr), r33(npr), r55(npr), rrho(npr);
+        std::vector<double> hjac((size_t)np * 5 * npr, 0.0);
         std::vector<float> p(np);
         std::vector<std::complex<double>> pc(np);
-        for (int j = -P; j <= nz + P + 1; ++j)
+        auto rc = [&](int i, int j) { return (size_t)(j + P) * nxq_ + (size_t)(i + P); };
+        for (int j = -P; j <= nzr + P + 1; ++j)
             for (int i = -P; i <= nx + P + 1; ++i) {
-                const int ii = std::min(std::max(i, 1), nx), jj = std::min(std::max(j, 1), nz);
-                const size_t src = (size_t)(ii - 1) * nz + (jj - 1);
+                const int ii = std::min(std::max(i, 1), nx), jj = std::min(std::max(j, 1), nzr);
+                const size_t src = (size_t)(ii - 1) * nzr + (jj - 1);
                 for (int q = 0; q < np; ++q) p[q] = f[q][src];
                 for (int q = 0; q < np; ++q)
                     OWL_CHECK(std::isfinite(p[q]), OWL_ERR_INVALID, "model parameters must be finite");
@@ -721,16 +823,35 @@ struct El2dEngine : SsgBase {
                 cij_of<float>(aniso, p.data(), a11, a13, a33, a55, r);
                 OWL_CHECK(r > 0 && a11 > 0 && a33 > 0 && a55 > 0, OWL_ERR_INVALID,
                           "rho, c11, c33 and c55 must be positive");
-                const long long o = soff(i, 1, j);
-                hc11[o] = a11; hc13[o] = a13; hc33[o] = a33; hc55[o] = a55; hrho[o] = r;
+                const size_t cell = rc(i, j);
+                r11[cell] = a11; r13[cell] = a13; r33[cell] = a33; r55[cell] = a55; rrho[cell] = r;
                 // Jacobian d(c11, c13, c33, c55, rho) / d(param) by complex step in FP64
-                const long long cell = pad_index(i, 1, j);
                 for (int q = 0; q < np; ++q) {
                     for (int r2 = 0; r2 < np; ++r2) pc[r2] = std::complex<double>(p[r2], r2 == q ? 1e-30 : 0.0);
                     std::complex<double> o5[5];
                     cij_of(aniso, pc.data(), o5[0], o5[1], o5[2], o5[3], o5[4]);
-                    for (int k = 0; k < 5; ++k) hjac[((size_t)q * 5 + k) * np_ + cell] = o5[k].imag() / 1e-30;
+                    for (int k = 0; k < 5; ++k) hjac[((size_t)q * 5 + k) * npr + cell] = o5[k].imag() / 1e-30;
                 }
+            }
+        // the engine's rows: the regular ones, or on the refined mesh the Cij
+        // interpolated linearly in depth (map_regular_to_irregular, module_vars.f90:139-169)
+        std::vector<float> hc11(fs, 0.f), hc13(fs, 0.f), hc33(fs, 0.f), hc55(fs, 0.f), hrho(fs, 0.f);
+        for (int j = -P; j <= nz + P + 1; ++j)
+            for (int i = -P; i <= nx + P + 1; ++i) {
+                const long long o = soff(i, 1, j);
+                if (!vm.refined) {
+                    const size_t cell = rc(i, j);
+                    hc11[o] = r11[cell]; hc13[o] = r13[cell]; hc33[o] = r33[cell]; hc55[o] = r55[cell];
+                    hrho[o] = rrho[cell];
+                    continue;
+                }
+                const int r0 = zt.r0[(size_t)(j + P)];
+                const size_t c0 = rc(i, r0), c1 = rc(i, r0 + 1);
+                hc11[o] = zinterp_apply(zt, j, P, r11[c0], r11[c1]);
+                hc13[o] = zinterp_apply(zt, j, P, r13[c0], r13[c1]);
+                hc33[o] = zinterp_apply(zt, j, P, r33[c0], r33[c1]);
+                hc55[o] = zinterp_apply(zt, j, P, r55[c0], r55[c1]);
+                hrho[o] = zinterp_apply(zt, j, P, rrho[c0], rrho[c1]);
             }
         // harmonic c55 at the sigma_xz nodes and buoyancies (module_wavefield.f90:31-35)
         std::vector<float> hc55e(fs, 0.f), hbx(fs, 0.f), hbz(fs, 0.f);
@@ -743,24 +864,39 @@ struct El2dEngine : SsgBase {
                 hbx[o] = dt / (0.5f * (hrho[soff(m - 1, 1, n)] + hrho[o]));
                 hbz[o] = dt / (0.5f * (hrho[soff(m, 1, n - 1)] + hrho[o]));
             }
-        // pmlvp (module_vars.f90:289-293) and the stability bound (:408-420)
+        // pmlvp from the regular model's edges (module_vars.f90:298-302) and the
+        // stability bound (:381-420; on the refined mesh the least over the
+        // cells with the row's smaller spacing)
         float pv = -1e30f, maxv = 0.f;
         auto edge = [&](int i, int j) {
-            const long long o = soff(i, 1, j);
-            pv = std::max({pv, hc11[o] / hrho[o], hc33[o] / hrho[o]});
+            const size_t cell = rc(i, j);
+            pv = std::max({pv, r11[cell] / rrho[cell], r33[cell] / rrho[cell]});
         };
-        for (int j = 1; j <= nz; ++j) { edge(1, j); edge(nx, j); }
-        for (int i = 1; i <= nx; ++i) { edge(i, 1); edge(i, nz); }
+        for (int j = 1; j <= nzr; ++j) { edge(1, j); edge(nx, j); }
+        for (int i = 1; i <= nx; ++i) { edge(i, 1); edge(i, nzr); }
         const float pmlvp = std::sqrt(pv);
-        for (int j = 1; j <= nz; ++j)
-            for (int i = 1; i <= nx; ++i) {
-                const long long o = soff(i, 1, j);
-                maxv = std::max({maxv, std::sqrt(hc11[o] / hrho[o]), std::sqrt(hc33[o] / hrho[o])});
-            }
         const float* c = fd_coefs(R);
         float temp = 0.f;
         for (int k = 0; k < R; ++k) temp += std::fabs(c[k]);
-        dt_stable_ = 1.0f / (temp * maxv * std::sqrt(1.0f / (desc.dx * desc.dx) + 1.0f / (desc.dz * desc.dz)));
+        if (!vm.refined) {
+            for (int j = 1; j <= nz; ++j)
+                for (int i = 1; i <= nx; ++i) {
+                    const long long o = soff(i, 1, j);
+                    maxv = std::max({maxv, std::sqrt(hc11[o] / hrho[o]), std::sqrt(hc33[o] / hrho[o])});
+                }
+            dt_stable_ = 1.0f / (temp * maxv * std::sqrt(1.0f / (desc.dx * desc.dx) + 1.0f / (desc.dz * desc.dz)));
+        } else {
+            float best = 3.0e38f;
+            for (int j = 1; j <= nz; ++j) {
+                const float hz = std::min(vm.get(vm.dzi, j), vm.get(vm.dzh, j));
+                for (int i = 1; i <= nx; ++i) {
+                    const long long o = soff(i, 1, j);
+                    const float mv = std::max(std::sqrt(hc11[o] / hrho[o]), std::sqrt(hc33[o] / hrho[o]));
+                    best = std::min(best, 1.0f / (temp * mv * std::sqrt(1.0f / (desc.dx * desc.dx) + 1.0f / (hz * hz))));
+                }
+            }
+            dt_stable_ = best;
+        }
         if (dt > dt_stable_ && !desc.allow_dt_adjust)
             throw OwlError(OWL_ERR_UNSTABLE, "dt = " + std::to_string(dt) + " exceeds the stable dt " +
                                                  std::to_string(dt_stable_));
@@ -801,10 +937,12 @@ struct El2dEngine : SsgBase {
                 if (i <= 1) rx = rl[j + P]; else if (i >= nx) rx = rr[j + P];
                 if (j <= 1) rz = rt[i + P]; else if (j >= nz) rz = rb[i + P];
                 const long long o = soff(i, 1, j);
-                hii[o] = mpml_coef(pmlvp, xdi, zdi, desc.dx, desc.dz, P, dt, alphamax, rx, rz);
-                hih[o] = mpml_coef(pmlvp, xdi, zdh, desc.dx, desc.dz, P, dt, alphamax, rx, rz);
-                hhi[o] = mpml_coef(pmlvp, xdh, zdi, desc.dx, desc.dz, P, dt, alphamax, rx, rz);
-                hhh[o] = mpml_coef(pmlvp, xdh, zdh, desc.dx, desc.dz, P, dt, alphamax, rx, rz);
+                // the row's own spacing dz_i(j) on the refined mesh (module_cfspml.f90:446-473)
+                const float dzj = vm.refined ? vm.get(vm.dzi, j) : desc.dz;
+                hii[o] = mpml_coef(pmlvp, xdi, zdi, desc.dx, dzj, P, dt, alphamax, rx, rz);
+                hih[o] = mpml_coef(pmlvp, xdi, zdh, desc.dx, dzj, P, dt, alphamax, rx, rz);
+                hhi[o] = mpml_coef(pmlvp, xdh, zdi, desc.dx, dzj, P, dt, alphamax, rx, rz);
+                hhh[o] = mpml_coef(pmlvp, xdh, zdh, desc.dx, dzj, P, dt, alphamax, rx, rz);
             }
         c11.upload(hc11.data(), fs, stream);
         c13.upload(hc13.data(), fs, stream);
@@ -820,7 +958,6 @@ struct El2dEngine : SsgBase {
         pih.upload(hih.data(), fs, stream);
         jac.upload(hjac.data(), hjac.size(), stream);
         OWL_CUDA(cudaStreamSynchronize(stream));
-        (void)nxq_; (void)nzq_;
         h_rhop = std::move(hrho);
         model_set = true;
         invalidate_graphs();
@@ -853,9 +990,12 @@ struct El2dEngine : SsgBase {
                 }
             return;
         }
-        // explosion / moment tensor: stress drop amp / (dx dz), module_wavefield.f90:339-399
+        // explosion / moment tensor: stress drop amp / (dx dz_s), dz_s the local
+        // spacing dz_i(gz) on the refined mesh, module_wavefield.f90:305-399
         const bool mt = q.mechanism == OWL_SRC_MT;
-        const float inv = 1.0f / (desc.dx * desc.dz);
+        OWL_CHECK(!vm.refined || (q.gz >= -P && q.gz <= nz + P + 1), OWL_ERR_INVALID, "source outside the grid");
+        const float dzs = vm.refined ? vm.get(vm.dzi, q.gz) : desc.dz;
+        const float inv = 1.0f / (desc.dx * dzs);
         const float mxx = mt ? q.mt[0] : 1.f, mzz = mt ? q.mt[2] : 1.f, mxz = q.mt[4];
         for (int irz = -4; irz <= 4; ++irz)
             for (int irx = -4; irx <= 4; ++irx) {
@@ -910,6 +1050,7 @@ struct El2dEngine : SsgBase {
         a.nshots = S;
         a.c11 = c11.p; a.c13 = c13.p; a.c33 = c33.p; a.c55e = c55e.p; a.bx = bxp.p; a.bz = bzp.p;
         a.pii = pii.p; a.phh = phh.p; a.phi = phi.p; a.pih = pih.p;
+        a.zfi = zfi.p; a.zfh = zfh.p;
         a.st = st.p;
         a.k = std::max(1, cur_k);
         a.d_step = ctr.p;
@@ -1046,13 +1187,61 @@ struct El2dEngine : SsgBase {
     void chain_rule(int S, int groups) override {
         El2dDev a = dev(S);
         const dim3 b(32, 8), g((nxq() + 31) / 32, (nzq() + 7) / 8);
-        k_el2d_chain<<<g, b, 0, stream>>>(a, groups, c55p.p, rhop.p, jac.p, nparam, (long long)npad(), gpad.p, nxq(),
-                                          nzq());
+        k_el2d_chain<<<g, b, 0, stream>>>(a, groups, c55p.p, rhop.p, vm.refined ? nullptr : jac.p, nparam,
+                                          (long long)npad(), gpad.p, nxq(), nzq());
         OWL_LAUNCH_CHECK();
         launches++;
+    }
+
+    // refined mesh: the mesh cells' d J / d Cij to the regular rows and the
+    // model parameters (k_el2d_zmap), then the fold of the padding
+    void fold_out(float* grad, int mem) override {
+        if (!vm.refined) {
+            SsgBase::fold_out(grad, mem);
+            return;
+        }
+        const int nzq_r = nz_model + 2 * P + 2;
+        const size_t npr = (size_t)nxq() * nzq_r;
+        gzmap.reserve((size_t)nparam * npr);
+        const dim3 b(32, 8), g((nxq() + 31) / 32, (nzq_r + 7) / 8);
+        k_el2d_zmap<<<g, b, 0, stream>>>(gpad.p, (long long)npad(), zptr.p, zrow.p, zw.p, jac.p, nparam,
+                                         (long long)npr, gzmap.p, nxq(), nzq_r);
+        OWL_LAUNCH_CHECK();
+        launches++;
+        const size_t nm = (size_t)nx * nz_model;
+        seis_tmp.reserve((size_t)nparam * nm);
+        for (int q = 0; q < nparam; ++q) {
+            launch_fold(gzmap.p + (size_t)q * npr, nxq(), 1, P, nx, 1, nz_model, 2, seis_tmp.p + (size_t)q * nm,
+                        stream);
+            launches++;
+        }
+        copy_out(grad, seis_tmp.p, (size_t)nparam * nm * sizeof(float), mem);
     }
 };
 
 Engine* make_el2d_engine(const owl_ssg_desc& d) { return new El2dEngine(d); }
+
+// refine_nz = ceiling(0.5 lambda / dz), lambda = sqrt(mean(c55 / rho over the
+// padded surface row)) / f0_min (module_vars.f90:315-317)
+int el2d_refine_rows(const owl_ssg_desc& d, int np, const float* const* f, float f0_min) {
+    OWL_CHECK(np == el_nparam(d.aniso) && f, OWL_ERR_INVALID,
+              "elastic 2D model needs " + std::to_string(el_nparam(d.aniso)) + " parameters for this parameterisation");
+    for (int q = 0; q < np; ++q) OWL_CHECK(f[q], OWL_ERR_INVALID, "null model parameter");
+    OWL_CHECK(d.nx >= 1 && d.nz >= 1 && d.pml >= 0 && d.dz > 0, OWL_ERR_INVALID, "bad grid");
+    std::vector<float> p(np);
+    float sum = 0.f;
+    int cnt = 0;
+    for (int i = -d.pml; i <= d.nx + d.pml + 1; ++i) {
+        const int ii = std::min(std::max(i, 1), d.nx);
+        for (int q = 0; q < np; ++q) p[q] = f[q][(size_t)(ii - 1) * d.nz];
+        float a11, a13, a33, a55, r;
+        cij_of<float>(d.aniso, p.data(), a11, a13, a33, a55, r);
+        OWL_CHECK(r > 0 && a55 > 0, OWL_ERR_INVALID, "rho and c55 must be positive");
+        sum += a55 / r;
+        ++cnt;
+    }
+    const float lambda = std::sqrt(sum / (float)cnt) / f0_min;
+    return (int)std::ceil(0.5f * lambda / d.dz);
+}
 
 }  // namespace owl

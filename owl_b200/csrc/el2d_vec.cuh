@@ -97,9 +97,10 @@ __global__ void __launch_bounds__(256) k_el2d_fwd_s4(El2dDev a) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) sz[q] = sz[q] + c_fde[k - 1] * (f4at(up, q) - f4at(dn, q));
             }
+            const float zsi = a.idz * __ldg(a.zfi + z);  // 1/dz times the row's dz scaling (refined mesh)
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                dzv[q] = a.idz * sz[q];
+                dzv[q] = zsi * sz[q];
                 if (pii[q]) {
                     const float4 ci = __ldg(a.pii + o + q);
                     const float m1 = ci.x * dxv[q] + ci.y * f4at(mxv, q);
@@ -149,9 +150,10 @@ __global__ void __launch_bounds__(256) k_el2d_fwd_s4(El2dDev a) {
             }
             float4 xzn, gS;
             const float4 c55 = ldg4(a.c55e + o);
+            const float zsh = a.idz * __ldg(a.zfh + z);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                float dzvx = a.idz * szx[q], dxvz = a.idx * sxz[q];
+                float dzvx = zsh * szx[q], dxvz = a.idx * sxz[q];
                 if (phh[q]) {
                     const float4 ch = __ldg(a.phh + o + q);
                     const float m3 = ch.x * dxvz + ch.y * f4at(mxz, q);
@@ -224,12 +226,13 @@ __global__ void __launch_bounds__(256) k_el2d_fwd_v4(El2dDev a) {
             }
             float4 vn, hS;
             const float4 bx = ldg4(a.bx + o);
+            const float zsi = a.idz * __ldg(a.zfi + z);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 float sx = 0.f;
 #pragma unroll
                 for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (w[R + q + k - 1] - w[R + q - k]);
-                float hx = a.idx * sx, hz = a.idz * sz[q];
+                float hx = a.idx * sx, hz = zsi * sz[q];
                 if (phi[q]) {
                     const float4 ch = __ldg(a.phi + o + q);
                     const float m1 = ch.x * hx + ch.y * f4at(m_xxx, q);
@@ -261,12 +264,13 @@ __global__ void __launch_bounds__(256) k_el2d_fwd_v4(El2dDev a) {
             }
             float4 vn, hS;
             const float4 bz = ldg4(a.bz + o);
+            const float zsh = a.idz * __ldg(a.zfh + z);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 float sx = 0.f;
 #pragma unroll
                 for (int k = 1; k <= R; ++k) sx = sx + c_fde[k - 1] * (w[R + q + k] - w[R + q + 1 - k]);
-                float hx = a.idx * sx, hz = a.idz * sz[q];
+                float hx = a.idx * sx, hz = zsh * sz[q];
                 if (pih[q]) {
                     const float4 ch = __ldg(a.pih + o + q);
                     const float m1 = ch.x * hx + ch.y * f4at(m_xxz, q);

@@ -991,6 +991,9 @@ struct El3dEngine : SsgBase {
         OWL_CHECK(aniso == OWL_ANISO_ISO || aniso == OWL_ANISO_CIJ || aniso == OWL_ANISO_THOMSEN, OWL_ERR_UNSUPPORTED,
                   "elastic 3D takes the iso (vp, vs, rho), thomsen (vp, vs, epsilon, delta, gamma, theta, phi, rho) "
                   "or cij (nine moduli, rho) parameterisation");
+        OWL_CHECK(!(d.free_surface && (d.free_surface_dz_refine > 1.f || (d.dz_max > 0.f && d.dz_max != d.dz))),
+                  OWL_ERR_UNSUPPORTED, "elastic 3D runs the free surface on the uniform grid "
+                                       "(free_surface_dz_refine 1, dz_max dz)");
         idx = (float)(1.0 / (double)d.dx);
         idy = (float)(1.0 / (double)d.dy);
         idz = (float)(1.0 / (double)d.dz);

@@ -187,6 +187,12 @@ __global__ void k_fold(const double* __restrict__ gp, int nxq, int nyq, int P, i
     }
 }
 
+void launch_fold(const double* gp, int nxq, int nyq, int P, int nx, int ny, int nz, int dim, float* out,
+                 cudaStream_t s) {
+    k_fold<<<148 * 4, 256, 0, s>>>(gp, nxq, nyq, P, nx, ny, nz, dim, out);
+    OWL_LAUNCH_CHECK();
+}
+
 __global__ void k_add_points_f64(double* g, const long long* idx, const double* val, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) g[idx[i]] += val[i];
@@ -525,7 +531,7 @@ double SsgBase::batch_bytes(int S, int k, bool grad, int rec_per_shot) const {
              + f4 * 2.0 * ngrad * S * (double)fs   // Kahan sums, one group per shot at most
              + f4 * nS * (double)kk * S * fs       // stencil terms of a segment
              + nseg * ck * sst * S                 // checkpoints
-             + 8.0 * nparam * (double)npad();      // FP64 padded gradient
+             + 8.0 * grad_planes() * (double)npad();  // FP64 padded gradient
     }
     return b;
 }
@@ -956,8 +962,8 @@ void SsgBase::gradient_impl(int nshots, const owl_shot* shots, const float* data
     launches = 0;
     const int nt = desc.nt;
     EventTimer tm(stream);
-    gpad.reserve((size_t)nparam * npad());
-    OWL_CUDA(cudaMemsetAsync(gpad.p, 0, sizeof(double) * nparam * npad(), stream));
+    gpad.reserve((size_t)grad_planes() * npad());
+    OWL_CUDA(cudaMemsetAsync(gpad.p, 0, sizeof(double) * grad_planes() * npad(), stream));
     size_t data_off = 0, stf_off = 0;
     int batches = 0, shot0 = 0;
     for (int b0 = 0; b0 < nshots; b0 += B) {

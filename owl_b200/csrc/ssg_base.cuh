@@ -61,6 +61,9 @@ enum { PA_SCATTER = 1, PA_SRC = 2, PA_TICK = 4, PA_SRC_NOW = 8 };
 
 void launch_point_fwd(const PointDev& q, int S, int nb, int mode, cudaStream_t s);
 void launch_point_adj(const PointDev& q, int S, int nb, int mode, cudaStream_t s);
+// padded-grid FP64 gradient -> model cells, the adjoint of the edge padding
+void launch_fold(const double* gp, int nxq, int nyq, int P, int nx, int ny, int nz, int dim, float* out,
+                 cudaStream_t s);
 
 // one interpolation tap of a source / receiver on field `field` at reference node (i, j, k)
 struct TapPt {
@@ -220,7 +223,10 @@ struct SsgBase : Engine {
     void check_nonfinite(const float* f, size_t n);
     void check_timeout();  // OWL_ERR_TIMEOUT if a kernel's bounded wait gave up
     void copy_out(void* dst, const void* src, size_t bytes, int mem);
-    void fold_out(float* grad, int mem);
+    virtual void fold_out(float* grad, int mem);
+    // FP64 planes of the padded gradient accumulator gpad (the model parameters;
+    // a medium may keep other per-cell sums there that fold_out maps)
+    virtual int grad_planes() const { return nparam; }
     void invalidate_graphs();
     void fill_info(owl_run_info& info, int nshots, int batches, bool grad);
 

@@ -174,6 +174,42 @@ def _node(x, o, d):
 
 
 @dataclass
+class ZMesh:
+    """Computational rows of the depth-refined free-surface mesh
+    (owl_vertical_mesh): rows -pml .. n + pml + 1 of the reference's zz_i,
+    zz_h, dz_i, dz_h (src/solver/elastic_vhtiort_2d/module_vars.f90:313-376)."""
+    pml: int
+    z_i: np.ndarray
+    z_h: np.ndarray
+    dz_i: np.ndarray
+    dz_h: np.ndarray
+
+    def at(self, arr: np.ndarray, j: int) -> np.float32:
+        return arr[j + self.pml]
+
+
+#: the small offset that places a source or receiver at z = 0 on the half row
+#: below the free surface (module_source_receiver.f90:614-616); FLIT's own
+#: value is not vendored, any positive offset well below the row spacing gives
+#: the same row
+FLOAT_SMALL = f32(1.0e-6)
+
+
+def _node_mesh(z, o, m: ZMesh):
+    """gz / hz as the nearest integer / half row of the mesh (the first on a
+    tie), taps from the offset in units of the row's spacing
+    (module_source_receiver.f90:596-616, 640-680)."""
+    z, o = f32(z), f32(o)
+    rel = f32(z - o)
+    g = int(np.argmin(np.abs(f32(rel) - m.z_i))) - m.pml
+    relh = f32(f32(z + (FLOAT_SMALL if z == 0 else f32(0))) - o)
+    h = int(np.argmin(np.abs(relh - m.z_h))) - m.pml
+    ti = kaiser_sinc_kernel(f32(f32(rel - m.at(m.z_i, g)) / m.at(m.dz_i, g)))
+    th = kaiser_sinc_kernel(f32(f32(rel - m.at(m.z_h, h)) / m.at(m.dz_h, h)))
+    return g, h, ti, th
+
+
+@dataclass
 class GridSpec:
     nx: int
     nz: int
@@ -184,6 +220,10 @@ class GridSpec:
     ny: int = 1
     dy: float = 1.0
     oy: float = 0.0
+    zmesh: Optional[ZMesh] = None  # rows of the refined free-surface mesh, None on the uniform grid
+
+    def node_z(self, z):
+        return _node(z, self.oz, self.dz) if self.zmesh is None else _node_mesh(z, self.oz, self.zmesh)
 
 
 class PreparedShots:
@@ -217,7 +257,7 @@ class PreparedShots:
                 valid = grid.ox <= q.x <= xmax and grid.oz <= q.z <= zmax and (not dim3 or grid.oy <= q.y <= ymax)
                 if q.weight != 0 and valid:
                     o.gx, o.hx, ix, hx = _node(q.x, grid.ox, grid.dx)
-                    o.gz, o.hz, iz, hz = _node(q.z, grid.oz, grid.dz)
+                    o.gz, o.hz, iz, hz = grid.node_z(q.z)
                     o.interp_ix[:] = ix.tolist(); o.interp_hx[:] = hx.tolist()
                     o.interp_iz[:] = iz.tolist(); o.interp_hz[:] = hz.tolist()
                     if dim3:
@@ -238,7 +278,7 @@ class PreparedShots:
     def _fill_source(self, o, q: Source, grid: GridSpec, dt, f0factor, time_integration):
         o.mechanism = {"explosion": L.OWL_SRC_EXPLOSION, "force": L.OWL_SRC_FORCE, "mt": L.OWL_SRC_MT}[q.mechanism]
         o.gx, o.hx, ix, hx = _node(q.x, grid.ox, grid.dx)
-        o.gz, o.hz, iz, hz = _node(q.z, grid.oz, grid.dz)
+        o.gz, o.hz, iz, hz = grid.node_z(q.z)
         o.interp_ix[:] = ix.tolist(); o.interp_hx[:] = hx.tolist()
         o.interp_iz[:] = iz.tolist(); o.interp_hz[:] = hz.tolist()
         if grid.ny > 1:

@@ -13,7 +13,7 @@ from typing import List, Optional, Sequence, Tuple
 import numpy as np
 
 from . import _lib as L
-from .geometry import GridSpec, PreparedShots
+from .geometry import GridSpec, PreparedShots, ZMesh
 
 f32 = np.float32
 
@@ -171,12 +171,13 @@ def elastic_time_integration(mechanism: str) -> int:
     return -1 if mechanism in ("explosion", "mt") else 0
 
 
-def elastic_geometry(shots, desc):
-    """With a free surface, sources above the first grid step (z < dz) are moved
-    to z = dz and their amplitude multiplied by 1.2 (module_vars.f90:466-469)."""
+def elastic_geometry(shots, desc, zmesh=None):
+    """With a free surface, sources above the first row's spacing (z < dz_i(1):
+    dz, or dz / free_surface_dz_refine on the refined mesh) are moved to that
+    depth and their amplitude multiplied by 1.2 (module_vars.f90:463-466)."""
     if not desc.free_surface:
         return shots
-    dz = np.float32(desc.dz)
+    dz = np.float32(desc.dz) if zmesh is None else np.float32(zmesh.at(zmesh.dz_i, 1))
     out = []
     for sh in shots:
         srcs = [replace(q, z=float(dz), amp=float(np.float32(q.amp) * np.float32(1.2))) if np.float32(q.z) < dz else q
@@ -185,13 +186,54 @@ def elastic_geometry(shots, desc):
     return out
 
 
+def mesh_is_refined(desc) -> bool:
+    """A free-surface descriptor whose vertical mesh is not the uniform grid."""
+    rr = desc.free_surface_dz_refine if desc.free_surface_dz_refine > 0 else 1.0
+    cap = desc.dz_max if desc.dz_max > 0 else desc.dz
+    return bool(desc.free_surface) and (rr != 1.0 or cap != desc.dz)
+
+
+def vertical_mesh(desc) -> Optional[ZMesh]:
+    """Rows of the depth-refined free-surface mesh of a descriptor
+    (owl_vertical_mesh), None on the uniform grid."""
+    if not mesh_is_refined(desc):
+        return None
+    lib = L.load()
+    n = C.c_int()
+    L.check(lib.owl_vertical_mesh(C.byref(desc), C.byref(n), None, None, None, None))
+    arr = [np.zeros(n.value + 2 * desc.pml + 2, dtype=f32) for _ in range(4)]
+    L.check(lib.owl_vertical_mesh(C.byref(desc), C.byref(n), *[a.ctypes.data_as(C.c_void_p) for a in arr]))
+    return ZMesh(int(desc.pml), *arr)
+
+
+def free_surface_refine_rows(desc, fields, f0_min: float) -> int:
+    """refine_nz of the refined mesh from the model's surface row and the lowest
+    source f0 (module_vars.f90:315-317); fields as owl_ssg_set_model takes them."""
+    lib = L.load()
+    keep = [np.asfortranarray(np.asarray(f, dtype=f32)) for f in fields]
+    arr = (C.POINTER(C.c_float) * len(keep))()
+    for i, f in enumerate(keep):
+        arr[i] = f.ctypes.data_as(C.POINTER(C.c_float))
+    rows = C.c_int()
+    L.check(lib.owl_free_surface_refine_rows(C.byref(desc), len(keep), arr, float(f0_min), C.byref(rows)))
+    return int(rows.value)
+
+
 class SSGSolver:
-    """One solver handle: grid, PML, time axis and model of one medium."""
+    """One solver handle: grid, PML, time axis and model of one medium.
+
+    Elastic 2D with a free surface may run on the reference's depth-refined
+    vertical mesh: free_surface_dz_refine (rows dz / refine apart at the
+    surface), dz_max (largest spacing) and refine_rows (the reference's
+    refine_nz, free_surface_refine_rows()). The model and the gradient stay on
+    the regular (nz, nx) grid; prepare() places sources and receivers on the
+    mesh rows."""
 
     def __init__(self, medium: int, nx: int, nz: int, dx: float, dz: float, dt: float, nt: int,
                  pml: int = 15, fdhalf: int = 4, free_surface: bool = False, f0_max: float = 20.0,
                  max_shots: int = 1, ny: int = 1, dy: float = 0.0, ox: float = 0.0, oy: float = 0.0,
-                 oz: float = 0.0, allow_dt_adjust: bool = False, aniso: int = 0):
+                 oz: float = 0.0, allow_dt_adjust: bool = False, aniso: int = 0,
+                 free_surface_dz_refine: float = 0.0, dz_max: float = 0.0, refine_rows: int = 0):
         self.lib = L.load()
         d = L.OwlSsgDesc()
         d.medium = medium
@@ -203,8 +245,12 @@ class SSGSolver:
         d.max_shots = max_shots
         d.allow_dt_adjust = int(bool(allow_dt_adjust))
         d.aniso = int(aniso)
+        d.free_surface_dz_refine = float(free_surface_dz_refine)
+        d.dz_max = float(dz_max)
+        d.free_surface_refine_rows = int(refine_rows)
         self.desc = d
-        self.grid = GridSpec(nx=nx, nz=nz, dx=dx, dz=dz, ox=ox, oz=oz, ny=ny, dy=(dy if dy else dx), oy=oy)
+        self.grid = GridSpec(nx=nx, nz=nz, dx=dx, dz=dz, ox=ox, oz=oz, ny=ny, dy=(dy if dy else dx), oy=oy,
+                             zmesh=vertical_mesh(d))
         h = C.c_void_p()
         L.check(self.lib.owl_ssg_create(C.byref(d), C.byref(h)))
         self.h = h
@@ -243,7 +289,7 @@ class SSGSolver:
         shallower than the first grid step move down to it with 1.2 x amplitude
         (src/solver/elastic_vhtiort_2d/module_vars.f90:466-477)."""
         if self.desc.medium in (L.OWL_ELASTIC_VHTIORT_2D, L.OWL_ELASTIC_VHTIORT_3D):
-            shots = elastic_geometry(shots, self.desc)
+            shots = elastic_geometry(shots, self.desc, self.grid.zmesh)
             if time_integration is None:
                 time_integration = elastic_time_integration
         return PreparedShots(shots, self.grid, self.desc.dt, f0factor,

@@ -30,7 +30,7 @@ def test_header_symbols_exported():
 
 def test_queries():
     lib = L.load()
-    assert lib.owl_ssg_abi_version() == 9
+    assert lib.owl_ssg_abi_version() == 10
     assert lib.owl_ssg_nparam(L.OWL_ACOUSTIC_ISO_2D) == 2
     assert lib.owl_ssg_ncomp(L.OWL_ELASTIC_VHTIORT_2D) == 2
     assert lib.owl_ssg_nparam(99) == -1
@@ -45,7 +45,7 @@ def test_queries():
 
 def test_struct_sizes_match_header():
     # ctypes mirrors the C structs field for field (no padding surprises)
-    assert C.sizeof(L.OwlSsgDesc) == 4 * 19
+    assert C.sizeof(L.OwlSsgDesc) == 4 * 22
     assert C.sizeof(L.OwlRunOpts) == 4 * 8
     assert C.sizeof(L.OwlReceiver) == 4 * (6 + 54 + 1)
 

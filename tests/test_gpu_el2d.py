@@ -161,3 +161,109 @@ def test_el2d_lamb_flat_free_surface():
     shape_err = 0.5 * (_shape_misfit(vx[:n], g["ref_t"]) + _shape_misfit(vz[:n], g["ref_n"]))
     print(f"Lamb shape misfit {shape_err:.4f}")
     assert shape_err < 0.20, shape_err
+
+
+# ---------------- depth-refined free-surface mesh (module_vars.f90:313-376) ----------------
+def make_refined(d, fields):
+    s = SSGSolver(L.OWL_ELASTIC_VHTIORT_2D, d.nx, d.nz, d.dx, d.dz, d.dt, d.nt, pml=d.pml, fdhalf=d.fdhalf,
+                  free_surface=True, f0_max=d.f0_max, max_shots=d.max_shots, aniso=d.aniso,
+                  free_surface_dz_refine=d.free_surface_dz_refine, dz_max=d.dz_max,
+                  refine_rows=d.free_surface_refine_rows)
+    s.set_model(*fields)
+    return s
+
+
+@pytest.mark.parametrize("aniso", [L.OWL_ANISO_ISO, L.OWL_ANISO_THOMSEN])
+def test_el2d_refined_forward_parity(aniso):
+    """Refined mesh (rows dz / 4 apart to 20 m, then 2.5 % wider per row up to
+    1.5 dz): CUDA vs the FP32 oracle through one-cell and four-cell kernels."""
+    from test_refined_mesh_cpu import refined_desc, refined_shots
+    d = refined_desc(aniso=aniso, nt=240)
+    f = el_model(aniso)
+    s = make_refined(d, f)
+    ps = s.prepare(refined_shots() * 2)
+    ref = oracle.el2d_forward(d, f, ps, "f32")
+    for opts in (RunOpts(), RunOpts(shots_per_launch=1, use_graph=-1), RunOpts(tile_z=104),
+                 RunOpts(tile_z=102, shots_per_cta=2, use_graph=-1)):
+        got = s.forward(ps, opts)
+        assert rel(got, ref) < FWD_TOL, (opts, rel(got, ref))
+    assert abs(s.dt_stable - oracle.el2d_dt_stable(d, f)) <= 1e-6 * s.dt_stable
+
+
+@pytest.mark.parametrize("aniso", [L.OWL_ANISO_ISO, L.OWL_ANISO_THOMSEN])
+def test_el2d_refined_gradient_parity(aniso):
+    """Refined mesh: CUDA gradient (mesh-cell correlations, the transpose of
+    the row interpolation and the chain rule in FP64 on the regular rows) vs
+    the FP64 exact-adjoint oracle, with a surface force source (moved to
+    dz_i(1)) whose density gradient enters through the mesh cells."""
+    from test_refined_mesh_cpu import refined_desc, refined_shots
+    d = refined_desc(aniso=aniso, nt=200)
+    f = el_model(aniso)
+    s = make_refined(d, f)
+    ps = s.prepare(refined_shots() * 2)
+    obs = oracle.el2d_forward(d, el_model(aniso, seed=2), ps, "f64").astype(np.float32)
+    mref, gref, _ = oracle.el2d_gradient(d, f, ps, obs, adj_kind=L.OWL_ADJ_L2_RESIDUAL, k=7)
+    for opts in (RunOpts(checkpoint_interval=7), RunOpts(checkpoint_interval=7, shots_per_launch=1, use_graph=-1),
+                 RunOpts(checkpoint_interval=7, tile_z=104, shots_per_cta=2)):
+        misfit, g = s.gradient(ps, obs, opts=opts)
+        assert rel(g, gref) < GRAD_TOL, (opts, rel(g, gref))
+        assert np.allclose(misfit, mref, rtol=1e-4)
+
+
+def test_el2d_refined_source_gradient_parity():
+    from test_refined_mesh_cpu import refined_desc, refined_shots
+    d = refined_desc(nt=160)
+    f = el_model(L.OWL_ANISO_ISO)
+    s = make_refined(d, f)
+    ps = s.prepare(refined_shots())
+    rng = np.random.default_rng(5)
+    adj = rng.standard_normal(s.seis_size(ps)).astype(np.float32)
+    _, _, sref = oracle.el2d_gradient(d, f, ps, adj, adj_kind=L.OWL_ADJ_GIVEN, k=7, stf_grad=True)
+    got = s.source_gradient(ps, adj, RunOpts(checkpoint_interval=7))
+    assert rel(got, sref) < GRAD_TOL, rel(got, sref)
+
+
+def test_el2d_lamb_refined_mesh_10m():
+    """The reference's elastic free-surface test at its own configuration
+    (test/test_elastic_lamb.py, flat surface): 10 m cells, 121 x 241 cells,
+    15-cell PML, dt 0.2 ms, the depth-refined mesh with refine factor 4 and
+    dz_max 1.5 dz, refine_nz from the surface row and the source f0
+    (module_vars.f90:315-317). Vertical force at the surface, surface
+    receivers 150 .. 550 m away, vx / vz against the reference's own
+    discrete-wavenumber Lamb solution (tests/golden/lamb_flat.npz) by the
+    test's per-trace shape misfit, which the reference passes below 0.20."""
+    import os
+    from owl_b200.geometry import Receiver, Shot, Source
+    from owl_b200.solver import free_surface_refine_rows
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "lamb_flat.npz"))
+    h, pml, dt = 10.0, 15, float(g["dt"])
+    nx, nz = 121, 241
+    nt = int(round(float(g["tmax"]) / dt)) + 1
+    d = L.OwlSsgDesc()
+    d.medium = L.OWL_ELASTIC_VHTIORT_2D
+    d.nx, d.ny, d.nz = nx, 1, nz
+    d.dx = d.dy = d.dz = h
+    d.pml, d.fdhalf, d.free_surface = pml, 4, 1
+    d.dt, d.nt, d.f0_max, d.max_shots = dt, nt, float(g["f0"]), 1
+    d.aniso = L.OWL_ANISO_ISO
+    d.free_surface_dz_refine, d.dz_max = 4.0, 1.5 * h
+    full = lambda v: np.full((nz, nx), v, dtype=np.float32)
+    model = [full(g["vp"]), full(g["vs"]), full(g["rho"])]
+    d.free_surface_refine_rows = free_surface_refine_rows(d, model, float(g["f0"]))
+    assert d.free_surface_refine_rows == 5  # ceil(0.5 * 1732 / 20 / 10)
+    s = make_refined(d, model)
+    xs = 250.0
+    offsets = g["offsets"]
+    shot = Shot(1, [Source(x=xs, z=0.0, mechanism="force", polar=0.0, f0=float(g["f0"]), amp=1.0e6)],
+                [Receiver(x=xs + float(r), z=0.0) for r in offsets])
+    ps = s.prepare([shot])
+    seis = s.forward(ps, RunOpts())
+    step = int(round(float(g["data_dt"]) / dt))
+    gather = s.split(ps, seis)[0]
+    vx = gather[0][:, ::step].T.astype(np.float64)
+    vz = gather[1][:, ::step].T.astype(np.float64)
+    n = g["ref_n"].shape[0]
+    assert vx.shape[0] >= n
+    shape_err = 0.5 * (_shape_misfit(vx[:n], g["ref_t"]) + _shape_misfit(vz[:n], g["ref_n"]))
+    print(f"Lamb shape misfit on the refined 10 m mesh {shape_err:.4f}")
+    assert shape_err < 0.20, shape_err
