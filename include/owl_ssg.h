@@ -170,10 +170,10 @@ typedef struct {
     int max_shots;       /* capacity of one batched launch (>= 1) */
     int allow_dt_adjust; /* 0: dt above the CFL bound is OWL_ERR_UNSTABLE */
     int aniso;           /* OWL_ANISO_*: model parameterisation of elastic media */
-    /* Depth-refined vertical mesh of the elastic 2D solver with a free surface
-     * (free_surface_dz_refine and dz_max of wave_solver_elastic_vhtiort_2d,
+    /* Depth-refined vertical mesh of the elastic solvers with a free surface
+     * (free_surface_dz_refine and dz_max of wave_solver_elastic_vhtiort_2d / _3d,
      * elastic_vhtiort_2d/interface.f90:61-62; prepare_modeling,
-     * module_vars.f90:313-376): rows dz / free_surface_dz_refine apart from the
+     * module_vars.f90:313-376, 3D :424-490): rows dz / free_surface_dz_refine apart from the
      * surface down to (free_surface_refine_rows - 1) dz, then 2.5 % wider per
      * row up to dz_max. The model, the gradient and the geometry's x / z stay on
      * the regular (nz, nx) grid; owl_vertical_mesh gives the computational rows
@@ -501,13 +501,14 @@ float owl_mpml_damp_ratio(const float *c, int axis);
  * high: (nz + 2 pml) x (ny + 2 pml), y fastest), front, back (y: (nz + 2 pml) x
  * (nx + 2 pml), x fastest), top, bottom (z: (ny + 2 pml) x (nx + 2 pml), x
  * fastest), concatenated; index 0 of each axis is the reference's -pml + 1.
- * With a free surface the x / y faces hold zeros above row 1. */
+ * With a free surface the x / y faces hold zeros above row 1. On the
+ * depth-refined free-surface mesh nz is the mesh's planes (owl_vertical_mesh). */
 int owl_ssg_mpml_ratios(const owl_ssg *h, float *faces);
 
 /* ---- queries ------------------------------------------------------------ */
 
 /* Vertical mesh of a descriptor (host only, no device needed): the
- * computational rows of the elastic 2D solver with a free surface
+ * computational rows of the elastic solvers with a free surface
  * (module_vars.f90:313-376). nz_mesh gets the number of rows (desc->nz for the
  * uniform grid); each non-null array gets nz_mesh + 2 pml + 2 values, rows
  * -pml .. nz_mesh + pml + 1 of the reference's zz_i, zz_h, dz_i, dz_h (depths
@@ -520,7 +521,9 @@ int owl_ssg_mpml_ratios(const owl_ssg *h, float *faces);
 int owl_vertical_mesh(const owl_ssg_desc *desc, int *nz_mesh, float *z_i, float *z_h, float *dz_i, float *dz_h);
 /* refine_nz of the refined mesh (module_vars.f90:315-317): ceil(0.5 lambda / dz)
  * with lambda = sqrt(mean over the padded surface row of c55 / rho) / f0_min,
- * c55 and rho of the model in desc->aniso's parameterisation (elastic 2D),
+ * c55 and rho of the model in desc->aniso's parameterisation (elastic 2D;
+ * elastic 3D: the largest of the means of c44 / rho, c55 / rho, c66 / rho over
+ * the padded surface plane, elastic_vhtiort_3d/module_vars.f90:424-428),
  * f0_min the lowest peak frequency of the sources. Host only. */
 int owl_free_surface_refine_rows(const owl_ssg_desc *desc, int nparam, const float *const *fields, float f0_min,
                                  int *refine_rows);

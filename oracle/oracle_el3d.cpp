@@ -9,10 +9,13 @@
 //                                src/solver/elastic_vhtiort_3d/module_wavefield.f90:52-537
 //   add_source                   src/solver/elastic_vhtiort_3d/module_wavefield.f90:1095-1333
 //   sampling                     src/solver/elastic_vhtiort_3d/submodule_forward_modeling.f90:82-145
-//   update_wavefield_free_surface (flat free surface on the uniform grid,
-//   free_surface_dz_refine = 1): zero velocities above the surface, the row-1
-//   traction condition pdzvz = -c13/c33 pdxvx - c23/c33 pdyvy, sigma_zz(1) = 0
-//   and the odd stress images      module_wavefield.f90:549-1090
+//   update_wavefield_free_surface (flat free surface): zero velocities above
+//   the surface, the row-1 traction condition pdzvz = -c13/c33 pdxvx - c23/c33
+//   pdyvy, sigma_zz(1) = 0 and the odd stress images; on the uniform grid or
+//   the depth-refined mesh (Cij interpolated linearly to the mesh planes, z
+//   derivatives scaled by dz / dz_i or dz / dz_h, the z PML and the explosion
+//   source on the plane's own dz_i)
+//                                  module_wavefield.f90:549-1090, module_vars.f90:419-490
 //   surface images before sampling submodule_forward_modeling.f90:66-82
 //   sources above row 2 skipped    module_wavefield.f90:1107-1315
 // plus the exact discrete adjoint and the chain rule to the model parameters.
@@ -131,9 +134,11 @@ void el3_cij(int aniso, const T* p, T* c) {
 
 // 1D damping profile of one axis (module_cfspml.f90:517-600): d and alpha at
 // integer (i) and half (h) positions over [-pml+1, n+pml]
+// (zm: the per-row spacing dz_i(k) of the refined free-surface mesh,
+// module_cfspml.f90:581-582 of the 3D solver)
 struct Prof3 {
     Arr1<float> di, dh, ai, ah;
-    void build(int n, int pml, float d, float pmlvp, float alphamax) {
+    void build(int n, int pml, float d, float pmlvp, float alphamax, const ZMesh* zm = nullptr) {
         di.init(-pml + 1, n + pml, 0.f); dh.init(-pml + 1, n + pml, 0.f);
         ai.init(-pml + 1, n + pml, alphamax); ah.init(-pml + 1, n + pml, alphamax);
         const float R0 = 1.0e-5f;
@@ -148,7 +153,8 @@ struct Prof3 {
             } else {
                 continue;
             }
-            const float c0 = std::log(1.0f / R0) * 3.0f * pmlvp / (2.0f * (float)pml * d);
+            const float dd = zm && zm->refined ? zm->dzi(i) : d;
+            const float c0 = std::log(1.0f / R0) * 3.0f * pmlvp / (2.0f * (float)pml * dd);
             di(i) = c0 * (nd * nd);
             dh(i) = c0 * (ndh * ndh);
             ai(i) = std::max(alphamax * (1.0f - nd), 0.25f * alphamax);
@@ -186,38 +192,59 @@ static std::vector<float> g_el3_faces;
 template <typename T>
 struct El3 {
     int nx, ny, nz, P, R, nt, aniso, np;
+    int nzm;                  // regular (model) planes; nz: the mesh's planes
     bool fs;
     float dx, dy, dz, dt, idx, idy, idz;
     const float* c;
-    E3<T> C[10];              // c11 c12 c13 c22 c23 c33 c44 c55 c66 rho, padded by pml+1
+    ZMesh zm;
+    ZLinear zl;
+    E3<T> C[10];              // c11 c12 c13 c22 c23 c33 c44 c55 c66 rho, padded by pml+1, mesh planes
     E3<T> c44e, c55e, c66e;   // harmonic shear moduli at the shear-stress nodes
-    std::vector<E3<T>> par;
+    std::vector<E3<T>> par;   // model parameters, regular planes
     Prof3 px, py, pz;
     int lo[3], hi[3];
     float dt_stable = 0;
 
     El3(const owl_ssg_desc& d, const T* const* fields) {
-        nx = d.nx; ny = d.ny; nz = d.nz; P = d.pml; R = d.fdhalf; nt = d.nt; aniso = d.aniso;
+        nx = d.nx; ny = d.ny; nzm = d.nz; P = d.pml; R = d.fdhalf; nt = d.nt; aniso = d.aniso;
         dx = d.dx; dy = d.dy; dz = d.dz; dt = d.dt;
         fs = d.free_surface != 0;
         np = el3_nparam(aniso);
         if (np < 0) throw std::runtime_error("bad aniso");
         idx = (float)(1.0 / (double)dx); idy = (float)(1.0 / (double)dy); idz = (float)(1.0 / (double)dz);
         c = fdcoefs(R);
-        for (auto& x : C) x.init(-P, nx + P + 1, -P, ny + P + 1, -P, nz + P + 1);
+        zm = zmesh_build(d);
+        nz = zm.n;
+        if (zm.refined) zl = zlinear_build(zm, nzm, dz);
+        // Cij of the regular padded planes
+        E3<T> Cr[10];
+        for (auto& x : Cr) x.init(-P, nx + P + 1, -P, ny + P + 1, -P, nzm + P + 1);
         par.resize(np);
-        for (auto& x : par) x.init(-P, nx + P + 1, -P, ny + P + 1, -P, nz + P + 1);
-        for (int k = -P; k <= nz + P + 1; ++k)
+        for (auto& x : par) x.init(-P, nx + P + 1, -P, ny + P + 1, -P, nzm + P + 1);
+        for (int k = -P; k <= nzm + P + 1; ++k)
             for (int j = -P; j <= ny + P + 1; ++j)
                 for (int i = -P; i <= nx + P + 1; ++i) {
                     const int ii = std::min(std::max(i, 1), nx), jj = std::min(std::max(j, 1), ny),
-                              kk = std::min(std::max(k, 1), nz);
-                    const size_t src = ((size_t)(ii - 1) * ny + (jj - 1)) * nz + (kk - 1);
+                              kk = std::min(std::max(k, 1), nzm);
+                    const size_t src = ((size_t)(ii - 1) * ny + (jj - 1)) * nzm + (kk - 1);
                     T p[10], o[10];
                     for (int q = 0; q < np; ++q) p[q] = par[q](i, j, k) = fields[q][src];
                     el3_cij(aniso, p, o);
-                    for (int q = 0; q < 10; ++q) C[q](i, j, k) = o[q];
+                    for (int q = 0; q < 10; ++q) Cr[q](i, j, k) = o[q];
                 }
+        // the mesh's planes (map_regular_to_irregular, module_vars.f90:164-180)
+        for (auto& x : C) x.init(-P, nx + P + 1, -P, ny + P + 1, -P, nz + P + 1);
+        for (int k = -P; k <= nz + P + 1; ++k)
+            for (int j = -P; j <= ny + P + 1; ++j)
+                for (int i = -P; i <= nx + P + 1; ++i)
+                    for (int q = 0; q < 10; ++q) {
+                        if (!zm.refined) {
+                            C[q](i, j, k) = Cr[q](i, j, k);
+                            continue;
+                        }
+                        const int k0 = zl.j0(k);
+                        C[q](i, j, k) = Cr[q](i, j, k0) + T(zl.w(k)) * (Cr[q](i, j, k0 + 1) - Cr[q](i, j, k0));
+                    }
         c44e.init(-P + 1, nx + P, -P + 1, ny + P, -P + 1, nz + P);
         c55e.init(-P + 1, nx + P, -P + 1, ny + P, -P + 1, nz + P);
         c66e.init(-P + 1, nx + P, -P + 1, ny + P, -P + 1, nz + P);
@@ -234,26 +261,45 @@ struct El3 {
                     c66e(i, j, k) = T(4) / (T(1) / a66(i - 1, j - 1, k) + T(1) / a66(i, j - 1, k) + T(1) / a66(i - 1, j, k) +
                                             T(1) / a66(i, j, k));
                 }
-        // pmlvp over the six faces (module_vars.f90:384-406) and dt_stable (:534-537)
+        // pmlvp over the six faces of the regular model (module_vars.f90:384-406)
+        // and dt_stable (:500-537; on the refined mesh the least over the
+        // cells, each with its plane's smaller spacing)
         float pv = -1e30f, maxv = 0.f;
         auto rr = [&](int q, int i, int j, int k) { return (float)re(C[q](i, j, k)) / (float)re(C[9](i, j, k)); };
-        for (int k = 1; k <= nz; ++k)
+        for (int k = 1; k <= nzm; ++k)
             for (int j = 1; j <= ny; ++j)
                 for (int i = 1; i <= nx; ++i) {
-                    const bool face = i == 1 || i == nx || j == 1 || j == ny || k == 1 || k == nz;
-                    for (int q : {0, 3, 5}) {
-                        if (face) pv = std::max(pv, rr(q, i, j, k));
-                        maxv = std::max(maxv, std::sqrt(rr(q, i, j, k)));
-                    }
+                    const bool face = i == 1 || i == nx || j == 1 || j == ny || k == 1 || k == nzm;
+                    if (face)
+                        for (int q : {0, 3, 5}) pv = std::max(pv, (float)re(Cr[q](i, j, k)) / (float)re(Cr[9](i, j, k)));
                 }
         const float pmlvp = std::sqrt(pv);
         float temp = 0.f;
         for (int q = 0; q < R; ++q) temp += std::fabs(c[q]);
-        dt_stable = 1.0f / (temp * maxv * std::sqrt(1.0f / (dx * dx) + 1.0f / (dy * dy) + 1.0f / (dz * dz)));
+        if (!zm.refined) {
+            for (int k = 1; k <= nz; ++k)
+                for (int j = 1; j <= ny; ++j)
+                    for (int i = 1; i <= nx; ++i)
+                        for (int q : {0, 3, 5}) maxv = std::max(maxv, std::sqrt(rr(q, i, j, k)));
+            dt_stable = 1.0f / (temp * maxv * std::sqrt(1.0f / (dx * dx) + 1.0f / (dy * dy) + 1.0f / (dz * dz)));
+        } else {
+            float best = 3.0e38f;
+            for (int k = 1; k <= nz; ++k) {
+                const float h = std::min(zm.dzi(k), zm.dzh(k));
+                for (int j = 1; j <= ny; ++j)
+                    for (int i = 1; i <= nx; ++i) {
+                        const float mv = std::max({std::sqrt(rr(0, i, j, k)), std::sqrt(rr(3, i, j, k)),
+                                                   std::sqrt(rr(5, i, j, k))});
+                        best = std::min(best, 1.0f / (temp * mv * std::sqrt(1.0f / (dx * dx) + 1.0f / (dy * dy) +
+                                                                             1.0f / (h * h))));
+                    }
+            }
+            dt_stable = best;
+        }
         const float alphamax = (float)(1.0 * (double)d.f0_max * 3.14159265358979323846);
         px.build(nx, P, dx, pmlvp, alphamax);
         py.build(ny, P, dy, pmlvp, alphamax);
-        pz.build(nz, P, dz, pmlvp, alphamax);
+        pz.build(nz, P, dz, pmlvp, alphamax, &zm);
         const long long fx = (long long)(ny + 2 * P) * (nz + 2 * P), fy = (long long)(nx + 2 * P) * (nz + 2 * P),
                         fz = (long long)(nx + 2 * P) * (ny + 2 * P);
         if (g_el3_faces.size() == (size_t)(2 * (fx + fy + fz))) {
@@ -303,6 +349,10 @@ struct El3 {
         auto out = [](int v, int n, bool h) { return h ? (v <= 1 || v >= n + 1) : (v <= 0 || v >= n + 1); };
         return out(i, nx, hx) || out(j, ny, hy) || out(k, nz, hz);
     }
+
+    // dz scalings of the z derivatives at integer / half planes (1 on the uniform grid)
+    T zsi(int k) const { return zm.refined ? T(zm.si(k)) : T(1); }
+    T zsh(int k) const { return zm.refined ? T(zm.sh(k)) : T(1); }
 
     // stencils of pattern P (f(x+q) - f(x+1-q)) and M (f(x+q-1) - f(x-q)) along an axis
     T stP(const E3<T>& f, int i, int j, int k, int ax) const {
@@ -392,7 +442,7 @@ struct El3 {
                 }
                 dZ = -(C[2](i, j, k) / C[5](i, j, k)) * dX - (C[4](i, j, k) / C[5](i, j, k)) * dY;
             } else {
-                dZ = T(idz) * stP(s.f[F_VZ], i, j, k, 2);
+                dZ = T(idz) * stP(s.f[F_VZ], i, j, k, 2) * zsi(k);
                 if (shell(i, j, k, false, false, false)) {
                     float ca, cb;
                     coef(0, i, j, k, false, false, false, ca, cb); dX = pml_f(dX, ca, cb, s.m[M_XVX](i, j, k));
@@ -407,7 +457,7 @@ struct El3 {
         }, kmin(F_XX));
         // syz at (i, j-1/2, k-1/2) (:171-221)
         each([&](int i, int n, int p) {
-            T dzvy = T(idz) * stM(s.f[F_VY], i, n, p, 2), dyvz = T(idy) * stM(s.f[F_VZ], i, n, p, 1);
+            T dzvy = T(idz) * stM(s.f[F_VY], i, n, p, 2) * zsh(p), dyvz = T(idy) * stM(s.f[F_VZ], i, n, p, 1);
             if (shell(i, n, p, false, true, true)) {
                 float ca, cb;
                 coef(1, i, n, p, false, true, true, ca, cb); dyvz = pml_f(dyvz, ca, cb, s.m[M_YVZ](i, n, p));
@@ -418,7 +468,7 @@ struct El3 {
         }, kmin(F_YZ));
         // sxz at (i-1/2, j, k-1/2) (:228-278)
         each([&](int m, int j, int p) {
-            T dzvx = T(idz) * stM(s.f[F_VX], m, j, p, 2), dxvz = T(idx) * stM(s.f[F_VZ], m, j, p, 0);
+            T dzvx = T(idz) * stM(s.f[F_VX], m, j, p, 2) * zsh(p), dxvz = T(idx) * stM(s.f[F_VZ], m, j, p, 0);
             if (shell(m, j, p, true, false, true)) {
                 float ca, cb;
                 coef(0, m, j, p, true, false, true, ca, cb); dxvz = pml_f(dxvz, ca, cb, s.m[M_XVZ](m, j, p));
@@ -456,7 +506,7 @@ struct El3 {
         // vx at (i-1/2, j, k) (:350-410)
         each([&](int m, int j, int k) {
             T hx = T(idx) * stM(s.f[F_XX], m, j, k, 0), hy = T(idy) * stP(s.f[F_XY], m, j, k, 1),
-              hz = T(idz) * stP(s.f[F_XZ], m, j, k, 2);
+              hz = T(idz) * stP(s.f[F_XZ], m, j, k, 2) * zsi(k);
             if (shell(m, j, k, true, false, false)) {
                 float ca, cb;
                 coef(0, m, j, k, true, false, false, ca, cb); hx = pml_f(hx, ca, cb, s.m[M_XXX](m, j, k));
@@ -470,7 +520,7 @@ struct El3 {
         // vy at (i, j-1/2, k) (:416-476)
         each([&](int i, int n, int k) {
             T hx = T(idx) * stP(s.f[F_XY], i, n, k, 0), hy = T(idy) * stM(s.f[F_YY], i, n, k, 1),
-              hz = T(idz) * stP(s.f[F_YZ], i, n, k, 2);
+              hz = T(idz) * stP(s.f[F_YZ], i, n, k, 2) * zsi(k);
             if (shell(i, n, k, false, true, false)) {
                 float ca, cb;
                 coef(0, i, n, k, false, true, false, ca, cb); hx = pml_f(hx, ca, cb, s.m[M_XXY](i, n, k));
@@ -484,7 +534,7 @@ struct El3 {
         // vz at (i, j, k-1/2) (:482-542)
         each([&](int i, int j, int p) {
             T hx = T(idx) * stP(s.f[F_XZ], i, j, p, 0), hy = T(idy) * stP(s.f[F_YZ], i, j, p, 1),
-              hz = T(idz) * stM(s.f[F_ZZ], i, j, p, 2);
+              hz = T(idz) * stM(s.f[F_ZZ], i, j, p, 2) * zsh(p);
             if (shell(i, j, p, false, false, true)) {
                 float ca, cb;
                 coef(0, i, j, p, false, false, true, ca, cb); hx = pml_f(hx, ca, cb, s.m[M_XXZ](i, j, p));
@@ -518,7 +568,8 @@ struct El3 {
                                          T(std::cos(q.polar)) / r * T(ix[a]) * T(iy[b]) * T(hz[cc]));
                     } else {
                         const bool mt = q.mechanism == OWL_SRC_MT;
-                        const T inv = T(1) / (T(dx) * T(dy) * T(dz));
+                        // dz_s: the local spacing dz_i(gz) on the refined mesh (module_wavefield.f90:1107-1111)
+                        const T inv = T(1) / (T(dx) * T(dy) * T(zm.refined ? zm.dzi(q.gz) : dz));
                         const T w = T(ix[a]) * T(iy[b]) * T(iz[cc]);
                         out.emplace_back(F_XX, q.gx + irx, q.gy + iry, q.gz + irz, -inv * T(mt ? q.mt[0] : 1.f) * w);
                         out.emplace_back(F_YY, q.gx + irx, q.gy + iry, q.gz + irz, -inv * T(mt ? q.mt[1] : 1.f) * w);
@@ -641,7 +692,7 @@ struct El3 {
                 coef(1, i, j, k, hxh, hyh, hzh, ca, cb); ey = pml_e(q, ca, cb, a.m[my](i, j, k));
                 coef(2, i, j, k, hxh, hyh, hzh, ca, cb); ez = pml_e(q, ca, cb, a.m[mz](i, j, k));
             }
-            return std::array<T, 3>{T(idx) * ex, T(idy) * ey, T(idz) * ez};
+            return std::array<T, 3>{T(idx) * ex, T(idy) * ey, T(idz) * (hzh ? zsh(k) : zsi(k)) * ez};
         };
         for (int k = kmin(F_VX); k <= nz + P; ++k)
             for (int j = -P + 1; j <= ny + P; ++j)
@@ -704,9 +755,10 @@ struct El3 {
                 coef(ax1, i, j, k, hh[0], hh[1], hh[2], ca, cb); e1 = pml_e(q, ca, cb, a.m[m1](i, j, k));
                 coef(ax2, i, j, k, hh[0], hh[1], hh[2], ca, cb); e2 = pml_e(q, ca, cb, a.m[m2](i, j, k));
             }
-            const float id[3] = {idx, idy, idz};
-            scM(a.f[fa], i, j, k, ax1, T(id[ax1]) * e1);
-            scM(a.f[fb], i, j, k, ax2, T(id[ax2]) * e2);
+            // (the z derivatives of the shear nodes sit at half planes)
+            const T id[3] = {T(idx), T(idy), T(idz) * zsh(k)};
+            scM(a.f[fa], i, j, k, ax1, id[ax1] * e1);
+            scM(a.f[fb], i, j, k, ax2, id[ax2] * e2);
         };
         for (int k = kmin(F_XY); k <= nz + P; ++k)
             for (int j = -P + 1; j <= ny + P; ++j)
@@ -768,7 +820,7 @@ struct El3 {
                     }
                     scP(a.f[F_VX], i, j, k, 0, T(idx) * qx);
                     scP(a.f[F_VY], i, j, k, 1, T(idy) * qy);
-                    scP(a.f[F_VZ], i, j, k, 2, T(idz) * qz);
+                    scP(a.f[F_VZ], i, j, k, 2, T(idz) * zsi(k) * qz);
                 }
         clear_outside(a);
         // sampling of step t
@@ -839,11 +891,32 @@ struct El3 {
         }
     }
 
+    // (on the refined mesh first the transpose of the depth interpolation, from
+    // the mesh planes to the regular planes)
     void chain(Grad& g) const {
         typedef std::complex<double> Cx;
+        std::vector<E3<T>> rg;
+        const E3<T>* src[10];
+        for (int r = 0; r < 10; ++r) src[r] = &g.g[r];
+        if (zm.refined) {
+            rg.resize(10);
+            for (auto& x : rg) x.init(-P, nx + P + 1, -P, ny + P + 1, -P, nzm + P + 1);
+            for (int f = -P; f <= nz + P + 1; ++f) {
+                const int k0 = zl.j0(f);
+                const T w = T(zl.w(f));
+                for (int r = 0; r < 10; ++r)
+                    for (int j = -P; j <= ny + P + 1; ++j)
+                        for (int i = -P; i <= nx + P + 1; ++i) {
+                            const T v = g.g[r](i, j, f);
+                            rg[r](i, j, k0) = rg[r](i, j, k0) + (T(1) - w) * v;
+                            rg[r](i, j, k0 + 1) = rg[r](i, j, k0 + 1) + w * v;
+                        }
+            }
+            for (int r = 0; r < 10; ++r) src[r] = &rg[r];
+        }
         g.gpar.assign(np, E3<T>());
-        for (auto& x : g.gpar) x.init(-P, nx + P + 1, -P, ny + P + 1, -P, nz + P + 1);
-        for (int k = -P; k <= nz + P + 1; ++k)
+        for (auto& x : g.gpar) x.init(-P, nx + P + 1, -P, ny + P + 1, -P, nzm + P + 1);
+        for (int k = -P; k <= nzm + P + 1; ++k)
             for (int j = -P; j <= ny + P + 1; ++j)
                 for (int i = -P; i <= nx + P + 1; ++i)
                     for (int q = 0; q < np; ++q) {
@@ -851,19 +924,19 @@ struct El3 {
                         for (int r = 0; r < np; ++r) p[r] = Cx(re(par[r](i, j, k)), r == q ? 1e-30 : 0.0);
                         el3_cij(aniso, p, o);
                         T acc = T(0);
-                        for (int r = 0; r < 10; ++r) acc = acc + g.g[r](i, j, k) * T(o[r].imag() / 1e-30);
+                        for (int r = 0; r < 10; ++r) acc = acc + (*src[r])(i, j, k) * T(o[r].imag() / 1e-30);
                         g.gpar[q](i, j, k) = acc;
                     }
     }
 
     void fold(const E3<T>& gp, T* out) const {
-        std::fill(out, out + (size_t)nx * ny * nz, T(0));
-        for (int k = -P; k <= nz + P + 1; ++k)
+        std::fill(out, out + (size_t)nx * ny * nzm, T(0));
+        for (int k = -P; k <= nzm + P + 1; ++k)
             for (int j = -P; j <= ny + P + 1; ++j)
                 for (int i = -P; i <= nx + P + 1; ++i) {
                     const int ii = std::min(std::max(i, 1), nx), jj = std::min(std::max(j, 1), ny),
-                              kk = std::min(std::max(k, 1), nz);
-                    out[((size_t)(ii - 1) * ny + (jj - 1)) * nz + (kk - 1)] += gp(i, j, k);
+                              kk = std::min(std::max(k, 1), nzm);
+                    out[((size_t)(ii - 1) * ny + (jj - 1)) * nzm + (kk - 1)] += gp(i, j, k);
                 }
     }
 };

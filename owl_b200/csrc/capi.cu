@@ -130,9 +130,10 @@ int owl_free_surface_refine_rows(const owl_ssg_desc* desc, int nparam, const flo
     return guarded([&] {
         OWL_CHECK(desc && fields && refine_rows, OWL_ERR_INVALID, "null argument");
         OWL_CHECK(f0_min > 0, OWL_ERR_INVALID, "f0_min must be positive");
-        OWL_CHECK(desc->medium == OWL_ELASTIC_VHTIORT_2D, OWL_ERR_UNSUPPORTED,
-                  "the refined free-surface mesh is built for the elastic 2D medium");
-        *refine_rows = el2d_refine_rows(*desc, nparam, fields, f0_min);
+        OWL_CHECK(desc->medium == OWL_ELASTIC_VHTIORT_2D || desc->medium == OWL_ELASTIC_VHTIORT_3D,
+                  OWL_ERR_UNSUPPORTED, "the refined free-surface mesh belongs to the elastic media");
+        *refine_rows = desc->medium == OWL_ELASTIC_VHTIORT_2D ? el2d_refine_rows(*desc, nparam, fields, f0_min)
+                                                              : el3d_refine_rows(*desc, nparam, fields, f0_min);
     });
 }
 

@@ -44,6 +44,7 @@
 #include "mpml.cuh"
 #include "ring.cuh"
 #include "ssg_base.cuh"
+#include "vmesh.hpp"
 
 namespace owl {
 
@@ -81,6 +82,11 @@ struct El3dDev {
     const float *c11, *c12, *c13, *c22, *c23, *c33, *c44e, *c55e, *c66e, *bx, *by, *bz;
     // per axis: a and b at integer and half positions (storage index)
     const float *axi, *bxi, *axh, *bxh, *ayi, *byi, *ayh, *byh, *azi, *bzi, *azh, *bzh;
+    // per storage plane: dz / dz_i and dz / dz_h of the depth-refined free-surface
+    // mesh, the factors of the z derivatives at integer-z nodes (normal stresses,
+    // sxy, vx, vy) and half-z nodes (syz, sxz, vz); 1 on the uniform grid. Read
+    // by the per-cell kernels (the ring kernels run without a free surface).
+    const float *zfi, *zfh;
     float* st;
     float* S;
     long long sslot, sterm;
@@ -251,6 +257,8 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_s(El3dDev a) {
     const float c11 = __ldg(a.c11 + o), c12 = __ldg(a.c12 + o), c13 = __ldg(a.c13 + o), c22 = __ldg(a.c22 + o),
                 c23 = __ldg(a.c23 + o), c33 = __ldg(a.c33 + o);
     const float g44 = a.dt * __ldg(a.c44e + o), g55 = a.dt * __ldg(a.c55e + o), g66 = a.dt * __ldg(a.c66e + o);
+    // 1/dz times the plane's dz scaling (1/dz exactly on the uniform grid)
+    const float zsi = a.idz * __ldg(a.zfi + z), zsh = a.idz * __ldg(a.zfh + z);
     const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
     // free surface: row 1, whether the half-depth stresses exist at this row,
@@ -295,7 +303,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_s(El3dDev a) {
         if (row1) {
             dZ = -(c13 / c33) * dX - (c23 / c33) * dY;
         } else {
-            dZ = a.idz * stP<R>(vz, sz);
+            dZ = zsi * stP<R>(vz, sz);
             if (p2) dZ = pml_up(dZ, MP ? ca[2] : azi, MP ? e3_cb<E3_PERM_S>(a, o, 0, 2) : bzi, m2, m + N_ZVZ * a.fs);
         }
         st[E3_XX * a.fs + o] = xx0 + a.dt * (c11 * dX + c12 * dY + c13 * dZ);
@@ -310,7 +318,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_s(El3dDev a) {
         float dzvy = 0.f, dyvz = 0.f, dzvx = 0.f, dxvz = 0.f;
         if (hz_ok) {
             // syz: dz vy + dy vz
-            dzvy = a.idz * stM<R>(vy, sz);
+            dzvy = zsh * stM<R>(vy, sz);
             dyvz = a.idy * stM<R>(vz, sy);
             if (p3) dyvz = pml_up(dyvz, MP ? ca[3] : ayh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 3) : byh, m3, m + N_YVZ * a.fs);
             if (p4) dzvy = pml_up(dzvy, MP ? ca[4] : azh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 4) : bzh, m4, m + N_ZVY * a.fs);
@@ -318,7 +326,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_s(El3dDev a) {
             st[E3_YZ * a.fs + o] = yzn;
             if (mir) st[E3_YZ * a.fs + o + dsh] = -yzn;
             // sxz: dz vx + dx vz
-            dzvx = a.idz * stM<R>(vx, sz);
+            dzvx = zsh * stM<R>(vx, sz);
             dxvz = a.idx * stM<R>(vz, 1);
             if (p5) dxvz = pml_up(dxvz, MP ? ca[5] : axh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 5) : bxh, m5, m + N_XVZ * a.fs);
             if (p6) dzvx = pml_up(dzvx, MP ? ca[6] : azh, MP ? e3_cb<E3_PERM_S>(a, o, 0, 6) : bzh, m6, m + N_ZVX * a.fs);
@@ -365,6 +373,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_v(El3dDev a) {
     const float ayi = a.ayi[y], byi = a.byi[y], ayh = a.ayh[y], byh = a.byh[y];
     const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
     const float bx = __ldg(a.bx + o), by = __ldg(a.by + o), bz = __ldg(a.bz + o);
+    const float zsi = a.idz * __ldg(a.zfi + z), zsh = a.idz * __ldg(a.zfh + z);  // see k_el3d_fwd_s
     const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
     for (int s = s0; s < s1; ++s) {
@@ -389,14 +398,14 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_v(El3dDev a) {
         const float m3 = p3 ? m[N_XXY * a.fs] : 0.f, m4 = p4 ? m[N_YYY * a.fs] : 0.f, m5 = p5 ? m[N_ZYZ * a.fs] : 0.f;
         const float m6 = p6 ? m[N_XXZ * a.fs] : 0.f, m7 = p7 ? m[N_YYZ * a.fs] : 0.f, m8 = p8 ? m[N_ZZZ * a.fs] : 0.f;
         // vx: dx sxx (M) + dy sxy (P) + dz sxz (P)
-        float h1 = a.idx * stM<R>(sxx, 1), h2 = a.idy * stP<R>(sxy, sy), h3 = a.idz * stP<R>(sxz, sz);
+        float h1 = a.idx * stM<R>(sxx, 1), h2 = a.idy * stP<R>(sxy, sy), h3 = zsi * stP<R>(sxz, sz);
         if (p0) h1 = pml_up(h1, MP ? ca[0] : axh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 0) : bxh, m0, m + N_XXX * a.fs);
         if (p1) h2 = pml_up(h2, MP ? ca[1] : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 1) : byi, m1, m + N_YXY * a.fs);
         if (p2) h3 = pml_up(h3, MP ? ca[2] : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 2) : bzi, m2, m + N_ZXZ * a.fs);
         const float hx = h1 + h2 + h3;
         st[E3_VX * a.fs + o] = vx0 + bx * hx;
         // vy: dx sxy (P) + dy syy (M) + dz syz (P)
-        h1 = a.idx * stP<R>(sxy, 1); h2 = a.idy * stM<R>(syy, sy); h3 = a.idz * stP<R>(syz, sz);
+        h1 = a.idx * stP<R>(sxy, 1); h2 = a.idy * stM<R>(syy, sy); h3 = zsi * stP<R>(syz, sz);
         if (p3) h1 = pml_up(h1, MP ? ca[3] : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 3) : bxi, m3, m + N_XXY * a.fs);
         if (p4) h2 = pml_up(h2, MP ? ca[4] : ayh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 4) : byh, m4, m + N_YYY * a.fs);
         if (p5) h3 = pml_up(h3, MP ? ca[5] : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 5) : bzi, m5, m + N_ZYZ * a.fs);
@@ -405,7 +414,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_v(El3dDev a) {
         // vz: dx sxz (P) + dy syz (P) + dz szz (M); with a free surface from row 2
         float hz = 0.f;
         if (vz_ok) {
-            h1 = a.idx * stP<R>(sxz, 1); h2 = a.idy * stP<R>(syz, sy); h3 = a.idz * stM<R>(szz, sz);
+            h1 = a.idx * stP<R>(sxz, 1); h2 = a.idy * stP<R>(syz, sy); h3 = zsh * stM<R>(szz, sz);
             if (p6) h1 = pml_up(h1, MP ? ca[6] : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 6) : bxi, m6, m + N_XXZ * a.fs);
             if (p7) h2 = pml_up(h2, MP ? ca[7] : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 7) : byi, m7, m + N_YYZ * a.fs);
             if (p8) h3 = pml_up(h3, MP ? ca[8] : azh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 8) : bzh, m8, m + N_ZZZ * a.fs);
@@ -455,6 +464,9 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_v(El3dDev a) {
     const float ayi = a.ayi[y], byi = a.byi[y], ayh = a.ayh[y], byh = a.byh[y];
     const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
     const float bx = __ldg(a.bx + o), by = __ldg(a.by + o), bz = __ldg(a.bz + o);
+    // the z-derivative e terms carry the node's dz scaling, so that the
+    // neighbours' transposed stencils stay plain
+    const float fzi = __ldg(a.zfi + z), fzh = __ldg(a.zfh + z);
     const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
     float gx = 0.f, gy = 0.f, gz = 0.f;
     for (int s = s0; s < s1; ++s) {
@@ -485,7 +497,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_v(El3dDev a) {
         if (p0) e1 = pml_adr(q, MP ? ca[0] : axh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 0) : bxh, m0, mh + N_XXX * a.fs);
         if (p1) e2 = pml_adr(q, MP ? ca[1] : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 1) : byi, m1, mh + N_YXY * a.fs);
         if (p2) e3 = pml_adr(q, MP ? ca[2] : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 2) : bzi, m2, mh + N_ZXZ * a.fs);
-        ew[N_XXX * a.fs] = e1; ew[N_YXY * a.fs] = e2; ew[N_ZXZ * a.fs] = e3;
+        ew[N_XXX * a.fs] = e1; ew[N_YXY * a.fs] = e2; ew[N_ZXZ * a.fs] = e3 * fzi;
         // vy^ += Dy^T e_yvy (P) + Dz^T e_zvy (M) + Dx^T e_xvy (M)
         v = vy0 + a.idy * tP<R>(e + N_YVY * a.fs, sy) + a.idz * tM<R>(e + N_ZVY * a.fs, sz) +
             a.idx * tM<R>(e + N_XVY * a.fs, 1);
@@ -495,7 +507,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_v(El3dDev a) {
         if (p3) e1 = pml_adr(q, MP ? ca[3] : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 3) : bxi, m3, mh + N_XXY * a.fs);
         if (p4) e2 = pml_adr(q, MP ? ca[4] : ayh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 4) : byh, m4, mh + N_YYY * a.fs);
         if (p5) e3 = pml_adr(q, MP ? ca[5] : azi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 5) : bzi, m5, mh + N_ZYZ * a.fs);
-        ew[N_XXY * a.fs] = e1; ew[N_YYY * a.fs] = e2; ew[N_ZYZ * a.fs] = e3;
+        ew[N_XXY * a.fs] = e1; ew[N_YYY * a.fs] = e2; ew[N_ZYZ * a.fs] = e3 * fzi;
         // vz^ += Dz^T e_zvz (P) + Dy^T e_yvz (M) + Dx^T e_xvz (M); with a free surface from row 2
         if (vz_ok) {
             v = vz0 + a.idz * tP<R>(e + N_ZVZ * a.fs, sz) + a.idy * tM<R>(e + N_YVZ * a.fs, sy) +
@@ -506,7 +518,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_v(El3dDev a) {
             if (p6) e1 = pml_adr(q, MP ? ca[6] : axi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 6) : bxi, m6, mh + N_XXZ * a.fs);
             if (p7) e2 = pml_adr(q, MP ? ca[7] : ayi, MP ? e3_cb<E3_PERM_S>(a, o, 9, 7) : byi, m7, mh + N_YYZ * a.fs);
             if (p8) e3 = pml_adr(q, MP ? ca[8] : azh, MP ? e3_cb<E3_PERM_S>(a, o, 9, 8) : bzh, m8, mh + N_ZZZ * a.fs);
-            ew[N_XXZ * a.fs] = e1; ew[N_YYZ * a.fs] = e2; ew[N_ZZZ * a.fs] = e3;
+            ew[N_XXZ * a.fs] = e1; ew[N_YYZ * a.fs] = e2; ew[N_ZZZ * a.fs] = e3 * fzh;
         }
     }
     const long long go = (long long)c.grp * a.fs + o;
@@ -552,6 +564,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_s(El3dDev a) {
     const bool mir = FS && z > a.pr && z <= a.pr + a.R;
     const long long dzz = (long long)(2 * a.pr - 2 * z) * sz, dsh = dzz + sz;
     const float r13 = c13 / c33, r23 = c23 / c33;
+    const float fzi = __ldg(a.zfi + z), fzh = __ldg(a.zfh + z);  // see k_el3d_adj_v
     float G[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (int s = s0; s < s1; ++s) {
         float* ad = a.ad + s * a.sad;
@@ -639,7 +652,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_s(El3dDev a) {
             if (p1) qy = pml_adr(qy, MP ? ca[1] : ayi, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 1) : byi, m1, mh + N_YVY * a.fs);
             if (p2) qz = pml_adr(qz, MP ? ca[2] : azi, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 2) : bzi, m2, mh + N_ZVZ * a.fs);
         }
-        ew[N_XVX * a.fs] = qx; ew[N_YVY * a.fs] = qy; ew[N_ZVZ * a.fs] = qz;
+        ew[N_XVX * a.fs] = qx; ew[N_YVY * a.fs] = qy; ew[N_ZVZ * a.fs] = qz * fzi;
         float q, e1, e2;
         if (hz_ok) {
             G[6] += yzh * __ldg(S + 3 * a.sterm);
@@ -647,11 +660,11 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_s(El3dDev a) {
             q = g44 * yzh; e1 = q; e2 = q;
             if (p3) e1 = pml_adr(q, MP ? ca[3] : azh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 3) : bzh, m3, mh + N_ZVY * a.fs);
             if (p4) e2 = pml_adr(q, MP ? ca[4] : ayh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 4) : byh, m4, mh + N_YVZ * a.fs);
-            ew[N_ZVY * a.fs] = e1; ew[N_YVZ * a.fs] = e2;
+            ew[N_ZVY * a.fs] = e1 * fzh; ew[N_YVZ * a.fs] = e2;
             q = g55 * xzh; e1 = q; e2 = q;
             if (p5) e1 = pml_adr(q, MP ? ca[5] : azh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 5) : bzh, m5, mh + N_ZVX * a.fs);
             if (p6) e2 = pml_adr(q, MP ? ca[6] : axh, MP ? e3_cb<E3_PERM_AS>(a, o, 0, 6) : bxh, m6, mh + N_XVZ * a.fs);
-            ew[N_ZVX * a.fs] = e1; ew[N_XVZ * a.fs] = e2;
+            ew[N_ZVX * a.fs] = e1 * fzh; ew[N_XVZ * a.fs] = e2;
         }
         G[8] += xyh * __ldg(S + 5 * a.sterm);
         q = g66 * xyh; e1 = q; e2 = q;
@@ -820,6 +833,49 @@ __global__ void k_el3d_chain(El3dDev a, int ngroups, int iso, const float* __res
     }
 }
 
+// Refined free-surface mesh: the mesh cells' d J / d (c11 .. c66, rho) (gpad
+// planes 0..9, written by the cij branch of k_el3d_chain) to the regular padded
+// planes -- the transpose of the depth interpolation that maps the regular Cij
+// to the mesh (regular plane r gets the sum over mesh planes f of w(f, r) g(f),
+// the pairs zptr / zrow / zw) -- then the Jacobian of the parameterisation at
+// the regular cell: iso from (vp, vs, rho) in jpar, thomsen from its eight
+// parameters, cij the identity. FP64, one thread per regular padded cell.
+__global__ void k_el3d_zmap(const double* __restrict__ gmesh, long long npad_m, const int* __restrict__ zptr,
+                            const int* __restrict__ zrow, const double* __restrict__ zw, int aniso,
+                            const float* __restrict__ jpar, long long npad_r, double* __restrict__ gout, int nxq,
+                            int nyq) {
+    for (long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x; cell < npad_r;
+         cell += (long long)gridDim.x * blockDim.x) {
+        const int ix = (int)(cell % nxq), iy = (int)((cell / nxq) % nyq), iz = (int)(cell / ((long long)nxq * nyq));
+        double dc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int e = zptr[iz]; e < zptr[iz + 1]; ++e) {
+            const long long cm = ((long long)zrow[e] * nyq + iy) * nxq + ix;
+            const double w = zw[e];
+            for (int q = 0; q < 10; ++q) dc[q] += w * gmesh[q * npad_m + cm];
+        }
+        if (aniso == OWL_ANISO_THOMSEN) {
+            double pv[8];
+            for (int q = 0; q < 8; ++q) pv[q] = jpar[q * npad_r + cell];
+            for (int q = 0; q < 8; ++q) {
+                Dual pd[8], cd[10];
+                for (int r = 0; r < 8; ++r) pd[r] = Dual{pv[r], r == q ? 1.0 : 0.0};
+                thomsen3d_cij(pd, cd);
+                double g = 0.0;
+                for (int r = 0; r < 10; ++r) g += dc[r] * cd[r].d;
+                gout[q * npad_r + cell] = g;
+            }
+        } else if (aniso == OWL_ANISO_ISO) {
+            const double vp = jpar[cell], vs = jpar[npad_r + cell], rho = jpar[2 * npad_r + cell];
+            const double sn = dc[0] + dc[3] + dc[5], so = dc[1] + dc[2] + dc[4], ss = dc[6] + dc[7] + dc[8];
+            gout[cell] = 2.0 * rho * vp * (sn + so);
+            gout[npad_r + cell] = 2.0 * rho * vs * ss - 4.0 * rho * vs * so;
+            gout[2 * npad_r + cell] = vp * vp * sn + (vp * vp - 2.0 * vs * vs) * so + vs * vs * ss + dc[9];
+        } else {
+            for (int q = 0; q < 10; ++q) gout[q * npad_r + cell] = dc[q];
+        }
+    }
+}
+
 // ============================================================================
 // host engine
 // ============================================================================
@@ -827,8 +883,10 @@ namespace {
 // per-axis damping tables (module_cfspml.f90:517-600 profiles, damp_coef macro of
 // module_wavefield.f90:40-43, kappa = 1, zero M-PML ratio)
 // (low = false: no damping at the low end, the free-surface top, module_cfspml.f90:573-585)
+// (rows: the per-row spacing of the refined free-surface mesh, the reference's
+// dz_i(k) of module_cfspml.f90:581-582, else the uniform d)
 void e3_axis(int n, int pml, int R, int len, float d, float dt, float pmlvp, float alphamax, std::vector<float>& out,
-             bool low = true) {
+             bool low = true, const VMesh* rows = nullptr) {
     out.assign(4 * (size_t)len, 0.f);  // ai, bi, ah, bh
     const float R0 = 1.0e-5f, adt = std::fabs(dt);
     auto ab = [&](float dd, float al, float& a, float& b) {
@@ -848,17 +906,82 @@ void e3_axis(int n, int pml, int R, int len, float d, float dt, float pmlvp, flo
         } else {
             continue;
         }
-        const float c0 = std::log(1.0f / R0) * 3.0f * pmlvp / (2.0f * (float)pml * d);
+        const float di = rows && rows->refined ? rows->get(rows->dzi, i) : d;
+        const float c0 = std::log(1.0f / R0) * 3.0f * pmlvp / (2.0f * (float)pml * di);
         const int x = i + pml + R - 1;
         ab(c0 * (nd * nd), std::max(alphamax * (1.0f - nd), 0.25f * alphamax), out[x], out[len + x]);
         ab(c0 * (ndh * ndh), std::max(alphamax * (1.0f - ndh), 0.25f * alphamax), out[2 * len + x], out[3 * len + x]);
     }
 }
+VMesh checked_vmesh3(const owl_ssg_desc& d) {
+    try {
+        return build_vmesh(d);
+    } catch (const std::invalid_argument& e) {
+        throw OwlError(OWL_ERR_INVALID, e.what());
+    }
+}
+
+owl_ssg_desc with_rows3(owl_ssg_desc d, int nz) {
+    d.nz = nz;
+    return d;
+}
+
+int el3d_nparam(int aniso) { return aniso == OWL_ANISO_ISO ? 3 : aniso == OWL_ANISO_THOMSEN ? 8 : 10; }
+
+// Cij (c11, c12, c13, c22, c23, c33, c44, c55, c66, rho) of one model cell from
+// its parameters (module_vars.f90:278-296, 362-375); pp gets the parameters
+void e3_cell_cij(int aniso, const float* const* f, size_t src, float* v, float* pp) {
+    if (aniso == OWL_ANISO_ISO) {
+        const float vp = f[0][src], vs = f[1][src], rho = f[2][src];
+        const float a11 = rho * (vp * vp), a44 = rho * (vs * vs), a12 = a11 - 2 * a44;
+        const float w[10] = {a11, a12, a12, a11, a12, a11, a44, a44, a44, rho};
+        std::copy(w, w + 10, v);
+        pp[0] = vp; pp[1] = vs; pp[2] = rho;
+    } else if (aniso == OWL_ANISO_THOMSEN) {
+        for (int q = 0; q < 8; ++q) pp[q] = f[q][src];
+        thomsen3d_cij(pp, v);
+    } else {
+        for (int q = 0; q < 10; ++q) v[q] = pp[q] = f[q][src];
+    }
+}
 }  // namespace
+
+// refine_nz of the refined free-surface mesh (module_vars.f90:424-428 of the 3D
+// solver): ceiling(0.5 lambda / dz), lambda = sqrt(max of the means of c44 / rho,
+// c55 / rho, c66 / rho over the padded surface plane) / f0_min
+int el3d_refine_rows(const owl_ssg_desc& d, int np, const float* const* f, float f0_min) {
+    OWL_CHECK(np == el3d_nparam(d.aniso) && f, OWL_ERR_INVALID,
+              "elastic 3D model needs " + std::to_string(el3d_nparam(d.aniso)) + " parameters for this parameterisation");
+    for (int q = 0; q < np; ++q) OWL_CHECK(f[q], OWL_ERR_INVALID, "null model parameter");
+    OWL_CHECK(d.nx >= 1 && d.ny >= 1 && d.nz >= 1 && d.pml >= 0 && d.dz > 0, OWL_ERR_INVALID, "bad grid");
+    float sum[3] = {0.f, 0.f, 0.f};
+    long long cnt = 0;
+    for (int j = -d.pml; j <= d.ny + d.pml + 1; ++j)
+        for (int i = -d.pml; i <= d.nx + d.pml + 1; ++i) {
+            const int ii = std::min(std::max(i, 1), d.nx), jj = std::min(std::max(j, 1), d.ny);
+            const size_t src = ((size_t)(ii - 1) * d.ny + (jj - 1)) * d.nz;
+            float v[10], pp[10];
+            e3_cell_cij(d.aniso, f, src, v, pp);
+            OWL_CHECK(v[9] > 0, OWL_ERR_INVALID, "rho must be positive");
+            for (int q = 0; q < 3; ++q) sum[q] += v[6 + q] / v[9];
+            ++cnt;
+        }
+    const float m = std::max({sum[0] / (float)cnt, sum[1] / (float)cnt, sum[2] / (float)cnt});
+    const float lambda = std::sqrt(m) / f0_min;
+    return (int)std::ceil(0.5f * lambda / d.dz);
+}
 
 struct El3dEngine : SsgBase {
     int aniso;
     float idx, idy, idz;
+    // depth-refined free-surface mesh: the engine runs on the mesh's planes (nz
+    // of the base), the model and the gradient stay on the regular nz_model planes
+    VMesh vm;
+    int nz_model;
+    DevBuf<float> zfi, zfh, jparp;
+    DevBuf<double> zw, gzmap;
+    DevBuf<int> zptr, zrow;
+    ZInterp zt;
     DevBuf<float> c11, c12, c13, c22, c23, c33, c44e, c55e, c66e, bxp, byp, bzp;
     DevBuf<float> c44p, c55p, c66p, rhop, p0p, p1p, tabx, taby, tabz, tparp;
     // M-PML: nonzero face ratios, the faces in the layout of owl_ssg_mpml_ratios,
@@ -894,7 +1017,8 @@ struct El3dEngine : SsgBase {
                 } else {
                     continue;
                 }
-                const float c0 = std::log(1.0f / R0) * 3.0f * pmlvp / (2.0f * (float)P * dd[ax]);
+                const float di = ax == 2 && vm.refined ? vm.get(vm.dzi, i) : dd[ax];
+                const float c0 = std::log(1.0f / R0) * 3.0f * pmlvp / (2.0f * (float)P * di);
                 const int x = i + pr - 1;
                 t[x] = c0 * (nd * nd);
                 t[L + x] = c0 * (ndh * ndh);
@@ -986,14 +1110,12 @@ struct El3dEngine : SsgBase {
         return m;
     }
 
-    explicit El3dEngine(const owl_ssg_desc& d) : SsgBase(d, 3) {
+    explicit El3dEngine(const owl_ssg_desc& d) : El3dEngine(d, checked_vmesh3(d)) {}
+    El3dEngine(const owl_ssg_desc& d, VMesh m) : SsgBase(with_rows3(d, m.nz), 3), vm(std::move(m)), nz_model(d.nz) {
         aniso = d.aniso;
         OWL_CHECK(aniso == OWL_ANISO_ISO || aniso == OWL_ANISO_CIJ || aniso == OWL_ANISO_THOMSEN, OWL_ERR_UNSUPPORTED,
                   "elastic 3D takes the iso (vp, vs, rho), thomsen (vp, vs, epsilon, delta, gamma, theta, phi, rho) "
                   "or cij (nine moduli, rho) parameterisation");
-        OWL_CHECK(!(d.free_surface && (d.free_surface_dz_refine > 1.f || (d.dz_max > 0.f && d.dz_max != d.dz))),
-                  OWL_ERR_UNSUPPORTED, "elastic 3D runs the free surface on the uniform grid "
-                                       "(free_surface_dz_refine 1, dz_max dz)");
         idx = (float)(1.0 / (double)d.dx);
         idy = (float)(1.0 / (double)d.dy);
         idz = (float)(1.0 / (double)d.dz);
@@ -1002,14 +1124,48 @@ struct El3dEngine : SsgBase {
         sad = E3_NAD * fs;
         nS = 9;
         ngrad = 12;
-        nparam = aniso == OWL_ANISO_ISO ? 3 : aniso == OWL_ANISO_THOMSEN ? 8 : 10;
+        nparam = el3d_nparam(aniso);
         ncomp = 3;
         for (int f = 0; f < E3_NST; ++f) st_segments.push_back({f * fs, fs});
+        // dz scalings of the storage planes (1 outside the mesh arrays and on the uniform grid)
+        std::vector<float> hi(NZs, 1.f), hh(NZs, 1.f);
+        if (vm.refined) {
+            for (int z = 0; z < NZs; ++z) {
+                const int k = z - pr + 1;
+                if (k < -P || k > nz + P + 1) continue;
+                hi[z] = vm.get(vm.si, k);
+                hh[z] = vm.get(vm.sh, k);
+            }
+            zt = build_zinterp(vm, nz_model, d.dz);
+            // transpose of the depth interpolation, per regular padded plane
+            std::vector<std::vector<std::pair<int, double>>> by((size_t)nz_model + 2 * P + 2);
+            for (int f = -P; f <= nz + P + 1; ++f) {
+                const int r0 = zt.r0[(size_t)(f + P)];
+                const double w = zt.w[(size_t)(f + P)];
+                by[(size_t)(r0 + P)].push_back({f + P, 1.0 - w});
+                by[(size_t)(r0 + 1 + P)].push_back({f + P, w});
+            }
+            std::vector<int> hp(1, 0), hr;
+            std::vector<double> hw;
+            for (auto& v : by) {
+                for (auto& e : v) { hr.push_back(e.first); hw.push_back(e.second); }
+                hp.push_back((int)hr.size());
+            }
+            zptr.upload(hp.data(), hp.size(), stream);
+            zrow.upload(hr.data(), hr.size(), stream);
+            zw.upload(hw.data(), hw.size(), stream);
+        }
+        zfi.upload(hi.data(), hi.size(), stream);
+        zfh.upload(hh.data(), hh.size(), stream);
+        OWL_CUDA(cudaStreamSynchronize(stream));
     }
+
+    // refined mesh: gpad holds the mesh cells' d J / d (c11 .. c66, rho)
+    int grad_planes() const override { return vm.refined ? 10 : nparam; }
 
     float* st_field(int f) const override { return f < 9 ? st.p + f * fs : nullptr; }
     float* ad_field(int f) const override { return f < 9 ? ad.p + f * fs : nullptr; }
-    int rho_param() const override { return nparam - 1; }
+    int rho_param() const override { return vm.refined ? 9 : nparam - 1; }
     std::vector<int> tune_spt(int) const override { return {1, 2, 4}; }
     // forward pass: 2 = thread per cell (2 planes per block), 1 = the z-marching
     // ring kernels (half-width 4, no free surface)
@@ -1037,34 +1193,64 @@ struct El3dEngine : SsgBase {
         std::vector<float> hp0, hp1, htp;
         if (aniso == OWL_ANISO_ISO) { hp0.assign(fs, 0.f); hp1.assign(fs, 0.f); }
         if (aniso == OWL_ANISO_THOMSEN) htp.assign((size_t)8 * fs, 0.f);
-        // Cij of the padded model (module_vars.f90:278-296, 362-375; padding by pml+1, :409-418)
-        for (int k = -P; k <= nz + P + 1; ++k)
+        const int nzr = nz_model;
+        auto regular = [&](int i, int j, int k, float* v, float* pp) {
+            const int ii = std::min(std::max(i, 1), nx), jj = std::min(std::max(j, 1), ny),
+                      kk = std::min(std::max(k, 1), nzr);
+            const size_t src = ((size_t)(ii - 1) * ny + (jj - 1)) * nzr + (kk - 1);
+            e3_cell_cij(aniso, f, src, v, pp);
+            for (int q = 0; q < 10; ++q) OWL_CHECK(std::isfinite(v[q]), OWL_ERR_INVALID, "non-finite model value");
+            OWL_CHECK(v[9] > 0 && v[0] > 0 && v[3] > 0 && v[5] > 0 && v[6] > 0 && v[7] > 0 && v[8] > 0,
+                      OWL_ERR_INVALID, "rho, c11, c22, c33, c44, c55, c66 must be positive");
+        };
+        // pmlvp over the six faces of the regular model (module_vars.f90:384-406)
+        float pv = -1e30f;
+        auto face = [&](int i, int j, int k, const float* v) {
+            if (i == 1 || i == nx || j == 1 || j == ny || k == 1 || k == nzr)
+                for (int q : {0, 3, 5}) pv = std::max(pv, v[q] / v[9]);
+        };
+        if (!vm.refined) {
+            // Cij of the padded model (module_vars.f90:278-296, 362-375; padding by pml+1, :409-418)
+            for (int k = -P; k <= nz + P + 1; ++k)
+                for (int j = -P; j <= ny + P + 1; ++j)
+                    for (int i = -P; i <= nx + P + 1; ++i) {
+                        const long long o = soff(i, j, k);
+                        float v[10], pp[10];
+                        regular(i, j, k, v, pp);
+                        if (aniso == OWL_ANISO_ISO) { hp0[o] = pp[0]; hp1[o] = pp[1]; }
+                        if (aniso == OWL_ANISO_THOMSEN)
+                            for (int q = 0; q < 8; ++q) htp[(size_t)q * fs + o] = pp[q];
+                        for (int q = 0; q < 10; ++q) hc[q][o] = v[q];
+                        if (i >= 1 && i <= nx && j >= 1 && j <= ny && k >= 1 && k <= nzr) face(i, j, k, v);
+                    }
+        } else {
+            // per (x, y) column: the regular padded column's Cij, interpolated
+            // linearly to the mesh planes (map_regular_to_irregular,
+            // module_vars.f90:164-180 of the 3D solver); the parameters of the
+            // regular cells for the chain rule
+            const int nq = nzr + 2 * P + 2, npj = aniso == OWL_ANISO_ISO ? 3 : aniso == OWL_ANISO_THOMSEN ? 8 : 0;
+            const size_t npr = (size_t)nxq() * nyq() * nq;
+            std::vector<float> hj((size_t)npj * npr, 0.f), col((size_t)10 * nq);
             for (int j = -P; j <= ny + P + 1; ++j)
                 for (int i = -P; i <= nx + P + 1; ++i) {
-                    const int ii = std::min(std::max(i, 1), nx), jj = std::min(std::max(j, 1), ny),
-                              kk = std::min(std::max(k, 1), nz);
-                    const size_t src = ((size_t)(ii - 1) * ny + (jj - 1)) * nz + (kk - 1);
-                    const long long o = soff(i, j, k);
-                    float v[10];
-                    if (aniso == OWL_ANISO_ISO) {
-                        const float vp = f[0][src], vs = f[1][src], rho = f[2][src];
-                        const float a11 = rho * (vp * vp), a44 = rho * (vs * vs), a12 = a11 - 2 * a44;
-                        const float w[10] = {a11, a12, a12, a11, a12, a11, a44, a44, a44, rho};
-                        std::copy(w, w + 10, v);
-                        hp0[o] = vp;
-                        hp1[o] = vs;
-                    } else if (aniso == OWL_ANISO_THOMSEN) {
-                        float pp[8];
-                        for (int q = 0; q < 8; ++q) htp[(size_t)q * fs + o] = pp[q] = f[q][src];
-                        thomsen3d_cij(pp, v);
-                    } else {
-                        for (int q = 0; q < 10; ++q) v[q] = f[q][src];
+                    for (int k = -P; k <= nzr + P + 1; ++k) {
+                        float v[10], pp[10];
+                        regular(i, j, k, v, pp);
+                        for (int q = 0; q < 10; ++q) col[(size_t)q * nq + (k + P)] = v[q];
+                        const size_t cell = ((size_t)(k + P) * nyq() + (j + P)) * nxq() + (i + P);
+                        for (int q = 0; q < npj; ++q) hj[(size_t)q * npr + cell] = pp[q];
+                        if (i >= 1 && i <= nx && j >= 1 && j <= ny && k >= 1 && k <= nzr) face(i, j, k, v);
                     }
-                    for (int q = 0; q < 10; ++q) OWL_CHECK(std::isfinite(v[q]), OWL_ERR_INVALID, "non-finite model value");
-                    OWL_CHECK(v[9] > 0 && v[0] > 0 && v[3] > 0 && v[5] > 0 && v[6] > 0 && v[7] > 0 && v[8] > 0,
-                              OWL_ERR_INVALID, "rho, c11, c22, c33, c44, c55, c66 must be positive");
-                    for (int q = 0; q < 10; ++q) hc[q][o] = v[q];
+                    for (int k = -P; k <= nz + P + 1; ++k) {
+                        const int r0 = zt.r0[(size_t)(k + P)];
+                        const long long o = soff(i, j, k);
+                        for (int q = 0; q < 10; ++q)
+                            hc[q][o] = zinterp_apply(zt, k, P, col[(size_t)q * nq + (r0 + P)],
+                                                     col[(size_t)q * nq + (r0 + 1 + P)]);
+                    }
                 }
+            if (npj) jparp.upload(hj.data(), hj.size(), stream);
+        }
         // harmonic shear moduli and buoyancies (module_wavefield.f90:30-38)
         std::vector<float> h44(fs, 0.f), h55(fs, 0.f), h66(fs, 0.f), hbx(fs, 0.f), hby(fs, 0.f), hbz(fs, 0.f);
         const std::vector<float>& r = hc[9];
@@ -1082,25 +1268,37 @@ struct El3dEngine : SsgBase {
                     hby[o] = dt / (0.5f * (r[soff(i, j - 1, k)] + r[o]));
                     hbz[o] = dt / (0.5f * (r[soff(i, j, k - 1)] + r[o]));
                 }
-        // pmlvp over the six faces (module_vars.f90:384-406) and dt_stable (:534-537)
-        float pv = -1e30f, maxv = 0.f;
-        for (int k = 1; k <= nz; ++k)
-            for (int j = 1; j <= ny; ++j)
-                for (int i = 1; i <= nx; ++i) {
-                    const long long o = soff(i, j, k);
-                    const bool face = i == 1 || i == nx || j == 1 || j == ny || k == 1 || k == nz;
-                    for (int q : {0, 3, 5}) {
-                        const float w = hc[q][o] / r[o];
-                        if (face) pv = std::max(pv, w);
-                        maxv = std::max(maxv, std::sqrt(w));
-                    }
-                }
+        // dt_stable (module_vars.f90:500-537; on the refined mesh the least over
+        // the cells, each with its plane's smaller spacing)
         const float pmlvp = std::sqrt(pv);
         const float* cf = fd_coefs(R);
         float temp = 0.f;
         for (int q = 0; q < R; ++q) temp += std::fabs(cf[q]);
-        dt_stable_ = 1.0f / (temp * maxv *
-                             std::sqrt(1.0f / (desc.dx * desc.dx) + 1.0f / (desc.dy * desc.dy) + 1.0f / (desc.dz * desc.dz)));
+        if (!vm.refined) {
+            float maxv = 0.f;
+            for (int k = 1; k <= nz; ++k)
+                for (int j = 1; j <= ny; ++j)
+                    for (int i = 1; i <= nx; ++i) {
+                        const long long o = soff(i, j, k);
+                        for (int q : {0, 3, 5}) maxv = std::max(maxv, std::sqrt(hc[q][o] / r[o]));
+                    }
+            dt_stable_ = 1.0f / (temp * maxv * std::sqrt(1.0f / (desc.dx * desc.dx) + 1.0f / (desc.dy * desc.dy) +
+                                                         1.0f / (desc.dz * desc.dz)));
+        } else {
+            float best = 3.0e38f;
+            for (int k = 1; k <= nz; ++k) {
+                const float hz = std::min(vm.get(vm.dzi, k), vm.get(vm.dzh, k));
+                const float g = std::sqrt(1.0f / (desc.dx * desc.dx) + 1.0f / (desc.dy * desc.dy) + 1.0f / (hz * hz));
+                for (int j = 1; j <= ny; ++j)
+                    for (int i = 1; i <= nx; ++i) {
+                        const long long o = soff(i, j, k);
+                        const float mv = std::max({std::sqrt(hc[0][o] / r[o]), std::sqrt(hc[3][o] / r[o]),
+                                                   std::sqrt(hc[5][o] / r[o])});
+                        best = std::min(best, 1.0f / (temp * mv * g));
+                    }
+            }
+            dt_stable_ = best;
+        }
         if (dt > dt_stable_ && !desc.allow_dt_adjust)
             throw OwlError(OWL_ERR_UNSTABLE, "dt = " + std::to_string(dt) + " exceeds the stable dt " +
                                                  std::to_string(dt_stable_));
@@ -1108,7 +1306,7 @@ struct El3dEngine : SsgBase {
         std::vector<float> tx, ty, tz;
         e3_axis(nx, P, R, pitch, desc.dx, dt, pmlvp, alphamax, tx);
         e3_axis(ny, P, R, NYs, desc.dy, dt, pmlvp, alphamax, ty);
-        e3_axis(nz, P, R, NZs, desc.dz, dt, pmlvp, alphamax, tz, desc.free_surface == 0);
+        e3_axis(nz, P, R, NZs, desc.dz, dt, pmlvp, alphamax, tz, desc.free_surface == 0, &vm);
         build_mpml(hc, pmlvp, alphamax);
         c11.upload(hc[0].data(), fs, stream); c12.upload(hc[1].data(), fs, stream); c13.upload(hc[2].data(), fs, stream);
         c22.upload(hc[3].data(), fs, stream); c23.upload(hc[4].data(), fs, stream); c33.upload(hc[5].data(), fs, stream);
@@ -1160,7 +1358,10 @@ struct El3dEngine : SsgBase {
             return;
         }
         const bool mt = q.mechanism == OWL_SRC_MT;
-        const float inv = 1.0f / (desc.dx * desc.dy * desc.dz);
+        // dz_s: the local spacing dz_i(gz) on the refined mesh (module_wavefield.f90:1107-1111)
+        OWL_CHECK(!vm.refined || (q.gz >= -P && q.gz <= nz + P + 1), OWL_ERR_INVALID, "source outside the grid");
+        const float dzs = vm.refined ? vm.get(vm.dzi, q.gz) : desc.dz;
+        const float inv = 1.0f / (desc.dx * desc.dy * dzs);
         for (int irz = -4; irz <= 4; ++irz)
             for (int iry = -4; iry <= 4; ++iry)
                 for (int irx = -4; irx <= 4; ++irx) {
@@ -1226,6 +1427,7 @@ struct El3dEngine : SsgBase {
         a.axi = tabx.p; a.bxi = tabx.p + pitch; a.axh = tabx.p + 2 * pitch; a.bxh = tabx.p + 3 * pitch;
         a.ayi = taby.p; a.byi = taby.p + NYs; a.ayh = taby.p + 2 * NYs; a.byh = taby.p + 3 * NYs;
         a.azi = tabz.p; a.bzi = tabz.p + NZs; a.azh = tabz.p + 2 * NZs; a.bzh = tabz.p + 3 * NZs;
+        a.zfi = zfi.p; a.zfh = zfh.p;
         a.st = st.p;
         a.k = std::max(1, cur_k);
         a.d_step = ctr.p;
@@ -1401,12 +1603,38 @@ struct El3dEngine : SsgBase {
         El3dDev a = dev(S);
         const long long n = (long long)nxq() * nyq() * nzq();
         const int nb = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
-        const bool iso = aniso == OWL_ANISO_ISO;
+        // refined mesh: d J / d Cij of the mesh cells (the cij branch), mapped in fold_out
+        const bool iso = aniso == OWL_ANISO_ISO && !vm.refined;
         k_el3d_chain<<<nb, 256, 0, stream>>>(a, groups, iso ? 1 : 0, iso ? p0p.p : nullptr, iso ? p1p.p : nullptr,
-                                             aniso == OWL_ANISO_THOMSEN ? tparp.p : nullptr, c44p.p,
+                                             aniso == OWL_ANISO_THOMSEN && !vm.refined ? tparp.p : nullptr, c44p.p,
                                              c55p.p, c66p.p, rhop.p, gpad.p, nxq(), nyq(), nzq());
         OWL_LAUNCH_CHECK();
         launches++;
+    }
+
+    // refined mesh: the mesh cells' d J / d Cij to the regular planes and the
+    // model parameters (k_el3d_zmap), then the fold of the padding
+    void fold_out(float* grad, int mem) override {
+        if (!vm.refined) {
+            SsgBase::fold_out(grad, mem);
+            return;
+        }
+        const int nzq_r = nz_model + 2 * P + 2;
+        const long long npr = (long long)nxq() * nyq() * nzq_r;
+        gzmap.reserve((size_t)nparam * npr);
+        const int nb = (int)std::min<long long>((npr + 255) / 256, 148LL * 16);
+        k_el3d_zmap<<<nb, 256, 0, stream>>>(gpad.p, (long long)npad(), zptr.p, zrow.p, zw.p, aniso, jparp.p, npr,
+                                            gzmap.p, nxq(), nyq());
+        OWL_LAUNCH_CHECK();
+        launches++;
+        const size_t nm = (size_t)nx * ny * nz_model;
+        seis_tmp.reserve((size_t)nparam * nm);
+        for (int q = 0; q < nparam; ++q) {
+            launch_fold(gzmap.p + (size_t)q * npr, nxq(), nyq(), P, nx, ny, nz_model, 3, seis_tmp.p + (size_t)q * nm,
+                        stream);
+            launches++;
+        }
+        copy_out(grad, seis_tmp.p, (size_t)nparam * nm * sizeof(float), mem);
     }
 };
 

@@ -43,6 +43,7 @@ Engine* make_el2d_engine(const owl_ssg_desc& d);
 Engine* make_el3d_engine(const owl_ssg_desc& d);
 // refine_nz of the depth-refined free-surface mesh from the model's surface row (el2d.cu)
 int el2d_refine_rows(const owl_ssg_desc& d, int nparam, const float* const* fields, float f0_min);
+int el3d_refine_rows(const owl_ssg_desc& d, int nparam, const float* const* fields, float f0_min);  // el3d.cu
 
 // -------- shared device helpers (defined in shared.cu) ----------------------
 

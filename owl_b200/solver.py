@@ -419,7 +419,9 @@ class SSGSolver:
         """The six M-PML face-ratio arrays of an elastic 3D model (left, right,
         front, back, top, bottom; the layout of owl_ssg_mpml_ratios)."""
         d = self.desc
-        nx, ny, nz = d.nx + 2 * d.pml, d.ny + 2 * d.pml, d.nz + 2 * d.pml
+        m = self.grid.zmesh  # on the refined free-surface mesh the faces span its planes
+        nzm = d.nz if m is None else len(m.z_i) - 2 * d.pml - 2
+        nx, ny, nz = d.nx + 2 * d.pml, d.ny + 2 * d.pml, nzm + 2 * d.pml
         out = np.zeros(2 * (ny * nz + nx * nz + nx * ny), dtype=f32)
         L.check(self.lib.owl_ssg_mpml_ratios(self.h, out.ctypes.data_as(C.POINTER(C.c_float))))
         return out

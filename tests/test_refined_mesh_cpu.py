@@ -175,3 +175,57 @@ def test_refined_forward_differs_from_uniform_and_is_stable():
                        time_integration=elastic_time_integration)
     b = oracle.el2d_forward(du, f, pu, "f64")
     assert np.linalg.norm(a - b) > 1e-3 * np.linalg.norm(b)
+
+
+# ------------------------------ elastic 3D ----------------------------------
+def refined_desc3(aniso=L.OWL_ANISO_ISO, rr=2.0, dz_max=12.5, rows=2, nt=100):
+    from test_oracle_el3d import N
+    d = L.OwlSsgDesc()
+    d.medium = L.OWL_ELASTIC_VHTIORT_3D
+    d.nx = d.ny = d.nz = N
+    d.dx = d.dy = d.dz = DX
+    d.pml, d.fdhalf, d.free_surface = 5, 4, 1
+    d.dt, d.nt, d.f0_max, d.max_shots = 5e-4, nt, 20.0, 4
+    d.aniso = aniso
+    d.free_surface_dz_refine, d.dz_max, d.free_surface_refine_rows = rr, dz_max, rows
+    return d
+
+
+def refined_prep3(d, shots):
+    from test_oracle_el3d import N
+    m = vertical_mesh(d)
+    return PreparedShots(elastic_geometry(shots, d, m), GridSpec(nx=N, nz=N, dx=DX, dz=DX, ny=N, dy=DX, zmesh=m),
+                         d.dt, time_integration=elastic_time_integration)
+
+
+@pytest.mark.parametrize("aniso", [L.OWL_ANISO_ISO, L.OWL_ANISO_CIJ])
+def test_refined_adjoint_dot_product_3d(aniso):
+    """The elastic 3D oracle on the refined mesh: exact adjoint against
+    complex-step Jacobian-vector products of the forward."""
+    from test_oracle_el3d import el3_model, el3_shots, _dot
+    d = refined_desc3(aniso, nt=60)
+    f = el3_model(aniso)
+    ps = refined_prep3(d, el3_shots(1))
+    rng = np.random.default_rng(7)
+    dm = [rng.standard_normal(x.shape) * np.std(x) * 1e-3 for x in f]
+    seis, jvp = oracle.el3d_jvp(d, f, dm, ps)
+    r = rng.standard_normal(seis.shape)
+    _, g, _ = oracle.el3d_gradient(d, f, ps, r, adj_kind=L.OWL_ADJ_GIVEN, k=7)
+    lhs, rhs = float(np.dot(jvp, r)), _dot(g, dm)
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs), (lhs, rhs)
+
+
+def test_refine_rows_3d_formula():
+    """3D refine_nz: the largest of the means of c44 / rho, c55 / rho, c66 / rho
+    over the padded surface plane (module_vars.f90:424-428 of the 3D solver)."""
+    from test_oracle_el3d import N, el3_model
+    d = refined_desc3(L.OWL_ANISO_CIJ)
+    f = el3_model(L.OWL_ANISO_CIJ)
+    P = d.pml
+    idx = np.clip(np.arange(-P, N + P + 2), 1, N) - 1
+    rho = f[9][0][np.ix_(idx, idx)].astype(np.float32)  # (y, x) at the surface (z index 0)
+    means = [float(np.mean((f[q][0][np.ix_(idx, idx)].astype(np.float32) / rho).astype(np.float64)))
+             for q in (6, 7, 8)]
+    lam = math.sqrt(max(means)) / 17.0
+    want = math.ceil(0.5 * lam / DX)
+    assert free_surface_refine_rows(d, f, 17.0) == want
