@@ -84,7 +84,9 @@ __device__ __forceinline__ float pml_e(float q, float a, float b, float psih, fl
 
 // ------------------------------- forward ------------------------------------
 // 48 registers at R = 4 (no spills): five 256-thread CTAs per SM instead of four
-template <int R, bool STORE>
+// ZR: the depth-refined free-surface mesh (per-row dz scalings); the uniform
+// grid's instances leave them out
+template <int R, bool STORE, bool ZR>
 __global__ void __maxnreg__(R == 4 ? 48 : 128) k_el2d_fwd_s(El2dDev a) {
     const int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int z = a.zs0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -100,8 +102,8 @@ __global__ void __maxnreg__(R == 4 ? 48 : 128) k_el2d_fwd_s(El2dDev a) {
     const float4 chh = (phh && dxz) ? __ldg(a.phh + o) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float c11 = __ldg(a.c11 + o), c13 = __ldg(a.c13 + o), c33 = __ldg(a.c33 + o);
     const float c55dt = dxz ? a.dt * __ldg(a.c55e + o) : 0.f;
-    // 1/dz times the row's dz scaling (refined mesh; 1/dz exactly on the uniform grid)
-    const float zsi = a.idz * __ldg(a.zfi + z), zsh = a.idz * __ldg(a.zfh + z);
+    // 1/dz times the row's dz scaling (refined mesh)
+    const float zsi = ZR ? a.idz * __ldg(a.zfi + z) : a.idz, zsh = ZR ? a.idz * __ldg(a.zfh + z) : a.idz;
     const bool mir = a.fsurf && z > a.pr && z <= a.pr + a.R;
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
@@ -183,7 +185,7 @@ __global__ void __maxnreg__(R == 4 ? 48 : 128) k_el2d_fwd_s(El2dDev a) {
     }
 }
 
-template <int R, bool STORE>
+template <int R, bool STORE, bool ZR>
 __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
     const int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int z = a.zvx0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -196,7 +198,7 @@ __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
     const float4 chi = phi ? __ldg(a.phi + o) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 cih = (pih && dvz) ? __ldg(a.pih + o) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float bx = __ldg(a.bx + o), bz = dvz ? __ldg(a.bz + o) : 0.f;
-    const float zsi = a.idz * __ldg(a.zfi + z), zsh = a.idz * __ldg(a.zfh + z);  // see k_el2d_fwd_s
+    const float zsi = ZR ? a.idz * __ldg(a.zfi + z) : a.idz, zsh = ZR ? a.idz * __ldg(a.zfh + z) : a.idz;  // see k_el2d_fwd_s
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
     for (int s = s0; s < s1; ++s) {
@@ -267,7 +269,7 @@ __device__ __forceinline__ void kahan_g(float* G, long long gg, long long go, in
 // velocity nodes: finish the adjoint of the stress update of step t+1
 // (v^ += D^T e of the sigma nodes), correlate v^ with the stored terms of step
 // t (rho gradient), then the adjoint PML terms of the velocity update of step t
-template <int R>
+template <int R, bool ZR>
 __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
     const int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int z = a.zvx0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -284,7 +286,7 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
     const float bx = __ldg(a.bx + o), bz = dvz ? __ldg(a.bz + o) : 0.f;
     // the z-derivative e terms carry the node's dz scaling, so that the
     // neighbours' transposed stencils stay plain
-    const float zsi = __ldg(a.zfi + z), zsh = __ldg(a.zfh + z);
+    const float zsi = ZR ? __ldg(a.zfi + z) : 1.f, zsh = ZR ? __ldg(a.zfh + z) : 1.f;
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     float gbx = 0.f, gbz = 0.f;
     for (int s = s0; s < s1; ++s) {
@@ -314,7 +316,7 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
                 ez = pml_e(q, chi.z, chi.w, m_zxz, mh + M_DZXZ * a.fs);
             }
             e[M_DXXX * a.fs] = ex;
-            e[M_DZXZ * a.fs] = ez * zsi;
+            e[M_DZXZ * a.fs] = ZR ? ez * zsi : ez;
         }
         if (dvz) {
             const float* e4 = e + M_DZVZ * a.fs;
@@ -334,7 +336,7 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
                 ez = pml_e(q, cih.z, cih.w, m_zzz, mh + M_DZZZ * a.fs);
             }
             e[M_DXXZ * a.fs] = ex;
-            e[M_DZZZ * a.fs] = ez * zsh;
+            e[M_DZZZ * a.fs] = ZR ? ez * zsh : ez;
         }
     }
     const long long go = (long long)blockIdx.z * a.fs + o;
@@ -349,7 +351,7 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
 // 64 registers at R = 4 (a few bytes spilled) instead of the 128 that a
 // 512-thread bound allows: four 256-thread CTAs per SM instead of two, which
 // hides more of the load latency this kernel is bound by
-template <int R>
+template <int R, bool ZR>
 __global__ void __maxnreg__(R == 4 ? 64 : 128) k_el2d_adj_s(El2dDev a) {
     const int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int z = a.zs0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -371,7 +373,7 @@ __global__ void __maxnreg__(R == 4 ? 64 : 128) k_el2d_adj_s(El2dDev a) {
     const long long ozz = (long long)(2 * a.pr - z) * pt + x;      // sigma_zz image row
     const long long oxz = (long long)(2 * a.pr + 1 - z) * pt + x;  // sigma_xz image row
     const float r13 = c13 / c33;
-    const float zsi = __ldg(a.zfi + z), zsh = __ldg(a.zfh + z);  // see k_el2d_adj_v
+    const float zsi = ZR ? __ldg(a.zfi + z) : 1.f, zsh = ZR ? __ldg(a.zfh + z) : 1.f;  // see k_el2d_adj_v
     const int s0 = blockIdx.z * a.spt, s1 = min(a.nshots, s0 + a.spt);
     float g11 = 0.f, g13 = 0.f, g33 = 0.f, g55 = 0.f;
     for (int s = s0; s < s1; ++s) {
@@ -432,7 +434,7 @@ __global__ void __maxnreg__(R == 4 ? 64 : 128) k_el2d_adj_s(El2dDev a) {
                 ex = pml_e(qx, cii.x, cii.y, m_xvx, mh + M_DXVX * a.fs);
                 ez = pml_e(qz, cii.z, cii.w, m_zvz, mh + M_DZVZ * a.fs);
             }
-            e[M_DZVZ * a.fs + o] = ez * zsi;
+            e[M_DZVZ * a.fs + o] = ZR ? ez * zsi : ez;
         }
         e[M_DXVX * a.fs + o] = ex;
         // sigma_xz
@@ -464,7 +466,7 @@ __global__ void __maxnreg__(R == 4 ? 64 : 128) k_el2d_adj_s(El2dDev a) {
                 exz = pml_e(q, chh.x, chh.y, m_xvz, mh + M_DXVZ * a.fs);
                 ezx = pml_e(q, chh.z, chh.w, m_zvx, mh + M_DZVX * a.fs);
             }
-            e[M_DZVX * a.fs + o] = ezx * zsh;
+            e[M_DZVX * a.fs + o] = ZR ? ezx * zsh : ezx;
             e[M_DXVZ * a.fs + o] = exz;
         }
     }
@@ -1087,7 +1089,7 @@ struct El2dEngine : SsgBase {
         }
     }
 
-    template <int RR>
+    template <int RR, bool ZR>
     void launch_r(int id, int S, bool store) {
         El2dDev a = dev(S);
         const int rows_s = a.z1 - a.zs0, rows_v = a.z1 - a.zvx0;
@@ -1102,33 +1104,38 @@ struct El2dEngine : SsgBase {
                     return dim3((NXp + 127) / 128, (rows + ty - 1) / ty, (S + spt_f - 1) / spt_f);
                 };
                 if (id == OWL_K_FWD_P) {
-                    if (store) k_el2d_fwd_s4<RR, true><<<grid(rows_s), b, 0, stream>>>(a);
-                    else k_el2d_fwd_s4<RR, false><<<grid(rows_s), b, 0, stream>>>(a);
+                    if (store) k_el2d_fwd_s4<RR, true, ZR><<<grid(rows_s), b, 0, stream>>>(a);
+                    else k_el2d_fwd_s4<RR, false, ZR><<<grid(rows_s), b, 0, stream>>>(a);
                 } else {
-                    if (store) k_el2d_fwd_v4<RR, true><<<grid(rows_v), b, 0, stream>>>(a);
-                    else k_el2d_fwd_v4<RR, false><<<grid(rows_v), b, 0, stream>>>(a);
+                    if (store) k_el2d_fwd_v4<RR, true, ZR><<<grid(rows_v), b, 0, stream>>>(a);
+                    else k_el2d_fwd_v4<RR, false, ZR><<<grid(rows_v), b, 0, stream>>>(a);
                 }
                 return;
             }
             const dim3 b(tile_x, tz_f);
             if (id == OWL_K_FWD_P) {
-                if (store) k_el2d_fwd_s<RR, true><<<grid_for(rows_s, S, spt_f, tz_f), b, 0, stream>>>(a);
-                else k_el2d_fwd_s<RR, false><<<grid_for(rows_s, S, spt_f, tz_f), b, 0, stream>>>(a);
+                if (store) k_el2d_fwd_s<RR, true, ZR><<<grid_for(rows_s, S, spt_f, tz_f), b, 0, stream>>>(a);
+                else k_el2d_fwd_s<RR, false, ZR><<<grid_for(rows_s, S, spt_f, tz_f), b, 0, stream>>>(a);
             } else {
-                if (store) k_el2d_fwd_v<RR, true><<<grid_for(rows_v, S, spt_f, tz_f), b, 0, stream>>>(a);
-                else k_el2d_fwd_v<RR, false><<<grid_for(rows_v, S, spt_f, tz_f), b, 0, stream>>>(a);
+                if (store) k_el2d_fwd_v<RR, true, ZR><<<grid_for(rows_v, S, spt_f, tz_f), b, 0, stream>>>(a);
+                else k_el2d_fwd_v<RR, false, ZR><<<grid_for(rows_v, S, spt_f, tz_f), b, 0, stream>>>(a);
             }
         } else {
             OWL_CHECK(a.ad && a.S && a.G, OWL_ERR_INVALID, "adjoint buffers not allocated");
             a.spt = spt_a;
             const dim3 b(tile_x, tz_a);
-            if (id == OWL_K_ADJ_P) k_el2d_adj_v<RR><<<grid_for(rows_v, S, spt_a, tz_a), b, 0, stream>>>(a);
-            else k_el2d_adj_s<RR><<<grid_for(rows_s, S, spt_a, tz_a), b, 0, stream>>>(a);
+            if (id == OWL_K_ADJ_P) k_el2d_adj_v<RR, ZR><<<grid_for(rows_v, S, spt_a, tz_a), b, 0, stream>>>(a);
+            else k_el2d_adj_s<RR, ZR><<<grid_for(rows_s, S, spt_a, tz_a), b, 0, stream>>>(a);
         }
     }
     void launch_kernel(int id, int S, bool store) override {
-        if (R == 4) launch_r<4>(id, S, store);
-        else launch_r<8>(id, S, store);
+        if (vm.refined) {
+            if (R == 4) launch_r<4, true>(id, S, store);
+            else launch_r<8, true>(id, S, store);
+        } else {
+            if (R == 4) launch_r<4, false>(id, S, store);
+            else launch_r<8, false>(id, S, store);
+        }
     }
 
     // the adjoint of a step: velocity nodes, then the source-side adjoint (it

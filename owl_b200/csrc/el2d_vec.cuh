@@ -27,8 +27,10 @@ __device__ __forceinline__ bool el2d_v4(const El2dDev& a, int zr0, El2dV4& c) {
     return c.x < a.x1 && c.z < a.z1;
 }
 
-template <int R, bool STORE>
-__global__ void __launch_bounds__(256) k_el2d_fwd_s4(El2dDev a) {
+// (256, 3): 80 registers, three CTAs per SM instead of two (a few bytes
+// spilled); ZR as in k_el2d_fwd_s
+template <int R, bool STORE, bool ZR>
+__global__ void __launch_bounds__(256, 3) k_el2d_fwd_s4(El2dDev a) {
     El2dV4 c;
     if (!el2d_v4(a, a.zs0, c)) return;
     const int x = c.x, z = c.z, n = c.n;
@@ -97,7 +99,7 @@ __global__ void __launch_bounds__(256) k_el2d_fwd_s4(El2dDev a) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) sz[q] = sz[q] + c_fde[k - 1] * (f4at(up, q) - f4at(dn, q));
             }
-            const float zsi = a.idz * __ldg(a.zfi + z);  // 1/dz times the row's dz scaling (refined mesh)
+            const float zsi = ZR ? a.idz * __ldg(a.zfi + z) : a.idz;  // 1/dz times the row's dz scaling
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 dzv[q] = zsi * sz[q];
@@ -150,7 +152,7 @@ __global__ void __launch_bounds__(256) k_el2d_fwd_s4(El2dDev a) {
             }
             float4 xzn, gS;
             const float4 c55 = ldg4(a.c55e + o);
-            const float zsh = a.idz * __ldg(a.zfh + z);
+            const float zsh = ZR ? a.idz * __ldg(a.zfh + z) : a.idz;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 float dzvx = zsh * szx[q], dxvz = a.idx * sxz[q];
@@ -179,8 +181,9 @@ __global__ void __launch_bounds__(256) k_el2d_fwd_s4(El2dDev a) {
     }
 }
 
-template <int R, bool STORE>
-__global__ void __launch_bounds__(256) k_el2d_fwd_v4(El2dDev a) {
+// (256, 4): 64 registers, four CTAs per SM instead of three
+template <int R, bool STORE, bool ZR>
+__global__ void __launch_bounds__(256, 4) k_el2d_fwd_v4(El2dDev a) {
     El2dV4 c;
     if (!el2d_v4(a, a.zvx0, c)) return;
     const int x = c.x, z = c.z, n = c.n;
@@ -226,7 +229,7 @@ __global__ void __launch_bounds__(256) k_el2d_fwd_v4(El2dDev a) {
             }
             float4 vn, hS;
             const float4 bx = ldg4(a.bx + o);
-            const float zsi = a.idz * __ldg(a.zfi + z);
+            const float zsi = ZR ? a.idz * __ldg(a.zfi + z) : a.idz;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 float sx = 0.f;
@@ -264,7 +267,7 @@ __global__ void __launch_bounds__(256) k_el2d_fwd_v4(El2dDev a) {
             }
             float4 vn, hS;
             const float4 bz = ldg4(a.bz + o);
-            const float zsh = a.idz * __ldg(a.zfh + z);
+            const float zsh = ZR ? a.idz * __ldg(a.zfh + z) : a.idz;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 float sx = 0.f;
