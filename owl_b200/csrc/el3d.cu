@@ -257,8 +257,9 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_s(El3dDev a) {
     const float c11 = __ldg(a.c11 + o), c12 = __ldg(a.c12 + o), c13 = __ldg(a.c13 + o), c22 = __ldg(a.c22 + o),
                 c23 = __ldg(a.c23 + o), c33 = __ldg(a.c33 + o);
     const float g44 = a.dt * __ldg(a.c44e + o), g55 = a.dt * __ldg(a.c55e + o), g66 = a.dt * __ldg(a.c66e + o);
-    // 1/dz times the plane's dz scaling (1/dz exactly on the uniform grid)
-    const float zsi = a.idz * __ldg(a.zfi + z), zsh = a.idz * __ldg(a.zfh + z);
+    // 1/dz times the plane's dz scaling (the refined mesh exists only under a
+    // free surface: the FS instances read the factors, exactly 1 on the uniform grid)
+    const float zsi = FS ? a.idz * __ldg(a.zfi + z) : a.idz, zsh = FS ? a.idz * __ldg(a.zfh + z) : a.idz;
     const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
     // free surface: row 1, whether the half-depth stresses exist at this row,
@@ -373,7 +374,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_fwd_v(El3dDev a) {
     const float ayi = a.ayi[y], byi = a.byi[y], ayh = a.ayh[y], byh = a.byh[y];
     const float azi = a.azi[z], bzi = a.bzi[z], azh = a.azh[z], bzh = a.bzh[z];
     const float bx = __ldg(a.bx + o), by = __ldg(a.by + o), bz = __ldg(a.bz + o);
-    const float zsi = a.idz * __ldg(a.zfi + z), zsh = a.idz * __ldg(a.zfh + z);  // see k_el3d_fwd_s
+    const float zsi = FS ? a.idz * __ldg(a.zfi + z) : a.idz, zsh = FS ? a.idz * __ldg(a.zfh + z) : a.idz;  // see k_el3d_fwd_s
     const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
     const long long slot = STORE ? (long long)(*a.d_step % a.k) * a.sslot : 0;
     for (int s = s0; s < s1; ++s) {
@@ -466,7 +467,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_v(El3dDev a) {
     const float bx = __ldg(a.bx + o), by = __ldg(a.by + o), bz = __ldg(a.bz + o);
     // the z-derivative e terms carry the node's dz scaling, so that the
     // neighbours' transposed stencils stay plain
-    const float fzi = __ldg(a.zfi + z), fzh = __ldg(a.zfh + z);
+    const float fzi = FS ? __ldg(a.zfi + z) : 1.f, fzh = FS ? __ldg(a.zfh + z) : 1.f;
     const int s0 = c.grp * a.spt, s1 = min(a.nshots, s0 + a.spt);
     float gx = 0.f, gy = 0.f, gz = 0.f;
     for (int s = s0; s < s1; ++s) {
@@ -564,7 +565,7 @@ __global__ void __launch_bounds__(256, MP ? 2 : 3) k_el3d_adj_s(El3dDev a) {
     const bool mir = FS && z > a.pr && z <= a.pr + a.R;
     const long long dzz = (long long)(2 * a.pr - 2 * z) * sz, dsh = dzz + sz;
     const float r13 = c13 / c33, r23 = c23 / c33;
-    const float fzi = __ldg(a.zfi + z), fzh = __ldg(a.zfh + z);  // see k_el3d_adj_v
+    const float fzi = FS ? __ldg(a.zfi + z) : 1.f, fzh = FS ? __ldg(a.zfh + z) : 1.f;  // see k_el3d_adj_v
     float G[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (int s = s0; s < s1; ++s) {
         float* ad = a.ad + s * a.sad;
