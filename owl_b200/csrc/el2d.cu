@@ -88,6 +88,7 @@ __device__ __forceinline__ float pml_e(float q, float a, float b, float psih, fl
 // grid's instances leave them out
 template <int R, bool STORE, bool ZR>
 __global__ void __maxnreg__(R == 4 ? 48 : 128) k_el2d_fwd_s(El2dDev a) {
+    pdl_prologue();  // before the first global read (launched with launch_pdl)
     const int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int z = a.zs0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
@@ -187,6 +188,7 @@ __global__ void __maxnreg__(R == 4 ? 48 : 128) k_el2d_fwd_s(El2dDev a) {
 
 template <int R, bool STORE, bool ZR>
 __global__ void __launch_bounds__(512) k_el2d_fwd_v(El2dDev a) {
+    pdl_prologue();  // before the first global read (launched with launch_pdl)
     const int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int z = a.zvx0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
@@ -271,6 +273,7 @@ __device__ __forceinline__ void kahan_g(float* G, long long gg, long long go, in
 // t (rho gradient), then the adjoint PML terms of the velocity update of step t
 template <int R, bool ZR>
 __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
+    pdl_prologue();  // before the first global read (launched with launch_pdl)
     const int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int z = a.zvx0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
@@ -353,6 +356,7 @@ __global__ void __launch_bounds__(512) k_el2d_adj_v(El2dDev a) {
 // hides more of the load latency this kernel is bound by
 template <int R, bool ZR>
 __global__ void __maxnreg__(R == 4 ? 64 : 128) k_el2d_adj_s(El2dDev a) {
+    pdl_prologue();  // before the first global read (launched with launch_pdl)
     const int x = a.x0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int z = a.zs0 + blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.x1 || z >= a.z1) return;
@@ -1104,28 +1108,28 @@ struct El2dEngine : SsgBase {
                     return dim3((NXp + 127) / 128, (rows + ty - 1) / ty, (S + spt_f - 1) / spt_f);
                 };
                 if (id == OWL_K_FWD_P) {
-                    if (store) k_el2d_fwd_s4<RR, true, ZR><<<grid(rows_s), b, 0, stream>>>(a);
-                    else k_el2d_fwd_s4<RR, false, ZR><<<grid(rows_s), b, 0, stream>>>(a);
+                    if (store) launch_pdl(k_el2d_fwd_s4<RR, true, ZR>, grid(rows_s), b, 0, stream, a);
+                    else launch_pdl(k_el2d_fwd_s4<RR, false, ZR>, grid(rows_s), b, 0, stream, a);
                 } else {
-                    if (store) k_el2d_fwd_v4<RR, true, ZR><<<grid(rows_v), b, 0, stream>>>(a);
-                    else k_el2d_fwd_v4<RR, false, ZR><<<grid(rows_v), b, 0, stream>>>(a);
+                    if (store) launch_pdl(k_el2d_fwd_v4<RR, true, ZR>, grid(rows_v), b, 0, stream, a);
+                    else launch_pdl(k_el2d_fwd_v4<RR, false, ZR>, grid(rows_v), b, 0, stream, a);
                 }
                 return;
             }
             const dim3 b(tile_x, tz_f);
             if (id == OWL_K_FWD_P) {
-                if (store) k_el2d_fwd_s<RR, true, ZR><<<grid_for(rows_s, S, spt_f, tz_f), b, 0, stream>>>(a);
-                else k_el2d_fwd_s<RR, false, ZR><<<grid_for(rows_s, S, spt_f, tz_f), b, 0, stream>>>(a);
+                if (store) launch_pdl(k_el2d_fwd_s<RR, true, ZR>, grid_for(rows_s, S, spt_f, tz_f), b, 0, stream, a);
+                else launch_pdl(k_el2d_fwd_s<RR, false, ZR>, grid_for(rows_s, S, spt_f, tz_f), b, 0, stream, a);
             } else {
-                if (store) k_el2d_fwd_v<RR, true, ZR><<<grid_for(rows_v, S, spt_f, tz_f), b, 0, stream>>>(a);
-                else k_el2d_fwd_v<RR, false, ZR><<<grid_for(rows_v, S, spt_f, tz_f), b, 0, stream>>>(a);
+                if (store) launch_pdl(k_el2d_fwd_v<RR, true, ZR>, grid_for(rows_v, S, spt_f, tz_f), b, 0, stream, a);
+                else launch_pdl(k_el2d_fwd_v<RR, false, ZR>, grid_for(rows_v, S, spt_f, tz_f), b, 0, stream, a);
             }
         } else {
             OWL_CHECK(a.ad && a.S && a.G, OWL_ERR_INVALID, "adjoint buffers not allocated");
             a.spt = spt_a;
             const dim3 b(tile_x, tz_a);
-            if (id == OWL_K_ADJ_P) k_el2d_adj_v<RR, ZR><<<grid_for(rows_v, S, spt_a, tz_a), b, 0, stream>>>(a);
-            else k_el2d_adj_s<RR, ZR><<<grid_for(rows_s, S, spt_a, tz_a), b, 0, stream>>>(a);
+            if (id == OWL_K_ADJ_P) launch_pdl(k_el2d_adj_v<RR, ZR>, grid_for(rows_v, S, spt_a, tz_a), b, 0, stream, a);
+            else launch_pdl(k_el2d_adj_s<RR, ZR>, grid_for(rows_s, S, spt_a, tz_a), b, 0, stream, a);
         }
     }
     void launch_kernel(int id, int S, bool store) override {

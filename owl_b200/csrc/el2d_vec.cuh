@@ -31,6 +31,7 @@ __device__ __forceinline__ bool el2d_v4(const El2dDev& a, int zr0, El2dV4& c) {
 // spilled); ZR as in k_el2d_fwd_s
 template <int R, bool STORE, bool ZR>
 __global__ void __launch_bounds__(256, 3) k_el2d_fwd_s4(El2dDev a) {
+    pdl_prologue();  // before the first global read (launched with launch_pdl)
     El2dV4 c;
     if (!el2d_v4(a, a.zs0, c)) return;
     const int x = c.x, z = c.z, n = c.n;
@@ -184,6 +185,7 @@ __global__ void __launch_bounds__(256, 3) k_el2d_fwd_s4(El2dDev a) {
 // (256, 4): 64 registers, four CTAs per SM instead of three
 template <int R, bool STORE, bool ZR>
 __global__ void __launch_bounds__(256, 4) k_el2d_fwd_v4(El2dDev a) {
+    pdl_prologue();  // before the first global read (launched with launch_pdl)
     El2dV4 c;
     if (!el2d_v4(a, a.zvx0, c)) return;
     const int x = c.x, z = c.z, n = c.n;
