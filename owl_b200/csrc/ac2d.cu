@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(512) k_ac2d_fwd_p(Ac2dDev a) {
         const float pn = p0 - dtbk * g;
         a.p[so] = pn;
         if (mirror) a.p[s * a.sst + omir] = -pn;
-        if (STORE) a.Sp[slot + s * a.fs + o] = g;
+        if (STORE) __stcs(a.Sp + slot + s * a.fs + o, g);  // streaming: see st4n_cs
     }
 }
 
@@ -265,7 +265,7 @@ __device__ __forceinline__ void ac2d_fwd_v_cells(const Ac2dDev& a, int cur) {
             if (FUSE && (a.pt.mode & FZ_INJ) && ac2d_inj_near(a.pt, s, 2, cx0, cx0 + blockDim.x, cz0, cz0 + blockDim.y))
                 vn = ac2d_inj(a.pt, s, 1, x, z, cur, vn);
             a.vx[so] = vn;
-            if (STORE) a.Svx[slot + s * a.fs + o] = h;
+            if (STORE) __stcs(a.Svx + slot + s * a.fs + o, h);
         }
         if (doz) {
             float sz = 0.f;
@@ -281,7 +281,7 @@ __device__ __forceinline__ void ac2d_fwd_v_cells(const Ac2dDev& a, int cur) {
             if (FUSE && (a.pt.mode & FZ_INJ) && ac2d_inj_near(a.pt, s, 4, cx0, cx0 + blockDim.x, cz0, cz0 + blockDim.y))
                 vn = ac2d_inj(a.pt, s, 2, x, z, cur, vn);
             a.vz[so] = vn;
-            if (STORE) a.Svz[slot + s * a.fs + o] = h;
+            if (STORE) __stcs(a.Svz + slot + s * a.fs + o, h);
         }
     }
 }
@@ -360,11 +360,11 @@ __device__ __forceinline__ void ac2d_adj_p_cells(const Ac2dDev& a) {
     auto load = [&](int s, Cell& L) {
         const long long sa = s * a.sad + o, ss = slot + s * a.fs + o;
         L.vx = ownx ? a.avx[sa] : 0.f;
-        L.svx = ownx ? __ldg(a.Svx + ss) : 0.f;
+        L.svx = ownx ? __ldcs(a.Svx + ss) : 0.f;
         L.vz = ownz ? a.avz[sa] : 0.f;
-        L.svz = ownz ? __ldg(a.Svz + ss) : 0.f;
+        L.svz = ownz ? __ldcs(a.Svz + ss) : 0.f;
         L.p0 = dop ? a.ap[sa] : 0.f;
-        L.sp = dop ? __ldg(a.Sp + ss) : 0.f;
+        L.sp = dop ? __ldcs(a.Sp + ss) : 0.f;
         L.m1 = dop && px ? a.am1[sa] : 0.f;
         L.m2 = dop && pz ? a.am2[sa] : 0.f;
     };

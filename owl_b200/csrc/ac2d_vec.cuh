@@ -127,7 +127,7 @@ __device__ __forceinline__ void ac2d_fwd_p4_tile(const Ac2dDev& a, uint3 b, int 
         if (anyx) st4n(a.m1 + so, m1, n);
         if (pz) st4n(a.m2 + so, m2, n);
         if (mirror) st4n(a.p + s * a.sst + omir, make_float4(-pn.x, -pn.y, -pn.z, -pn.w), n);
-        if (STORE) st4n(a.Sp + slot + s * a.fs + o, gS, n);
+        if (STORE) st4n_cs(a.Sp + slot + s * a.fs + o, gS, n);
     }
 }
 
@@ -191,7 +191,7 @@ __device__ __forceinline__ void ac2d_fwd_v4_tile(const Ac2dDev& a, uint3 b, int 
                 f4set(hS, q, h);
             }
             if (anyx) st4n(a.m3 + so, m3, n);
-            if (STORE) st4n(a.Svx + slot + s * a.fs + o, hS, n);
+            if (STORE) st4n_cs(a.Svx + slot + s * a.fs + o, hS, n);
             // force sources of step t, added to the updated cells (out of the
             // loop above, so that the calls hold no stencil values live)
             if (FUSE && injx) vn = ac2d_inj4(a.pt, s, 1, x, z, cur, vn, n);
@@ -218,7 +218,7 @@ __device__ __forceinline__ void ac2d_fwd_v4_tile(const Ac2dDev& a, uint3 b, int 
                 f4set(hS, q, h);
             }
             if (pz) st4n(a.m4 + so, m4, n);
-            if (STORE) st4n(a.Svz + slot + s * a.fs + o, hS, n);
+            if (STORE) st4n_cs(a.Svz + slot + s * a.fs + o, hS, n);
             if (FUSE && injz) vn = ac2d_inj4(a.pt, s, 2, x, z, cur, vn, n);
             st4n(a.vz + so, vn, n);
         }
@@ -276,11 +276,11 @@ __device__ __forceinline__ void ac2d_adj_p4_cells(const Ac2dDev& a) {
     auto load = [&](int s, Cell& L) {
         const long long sa = s * a.sad + o, ss = slot + s * a.fs + o;
         L.vx = ownx ? ld4(a.avx + sa) : zero;
-        L.svx = ownx ? ldg4(a.Svx + ss) : zero;
+        L.svx = ownx ? ldcs4(a.Svx + ss) : zero;
         L.vz = ownz ? ld4(a.avz + sa) : zero;
-        L.svz = ownz ? ldg4(a.Svz + ss) : zero;
+        L.svz = ownz ? ldcs4(a.Svz + ss) : zero;
         L.p0 = dop ? ld4(a.ap + sa) : zero;
-        L.sp = dop ? ldg4(a.Sp + ss) : zero;
+        L.sp = dop ? ldcs4(a.Sp + ss) : zero;
         L.m1 = dop && anyx ? ld4(a.am1 + sa) : zero;
         L.m2 = dop && pz ? ld4(a.am2 + sa) : zero;
     };

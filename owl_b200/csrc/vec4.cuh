@@ -35,4 +35,18 @@ __device__ __forceinline__ void st4n(float* p, const float4& v, int n) {
     }
 }
 
+// the same with evict-first (streaming) stores and loads, for data written once
+// and read once a segment later (the stored stencil terms): they pass through
+// L2 without displacing the wavefields that stay resident there between launches
+__device__ __forceinline__ void st4n_cs(float* p, const float4& v, int n) {
+    if (n == 4) {
+        __stcs(reinterpret_cast<float4*>(p), v);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if (c < n) __stcs(p + c, f4at(v, c));
+    }
+}
+__device__ __forceinline__ float4 ldcs4(const float* p) { return __ldcs(reinterpret_cast<const float4*>(p)); }
+
 }  // namespace owl
