@@ -893,7 +893,7 @@ struct Ac2dEngine : SsgBase {
     int num_sms = 0;
     bool run_steps_persistent(int kind, int n, int S) override {
         const char* e = std::getenv("OWL_PERSIST");
-        if (!(e && e[0] == '1' && e[1] == 0) || kind == 2 || !fuse_on || tz_f < 100 || tz_f >= 200) return false;
+        if (!(e && e[0] == '1' && e[1] == 0) || kind == 2 || !fuse_fwd || tz_f < 100 || tz_f >= 200) return false;
         if (R == 4) return persist_r<4>(kind, n, S);
         return persist_r<8>(kind, n, S);
     }

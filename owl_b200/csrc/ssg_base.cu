@@ -390,10 +390,14 @@ void SsgBase::build_tables(int S, const owl_shot* shots, bool need_sct) {
     if (hbox.empty()) { hbox.push_back(int4{-1, 0, 0, 0}); hbw.resize(boxn, 0.f); }
     inj_box.upload(hbox.data(), hbox.size(), stream);
     inj_bw.upload(hbw.data(), hbw.size(), stream);
-    // the point work inside the stencil kernels where the medium supports it;
-    // OWL_FUSE=0 keeps the separate point kernel
+    // the point work inside the stencil kernels where the medium supports it:
+    // the adjoint's residual scatter by default; OWL_FUSE=1 also the forward's
+    // injection and sampling (measured 3 % slower on the 32-shot gradient than
+    // the separate point kernel, whose one small launch per step costs less
+    // than the extra work of the stencil CTAs), OWL_FUSE=0 neither
     const char* fz = std::getenv("OWL_FUSE");
     fuse_on = fuse && !(fz && fz[0] == '0' && fz[1] == 0);
+    fuse_fwd = fuse_on && fz && fz[0] == '1' && fz[1] == 0;
 }
 
 void SsgBase::ensure_state(int S, int k, bool grad) {
@@ -428,14 +432,15 @@ PointDev SsgBase::pdev(int S, bool adjoint, bool want_src_adj) {
 // adjoint step; 3: forward step storing the stencil terms (the last segment of
 // a gradient's forward, whose recompute it replaces)
 int SsgBase::step_launches(int kind) const {
-    if (fuse_on) return kind == 2 && want_src_now ? 3 : 2;
+    if (kind == 2 && fuse_on) return want_src_now ? 3 : 2;
+    if (kind != 2 && fuse_fwd) return 2;
     if (kind == 1) return 3;
     if (kind != 2) return nb_rec <= 4 ? 3 : 4;
     return nb_sct <= 4 ? 3 : 4;
 }
 
 void SsgBase::launch_step(int kind, int S, const PointDev& q) {
-    if (fuse_on) {
+    if ((kind == 2 && fuse_on) || (kind != 2 && fuse_fwd)) {
         // the stencil kernels inject, sample / scatter and advance the step counter
         if (kind != 2) {
             fz_mode = FZ_INJ | FZ_TICK | (kind == 1 ? 0 : FZ_SMP);
@@ -498,7 +503,8 @@ void SsgBase::run_steps(int kind, int n, int S, const PointDev& q, bool graph) {
                                   (uintptr_t)sct.ptr.p, (uintptr_t)sct.w.p, (uintptr_t)sct.off.p, (uintptr_t)amp.p,
                                   (uintptr_t)inj_shot_ptr.p, (uintptr_t)rec_shot_ptr.p, (uintptr_t)sct_shot_ptr.p,
                                   (uintptr_t)q.rtot, (uintptr_t)nb_rec, (uintptr_t)nb_sct, (uintptr_t)inj_box.p,
-                                  (uintptr_t)inj_bw.p, (uintptr_t)fuse_on, (uintptr_t)want_src_now};
+                                  (uintptr_t)inj_bw.p, (uintptr_t)fuse_on, (uintptr_t)fuse_fwd,
+                                  (uintptr_t)want_src_now};
     if (!gc.exec || gc.sig != sig) {
         gc.reset();
         cudaGraph_t g;
@@ -651,7 +657,7 @@ void SsgBase::autotune(int S, int k, bool grad) {
                 // buffer does not exist yet: its stencil kernels are timed alone
                 auto run = [&]() {
                     if (pass == 0) {
-                        fz_mode = fuse_on ? FZ_INJ : 0;
+                        fz_mode = fuse_fwd ? FZ_INJ : 0;
                         launch_kernel(OWL_K_FWD_P, S, false);
                         launch_kernel(OWL_K_FWD_V, S, false);
                     } else {
@@ -1137,7 +1143,7 @@ void SsgBase::kernel_time(int id, int nlaunch, double* avg_ms, double* bytes) {
               OWL_ERR_INVALID, "adjoint kernels and store variants need a gradient call first");
     set_step(cur_k);
     // the variant the time loop launches, without advancing the step counter
-    const int fz = fuse_on ? (kid < OWL_K_ADJ_P ? FZ_INJ : FZ_SCT) : 0;
+    const int fz = kid < OWL_K_ADJ_P ? (fuse_fwd ? FZ_INJ : 0) : (fuse_on ? FZ_SCT : 0);
     fz_mode = fz;
     for (int i = 0; i < 3; ++i) launch_kernel(kid, S, store);
     OWL_LAUNCH_CHECK();

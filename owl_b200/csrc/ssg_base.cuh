@@ -103,6 +103,7 @@ struct SsgBase : Engine {
     // then on every other field (2D media)
     DevBuf<int4> inj_bbox;
     bool fuse_on = false;  // this batch's point work runs inside the stencil kernels
+    bool fuse_fwd = false; // ... in the forward steps too (else only the adjoint's residual scatter)
     int inj_fmask = 0;     // fields the batch's sources inject into (bit f: field f)
     bool want_src_now = false;  // the adjoint sweep records the source-side adjoint
     int fz_mode = 0;       // FZ_* work of the next stencil launches

@@ -170,8 +170,10 @@ def test_unstable_dt_rejected():
 @pytest.mark.parametrize("fs", [0, 1])
 def test_fused_point_work_matches_point_kernels(fs, tz):
     """Injection, sampling and the residual scatter inside the stencil kernels
-    (OWL_FUSE=0) to the bit: explosion and force sources, two overlapping
-    sources in one shot, off-grid receivers sharing taps, a zero-weight trace."""
+    (OWL_FUSE=1), the residual scatter alone (the default), and the separate
+    point kernel (OWL_FUSE=0) agree to the bit: explosion and force sources,
+    two overlapping sources in one shot, off-grid receivers sharing taps, a
+    zero-weight trace."""
     import os
     nx, nz, dx, dt, nt = 48, 40, 10.0, 1e-3, 300
     d = desc(nx, nz, dx, dt, nt, fs=fs)
@@ -180,9 +182,9 @@ def test_fused_point_work_matches_point_kernels(fs, tz):
     obs = oracle.ac2d_forward(d, vp, rho, ps, "f64").astype(np.float32)
     s = make_solver(d, vp * np.float32(1.02), rho)
     out = {}
-    for off in (False, True):
-        if off:
-            os.environ["OWL_FUSE"] = "0"
+    for mode in ("1", None, "0"):
+        if mode is not None:
+            os.environ["OWL_FUSE"] = mode
         try:
             seis = s.forward(ps, RunOpts(tile_z=tz))
             mf, g = s.gradient(ps, obs, L.OWL_ADJ_L2_RESIDUAL, RunOpts(checkpoint_interval=40, tile_z=tz))
@@ -190,10 +192,12 @@ def test_fused_point_work_matches_point_kernels(fs, tz):
             gs = s.source_gradient(ps, obs, RunOpts(checkpoint_interval=40, tile_z=tz))
         finally:
             os.environ.pop("OWL_FUSE", None)
-        out[off] = (seis, mf, g, gs, launches)
-    for a, b in zip(out[False][:4], out[True][:4]):
-        assert np.array_equal(np.asarray(a), np.asarray(b))
-    assert out[False][4] < out[True][4]  # fewer launches with the fused point work
+        out[mode] = (seis, mf, g, gs, launches)
+    for m in (None, "0"):
+        for a, b in zip(out["1"][:4], out[m][:4]):
+            assert np.array_equal(np.asarray(a), np.asarray(b))
+    # fewer launches the more point work the stencil kernels take
+    assert out["1"][4] < out[None][4] < out["0"][4]
 
 
 @pytest.mark.parametrize("fs", [0, 1])
@@ -211,6 +215,7 @@ def test_persistent_forward_segments_match_step_launches(fs):
     obs = oracle.ac2d_forward(d, vp, rho, ps, "f64").astype(np.float32)
     s = make_solver(d, vp * np.float32(1.02), rho)
     out = {}
+    os.environ["OWL_FUSE"] = "1"  # the persistent segments carry the forward's point work
     for persist in (False, True):
         if persist:
             os.environ["OWL_PERSIST"] = "1"
@@ -222,6 +227,8 @@ def test_persistent_forward_segments_match_step_launches(fs):
             launches = s.last_info.gpu_launches
         finally:
             os.environ.pop("OWL_PERSIST", None)
+            if persist:
+                os.environ.pop("OWL_FUSE", None)
         out[persist] = (seis, mf, g, mf2, g2, launches)
     for a, b in zip(out[False][:5], out[True][:5]):
         assert np.array_equal(np.asarray(a), np.asarray(b))
@@ -241,6 +248,7 @@ def test_persistent_barrier_wait_runs_out():
     s = make_solver(d, vp, rho)
     ref = s.forward(ps, RunOpts(tile_z=104))
     os.environ["OWL_PERSIST"] = "1"
+    os.environ["OWL_FUSE"] = "1"
     try:
         os.environ["OWL_PERSIST_STALL"] = "1"
         try:
@@ -252,6 +260,7 @@ def test_persistent_barrier_wait_runs_out():
         got = s.forward(ps, RunOpts(tile_z=104))
     finally:
         os.environ.pop("OWL_PERSIST", None)
+        os.environ.pop("OWL_FUSE", None)
     assert np.array_equal(got, ref)
 
 
