@@ -196,8 +196,10 @@ def test_fused_point_work_matches_point_kernels(fs, tz):
     for m in (None, "0"):
         for a, b in zip(out["1"][:4], out[m][:4]):
             assert np.array_equal(np.asarray(a), np.asarray(b))
-    # fewer launches the more point work the stencil kernels take
-    assert out["1"][4] < out[None][4] < out["0"][4]
+    # fewer launches the more point work the stencil kernels take (the adjoint
+    # steps of this case keep a point launch for the force source's rho term,
+    # so fusing their residual scatter saves none)
+    assert out["1"][4] < out[None][4] <= out["0"][4]
 
 
 @pytest.mark.parametrize("fs", [0, 1])
